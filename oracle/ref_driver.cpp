@@ -1,0 +1,205 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- driver for the reference compiled in place
+ * (oracle/Makefile, target _ref/nova_ref).  It builds the reference's Mesh,
+ * Field, poisson objects exactly as app/TG_Piosson/TG.cpp and
+ * app/OT_Poisson/OT.cpp do, then runs the reference's own loop bodies
+ * (app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H) for the literal
+ * mode, or the same loop with the stage state refreshed for the classical
+ * RK4 mode.  I/O is raw little-endian float64 in the Field<T> layout.
+ *
+ *   nova_ref run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U.bin> <B.bin|-> <out>
+ *   nova_ref ops <case> <nu> <U.bin> <s.bin> <out>
+ *
+ * <case> holds `mesh` and the BC files (UBC, pBC, BBC, pBBC).
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "Field/Field.h"
+#include "BC/BC.h"
+#include "Time/Time.h"
+#include "Tools/Tools.h"
+#include "Types/vector/vector.h"
+#include "ex/curl/curl.h"
+#include "ex/div/div.h"
+#include "ex/grad/grad.h"
+#include "ex/laplacian/laplacian.h"
+#include "parallelCom/parallelCom.h"
+#include "poisson/poisson.h"
+#include "settings/settings.h"
+
+template <class T> static void load(Field<T> &f, const std::string &path)
+{
+    FILE *fp = std::fopen(path.c_str(), "rb");
+    if (!fp) { std::fprintf(stderr, "cannot open %s\n", path.c_str()); std::exit(2); }
+    size_t n = (size_t)f.ni() * f.nj() * f.nk();
+    if (std::fread(f.ptr(), sizeof(T), n, fp) != n) { std::fprintf(stderr, "short read %s\n", path.c_str()); std::exit(2); }
+    std::fclose(fp);
+}
+
+template <class T> static void save(const Field<T> &f, const std::string &path)
+{
+    FILE *fp = std::fopen(path.c_str(), "wb");
+    if (!fp) { std::fprintf(stderr, "cannot write %s\n", path.c_str()); std::exit(2); }
+    size_t n = (size_t)f.ni() * f.nj() * f.nk();
+    std::fwrite(f.ptr(), sizeof(T), n, fp);
+    std::fclose(fp);
+}
+
+/* app/TG_Piosson/TG.cpp:148-166 */
+static double ek_mean(const Mesh &mesh, const Field<vector> &U)
+{
+    scalar Ek = 0.0;
+    int n = 0;
+    for (int i = settings::m() / 2; i < mesh.ni() - settings::m() / 2 - 1; i++)
+        for (int j = settings::m() / 2; j < mesh.nj() - settings::m() / 2 - 1; j++)
+            for (int k = settings::m() / 2; k < mesh.nk() - settings::m() / 2 - 1; k++) {
+                Ek += 0.5 * (U(i, j, k).x() * U(i, j, k).x() + U(i, j, k).y() * U(i, j, k).y()
+                             + U(i, j, k).z() * U(i, j, k).z());
+                n++;
+            }
+    return Ek / n;
+}
+
+static int run(int argc, char **argv)
+{
+    if (argc < 12) { std::fprintf(stderr, "usage: run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U> <B|-> <out>\n"); return 2; }
+    settings::zoneName() = argv[2];
+    const bool mhd = std::string(argv[3]) == "mhd";
+    const bool classical = std::string(argv[4]) == "classical";
+    const int nsteps = std::atoi(argv[5]);
+    const double dt = std::atof(argv[6]);
+    const scalar mu = std::atof(argv[7]);
+    const scalar eta = std::atof(argv[8]);
+    const std::string inU = argv[9], inB = argv[10], out = argv[11];
+
+    Time time(dt, dt * (nsteps + 0.5), 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+
+    Field<vector> U(mesh, vector(0, 0, 0), "U");
+    Field<vector> Ustar(mesh, vector(0, 0, 0), "U");
+    Field<vector> B(mesh, vector(0, 0, 0), "B");
+    Field<vector> Bstar(mesh, vector(0, 0, 0), "B");
+    Field<vector> J(mesh, vector(0, 0, 0), "B");
+    std::shared_ptr<Field<scalar> > p_ptr(std::make_shared<Field<scalar> >(mesh, 0, "p"));
+    auto &p = (*p_ptr);
+    std::shared_ptr<Field<scalar> > pB_ptr(std::make_shared<Field<scalar> >(mesh, 0, "pB"));
+    auto &pB = (*pB_ptr);
+    /* never destroyed: poisson::~poisson frees memory it does not own */
+    poisson &pEqn = *new poisson(p_ptr);
+    poisson &pBEqn = *new poisson(pB_ptr);
+
+    load(U, inU);
+    U.correctBoundaryConditions();
+    p.correctBoundaryConditions();
+    if (mhd) {
+        load(B, inB);
+        B.correctBoundaryConditions();
+        pB.correctBoundaryConditions();
+    }
+
+    std::vector<double> hist;
+    for (int step = 0; step < nsteps; step++) {
+        time++;
+        if (!mhd && !classical) {
+#include "TG_Piosson/RKLoop.H"
+        } else if (mhd && !classical) {
+#include "OT_Poisson/UEqn.H"
+#include "OT_Poisson/BEqn.H"
+        } else {
+            /* RKLoop.H / UEqn.H with U = Ustar refreshed per stage (the pattern of OT_Poisson/BEqn.H:86-87) */
+            std::array<std::shared_ptr<Field<vector> >, 4> dU;
+            for (int i = 0; i < 4; i++) {
+                reuseTmp<vector> dUt(mesh);
+                dU[i] = dUt();
+            }
+            reuseTmp<vector> UOldt(mesh);
+            std::shared_ptr<Field<vector> > UOld(UOldt());
+            *UOld = U;
+            for (int rk = 0; rk < 4; rk++) {
+                if (mhd)
+                    dU[rk] = time.dt() * (-ex::div(U, U) + ex::laplacian(mu, U) + ex::div(B, B) - ex::grad(0.5 * (B & B)));
+                else
+                    dU[rk] = time.dt() * (-ex::div(U, U) + ex::laplacian(mu, U));
+                Ustar = UOld;
+                for (int j = 0; j <= rk; j++) Ustar = Ustar + settings::RK4a()[rk][j] * dU[j];
+                U = Ustar;
+                U.correctBoundaryConditions();
+            }
+            Ustar.correctBoundaryConditions();
+            pEqn.rhs(ex::div(Ustar) / time.dt());
+            pEqn.solve();
+            p.correctBoundaryConditions();
+            U = Ustar - time.dt() * ex::grad(p);
+            U.correctBoundaryConditions();
+            if (mhd) {
+#include "OT_Poisson/BEqn.H"
+            }
+        }
+        double row[6] = {double(step + 1), time.curTime(), ek_mean(mesh, U), mhd ? ek_mean(mesh, B) : 0.0, 0.0, 0.0};
+        {
+            auto d = ex::div(U);
+            row[4] = tools::maximum(d);
+        }
+        if (mhd) {
+            auto d = ex::div(B);
+            row[5] = tools::maximum(d);
+        }
+        hist.insert(hist.end(), row, row + 6);
+    }
+
+    save(U, out + "_U.bin");
+    save(p, out + "_p.bin");
+    if (mhd) {
+        save(B, out + "_B.bin");
+        save(pB, out + "_pB.bin");
+    }
+    FILE *fp = std::fopen((out + "_hist.bin").c_str(), "wb");
+    std::fwrite(hist.data(), sizeof(double), hist.size(), fp);
+    std::fclose(fp);
+    return 0;
+}
+
+static int ops(int argc, char **argv)
+{
+    if (argc < 7) { std::fprintf(stderr, "usage: ops <case> <nu> <U> <s> <out>\n"); return 2; }
+    settings::zoneName() = argv[2];
+    const scalar nu = std::atof(argv[3]);
+    const std::string out = argv[6];
+    Time time(0.01, 1.0, 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+    Field<vector> U(mesh, vector(0, 0, 0), "U");
+    std::shared_ptr<Field<scalar> > s_ptr(std::make_shared<Field<scalar> >(mesh, 0, "p"));
+    auto &s = *s_ptr;
+    std::shared_ptr<Field<scalar> > p_ptr(std::make_shared<Field<scalar> >(mesh, 0, "p"));
+    poisson &pEqn = *new poisson(p_ptr);
+    load(U, argv[4]);
+    load(s, argv[5]);
+
+    save(*ex::grad(s), out + "_grad_s.bin");
+    save(*ex::div(U), out + "_div_v.bin");
+    save(*ex::div(U, U), out + "_div_vv.bin");
+    save(*ex::div(U, s), out + "_div_vs.bin");
+    save(*ex::laplacian(nu, U), out + "_lap_v.bin");
+    save(*ex::laplacian(nu, s), out + "_lap_s.bin");
+    save(*ex::curl(U), out + "_curl.bin");
+    pEqn.rhs(s_ptr);
+    pEqn.solve();
+    save(*p_ptr, out + "_poisson.bin");
+    return 0;
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops ...\n"); return 2; }
+    std::string mode = argv[1];
+    if (mode == "run") return run(argc, argv);
+    if (mode == "ops") return ops(argc, argv);
+    std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
+    return 2;
+}
