@@ -1,0 +1,279 @@
+// nova.hpp -- header-only C++ adapter over include/nova_gpu.h that keeps the
+// reference's host API: Mesh(file), Field<scalar>/Field<vector> with the
+// ghosted array-of-structs storage of src/Field/Field.h:56-157,
+// correctBoundaryConditions(), ex::grad/div/curl/laplacian returning
+// std::shared_ptr<Field<T>> (src/ex/*/ *.h), poisson(p).rhs(f).solve()
+// (src/poisson/poisson.h:36-115) and tools::maximum (src/Tools/Tools.h:19-36).
+// Each call runs on the GPU through the C ABI; host Fields are the caller's
+// buffers in the reference layout, uploaded and downloaded per call.  The
+// fused path replaces a whole loop body (RKLoop.H / UEqn.H + BEqn.H) with
+// nova::Advance, which keeps the state resident on the device.
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nova_gpu.h"
+
+namespace nova {
+
+typedef double scalar;
+
+// layout-compatible with the reference's vector (scalar v_[3], src/Types/vector/vector.h:24)
+struct vector {
+    scalar v_[3];
+    vector() : v_{0, 0, 0} {}
+    vector(scalar a, scalar b, scalar c) : v_{a, b, c} {}
+    scalar &x() { return v_[0]; }
+    scalar &y() { return v_[1]; }
+    scalar &z() { return v_[2]; }
+    scalar x() const { return v_[0]; }
+    scalar y() const { return v_[1]; }
+    scalar z() const { return v_[2]; }
+    scalar &operator[](int d) { return v_[d]; }
+};
+
+template <class T> struct nComp;
+template <> struct nComp<scalar> { static constexpr int value = 1; };
+template <> struct nComp<vector> { static constexpr int value = 3; };
+
+class Error : public std::runtime_error {
+public:
+    nova_status status;
+    Error(nova_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check(nova_ctx *ctx, nova_status s, const char *what)
+{
+    if (s != NOVA_OK) throw Error(s, std::string(what) + ": " + (ctx ? nova_last_error(ctx) : "no context"));
+}
+
+// Mesh(std::string file): reads "origin:", "N:", "L:", "hypz:" (src/Mesh/Mesh.cpp:38-62)
+class Mesh {
+    std::shared_ptr<nova_ctx> ctx_;
+    nova_mesh_desc d_{};
+    int n_[3] = {0, 0, 0};
+
+public:
+    explicit Mesh(const nova_mesh_desc &d) : d_(d) { init(); }
+    Mesh(const std::string &file, int m = 6)
+    {
+        std::ifstream fin(file);
+        if (!fin) throw Error(NOVA_E_INVALID, "cannot open mesh file " + file);
+        std::string line;
+        d_.m = m;
+        while (std::getline(fin, line)) {
+            std::stringstream sp(line);
+            std::string key;
+            sp >> key;
+            if (key == "origin:") sp >> d_.origin[0] >> d_.origin[1] >> d_.origin[2];
+            else if (key == "N:") sp >> d_.N[0] >> d_.N[1] >> d_.N[2];
+            else if (key == "L:") sp >> d_.L[0] >> d_.L[1] >> d_.L[2];
+            else if (key == "hypz:") { d_.hyperbolic_z = 1; sp >> d_.s1 >> d_.s2; }
+        }
+        init();
+    }
+    void init()
+    {
+        nova_ctx *c = nullptr;
+        check(nullptr, nova_create(&d_, &c), "nova_create");
+        ctx_.reset(c, [](nova_ctx *p) { nova_destroy(p); });
+        check(c, nova_mesh_local_n(c, n_), "nova_mesh_local_n");
+    }
+    nova_ctx *ctx() const { return ctx_.get(); }
+    int ni() const { return n_[0]; }
+    int nj() const { return n_[1]; }
+    int nk() const { return n_[2]; }
+    const int *local_n() const { return n_; }
+    scalar dx() const { return d_.L[0] / d_.N[0]; }
+    scalar dy() const { return d_.L[1] / d_.N[1]; }
+    scalar dz() const { return d_.L[2] / d_.N[2]; }
+    int m() const { return d_.m; }
+    const nova_mesh_desc &desc() const { return d_; }
+};
+
+// Host field in the reference layout plus its device mirror.
+template <class T> class Field {
+    Mesh mesh_;
+    std::vector<T> v_;
+    std::shared_ptr<nova_field> dev_;
+
+public:
+    explicit Field(const Mesh &m, const T &val = T()) : mesh_(m), v_((size_t)m.ni() * m.nj() * m.nk(), val)
+    {
+        nova_field *f = nullptr;
+        check(mesh_.ctx(), nova_field_create(mesh_.ctx(), nComp<T>::value, NOVA_F64, &f), "nova_field_create");
+        Mesh keep = mesh_;
+        dev_.reset(f, [keep](nova_field *p) { nova_field_destroy(keep.ctx(), p); });
+    }
+    int index(int i, int j, int k) const { return k + j * mesh_.nk() + i * (mesh_.nk() * mesh_.nj()); }
+    T &operator()(int i, int j, int k) { return v_[index(i, j, k)]; }
+    const T &operator()(int i, int j, int k) const { return v_[index(i, j, k)]; }
+    T *ptr() { return v_.data(); }
+    const T *ptr() const { return v_.data(); }
+    const Mesh &mesh() const { return mesh_; }
+    int ni() const { return mesh_.ni(); }
+    int nj() const { return mesh_.nj(); }
+    int nk() const { return mesh_.nk(); }
+    nova_field *dev() const { return dev_.get(); }
+
+    void toDevice() const
+    {
+        check(mesh_.ctx(), nova_field_upload(mesh_.ctx(), dev_.get(), (const double *)v_.data(), mesh_.local_n()),
+              "nova_field_upload");
+    }
+    // device -> host, ghosts and the duplicate periodic node filled (periodic)
+    void fromDevice()
+    {
+        check(mesh_.ctx(), nova_field_download(mesh_.ctx(), dev_.get(), (double *)v_.data(), mesh_.local_n(), nullptr),
+              "nova_field_download");
+    }
+    // periodicBC::update on every face: a round trip through the device ghost synthesis
+    void correctBoundaryConditions()
+    {
+        toDevice();
+        fromDevice();
+    }
+};
+
+namespace ex {
+
+inline std::shared_ptr<Field<vector>> grad(const Field<scalar> &f)
+{
+    auto out = std::make_shared<Field<vector>>(f.mesh());
+    f.toDevice();
+    check(f.mesh().ctx(), nova_grad_s(f.mesh().ctx(), f.dev(), out->dev()), "nova_grad_s");
+    out->fromDevice();
+    return out;
+}
+
+inline std::shared_ptr<Field<scalar>> div(const Field<vector> &U)
+{
+    auto out = std::make_shared<Field<scalar>>(U.mesh());
+    U.toDevice();
+    check(U.mesh().ctx(), nova_div_v(U.mesh().ctx(), U.dev(), out->dev()), "nova_div_v");
+    out->fromDevice();
+    return out;
+}
+
+template <class T> std::shared_ptr<Field<T>> div(const Field<vector> &U, const Field<T> &f)
+{
+    auto out = std::make_shared<Field<T>>(U.mesh());
+    U.toDevice();
+    f.toDevice();
+    check(U.mesh().ctx(), nova_div_vf(U.mesh().ctx(), U.dev(), f.dev(), out->dev()), "nova_div_vf");
+    out->fromDevice();
+    return out;
+}
+
+inline std::shared_ptr<Field<vector>> curl(const Field<vector> &U)
+{
+    auto out = std::make_shared<Field<vector>>(U.mesh());
+    U.toDevice();
+    check(U.mesh().ctx(), nova_curl(U.mesh().ctx(), U.dev(), out->dev()), "nova_curl");
+    out->fromDevice();
+    return out;
+}
+
+template <class T> std::shared_ptr<Field<T>> laplacian(const scalar &nu, const Field<T> &f)
+{
+    auto out = std::make_shared<Field<T>>(f.mesh());
+    f.toDevice();
+    check(f.mesh().ctx(), nova_laplacian(f.mesh().ctx(), nu, f.dev(), out->dev()), "nova_laplacian");
+    out->fromDevice();
+    return out;
+}
+
+}  // namespace ex
+
+// poisson(p): rhs(f); solve() writes p's unique nodes (src/poisson/poisson.cpp:167-265)
+class poisson {
+    std::shared_ptr<Field<scalar>> p_;
+    std::shared_ptr<Field<scalar>> rhs_;
+
+public:
+    explicit poisson(std::shared_ptr<Field<scalar>> p) : p_(std::move(p)) {}
+    void rhs(std::shared_ptr<Field<scalar>> f) { rhs_ = std::move(f); }
+    void solve()
+    {
+        rhs_->toDevice();
+        check(p_->mesh().ctx(), nova_poisson_solve(p_->mesh().ctx(), rhs_->dev(), p_->dev()), "nova_poisson_solve");
+        p_->fromDevice();
+    }
+};
+
+namespace tools {
+inline scalar maximum(const std::shared_ptr<Field<scalar>> &f)
+{
+    f->toDevice();
+    double v = 0.0;
+    check(f->mesh().ctx(), nova_field_maxabs(f->mesh().ctx(), f->dev(), &v), "nova_field_maxabs");
+    return v;
+}
+}  // namespace tools
+
+// The fused loop body: state resident on the device between calls.
+class Advance {
+    Mesh mesh_;
+    nova_run_desc rd_{};
+    std::shared_ptr<nova_field> U_, p_, B_, pB_;
+
+    std::shared_ptr<nova_field> make(int nc, int prec)
+    {
+        nova_field *f = nullptr;
+        check(mesh_.ctx(), nova_field_create(mesh_.ctx(), nc, prec, &f), "nova_field_create");
+        Mesh keep = mesh_;
+        return std::shared_ptr<nova_field>(f, [keep](nova_field *p) { nova_field_destroy(keep.ctx(), p); });
+    }
+
+public:
+    Advance(const Mesh &m, const nova_run_desc &rd) : mesh_(m), rd_(rd)
+    {
+        U_ = make(3, rd.precision);
+        p_ = make(1, NOVA_F64);
+        if (rd.model == NOVA_MODEL_MHD) {
+            B_ = make(3, rd.precision);
+            pB_ = make(1, NOVA_F64);
+        }
+    }
+    void setU(const Field<vector> &U)
+    {
+        check(mesh_.ctx(), nova_field_upload(mesh_.ctx(), U_.get(), (const double *)U.ptr(), mesh_.local_n()), "upload U");
+    }
+    void setB(const Field<vector> &B)
+    {
+        check(mesh_.ctx(), nova_field_upload(mesh_.ctx(), B_.get(), (const double *)B.ptr(), mesh_.local_n()), "upload B");
+    }
+    // run nsteps; returns the diagnostics history (nsteps rows of NOVA_HIST_COLS)
+    std::vector<double> run(int nsteps)
+    {
+        std::vector<double> hist((size_t)nsteps * NOVA_HIST_COLS, 0.0);
+        nova_state st{U_.get(), p_.get(), B_.get(), pB_.get()};
+        check(mesh_.ctx(), nova_advance(mesh_.ctx(), &rd_, &st, nsteps, hist.data()), "nova_advance");
+        rd_.t0 += nsteps * rd_.dt;
+        return hist;
+    }
+    void getU(Field<vector> &U) const
+    {
+        check(mesh_.ctx(), nova_field_download(mesh_.ctx(), U_.get(), (double *)U.ptr(), mesh_.local_n(), nullptr),
+              "download U");
+    }
+    void getB(Field<vector> &B) const
+    {
+        check(mesh_.ctx(), nova_field_download(mesh_.ctx(), B_.get(), (double *)B.ptr(), mesh_.local_n(), nullptr),
+              "download B");
+    }
+    void getp(Field<scalar> &p) const
+    {
+        check(mesh_.ctx(), nova_field_download(mesh_.ctx(), p_.get(), (double *)p.ptr(), mesh_.local_n(), nullptr),
+              "download p");
+    }
+};
+
+}  // namespace nova

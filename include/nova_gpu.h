@@ -1,0 +1,153 @@
+/*
+ * nova_gpu.h -- C ABI of the B200 explicit time advance for NOVA.
+ *
+ * Plain C types only: opaque handles, pointers and sizes.  Every entry point
+ * returns a nova_status; nova_last_error(ctx) gives the message of the last
+ * failure on that context.  A context owns one CUDA stream (or uses the one
+ * given to nova_set_stream) and all device memory it allocates; calls are
+ * synchronous at the ABI unless documented otherwise.  A context is not
+ * thread-safe, like the reference's one-thread-per-rank model.
+ *
+ * Reference interfaces replaced (paths inside the NOVA source tree):
+ *   Mesh(std::string, Time&)                  src/Mesh/Mesh.cpp:24-179   -> nova_create
+ *   Field<T>(Mesh&, const T&, std::string)    src/Field/Field.hxx:84-101 -> nova_field_create
+ *   Field<T>::ptr() data / correctBoundaryConditions()
+ *                                             src/Field/Field.h:98-101, Field.hxx:310-401
+ *                                                        -> nova_field_upload / nova_field_download
+ *   ex::grad(const Field<scalar>&)            src/ex/grad/grad.h:37-40     -> nova_grad_s
+ *   ex::grad(const Field<vector>&)            src/ex/grad/grad.h:43-46     -> nova_grad_v
+ *   ex::div(const Field<vector>&)             src/ex/div/div.h (div.hxx:22-81)  -> nova_div_v
+ *   ex::div(const Field<vector>&, const Field<T>&)
+ *                                             src/ex/div/div.h (div.hxx:84-172) -> nova_div_vf
+ *   ex::curl(const Field<vector>&)            src/ex/curl/curl.h:35-43     -> nova_curl
+ *   ex::laplacian(const scalar&, const Field<T>&)
+ *                                             src/ex/laplacian/laplacian.h (laplacian.hxx:130-191)
+ *                                                        -> nova_laplacian
+ *   poisson::rhs(...) + poisson::solve()      src/poisson/poisson.h:111-113 -> nova_poisson_solve
+ *   tools::maximum(shared_ptr<Field<T>>)      src/Tools/Tools.h:19-36      -> nova_field_maxabs
+ *   the loop bodies app/TG_Piosson/RKLoop.H:1-54, app/OT_Poisson/UEqn.H:1-54 and
+ *   app/OT_Poisson/BEqn.H:1-110 (one time step each)           -> nova_advance
+ */
+#ifndef NOVA_GPU_H
+#define NOVA_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NOVA_OK = 0,
+    NOVA_E_INVALID = 1,     /* bad argument (sizes, null pointers, mismatched fields) */
+    NOVA_E_CUDA = 2,        /* a CUDA or cuFFT call failed */
+    NOVA_E_OOM = 3,         /* device allocation failed */
+    NOVA_E_NONFINITE = 4,   /* a diagnostic reduction saw NaN/Inf in the state */
+    NOVA_E_TIMEOUT = 5,     /* reserved: a bounded device wait gave up */
+    NOVA_E_UNSUPPORTED = 6  /* valid request this build does not implement */
+} nova_status;
+
+typedef enum {
+    NOVA_F64 = 0,       /* FP64 storage and arithmetic */
+    NOVA_F32SPLIT = 1   /* FP32 stencils/storage, state kept as a (hi, lo) float pair */
+} nova_precision;
+
+typedef enum { NOVA_BC_PERIODIC = 0, NOVA_BC_NEUMANN = 1, NOVA_BC_DIRICHLET = 2 } nova_bc_type;
+
+/* Face order of the reference's BC files (src/BC/BCenums.h:8). */
+typedef enum { NOVA_NORTH = 0, NOVA_SOUTH, NOVA_EAST, NOVA_WEST, NOVA_TOP, NOVA_BOTTOM } nova_face;
+
+typedef struct nova_ctx nova_ctx;
+typedef struct nova_field nova_field;
+
+/* Mesh file contents (src/Mesh/Mesh.cpp:38-62) plus settings::m_. */
+typedef struct {
+    int N[3];            /* "N:"  intervals per axis (global; one GPU holds all of them) */
+    double L[3];         /* "L:"  domain lengths */
+    double origin[3];    /* "origin:" */
+    int m;               /* stencil order 2, 4, 6 or 8 (settings::m_, default 6) */
+    int hyperbolic_z;    /* "hypz:" present */
+    double s1, s2;       /* "hypz:" arguments */
+} nova_mesh_desc;
+
+/* BC lines "<face> <type> <val> <comp>" (src/Field/Field.hxx:519-547), index face + 6*comp. */
+typedef struct {
+    int type[18];
+    double val[18];
+} nova_bc;
+
+typedef enum { NOVA_MODEL_NS = 0, NOVA_MODEL_MHD = 1 } nova_model;
+typedef enum { NOVA_RK_LITERAL = 0, NOVA_RK_CLASSICAL = 1 } nova_rk_mode;
+
+/* One nova_advance call = nsteps of the reference's per-step loop body. */
+typedef struct {
+    int model;        /* nova_model: NS = app/TG_Piosson, MHD = app/OT_Poisson */
+    int rk_mode;      /* nova_rk_mode: LITERAL keeps the reference's stage loop as written
+                         (U not refreshed between stages), CLASSICAL refreshes it (RK4) */
+    int precision;    /* nova_precision of the state fields */
+    int diag_every;   /* diagnostics row every diag_every steps (0 = none) */
+    double dt, nu, eta;
+    double t0;        /* time of the state on entry (only reported in the history) */
+} nova_run_desc;
+
+/* Fields advanced by nova_advance.  U (3 comps) and p (1) always; B, pB for MHD. */
+typedef struct {
+    nova_field *U, *p, *B, *pB;
+} nova_state;
+
+#define NOVA_HIST_COLS 6 /* step, t, Ek, Em, max|div U|, max|div B| */
+
+/* ---- context ---- */
+nova_status nova_create(const nova_mesh_desc *mesh, nova_ctx **out);
+nova_status nova_destroy(nova_ctx *ctx);
+const char *nova_last_error(const nova_ctx *ctx);
+nova_status nova_set_stream(nova_ctx *ctx, void *cuda_stream);   /* cudaStream_t; NULL = own stream */
+nova_status nova_synchronize(nova_ctx *ctx);
+/* local ghosted sizes N+1+m of the reference Field layout */
+nova_status nova_mesh_local_n(const nova_ctx *ctx, int local_n[3]);
+/* Mesh::dzdxi_ / d2zdxi2_ (length local_n[2]), as the reference computes them */
+nova_status nova_mesh_metrics(const nova_ctx *ctx, double *dzdxi, double *d2zdxi2);
+
+/* ---- fields ---- */
+nova_status nova_field_create(nova_ctx *ctx, int ncomp, int precision, nova_field **out);
+nova_status nova_field_destroy(nova_ctx *ctx, nova_field *f);
+/* Reference Field<T>::ptr() layout: ghosted, AoS, z fastest, local_n = N+1+m per axis.
+ * Upload reads the N0*N1*N2 unique interior nodes; download writes the interior
+ * (incl. the duplicate node) and fills the ghosts per `bc` (NULL = all periodic). */
+nova_status nova_field_upload(nova_ctx *ctx, nova_field *f, const double *host_aos, const int local_n[3]);
+nova_status nova_field_download(nova_ctx *ctx, const nova_field *f, double *host_aos, const int local_n[3],
+                                const nova_bc *bc);
+/* Device-native layout: component-major, unique points, z fastest: [c][i][j][k], float64. */
+nova_status nova_field_upload_soa(nova_ctx *ctx, nova_field *f, const double *host_soa);
+nova_status nova_field_download_soa(nova_ctx *ctx, const nova_field *f, double *host_soa);
+/* Same, from/to device memory the caller owns (e.g. a torch tensor). */
+nova_status nova_field_copy_from_device(nova_ctx *ctx, nova_field *f, const double *dev_soa);
+nova_status nova_field_copy_to_device(nova_ctx *ctx, const nova_field *f, double *dev_soa);
+
+/* ---- ex:: operators (one call each; out must have the right ncomp) ---- */
+nova_status nova_grad_s(nova_ctx *ctx, const nova_field *s, nova_field *out);          /* 1 -> 3 */
+nova_status nova_grad_v(nova_ctx *ctx, const nova_field *U, nova_field *out);          /* 3 -> 9 */
+nova_status nova_curl(nova_ctx *ctx, const nova_field *U, nova_field *out);            /* 3 -> 3 */
+nova_status nova_div_v(nova_ctx *ctx, const nova_field *U, nova_field *out);           /* 3 -> 1 */
+nova_status nova_div_vf(nova_ctx *ctx, const nova_field *U, const nova_field *f, nova_field *out);
+nova_status nova_laplacian(nova_ctx *ctx, double nu, const nova_field *f, nova_field *out);
+/* poisson::rhs(rhs); poisson::solve(): p = L^-1 rhs on the unique nodes (mean mode 0) */
+nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, nova_field *p);
+nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *s, double *out);
+
+/* ---- fused time advance ---- */
+/* hist: nsteps x NOVA_HIST_COLS doubles (rows of steps without diagnostics are zero); may be NULL */
+nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *run, nova_state *state, int nsteps, double *hist);
+
+/* ---- instrumentation: per-kernel CUDA-event timing of nova_advance ---- */
+typedef enum { NOVA_K_STAGE = 0, NOVA_K_DIV = 1, NOVA_K_FFT = 2, NOVA_K_CORRECT = 3, NOVA_K_DIAG = 4, NOVA_K_COUNT = 5 } nova_kernel_class;
+nova_status nova_profile_enable(nova_ctx *ctx, int on);
+/* total milliseconds and launch count per class since the last reset */
+nova_status nova_profile_read(nova_ctx *ctx, int kernel_class, double *total_ms, long *launches, int reset);
+/* number of kernels this library launched since the last reset */
+nova_status nova_launch_count(nova_ctx *ctx, long *launches, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

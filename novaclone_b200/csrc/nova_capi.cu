@@ -1,0 +1,856 @@
+// C ABI of libnova_b200 (include/nova_gpu.h): contexts, fields, the ex::
+// drop-in operators, the cuFFT projection and the fused time advance.
+#include "nova_gpu.h"
+#include "nova_internal.cuh"
+#include "nova_ops.cuh"
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace nova;
+
+struct nova_field {
+    int nc;
+    int prec;
+    long long n3;
+    double *d64;
+    float *hi, *lo;
+};
+
+namespace {
+
+// settings::coef_ (src/settings/settings.cpp:25-31)
+const double kCoef[4][4] = {
+    {1.0, 0.0, 0.0, 0.0},
+    {4.0 / 3.0, -1.0 / 3.0, 0.0, 0.0},
+    {6.0 / 4.0, -12.0 / 20.0, 1.0 / 10.0, 0.0},
+    {8.0 / 5.0, -4.0 / 5.0, 24.0 / 105.0, -8.0 / 280.0},
+};
+
+struct ProfRec {
+    int cls;
+    cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct nova_ctx {
+    nova_mesh_desc md{};
+    int h = 3;
+    int local_n[3] = {0, 0, 0};
+    Geo g{};
+    Coef<double> co64{};
+    Coef<float> co32{};
+    std::vector<double> dzdxi, d2zdxi2;  // ghosted length n2 (Mesh::dzdxi_)
+    double *d_ia64 = nullptr, *d_corr64 = nullptr;
+    float *d_ia32 = nullptr, *d_corr32 = nullptr;
+    double *d_kx2 = nullptr, *d_ky2 = nullptr, *d_kz2 = nullptr;
+    cufftHandle plan_f = 0, plan_b = 0;
+    bool plans = false;
+    void *d_spec = nullptr;
+    double *d_rhs = nullptr;
+    double *w64[3] = {nullptr, nullptr, nullptr};
+    float *w32[3] = {nullptr, nullptr, nullptr};
+    double *d_part = nullptr;
+    double *d_scalar = nullptr;
+    int *d_flag = nullptr;
+    double *d_hist = nullptr;
+    long long hist_cap = 0;
+    double *d_stage = nullptr;
+    size_t stage_cap = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    bool prof = false;
+    std::vector<ProfRec> prof_live;
+    std::vector<cudaEvent_t> ev_pool;
+    double prof_ms[NOVA_K_COUNT] = {0};
+    long prof_n[NOVA_K_COUNT] = {0};
+    long launches = 0;
+};
+
+namespace {
+
+nova_status fail(nova_ctx *c, nova_status s, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return s;
+}
+
+nova_status cuda_check(nova_ctx *c, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return NOVA_OK;
+    if (e == cudaErrorMemoryAllocation) return fail(c, NOVA_E_OOM, std::string(what) + ": out of device memory");
+    return fail(c, NOVA_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                        \
+    do {                                                                \
+        nova_status _s = cuda_check(ctx, (call), #call);                \
+        if (_s != NOVA_OK) return _s;                                   \
+    } while (0)
+
+#define CKL(what)                                                       \
+    do {                                                                \
+        nova_status _s = cuda_check(ctx, cudaGetLastError(), what);     \
+        if (_s != NOVA_OK) return _s;                                   \
+    } while (0)
+
+nova_status fft_check(nova_ctx *ctx, cufftResult r, const char *what)
+{
+    if (r == CUFFT_SUCCESS) return NOVA_OK;
+    if (r == CUFFT_ALLOC_FAILED) return fail(ctx, NOVA_E_OOM, std::string(what) + ": cuFFT allocation failed");
+    return fail(ctx, NOVA_E_CUDA, std::string(what) + ": cuFFT error " + std::to_string((int)r));
+}
+
+template <typename T>
+nova_status dalloc(nova_ctx *ctx, T **p, size_t n)
+{
+    if (*p) return NOVA_OK;
+    return cuda_check(ctx, cudaMalloc((void **)p, sizeof(T) * (n ? n : 1)), "cudaMalloc");
+}
+
+// Mesh::z (src/Mesh/Mesh.cpp:373-407) for a single rank
+double mesh_z(const nova_mesh_desc &m, int h, double bcoef, int k)
+{
+    const double dz = m.L[2] / m.N[2];
+    if (m.hyperbolic_z) {
+        const double A = std::pow(m.s1 / m.s2, 0.5);
+        const int globK = k - h + (int)(long)m.origin[2];
+        const int globN = m.N[2] + 1;
+        const double R = (double)globK / (double)(globN - 1) - 0.5;
+        const double U = 1.0 + std::tanh(bcoef * R) / std::tanh(bcoef / 2.0);
+        return U / (2.0 * A + (1 - A) * U) * m.L[2];
+    }
+    return (k - h) * dz + m.origin[2];
+}
+
+// Mesh::dzdxi_, d2zdxi2_ (src/Mesh/Mesh.cpp:146-179)
+void mesh_metrics(const nova_mesh_desc &m, std::vector<double> &dz1, std::vector<double> &dz2)
+{
+    const int h = m.m / 2;
+    const int nk = m.N[2] + 1 + m.m;
+    const double *c = kCoef[(m.m - 2) / 2];
+    const double dz = m.L[2] / m.N[2];
+    double b = 1.0;
+    if (m.hyperbolic_z) {
+        const int globN = m.N[2] + 1;
+        for (int i = 1; i < 10000; i++) b = std::asinh(b / ((globN - 1) * std::pow(m.s1 * m.s2, 0.5)));
+    }
+    dz1.assign(nk, 0.0);
+    dz2.assign(nk, 0.0);
+    for (int k = h; k < nk - h; k++) {
+        double s = 0.0, s2 = 0.0;
+        for (int l = 0; l < h; l++) {
+            s += (c[l] / 2.0 / (l + 1) / dz * mesh_z(m, h, b, k + 1 + l)
+                  - c[l] / 2.0 / (l + 1) / dz * mesh_z(m, h, b, k - 1 - l));
+            s2 += (c[l] / std::pow((l + 1) * dz, 2) * mesh_z(m, h, b, k + 1 + l)
+                   + c[l] / std::pow((l + 1) * dz, 2) * mesh_z(m, h, b, k - 1 - l)
+                   + (-2.0 * c[l] / std::pow((l + 1) * dz, 2)) * mesh_z(m, h, b, k));
+        }
+        dz1[k] = s;
+        dz2[k] = s2;
+    }
+}
+
+// squared modified wavenumbers along one axis (poisson::wavenumbersFFT_, poisson.cpp:352-391)
+std::vector<double> kp2_table(int n, double L, double delta, int h, const double *coef, bool fold, int count)
+{
+    std::vector<double> t(count);
+    const double pi = M_PI, eps = 1.0e-16;
+    for (int i = 0; i < count; i++) {
+        double kk;
+        if (!fold || 2 * i < n)
+            kk = 2.0 * pi * (i) / L;
+        else
+            kk = 2.0 * pi * (n - i) / L;
+        double kp = 0.0;
+        if (kk > eps)
+            for (int ll = 0; ll < h; ll++) kp += kk * coef[ll] / (ll + 1) * std::sin((ll + 1) * kk * delta) / (kk * delta);
+        t[i] = kp * kp;
+    }
+    return t;
+}
+
+void prof_begin(nova_ctx *ctx, int cls, cudaEvent_t *a)
+{
+    *a = nullptr;
+    if (!ctx->prof) return;
+    if (ctx->ev_pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->ev_pool.push_back(e);
+    }
+    *a = ctx->ev_pool.back();
+    ctx->ev_pool.pop_back();
+    cudaEventRecord(*a, ctx->stream);
+    (void)cls;
+}
+
+void prof_end(nova_ctx *ctx, int cls, cudaEvent_t a)
+{
+    if (!ctx->prof || !a) return;
+    if (ctx->ev_pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->ev_pool.push_back(e);
+    }
+    cudaEvent_t b = ctx->ev_pool.back();
+    ctx->ev_pool.pop_back();
+    cudaEventRecord(b, ctx->stream);
+    ctx->prof_live.push_back({cls, a, b});
+}
+
+void prof_collect(nova_ctx *ctx)
+{
+    if (ctx->prof_live.empty()) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &r : ctx->prof_live) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        ctx->prof_ms[r.cls] += ms;
+        ctx->prof_n[r.cls] += 1;
+        ctx->ev_pool.push_back(r.a);
+        ctx->ev_pool.push_back(r.b);
+    }
+    ctx->prof_live.clear();
+}
+
+struct ProfScope {
+    nova_ctx *ctx;
+    int cls;
+    cudaEvent_t a;
+    ProfScope(nova_ctx *c, int k) : ctx(c), cls(k) { prof_begin(ctx, cls, &a); }
+    ~ProfScope() { prof_end(ctx, cls, a); }
+};
+
+nova_status ensure_fft(nova_ctx *ctx)
+{
+    if (ctx->plans) return NOVA_OK;
+    const Geo &g = ctx->g;
+    nova_status s;
+    if ((s = fft_check(ctx, cufftPlan3d(&ctx->plan_f, g.N0, g.N1, g.N2, CUFFT_D2Z), "cufftPlan3d D2Z")) != NOVA_OK)
+        return s;
+    if ((s = fft_check(ctx, cufftPlan3d(&ctx->plan_b, g.N0, g.N1, g.N2, CUFFT_Z2D), "cufftPlan3d Z2D")) != NOVA_OK) {
+        cufftDestroy(ctx->plan_f);
+        return s;
+    }
+    ctx->plans = true;
+    const size_t nspec = (size_t)g.N0 * g.N1 * (g.N2 / 2 + 1);
+    if ((s = dalloc(ctx, (double **)&ctx->d_spec, 2 * nspec)) != NOVA_OK) return s;
+    if ((s = dalloc(ctx, &ctx->d_rhs, (size_t)g.N3)) != NOVA_OK) return s;
+    return NOVA_OK;
+}
+
+nova_status ensure_red(nova_ctx *ctx)
+{
+    nova_status s;
+    if ((s = dalloc(ctx, &ctx->d_part, (size_t)diag_blocks(ctx->g) * 4)) != NOVA_OK) return s;
+    if ((s = dalloc(ctx, &ctx->d_scalar, 1)) != NOVA_OK) return s;
+    if ((s = dalloc(ctx, &ctx->d_flag, 1)) != NOVA_OK) return s;
+    return NOVA_OK;
+}
+
+// rhs (device, N3 doubles) -> p: spectral inverse of div(grad(.)) (poisson::solve)
+nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
+{
+    nova_status s;
+    if ((s = ensure_fft(ctx)) != NOVA_OK) return s;
+    ProfScope ps(ctx, NOVA_K_FFT);
+    cufftSetStream(ctx->plan_f, ctx->stream);
+    cufftSetStream(ctx->plan_b, ctx->stream);
+    if ((s = fft_check(ctx, cufftExecD2Z(ctx->plan_f, (cufftDoubleReal *)rhs, (cufftDoubleComplex *)ctx->d_spec),
+                       "cufftExecD2Z")) != NOVA_OK)
+        return s;
+    launch_scale(ctx->g, ctx->d_spec, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2, 1.0 / (double)ctx->g.N3, ctx->stream);
+    ctx->launches += 1;
+    CKL("k_scale");
+    if ((s = fft_check(ctx, cufftExecZ2D(ctx->plan_b, (cufftDoubleComplex *)ctx->d_spec, (cufftDoubleReal *)p),
+                       "cufftExecZ2D")) != NOVA_OK)
+        return s;
+    return NOVA_OK;
+}
+
+bool valid_field(const nova_field *f, int nc)
+{
+    return f && f->nc == nc;
+}
+
+nova_status ensure_stage(nova_ctx *ctx, size_t n)
+{
+    if (ctx->stage_cap >= n) return NOVA_OK;
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    ctx->d_stage = nullptr;
+    ctx->stage_cap = 0;
+    nova_status s = dalloc(ctx, &ctx->d_stage, n);
+    if (s == NOVA_OK) ctx->stage_cap = n;
+    return s;
+}
+
+}  // namespace
+
+// ================================================================== context ==
+extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
+{
+    if (!md || !out) return NOVA_E_INVALID;
+    *out = nullptr;
+    if (md->m != 2 && md->m != 4 && md->m != 6 && md->m != 8) return NOVA_E_INVALID;
+    for (int a = 0; a < 3; a++)
+        if (md->N[a] < 1 || !(md->L[a] > 0.0)) return NOVA_E_INVALID;
+    nova_ctx *ctx = new (std::nothrow) nova_ctx();
+    if (!ctx) return NOVA_E_OOM;
+    ctx->md = *md;
+    ctx->h = md->m / 2;
+    for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
+    Geo &g = ctx->g;
+    g.N0 = md->N[0];
+    g.N1 = md->N[1];
+    g.N2 = md->N[2];
+    g.N12 = (long long)g.N1 * g.N2;
+    g.N3 = (long long)g.N0 * g.N12;
+    const double *c = kCoef[(md->m - 2) / 2];
+    for (int d = 0; d < 3; d++) {
+        const double del = md->L[d] / md->N[d];
+        double b2 = 0.0;
+        for (int l = 0; l < 4; l++) {
+            const double a = (l < ctx->h) ? c[l] / 2.0 / (l + 1) / del : 0.0;
+            const double b = (l < ctx->h) ? c[l] / std::pow((l + 1) * del, 2) : 0.0;
+            ctx->co64.a[d][l] = a;
+            ctx->co64.b[d][l] = b;
+            ctx->co32.a[d][l] = (float)a;
+            ctx->co32.b[d][l] = (float)b;
+            b2 += 2.0 * b;
+        }
+        ctx->co64.b2[d] = b2;
+        ctx->co32.b2[d] = (float)b2;
+    }
+    mesh_metrics(*md, ctx->dzdxi, ctx->d2zdxi2);
+    std::vector<double> ia(g.N2), cr(g.N2);
+    std::vector<float> ia32(g.N2), cr32(g.N2);
+    for (int k = 0; k < g.N2; k++) {
+        const double d1 = ctx->dzdxi[k + ctx->h], d2 = ctx->d2zdxi2[k + ctx->h];
+        ia[k] = 1.0 / d1;
+        cr[k] = d2 / (d1 * d1);
+        ia32[k] = (float)ia[k];
+        cr32[k] = (float)cr[k];
+    }
+    const double dx = md->L[0] / md->N[0], dy = md->L[1] / md->N[1], dz = md->L[2] / md->N[2];
+    std::vector<double> kx2 = kp2_table(g.N0, md->L[0], dx, ctx->h, c, true, g.N0);
+    std::vector<double> ky2 = kp2_table(g.N1, md->L[1], dy, ctx->h, c, true, g.N1);
+    std::vector<double> kz2 = kp2_table(g.N2, md->L[2], dz, ctx->h, c, false, g.N2 / 2 + 1);
+
+    nova_status s = NOVA_OK;
+    auto up = [&](auto **dptr, const auto &vec) {
+        if (s != NOVA_OK) return;
+        using T = typename std::remove_reference<decltype(vec)>::type::value_type;
+        s = dalloc(ctx, (T **)dptr, vec.size());
+        if (s == NOVA_OK)
+            s = cuda_check(ctx, cudaMemcpy(*dptr, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice),
+                           "cudaMemcpy");
+    };
+    up(&ctx->d_ia64, ia);
+    up(&ctx->d_corr64, cr);
+    up(&ctx->d_ia32, ia32);
+    up(&ctx->d_corr32, cr32);
+    up(&ctx->d_kx2, kx2);
+    up(&ctx->d_ky2, ky2);
+    up(&ctx->d_kz2, kz2);
+    if (s == NOVA_OK) {
+        s = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ctx->own_stream = (s == NOVA_OK);
+    }
+    if (s != NOVA_OK) {
+        nova_destroy(ctx);
+        return s;
+    }
+    *out = ctx;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_destroy(nova_ctx *ctx)
+{
+    if (!ctx) return NOVA_E_INVALID;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    prof_collect(ctx);
+    for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->plans) {
+        cufftDestroy(ctx->plan_f);
+        cufftDestroy(ctx->plan_b);
+    }
+    void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
+                    ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return NOVA_OK;
+}
+
+extern "C" const char *nova_last_error(const nova_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" nova_status nova_set_stream(nova_ctx *ctx, void *stream)
+{
+    if (!ctx) return NOVA_E_INVALID;
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+        ctx->own_stream = false;
+    } else {
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_synchronize(nova_ctx *ctx)
+{
+    if (!ctx) return NOVA_E_INVALID;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_mesh_local_n(const nova_ctx *ctx, int local_n[3])
+{
+    if (!ctx || !local_n) return NOVA_E_INVALID;
+    for (int a = 0; a < 3; a++) local_n[a] = ctx->local_n[a];
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_mesh_metrics(const nova_ctx *ctx, double *dzdxi, double *d2zdxi2)
+{
+    if (!ctx) return NOVA_E_INVALID;
+    if (dzdxi) std::memcpy(dzdxi, ctx->dzdxi.data(), sizeof(double) * ctx->dzdxi.size());
+    if (d2zdxi2) std::memcpy(d2zdxi2, ctx->d2zdxi2.data(), sizeof(double) * ctx->d2zdxi2.size());
+    return NOVA_OK;
+}
+
+// =================================================================== fields ==
+extern "C" nova_status nova_field_create(nova_ctx *ctx, int ncomp, int precision, nova_field **out)
+{
+    if (!ctx || !out || ncomp < 1 || ncomp > 9) return fail(ctx, NOVA_E_INVALID, "nova_field_create: bad arguments");
+    if (precision != NOVA_F64 && precision != NOVA_F32SPLIT)
+        return fail(ctx, NOVA_E_INVALID, "nova_field_create: unknown precision");
+    nova_field *f = new (std::nothrow) nova_field();
+    if (!f) return fail(ctx, NOVA_E_OOM, "nova_field_create: host allocation");
+    f->nc = ncomp;
+    f->prec = precision;
+    f->n3 = ctx->g.N3;
+    const size_t n = (size_t)ncomp * f->n3;
+    nova_status s;
+    if (precision == NOVA_F64) {
+        s = dalloc(ctx, &f->d64, n);
+        if (s == NOVA_OK) s = cuda_check(ctx, cudaMemsetAsync(f->d64, 0, sizeof(double) * n, ctx->stream), "memset");
+    } else {
+        s = dalloc(ctx, &f->hi, n);
+        if (s == NOVA_OK) s = dalloc(ctx, &f->lo, n);
+        if (s == NOVA_OK) s = cuda_check(ctx, cudaMemsetAsync(f->hi, 0, sizeof(float) * n, ctx->stream), "memset");
+        if (s == NOVA_OK) s = cuda_check(ctx, cudaMemsetAsync(f->lo, 0, sizeof(float) * n, ctx->stream), "memset");
+    }
+    if (s != NOVA_OK) {
+        nova_field_destroy(ctx, f);
+        return s;
+    }
+    *out = f;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_destroy(nova_ctx *ctx, nova_field *f)
+{
+    if (!f) return NOVA_E_INVALID;
+    if (ctx && ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (f->d64) cudaFree(f->d64);
+    if (f->hi) cudaFree(f->hi);
+    if (f->lo) cudaFree(f->lo);
+    delete f;
+    return NOVA_OK;
+}
+
+static nova_status check_local_n(nova_ctx *ctx, const int local_n[3])
+{
+    if (!local_n) return fail(ctx, NOVA_E_INVALID, "local_n is null");
+    for (int a = 0; a < 3; a++)
+        if (local_n[a] != ctx->local_n[a])
+            return fail(ctx, NOVA_E_INVALID, "local_n does not match the mesh (expected N+1+m per axis)");
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_upload(nova_ctx *ctx, nova_field *f, const double *host, const int local_n[3])
+{
+    if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_upload: null argument");
+    nova_status s = check_local_n(ctx, local_n);
+    if (s != NOVA_OK) return s;
+    const size_t n = (size_t)local_n[0] * local_n[1] * local_n[2] * f->nc;
+    if ((s = ensure_stage(ctx, n)) != NOVA_OK) return s;
+    CK(cudaMemcpyAsync(ctx->d_stage, host, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    launch_aos_to_soa(ctx->g, ctx->h, ctx->local_n, f->nc, ctx->d_stage, f->d64, f->hi, f->lo, ctx->stream);
+    ctx->launches += 1;
+    CKL("k_aos_to_soa");
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_download(nova_ctx *ctx, const nova_field *f, double *host, const int local_n[3],
+                                           const nova_bc *bc)
+{
+    if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_download: null argument");
+    nova_status s = check_local_n(ctx, local_n);
+    if (s != NOVA_OK) return s;
+    if (bc)
+        for (int q = 0; q < 6 * f->nc && q < 18; q++)
+            if (bc->type[q] != NOVA_BC_PERIODIC)
+                return fail(ctx, NOVA_E_UNSUPPORTED, "nova_field_download: only periodic ghost fills are built");
+    const size_t n = (size_t)local_n[0] * local_n[1] * local_n[2] * f->nc;
+    if ((s = ensure_stage(ctx, n)) != NOVA_OK) return s;
+    launch_soa_to_aos(ctx->g, ctx->h, ctx->local_n, f->nc, f->d64, f->hi, f->lo, ctx->d_stage, ctx->stream);
+    ctx->launches += 1;
+    CKL("k_soa_to_aos");
+    CK(cudaMemcpyAsync(host, ctx->d_stage, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+static nova_status soa_in(nova_ctx *ctx, nova_field *f, const double *src, cudaMemcpyKind kind)
+{
+    const size_t n = (size_t)f->nc * f->n3;
+    if (f->prec == NOVA_F64) {
+        CK(cudaMemcpyAsync(f->d64, src, sizeof(double) * n, kind, ctx->stream));
+    } else {
+        nova_status s = ensure_stage(ctx, n);
+        if (s != NOVA_OK) return s;
+        CK(cudaMemcpyAsync(ctx->d_stage, src, sizeof(double) * n, kind, ctx->stream));
+        launch_split((long long)n, ctx->d_stage, f->hi, f->lo, ctx->stream);
+        ctx->launches += 1;
+        CKL("k_split");
+    }
+    return NOVA_OK;
+}
+
+static nova_status soa_out(nova_ctx *ctx, const nova_field *f, double *dst, cudaMemcpyKind kind)
+{
+    const size_t n = (size_t)f->nc * f->n3;
+    if (f->prec == NOVA_F64) {
+        CK(cudaMemcpyAsync(dst, f->d64, sizeof(double) * n, kind, ctx->stream));
+    } else {
+        nova_status s = ensure_stage(ctx, n);
+        if (s != NOVA_OK) return s;
+        launch_join((long long)n, f->hi, f->lo, ctx->d_stage, ctx->stream);
+        ctx->launches += 1;
+        CKL("k_join");
+        CK(cudaMemcpyAsync(dst, ctx->d_stage, sizeof(double) * n, kind, ctx->stream));
+    }
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_upload_soa(nova_ctx *ctx, nova_field *f, const double *host)
+{
+    if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_upload_soa: null argument");
+    nova_status s = soa_in(ctx, f, host, cudaMemcpyHostToDevice);
+    if (s != NOVA_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_download_soa(nova_ctx *ctx, const nova_field *f, double *host)
+{
+    if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_download_soa: null argument");
+    nova_status s = soa_out(ctx, f, host, cudaMemcpyDeviceToHost);
+    if (s != NOVA_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_copy_from_device(nova_ctx *ctx, nova_field *f, const double *dev)
+{
+    if (!ctx || !f || !dev) return fail(ctx, NOVA_E_INVALID, "nova_field_copy_from_device: null argument");
+    return soa_in(ctx, f, dev, cudaMemcpyDeviceToDevice);
+}
+
+extern "C" nova_status nova_field_copy_to_device(nova_ctx *ctx, const nova_field *f, double *dev)
+{
+    if (!ctx || !f || !dev) return fail(ctx, NOVA_E_INVALID, "nova_field_copy_to_device: null argument");
+    return soa_out(ctx, f, dev, cudaMemcpyDeviceToDevice);
+}
+
+// ================================================================ operators ==
+static nova_status op_common(nova_ctx *ctx, int op, const nova_field *a, const nova_field *b, nova_field *out,
+                             int nc_in, int nc_out, double nu)
+{
+    if (!ctx || !a || !out) return fail(ctx, NOVA_E_INVALID, "operator: null argument");
+    if ((nc_in && a->nc != nc_in) || (nc_out && out->nc != nc_out))
+        return fail(ctx, NOVA_E_INVALID, "operator: wrong number of components");
+    if (a->prec != NOVA_F64 || out->prec != NOVA_F64 || (b && b->prec != NOVA_F64))
+        return fail(ctx, NOVA_E_UNSUPPORTED, "operator: the ex:: entry points take FP64 fields");
+    if (a == out || (b && b == out)) return fail(ctx, NOVA_E_INVALID, "operator: output aliases an input");
+    launch_op(op, ctx->h, ctx->g, ctx->co64, ctx->d_ia64, ctx->d_corr64, a->d64, b ? b->d64 : nullptr,
+              (op == OP_DIV_VF) ? b->nc : a->nc, nu, out->d64, ctx->stream);
+    ctx->launches += 1;
+    CKL("operator kernel");
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_grad_s(nova_ctx *ctx, const nova_field *s, nova_field *out)
+{
+    return op_common(ctx, OP_GRAD_S, s, nullptr, out, 1, 3, 0.0);
+}
+
+extern "C" nova_status nova_grad_v(nova_ctx *ctx, const nova_field *U, nova_field *out)
+{
+    return op_common(ctx, OP_GRAD_V, U, nullptr, out, 3, 9, 0.0);
+}
+
+extern "C" nova_status nova_curl(nova_ctx *ctx, const nova_field *U, nova_field *out)
+{
+    return op_common(ctx, OP_CURL, U, nullptr, out, 3, 3, 0.0);
+}
+
+extern "C" nova_status nova_div_v(nova_ctx *ctx, const nova_field *U, nova_field *out)
+{
+    return op_common(ctx, OP_DIV_V, U, nullptr, out, 3, 1, 0.0);
+}
+
+extern "C" nova_status nova_div_vf(nova_ctx *ctx, const nova_field *U, const nova_field *f, nova_field *out)
+{
+    if (!ctx || !f) return fail(ctx, NOVA_E_INVALID, "nova_div_vf: null argument");
+    if (out && out->nc != f->nc) return fail(ctx, NOVA_E_INVALID, "nova_div_vf: out must match f");
+    return op_common(ctx, OP_DIV_VF, U, f, out, 3, 0, 0.0);
+}
+
+extern "C" nova_status nova_laplacian(nova_ctx *ctx, double nu, const nova_field *f, nova_field *out)
+{
+    if (!ctx || !f || !out) return fail(ctx, NOVA_E_INVALID, "nova_laplacian: null argument");
+    if (out->nc != f->nc) return fail(ctx, NOVA_E_INVALID, "nova_laplacian: out must match f");
+    return op_common(ctx, OP_LAP, f, nullptr, out, 0, 0, nu);
+}
+
+extern "C" nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, nova_field *p)
+{
+    if (!ctx || !rhs || !p) return fail(ctx, NOVA_E_INVALID, "nova_poisson_solve: null argument");
+    if (rhs->nc != 1 || p->nc != 1 || rhs->prec != NOVA_F64 || p->prec != NOVA_F64)
+        return fail(ctx, NOVA_E_INVALID, "nova_poisson_solve: needs FP64 scalar fields");
+    nova_status s = ensure_fft(ctx);
+    if (s != NOVA_OK) return s;
+    CK(cudaMemcpyAsync(ctx->d_rhs, rhs->d64, sizeof(double) * ctx->g.N3, cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((s = poisson_device(ctx, ctx->d_rhs, p->d64)) != NOVA_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *f, double *out)
+{
+    if (!ctx || !f || !out) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs: null argument");
+    if (f->nc != 1 || f->prec != NOVA_F64) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs: FP64 scalar only");
+    nova_status s = ensure_red(ctx);
+    if (s != NOVA_OK) return s;
+    launch_maxabs(ctx->g, f->d64, ctx->d_part, ctx->d_scalar, ctx->stream);
+    ctx->launches += 2;
+    CKL("maxabs");
+    CK(cudaMemcpyAsync(out, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+// ================================================================== advance ==
+namespace {
+
+nova_status ensure_work(nova_ctx *ctx, int prec)
+{
+    const size_t n = 3 * (size_t)ctx->g.N3;
+    nova_status s = NOVA_OK;
+    for (int q = 0; q < 3 && s == NOVA_OK; q++) {
+        if (prec == NOVA_F64)
+            s = dalloc(ctx, &ctx->w64[q], n);
+        else
+            s = dalloc(ctx, &ctx->w32[q], n);
+    }
+    if (s == NOVA_OK) s = ensure_fft(ctx);
+    if (s == NOVA_OK) s = ensure_red(ctx);
+    return s;
+}
+
+// One RK4 (or literal) sweep of an evolved field Y with the frozen field X,
+// followed by its projection.  Y is updated in place.
+nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field *Y, const nova_field *X,
+                   nova_field *p, double visc, double divisor, double corr_scale)
+{
+    const Geo &g = ctx->g;
+    cudaStream_t st = ctx->stream;
+    const bool lit = rd->rk_mode == NOVA_RK_LITERAL;
+    if (Y->prec == NOVA_F64) {
+        double *Ustar;
+        auto run64 = [&](int stage, const StageArgs64 &a) {
+            ProfScope ps(ctx, NOVA_K_STAGE);
+            launch_stage64(phys, stage, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc, a, st);
+            ctx->launches += 1;
+        };
+        if (lit) {
+            run64(4, StageArgs64{Y->d64, X ? X->d64 : nullptr, nullptr, nullptr, ctx->w64[1]});
+            Ustar = ctx->w64[1];
+        } else {
+            double *w0 = ctx->w64[0], *w1 = ctx->w64[1], *A = ctx->w64[2];
+            const double *Xp = X ? X->d64 : nullptr;
+            run64(0, StageArgs64{Y->d64, Xp, nullptr, A, w0});
+            run64(1, StageArgs64{w0, Xp, Y->d64, A, w1});
+            run64(2, StageArgs64{w1, Xp, Y->d64, A, w0});
+            run64(3, StageArgs64{w0, Xp, nullptr, A, Y->d64});
+            Ustar = Y->d64;
+        }
+        CKL("stage kernel");
+        {
+            ProfScope ps(ctx, NOVA_K_DIV);
+            launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, Ustar, nullptr, nullptr, divisor, ctx->d_rhs, st);
+            ctx->launches += 1;
+        }
+        CKL("k_div_proj");
+        nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
+        if (s != NOVA_OK) return s;
+        {
+            ProfScope ps(ctx, NOVA_K_CORRECT);
+            launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, p->d64, corr_scale, Ustar, Y->d64, nullptr, nullptr,
+                           nullptr, nullptr, st);
+            ctx->launches += 1;
+        }
+        CKL("k_correct");
+    } else {
+        const float *Ushi, *Uslo;
+        auto run32 = [&](int stage, const StageArgs32 &a) {
+            ProfScope ps(ctx, NOVA_K_STAGE);
+            launch_stage32(phys, stage, g, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt, (float)visc, a, st);
+            ctx->launches += 1;
+        };
+        const float *Xp = X ? X->hi : nullptr;
+        if (lit) {
+            run32(4, StageArgs32{Y->hi, Xp, nullptr, Y->lo, nullptr, nullptr, ctx->w32[0], ctx->w32[1]});
+            Ushi = ctx->w32[0];
+            Uslo = ctx->w32[1];
+        } else {
+            float *w0 = ctx->w32[0], *w1 = ctx->w32[1], *A = ctx->w32[2];
+            run32(0, StageArgs32{Y->hi, Xp, nullptr, nullptr, A, w0, nullptr, nullptr});
+            run32(1, StageArgs32{w0, Xp, Y->hi, nullptr, A, w1, nullptr, nullptr});
+            run32(2, StageArgs32{w1, Xp, Y->hi, nullptr, A, w0, nullptr, nullptr});
+            run32(3, StageArgs32{w0, Xp, Y->hi, Y->lo, A, nullptr, Y->hi, Y->lo});
+            Ushi = Y->hi;
+            Uslo = Y->lo;
+        }
+        CKL("stage kernel");
+        {
+            ProfScope ps(ctx, NOVA_K_DIV);
+            launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo, divisor, ctx->d_rhs, st);
+            ctx->launches += 1;
+        }
+        CKL("k_div_proj");
+        nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
+        if (s != NOVA_OK) return s;
+        {
+            ProfScope ps(ctx, NOVA_K_CORRECT);
+            launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, p->d64, corr_scale, nullptr, nullptr, Ushi, Uslo, Y->hi,
+                           Y->lo, st);
+            ctx->launches += 1;
+        }
+        CKL("k_correct");
+    }
+    return NOVA_OK;
+}
+
+}  // namespace
+
+extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova_state *st, int nsteps, double *hist)
+{
+    if (!ctx || !rd || !st || nsteps < 0) return fail(ctx, NOVA_E_INVALID, "nova_advance: bad arguments");
+    const bool mhd = rd->model == NOVA_MODEL_MHD;
+    if (rd->model != NOVA_MODEL_NS && !mhd) return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown model");
+    if (rd->rk_mode != NOVA_RK_LITERAL && rd->rk_mode != NOVA_RK_CLASSICAL)
+        return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown rk_mode");
+    if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: the fused kernels are built for m = 6");
+    if (!valid_field(st->U, 3) || !valid_field(st->p, 1) || st->p->prec != NOVA_F64 || st->U->prec != rd->precision)
+        return fail(ctx, NOVA_E_INVALID, "nova_advance: U (3 comps, run precision) and p (FP64 scalar) required");
+    if (mhd && (!valid_field(st->B, 3) || !valid_field(st->pB, 1) || st->pB->prec != NOVA_F64 ||
+                st->B->prec != rd->precision))
+        return fail(ctx, NOVA_E_INVALID, "nova_advance: MHD needs B (3 comps) and pB (FP64 scalar)");
+    if (!(rd->dt > 0.0)) return fail(ctx, NOVA_E_INVALID, "nova_advance: dt must be positive");
+    nova_status s = ensure_work(ctx, rd->precision);
+    if (s != NOVA_OK) return s;
+    if (hist && rd->diag_every > 0) {
+        if (ctx->hist_cap < (long long)nsteps * NOVA_HIST_COLS) {
+            if (ctx->d_hist) cudaFree(ctx->d_hist);
+            ctx->d_hist = nullptr;
+            ctx->hist_cap = 0;
+            if ((s = dalloc(ctx, &ctx->d_hist, (size_t)nsteps * NOVA_HIST_COLS)) != NOVA_OK) return s;
+            ctx->hist_cap = (long long)nsteps * NOVA_HIST_COLS;
+        }
+        CK(cudaMemsetAsync(ctx->d_hist, 0, sizeof(double) * nsteps * NOVA_HIST_COLS, ctx->stream));
+    }
+    CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    for (int n = 0; n < nsteps; n++) {
+        // app/TG_Piosson/RKLoop.H (NS) or app/OT_Poisson/UEqn.H then BEqn.H (MHD)
+        s = evolve(ctx, rd, mhd ? PHYS_MHD_U : PHYS_NS, st->U, mhd ? st->B : nullptr, st->p, rd->nu, rd->dt, rd->dt);
+        if (s != NOVA_OK) return s;
+        if (mhd) {
+            // B loop is always the refreshed RK4 (BEqn.H:86-87); B cleaning has no 1/dt (BEqn.H:91-94)
+            nova_run_desc rb = *rd;
+            rb.rk_mode = NOVA_RK_CLASSICAL;
+            s = evolve(ctx, &rb, PHYS_MHD_B, st->B, st->U, st->pB, rd->eta, 1.0, 1.0);
+            if (s != NOVA_OK) return s;
+        }
+        if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps)) {
+            ProfScope ps(ctx, NOVA_K_DIAG);
+            const nova_field *U = st->U, *B = mhd ? st->B : nullptr;
+            launch_diag(ctx->h, ctx->g, ctx->co64, ctx->d_ia64, U->d64, U->hi, U->lo, B ? B->d64 : nullptr,
+                        B ? B->hi : nullptr, B ? B->lo : nullptr, mhd ? 1 : 0, ctx->d_part, (double)(n + 1),
+                        rd->t0 + (n + 1) * rd->dt, ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag,
+                        ctx->stream);
+            ctx->launches += 2;
+            CKL("k_diag");
+        }
+    }
+    if (hist && rd->diag_every > 0)
+        CK(cudaMemcpyAsync(hist, ctx->d_hist, sizeof(double) * nsteps * NOVA_HIST_COLS, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (flag) return fail(ctx, NOVA_E_NONFINITE, "nova_advance: non-finite value in the diagnostics");
+    return NOVA_OK;
+}
+
+// ========================================================== instrumentation ==
+extern "C" nova_status nova_profile_enable(nova_ctx *ctx, int on)
+{
+    if (!ctx) return NOVA_E_INVALID;
+    prof_collect(ctx);
+    ctx->prof = on != 0;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_profile_read(nova_ctx *ctx, int cls, double *total_ms, long *launches, int reset)
+{
+    if (!ctx || cls < 0 || cls >= NOVA_K_COUNT) return NOVA_E_INVALID;
+    prof_collect(ctx);
+    if (total_ms) *total_ms = ctx->prof_ms[cls];
+    if (launches) *launches = ctx->prof_n[cls];
+    if (reset) {
+        ctx->prof_ms[cls] = 0.0;
+        ctx->prof_n[cls] = 0;
+    }
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_launch_count(nova_ctx *ctx, long *launches, int reset)
+{
+    if (!ctx || !launches) return NOVA_E_INVALID;
+    *launches = ctx->launches;
+    if (reset) ctx->launches = 0;
+    return NOVA_OK;
+}

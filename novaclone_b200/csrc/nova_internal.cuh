@@ -1,0 +1,98 @@
+// Internal declarations shared by the CUDA translation units of libnova_b200.
+//
+// Device layout: every field is component-major over the unique nodes,
+// [c][i][j][k] with k (z) fastest -- the reference Field<T> index order
+// k + j*nk + i*nk*nj (src/Field/Field.h:82-85) without ghosts and without the
+// duplicated periodic node.  Periodic ghosts are synthesised in the kernels by
+// index wrapping (src/BC/periodicBC.hxx:1-66 becomes address arithmetic).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace nova {
+
+// Half-width of the fused kernels' stencil (settings::m_ = 6 -> 3 ghost layers).
+constexpr int kTK = 32;   // tile extent along k (one warp, coalesced)
+constexpr int kTJ = 8;    // tile extent along j
+constexpr int kThreads = kTK * kTJ;
+
+struct Geo {
+    int N0, N1, N2;
+    long long N12, N3;
+};
+
+// First/second-derivative weights of src/settings/settings.cpp:25-31 for half
+// width H, per direction d: a[d][l] = c_l / (2 (l+1) delta_d) (grad.cpp:46),
+// b[d][l] = c_l / ((l+1) delta_d)^2 (laplacian.hxx:153), b2[d] = 2 sum_l b[d][l].
+template <typename T> struct Coef {
+    T a[3][4];
+    T b[3][4];
+    T b2[3];
+};
+
+__host__ __device__ inline int wrapi(int x, int n)
+{
+    int r = x % n;
+    return r < 0 ? r + n : r;
+}
+
+// ------------------------------------------------------------------ stencil math --
+// `v(c, s)` returns component c at offset s (-H..H) along the current direction.
+
+template <typename T, int H, class V>
+__device__ __forceinline__ T d1(const V &v, int c, const T *a)
+{
+    T r = a[0] * (v(c, 1) - v(c, -1));
+#pragma unroll
+    for (int l = 1; l < H; l++) r = fma(a[l], v(c, l + 1) - v(c, -l - 1), r);
+    return r;
+}
+
+// derivative of the product v_c1 * v_c2
+template <typename T, int H, class V>
+__device__ __forceinline__ T d1p(const V &v, int c1, int c2, const T *a)
+{
+    T r = a[0] * (v(c1, 1) * v(c2, 1) - v(c1, -1) * v(c2, -1));
+#pragma unroll
+    for (int l = 1; l < H; l++) r = fma(a[l], v(c1, l + 1) * v(c2, l + 1) - v(c1, -l - 1) * v(c2, -l - 1), r);
+    return r;
+}
+
+template <typename T, int H, class V>
+__device__ __forceinline__ T d2(const V &v, int c, const T *b, T b2)
+{
+    T r = b[0] * (v(c, 1) + v(c, -1));
+#pragma unroll
+    for (int l = 1; l < H; l++) r = fma(b[l], v(c, l + 1) + v(c, -l - 1), r);
+    return fma(-b2, v(c, 0), r);
+}
+
+// ------------------------------------------------------------- launch helpers --
+struct StageArgs64 {
+    const double *Y;   // halo'd stage state (3 comps)
+    const double *X;   // second halo'd field (MHD), else nullptr
+    const double *U0;  // RK base (stages 1, 2)
+    double *A;         // RK accumulator
+    double *Ynext;     // next stage state, or U* after the last stage
+};
+
+struct StageArgs32 {
+    const float *Y;      // halo'd stage state (3 comps, FP32)
+    const float *X;      // second halo'd field hi part (MHD)
+    const float *U0hi;   // base hi
+    const float *U0lo;   // base lo (last stage / literal)
+    float *A;            // FP32 increment accumulator
+    float *Ynext;        // next stage state (FP32)
+    float *outhi, *outlo;  // U* (last stage / literal)
+};
+
+enum Physics { PHYS_NS = 0, PHYS_MHD_U = 1, PHYS_MHD_B = 2 };
+
+// stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum)
+void launch_stage64(int phys, int stage, const Geo &g, const Coef<double> &co, const double *ia,
+                    const double *corr2, double dt, double visc, const StageArgs64 &a, cudaStream_t st);
+void launch_stage32(int phys, int stage, const Geo &g, const Coef<float> &co, const float *ia,
+                    const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st);
+
+}  // namespace nova

@@ -1,0 +1,587 @@
+// Projection, diagnostics, drop-in ex:: operators and layout conversion.
+//
+// Projection (app/TG_Piosson/RKLoop.H:30-38, app/OT_Poisson/BEqn.H:91-95):
+//   rhs = div(U*) / dt                       k_div_proj    (src/ex/div/div.hxx:22-81)
+//   rhs^ = D2Z(rhs)                          cuFFT         (src/poisson/poisson.cpp:225)
+//   rhs^ = -rhs^ / k'^2 / (N0 N1 N2)         k_scale       (poisson.cpp:230-249, 259)
+//   p = Z2D(rhs^)                            cuFFT         (poisson.cpp:250)
+//   U = U* - dt * grad(p)                    k_correct     (src/ex/grad/grad.cpp:25-62)
+// k'^2 is built from 1-D tables of squared modified wavenumbers
+// (poisson::wavenumbersFFT_, poisson.cpp:337-396) summed in the reference's order.
+#include "nova_internal.cuh"
+#include "nova_ops.cuh"
+
+#include <cuComplex.h>
+
+namespace nova {
+
+namespace {
+
+// value of component array f at (i,j,k) shifted by s along direction d, periodic
+template <typename P>
+__device__ __forceinline__ double at(const P &f, const Geo &g, int c, int i, int j, int k, int d, int s)
+{
+    if (d == 0) i = wrapi(i + s, g.N0);
+    else if (d == 1) j = wrapi(j + s, g.N1);
+    else k = wrapi(k + s, g.N2);
+    return f(c, (long long)i * g.N12 + (long long)j * g.N2 + k);
+}
+
+struct Ld64 {
+    const double *p;
+    long long n3;
+    __device__ double operator()(int c, long long o) const { return p[(long long)c * n3 + o]; }
+};
+struct LdSplit {
+    const float *hi, *lo;
+    long long n3;
+    __device__ double operator()(int c, long long o) const
+    {
+        return (double)hi[(long long)c * n3 + o] + (double)lo[(long long)c * n3 + o];
+    }
+};
+
+__device__ __forceinline__ void pt_index(const Geo &g, long long t, int &i, int &j, int &k)
+{
+    k = (int)(t % g.N2);
+    long long r = t / g.N2;
+    j = (int)(r % g.N1);
+    i = (int)(r / g.N1);
+}
+
+// first derivative along d of component c with weights a (already metric-scaled)
+template <int H, typename P>
+__device__ __forceinline__ double dd1(const P &f, const Geo &g, int c, int i, int j, int k, int d, const double *a)
+{
+    double r = 0.0;
+#pragma unroll
+    for (int l = 0; l < H; l++) r = fma(a[l], at(f, g, c, i, j, k, d, l + 1) - at(f, g, c, i, j, k, d, -l - 1), r);
+    return r;
+}
+
+template <int H, class LD>
+__global__ void k_div_proj(Geo g, Coef<double> co, const double *__restrict__ ia, LD U, double divisor,
+                           double *__restrict__ rhs)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    double az[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+    const double d = dd1<H>(U, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(U, g, 1, i, j, k, 1, co.a[1])
+                     + dd1<H>(U, g, 2, i, j, k, 2, az);
+    rhs[t] = d / divisor;
+}
+
+__global__ void k_scale(Geo g, cuDoubleComplex *__restrict__ spec, const double *__restrict__ kx2,
+                        const double *__restrict__ ky2, const double *__restrict__ kz2, double invN3)
+{
+    const int nzh = g.N2 / 2 + 1;
+    const long long tot = (long long)g.N0 * g.N1 * nzh;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= tot) return;
+    const int kz = (int)(t % nzh);
+    const long long r = t / nzh;
+    const int j = (int)(r % g.N1);
+    const int i = (int)(r / g.N1);
+    const double k2 = (kx2[i] + ky2[j]) + kz2[kz];
+    cuDoubleComplex v = spec[t];
+    if (k2 < 1.0e-16) {
+        v = make_cuDoubleComplex(0.0, 0.0);
+    } else {
+        v = make_cuDoubleComplex((-v.x / k2) * invN3, (-v.y / k2) * invN3);
+    }
+    spec[t] = v;
+}
+
+// U = U* - s*grad(p) (U may alias U*: each node reads and writes only itself)
+template <int H>
+__global__ void k_correct64(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ p,
+                            double s, const double *Us, double *U)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 P{p, g.N3};
+    double az[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+    double gr[3];
+    gr[0] = dd1<H>(P, g, 0, i, j, k, 0, co.a[0]);
+    gr[1] = dd1<H>(P, g, 0, i, j, k, 1, co.a[1]);
+    gr[2] = dd1<H>(P, g, 0, i, j, k, 2, az);
+#pragma unroll
+    for (int c = 0; c < 3; c++) U[c * g.N3 + t] = Us[c * g.N3 + t] - gr[c] * s;
+}
+
+// same for the (hi, lo) state: the correction is applied in FP64
+template <int H>
+__global__ void k_correct32(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ p,
+                            double s, const float *Ushi, const float *Uslo, float *hi, float *lo)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 P{p, g.N3};
+    double az[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+    double gr[3];
+    gr[0] = dd1<H>(P, g, 0, i, j, k, 0, co.a[0]);
+    gr[1] = dd1<H>(P, g, 0, i, j, k, 1, co.a[1]);
+    gr[2] = dd1<H>(P, g, 0, i, j, k, 2, az);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const long long o = c * g.N3 + t;
+        const double x = ((double)Ushi[o] + (double)Uslo[o]) - gr[c] * s;
+        const float h = (float)x;
+        hi[o] = h;
+        lo[o] = (float)(x - (double)h);
+    }
+}
+
+// ------------------------------------------------------------- diagnostics --
+constexpr int kRedThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T block_reduce_sum(T v, T *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    T r = 0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) r += sh[q];
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_reduce_max(T v, T *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    T r = 0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) r = fmax(r, sh[q]);
+    return r;
+}
+
+// per-block partials: [0] sum 1/2|U|^2, [1] sum 1/2|B|^2, [2] max|div U|, [3] max|div B|
+template <int H, class LD>
+__global__ void k_diag(Geo g, Coef<double> co, const double *__restrict__ ia, LD U, LD B, int hasB,
+                       double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    double ek = 0.0, em = 0.0, mdu = 0.0, mdb = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.N3;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        pt_index(g, t, i, j, k);
+        double az[H];
+#pragma unroll
+        for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+        const double u = U(0, t), v = U(1, t), w = U(2, t);
+        ek += 0.5 * (u * u + v * v + w * w);
+        const double du = dd1<H>(U, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(U, g, 1, i, j, k, 1, co.a[1])
+                          + dd1<H>(U, g, 2, i, j, k, 2, az);
+        mdu = fmax(mdu, fabs(du));
+        if (hasB) {
+            const double bx = B(0, t), by = B(1, t), bz = B(2, t);
+            em += 0.5 * (bx * bx + by * by + bz * bz);
+            const double db = dd1<H>(B, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(B, g, 1, i, j, k, 1, co.a[1])
+                              + dd1<H>(B, g, 2, i, j, k, 2, az);
+            mdb = fmax(mdb, fabs(db));
+        }
+    }
+    const double s0 = block_reduce_sum(ek, sh);
+    const double s1 = block_reduce_sum(em, sh);
+    const double s2 = block_reduce_max(mdu, sh);
+    const double s3 = block_reduce_max(mdb, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 4 + 0] = s0;
+        part[blockIdx.x * 4 + 1] = s1;
+        part[blockIdx.x * 4 + 2] = s2;
+        part[blockIdx.x * 4 + 3] = s3;
+    }
+}
+
+__global__ void k_diag_final(const double *__restrict__ part, int nblk, double invN3, double step, double time,
+                             double *__restrict__ row, int *__restrict__ flag)
+{
+    __shared__ double sh[32];
+    double a = 0, b = 0, c = 0, d = 0;
+    for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
+        a += part[q * 4 + 0];
+        b += part[q * 4 + 1];
+        c = fmax(c, part[q * 4 + 2]);
+        d = fmax(d, part[q * 4 + 3]);
+    }
+    a = block_reduce_sum(a, sh);
+    b = block_reduce_sum(b, sh);
+    c = block_reduce_max(c, sh);
+    d = block_reduce_max(d, sh);
+    if (threadIdx.x == 0) {
+        row[0] = step;
+        row[1] = time;
+        row[2] = a * invN3;
+        row[3] = b * invN3;
+        row[4] = c;
+        row[5] = d;
+        if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(d)) atomicExch(flag, 1);
+    }
+}
+
+template <class LD>
+__global__ void k_maxabs_part(long long n, LD f, double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    double m = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(f(0, t)));
+    m = block_reduce_max(m, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+__global__ void k_max_final(const double *__restrict__ part, int n, double *__restrict__ out)
+{
+    __shared__ double sh[32];
+    double m = 0.0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, part[q]);
+    m = block_reduce_max(m, sh);
+    if (threadIdx.x == 0) *out = m;
+}
+
+// --------------------------------------------------------------- operators --
+// Simple one-thread-per-node kernels for the drop-in ex:: entry points.
+
+template <int H>
+__global__ void k_op_grad_s(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ s,
+                            double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 S{s, g.N3};
+    double az[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+    out[t] = dd1<H>(S, g, 0, i, j, k, 0, co.a[0]);
+    out[g.N3 + t] = dd1<H>(S, g, 0, i, j, k, 1, co.a[1]);
+    out[2 * g.N3 + t] = dd1<H>(S, g, 0, i, j, k, 2, az);
+}
+
+// ex::grad(Field<vector>) keeps the reference's stencil c_l/(l+1)/delta*(f(+l) - f(-1-l)) (grad.cpp:82-94)
+template <int H>
+__global__ void k_op_grad_v(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+                            double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 F{U, g.N3};
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double r = 0.0;
+#pragma unroll
+            for (int l = 0; l < H; l++) {
+                double w = 2.0 * co.a[d][l];  // c_l/(l+1)/delta
+                if (d == 2) w *= ia[k];
+                r = fma(w, at(F, g, c, i, j, k, d, l) - at(F, g, c, i, j, k, d, -1 - l), r);
+            }
+            out[(long long)(3 * c + d) * g.N3 + t] = r;
+        }
+}
+
+// ex::curl = antisymmetric part of ex::grad(vector) (src/ex/curl/curl.cpp:44-50)
+template <int H>
+__global__ void k_op_curl(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+                          double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 F{U, g.N3};
+    auto gv = [&](int c, int d) {
+        double r = 0.0;
+#pragma unroll
+        for (int l = 0; l < H; l++) {
+            double w = 2.0 * co.a[d][l];
+            if (d == 2) w *= ia[k];
+            r = fma(w, at(F, g, c, i, j, k, d, l) - at(F, g, c, i, j, k, d, -1 - l), r);
+        }
+        return r;
+    };
+    out[t] = gv(2, 1) - gv(1, 2);
+    out[g.N3 + t] = gv(0, 2) - gv(2, 0);
+    out[2 * g.N3 + t] = gv(1, 0) - gv(0, 1);
+}
+
+template <int H>
+__global__ void k_op_div_v(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+                           double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 F{U, g.N3};
+    double az[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+    out[t] = dd1<H>(F, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(F, g, 1, i, j, k, 1, co.a[1])
+             + dd1<H>(F, g, 2, i, j, k, 2, az);
+}
+
+// skew div(U, f), f with nc components (src/ex/div/div.hxx:84-172)
+template <int H>
+__global__ void k_op_div_vf(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+                            const double *__restrict__ f, int nc, double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 V{U, g.N3}, F{f, g.N3};
+    double a[3][H];
+#pragma unroll
+    for (int l = 0; l < H; l++) {
+        a[0][l] = co.a[0][l];
+        a[1][l] = co.a[1][l];
+        a[2][l] = co.a[2][l] * ia[k];
+    }
+    double divU = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) divU += dd1<H>(V, g, d, i, j, k, d, a[d]);
+    for (int c = 0; c < nc; c++) {
+        const double f0 = F(c, t);
+        double acc = f0 * divU;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double dq = 0.0;
+#pragma unroll
+            for (int l = 0; l < H; l++)
+                dq = fma(a[d][l],
+                         at(V, g, d, i, j, k, d, l + 1) * at(F, g, c, i, j, k, d, l + 1)
+                             - at(V, g, d, i, j, k, d, -l - 1) * at(F, g, c, i, j, k, d, -l - 1),
+                         dq);
+            acc += dq + V(d, t) * dd1<H>(F, g, c, i, j, k, d, a[d]);
+        }
+        out[(long long)c * g.N3 + t] = 0.5 * acc;
+    }
+}
+
+// laplacian(nu, f) with the stretched-z term (src/ex/laplacian/laplacian.hxx:130-191)
+template <int H>
+__global__ void k_op_lap(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ corr2,
+                         double nu, const double *__restrict__ f, int nc, double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 F{f, g.N3};
+    const double i2 = ia[k] * ia[k];
+    for (int c = 0; c < nc; c++) {
+        const double f0 = F(c, t);
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double m = (d == 2) ? i2 : 1.0;
+            double s = 0.0;
+#pragma unroll
+            for (int l = 0; l < H; l++)
+                s = fma(co.b[d][l] * m, at(F, g, c, i, j, k, d, l + 1) + at(F, g, c, i, j, k, d, -l - 1), s);
+            r += fma(-co.b2[d] * m, f0, s);
+        }
+        double az[H];
+#pragma unroll
+        for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+        const double dz = dd1<H>(F, g, c, i, j, k, 2, az);
+        out[(long long)c * g.N3 + t] = nu * fma(-corr2[k], dz, r);
+    }
+}
+
+// ------------------------------------------------------------------ layout --
+// reference ghosted AoS (n0, n1, n2, nc) -> unique SoA
+__global__ void k_aos_to_soa(Geo g, int h, int n1, int n2, int nc, const double *__restrict__ aos,
+                             double *__restrict__ d64, float *__restrict__ hi, float *__restrict__ lo)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    const long long src = (((long long)(i + h) * n1 + (j + h)) * n2 + (k + h)) * nc;
+    for (int c = 0; c < nc; c++) {
+        const double x = aos[src + c];
+        if (d64) {
+            d64[(long long)c * g.N3 + t] = x;
+        } else {
+            const float xh = (float)x;
+            hi[(long long)c * g.N3 + t] = xh;
+            lo[(long long)c * g.N3 + t] = (float)(x - (double)xh);
+        }
+    }
+}
+
+// unique SoA -> ghosted AoS with every slot filled by periodic wrap
+// (interior incl. the duplicate node as periodicBC::update leaves it)
+__global__ void k_soa_to_aos(Geo g, int h, int n0, int n1, int n2, int nc, const double *__restrict__ d64,
+                             const float *__restrict__ hi, const float *__restrict__ lo, double *__restrict__ aos)
+{
+    const long long tot = (long long)n0 * n1 * n2;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= tot) return;
+    const int kk = (int)(t % n2);
+    const long long r = t / n2;
+    const int jj = (int)(r % n1);
+    const int ii = (int)(r / n1);
+    const long long s = (long long)wrapi(ii - h, g.N0) * g.N12 + (long long)wrapi(jj - h, g.N1) * g.N2
+                        + wrapi(kk - h, g.N2);
+    for (int c = 0; c < nc; c++) {
+        const long long o = (long long)c * g.N3 + s;
+        aos[t * nc + c] = d64 ? d64[o] : (double)hi[o] + (double)lo[o];
+    }
+}
+
+__global__ void k_split(long long n, const double *__restrict__ x, float *__restrict__ hi, float *__restrict__ lo)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double v = x[t];
+    const float h = (float)v;
+    hi[t] = h;
+    lo[t] = (float)(v - (double)h);
+}
+
+__global__ void k_join(long long n, const float *__restrict__ hi, const float *__restrict__ lo, double *__restrict__ x)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    x[t] = (double)hi[t] + (double)lo[t];
+}
+
+inline unsigned nblocks(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers --
+#define NOVA_DISPATCH_H(h, ...)                 \
+    switch (h) {                                \
+    case 1: { constexpr int HH = 1; __VA_ARGS__; } break; \
+    case 2: { constexpr int HH = 2; __VA_ARGS__; } break; \
+    case 3: { constexpr int HH = 3; __VA_ARGS__; } break; \
+    default: { constexpr int HH = 4; __VA_ARGS__; } break; \
+    }
+
+void launch_div_proj(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64,
+                     const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st)
+{
+    const unsigned nb = nblocks(g.N3, 256);
+    if (U64) {
+        NOVA_DISPATCH_H(h, (k_div_proj<HH, Ld64><<<nb, 256, 0, st>>>(g, co, ia, Ld64{U64, g.N3}, divisor, rhs)));
+    } else {
+        NOVA_DISPATCH_H(h, (k_div_proj<HH, LdSplit><<<nb, 256, 0, st>>>(g, co, ia, LdSplit{hi, lo, g.N3}, divisor, rhs)));
+    }
+}
+
+void launch_scale(const Geo &g, void *spec, const double *kx2, const double *ky2, const double *kz2, double invN3,
+                  cudaStream_t st)
+{
+    const long long tot = (long long)g.N0 * g.N1 * (g.N2 / 2 + 1);
+    k_scale<<<nblocks(tot, 256), 256, 0, st>>>(g, (cuDoubleComplex *)spec, kx2, ky2, kz2, invN3);
+}
+
+void launch_correct(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,
+                    const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi, float *lo,
+                    cudaStream_t st)
+{
+    const unsigned nb = nblocks(g.N3, 256);
+    if (U64) {
+        NOVA_DISPATCH_H(h, (k_correct64<HH><<<nb, 256, 0, st>>>(g, co, ia, p, s, Us64, U64)));
+    } else {
+        NOVA_DISPATCH_H(h, (k_correct32<HH><<<nb, 256, 0, st>>>(g, co, ia, p, s, Ushi, Uslo, hi, lo)));
+    }
+}
+
+int diag_blocks(const Geo &g)
+{
+    long long b = (g.N3 + 255) / 256;
+    return (int)(b < 1184 ? b : 1184);
+}
+
+void launch_diag(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *Uhi,
+                 const float *Ulo, const double *B64, const float *Bhi, const float *Blo, int hasB, double *part,
+                 double step, double time, double *row, int *flag, cudaStream_t st)
+{
+    const int nb = diag_blocks(g);
+    if (U64) {
+        Ld64 U{U64, g.N3}, B{hasB ? B64 : U64, g.N3};
+        NOVA_DISPATCH_H(h, (k_diag<HH, Ld64><<<nb, kRedThreads, 0, st>>>(g, co, ia, U, B, hasB, part)));
+    } else {
+        LdSplit U{Uhi, Ulo, g.N3}, B{hasB ? Bhi : Uhi, hasB ? Blo : Ulo, g.N3};
+        NOVA_DISPATCH_H(h, (k_diag<HH, LdSplit><<<nb, kRedThreads, 0, st>>>(g, co, ia, U, B, hasB, part)));
+    }
+    k_diag_final<<<1, 256, 0, st>>>(part, nb, 1.0 / (double)g.N3, step, time, row, flag);
+}
+
+void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st)
+{
+    const int nb = diag_blocks(g);
+    k_maxabs_part<<<nb, 256, 0, st>>>(g.N3, Ld64{s, g.N3}, part);
+    k_max_final<<<1, 256, 0, st>>>(part, nb, out);
+}
+
+void launch_op(int op, int h, const Geo &g, const Coef<double> &co, const double *ia, const double *corr2,
+               const double *a, const double *b, int nc, double nu, double *out, cudaStream_t st)
+{
+    const unsigned nb = nblocks(g.N3, 128);
+    switch (op) {
+    case OP_GRAD_S: NOVA_DISPATCH_H(h, (k_op_grad_s<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
+    case OP_GRAD_V: NOVA_DISPATCH_H(h, (k_op_grad_v<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
+    case OP_DIV_V: NOVA_DISPATCH_H(h, (k_op_div_v<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
+    case OP_CURL: NOVA_DISPATCH_H(h, (k_op_curl<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
+    case OP_DIV_VF: NOVA_DISPATCH_H(h, (k_op_div_vf<HH><<<nb, 128, 0, st>>>(g, co, ia, a, b, nc, out))); break;
+    default: NOVA_DISPATCH_H(h, (k_op_lap<HH><<<nb, 128, 0, st>>>(g, co, ia, corr2, nu, a, nc, out))); break;
+    }
+}
+
+void launch_aos_to_soa(const Geo &g, int h, const int n[3], int nc, const double *aos, double *d64, float *hi,
+                       float *lo, cudaStream_t st)
+{
+    k_aos_to_soa<<<nblocks(g.N3, 256), 256, 0, st>>>(g, h, n[1], n[2], nc, aos, d64, hi, lo);
+}
+
+void launch_soa_to_aos(const Geo &g, int h, const int n[3], int nc, const double *d64, const float *hi,
+                       const float *lo, double *aos, cudaStream_t st)
+{
+    const long long tot = (long long)n[0] * n[1] * n[2];
+    k_soa_to_aos<<<nblocks(tot, 256), 256, 0, st>>>(g, h, n[0], n[1], n[2], nc, d64, hi, lo, aos);
+}
+
+void launch_split(long long n, const double *x, float *hi, float *lo, cudaStream_t st)
+{
+    k_split<<<nblocks(n, 256), 256, 0, st>>>(n, x, hi, lo);
+}
+
+void launch_join(long long n, const float *hi, const float *lo, double *x, cudaStream_t st)
+{
+    k_join<<<nblocks(n, 256), 256, 0, st>>>(n, hi, lo, x);
+}
+
+}  // namespace nova

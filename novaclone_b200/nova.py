@@ -1,0 +1,337 @@
+"""ctypes binding of libnova_b200 (include/nova_gpu.h) with the reference's names.
+
+The reference is C++ (``Mesh``, ``Field<T>``, ``ex::grad/div/curl/laplacian``,
+``poisson``, ``tools::maximum``); this module gives the same operations to
+Python callers over the C ABI.  Everything here is a thin wrapper: every
+computation runs in the CUDA library, and importing fails loudly if the
+library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libnova_b200.so")
+
+OK, E_INVALID, E_CUDA, E_OOM, E_NONFINITE, E_TIMEOUT, E_UNSUPPORTED = range(7)
+F64, F32SPLIT = 0, 1
+PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
+MODEL_NS, MODEL_MHD = 0, 1
+RK_LITERAL, RK_CLASSICAL = 0, 1
+HIST_COLS = 6
+K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG = range(5)
+STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_OOM", 4: "NOVA_E_NONFINITE",
+                5: "NOVA_E_TIMEOUT", 6: "NOVA_E_UNSUPPORTED"}
+
+# every symbol declared in include/nova_gpu.h
+EXPORTS = (
+    "nova_create", "nova_destroy", "nova_last_error", "nova_set_stream", "nova_synchronize", "nova_mesh_local_n",
+    "nova_mesh_metrics", "nova_field_create", "nova_field_destroy", "nova_field_upload", "nova_field_download",
+    "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
+    "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
+    "nova_field_maxabs", "nova_advance", "nova_profile_enable", "nova_profile_read", "nova_launch_count",
+)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("N", C.c_int * 3), ("L", C.c_double * 3), ("origin", C.c_double * 3), ("m", C.c_int),
+                ("hyperbolic_z", C.c_int), ("s1", C.c_double), ("s2", C.c_double)]
+
+
+class BCDesc(C.Structure):
+    _fields_ = [("type", C.c_int * 18), ("val", C.c_double * 18)]
+
+
+class RunDesc(C.Structure):
+    _fields_ = [("model", C.c_int), ("rk_mode", C.c_int), ("precision", C.c_int), ("diag_every", C.c_int),
+                ("dt", C.c_double), ("nu", C.c_double), ("eta", C.c_double), ("t0", C.c_double)]
+
+
+class State(C.Structure):
+    _fields_ = [("U", C.c_void_p), ("p", C.c_void_p), ("B", C.c_void_p), ("pB", C.c_void_p)]
+
+
+class NovaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), msg))
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libnova_b200.so; raises if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("libnova_b200.so not built: run `python -m novaclone_b200.build` (%s)" % path)
+    L = C.CDLL(path)
+    vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    sig = {
+        "nova_create": [C.POINTER(MeshDesc), C.POINTER(C.c_void_p)],
+        "nova_destroy": [vp],
+        "nova_set_stream": [vp, vp],
+        "nova_synchronize": [vp],
+        "nova_mesh_local_n": [vp, ip],
+        "nova_mesh_metrics": [vp, dp, dp],
+        "nova_field_create": [vp, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+        "nova_field_destroy": [vp, vp],
+        "nova_field_upload": [vp, vp, dp, ip],
+        "nova_field_download": [vp, vp, dp, ip, C.POINTER(BCDesc)],
+        "nova_field_upload_soa": [vp, vp, dp],
+        "nova_field_download_soa": [vp, vp, dp],
+        "nova_field_copy_from_device": [vp, vp, vp],
+        "nova_field_copy_to_device": [vp, vp, vp],
+        "nova_grad_s": [vp, vp, vp],
+        "nova_grad_v": [vp, vp, vp],
+        "nova_curl": [vp, vp, vp],
+        "nova_div_v": [vp, vp, vp],
+        "nova_div_vf": [vp, vp, vp, vp],
+        "nova_laplacian": [vp, C.c_double, vp, vp],
+        "nova_poisson_solve": [vp, vp, vp],
+        "nova_field_maxabs": [vp, vp, dp],
+        "nova_advance": [vp, C.POINTER(RunDesc), C.POINTER(State), C.c_int, dp],
+        "nova_profile_enable": [vp, C.c_int],
+        "nova_profile_read": [vp, C.c_int, dp, C.POINTER(C.c_long), C.c_int],
+        "nova_launch_count": [vp, C.POINTER(C.c_long), C.c_int],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.nova_last_error.argtypes = [vp]
+    L.nova_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Mesh:
+    """A nova_ctx: the reference's Mesh for one GPU (src/Mesh/Mesh.cpp:24-179)."""
+
+    def __init__(self, N, L=(2 * math.pi,) * 3, origin=(0.0, 0.0, 0.0), m=6, hyperbolic_z=None):
+        self.lib = load_library()
+        d = MeshDesc()
+        d.N[:] = [int(v) for v in N]
+        d.L[:] = [float(v) for v in L]
+        d.origin[:] = [float(v) for v in origin]
+        d.m = int(m)
+        d.hyperbolic_z = int(hyperbolic_z is not None)
+        d.s1, d.s2 = hyperbolic_z if hyperbolic_z is not None else (0.0, 0.0)
+        h = C.c_void_p()
+        st = self.lib.nova_create(C.byref(d), C.byref(h))
+        if st != OK:
+            raise NovaError(st, "nova_create")
+        self.h = h
+        self.N = tuple(int(v) for v in N)
+        self.L = tuple(float(v) for v in L)
+        self.origin = tuple(float(v) for v in origin)
+        self.m = int(m)
+        n = np.zeros(3, np.int32)
+        self.check(self.lib.nova_mesh_local_n(self.h, _iptr(n)))
+        self.local_n = tuple(int(v) for v in n)
+
+    def check(self, st, what=""):
+        if st != OK:
+            raise NovaError(st, self.lib.nova_last_error(self.h).decode() or what)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nova_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def d(self):
+        return tuple(self.L[a] / self.N[a] for a in range(3))
+
+    def metrics(self):
+        a = np.zeros(self.local_n[2])
+        b = np.zeros(self.local_n[2])
+        self.check(self.lib.nova_mesh_metrics(self.h, _dptr(a), _dptr(b)))
+        return a, b
+
+    def set_stream(self, stream_ptr):
+        self.check(self.lib.nova_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        self.check(self.lib.nova_synchronize(self.h))
+
+    def profile(self, on=True):
+        self.check(self.lib.nova_profile_enable(self.h, int(on)))
+
+    def profile_read(self, cls, reset=False):
+        ms = C.c_double()
+        n = C.c_long()
+        self.check(self.lib.nova_profile_read(self.h, cls, C.byref(ms), C.byref(n), int(reset)))
+        return ms.value, n.value
+
+    def launch_count(self, reset=False):
+        n = C.c_long()
+        self.check(self.lib.nova_launch_count(self.h, C.byref(n), int(reset)))
+        return n.value
+
+
+class Field:
+    """Device field with ncomp components (Field<T>, src/Field/Field.h:56-157)."""
+
+    def __init__(self, mesh: Mesh, ncomp: int, precision: int = F64):
+        self.mesh = mesh
+        self.nc = int(ncomp)
+        self.precision = precision
+        h = C.c_void_p()
+        mesh.check(mesh.lib.nova_field_create(mesh.h, self.nc, precision, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and self.mesh.h:
+            self.mesh.lib.nova_field_destroy(self.mesh.h, self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # reference Field<T>::ptr() layout
+    def upload(self, aos):
+        a = np.ascontiguousarray(aos, np.float64)
+        if a.shape[:3] != self.mesh.local_n:
+            raise ValueError("expected ghosted shape %s, got %s" % (self.mesh.local_n, a.shape))
+        n = np.array(self.mesh.local_n, np.int32)
+        self.mesh.check(self.mesh.lib.nova_field_upload(self.mesh.h, self.h, _dptr(a), _iptr(n)))
+        return self
+
+    def download(self, bc=None):
+        out = np.zeros(self.mesh.local_n + (self.nc,))
+        n = np.array(self.mesh.local_n, np.int32)
+        bcp = None
+        if bc is not None:
+            b = BCDesc()
+            b.type[:] = list(bc[0])
+            b.val[:] = list(bc[1])
+            bcp = C.byref(b)
+        self.mesh.check(self.mesh.lib.nova_field_download(self.mesh.h, self.h, _dptr(out), _iptr(n), bcp))
+        return out
+
+    # device-native layout [c][i][j][k]
+    def upload_soa(self, soa):
+        a = np.ascontiguousarray(soa, np.float64)
+        if a.size != self.nc * int(np.prod(self.mesh.N)):
+            raise ValueError("wrong size")
+        self.mesh.check(self.mesh.lib.nova_field_upload_soa(self.mesh.h, self.h, _dptr(a)))
+        return self
+
+    def download_soa(self):
+        out = np.zeros((self.nc,) + self.mesh.N)
+        self.mesh.check(self.mesh.lib.nova_field_download_soa(self.mesh.h, self.h, _dptr(out)))
+        return out
+
+    def copy_from_device(self, dev_ptr):
+        self.mesh.check(self.mesh.lib.nova_field_copy_from_device(self.mesh.h, self.h, C.c_void_p(dev_ptr)))
+
+    def copy_to_device(self, dev_ptr):
+        self.mesh.check(self.mesh.lib.nova_field_copy_to_device(self.mesh.h, self.h, C.c_void_p(dev_ptr)))
+
+
+class ex:
+    """The reference's explicit operators (src/ex), each one C-ABI call."""
+
+    @staticmethod
+    def grad(f: Field) -> Field:
+        M = f.mesh
+        if f.nc == 1:
+            out = Field(M, 3)
+            M.check(M.lib.nova_grad_s(M.h, f.h, out.h))
+        else:
+            out = Field(M, 9)
+            M.check(M.lib.nova_grad_v(M.h, f.h, out.h))
+        return out
+
+    @staticmethod
+    def div(U: Field, f: Field = None) -> Field:
+        M = U.mesh
+        if f is None:
+            out = Field(M, 1)
+            M.check(M.lib.nova_div_v(M.h, U.h, out.h))
+        else:
+            out = Field(M, f.nc)
+            M.check(M.lib.nova_div_vf(M.h, U.h, f.h, out.h))
+        return out
+
+    @staticmethod
+    def curl(U: Field) -> Field:
+        M = U.mesh
+        out = Field(M, 3)
+        M.check(M.lib.nova_curl(M.h, U.h, out.h))
+        return out
+
+    @staticmethod
+    def laplacian(nu: float, f: Field) -> Field:
+        M = f.mesh
+        out = Field(M, f.nc)
+        M.check(M.lib.nova_laplacian(M.h, float(nu), f.h, out.h))
+        return out
+
+
+class poisson:
+    """poisson(p): rhs(f) then solve() writes p (src/poisson/poisson.h:36-115)."""
+
+    def __init__(self, p: Field):
+        self.p = p
+        self._rhs = None
+
+    def rhs(self, f: Field):
+        self._rhs = f
+
+    def solve(self):
+        M = self.p.mesh
+        M.check(M.lib.nova_poisson_solve(M.h, self._rhs.h, self.p.h))
+
+
+class tools:
+    @staticmethod
+    def maximum(f: Field) -> float:
+        M = f.mesh
+        v = C.c_double()
+        M.check(M.lib.nova_field_maxabs(M.h, f.h, C.byref(v)))
+        return v.value
+
+
+def run_desc(model="ns", rk_mode="classical", precision=F64, dt=0.01, nu=0.0, eta=0.0, diag_every=1, t0=0.0):
+    r = RunDesc()
+    r.model = MODEL_MHD if model == "mhd" else MODEL_NS
+    r.rk_mode = RK_CLASSICAL if rk_mode == "classical" else RK_LITERAL
+    r.precision = precision
+    r.diag_every = diag_every
+    r.dt, r.nu, r.eta, r.t0 = float(dt), float(nu), float(eta), float(t0)
+    return r
+
+
+def advance(mesh: Mesh, rd: RunDesc, U: Field, p: Field, B: Field = None, pB: Field = None, nsteps: int = 1,
+            history: bool = True):
+    """nsteps of the reference loop body; returns the (nsteps, 6) history or None."""
+    st = State(U.h, p.h, B.h if B is not None else None, pB.h if pB is not None else None)
+    hist = np.zeros((max(nsteps, 1), HIST_COLS)) if history else None
+    mesh.check(mesh.lib.nova_advance(mesh.h, C.byref(rd), C.byref(st), int(nsteps),
+                                     _dptr(hist) if history else None))
+    return hist

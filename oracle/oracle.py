@@ -280,7 +280,7 @@ def ref_run(mesh, U, B=None, *, model="ns", rk_mode="classical", nsteps=1, dt=0.
             np.ascontiguousarray(B, np.float64).tofile(bpath)
         out = os.path.join(td, "out")
         subprocess.run([REF_BIN, "run", case, model, rk_mode, str(nsteps), repr(float(dt)), repr(float(nu)),
-                        repr(float(eta)), os.path.join(td, "U.bin"), bpath, out],
+                        repr(float(eta)), os.path.join(td, "U.bin"), bpath, out, "-m", str(mesh.m)],
                        check=True, stdout=subprocess.DEVNULL)
         shp3 = mesh.n + (3,)
         shp1 = mesh.n + (1,)
@@ -302,7 +302,7 @@ def ref_ops(mesh, U, s, nu):
         np.ascontiguousarray(s, np.float64).tofile(os.path.join(td, "s.bin"))
         out = os.path.join(td, "out")
         subprocess.run([REF_BIN, "ops", case, repr(float(nu)), os.path.join(td, "U.bin"),
-                        os.path.join(td, "s.bin"), out], check=True, stdout=subprocess.DEVNULL)
+                        os.path.join(td, "s.bin"), out, "-m", str(mesh.m)], check=True, stdout=subprocess.DEVNULL)
         return {k: np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (nc,)) for k, nc in names.items()}
 
 

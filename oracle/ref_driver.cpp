@@ -9,6 +9,7 @@
  *
  *   nova_ref run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U.bin> <B.bin|-> <out>
  *   nova_ref ops <case> <nu> <U.bin> <s.bin> <out>
+ *   (either may end with the reference's `-m <order>` option)
  *
  * <case> holds `mesh` and the BC files (UBC, pBC, BBC, pBBC).
  */
@@ -196,7 +197,8 @@ static int ops(int argc, char **argv)
 
 int main(int argc, char **argv)
 {
-    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops ...\n"); return 2; }
+    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops ... [-m order]\n"); return 2; }
+    settings::process(argc, argv); /* the reference's own -m option (settings.cpp:53-78) */
     std::string mode = argv[1];
     if (mode == "run") return run(argc, argv);
     if (mode == "ops") return ops(argc, argv);

@@ -1,0 +1,119 @@
+"""GPU parity of the ex:: drop-in operators and the Poisson solve, through the
+C ABI, against the oracle (same seeded inputs) and the reference's golden
+vectors.  FP64: relative max error <= 1e-12 (operators are O(1/dx^2) sums of
+O(1) inputs, so this bounds a few ulps of the largest term)."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_max
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def nova():
+    from novaclone_b200 import nova
+    return nova
+
+
+SIZES = [((10, 8, 6), (2 * np.pi, 2.0, 3.0), 6), ((33, 17, 40), (2 * np.pi,) * 3, 6), ((16, 12, 8), (1.0, 2.0, 3.0), 4),
+         ((8, 8, 8), (2 * np.pi,) * 3, 2), ((12, 10, 20), (2 * np.pi,) * 3, 8), ((3, 5, 7), (1.0, 1.0, 1.0), 6)]
+
+
+@pytest.mark.parametrize("N,L,m", SIZES)
+def test_operators_vs_oracle(nova, oracle, N, L, m):
+    rng = np.random.default_rng(11)
+    OM = oracle.Mesh(N, L=L, m=m)
+    GM = nova.Mesh(N, L=L, m=m)
+    U = rng.standard_normal((3,) + N)
+    s = rng.standard_normal((1,) + N)
+    Ug, sg = OM.to_ghosted(U), OM.to_ghosted(s)
+    dU = nova.Field(GM, 3).upload(Ug)
+    ds = nova.Field(GM, 1).upload(sg)
+    nu = 0.013
+    cases = {
+        "grad_s": (nova.ex.grad(ds), oracle.grad_s(OM, sg)),
+        "grad_v": (nova.ex.grad(dU), oracle.grad_v(OM, Ug)),
+        "div_v": (nova.ex.div(dU), oracle.div_v(OM, Ug)),
+        "div_vv": (nova.ex.div(dU, dU), oracle.div_vf(OM, Ug, Ug)),
+        "div_vs": (nova.ex.div(dU, ds), oracle.div_vf(OM, Ug, sg)),
+        "curl": (nova.ex.curl(dU), oracle.curl(OM, Ug)),
+        "lap_v": (nova.ex.laplacian(nu, dU), oracle.lap(OM, nu, Ug)),
+        "lap_s": (nova.ex.laplacian(nu, ds), oracle.lap(OM, nu, sg)),
+    }
+    for name, (g, o) in cases.items():
+        got = OM.interior(g.download())
+        ref = OM.interior(o)
+        assert rel_max(got, ref) < TOL, (name, rel_max(got, ref))
+
+
+@pytest.mark.parametrize("name", ["ops_10x8x6.npz", "ops_16x12x8_m4.npz"])
+def test_operators_vs_reference_golden(nova, oracle, name):
+    g = load_golden(name)
+    N, L, m = tuple(int(v) for v in g["N"]), tuple(g["L"]), int(g["m"])
+    OM = oracle.Mesh(N, L=L, m=m)
+    GM = nova.Mesh(N, L=L, m=m)
+    dU = nova.Field(GM, 3).upload(OM.to_ghosted(g["U"]))
+    ds = nova.Field(GM, 1).upload(OM.to_ghosted(g["s"]))
+    nu = float(g["nu"])
+    p = nova.Field(GM, 1)
+    pe = nova.poisson(p)
+    pe.rhs(ds)
+    pe.solve()
+    got = {"grad_s": nova.ex.grad(ds), "div_v": nova.ex.div(dU), "div_vv": nova.ex.div(dU, dU),
+           "div_vs": nova.ex.div(dU, ds), "lap_v": nova.ex.laplacian(nu, dU), "lap_s": nova.ex.laplacian(nu, ds),
+           "curl": nova.ex.curl(dU)}
+    for k, f in got.items():
+        assert rel_max(OM.interior(f.download()), g["out_" + k]) < TOL, k
+    # poisson::solve writes only the N^3 unique nodes (the duplicate node stays as it was)
+    ref_p = g["out_poisson"][:, :N[0], :N[1], :N[2]]
+    assert rel_max(p.download_soa(), ref_p) < TOL
+
+
+@pytest.mark.parametrize("N", [(16, 16, 16), (24, 12, 18), (9, 6, 15)])
+def test_poisson_vs_oracle(nova, oracle, N):
+    rng = np.random.default_rng(2)
+    OM = oracle.Mesh(N)
+    GM = nova.Mesh(N)
+    s = rng.standard_normal((1,) + N)
+    ds = nova.Field(GM, 1).upload(OM.to_ghosted(s))
+    p = nova.Field(GM, 1)
+    pe = nova.poisson(p)
+    pe.rhs(ds)
+    pe.solve()
+    ref = OM.unique(oracle.poisson_solve(OM, OM.to_ghosted(s)))
+    assert rel_max(p.download_soa(), ref) < TOL
+
+
+def test_maximum_and_layout_round_trip(nova, oracle):
+    N = (12, 10, 14)
+    rng = np.random.default_rng(4)
+    OM = oracle.Mesh(N)
+    GM = nova.Mesh(N)
+    U = rng.standard_normal((3,) + N)
+    f = nova.Field(GM, 3).upload(OM.to_ghosted(U))
+    assert np.array_equal(f.download(), OM.to_ghosted(U))       # ghosts = periodic images
+    assert np.array_equal(f.download_soa(), U)
+    d = nova.ex.div(f)
+    assert nova.tools.maximum(d) == pytest.approx(oracle.maximum(OM, oracle.div_v(OM, OM.to_ghosted(U))), rel=1e-12)
+
+
+def test_split_field_holds_48_bits(nova):
+    N = (8, 8, 8)
+    GM = nova.Mesh(N)
+    x = np.random.default_rng(5).standard_normal((3,) + N) * 3.0
+    f = nova.Field(GM, 3, nova.F32SPLIT).upload_soa(x)
+    assert np.abs(f.download_soa() - x).max() <= 4e-14 * np.abs(x).max()
+
+
+def test_operator_argument_errors(nova):
+    GM = nova.Mesh((8, 8, 8))
+    a = nova.Field(GM, 3)
+    s = nova.Field(GM, 1)
+    with pytest.raises(nova.NovaError) as e:
+        GM.check(GM.lib.nova_grad_s(GM.h, a.h, s.h))  # wrong component counts
+    assert e.value.status == nova.E_INVALID
+    with pytest.raises(nova.NovaError):
+        nova.Field(GM, 3).upload(np.zeros((5, 5, 5, 3)))

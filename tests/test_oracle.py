@@ -1,0 +1,124 @@
+"""CPU tests of the oracle: pinned against the reference's golden vectors
+(tests/golden, produced by the reference compiled in place), against numpy's
+FFT, and against the analytic identities of the central stencils."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_max
+
+
+def test_fft_matches_numpy():
+    import ctypes as C
+    from oracle import oracle as O
+    lib = C.CDLL(O.LIB_PATH)
+    rng = np.random.default_rng(3)
+    for n in [(8, 6, 5), (12, 9, 16), (24, 18, 12), (1, 4, 3), (7, 11, 13)]:
+        a = rng.standard_normal(n[::-1]) + 1j * rng.standard_normal(n[::-1])
+        buf = np.ascontiguousarray(np.stack([a.real, a.imag], -1))
+        for sign, ref in ((-1, np.fft.fftn(a)), (+1, np.fft.ifftn(a) * a.size)):
+            b = buf.copy()
+            lib.orc_fft3d(np.array(n, np.int32).ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), sign)
+            got = b[..., 0] + 1j * b[..., 1]
+            assert np.abs(got - ref).max() / np.abs(ref).max() < 5e-15
+
+
+@pytest.mark.parametrize("name", ["ops_10x8x6.npz", "ops_16x12x8_m4.npz"])
+def test_operators_bitwise_vs_reference_golden(oracle, name):
+    g = load_golden(name)
+    M = oracle.Mesh(tuple(g["N"]), L=tuple(g["L"]), m=int(g["m"]))
+    U = M.to_ghosted(g["U"])
+    s = M.to_ghosted(g["s"])
+    nu = float(g["nu"])
+    mine = {"grad_s": oracle.grad_s(M, s), "div_v": oracle.div_v(M, U), "div_vv": oracle.div_vf(M, U, U),
+            "div_vs": oracle.div_vf(M, U, s), "lap_v": oracle.lap(M, nu, U), "lap_s": oracle.lap(M, nu, s),
+            "curl": oracle.curl(M, U), "poisson": oracle.poisson_solve(M, s)}
+    for k, v in mine.items():
+        assert np.array_equal(M.interior(v), g["out_" + k]), k
+
+
+@pytest.mark.parametrize("name", ["tg_12_classical.npz", "tg_12_literal.npz", "ot_12_classical.npz",
+                                  "ot_12_literal.npz"])
+def test_time_loop_bitwise_vs_reference_golden(oracle, name):
+    g = load_golden(name)
+    M = oracle.Mesh(tuple(g["N"]), L=tuple(g["L"]))
+    model = str(g["model"])
+    B0 = M.to_ghosted(g["B0"]) if model == "mhd" else None
+    U, B, p, pB, hist = oracle.run(M, M.to_ghosted(g["U0"]), B0, model=model, rk_mode=str(g["rk_mode"]),
+                                   nsteps=int(g["nsteps"]), dt=float(g["dt"]), nu=float(g["nu"]),
+                                   eta=float(g["eta"]))
+    assert np.array_equal(M.unique(U), g["U"])
+    assert np.array_equal(M.unique(p), g["p"])
+    assert np.array_equal(hist, g["hist"])
+    if model == "mhd":
+        assert np.array_equal(M.unique(B), g["B"])
+        assert np.array_equal(M.unique(pB), g["pB"])
+
+
+def test_live_reference_matches_restatement_with_walls(oracle):
+    """Neumann/Dirichlet walls and the periodic solve of the wall case (Q8) vs the reference build."""
+    if not oracle.ref_available():
+        pytest.skip("reference not compiled here (make -C oracle ref)")
+    M = oracle.Mesh((12, 10, 8))
+    rng = np.random.default_rng(1)
+    U0 = M.to_ghosted(oracle.ic_taylor_green(M) + 0.1 * rng.standard_normal((3,) + M.N))
+    wallU = {"north": [(1, 0.0), (2, 0.3), (1, 0.1)], "south": [(1, 0.2), (2, 0.0), (1, 0.0)],
+             "top": [(2, 0.1), (1, 0.0), (2, 0.0)], "bottom": [(1, 0.0), (1, 0.5), (2, 0.0)]}
+    wallp = {"north": (1, 0.0), "south": (1, 0.0)}
+    for mode in ("literal", "classical"):
+        r = oracle.ref_run(M, U0, model="ns", rk_mode=mode, nsteps=3, dt=0.01, nu=1e-2,
+                           bc={"U": wallU, "p": wallp})
+        o = oracle.run(M, U0, model="ns", rk_mode=mode, nsteps=3, dt=0.01, nu=1e-2, bcU=wallU, bcp=wallp)
+        assert np.array_equal(r[0], o[0]) and np.array_equal(r[2], o[2]) and np.array_equal(r[4], o[4])
+
+
+def test_first_derivative_modified_wavenumber(oracle):
+    """D_x sin(kx) = k'(k) cos(kx), k' = sum_l c_l/(l+1) sin((l+1)k dx)/dx (exact for central stencils)."""
+    N = (32, 8, 8)
+    M = oracle.Mesh(N)
+    x = M.coords()[0]
+    dx = M.d[0]
+    for kk in (1, 3, 7, 15):
+        f = np.broadcast_to(np.sin(kk * x)[:, None, None], N)[None]
+        g = M.unique(oracle.grad_s(M, M.to_ghosted(f)))[0]
+        c = [1.5, -0.6, 0.1]
+        kp = sum(c[l] / (l + 1) * np.sin((l + 1) * kk * dx) / dx for l in range(3))
+        assert rel_max(g, kp * np.cos(kk * x)[:, None, None] * np.ones(N)) < 1e-12
+
+
+def test_laplacian_symbol(oracle):
+    N = (8, 32, 8)
+    M = oracle.Mesh(N)
+    y = M.coords()[1]
+    dy = M.d[1]
+    kk = 5
+    f = np.broadcast_to(np.sin(kk * y)[None, :, None], N)[None]
+    lap = M.unique(oracle.lap(M, 1.0, M.to_ghosted(f)))[0]
+    c = [1.5, -0.6, 0.1]
+    sym = -sum(2 * c[l] * (1 - np.cos((l + 1) * kk * dy)) / ((l + 1) * dy) ** 2 for l in range(3))
+    assert rel_max(lap, sym * np.sin(kk * y)[None, :, None] * np.ones(N)) < 1e-11
+
+
+def test_projection_makes_discrete_divergence_vanish(oracle):
+    M = oracle.Mesh((16, 12, 10))
+    rng = np.random.default_rng(5)
+    U = M.to_ghosted(rng.standard_normal((3,) + M.N))
+    d0 = oracle.maximum(M, oracle.div_v(M, U))
+    p = oracle.poisson_solve(M, oracle.div_v(M, U))
+    p = oracle.bc_apply(M, p)
+    U2 = oracle.bc_apply(M, U - oracle.grad_s(M, p))
+    d1 = oracle.maximum(M, oracle.div_v(M, U2))
+    assert d0 > 1.0 and d1 < 1e-12
+
+
+def test_taylor_green_initial_field_is_discretely_solenoidal(oracle):
+    M = oracle.Mesh((24, 24, 24))
+    U = M.to_ghosted(oracle.ic_taylor_green(M))
+    assert oracle.maximum(M, oracle.div_v(M, U)) < 1e-13
+
+
+def test_metrics_of_uniform_mesh(oracle):
+    """Mesh::dzdxi_ is 1 and d2zdxi2_ is 0 up to round-off on a uniform mesh."""
+    M = oracle.Mesh((8, 8, 256))
+    h = M.h
+    assert np.abs(M.dzdxi[h:-h] - 1).max() < 1e-12
+    assert np.abs(M.d2zdxi2[h:-h]).max() < 1e-9
