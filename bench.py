@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit time advance: Mpoint-steps/s on one B200.
+
+Workload: Taylor-Green vortex, incompressible, periodic [0,2pi]^3 at 256^3,
+classical RK4 (four fused stage kernels) + one FFT pressure projection per
+step, nu = 1/1600, dt fixed from CFL 0.3 of the initial field.  A step is one
+call of the reference's loop body (app/TG_Piosson/RKLoop.H in its
+stage-refreshed form).  Synthetic data: the analytic initial field.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--n 256]
+
+One JSON line on rank 0.  `value` is the FP64 path with the state resident in
+HBM; the FP32-split path (FP32 stencils, (hi,lo) state, FP64 projection) is
+reported beside it with its error against FP64.  `e2e` runs the same steps
+through the reference-layout C ABI with host buffers: the ghosted
+array-of-structs field is uploaded from pinned memory, the diagnostics row is
+read back every step and the final field is downloaded, all inside the timed
+region.  With N > 1 GPUs each rank advances its own replica (the reference
+path does not shard on one GPU per rank here), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpoint-steps/s at 256^3: FP64 vs FP32-split (stated err); adjoint/fwd time ratio"
+UNIT = "Mpoint-steps/s"
+NU = 1.0 / 1600.0
+CFL = 0.3
+# algorithmic HBM bytes per grid point for one classical RK4 step of the NS
+# stage kernels (3 components): FP64 stages 72 + 120 + 120 + 72; FP32-split
+# stages 36 + 60 + 60 + 72 (see the stage-kernel epilogue in nova_stage.cu)
+STAGE_BYTES = {"f64": 384.0, "f32split": 228.0}
+STAGE_LAUNCHES_PER_STEP = 4
+
+
+def workload_config(n, extra=None):
+    c = {"workload": "Taylor-Green vortex, incompressible, periodic [0,2pi]^3, %d^3, classical RK4 + FFT "
+                     "projection per step, nu=1/1600, CFL 0.3" % n,
+         "grid": [n, n, n], "rk": "classical", "stencil_order": 6,
+         "l2": "inputs larger than L2 (FP64 state %.0f MB)" % (3 * 8 * n ** 3 / 1e6),
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def tg_field(n):
+    x = np.arange(n) * (2 * math.pi / n)
+    s, c = np.sin(x), np.cos(x)
+    u = s[:, None, None] * c[None, :, None] * c[None, None, :]
+    v = -c[:, None, None] * s[None, :, None] * c[None, None, :]
+    return np.stack([u, v, np.zeros_like(u)])
+
+
+def ghosted(U, h=3):
+    """(3, n, n, n) unique nodes -> the reference's ghosted AoS Field<vector> layout (periodic images)."""
+    n = U.shape[1]
+    idx = (np.arange(n + 1 + 2 * h) - h) % n
+    g = U[:, idx][:, :, idx][:, :, :, idx]
+    return np.ascontiguousarray(np.moveaxis(g, 0, -1))
+
+
+def cfl_dt(n, U):
+    return CFL * (2 * math.pi / n) / float(np.abs(U).sum(axis=0).max())
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per grid point per stage launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "stage_kernel_ns_f64.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_point_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """NVML SM clock and throttle-reason samples while the timed region runs."""
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if ids and self.cuda_index < len(ids):
+                sel = ids[self.cuda_index]
+                if sel.isdigit():
+                    self._h = pynvml.nvmlDeviceGetHandleByIndex(int(sel))
+                else:
+                    self._h = pynvml.nvmlDeviceGetHandleByUUID(sel)
+            else:
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nvml = None
+            return self
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        nv = self._nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ reference arm --
+
+def reference_bin():
+    omp = os.path.join(ROOT, "oracle", "_ref", "nova_ref_omp")
+    ser = os.path.join(ROOT, "oracle", "_ref", "nova_ref")
+    if os.path.exists(omp):
+        return omp, os.cpu_count() or 1
+    if os.path.exists(ser):
+        return ser, 1
+    return None, 0
+
+
+def run_reference(n, nsteps, threads=None):
+    """Run the reference's own loop body (compiled in place) on an n^3 Taylor-Green field.
+    Returns per-step wall seconds of the loop bodies."""
+    from oracle import oracle as O
+    exe, cores = reference_bin()
+    if exe is None:
+        raise RuntimeError("reference not built (make -C oracle ref ref-omp)")
+    M = O.Mesh((n, n, n))
+    U = O.ic_taylor_green(M)
+    dt = cfl_dt(n, U)
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(threads or cores)
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        O.write_case(case, M)
+        M.to_ghosted(U).tofile(os.path.join(td, "U.bin"))
+        out = os.path.join(td, "out")
+        subprocess.run([exe, "run", case, "ns", "classical", str(nsteps), repr(dt), repr(NU), "0",
+                        os.path.join(td, "U.bin"), "-", out], check=True, stdout=subprocess.DEVNULL, env=env)
+        return [float(v) for v in open(out + "_time.txt").read().split()], cores, exe
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    exe, cores = reference_bin()
+    if exe is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference not compiled (make -C oracle ref)"}))
+        return 0
+    n = args.ref_n
+    if args.warmup + args.steps > 120:  # keep the whole reference run within a few minutes
+        n = 48 if args.warmup + args.steps <= 300 else 32
+    times, cores, exe = run_reference(n, args.warmup + args.steps)
+    t = sum(times[args.warmup:])
+    value = n ** 3 * args.steps / t / 1e6
+    kind = "reference"
+    sample = ("Taylor-Green %d^3, %d warm-up + %d timed steps of the reference's own RKLoop body (classical "
+              "form), compiled in place with its #pragma omp loops on %d threads" % (n, args.warmup, args.steps, cores))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: analytic Taylor-Green field",
+            "config": workload_config(args.n, {"sample_grid": [n, n, n]}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm --
+
+def time_device(nova, torch, GM, U, p, rd, steps, warmup, dist, stage_bytes):
+    """Warm up, then time exactly `steps` device-resident steps; returns (seconds, stage stats, launches, clocks)."""
+    nova.advance(GM, rd, U, p, nsteps=warmup, history=False)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    GM.profile(True)
+    GM.profile_read(nova.K_STAGE, reset=True)
+    GM.launch_count(reset=True)
+    dev = torch.cuda.current_device()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        nova.advance(GM, rd, U, p, nsteps=steps, history=False)
+        ev1.record()
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    GM.profile(False)
+    sec = ev0.elapsed_time(ev1) / 1e3
+    st_ms, st_n = GM.profile_read(nova.K_STAGE, reset=True)
+    launches = GM.launch_count(reset=True)
+    return sec, (st_ms, st_n), launches, clk.summary()
+
+
+def time_e2e(nova, torch, GM, U, p, rd, U0_aos_pinned, out_pinned, steps, dist):
+    """Same steps through the reference-layout ABI with host buffers, copies inside the timed region."""
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    hist_rows = 0
+    ev0.record()
+    U.upload(U0_aos_pinned)
+    hist = nova.advance(GM, rd, U, p, nsteps=steps, history=True)
+    hist_rows = hist.shape[0]
+    U.download(out=out_pinned)
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sec = ev0.elapsed_time(ev1) / 1e3
+    h2d = U0_aos_pinned.nbytes
+    d2h = out_pinned.nbytes + hist_rows * nova.HIST_COLS * 8
+    return sec, h2d, d2h
+
+
+def our_arm(args, rank, world, dist):
+    import torch
+    from novaclone_b200 import nova
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    # one explicit stream for the library and for torch's timing events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    n = args.n
+    U0 = tg_field(n)
+    dt = cfl_dt(n, U0)
+    GM = nova.Mesh((n, n, n))
+    GM.set_stream(torch.cuda.current_stream().cuda_stream)
+    p = nova.Field(GM, 1)
+
+    def maxover(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    res = {}
+    finals = {}
+    for prec_name, prec in (("f64", nova.F64), ("f32split", nova.F32SPLIT)):
+        U = nova.Field(GM, 3, prec).upload_soa(U0)
+        rd = nova.run_desc(model="ns", rk_mode="classical", precision=prec, dt=dt, nu=NU, diag_every=0)
+        sec, (st_ms, st_n), launches, clocks = time_device(nova, torch, GM, U, p, rd, args.steps, args.warmup, dist,
+                                                           STAGE_BYTES[prec_name])
+        finals[prec_name] = U.download_soa()
+        sec = maxover(sec)
+        res[prec_name] = {"sec": sec, "stage_ms": st_ms, "stage_launches": st_n, "launches": launches,
+                          "clocks": clocks, "value": world * n ** 3 * args.steps / sec / 1e6,
+                          "ms_per_step": 1e3 * sec / args.steps}
+        U.close()
+
+    err = float(np.linalg.norm(finals["f32split"] - finals["f64"]) / np.linalg.norm(finals["f64"]))
+    t_end = (args.warmup + args.steps) * dt
+
+    # e2e through the reference-layout ABI (ghosted AoS host buffers, pinned)
+    e2e = {}
+    if not args.no_e2e:
+        aos = ghosted(U0)
+        pin_in = torch.empty(aos.shape, dtype=torch.float64, pin_memory=True).numpy()
+        pin_in[...] = aos
+        pin_out = torch.empty(aos.shape, dtype=torch.float64, pin_memory=True).numpy()
+        for prec_name, prec in (("f64", nova.F64), ("f32split", nova.F32SPLIT)):
+            U = nova.Field(GM, 3, prec)
+            rd = nova.run_desc(model="ns", rk_mode="classical", precision=prec, dt=dt, nu=NU, diag_every=1)
+            U.upload(pin_in)
+            nova.advance(GM, rd, U, p, nsteps=1, history=True)  # warm the path (plans, buffers)
+            sec, h2d, d2h = time_e2e(nova, torch, GM, U, p, rd, pin_in, pin_out, args.steps, dist)
+            sec = maxover(sec)
+            e2e[prec_name] = {"value": world * n ** 3 * args.steps / sec / 1e6, "unit": UNIT,
+                              "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                              "ms_per_step": 1e3 * sec / args.steps}
+            U.close()
+
+    if rank != 0:
+        return 0
+
+    peak, peak_kind = measured_peaks()
+
+    def roof(prec_name):
+        r = res[prec_name]
+        if r["stage_launches"] == 0:
+            return None
+        bytes_total = STAGE_BYTES[prec_name] * n ** 3 * r["stage_launches"] / STAGE_LAUNCHES_PER_STEP
+        achieved = bytes_total / (r["stage_ms"] / 1e3) / 1e9
+        tr = profiled_traffic() if prec_name == "f64" else None
+        return {"bound": "hbm", "kernel": "k_stage (fused RHS + RK stage update), NS %s" % prec_name,
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "avg_launch_ms": r["stage_ms"] / r["stage_launches"],
+                "alg_bytes_per_launch": STAGE_BYTES[prec_name] * n ** 3 / STAGE_LAUNCHES_PER_STEP,
+                "traffic": None if tr is None else tr * n ** 3, "stage_share_of_step": r["stage_ms"] / (1e3 * r["sec"])}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        exe, cores = reference_bin()
+        if exe is not None:
+            ns = args.cpu_n
+            times, cores, exe = run_reference(ns, args.cpu_steps + 1)
+            t = sum(times[1:])
+            cpu = {"value": ns ** 3 * args.cpu_steps / t / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": "Taylor-Green %d^3, %d timed steps (after 1 untimed) of the reference's own loop body, "
+                             "compiled in place, OpenMP threads=%d" % (ns, args.cpu_steps, cores)}
+
+    f64 = res["f64"]
+    f32 = res["f32split"]
+    line = {
+        "metric": METRIC, "value": f64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": f64["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: analytic Taylor-Green initial field",
+        "config": workload_config(n),
+        "roofline": roof("f64"),
+        "cpu_baseline": cpu,
+        "e2e": e2e.get("f64"),
+        "gpu_launches": f64["launches"],
+        "clocks": f64["clocks"],
+        "fp32split": {"value": f32["value"], "unit": UNIT, "ms_per_step": f32["ms_per_step"],
+                      "speedup_vs_fp64": f64["ms_per_step"] / f32["ms_per_step"],
+                      "rel_l2_vs_fp64": err, "at_time": t_end, "steps_compared": args.warmup + args.steps,
+                      "dtype": "f32 stencils, (hi,lo) f32 state, f64 projection", "roofline": roof("f32split"),
+                      "e2e": e2e.get("f32split"), "gpu_launches": f32["launches"], "clocks": f32["clocks"]},
+        "adjoint_fwd_ratio": None,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--ref-n", type=int, default=64, help="grid of the reference arm's bounded sample")
+    ap.add_argument("--cpu-n", type=int, default=64)
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return our_arm(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

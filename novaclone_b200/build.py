@@ -23,9 +23,9 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 SOURCES = ["nova_stage.cu", "nova_ops.cu", "nova_capi.cu"]
-HEADERS = ["nova_internal.cuh", "nova_ops.cuh"]
+HEADERS = ["nova_internal.cuh", "nova_ops.cuh", "nova_tile.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-diag-suppress", "177", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 
 
 def _newer(target, deps):

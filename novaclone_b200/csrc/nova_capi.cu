@@ -692,7 +692,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         double *Ustar;
         auto run64 = [&](int stage, const StageArgs64 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
-            launch_stage64(phys, stage, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc, a, st);
+            launch_stage64(phys, stage, ctx->md.hyperbolic_z != 0, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc, a, st);
             ctx->launches += 1;
         };
         if (lit) {
@@ -713,7 +713,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, Ustar, nullptr, nullptr, divisor, ctx->d_rhs, st);
             ctx->launches += 1;
         }
-        CKL("k_div_proj");
+        CKL("k_div_tiled");
         nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
         if (s != NOVA_OK) return s;
         {
@@ -722,12 +722,12 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
                            nullptr, nullptr, st);
             ctx->launches += 1;
         }
-        CKL("k_correct");
+        CKL("k_correct_tiled");
     } else {
         const float *Ushi, *Uslo;
         auto run32 = [&](int stage, const StageArgs32 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
-            launch_stage32(phys, stage, g, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt, (float)visc, a, st);
+            launch_stage32(phys, stage, ctx->md.hyperbolic_z != 0, g, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt, (float)visc, a, st);
             ctx->launches += 1;
         };
         const float *Xp = X ? X->hi : nullptr;
@@ -750,7 +750,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo, divisor, ctx->d_rhs, st);
             ctx->launches += 1;
         }
-        CKL("k_div_proj");
+        CKL("k_div_tiled");
         nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
         if (s != NOVA_OK) return s;
         {
@@ -759,7 +759,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
                            Y->lo, st);
             ctx->launches += 1;
         }
-        CKL("k_correct");
+        CKL("k_correct_tiled");
     }
     return NOVA_OK;
 }

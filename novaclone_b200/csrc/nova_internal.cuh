@@ -12,7 +12,6 @@
 
 namespace nova {
 
-// Half-width of the fused kernels' stencil (settings::m_ = 6 -> 3 ghost layers).
 constexpr int kTK = 32;   // tile extent along k (one warp, coalesced)
 constexpr int kTJ = 8;    // tile extent along j
 constexpr int kThreads = kTK * kTJ;
@@ -90,9 +89,11 @@ struct StageArgs32 {
 enum Physics { PHYS_NS = 0, PHYS_MHD_U = 1, PHYS_MHD_B = 2 };
 
 // stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum)
-void launch_stage64(int phys, int stage, const Geo &g, const Coef<double> &co, const double *ia,
+// stretch: apply the stretched-z Laplacian term (Mesh "hypz:"); on uniform
+// meshes d2zdxi2 is round-off (|.| < 1e-9) and the term is skipped
+void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
                     const double *corr2, double dt, double visc, const StageArgs64 &a, cudaStream_t st);
-void launch_stage32(int phys, int stage, const Geo &g, const Coef<float> &co, const float *ia,
+void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
                     const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st);
 
 }  // namespace nova

@@ -1,15 +1,16 @@
 // Projection, diagnostics, drop-in ex:: operators and layout conversion.
 //
 // Projection (app/TG_Piosson/RKLoop.H:30-38, app/OT_Poisson/BEqn.H:91-95):
-//   rhs = div(U*) / dt                       k_div_proj    (src/ex/div/div.hxx:22-81)
+//   rhs = div(U*) / dt                       k_div_tiled   (src/ex/div/div.hxx:22-81)
 //   rhs^ = D2Z(rhs)                          cuFFT         (src/poisson/poisson.cpp:225)
 //   rhs^ = -rhs^ / k'^2 / (N0 N1 N2)         k_scale       (poisson.cpp:230-249, 259)
 //   p = Z2D(rhs^)                            cuFFT         (poisson.cpp:250)
-//   U = U* - dt * grad(p)                    k_correct     (src/ex/grad/grad.cpp:25-62)
+//   U = U* - dt * grad(p)                    k_correct_tiled (src/ex/grad/grad.cpp:25-62)
 // k'^2 is built from 1-D tables of squared modified wavenumbers
 // (poisson::wavenumbersFFT_, poisson.cpp:337-396) summed in the reference's order.
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"
+#include "nova_tile.cuh"
 
 #include <cuComplex.h>
 
@@ -59,22 +60,6 @@ __device__ __forceinline__ double dd1(const P &f, const Geo &g, int c, int i, in
     return r;
 }
 
-template <int H, class LD>
-__global__ void k_div_proj(Geo g, Coef<double> co, const double *__restrict__ ia, LD U, double divisor,
-                           double *__restrict__ rhs)
-{
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= g.N3) return;
-    int i, j, k;
-    pt_index(g, t, i, j, k);
-    double az[H];
-#pragma unroll
-    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
-    const double d = dd1<H>(U, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(U, g, 1, i, j, k, 1, co.a[1])
-                     + dd1<H>(U, g, 2, i, j, k, 2, az);
-    rhs[t] = d / divisor;
-}
-
 __global__ void k_scale(Geo g, cuDoubleComplex *__restrict__ spec, const double *__restrict__ kx2,
                         const double *__restrict__ ky2, const double *__restrict__ kz2, double invN3)
 {
@@ -96,52 +81,62 @@ __global__ void k_scale(Geo g, cuDoubleComplex *__restrict__ spec, const double 
     spec[t] = v;
 }
 
-// U = U* - s*grad(p) (U may alias U*: each node reads and writes only itself)
-template <int H>
-__global__ void k_correct64(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ p,
-                            double s, const double *Us, double *U)
+// rhs = div(U*)/divisor and U = U* - s*grad(p): the 2.5-D march of nova_tile.cuh
+// (register queue along i, shared plane for j/k), one read of each input.
+template <int H, class LD>
+__global__ void __launch_bounds__(kThreads) k_div_tiled(Geo g, Coef<double> co, const double *__restrict__ ia, LD U,
+                                                        double divisor, double *__restrict__ rhs, int ichunk)
 {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= g.N3) return;
-    int i, j, k;
-    pt_index(g, t, i, j, k);
-    Ld64 P{p, g.N3};
+    extern __shared__ __align__(16) unsigned char smraw[];
+    auto &sm = *reinterpret_cast<TileSmem<double, H, 3> *>(smraw);
+    const int ib = blockIdx.z * ichunk;
+    const int ie = min(ib + ichunk, g.N0);
+    const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
     double az[H];
 #pragma unroll
-    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
-    double gr[3];
-    gr[0] = dd1<H>(P, g, 0, i, j, k, 0, co.a[0]);
-    gr[1] = dd1<H>(P, g, 0, i, j, k, 1, co.a[1]);
-    gr[2] = dd1<H>(P, g, 0, i, j, k, 2, az);
-#pragma unroll
-    for (int c = 0; c < 3; c++) U[c * g.N3 + t] = Us[c * g.N3 + t] - gr[c] * s;
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
+    tile_march<double, H, 3>(g, sm, U, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy, const auto &vz) {
+        const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
+        rhs[idx] = d / divisor;
+    });
 }
 
-// same for the (hi, lo) state: the correction is applied in FP64
-template <int H>
-__global__ void k_correct32(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ p,
-                            double s, const float *Ushi, const float *Uslo, float *hi, float *lo)
+template <int H, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Coef<double> co, const double *__restrict__ ia,
+                                                            const double *__restrict__ p, double s, const double *Us64,
+                                                            double *U64, const float *Ushi, const float *Uslo,
+                                                            float *hi, float *lo, int ichunk)
 {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= g.N3) return;
-    int i, j, k;
-    pt_index(g, t, i, j, k);
-    Ld64 P{p, g.N3};
+    extern __shared__ __align__(16) unsigned char smraw[];
+    auto &sm = *reinterpret_cast<TileSmem<double, H, 1> *>(smraw);
+    const int ib = blockIdx.z * ichunk;
+    const int ie = min(ib + ichunk, g.N0);
+    const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
     double az[H];
 #pragma unroll
-    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
-    double gr[3];
-    gr[0] = dd1<H>(P, g, 0, i, j, k, 0, co.a[0]);
-    gr[1] = dd1<H>(P, g, 0, i, j, k, 1, co.a[1]);
-    gr[2] = dd1<H>(P, g, 0, i, j, k, 2, az);
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
+    auto ld = [&](int, long long o) { return p[o]; };
+    tile_march<double, H, 1>(g, sm, ld, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy, const auto &vz) {
+        double us[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const long long o = c * g.N3 + t;
-        const double x = ((double)Ushi[o] + (double)Uslo[o]) - gr[c] * s;
-        const float h = (float)x;
-        hi[o] = h;
-        lo[o] = (float)(x - (double)h);
-    }
+        for (int c = 0; c < 3; c++) {
+            const long long o = c * g.N3 + idx;
+            us[c] = SPLIT ? (double)Ushi[o] + (double)Uslo[o] : Us64[o];
+        }
+        const double gr[3] = {d1<double, H>(vx, 0, co.a[0]), d1<double, H>(vy, 0, co.a[1]), d1<double, H>(vz, 0, az)};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const long long o = c * g.N3 + idx;
+            const double x = us[c] - gr[c] * s;
+            if constexpr (SPLIT) {
+                const float h = (float)x;
+                hi[o] = h;
+                lo[o] = (float)(x - (double)h);
+            } else {
+                U64[o] = x;
+            }
+        }
+    });
 }
 
 // ------------------------------------------------------------- diagnostics --
@@ -492,11 +487,18 @@ inline unsigned nblocks(long long n, int b) { return (unsigned)((n + b - 1) / b)
 void launch_div_proj(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64,
                      const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st)
 {
-    const unsigned nb = nblocks(g.N3, 256);
+    const int ch = pick_ichunk(g, 3);
+    const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     if (U64) {
-        NOVA_DISPATCH_H(h, (k_div_proj<HH, Ld64><<<nb, 256, 0, st>>>(g, co, ia, Ld64{U64, g.N3}, divisor, rhs)));
+        NOVA_DISPATCH_H(h, {
+            constexpr size_t sb = tile_smem_bytes<double, HH, 3>();
+            k_div_tiled<HH, Ld64><<<grid, block, sb, st>>>(g, co, ia, Ld64{U64, g.N3}, divisor, rhs, ch);
+        });
     } else {
-        NOVA_DISPATCH_H(h, (k_div_proj<HH, LdSplit><<<nb, 256, 0, st>>>(g, co, ia, LdSplit{hi, lo, g.N3}, divisor, rhs)));
+        NOVA_DISPATCH_H(h, {
+            constexpr size_t sb = tile_smem_bytes<double, HH, 3>();
+            k_div_tiled<HH, LdSplit><<<grid, block, sb, st>>>(g, co, ia, LdSplit{hi, lo, g.N3}, divisor, rhs, ch);
+        });
     }
 }
 
@@ -511,11 +513,19 @@ void launch_correct(int h, const Geo &g, const Coef<double> &co, const double *i
                     const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi, float *lo,
                     cudaStream_t st)
 {
-    const unsigned nb = nblocks(g.N3, 256);
+    const int ch = pick_ichunk(g, 4);
+    const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     if (U64) {
-        NOVA_DISPATCH_H(h, (k_correct64<HH><<<nb, 256, 0, st>>>(g, co, ia, p, s, Us64, U64)));
+        NOVA_DISPATCH_H(h, {
+            constexpr size_t sb = tile_smem_bytes<double, HH, 1>();
+            k_correct_tiled<HH, false><<<grid, block, sb, st>>>(g, co, ia, p, s, Us64, U64, nullptr, nullptr, nullptr,
+                                                                nullptr, ch);
+        });
     } else {
-        NOVA_DISPATCH_H(h, (k_correct32<HH><<<nb, 256, 0, st>>>(g, co, ia, p, s, Ushi, Uslo, hi, lo)));
+        NOVA_DISPATCH_H(h, {
+            constexpr size_t sb = tile_smem_bytes<double, HH, 1>();
+            k_correct_tiled<HH, true><<<grid, block, sb, st>>>(g, co, ia, p, s, nullptr, nullptr, Ushi, Uslo, hi, lo, ch);
+        });
     }
 }
 

@@ -8,17 +8,16 @@
 //   MHD B (app/OT_Poisson/BEqn.H:72-78):
 //         dB = dt*( -div(U,B) + div(B,U) + laplacian(eta,B) )
 //
-// with ex::div(V,F) the skew form of src/ex/div/div.hxx:84-172,
+// ex::div(V,F) is the skew form of src/ex/div/div.hxx:84-172,
 //   div(V,F)_c = 1/2 sum_d [ D_d(V_d F_c) + V_d D_d F_c + F_c D_d V_d ],
-// ex::laplacian(nu,F) of src/ex/laplacian/laplacian.hxx:130-191 including its
-// stretched-z term, and ex::grad of src/ex/grad/grad.cpp:25-62; the z
-// derivatives carry the Mesh::dzdxi_ metric (src/Mesh/Mesh.cpp:147-179).
-//
-// Tiling (2.5-D): a block owns a 32(k) x 8(j) column of the grid and marches
-// along i.  Each thread keeps its column's 2H+1 planes in a register queue (the
-// i-direction stencil), the current plane plus its j/k halo sits in shared
-// memory (the j- and k-direction stencils).  Periodic ghosts are synthesised by
-// wrapping indices at load time, which replaces periodicBC::update.
+// evaluated here as 1/2 sum_d [ A_d(V,F)_c + F_c D_d V_d ] with
+//   A_d(V,F)_c = sum_l a_l [ F_c(+l) (V_d(+l) + V_d(0)) - F_c(-l) (V_d(-l) + V_d(0)) ],
+// which equals D_d(V_d F_c) + V_d(0) D_d F_c and costs one product per node
+// pair instead of three.  ex::laplacian(nu,F) follows
+// src/ex/laplacian/laplacian.hxx:130-191 (centre terms of the three
+// directions folded into one), the stretched-z term included when the mesh is
+// stretched; ex::grad follows src/ex/grad/grad.cpp:25-62.  z derivatives carry
+// the Mesh::dzdxi_ metric (src/Mesh/Mesh.cpp:147-179).
 //
 // Epilogue (stage s of the classical RK4 of src/settings/settings.cpp:44-51,
 // association order of app/TG_Piosson/RKLoop.H:24-28 kept):
@@ -31,304 +30,287 @@
 // The FP32-split variant keeps A as an FP32 sum of increments and adds it to
 // the (hi, lo) base in FP64 at the last stage.
 #include "nova_internal.cuh"
+#include "nova_tile.cuh"
 
 #include <type_traits>
+
+// minimum resident blocks per SM requested from the register allocator
+#ifndef NOVA_STAGE_MINB
+#define NOVA_STAGE_MINB 2
+#endif
 
 namespace nova {
 
 namespace {
 
-template <typename T, int H, int PHYS, int STAGE, class Args>
-__global__ void __launch_bounds__(kThreads) k_stage(Geo g, Coef<T> co, const T *__restrict__ ia,
+// A_d(V,F)_c of the header: cf = component of F, cv = component V_d, v0 = V_d(0)
+template <typename T, int H, class V>
+__device__ __forceinline__ T adv1(const V &v, int cf, int cv, T v0, const T *a)
+{
+    T r = a[0] * (v(cf, 1) * (v(cv, 1) + v0) - v(cf, -1) * (v(cv, -1) + v0));
+#pragma unroll
+    for (int l = 1; l < H; l++)
+        r = fma(a[l], v(cf, l + 1) * (v(cv, l + 1) + v0) - v(cf, -l - 1) * (v(cv, -l - 1) + v0), r);
+    return r;
+}
+
+// sum_l b_l (f(+l) + f(-l)); the centre term is added once for all directions
+template <typename T, int H, class V>
+__device__ __forceinline__ T lsum(const V &v, int c, const T *b)
+{
+    T r = b[0] * (v(c, 1) + v(c, -1));
+#pragma unroll
+    for (int l = 1; l < H; l++) r = fma(b[l], v(c, l + 1) + v(c, -l - 1), r);
+    return r;
+}
+
+template <typename T, int H, int PHYS, int STAGE, bool STRETCH, class Args>
+__global__ void __launch_bounds__(kThreads, NOVA_STAGE_MINB) k_stage(Geo g, Coef<T> co, const T *__restrict__ ia,
                                                       const T *__restrict__ corr2, T dt, T visc, Args args,
                                                       int ichunk)
 {
     constexpr int NC = (PHYS == PHYS_NS) ? 3 : 6;
-    constexpr int W = kTK + 2 * H;
-    constexpr int R = kTJ + 2 * H;
-    constexpr int NJH = 2 * H * kTK;
-    constexpr int NKH = 2 * H * kTJ;
-    constexpr int NH = NJH + NKH;
-    constexpr int HS = (NH + kThreads - 1) / kThreads;
-    __shared__ T sm[NC][R][W];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    auto &sm = *reinterpret_cast<TileSmem<T, H, NC> *>(smraw);
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTK + tx;
-    const int k0 = blockIdx.x * kTK, j0 = blockIdx.y * kTJ;
-    const int k = k0 + tx, j = j0 + ty;
-    const bool valid = (k < g.N2) && (j < g.N1);
-    const int kw = wrapi(k, g.N2), jw = wrapi(j, g.N1);
     const int ib = blockIdx.z * ichunk;
     const int ie = min(ib + ichunk, g.N0);
-
-    const T *src[NC];
-#pragma unroll
-    for (int c = 0; c < NC; c++) {
-        const T *base;
-        if constexpr (std::is_same<Args, StageArgs64>::value)
-            base = (c < 3) ? args.Y : args.X;
-        else
-            base = (c < 3) ? args.Y : args.X;
-        src[c] = base + (long long)(c % 3) * g.N3;
-    }
-
-    // halo cells of the current plane owned by this thread
-    int hrow[HS], hcol[HS];
-    long long hoff[HS];
-    bool hon[HS];
-#pragma unroll
-    for (int s = 0; s < HS; s++) {
-        const int t = tid + s * kThreads;
-        hon[s] = t < NH;
-        int row, col;
-        if (t < NJH) {
-            const int r = t / kTK;
-            row = r < H ? r : kTJ + r;
-            col = H + t % kTK;
-        } else {
-            const int u = t - NJH;
-            row = H + u / (2 * H);
-            const int cc = u % (2 * H);
-            col = cc < H ? cc : kTK + cc;
-        }
-        if (!hon[s]) { row = 0; col = 0; }
-        hrow[s] = row;
-        hcol[s] = col;
-        hoff[s] = (long long)wrapi(j0 + row - H, g.N1) * g.N2 + wrapi(k0 + col - H, g.N2);
-    }
+    const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
 
     // z metric of this thread's column (src/ex/*: terms divided by dzdxi(k))
     const T iak = ia[kw];
-    const T c2k = corr2[kw];
     T az[H], bz[H];
 #pragma unroll
     for (int l = 0; l < H; l++) {
         az[l] = co.a[2][l] * iak;
         bz[l] = co.b[2][l] * iak * iak;
     }
-    const T b2z = co.b2[2] * iak * iak;
+    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
+    const T c2k = STRETCH ? corr2[kw] : T(0);
 
-    const long long colOff = (long long)jw * g.N2 + kw;
-    T q[2 * H + 1][NC];
+    const T *src[NC];
 #pragma unroll
-    for (int s = 0; s < 2 * H; s++) {
-        const long long p = (long long)wrapi(ib - H + s, g.N0) * g.N12 + colOff;
-#pragma unroll
-        for (int c = 0; c < NC; c++) q[s + 1][c] = src[c][p];
-    }
+    for (int c = 0; c < NC; c++) src[c] = ((c < 3) ? args.Y : args.X) + (long long)(c % 3) * g.N3;
 
-    for (int i = ib; i < ie; i++) {
+    tile_march<T, H, NC>(
+        g, sm, [&](int c, long long o) { return src[c][o]; }, ib, ie,
+        [&](long long idx, auto &q, const auto &vx, const auto &vy, const auto &vz) {
+            // epilogue operands first, so their latency overlaps the arithmetic
+            T e0[3], e1[3];
 #pragma unroll
-        for (int s = 0; s < 2 * H; s++)
-#pragma unroll
-            for (int c = 0; c < NC; c++) q[s][c] = q[s + 1][c];
-        {
-            const long long p = (long long)wrapi(i + H, g.N0) * g.N12 + colOff;
-#pragma unroll
-            for (int c = 0; c < NC; c++) q[2 * H][c] = src[c][p];
-        }
-        const long long plane = (long long)i * g.N12;
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < NC; c++) sm[c][ty + H][tx + H] = q[H][c];
-#pragma unroll
-        for (int s = 0; s < HS; s++)
-            if (hon[s])
-#pragma unroll
-                for (int c = 0; c < NC; c++) sm[c][hrow[s]][hcol[s]] = src[c][plane + hoff[s]];
-        __syncthreads();
-        if (!valid) continue;
-
-        auto vx = [&](int c, int s) -> T { return q[H + s][c]; };
-        auto vy = [&](int c, int s) -> T { return sm[c][ty + H + s][tx + H]; };
-        auto vz = [&](int c, int s) -> T { return sm[c][ty + H][tx + H + s]; };
-
-        T rhs[3];
-        if constexpr (PHYS == PHYS_NS) {
-            T u0[3] = {q[H][0], q[H][1], q[H][2]};
-            T adv[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, div = 0, duz[3];
-            auto dir = [&](const auto &v, int d, const T *a, const T *b, T b2, T *du_keep) {
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const T du = d1<T, H>(v, c, a);
-                    adv[c] += fma(u0[d], du, d1p<T, H>(v, d, c, a));
-                    lap[c] += d2<T, H>(v, c, b, b2);
-                    if (c == d) div += du;
-                    if (du_keep) du_keep[c] = du;
+            for (int c = 0; c < 3; c++) {
+                const long long o = (long long)c * g.N3 + idx;
+                if constexpr (std::is_same<T, double>::value) {
+                    if constexpr (STAGE == 1 || STAGE == 2) {
+                        e0[c] = args.U0[o];
+                        e1[c] = args.A[o];
+                    } else if constexpr (STAGE == 3) {
+                        e1[c] = args.A[o];
+                    }
+                } else {
+                    if constexpr (STAGE == 1 || STAGE == 2) {
+                        e0[c] = args.U0hi[o];
+                        e1[c] = args.A[o];
+                    } else if constexpr (STAGE == 3) {
+                        e0[c] = args.U0hi[o];
+                        e1[c] = args.A[o];
+                    }
                 }
-            };
-            dir(vx, 0, co.a[0], co.b[0], co.b2[0], nullptr);
-            dir(vy, 1, co.a[1], co.b[1], co.b2[1], nullptr);
-            dir(vz, 2, az, bz, b2z, duz);
+            }
+
+            T rhs[3];
+            if constexpr (PHYS == PHYS_NS) {
+                const T u0[3] = {q[H][0], q[H][1], q[H][2]};
+                T adv[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, div = 0, duz[3] = {0, 0, 0};
+                auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-                rhs[c] = T(-0.5) * fma(u0[c], div, adv[c]) + visc * fma(-c2k, duz[c], lap[c]);
-        } else if constexpr (PHYS == PHYS_MHD_U) {
-            // comps 0-2: U (stage state), 3-5: B (frozen)
-            T u0[3] = {q[H][0], q[H][1], q[H][2]};
-            T b0[3] = {q[H][3], q[H][4], q[H][5]};
-            T advU[3] = {0, 0, 0}, advB[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, gb[3], divU = 0, divB = 0, duz[3];
-            auto dir = [&](const auto &v, int d, const T *a, const T *b, T b2, T *du_keep) {
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const T du = d1<T, H>(v, c, a);
-                    const T db = d1<T, H>(v, 3 + c, a);
-                    advU[c] += fma(u0[d], du, d1p<T, H>(v, d, c, a));
-                    advB[c] += fma(b0[d], db, d1p<T, H>(v, 3 + d, 3 + c, a));
-                    lap[c] += d2<T, H>(v, c, b, b2);
-                    if (c == d) { divU += du; divB += db; }
-                    if (du_keep) du_keep[c] = du;
-                }
-                // grad(0.5*(B&B)) along d (src/ex/grad/grad.cpp:43-54 on the product field)
-                auto e = [&](int, int s) -> T {
-                    return (v(3, s) * v(3, s) + v(4, s) * v(4, s) + v(5, s) * v(5, s)) * T(0.5);
+                    for (int c = 0; c < 3; c++) {
+                        adv[c] += adv1<T, H>(v, c, d, u0[d], a);
+                        lap[c] += lsum<T, H>(v, c, b);
+                        if (STRETCH && zdir) duz[c] = d1<T, H>(v, c, a);
+                    }
+                    div += d1<T, H>(v, d, a);
                 };
-                gb[d] = d1<T, H>(e, 0, a);
-            };
-            dir(vx, 0, co.a[0], co.b[0], co.b2[0], nullptr);
-            dir(vy, 1, co.a[1], co.b[1], co.b2[1], nullptr);
-            dir(vz, 2, az, bz, b2z, duz);
+                dir(vx, 0, co.a[0], co.b[0], false);
+                dir(vy, 1, co.a[1], co.b[1], false);
+                dir(vz, 2, az, bz, true);
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-                rhs[c] = T(-0.5) * fma(u0[c], divU, advU[c]) + visc * fma(-c2k, duz[c], lap[c])
-                         + T(0.5) * fma(b0[c], divB, advB[c]) - gb[c];
-        } else {
-            // comps 0-2: B (stage state), 3-5: U (frozen)
-            T b0[3] = {q[H][0], q[H][1], q[H][2]};
-            T u0[3] = {q[H][3], q[H][4], q[H][5]};
-            T advUB[3] = {0, 0, 0}, advBU[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, divU = 0, divB = 0, dbz[3];
-            auto dir = [&](const auto &v, int d, const T *a, const T *b, T b2, T *db_keep) {
+                for (int c = 0; c < 3; c++)
+                    rhs[c] = T(-0.5) * fma(u0[c], div, adv[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c]);
+            } else if constexpr (PHYS == PHYS_MHD_U) {
+                // comps 0-2: U (stage state), 3-5: B (frozen)
+                const T u0[3] = {q[H][0], q[H][1], q[H][2]};
+                const T b0[3] = {q[H][3], q[H][4], q[H][5]};
+                T advU[3] = {0, 0, 0}, advB[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, gb[3], divU = 0, divB = 0;
+                T duz[3] = {0, 0, 0};
+                auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        advU[c] += adv1<T, H>(v, c, d, u0[d], a);
+                        advB[c] += adv1<T, H>(v, 3 + c, 3 + d, b0[d], a);
+                        lap[c] += lsum<T, H>(v, c, b);
+                        if (STRETCH && zdir) duz[c] = d1<T, H>(v, c, a);
+                    }
+                    divU += d1<T, H>(v, d, a);
+                    divB += d1<T, H>(v, 3 + d, a);
+                    // grad(0.5*(B&B)) along d (src/ex/grad/grad.cpp:43-54 on the product field)
+                    auto e = [&](int, int s) -> T {
+                        return (v(3, s) * v(3, s) + v(4, s) * v(4, s) + v(5, s) * v(5, s)) * T(0.5);
+                    };
+                    gb[d] = d1<T, H>(e, 0, a);
+                };
+                dir(vx, 0, co.a[0], co.b[0], false);
+                dir(vy, 1, co.a[1], co.b[1], false);
+                dir(vz, 2, az, bz, true);
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    rhs[c] = T(-0.5) * fma(u0[c], divU, advU[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c])
+                             + T(0.5) * fma(b0[c], divB, advB[c]) - gb[c];
+            } else {
+                // comps 0-2: B (stage state), 3-5: U (frozen)
+                const T b0[3] = {q[H][0], q[H][1], q[H][2]};
+                const T u0[3] = {q[H][3], q[H][4], q[H][5]};
+                T advUB[3] = {0, 0, 0}, advBU[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, divU = 0, divB = 0;
+                T dbz[3] = {0, 0, 0};
+                auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        advUB[c] += adv1<T, H>(v, c, 3 + d, u0[d], a);
+                        advBU[c] += adv1<T, H>(v, 3 + c, d, b0[d], a);
+                        lap[c] += lsum<T, H>(v, c, b);
+                        if (STRETCH && zdir) dbz[c] = d1<T, H>(v, c, a);
+                    }
+                    divU += d1<T, H>(v, 3 + d, a);
+                    divB += d1<T, H>(v, d, a);
+                };
+                dir(vx, 0, co.a[0], co.b[0], false);
+                dir(vy, 1, co.a[1], co.b[1], false);
+                dir(vz, 2, az, bz, true);
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    rhs[c] = T(-0.5) * fma(b0[c], divU, advUB[c]) + T(0.5) * fma(u0[c], divB, advBU[c])
+                             + visc * (fma(-bsum, b0[c], lap[c]) - c2k * dbz[c]);
+            }
+
+            if constexpr (std::is_same<T, double>::value) {
+                // RK4a weights (src/settings/settings.cpp:44-50)
+                const double w6 = 1.0 / 6.0, w3 = 1.0 / 3.0;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
-                    const T db = d1<T, H>(v, c, a);
-                    const T du = d1<T, H>(v, 3 + c, a);
-                    advUB[c] += fma(u0[d], db, d1p<T, H>(v, 3 + d, c, a));
-                    advBU[c] += fma(b0[d], du, d1p<T, H>(v, d, 3 + c, a));
-                    lap[c] += d2<T, H>(v, c, b, b2);
-                    if (c == d) { divU += du; divB += db; }
-                    if (db_keep) db_keep[c] = db;
+                    const long long o = (long long)c * g.N3 + idx;
+                    const double du = dt * rhs[c];
+                    const double y0 = q[H][c];
+                    if constexpr (STAGE == 4) {
+                        args.Ynext[o] = (((y0 + du * w6) + du * w3) + du * w3) + du * w6;
+                    } else if constexpr (STAGE == 0) {
+                        args.Ynext[o] = y0 + du * 0.5;
+                        args.A[o] = y0 + du * w6;
+                    } else if constexpr (STAGE == 1) {
+                        args.Ynext[o] = e0[c] + du * 0.5;
+                        args.A[o] = e1[c] + du * w3;
+                    } else if constexpr (STAGE == 2) {
+                        args.Ynext[o] = e0[c] + du * 1.0;
+                        args.A[o] = e1[c] + du * w3;
+                    } else {
+                        args.Ynext[o] = e1[c] + du * w6;
+                    }
                 }
-            };
-            dir(vx, 0, co.a[0], co.b[0], co.b2[0], nullptr);
-            dir(vy, 1, co.a[1], co.b[1], co.b2[1], nullptr);
-            dir(vz, 2, az, bz, b2z, dbz);
+            } else {
+                const float w6 = 1.0f / 6.0f, w3 = 1.0f / 3.0f;
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-                rhs[c] = T(-0.5) * fma(b0[c], divU, advUB[c]) + T(0.5) * fma(u0[c], divB, advBU[c])
-                         + visc * fma(-c2k, dbz[c], lap[c]);
-        }
-
-        const long long idx = plane + colOff;
-        if constexpr (std::is_same<T, double>::value) {
-            // RK4a weights (src/settings/settings.cpp:44-50)
-            const double w6 = 1.0 / 6.0, w3 = 1.0 / 3.0;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const long long o = (long long)c * g.N3 + idx;
-                const double du = dt * rhs[c];
-                const double y0 = q[H][c];
-                if constexpr (STAGE == 4) {
-                    args.Ynext[o] = (((y0 + du * w6) + du * w3) + du * w3) + du * w6;
-                } else if constexpr (STAGE == 0) {
-                    args.Ynext[o] = y0 + du * 0.5;
-                    args.A[o] = y0 + du * w6;
-                } else if constexpr (STAGE == 1) {
-                    args.Ynext[o] = args.U0[o] + du * 0.5;
-                    args.A[o] = args.A[o] + du * w3;
-                } else if constexpr (STAGE == 2) {
-                    args.Ynext[o] = args.U0[o] + du * 1.0;
-                    args.A[o] = args.A[o] + du * w3;
-                } else {
-                    args.Ynext[o] = args.A[o] + du * w6;
-                }
-            }
-        } else {
-            const float w6 = 1.0f / 6.0f, w3 = 1.0f / 3.0f;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const long long o = (long long)c * g.N3 + idx;
-                const float du = dt * rhs[c];
-                if constexpr (STAGE == 4) {
-                    const float inc = ((du * w6 + du * w3) + du * w3) + du * w6;
-                    const double x = ((double)q[H][c] + (double)args.U0lo[o]) + (double)inc;
-                    const float hi = (float)x;
-                    args.outhi[o] = hi;
-                    args.outlo[o] = (float)(x - (double)hi);
-                } else if constexpr (STAGE == 0) {
-                    args.Ynext[o] = q[H][c] + du * 0.5f;
-                    args.A[o] = du * w6;
-                } else if constexpr (STAGE == 1) {
-                    args.Ynext[o] = args.U0hi[o] + du * 0.5f;
-                    args.A[o] = args.A[o] + du * w3;
-                } else if constexpr (STAGE == 2) {
-                    args.Ynext[o] = args.U0hi[o] + du;
-                    args.A[o] = args.A[o] + du * w3;
-                } else {
-                    const float inc = args.A[o] + du * w6;
-                    const double x = ((double)args.U0hi[o] + (double)args.U0lo[o]) + (double)inc;
-                    const float hi = (float)x;
-                    args.outhi[o] = hi;
-                    args.outlo[o] = (float)(x - (double)hi);
+                for (int c = 0; c < 3; c++) {
+                    const long long o = (long long)c * g.N3 + idx;
+                    const float du = dt * rhs[c];
+                    if constexpr (STAGE == 4) {
+                        const float inc = ((du * w6 + du * w3) + du * w3) + du * w6;
+                        const double x = ((double)q[H][c] + (double)args.U0lo[o]) + (double)inc;
+                        const float hi = (float)x;
+                        args.outhi[o] = hi;
+                        args.outlo[o] = (float)(x - (double)hi);
+                    } else if constexpr (STAGE == 0) {
+                        args.Ynext[o] = q[H][c] + du * 0.5f;
+                        args.A[o] = du * w6;
+                    } else if constexpr (STAGE == 1) {
+                        args.Ynext[o] = e0[c] + du * 0.5f;
+                        args.A[o] = e1[c] + du * w3;
+                    } else if constexpr (STAGE == 2) {
+                        args.Ynext[o] = e0[c] + du;
+                        args.A[o] = e1[c] + du * w3;
+                    } else {
+                        const float inc = e1[c] + du * w6;
+                        const double x = ((double)e0[c] + (double)args.U0lo[o]) + (double)inc;
+                        const float hi = (float)x;
+                        args.outhi[o] = hi;
+                        args.outlo[o] = (float)(x - (double)hi);
+                    }
                 }
             }
-        }
-    }
+        });
 }
 
 constexpr int kH = 3;
 
-int pick_ichunk(const Geo &g)
-{
-    // aim for >= 4 waves of ~2 resident blocks on 148 SMs while keeping the
-    // 2H-plane warm-up small against the chunk length
-    const long long tiles = (long long)((g.N2 + kTK - 1) / kTK) * ((g.N1 + kTJ - 1) / kTJ);
-    int ch = g.N0;
-    while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148 * 8) ch /= 2;
-    return ch;
-}
-
-template <typename T, int PHYS, int STAGE, class Args>
+template <typename T, int PHYS, int STAGE, bool STRETCH, class Args>
 void launch_one(const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc, const Args &a,
                 cudaStream_t st)
 {
-    const int ch = pick_ichunk(g);
-    dim3 block(kTK, kTJ);
-    dim3 grid((g.N2 + kTK - 1) / kTK, (g.N1 + kTJ - 1) / kTJ, (g.N0 + ch - 1) / ch);
-    k_stage<T, kH, PHYS, STAGE, Args><<<grid, block, 0, st>>>(g, co, ia, corr2, dt, visc, a, ch);
+    constexpr int NC = (PHYS == PHYS_NS) ? 3 : 6;
+    constexpr size_t smem = tile_smem_bytes<T, kH, NC>();
+    auto kern = k_stage<T, kH, PHYS, STAGE, STRETCH, Args>;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    const int bps = (std::is_same<T, double>::value && PHYS != PHYS_NS) ? 1 : 2;
+    const int ch = pick_ichunk(g, bps);
+    kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, corr2, dt, visc, a, ch);
 }
 
-template <typename T, int PHYS, class Args>
-void launch_phys(int stage, const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
-                 const Args &a, cudaStream_t st)
+template <typename T, int PHYS, bool STRETCH, class Args>
+void launch_stage_t(int stage, const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
+                    const Args &a, cudaStream_t st)
 {
     switch (stage) {
-    case 0: launch_one<T, PHYS, 0>(g, co, ia, corr2, dt, visc, a, st); break;
-    case 1: launch_one<T, PHYS, 1>(g, co, ia, corr2, dt, visc, a, st); break;
-    case 2: launch_one<T, PHYS, 2>(g, co, ia, corr2, dt, visc, a, st); break;
-    case 3: launch_one<T, PHYS, 3>(g, co, ia, corr2, dt, visc, a, st); break;
-    default: launch_one<T, PHYS, 4>(g, co, ia, corr2, dt, visc, a, st); break;
+    case 0: launch_one<T, PHYS, 0, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
+    case 1: launch_one<T, PHYS, 1, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
+    case 2: launch_one<T, PHYS, 2, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
+    case 3: launch_one<T, PHYS, 3, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
+    default: launch_one<T, PHYS, 4, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
+    }
+}
+
+template <typename T, class Args>
+void launch_stage_any(int phys, int stage, bool stretch, const Geo &g, const Coef<T> &co, const T *ia,
+                      const T *corr2, T dt, T visc, const Args &a, cudaStream_t st)
+{
+    if (stretch) {
+        switch (phys) {
+        case PHYS_NS: launch_stage_t<T, PHYS_NS, true>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, true>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        default: launch_stage_t<T, PHYS_MHD_B, true>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        }
+    } else {
+        switch (phys) {
+        case PHYS_NS: launch_stage_t<T, PHYS_NS, false>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, false>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        default: launch_stage_t<T, PHYS_MHD_B, false>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        }
     }
 }
 
 }  // namespace
 
-void launch_stage64(int phys, int stage, const Geo &g, const Coef<double> &co, const double *ia,
+void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
                     const double *corr2, double dt, double visc, const StageArgs64 &a, cudaStream_t st)
 {
-    switch (phys) {
-    case PHYS_NS: launch_phys<double, PHYS_NS>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-    case PHYS_MHD_U: launch_phys<double, PHYS_MHD_U>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-    default: launch_phys<double, PHYS_MHD_B>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-    }
+    launch_stage_any<double>(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, st);
 }
 
-void launch_stage32(int phys, int stage, const Geo &g, const Coef<float> &co, const float *ia,
+void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
                     const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st)
 {
-    switch (phys) {
-    case PHYS_NS: launch_phys<float, PHYS_NS>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-    case PHYS_MHD_U: launch_phys<float, PHYS_MHD_U>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-    default: launch_phys<float, PHYS_MHD_B>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-    }
+    launch_stage_any<float>(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, st);
 }
 
 }  // namespace nova

@@ -221,8 +221,12 @@ class Field:
         self.mesh.check(self.mesh.lib.nova_field_upload(self.mesh.h, self.h, _dptr(a), _iptr(n)))
         return self
 
-    def download(self, bc=None):
-        out = np.zeros(self.mesh.local_n + (self.nc,))
+    def download(self, bc=None, out=None):
+        shape = self.mesh.local_n + (self.nc,)
+        if out is None:
+            out = np.zeros(shape)
+        elif out.shape != shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape %s" % (shape,))
         n = np.array(self.mesh.local_n, np.int32)
         bcp = None
         if bc is not None:

@@ -5,7 +5,8 @@
  * app/OT_Poisson/OT.cpp do, then runs the reference's own loop bodies
  * (app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H) for the literal
  * mode, or the same loop with the stage state refreshed for the classical
- * RK4 mode.  I/O is raw little-endian float64 in the Field<T> layout.
+ * RK4 mode.  I/O is raw little-endian float64 in the Field<T> layout; the wall
+ * time of each step's loop body goes to <out>_time.txt, one line per step.
  *
  *   nova_ref run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U.bin> <B.bin|-> <out>
  *   nova_ref ops <case> <nu> <U.bin> <s.bin> <out>
@@ -13,6 +14,7 @@
  *
  * <case> holds `mesh` and the BC files (UBC, pBC, BBC, pBBC).
  */
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
@@ -103,8 +105,9 @@ static int run(int argc, char **argv)
         pB.correctBoundaryConditions();
     }
 
-    std::vector<double> hist;
+    std::vector<double> hist, step_s;
     for (int step = 0; step < nsteps; step++) {
+        const auto t0 = std::chrono::steady_clock::now();
         time++;
         if (!mhd && !classical) {
 #include "TG_Piosson/RKLoop.H"
@@ -141,6 +144,7 @@ static int run(int argc, char **argv)
 #include "OT_Poisson/BEqn.H"
             }
         }
+        step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
         double row[6] = {double(step + 1), time.curTime(), ek_mean(mesh, U), mhd ? ek_mean(mesh, B) : 0.0, 0.0, 0.0};
         {
             auto d = ex::div(U);
@@ -161,6 +165,10 @@ static int run(int argc, char **argv)
     }
     FILE *fp = std::fopen((out + "_hist.bin").c_str(), "wb");
     std::fwrite(hist.data(), sizeof(double), hist.size(), fp);
+    std::fclose(fp);
+    /* wall time of each time-step loop body (diagnostics and I/O excluded) */
+    fp = std::fopen((out + "_time.txt").c_str(), "w");
+    for (double t : step_s) std::fprintf(fp, "%.9f\n", t);
     std::fclose(fp);
     return 0;
 }

@@ -63,9 +63,8 @@ def test_taylor_green_fp64_vs_oracle(nova, oracle, rk_mode):
     kw = dict(model="ns", rk_mode=rk_mode, nsteps=20, dt=dt, nu=1 / 1600)
     g = gpu_run(nova, OM, U0, **kw)
     o = oracle_run(oracle, OM, U0, **kw)
-    for c in range(3):
-        assert rel_l2(g["U"][c], o["U"][c]) < TOL64 or np.abs(o["U"][c]).max() < 1e-12
-    assert np.abs(g["U"][2]).max() < 1e-12  # w stays zero for this field
+    for c in range(3):  # w = 0 initially; -dp/dz makes it grow
+        assert rel_l2(g["U"][c], o["U"][c]) < TOL64, (c, rel_l2(g["U"][c], o["U"][c]))
     assert rel_l2(g["p"], o["p"]) < TOL64
     check_hist(g["hist"], o["hist"])
 

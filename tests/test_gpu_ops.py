@@ -115,5 +115,9 @@ def test_operator_argument_errors(nova):
     with pytest.raises(nova.NovaError) as e:
         GM.check(GM.lib.nova_grad_s(GM.h, a.h, s.h))  # wrong component counts
     assert e.value.status == nova.E_INVALID
-    with pytest.raises(nova.NovaError):
-        nova.Field(GM, 3).upload(np.zeros((5, 5, 5, 3)))
+    # a host buffer whose ghosted shape does not match the mesh is refused by the C ABI
+    bad = np.zeros((5, 5, 5, 3))
+    n = np.array([5, 5, 5], np.int32)
+    st = GM.lib.nova_field_upload(GM.h, a.h, bad.ctypes.data_as(nova.C.POINTER(nova.C.c_double)),
+                                  n.ctypes.data_as(nova.C.POINTER(nova.C.c_int)))
+    assert st == nova.E_INVALID
