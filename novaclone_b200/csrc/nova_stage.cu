@@ -34,10 +34,20 @@
 
 #include <type_traits>
 
-// minimum resident blocks per SM requested from the register allocator
+// minimum resident blocks per SM requested from the register allocator for
+// the Navier-Stokes kernels (FP64, FP32); the MHD kernels (6 halo'd
+// components) ask for one
 #ifndef NOVA_STAGE_MINB
 #define NOVA_STAGE_MINB 2
 #endif
+#ifndef NOVA_STAGE_MINB32
+#define NOVA_STAGE_MINB32 2
+#endif
+
+template <typename T, int PHYS> constexpr int stage_minb()
+{
+    return PHYS != 0 ? 1 : (sizeof(T) == 8 ? NOVA_STAGE_MINB : NOVA_STAGE_MINB32);
+}
 
 namespace nova {
 
@@ -65,7 +75,7 @@ __device__ __forceinline__ T lsum(const V &v, int c, const T *b)
 }
 
 template <typename T, int H, int PHYS, int STAGE, bool STRETCH, class Args>
-__global__ void __launch_bounds__(kThreads, NOVA_STAGE_MINB) k_stage(Geo g, Coef<T> co, const T *__restrict__ ia,
+__global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo g, Coef<T> co, const T *__restrict__ ia,
                                                       const T *__restrict__ corr2, T dt, T visc, Args args,
                                                       int ichunk)
 {
@@ -92,32 +102,46 @@ __global__ void __launch_bounds__(kThreads, NOVA_STAGE_MINB) k_stage(Geo g, Coef
 #pragma unroll
     for (int c = 0; c < NC; c++) src[c] = ((c < 3) ? args.Y : args.X) + (long long)(c % 3) * g.N3;
 
-    tile_march<T, H, NC>(
-        g, sm, [&](int c, long long o) { return src[c][o]; }, ib, ie,
-        [&](long long idx, auto &q, const auto &vx, const auto &vy, const auto &vz) {
-            // epilogue operands first, so their latency overlaps the arithmetic
-            T e0[3], e1[3];
+    // pointwise epilogue operands (base, accumulator): prefetched one plane
+    // ahead in FP64; the FP32 kernels load them at the start of the plane
+    // (measured faster there: fewer live registers)
+    constexpr bool kE0 = (STAGE == 1 || STAGE == 2) || (!std::is_same<T, double>::value && STAGE == 3);
+    constexpr bool kE1 = (STAGE >= 1 && STAGE <= 3);
+    constexpr bool kAhead = std::is_same<T, double>::value;
+    const T *e0p = nullptr, *e1p = nullptr;
+    if constexpr (std::is_same<T, double>::value) {
+        e0p = args.U0;
+    } else {
+        e0p = args.U0hi;
+    }
+    e1p = args.A;
+    T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e0n[3] = {0, 0, 0}, e1n[3] = {0, 0, 0};
+    auto pre = [&](long long nidx, bool load) {
+        if constexpr (kAhead) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const long long o = (long long)c * g.N3 + idx;
-                if constexpr (std::is_same<T, double>::value) {
-                    if constexpr (STAGE == 1 || STAGE == 2) {
-                        e0[c] = args.U0[o];
-                        e1[c] = args.A[o];
-                    } else if constexpr (STAGE == 3) {
-                        e1[c] = args.A[o];
-                    }
-                } else {
-                    if constexpr (STAGE == 1 || STAGE == 2) {
-                        e0[c] = args.U0hi[o];
-                        e1[c] = args.A[o];
-                    } else if constexpr (STAGE == 3) {
-                        e0[c] = args.U0hi[o];
-                        e1[c] = args.A[o];
-                    }
+                e0[c] = e0n[c];
+                e1[c] = e1n[c];
+                if (load) {
+                    const long long o = (long long)c * g.N3 + nidx;
+                    if constexpr (kE0) e0n[c] = e0p[o];
+                    if constexpr (kE1) e1n[c] = e1p[o];
                 }
             }
+        }
+    };
 
+    tile_march<T, H, NC>(
+        g, sm, [&](int c, long long o) { return src[c][o]; }, ib, ie, pre,
+        [&](long long idx, auto &q, const auto &vx, const auto &vy, const auto &vz) {
+            if constexpr (!kAhead) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const long long o = (long long)c * g.N3 + idx;
+                    if constexpr (kE0) e0[c] = e0p[o];
+                    if constexpr (kE1) e1[c] = e1p[o];
+                }
+            }
             T rhs[3];
             if constexpr (PHYS == PHYS_NS) {
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
@@ -262,7 +286,7 @@ void launch_one(const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T 
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    const int bps = (std::is_same<T, double>::value && PHYS != PHYS_NS) ? 1 : 2;
+    const int bps = stage_minb<T, PHYS>();
     const int ch = pick_ichunk(g, bps);
     kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, corr2, dt, visc, a, ch);
 }

@@ -1,4 +1,5 @@
-// 2.5-D tile march shared by the fused forward and adjoint stage kernels.
+// 2.5-D tile march shared by the fused forward and adjoint stage kernels and
+// the tiled projection kernels.
 //
 // A block of kTK x kTJ threads owns a kTK(k) x kTJ(j) column of the grid and
 // walks it along i over [ib, ie).  Each thread keeps its column's 2H+1 planes
@@ -8,12 +9,21 @@
 // synthesises the periodic ghosts (src/BC/periodicBC.hxx:1-66) at load time.
 //
 // Pipelining: the shared plane is double-buffered, so one barrier per plane
-// suffices, and the global loads of the next plane (queue head and halo) are
-// issued right after that barrier, before the current plane's arithmetic, so
-// their latency overlaps the math.
+// suffices; the global loads of the next plane (queue head, halo and, through
+// the `pre` hook, the caller's pointwise operands) are issued right after that
+// barrier, before the current plane's arithmetic, so their latency overlaps
+// the math.
 #pragma once
 
 #include "nova_internal.cuh"
+
+// unroll factor of the plane loop (2H+1 would turn the queue rotation into
+// register renaming, but the extra live ranges cost more than the moves)
+#ifndef NOVA_MARCH_UNROLL
+#define NOVA_MARCH_UNROLL 1
+#endif
+#define NOVA_PRAGMA(x) _Pragma(#x)
+#define NOVA_UNROLL(n) NOVA_PRAGMA(unroll n)
 
 namespace nova {
 
@@ -23,13 +33,21 @@ template <typename T, int H, int NC> struct TileSmem {
 
 template <typename T, int H, int NC> constexpr size_t tile_smem_bytes() { return sizeof(TileSmem<T, H, NC>); }
 
+struct NoPre {
+    __device__ void operator()(long long, bool) const {}
+};
+
 // ld(c, o) returns component c at linear node index o.
-// body(idx, q, vx, vy, vz) runs for valid threads once per plane, with idx the
-// linear index of the thread's node, q the register queue and vx/vy/vz(c, s)
-// the neighbour accessors along i, j, k.
-template <typename T, int H, int NC, class Ld, class Body>
+// pre(idx, load) runs for valid threads once before the loop with the first
+// plane's node (load = true) and then once per plane before body, with the
+// next plane's node and load = (a next plane exists): it lets the caller
+// rotate its own prefetched pointwise operands and issue the next ones.
+// body(idx, q, vx, vy, vz) runs for valid threads once per plane, with idx
+// the thread's node, q the register queue and vx/vy/vz(c, s) the neighbour
+// accessors along i, j, k.
+template <typename T, int H, int NC, class Ld, class Pre, class Body>
 __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm, const Ld &ld, int ib, int ie,
-                                           Body &&body)
+                                           Pre &&pre, Body &&body)
 {
     constexpr int NJH = 2 * H * kTK;
     constexpr int NKH = 2 * H * kTJ;
@@ -74,10 +92,11 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
 #pragma unroll
         for (int c = 0; c < NC; c++) q[s + 1][c] = ld(c, p);
     }
-    // loads for the first plane
+    // plane index of the queue head, kept wrapped incrementally
+    int lead = wrapi(ib + H, g.N0);
     T qn[NC], hn[HS][NC];
     {
-        const long long p = (long long)wrapi(ib + H, g.N0) * g.N12 + colOff;
+        const long long p = (long long)lead * g.N12 + colOff;
         const long long plane = (long long)ib * g.N12;
 #pragma unroll
         for (int c = 0; c < NC; c++) qn[c] = ld(c, p);
@@ -85,8 +104,10 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
         for (int s = 0; s < HS; s++)
 #pragma unroll
             for (int c = 0; c < NC; c++) hn[s][c] = hon[s] ? ld(c, plane + hoff[s]) : T(0);
+        if (valid) pre(plane + colOff, true);
     }
 
+    NOVA_UNROLL(NOVA_MARCH_UNROLL)
     for (int i = ib; i < ie; i++) {
         const int b = (i - ib) & 1;
 #pragma unroll
@@ -104,23 +125,33 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
 #pragma unroll
                 for (int c = 0; c < NC; c++) sm.v[b][c][hrow[s]][hcol[s]] = hn[s][c];
         __syncthreads();
-        if (i + 1 < ie) {  // next plane's loads fly during this plane's arithmetic
-            const long long p = (long long)wrapi(i + 1 + H, g.N0) * g.N12 + colOff;
-            const long long plane = (long long)(i + 1) * g.N12;
+        const bool more = i + 1 < ie;
+        const long long nplane = (long long)(i + 1) * g.N12;
+        if (more) {  // next plane's loads fly during this plane's arithmetic
+            lead = (lead + 1 == g.N0) ? 0 : lead + 1;
+            const long long p = (long long)lead * g.N12 + colOff;
 #pragma unroll
             for (int c = 0; c < NC; c++) qn[c] = ld(c, p);
 #pragma unroll
             for (int s = 0; s < HS; s++)
                 if (hon[s])
 #pragma unroll
-                    for (int c = 0; c < NC; c++) hn[s][c] = ld(c, plane + hoff[s]);
+                    for (int c = 0; c < NC; c++) hn[s][c] = ld(c, nplane + hoff[s]);
         }
         if (!valid) continue;
+        pre(nplane + colOff, more);
         auto vx = [&](int c, int s) -> T { return q[H + s][c]; };
         auto vy = [&](int c, int s) -> T { return sm.v[b][c][ty + H + s][tx + H]; };
         auto vz = [&](int c, int s) -> T { return sm.v[b][c][ty + H][tx + H + s]; };
         body((long long)i * g.N12 + colOff, q, vx, vy, vz);
     }
+}
+
+template <typename T, int H, int NC, class Ld, class Body>
+__device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm, const Ld &ld, int ib, int ie,
+                                           Body &&body)
+{
+    tile_march<T, H, NC>(g, sm, ld, ib, ie, NoPre{}, body);
 }
 
 // grid shape of a tile march: k tiles x j tiles x i chunks
