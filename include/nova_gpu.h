@@ -139,8 +139,24 @@ nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *s, double *out);
 /* hist: nsteps x NOVA_HIST_COLS doubles (rows of steps without diagnostics are zero); may be NULL */
 nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *run, nova_state *state, int nsteps, double *hist);
 
+/* ---- discrete adjoint (no counterpart in the reference: added capability) ---- */
+typedef enum { NOVA_OBJ_EKIN_FINAL = 0 } nova_objective;
+typedef struct {
+    nova_run_desc run;     /* forward run: NS, classical RK4, FP64 */
+    int nsteps;            /* steps of the forward solve */
+    int checkpoint_every;  /* K: states kept every K steps, segments recomputed in reverse */
+    int objective;         /* nova_objective: J = mean(1/2 |U|^2) at the final step */
+} nova_adj_desc;
+/* Gradient of J(U(T)) with respect to the initial velocity by the hand-written
+ * discrete adjoint of the fused stage, the RK4 loop and the (self-adjoint)
+ * projection.  init->U is not modified; gradU receives dJ/dU0 (FP64, 3 comps);
+ * *objective receives J.  gradB is reserved for the MHD adjoint (pass NULL). */
+nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *adj, const nova_state *init, nova_field *gradU,
+                              nova_field *gradB, double *objective);
+
 /* ---- instrumentation: per-kernel CUDA-event timing of nova_advance ---- */
-typedef enum { NOVA_K_STAGE = 0, NOVA_K_DIV = 1, NOVA_K_FFT = 2, NOVA_K_CORRECT = 3, NOVA_K_DIAG = 4, NOVA_K_COUNT = 5 } nova_kernel_class;
+typedef enum { NOVA_K_STAGE = 0, NOVA_K_DIV = 1, NOVA_K_FFT = 2, NOVA_K_CORRECT = 3, NOVA_K_DIAG = 4, NOVA_K_ADJ = 5,
+               NOVA_K_COUNT = 6 } nova_kernel_class;
 nova_status nova_profile_enable(nova_ctx *ctx, int on);
 /* total milliseconds and launch count per class since the last reset */
 nova_status nova_profile_read(nova_ctx *ctx, int kernel_class, double *total_ms, long *launches, int reset);

@@ -65,6 +65,9 @@ struct nova_ctx {
     long long hist_cap = 0;
     double *d_stage = nullptr;
     size_t stage_cap = 0;
+    double *adj_pool = nullptr;  // adjoint checkpoints, segment states, adjoint fields
+    size_t adj_cap = 0;
+    double *d_row = nullptr;     // one diagnostics row
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::string err;
@@ -386,7 +389,7 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
     }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage};
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -822,6 +825,154 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     CK(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (flag) return fail(ctx, NOVA_E_NONFINITE, "nova_advance: non-finite value in the diagnostics");
+    return NOVA_OK;
+}
+
+// ================================================================== adjoint ==
+namespace {
+
+// One classical RK4 step + projection of an FP64 Navier-Stokes state:
+// Uin -> Uout (may alias), stage states into Y2, Y3, Y4 (Y4 may alias Y2).
+// Without `full` only the stage states are produced.
+nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin, double *Y2, double *Y3, double *Y4,
+                       double *Uout, bool full)
+{
+    const Geo &g = ctx->g;
+    cudaStream_t st = ctx->stream;
+    double *A = ctx->w64[2];
+    const bool str = ctx->md.hyperbolic_z != 0;
+    auto run = [&](int stage, const StageArgs64 &a) {
+        ProfScope ps(ctx, NOVA_K_STAGE);
+        launch_stage64(PHYS_NS, stage, str, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, rd->nu, a, st);
+        ctx->launches += 1;
+    };
+    run(0, StageArgs64{Uin, nullptr, nullptr, A, Y2});
+    run(1, StageArgs64{Y2, nullptr, Uin, A, Y3});
+    run(2, StageArgs64{Y3, nullptr, Uin, A, Y4});
+    if (!full) {
+        CKL("stage kernel");
+        return NOVA_OK;
+    }
+    run(3, StageArgs64{Y4, nullptr, nullptr, A, Uout});
+    CKL("stage kernel");
+    launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt, ctx->d_rhs, st);
+    ctx->launches += 1;
+    CKL("k_div_tiled");
+    nova_status s = poisson_device(ctx, ctx->d_rhs, ctx->w64[1]);
+    if (s != NOVA_OK) return s;
+    launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, ctx->w64[1], rd->dt, Uout, Uout, nullptr, nullptr, nullptr,
+                   nullptr, st);
+    ctx->launches += 1;
+    CKL("k_correct_tiled");
+    return NOVA_OK;
+}
+
+// out = P in = in - G L^-1 D in (the projection is symmetric: its own adjoint)
+nova_status project64(nova_ctx *ctx, const double *in, double *out, double *pbuf)
+{
+    const Geo &g = ctx->g;
+    launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, in, nullptr, nullptr, 1.0, ctx->d_rhs, ctx->stream);
+    ctx->launches += 1;
+    CKL("k_div_tiled");
+    nova_status s = poisson_device(ctx, ctx->d_rhs, pbuf);
+    if (s != NOVA_OK) return s;
+    launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, pbuf, 1.0, in, out, nullptr, nullptr, nullptr, nullptr,
+                   ctx->stream);
+    ctx->launches += 1;
+    CKL("k_correct_tiled");
+    return NOVA_OK;
+}
+
+}  // namespace
+
+extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init,
+                                         nova_field *gradU, nova_field *gradB, double *objective)
+{
+    if (!ctx || !ad || !init || !gradU) return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: null argument");
+    const nova_run_desc *rd = &ad->run;
+    if (rd->model != NOVA_MODEL_NS || rd->rk_mode != NOVA_RK_CLASSICAL || rd->precision != NOVA_F64 || gradB)
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: built for FP64 Navier-Stokes, classical RK4");
+    if (ad->objective != NOVA_OBJ_EKIN_FINAL) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: objective");
+    if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: the fused kernels are built for m = 6");
+    if (ad->nsteps < 1 || ad->checkpoint_every < 1 || !(rd->dt > 0.0))
+        return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: nsteps, checkpoint_every and dt must be positive");
+    if (!valid_field(init->U, 3) || init->U->prec != NOVA_F64 || !valid_field(gradU, 3) || gradU->prec != NOVA_F64)
+        return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: U and gradU must be FP64 3-component fields");
+    nova_status s = ensure_work(ctx, NOVA_F64);
+    if (s != NOVA_OK) return s;
+    const int N = ad->nsteps, K = ad->checkpoint_every;
+    const int nck = (N + K - 1) / K;
+    const int mmax = K < N ? K : N;
+    const size_t V = 3 * (size_t)ctx->g.N3;
+    // layout: nck checkpoints | 4*mmax segment fields | lam, mu, gA, gB, Lam
+    const size_t need = V * ((size_t)nck + 4 * (size_t)mmax + 5);
+    if (ctx->adj_cap < need) {
+        if (ctx->adj_pool) cudaFree(ctx->adj_pool);
+        ctx->adj_pool = nullptr;
+        ctx->adj_cap = 0;
+        if ((s = dalloc(ctx, &ctx->adj_pool, need)) != NOVA_OK) return s;
+        ctx->adj_cap = need;
+    }
+    double *ck = ctx->adj_pool;
+    double *seg = ck + V * nck;
+    double *lam = seg + V * 4 * mmax, *mu = lam + V, *gA = mu + V, *gB = gA + V, *Lam = gB + V;
+    auto St = [&](int t) { return seg + V * (4 * (size_t)t + 0); };
+    auto Y2 = [&](int t) { return seg + V * (4 * (size_t)t + 1); };
+    auto Y3 = [&](int t) { return seg + V * (4 * (size_t)t + 2); };
+    auto Y4 = [&](int t) { return seg + V * (4 * (size_t)t + 3); };
+    cudaStream_t st = ctx->stream;
+
+    // forward pass, keeping every K-th state (the running state lives in mu)
+    CK(cudaMemcpyAsync(ck, init->U->d64, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    for (int n = 0; n < N; n++) {
+        const double *src = (n % K == 0) ? ck + V * (n / K) : mu;
+        if ((s = fwd_step64(ctx, rd, src, ctx->w64[0], ctx->w64[1], ctx->w64[0], mu, true)) != NOVA_OK) return s;
+        if ((n + 1) % K == 0 && n + 1 < N)
+            CK(cudaMemcpyAsync(ck + V * ((n + 1) / K), mu, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    }
+    // J = mean 1/2 |U_N|^2 and lambda_N = U_N / N^3
+    if ((s = dalloc(ctx, &ctx->d_row, NOVA_HIST_COLS)) != NOVA_OK) return s;
+    launch_diag(ctx->h, ctx->g, ctx->co64, ctx->d_ia64, mu, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
+                ctx->d_part, (double)N, N * rd->dt, ctx->d_row, ctx->d_flag, st);
+    ctx->launches += 2;
+    double row[NOVA_HIST_COLS];
+    CK(cudaMemcpyAsync(row, ctx->d_row, sizeof(row), cudaMemcpyDeviceToHost, st));
+    launch_scale_copy((long long)V, 1.0 / (double)ctx->g.N3, mu, lam, st);
+    ctx->launches += 1;
+    CKL("adjoint seed");
+
+    // reverse sweep, segment by segment
+    for (int c = nck - 1; c >= 0; c--) {
+        const int n0 = c * K;
+        const int m = (N - n0) < K ? (N - n0) : K;
+        CK(cudaMemcpyAsync(St(0), ck + V * c, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+        for (int t = 0; t < m; t++) {
+            const bool full = t + 1 < m;
+            if ((s = fwd_step64(ctx, rd, St(t), Y2(t), Y3(t), Y4(t), full ? St(t + 1) : nullptr, full)) != NOVA_OK)
+                return s;
+        }
+        for (int t = m - 1; t >= 0; t--) {
+            {
+                ProfScope ps(ctx, NOVA_K_DIV);
+                if ((s = project64(ctx, lam, mu, gB)) != NOVA_OK) return s;
+            }
+            const double dt = rd->dt, nu = rd->nu;
+            auto adj = [&](int stage, const AdjArgs &a) {
+                ProfScope ps(ctx, NOVA_K_ADJ);
+                launch_adj_stage64(stage, ctx->g, ctx->co64, ctx->d_ia64, dt, nu, a, st);
+                ctx->launches += 1;
+            };
+            adj(4, AdjArgs{Y4(t), mu, mu, nullptr, gA, Lam});
+            adj(3, AdjArgs{Y3(t), gA, mu, Lam, gB, Lam});
+            adj(2, AdjArgs{Y2(t), gB, mu, Lam, gA, Lam});
+            adj(1, AdjArgs{St(t), gA, mu, Lam, lam, nullptr});
+            CKL("k_adj_stage");
+        }
+    }
+    CK(cudaMemcpyAsync(gradU->d64, lam, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    if (objective) *objective = row[2];
+    if (!std::isfinite(row[2])) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
     return NOVA_OK;
 }
 

@@ -67,6 +67,28 @@ __device__ __forceinline__ T d2(const V &v, int c, const T *b, T b2)
     return fma(-b2, v(c, 0), r);
 }
 
+// A_d(V,F)_c = sum_l a_l [ F_c(+l) (V_d(+l) + V_d(0)) - F_c(-l) (V_d(-l) + V_d(0)) ]
+//            = D_d(V_d F_c) + V_d(0) D_d F_c;  cf = component of F, cv = V_d, v0 = V_d(0)
+template <typename T, int H, class V>
+__device__ __forceinline__ T adv1(const V &v, int cf, int cv, T v0, const T *a)
+{
+    T r = a[0] * (v(cf, 1) * (v(cv, 1) + v0) - v(cf, -1) * (v(cv, -1) + v0));
+#pragma unroll
+    for (int l = 1; l < H; l++)
+        r = fma(a[l], v(cf, l + 1) * (v(cv, l + 1) + v0) - v(cf, -l - 1) * (v(cv, -l - 1) + v0), r);
+    return r;
+}
+
+// sum_l b_l (f(+l) + f(-l)); the centre term of the Laplacian is added once for all directions
+template <typename T, int H, class V>
+__device__ __forceinline__ T lsum(const V &v, int c, const T *b)
+{
+    T r = b[0] * (v(c, 1) + v(c, -1));
+#pragma unroll
+    for (int l = 1; l < H; l++) r = fma(b[l], v(c, l + 1) + v(c, -l - 1), r);
+    return r;
+}
+
 // ------------------------------------------------------------- launch helpers --
 struct StageArgs64 {
     const double *Y;   // halo'd stage state (3 comps)
@@ -87,6 +109,19 @@ struct StageArgs32 {
 };
 
 enum Physics { PHYS_NS = 0, PHYS_MHD_U = 1, PHYS_MHD_B = 2 };
+
+// reverse RK4 stage of the discrete adjoint (nova_adjoint.cu)
+struct AdjArgs {
+    const double *Y;    // forward stage state Y_s (3 comps, halo'd)
+    const double *G;    // adjoint stage direction g_s (halo'd); mu itself at s = 4
+    const double *mu;   // projected adjoint of U*
+    const double *Lam;  // running sum of xi (s < 4)
+    double *Gout;       // g_{s-1}, or dJ/dU at s = 1
+    double *LamOut;     // updated running sum (s > 1)
+};
+void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
+                        const AdjArgs &a, cudaStream_t st);
+void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);
 
 // stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum)
 // stretch: apply the stretched-z Laplacian term (Mesh "hypz:"); on uniform

@@ -53,27 +53,6 @@ namespace nova {
 
 namespace {
 
-// A_d(V,F)_c of the header: cf = component of F, cv = component V_d, v0 = V_d(0)
-template <typename T, int H, class V>
-__device__ __forceinline__ T adv1(const V &v, int cf, int cv, T v0, const T *a)
-{
-    T r = a[0] * (v(cf, 1) * (v(cv, 1) + v0) - v(cf, -1) * (v(cv, -1) + v0));
-#pragma unroll
-    for (int l = 1; l < H; l++)
-        r = fma(a[l], v(cf, l + 1) * (v(cv, l + 1) + v0) - v(cf, -l - 1) * (v(cv, -l - 1) + v0), r);
-    return r;
-}
-
-// sum_l b_l (f(+l) + f(-l)); the centre term is added once for all directions
-template <typename T, int H, class V>
-__device__ __forceinline__ T lsum(const V &v, int c, const T *b)
-{
-    T r = b[0] * (v(c, 1) + v(c, -1));
-#pragma unroll
-    for (int l = 1; l < H; l++) r = fma(b[l], v(c, l + 1) + v(c, -l - 1), r);
-    return r;
-}
-
 template <typename T, int H, int PHYS, int STAGE, bool STRETCH, class Args>
 __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo g, Coef<T> co, const T *__restrict__ ia,
                                                       const T *__restrict__ corr2, T dt, T visc, Args args,

@@ -23,7 +23,8 @@ PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
 MODEL_NS, MODEL_MHD = 0, 1
 RK_LITERAL, RK_CLASSICAL = 0, 1
 HIST_COLS = 6
-K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG = range(5)
+K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG, K_ADJ = range(6)
+OBJ_EKIN_FINAL = 0
 STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_OOM", 4: "NOVA_E_NONFINITE",
                 5: "NOVA_E_TIMEOUT", 6: "NOVA_E_UNSUPPORTED"}
 
@@ -33,7 +34,8 @@ EXPORTS = (
     "nova_mesh_metrics", "nova_field_create", "nova_field_destroy", "nova_field_upload", "nova_field_download",
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
-    "nova_field_maxabs", "nova_advance", "nova_profile_enable", "nova_profile_read", "nova_launch_count",
+    "nova_field_maxabs", "nova_advance", "nova_adjoint_grad", "nova_profile_enable", "nova_profile_read",
+    "nova_launch_count",
 )
 
 
@@ -49,6 +51,10 @@ class BCDesc(C.Structure):
 class RunDesc(C.Structure):
     _fields_ = [("model", C.c_int), ("rk_mode", C.c_int), ("precision", C.c_int), ("diag_every", C.c_int),
                 ("dt", C.c_double), ("nu", C.c_double), ("eta", C.c_double), ("t0", C.c_double)]
+
+
+class AdjDesc(C.Structure):
+    _fields_ = [("run", RunDesc), ("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("objective", C.c_int)]
 
 
 class State(C.Structure):
@@ -97,6 +103,7 @@ def load_library(path: str = LIB_PATH):
         "nova_poisson_solve": [vp, vp, vp],
         "nova_field_maxabs": [vp, vp, dp],
         "nova_advance": [vp, C.POINTER(RunDesc), C.POINTER(State), C.c_int, dp],
+        "nova_adjoint_grad": [vp, C.POINTER(AdjDesc), C.POINTER(State), vp, vp, dp],
         "nova_profile_enable": [vp, C.c_int],
         "nova_profile_read": [vp, C.c_int, dp, C.POINTER(C.c_long), C.c_int],
         "nova_launch_count": [vp, C.POINTER(C.c_long), C.c_int],
@@ -339,3 +346,17 @@ def advance(mesh: Mesh, rd: RunDesc, U: Field, p: Field, B: Field = None, pB: Fi
     mesh.check(mesh.lib.nova_advance(mesh.h, C.byref(rd), C.byref(st), int(nsteps),
                                      _dptr(hist) if history else None))
     return hist
+
+
+def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_every: int = 20):
+    """dJ/dU0 for J = mean(1/2 |U(nsteps)|^2) by the discrete adjoint; returns (J, grad Field)."""
+    a = AdjDesc()
+    a.run = rd
+    a.nsteps = int(nsteps)
+    a.checkpoint_every = int(checkpoint_every)
+    a.objective = OBJ_EKIN_FINAL
+    grad = Field(mesh, 3)
+    st = State(U0.h, None, None, None)
+    J = C.c_double()
+    mesh.check(mesh.lib.nova_adjoint_grad(mesh.h, C.byref(a), C.byref(st), grad.h, None, C.byref(J)))
+    return J.value, grad
