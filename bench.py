@@ -308,6 +308,32 @@ def our_arm(args, rank, world, dist):
         U.close()
 
     err = float(np.linalg.norm(finals["f32split"] - finals["f64"]) / np.linalg.norm(finals["f64"]))
+
+    # adjoint / forward wall-time ratio (FP64): gradient of E_kin after M steps
+    # with checkpoints every K steps, against an M-step forward solve
+    adj = None
+    if not args.no_adjoint:
+        M, K = args.adj_steps, args.adj_checkpoint
+        U = nova.Field(GM, 3).upload_soa(U0)
+        rd = nova.run_desc(model="ns", rk_mode="classical", precision=nova.F64, dt=dt, nu=NU, diag_every=0)
+        nova.adjoint_grad(GM, rd, U, 2, checkpoint_every=1)  # allocate and warm the path
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record()
+        nova.advance(GM, rd, U, p, nsteps=M, history=False)
+        e[1].record()
+        U.upload_soa(U0)
+        torch.cuda.synchronize()
+        e[2].record()
+        J, grad = nova.adjoint_grad(GM, rd, U, M, checkpoint_every=K)
+        e[3].record()
+        torch.cuda.synchronize()
+        t_fwd = e[0].elapsed_time(e[1]) / 1e3
+        t_adj = e[2].elapsed_time(e[3]) / 1e3
+        adj = {"ratio": maxover(t_adj) / maxover(t_fwd), "forward_s": t_fwd, "adjoint_s": t_adj, "steps": M,
+               "checkpoint_every": K, "objective": "E_kin at the final step", "dtype": "f64", "J": J}
+        grad.close()
+        U.close()
     t_end = (args.warmup + args.steps) * dt
 
     # e2e through the reference-layout ABI (ghosted AoS host buffers, pinned)
@@ -376,7 +402,8 @@ def our_arm(args, rank, world, dist):
                       "rel_l2_vs_fp64": err, "at_time": t_end, "steps_compared": args.warmup + args.steps,
                       "dtype": "f32 stencils, (hi,lo) f32 state, f64 projection", "roofline": roof("f32split"),
                       "e2e": e2e.get("f32split"), "gpu_launches": f32["launches"], "clocks": f32["clocks"]},
-        "adjoint_fwd_ratio": None,
+        "adjoint_fwd_ratio": None if adj is None else adj["ratio"],
+        "adjoint": adj,
     }
     print(json.dumps(line))
     return 0
@@ -394,6 +421,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=40)
+    ap.add_argument("--adj-checkpoint", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

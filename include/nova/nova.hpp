@@ -242,6 +242,25 @@ public:
             pB_ = make(1, NOVA_F64);
         }
     }
+    // aos: the reference's Field<vector>::ptr() (ghosted array-of-structs, 3 doubles per node)
+    void setU(const void *aos)
+    {
+        check(mesh_.ctx(), nova_field_upload(mesh_.ctx(), U_.get(), (const double *)aos, mesh_.local_n()), "upload U");
+    }
+    void setB(const void *aos)
+    {
+        check(mesh_.ctx(), nova_field_upload(mesh_.ctx(), B_.get(), (const double *)aos, mesh_.local_n()), "upload B");
+    }
+    void getU(void *aos) const
+    {
+        check(mesh_.ctx(), nova_field_download(mesh_.ctx(), U_.get(), (double *)aos, mesh_.local_n(), nullptr),
+              "download U");
+    }
+    void getB(void *aos) const
+    {
+        check(mesh_.ctx(), nova_field_download(mesh_.ctx(), B_.get(), (double *)aos, mesh_.local_n(), nullptr),
+              "download B");
+    }
     void setU(const Field<vector> &U)
     {
         check(mesh_.ctx(), nova_field_upload(mesh_.ctx(), U_.get(), (const double *)U.ptr(), mesh_.local_n()), "upload U");
