@@ -78,6 +78,16 @@ def cfl_dt(n, U):
     return CFL * (2 * math.pi / n) / float(np.abs(U).sum(axis=0).max())
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest of a per-rank float over all ranks (the identity without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -287,11 +297,7 @@ def our_arm(args, rank, world, dist):
     p = nova.Field(GM, 1)
 
     def maxover(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, dist)
 
     res = {}
     finals = {}

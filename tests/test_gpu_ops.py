@@ -121,3 +121,41 @@ def test_operator_argument_errors(nova):
     st = GM.lib.nova_field_upload(GM.h, a.h, bad.ctypes.data_as(nova.C.POINTER(nova.C.c_double)),
                                   n.ctypes.data_as(nova.C.POINTER(nova.C.c_int)))
     assert st == nova.E_INVALID
+
+
+def test_stretched_z_metrics_and_operators(nova, oracle):
+    """Mesh 'hypz:' stretching (src/Mesh/Mesh.cpp:373-407): metrics equal the
+    oracle's, and every operator carries the dz/dxi terms as the reference does."""
+    N, hz = (12, 10, 16), (0.03, 0.03)
+    OM = oracle.Mesh(N, L=(2 * np.pi, 2 * np.pi, 1.0), hyperbolic_z=hz)
+    GM = nova.Mesh(N, L=(2 * np.pi, 2 * np.pi, 1.0), hyperbolic_z=hz)
+    a, b = GM.metrics()
+    h = OM.h
+    assert np.array_equal(a[h:-h], OM.dzdxi[h:-h]) and np.array_equal(b[h:-h], OM.d2zdxi2[h:-h])
+    assert np.abs(OM.dzdxi[h:-h] - 1).max() > 0.1  # really stretched
+    rng = np.random.default_rng(8)
+    U = rng.standard_normal((3,) + N)
+    s = rng.standard_normal((1,) + N)
+    Ug, sg = OM.to_ghosted(U), OM.to_ghosted(s)
+    dU = nova.Field(GM, 3).upload(Ug)
+    ds = nova.Field(GM, 1).upload(sg)
+    for got, ref in ((nova.ex.grad(ds), oracle.grad_s(OM, sg)), (nova.ex.div(dU), oracle.div_v(OM, Ug)),
+                     (nova.ex.div(dU, dU), oracle.div_vf(OM, Ug, Ug)),
+                     (nova.ex.laplacian(0.1, dU), oracle.lap(OM, 0.1, Ug))):
+        assert rel_max(OM.interior(got.download()), OM.interior(ref)) < TOL
+
+
+def test_stretched_z_advance(nova, oracle):
+    N, hz = (12, 10, 16), (0.03, 0.03)
+    L = (2 * np.pi, 2 * np.pi, 1.0)
+    OM = oracle.Mesh(N, L=L, hyperbolic_z=hz)
+    GM = nova.Mesh(N, L=L, hyperbolic_z=hz)
+    rng = np.random.default_rng(2)
+    U0 = 0.3 * rng.standard_normal((3,) + N)
+    U = nova.Field(GM, 3).upload_soa(U0)
+    p = nova.Field(GM, 1)
+    nova.advance(GM, nova.run_desc(model="ns", rk_mode="classical", dt=2e-3, nu=0.01), U, p, nsteps=3)
+    r = oracle.run(OM, OM.to_ghosted(U0), model="ns", rk_mode="classical", nsteps=3, dt=2e-3, nu=0.01)
+    ref = OM.unique(r[0])
+    for c in range(3):
+        assert np.linalg.norm(U.download_soa()[c] - ref[c]) / np.linalg.norm(ref[c]) < 1e-11
