@@ -68,6 +68,8 @@ typedef struct {
     int m;               /* stencil order 2, 4, 6 or 8 (settings::m_, default 6) */
     int hyperbolic_z;    /* "hypz:" present */
     double s1, s2;       /* "hypz:" arguments */
+    int walls[3];        /* 0 = periodic axis (default); 1 = bounded by walls (Neumann/Dirichlet
+                            faces, N+1 nodes stored).  This build supports walls in y only. */
 } nova_mesh_desc;
 
 /* BC lines "<face> <type> <val> <comp>" (src/Field/Field.hxx:519-547), index face + 6*comp. */
@@ -111,13 +113,20 @@ nova_status nova_mesh_metrics(const nova_ctx *ctx, double *dzdxi, double *d2zdxi
 /* ---- fields ---- */
 nova_status nova_field_create(nova_ctx *ctx, int ncomp, int precision, nova_field **out);
 nova_status nova_field_destroy(nova_ctx *ctx, nova_field *f);
+/* Field<T>::setBC (src/Field/Field.hxx:519-547): the field's boundary conditions, used for
+ * its ghosts in every stencil and for the wall-node overwrites of nova_advance.  Periodic
+ * axes need periodic faces; wall axes need Neumann or Dirichlet faces.  Default: periodic,
+ * Neumann 0 on wall faces. */
+nova_status nova_field_set_bc(nova_ctx *ctx, nova_field *f, const nova_bc *bc);
+nova_status nova_field_get_bc(nova_ctx *ctx, const nova_field *f, nova_bc *bc);
 /* Reference Field<T>::ptr() layout: ghosted, AoS, z fastest, local_n = N+1+m per axis.
  * Upload reads the N0*N1*N2 unique interior nodes; download writes the interior
  * (incl. the duplicate node) and fills the ghosts per `bc` (NULL = all periodic). */
 nova_status nova_field_upload(nova_ctx *ctx, nova_field *f, const double *host_aos, const int local_n[3]);
 nova_status nova_field_download(nova_ctx *ctx, const nova_field *f, double *host_aos, const int local_n[3],
                                 const nova_bc *bc);
-/* Device-native layout: component-major, unique points, z fastest: [c][i][j][k], float64. */
+/* Device-native layout: component-major, z fastest: [c][i][j][k], float64, over the
+ * stored nodes (N per periodic axis, N+1 per wall axis). */
 nova_status nova_field_upload_soa(nova_ctx *ctx, nova_field *f, const double *host_soa);
 nova_status nova_field_download_soa(nova_ctx *ctx, const nova_field *f, double *host_soa);
 /* Same, from/to device memory the caller owns (e.g. a torch tensor). */

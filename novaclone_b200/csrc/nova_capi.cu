@@ -22,6 +22,7 @@ struct nova_field {
     long long n3;
     double *d64;
     float *hi, *lo;
+    nova_bc bc;  // setBC of the reference field: index face + 6*comp
 };
 
 namespace {
@@ -80,6 +81,65 @@ struct nova_ctx {
 };
 
 namespace {
+
+// default BCs: periodic faces; Neumann 0 on wall faces
+void default_bc(const nova_ctx *ctx, nova_bc *bc)
+{
+    for (int q = 0; q < 18; q++) {
+        const int face = q % 6;
+        const bool ywall = ctx->g.wallY && (face == NOVA_NORTH || face == NOVA_SOUTH);
+        bc->type[q] = ywall ? NOVA_BC_NEUMANN : NOVA_BC_PERIODIC;
+        bc->val[q] = 0.0;
+    }
+}
+
+// ghosts of a field's components beyond the y walls (Walls<T>, nova_internal.cuh)
+template <typename T>
+void add_walls(const nova_ctx *ctx, const nova_field *f, Walls<T> &w, int c0)
+{
+    if (!ctx->g.wallY || !f) return;
+    w.on = 1;
+    const double dy = ctx->md.L[1] / ctx->md.N[1];
+    for (int c = 0; c < f->nc && c0 + c < 9; c++) {
+        for (int side = 0; side < 2; side++) {
+            const int q = (side == 0 ? NOVA_SOUTH : NOVA_NORTH) + 6 * (c < 3 ? c : 0);
+            const int type = f->bc.type[q];
+            const double val = f->bc.val[q];
+            if (type == NOVA_BC_DIRICHLET) {
+                w.sgn[side][c0 + c] = T(-1);
+                w.off[side][c0 + c] = T(2.0 * val);
+            } else {
+                w.sgn[side][c0 + c] = T(1);
+                w.off[side][c0 + c] = T(-2.0 * val * dy);
+            }
+        }
+    }
+}
+
+template <typename T> Walls<T> walls_of(const nova_ctx *ctx, const nova_field *a, const nova_field *b = nullptr)
+{
+    Walls<T> w{};
+    add_walls<T>(ctx, a, w, 0);
+    add_walls<T>(ctx, b, w, 3);
+    return w;
+}
+
+// the reference's wall-node overwrite for a field (k_wall_fix)
+WallFix wall_fix_of(const nova_ctx *ctx, const nova_field *f)
+{
+    WallFix wf{};
+    if (!ctx->g.wallY) return wf;
+    wf.on = 1;
+    wf.nc = f->nc;
+    wf.dy = ctx->md.L[1] / ctx->md.N[1];
+    for (int c = 0; c < f->nc && c < 9; c++)
+        for (int side = 0; side < 2; side++) {
+            const int q = (side == 0 ? NOVA_SOUTH : NOVA_NORTH) + 6 * (c < 3 ? c : 0);
+            wf.type[side][c] = f->bc.type[q];
+            wf.val[side][c] = f->bc.val[q];
+        }
+    return wf;
+}
 
 nova_status fail(nova_ctx *c, nova_status s, const std::string &msg)
 {
@@ -239,14 +299,23 @@ nova_status ensure_fft(nova_ctx *ctx)
     if (ctx->plans) return NOVA_OK;
     const Geo &g = ctx->g;
     nova_status s;
-    if ((s = fft_check(ctx, cufftPlan3d(&ctx->plan_f, g.N0, g.N1, g.N2, CUFFT_D2Z), "cufftPlan3d D2Z")) != NOVA_OK)
+    // the transform runs over the N[1] unique y nodes of poisson::rhs (poisson.cpp:167-181),
+    // which with walls are the first N[1] of the N[1]+1 stored rows
+    const int ny = ctx->md.N[1];
+    int n[3] = {g.N0, ny, g.N2};
+    int rembed[3] = {g.N0, g.N1, g.N2};
+    int cembed[3] = {g.N0, ny, g.N2 / 2 + 1};
+    const int rdist = g.N0 * g.N1 * g.N2, cdist = g.N0 * ny * (g.N2 / 2 + 1);
+    if ((s = fft_check(ctx, cufftPlanMany(&ctx->plan_f, 3, n, rembed, 1, rdist, cembed, 1, cdist, CUFFT_D2Z, 1),
+                       "cufftPlanMany D2Z")) != NOVA_OK)
         return s;
-    if ((s = fft_check(ctx, cufftPlan3d(&ctx->plan_b, g.N0, g.N1, g.N2, CUFFT_Z2D), "cufftPlan3d Z2D")) != NOVA_OK) {
+    if ((s = fft_check(ctx, cufftPlanMany(&ctx->plan_b, 3, n, cembed, 1, cdist, rembed, 1, rdist, CUFFT_Z2D, 1),
+                       "cufftPlanMany Z2D")) != NOVA_OK) {
         cufftDestroy(ctx->plan_f);
         return s;
     }
     ctx->plans = true;
-    const size_t nspec = (size_t)g.N0 * g.N1 * (g.N2 / 2 + 1);
+    const size_t nspec = (size_t)g.N0 * ny * (g.N2 / 2 + 1);
     if ((s = dalloc(ctx, (double **)&ctx->d_spec, 2 * nspec)) != NOVA_OK) return s;
     if ((s = dalloc(ctx, &ctx->d_rhs, (size_t)g.N3)) != NOVA_OK) return s;
     return NOVA_OK;
@@ -272,7 +341,9 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
     if ((s = fft_check(ctx, cufftExecD2Z(ctx->plan_f, (cufftDoubleReal *)rhs, (cufftDoubleComplex *)ctx->d_spec),
                        "cufftExecD2Z")) != NOVA_OK)
         return s;
-    launch_scale(ctx->g, ctx->d_spec, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2, 1.0 / (double)ctx->g.N3, ctx->stream);
+    const long long nuniq = (long long)ctx->g.N0 * ctx->md.N[1] * ctx->g.N2;
+    launch_scale(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2, 1.0 / (double)nuniq,
+                 ctx->stream);
     ctx->launches += 1;
     CKL("k_scale");
     if ((s = fft_check(ctx, cufftExecZ2D(ctx->plan_b, (cufftDoubleComplex *)ctx->d_spec, (cufftDoubleReal *)p),
@@ -306,15 +377,18 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
     *out = nullptr;
     if (md->m != 2 && md->m != 4 && md->m != 6 && md->m != 8) return NOVA_E_INVALID;
     for (int a = 0; a < 3; a++)
-        if (md->N[a] < 1 || !(md->L[a] > 0.0)) return NOVA_E_INVALID;
+        if (md->N[a] < 1 || !(md->L[a] > 0.0) || (md->walls[a] != 0 && md->walls[a] != 1)) return NOVA_E_INVALID;
+    if (md->walls[0] || md->walls[2]) return NOVA_E_UNSUPPORTED;  // walls in y only
+    if (md->walls[1] && md->N[1] < md->m) return NOVA_E_INVALID;   // the mirrored halo needs m/2 nodes per wall
     nova_ctx *ctx = new (std::nothrow) nova_ctx();
     if (!ctx) return NOVA_E_OOM;
     ctx->md = *md;
     ctx->h = md->m / 2;
     for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
     Geo &g = ctx->g;
+    g.wallY = md->walls[1];
     g.N0 = md->N[0];
-    g.N1 = md->N[1];
+    g.N1 = md->N[1] + g.wallY;
     g.N2 = md->N[2];
     g.N12 = (long long)g.N1 * g.N2;
     g.N3 = (long long)g.N0 * g.N12;
@@ -346,7 +420,7 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
     }
     const double dx = md->L[0] / md->N[0], dy = md->L[1] / md->N[1], dz = md->L[2] / md->N[2];
     std::vector<double> kx2 = kp2_table(g.N0, md->L[0], dx, ctx->h, c, true, g.N0);
-    std::vector<double> ky2 = kp2_table(g.N1, md->L[1], dy, ctx->h, c, true, g.N1);
+    std::vector<double> ky2 = kp2_table(md->N[1], md->L[1], dy, ctx->h, c, true, md->N[1]);
     std::vector<double> kz2 = kp2_table(g.N2, md->L[2], dz, ctx->h, c, false, g.N2 / 2 + 1);
 
     nova_status s = NOVA_OK;
@@ -450,6 +524,7 @@ extern "C" nova_status nova_field_create(nova_ctx *ctx, int ncomp, int precision
     f->nc = ncomp;
     f->prec = precision;
     f->n3 = ctx->g.N3;
+    default_bc(ctx, &f->bc);
     const size_t n = (size_t)ncomp * f->n3;
     nova_status s;
     if (precision == NOVA_F64) {
@@ -477,6 +552,31 @@ extern "C" nova_status nova_field_destroy(nova_ctx *ctx, nova_field *f)
     if (f->hi) cudaFree(f->hi);
     if (f->lo) cudaFree(f->lo);
     delete f;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_set_bc(nova_ctx *ctx, nova_field *f, const nova_bc *bc)
+{
+    if (!ctx || !f || !bc) return fail(ctx, NOVA_E_INVALID, "nova_field_set_bc: null argument");
+    for (int q = 0; q < 6 * (f->nc < 3 ? f->nc : 3); q++) {
+        const int face = q % 6;
+        const int axis = (face == NOVA_EAST || face == NOVA_WEST) ? 0 : (face == NOVA_TOP || face == NOVA_BOTTOM) ? 2 : 1;
+        const int t = bc->type[q];
+        if (t != NOVA_BC_PERIODIC && t != NOVA_BC_NEUMANN && t != NOVA_BC_DIRICHLET)
+            return fail(ctx, NOVA_E_INVALID, "nova_field_set_bc: unknown BC type");
+        const bool wall_axis = ctx->md.walls[axis] != 0;
+        if (wall_axis == (t == NOVA_BC_PERIODIC))
+            return fail(ctx, NOVA_E_INVALID, "nova_field_set_bc: periodic faces on periodic axes, "
+                                             "Neumann/Dirichlet faces on wall axes");
+    }
+    f->bc = *bc;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_field_get_bc(nova_ctx *ctx, const nova_field *f, nova_bc *bc)
+{
+    if (!ctx || !f || !bc) return fail(ctx, NOVA_E_INVALID, "nova_field_get_bc: null argument");
+    *bc = f->bc;
     return NOVA_OK;
 }
 
@@ -510,13 +610,16 @@ extern "C" nova_status nova_field_download(nova_ctx *ctx, const nova_field *f, d
     if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_download: null argument");
     nova_status s = check_local_n(ctx, local_n);
     if (s != NOVA_OK) return s;
-    if (bc)
-        for (int q = 0; q < 6 * f->nc && q < 18; q++)
-            if (bc->type[q] != NOVA_BC_PERIODIC)
-                return fail(ctx, NOVA_E_UNSUPPORTED, "nova_field_download: only periodic ghost fills are built");
+    nova_field tmp = *f;  // ghosts from the given BCs, or the field's own
+    if (bc) {
+        nova_field probe = *f;
+        if ((s = nova_field_set_bc(ctx, &probe, bc)) != NOVA_OK) return s;
+        tmp.bc = *bc;
+    }
     const size_t n = (size_t)local_n[0] * local_n[1] * local_n[2] * f->nc;
     if ((s = ensure_stage(ctx, n)) != NOVA_OK) return s;
-    launch_soa_to_aos(ctx->g, ctx->h, ctx->local_n, f->nc, f->d64, f->hi, f->lo, ctx->d_stage, ctx->stream);
+    launch_soa_to_aos(ctx->g, walls_of<double>(ctx, &tmp), ctx->h, ctx->local_n, f->nc, f->d64, f->hi, f->lo,
+                      ctx->d_stage, ctx->stream);
     ctx->launches += 1;
     CKL("k_soa_to_aos");
     CK(cudaMemcpyAsync(host, ctx->d_stage, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -596,8 +699,9 @@ static nova_status op_common(nova_ctx *ctx, int op, const nova_field *a, const n
     if (a->prec != NOVA_F64 || out->prec != NOVA_F64 || (b && b->prec != NOVA_F64))
         return fail(ctx, NOVA_E_UNSUPPORTED, "operator: the ex:: entry points take FP64 fields");
     if (a == out || (b && b == out)) return fail(ctx, NOVA_E_INVALID, "operator: output aliases an input");
-    launch_op(op, ctx->h, ctx->g, ctx->co64, ctx->d_ia64, ctx->d_corr64, a->d64, b ? b->d64 : nullptr,
-              (op == OP_DIV_VF) ? b->nc : a->nc, nu, out->d64, ctx->stream);
+    launch_op(op, ctx->h, ctx->g, walls_of<double>(ctx, a), walls_of<double>(ctx, b), ctx->co64, ctx->d_ia64,
+              ctx->d_corr64, a->d64, b ? b->d64 : nullptr, (op == OP_DIV_VF) ? b->nc : a->nc, nu, out->d64,
+              ctx->stream);
     ctx->launches += 1;
     CKL("operator kernel");
     CK(cudaStreamSynchronize(ctx->stream));
@@ -684,18 +788,33 @@ nova_status ensure_work(nova_ctx *ctx, int prec)
 }
 
 // One RK4 (or literal) sweep of an evolved field Y with the frozen field X,
-// followed by its projection.  Y is updated in place.
+// followed by its projection.  Y is updated in place.  With walls, the
+// wall-node overwrites land where the reference calls correctBoundaryConditions:
+// on every refreshed stage state (CLASSICAL: U = Ustar; U.correctBC), on U*
+// before the projection, on p after the solve and on U after the correction.
 nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field *Y, const nova_field *X,
                    nova_field *p, double visc, double divisor, double corr_scale)
 {
     const Geo &g = ctx->g;
     cudaStream_t st = ctx->stream;
     const bool lit = rd->rk_mode == NOVA_RK_LITERAL;
+    const bool str = ctx->md.hyperbolic_z != 0;
+    const bool walls = g.wallY != 0;
+    const WallFix yfix = wall_fix_of(ctx, Y), pfix = wall_fix_of(ctx, p);
+    const Walls<double> yw64 = walls_of<double>(ctx, Y), pw64 = walls_of<double>(ctx, p);
+    auto fix64 = [&](double *f) {
+        if (walls) {
+            launch_wall_fix64(g, yfix, f, st);
+            ctx->launches += 1;
+        }
+    };
     if (Y->prec == NOVA_F64) {
+        const Walls<double> sw = walls_of<double>(ctx, Y, X);
+        fix64(Y->d64);
         double *Ustar;
         auto run64 = [&](int stage, const StageArgs64 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
-            launch_stage64(phys, stage, ctx->md.hyperbolic_z != 0, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc, a, st);
+            launch_stage64(phys, stage, str, g, sw, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc, a, st);
             ctx->launches += 1;
         };
         if (lit) {
@@ -705,63 +824,97 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             double *w0 = ctx->w64[0], *w1 = ctx->w64[1], *A = ctx->w64[2];
             const double *Xp = X ? X->d64 : nullptr;
             run64(0, StageArgs64{Y->d64, Xp, nullptr, A, w0});
+            fix64(w0);
             run64(1, StageArgs64{w0, Xp, Y->d64, A, w1});
+            fix64(w1);
             run64(2, StageArgs64{w1, Xp, Y->d64, A, w0});
+            fix64(w0);
             run64(3, StageArgs64{w0, Xp, nullptr, A, Y->d64});
             Ustar = Y->d64;
         }
+        fix64(Ustar);
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
-            launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, Ustar, nullptr, nullptr, divisor, ctx->d_rhs, st);
+            launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, Ustar, nullptr, nullptr, divisor, ctx->d_rhs, st);
             ctx->launches += 1;
         }
         CKL("k_div_tiled");
         nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
         if (s != NOVA_OK) return s;
-        {
-            ProfScope ps(ctx, NOVA_K_CORRECT);
-            launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, p->d64, corr_scale, Ustar, Y->d64, nullptr, nullptr,
-                           nullptr, nullptr, st);
+        if (walls) {
+            launch_wall_fix64(g, pfix, p->d64, st);
             ctx->launches += 1;
         }
+        {
+            ProfScope ps(ctx, NOVA_K_CORRECT);
+            launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, Ustar, Y->d64, nullptr,
+                           nullptr, nullptr, nullptr, st);
+            ctx->launches += 1;
+        }
+        fix64(Y->d64);
         CKL("k_correct_tiled");
     } else {
+        const Walls<float> sw = walls_of<float>(ctx, Y, X);
+        auto fix32 = [&](float *f) {
+            if (walls) {
+                launch_wall_fix32(g, yfix, f, st);
+                ctx->launches += 1;
+            }
+        };
+        auto fixpair = [&](float *hi, float *lo) {
+            if (walls) {
+                launch_wall_fix_split(g, yfix, hi, lo, st);
+                ctx->launches += 1;
+            }
+        };
+        fixpair(Y->hi, Y->lo);
         const float *Ushi, *Uslo;
         auto run32 = [&](int stage, const StageArgs32 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
-            launch_stage32(phys, stage, ctx->md.hyperbolic_z != 0, g, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt, (float)visc, a, st);
+            launch_stage32(phys, stage, str, g, sw, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt, (float)visc,
+                           a, st);
             ctx->launches += 1;
         };
         const float *Xp = X ? X->hi : nullptr;
         if (lit) {
             run32(4, StageArgs32{Y->hi, Xp, nullptr, Y->lo, nullptr, nullptr, ctx->w32[0], ctx->w32[1]});
+            fixpair(ctx->w32[0], ctx->w32[1]);
             Ushi = ctx->w32[0];
             Uslo = ctx->w32[1];
         } else {
             float *w0 = ctx->w32[0], *w1 = ctx->w32[1], *A = ctx->w32[2];
             run32(0, StageArgs32{Y->hi, Xp, nullptr, nullptr, A, w0, nullptr, nullptr});
+            fix32(w0);
             run32(1, StageArgs32{w0, Xp, Y->hi, nullptr, A, w1, nullptr, nullptr});
+            fix32(w1);
             run32(2, StageArgs32{w1, Xp, Y->hi, nullptr, A, w0, nullptr, nullptr});
+            fix32(w0);
             run32(3, StageArgs32{w0, Xp, Y->hi, Y->lo, A, nullptr, Y->hi, Y->lo});
+            fixpair(Y->hi, Y->lo);
             Ushi = Y->hi;
             Uslo = Y->lo;
         }
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
-            launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo, divisor, ctx->d_rhs, st);
+            launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo, divisor, ctx->d_rhs, st);
             ctx->launches += 1;
         }
         CKL("k_div_tiled");
         nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
         if (s != NOVA_OK) return s;
-        {
-            ProfScope ps(ctx, NOVA_K_CORRECT);
-            launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, p->d64, corr_scale, nullptr, nullptr, Ushi, Uslo, Y->hi,
-                           Y->lo, st);
+        if (walls) {
+            launch_wall_fix64(g, pfix, p->d64, st);
             ctx->launches += 1;
         }
+        {
+            ProfScope ps(ctx, NOVA_K_CORRECT);
+            launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, nullptr, nullptr, Ushi, Uslo,
+                           Y->hi, Y->lo, st);
+            ctx->launches += 1;
+        }
+        fixpair(Y->hi, Y->lo);
         CKL("k_correct_tiled");
     }
     return NOVA_OK;
@@ -810,7 +963,8 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
         if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps)) {
             ProfScope ps(ctx, NOVA_K_DIAG);
             const nova_field *U = st->U, *B = mhd ? st->B : nullptr;
-            launch_diag(ctx->h, ctx->g, ctx->co64, ctx->d_ia64, U->d64, U->hi, U->lo, B ? B->d64 : nullptr,
+            launch_diag(ctx->h, ctx->g, walls_of<double>(ctx, U, B), ctx->co64, ctx->d_ia64, U->d64, U->hi, U->lo,
+                        B ? B->d64 : nullptr,
                         B ? B->hi : nullptr, B ? B->lo : nullptr, mhd ? 1 : 0, ctx->d_part, (double)(n + 1),
                         rd->t0 + (n + 1) * rd->dt, ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag,
                         ctx->stream);
@@ -843,7 +997,8 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
     const bool str = ctx->md.hyperbolic_z != 0;
     auto run = [&](int stage, const StageArgs64 &a) {
         ProfScope ps(ctx, NOVA_K_STAGE);
-        launch_stage64(PHYS_NS, stage, str, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, rd->nu, a, st);
+        launch_stage64(PHYS_NS, stage, str, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, rd->nu,
+                       a, st);
         ctx->launches += 1;
     };
     run(0, StageArgs64{Uin, nullptr, nullptr, A, Y2});
@@ -855,13 +1010,14 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
     }
     run(3, StageArgs64{Y4, nullptr, nullptr, A, Uout});
     CKL("stage kernel");
-    launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt, ctx->d_rhs, st);
+    launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt, ctx->d_rhs,
+                    st);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, ctx->w64[1]);
     if (s != NOVA_OK) return s;
-    launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, ctx->w64[1], rd->dt, Uout, Uout, nullptr, nullptr, nullptr,
-                   nullptr, st);
+    launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->w64[1], rd->dt, Uout, Uout, nullptr,
+                   nullptr, nullptr, nullptr, st);
     ctx->launches += 1;
     CKL("k_correct_tiled");
     return NOVA_OK;
@@ -871,13 +1027,14 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
 nova_status project64(nova_ctx *ctx, const double *in, double *out, double *pbuf)
 {
     const Geo &g = ctx->g;
-    launch_div_proj(ctx->h, g, ctx->co64, ctx->d_ia64, in, nullptr, nullptr, 1.0, ctx->d_rhs, ctx->stream);
+    launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, in, nullptr, nullptr, 1.0, ctx->d_rhs,
+                    ctx->stream);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, pbuf);
     if (s != NOVA_OK) return s;
-    launch_correct(ctx->h, g, ctx->co64, ctx->d_ia64, pbuf, 1.0, in, out, nullptr, nullptr, nullptr, nullptr,
-                   ctx->stream);
+    launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, 1.0, in, out, nullptr, nullptr, nullptr,
+                   nullptr, ctx->stream);
     ctx->launches += 1;
     CKL("k_correct_tiled");
     return NOVA_OK;
@@ -894,6 +1051,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: built for FP64 Navier-Stokes, classical RK4");
     if (ad->objective != NOVA_OBJ_EKIN_FINAL) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: objective");
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: the fused kernels are built for m = 6");
+    if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: periodic meshes only");
     if (ad->nsteps < 1 || ad->checkpoint_every < 1 || !(rd->dt > 0.0))
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: nsteps, checkpoint_every and dt must be positive");
     if (!valid_field(init->U, 3) || init->U->prec != NOVA_F64 || !valid_field(gradU, 3) || gradU->prec != NOVA_F64)
@@ -932,7 +1090,8 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     }
     // J = mean 1/2 |U_N|^2 and lambda_N = U_N / N^3
     if ((s = dalloc(ctx, &ctx->d_row, NOVA_HIST_COLS)) != NOVA_OK) return s;
-    launch_diag(ctx->h, ctx->g, ctx->co64, ctx->d_ia64, mu, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
+    launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, mu, nullptr, nullptr, nullptr, nullptr,
+                nullptr, 0,
                 ctx->d_part, (double)N, N * rd->dt, ctx->d_row, ctx->d_flag, st);
     ctx->launches += 2;
     double row[NOVA_HIST_COLS];

@@ -16,9 +16,24 @@ constexpr int kTK = 32;   // tile extent along k (one warp, coalesced)
 constexpr int kTJ = 8;    // tile extent along j
 constexpr int kThreads = kTK * kTJ;
 
+// N1 is the number of stored y nodes: N[1] when y is periodic, N[1] + 1 when
+// y is bounded by walls (both wall nodes stored, as in the reference's
+// interior range [m/2, n - m/2)).
 struct Geo {
     int N0, N1, N2;
     long long N12, N3;
+    int wallY;
+};
+
+// Ghosts beyond the y walls of the halo'd components (src/BC/neumannBC.hxx,
+// src/BC/dirichletBC.hxx): ghost(l) = sgn * f(mirror l) + off * l, with
+//   Neumann:   sgn = +1, off = -2 val dy    (both faces, as the reference writes it)
+//   Dirichlet: sgn = -1, off = +2 val
+// side 0 = south face (j = 0), side 1 = north face (j = N1 - 1).
+template <typename T> struct Walls {
+    int on;
+    T sgn[2][9];
+    T off[2][9];
 };
 
 // First/second-derivative weights of src/settings/settings.cpp:25-31 for half
@@ -126,9 +141,10 @@ void launch_scale_copy(long long n, double a, const double *x, double *y, cudaSt
 // stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum)
 // stretch: apply the stretched-z Laplacian term (Mesh "hypz:"); on uniform
 // meshes d2zdxi2 is round-off (|.| < 1e-9) and the term is skipped
-void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
-                    const double *corr2, double dt, double visc, const StageArgs64 &a, cudaStream_t st);
-void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
-                    const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st);
+void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl, const Coef<double> &co,
+                    const double *ia, const double *corr2, double dt, double visc, const StageArgs64 &a,
+                    cudaStream_t st);
+void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl, const Coef<float> &co,
+                    const float *ia, const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st);
 
 }  // namespace nova

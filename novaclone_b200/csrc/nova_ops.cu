@@ -18,29 +18,43 @@ namespace nova {
 
 namespace {
 
-// value of component array f at (i,j,k) shifted by s along direction d, periodic
-template <typename P>
-__device__ __forceinline__ double at(const P &f, const Geo &g, int c, int i, int j, int k, int d, int s)
-{
-    if (d == 0) i = wrapi(i + s, g.N0);
-    else if (d == 1) j = wrapi(j + s, g.N1);
-    else k = wrapi(k + s, g.N2);
-    return f(c, (long long)i * g.N12 + (long long)j * g.N2 + k);
-}
-
 struct Ld64 {
     const double *p;
     long long n3;
+    Walls<double> wl;  // y-wall ghosts of this field (wl.on = 0: periodic)
     __device__ double operator()(int c, long long o) const { return p[(long long)c * n3 + o]; }
 };
 struct LdSplit {
     const float *hi, *lo;
     long long n3;
+    Walls<double> wl;
     __device__ double operator()(int c, long long o) const
     {
         return (double)hi[(long long)c * n3 + o] + (double)lo[(long long)c * n3 + o];
     }
 };
+
+// value of component c of f at (i,j,k) shifted by s along direction d:
+// periodic axes wrap, y walls mirror with the field's ghost formulas
+template <typename P>
+__device__ __forceinline__ double at(const P &f, const Geo &g, int c, int i, int j, int k, int d, int s)
+{
+    if (d == 0) {
+        i = wrapi(i + s, g.N0);
+    } else if (d == 2) {
+        k = wrapi(k + s, g.N2);
+    } else {
+        const int jj = j + s;
+        if (f.wl.on && (jj < 0 || jj >= g.N1)) {
+            const int side = jj < 0 ? 0 : 1;
+            const int l = side == 0 ? -jj : jj - (g.N1 - 1);
+            const int jm = side == 0 ? l : (g.N1 - 1) - l;
+            return f.wl.sgn[side][c] * f(c, (long long)i * g.N12 + (long long)jm * g.N2 + k) + f.wl.off[side][c] * l;
+        }
+        j = f.wl.on ? jj : wrapi(jj, g.N1);
+    }
+    return f(c, (long long)i * g.N12 + (long long)j * g.N2 + k);
+}
 
 __device__ __forceinline__ void pt_index(const Geo &g, long long t, int &i, int &j, int &k)
 {
@@ -60,17 +74,17 @@ __device__ __forceinline__ double dd1(const P &f, const Geo &g, int c, int i, in
     return r;
 }
 
-__global__ void k_scale(Geo g, cuDoubleComplex *__restrict__ spec, const double *__restrict__ kx2,
+__global__ void k_scale(Geo g, int ny, cuDoubleComplex *__restrict__ spec, const double *__restrict__ kx2,
                         const double *__restrict__ ky2, const double *__restrict__ kz2, double invN3)
 {
     const int nzh = g.N2 / 2 + 1;
-    const long long tot = (long long)g.N0 * g.N1 * nzh;
+    const long long tot = (long long)g.N0 * ny * nzh;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= tot) return;
     const int kz = (int)(t % nzh);
     const long long r = t / nzh;
-    const int j = (int)(r % g.N1);
-    const int i = (int)(r / g.N1);
+    const int j = (int)(r % ny);
+    const int i = (int)(r / ny);
     const double k2 = (kx2[i] + ky2[j]) + kz2[kz];
     cuDoubleComplex v = spec[t];
     if (k2 < 1.0e-16) {
@@ -95,17 +109,19 @@ __global__ void __launch_bounds__(kThreads) k_div_tiled(Geo g, Coef<double> co, 
     double az[H];
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
-    tile_march<double, H, 3>(g, sm, U, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy, const auto &vz) {
+    tile_march<double, H, 3>(g, U.wl, sm, U, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy,
+                                                          const auto &vz) {
         const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
         rhs[idx] = d / divisor;
     });
 }
 
 template <int H, bool SPLIT>
-__global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Coef<double> co, const double *__restrict__ ia,
-                                                            const double *__restrict__ p, double s, const double *Us64,
-                                                            double *U64, const float *Ushi, const float *Uslo,
-                                                            float *hi, float *lo, int ichunk)
+__global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Walls<double> pw, Coef<double> co,
+                                                            const double *__restrict__ ia, const double *__restrict__ p,
+                                                            double s, const double *Us64, double *U64,
+                                                            const float *Ushi, const float *Uslo, float *hi, float *lo,
+                                                            int ichunk)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     auto &sm = *reinterpret_cast<TileSmem<double, H, 1> *>(smraw);
@@ -116,7 +132,8 @@ __global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Coef<double> 
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
     auto ld = [&](int, long long o) { return p[o]; };
-    tile_march<double, H, 1>(g, sm, ld, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy, const auto &vz) {
+    tile_march<double, H, 1>(g, pw, sm, ld, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy,
+                                                          const auto &vz) {
         double us[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -173,41 +190,69 @@ __device__ __forceinline__ T block_reduce_max(T v, T *sh)
 }
 
 // per-block partials: [0] sum 1/2|U|^2, [1] sum 1/2|B|^2, [2] max|div U|, [3] max|div B|
-template <int H, class LD>
-__global__ void k_diag(Geo g, Coef<double> co, const double *__restrict__ ia, LD U, LD B, int hasB,
-                       double *__restrict__ part)
+// Energies sum the unique nodes as app/TG_Piosson/TG.cpp:148-166 does (the
+// stored north-wall row is the reference's last node and is skipped); the
+// divergence maxima cover every stored node (tools::maximum, src/Tools/Tools.h:19-36).
+template <int H, int NC, class LD>
+__global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl, Coef<double> co,
+                                                         const double *__restrict__ ia, LD U, LD B, int ichunk,
+                                                         double *__restrict__ part)
 {
-    __shared__ double sh[32];
-    double ek = 0.0, em = 0.0, mdu = 0.0, mdb = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.N3;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        pt_index(g, t, i, j, k);
-        double az[H];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    auto &sm = *reinterpret_cast<TileSmem<double, H, NC> *>(smraw);
+    __shared__ double red[4][kThreads / 32];
+    const int ib = blockIdx.z * ichunk;
+    const int ie = min(ib + ichunk, g.N0);
+    const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
+    double az[H];
 #pragma unroll
-        for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
-        const double u = U(0, t), v = U(1, t), w = U(2, t);
-        ek += 0.5 * (u * u + v * v + w * w);
-        const double du = dd1<H>(U, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(U, g, 1, i, j, k, 1, co.a[1])
-                          + dd1<H>(U, g, 2, i, j, k, 2, az);
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
+    const int rows_e = g.N1 - g.wallY;
+    double ek = 0.0, em = 0.0, mdu = 0.0, mdb = 0.0;
+    auto ld = [&](int c, long long o) -> double { return c < 3 ? U(c, o) : B(c - 3, o); };
+    tile_march<double, H, NC>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
+                                                          const auto &vz) {
+        const int j = (int)((idx % g.N12) / g.N2);
+        const bool ce = j < rows_e;
+        const double u = q[H][0], v = q[H][1], w = q[H][2];
+        if (ce) ek += 0.5 * (u * u + v * v + w * w);
+        const double du = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
         mdu = fmax(mdu, fabs(du));
-        if (hasB) {
-            const double bx = B(0, t), by = B(1, t), bz = B(2, t);
-            em += 0.5 * (bx * bx + by * by + bz * bz);
-            const double db = dd1<H>(B, g, 0, i, j, k, 0, co.a[0]) + dd1<H>(B, g, 1, i, j, k, 1, co.a[1])
-                              + dd1<H>(B, g, 2, i, j, k, 2, az);
+        if constexpr (NC == 6) {
+            const double bx = q[H][3], by = q[H][4], bz = q[H][5];
+            if (ce) em += 0.5 * (bx * bx + by * by + bz * bz);
+            const double db = d1<double, H>(vx, 3, co.a[0]) + d1<double, H>(vy, 4, co.a[1]) + d1<double, H>(vz, 5, az);
             mdb = fmax(mdb, fabs(db));
         }
+    });
+    const int tid = threadIdx.y * kTK + threadIdx.x, lane = tid & 31, w = tid >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ek += __shfl_down_sync(0xffffffffu, ek, o);
+        em += __shfl_down_sync(0xffffffffu, em, o);
+        mdu = fmax(mdu, __shfl_down_sync(0xffffffffu, mdu, o));
+        mdb = fmax(mdb, __shfl_down_sync(0xffffffffu, mdb, o));
     }
-    const double s0 = block_reduce_sum(ek, sh);
-    const double s1 = block_reduce_sum(em, sh);
-    const double s2 = block_reduce_max(mdu, sh);
-    const double s3 = block_reduce_max(mdb, sh);
-    if (threadIdx.x == 0) {
-        part[blockIdx.x * 4 + 0] = s0;
-        part[blockIdx.x * 4 + 1] = s1;
-        part[blockIdx.x * 4 + 2] = s2;
-        part[blockIdx.x * 4 + 3] = s3;
+    if (lane == 0) {
+        red[0][w] = ek;
+        red[1][w] = em;
+        red[2][w] = mdu;
+        red[3][w] = mdb;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int q = 0; q < kThreads / 32; q++) {
+            a0 += red[0][q];
+            a1 += red[1][q];
+            a2 = fmax(a2, red[2][q]);
+            a3 = fmax(a3, red[3][q]);
+        }
+        const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        part[blk * 4 + 0] = a0;
+        part[blk * 4 + 1] = a1;
+        part[blk * 4 + 2] = a2;
+        part[blk * 4 + 3] = a3;
     }
 }
 
@@ -261,14 +306,14 @@ __global__ void k_max_final(const double *__restrict__ part, int n, double *__re
 // Simple one-thread-per-node kernels for the drop-in ex:: entry points.
 
 template <int H>
-__global__ void k_op_grad_s(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ s,
+__global__ void k_op_grad_s(Geo g, Walls<double> wa, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ s,
                             double *__restrict__ out)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= g.N3) return;
     int i, j, k;
     pt_index(g, t, i, j, k);
-    Ld64 S{s, g.N3};
+    Ld64 S{s, g.N3, wa};
     double az[H];
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
@@ -279,14 +324,14 @@ __global__ void k_op_grad_s(Geo g, Coef<double> co, const double *__restrict__ i
 
 // ex::grad(Field<vector>) keeps the reference's stencil c_l/(l+1)/delta*(f(+l) - f(-1-l)) (grad.cpp:82-94)
 template <int H>
-__global__ void k_op_grad_v(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+__global__ void k_op_grad_v(Geo g, Walls<double> wa, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
                             double *__restrict__ out)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= g.N3) return;
     int i, j, k;
     pt_index(g, t, i, j, k);
-    Ld64 F{U, g.N3};
+    Ld64 F{U, g.N3, wa};
 #pragma unroll
     for (int c = 0; c < 3; c++)
 #pragma unroll
@@ -304,14 +349,14 @@ __global__ void k_op_grad_v(Geo g, Coef<double> co, const double *__restrict__ i
 
 // ex::curl = antisymmetric part of ex::grad(vector) (src/ex/curl/curl.cpp:44-50)
 template <int H>
-__global__ void k_op_curl(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+__global__ void k_op_curl(Geo g, Walls<double> wa, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
                           double *__restrict__ out)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= g.N3) return;
     int i, j, k;
     pt_index(g, t, i, j, k);
-    Ld64 F{U, g.N3};
+    Ld64 F{U, g.N3, wa};
     auto gv = [&](int c, int d) {
         double r = 0.0;
 #pragma unroll
@@ -328,14 +373,14 @@ __global__ void k_op_curl(Geo g, Coef<double> co, const double *__restrict__ ia,
 }
 
 template <int H>
-__global__ void k_op_div_v(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+__global__ void k_op_div_v(Geo g, Walls<double> wa, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
                            double *__restrict__ out)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= g.N3) return;
     int i, j, k;
     pt_index(g, t, i, j, k);
-    Ld64 F{U, g.N3};
+    Ld64 F{U, g.N3, wa};
     double az[H];
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
@@ -345,14 +390,14 @@ __global__ void k_op_div_v(Geo g, Coef<double> co, const double *__restrict__ ia
 
 // skew div(U, f), f with nc components (src/ex/div/div.hxx:84-172)
 template <int H>
-__global__ void k_op_div_vf(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
+__global__ void k_op_div_vf(Geo g, Walls<double> wa, Walls<double> wb, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ U,
                             const double *__restrict__ f, int nc, double *__restrict__ out)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= g.N3) return;
     int i, j, k;
     pt_index(g, t, i, j, k);
-    Ld64 V{U, g.N3}, F{f, g.N3};
+    Ld64 V{U, g.N3, wa}, F{f, g.N3, wb};
     double a[3][H];
 #pragma unroll
     for (int l = 0; l < H; l++) {
@@ -383,14 +428,14 @@ __global__ void k_op_div_vf(Geo g, Coef<double> co, const double *__restrict__ i
 
 // laplacian(nu, f) with the stretched-z term (src/ex/laplacian/laplacian.hxx:130-191)
 template <int H>
-__global__ void k_op_lap(Geo g, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ corr2,
+__global__ void k_op_lap(Geo g, Walls<double> wa, Coef<double> co, const double *__restrict__ ia, const double *__restrict__ corr2,
                          double nu, const double *__restrict__ f, int nc, double *__restrict__ out)
 {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= g.N3) return;
     int i, j, k;
     pt_index(g, t, i, j, k);
-    Ld64 F{f, g.N3};
+    Ld64 F{f, g.N3, wa};
     const double i2 = ia[k] * ia[k];
     for (int c = 0; c < nc; c++) {
         const double f0 = F(c, t);
@@ -436,8 +481,9 @@ __global__ void k_aos_to_soa(Geo g, int h, int n1, int n2, int nc, const double 
 
 // unique SoA -> ghosted AoS with every slot filled by periodic wrap
 // (interior incl. the duplicate node as periodicBC::update leaves it)
-__global__ void k_soa_to_aos(Geo g, int h, int n0, int n1, int n2, int nc, const double *__restrict__ d64,
-                             const float *__restrict__ hi, const float *__restrict__ lo, double *__restrict__ aos)
+__global__ void k_soa_to_aos(Geo g, Walls<double> wl, int h, int n0, int n1, int n2, int nc,
+                             const double *__restrict__ d64, const float *__restrict__ hi,
+                             const float *__restrict__ lo, double *__restrict__ aos)
 {
     const long long tot = (long long)n0 * n1 * n2;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -446,12 +492,67 @@ __global__ void k_soa_to_aos(Geo g, int h, int n0, int n1, int n2, int nc, const
     const long long r = t / n2;
     const int jj = (int)(r % n1);
     const int ii = (int)(r / n1);
-    const long long s = (long long)wrapi(ii - h, g.N0) * g.N12 + (long long)wrapi(jj - h, g.N1) * g.N2
-                        + wrapi(kk - h, g.N2);
+    int j = jj - h, side = -1, l = 0;
+    if (wl.on) {
+        if (j < 0) {
+            side = 0;
+            l = min(-j, g.N1 - 1);
+            j = l;
+        } else if (j >= g.N1) {
+            side = 1;
+            l = min(j - (g.N1 - 1), g.N1 - 1);
+            j = (g.N1 - 1) - l;
+        }
+    } else {
+        j = wrapi(j, g.N1);
+    }
+    const long long s = (long long)wrapi(ii - h, g.N0) * g.N12 + (long long)j * g.N2 + wrapi(kk - h, g.N2);
     for (int c = 0; c < nc; c++) {
         const long long o = (long long)c * g.N3 + s;
-        aos[t * nc + c] = d64 ? d64[o] : (double)hi[o] + (double)lo[o];
+        const double v = d64 ? d64[o] : (double)hi[o] + (double)lo[o];
+        aos[t * nc + c] = side < 0 ? v : wl.sgn[side][c] * v + wl.off[side][c] * l;
     }
+}
+
+// Wall-node overwrite of neumannBC / dirichletBC::update (src/BC/neumannBC.hxx:8-26,
+// src/BC/dirichletBC.hxx:8-24): south f(0) = f(1) - val dy | val, north
+// f(N1-1) = f(N1-2) + val dy | val, per component.
+template <typename T>
+__global__ void k_wall_fix(Geo g, WallFix wf, T *__restrict__ f, float *__restrict__ lo)
+{
+    const long long plane = (long long)g.N0 * g.N2;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= plane * wf.nc) return;
+    const int c = (int)(t / plane);
+    const long long r = t % plane;
+    const int i = (int)(r / g.N2), k = (int)(r % g.N2);
+    const long long base = (long long)c * g.N3 + (long long)i * g.N12 + k;
+    auto get = [&](int j) -> double {
+        const long long o = base + (long long)j * g.N2;
+        return lo ? (double)f[o] + (double)lo[o] : (double)f[o];
+    };
+    auto put = [&](int j, double x) {
+        const long long o = base + (long long)j * g.N2;
+        if (lo) {
+            const float h = (float)x;
+            f[o] = (T)h;
+            lo[o] = (float)(x - (double)h);
+        } else {
+            f[o] = (T)x;
+        }
+    };
+    // north face (bc index 0) is applied before south (1), as correctBoundaryConditions orders them
+    const int jn = g.N1 - 1;
+    if (wf.type[1][c] == 1)
+        put(jn, sizeof(T) == 4 && !lo ? (double)((float)get(jn - 1) + (float)(wf.val[1][c] * wf.dy))
+                                      : get(jn - 1) + wf.val[1][c] * wf.dy);
+    else if (wf.type[1][c] == 2)
+        put(jn, wf.val[1][c]);
+    if (wf.type[0][c] == 1)
+        put(0, sizeof(T) == 4 && !lo ? (double)((float)get(1) - (float)(wf.val[0][c] * wf.dy))
+                                     : get(1) - wf.val[0][c] * wf.dy);
+    else if (wf.type[0][c] == 2)
+        put(0, wf.val[0][c]);
 }
 
 __global__ void k_split(long long n, const double *__restrict__ x, float *__restrict__ hi, float *__restrict__ lo)
@@ -484,70 +585,103 @@ inline unsigned nblocks(long long n, int b) { return (unsigned)((n + b - 1) / b)
     default: { constexpr int HH = 4; __VA_ARGS__; } break; \
     }
 
-void launch_div_proj(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64,
-                     const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st)
+void launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
+                     const double *U64, const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st)
 {
     const int ch = pick_ichunk(g, 3);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     if (U64) {
         NOVA_DISPATCH_H(h, {
             constexpr size_t sb = tile_smem_bytes<double, HH, 3>();
-            k_div_tiled<HH, Ld64><<<grid, block, sb, st>>>(g, co, ia, Ld64{U64, g.N3}, divisor, rhs, ch);
+            k_div_tiled<HH, Ld64><<<grid, block, sb, st>>>(g, co, ia, Ld64{U64, g.N3, wl}, divisor, rhs, ch);
         });
     } else {
         NOVA_DISPATCH_H(h, {
             constexpr size_t sb = tile_smem_bytes<double, HH, 3>();
-            k_div_tiled<HH, LdSplit><<<grid, block, sb, st>>>(g, co, ia, LdSplit{hi, lo, g.N3}, divisor, rhs, ch);
+            k_div_tiled<HH, LdSplit><<<grid, block, sb, st>>>(g, co, ia, LdSplit{hi, lo, g.N3, wl}, divisor, rhs, ch);
         });
     }
 }
 
-void launch_scale(const Geo &g, void *spec, const double *kx2, const double *ky2, const double *kz2, double invN3,
-                  cudaStream_t st)
+void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const double *ky2, const double *kz2,
+                  double invN3, cudaStream_t st)
 {
-    const long long tot = (long long)g.N0 * g.N1 * (g.N2 / 2 + 1);
-    k_scale<<<nblocks(tot, 256), 256, 0, st>>>(g, (cuDoubleComplex *)spec, kx2, ky2, kz2, invN3);
+    const long long tot = (long long)g.N0 * ny * (g.N2 / 2 + 1);
+    k_scale<<<nblocks(tot, 256), 256, 0, st>>>(g, ny, (cuDoubleComplex *)spec, kx2, ky2, kz2, invN3);
 }
 
-void launch_correct(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,
-                    const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi, float *lo,
-                    cudaStream_t st)
+void launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
+                    const double *p, double s, const double *Us64, double *U64, const float *Ushi, const float *Uslo,
+                    float *hi, float *lo, cudaStream_t st)
 {
     const int ch = pick_ichunk(g, 4);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     if (U64) {
         NOVA_DISPATCH_H(h, {
             constexpr size_t sb = tile_smem_bytes<double, HH, 1>();
-            k_correct_tiled<HH, false><<<grid, block, sb, st>>>(g, co, ia, p, s, Us64, U64, nullptr, nullptr, nullptr,
-                                                                nullptr, ch);
+            k_correct_tiled<HH, false><<<grid, block, sb, st>>>(g, pw, co, ia, p, s, Us64, U64, nullptr, nullptr,
+                                                                nullptr, nullptr, ch);
         });
     } else {
         NOVA_DISPATCH_H(h, {
             constexpr size_t sb = tile_smem_bytes<double, HH, 1>();
-            k_correct_tiled<HH, true><<<grid, block, sb, st>>>(g, co, ia, p, s, nullptr, nullptr, Ushi, Uslo, hi, lo, ch);
+            k_correct_tiled<HH, true><<<grid, block, sb, st>>>(g, pw, co, ia, p, s, nullptr, nullptr, Ushi, Uslo, hi, lo,
+                                                               ch);
         });
     }
 }
 
 int diag_blocks(const Geo &g)
 {
-    long long b = (g.N3 + 255) / 256;
-    return (int)(b < 1184 ? b : 1184);
+    const dim3 gr = tile_grid(g, pick_ichunk(g, 2));
+    const long long tiled = (long long)gr.x * gr.y * gr.z;
+    return (int)(tiled > 1184 ? tiled : 1184);
 }
 
-void launch_diag(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *Uhi,
-                 const float *Ulo, const double *B64, const float *Bhi, const float *Blo, int hasB, double *part,
-                 double step, double time, double *row, int *flag, cudaStream_t st)
+void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
+                 const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
+                 const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,
+                 cudaStream_t st)
 {
-    const int nb = diag_blocks(g);
+    const int ch = pick_ichunk(g, 2);
+    const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
+    const int nb = (int)(grid.x * grid.y * grid.z);
     if (U64) {
-        Ld64 U{U64, g.N3}, B{hasB ? B64 : U64, g.N3};
-        NOVA_DISPATCH_H(h, (k_diag<HH, Ld64><<<nb, kRedThreads, 0, st>>>(g, co, ia, U, B, hasB, part)));
+        Ld64 U{U64, g.N3, wl}, B{hasB ? B64 : U64, g.N3, wl};
+        if (hasB) {
+            NOVA_DISPATCH_H(h, {
+                constexpr size_t sb = tile_smem_bytes<double, HH, 6>();
+                static bool attr = false;
+                if (!attr) {
+                    cudaFuncSetAttribute(k_diag_tiled<HH, 6, Ld64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+                    attr = true;
+                }
+                k_diag_tiled<HH, 6, Ld64><<<grid, block, sb, st>>>(g, wl, co, ia, U, B, ch, part);
+            });
+        } else {
+            NOVA_DISPATCH_H(h, (k_diag_tiled<HH, 3, Ld64><<<grid, block, tile_smem_bytes<double, HH, 3>(), st>>>(
+                                   g, wl, co, ia, U, B, ch, part)));
+        }
     } else {
-        LdSplit U{Uhi, Ulo, g.N3}, B{hasB ? Bhi : Uhi, hasB ? Blo : Ulo, g.N3};
-        NOVA_DISPATCH_H(h, (k_diag<HH, LdSplit><<<nb, kRedThreads, 0, st>>>(g, co, ia, U, B, hasB, part)));
+        LdSplit U{Uhi, Ulo, g.N3, wl}, B{hasB ? Bhi : Uhi, hasB ? Blo : Ulo, g.N3, wl};
+        if (hasB) {
+            NOVA_DISPATCH_H(h, {
+                constexpr size_t sb = tile_smem_bytes<double, HH, 6>();
+                static bool attr = false;
+                if (!attr) {
+                    cudaFuncSetAttribute(k_diag_tiled<HH, 6, LdSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sb);
+                    attr = true;
+                }
+                k_diag_tiled<HH, 6, LdSplit><<<grid, block, sb, st>>>(g, wl, co, ia, U, B, ch, part);
+            });
+        } else {
+            NOVA_DISPATCH_H(h, (k_diag_tiled<HH, 3, LdSplit><<<grid, block, tile_smem_bytes<double, HH, 3>(), st>>>(
+                                   g, wl, co, ia, U, B, ch, part)));
+        }
     }
-    k_diag_final<<<1, 256, 0, st>>>(part, nb, 1.0 / (double)g.N3, step, time, row, flag);
+    k_diag_final<<<1, 256, 0, st>>>(part, nb, 1.0 / (double)((long long)g.N0 * (g.N1 - g.wallY) * g.N2), step, time,
+                                    row, flag);
 }
 
 void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st)
@@ -557,17 +691,18 @@ void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cud
     k_max_final<<<1, 256, 0, st>>>(part, nb, out);
 }
 
-void launch_op(int op, int h, const Geo &g, const Coef<double> &co, const double *ia, const double *corr2,
-               const double *a, const double *b, int nc, double nu, double *out, cudaStream_t st)
+void launch_op(int op, int h, const Geo &g, const Walls<double> &wa, const Walls<double> &wb, const Coef<double> &co,
+               const double *ia, const double *corr2, const double *a, const double *b, int nc, double nu, double *out,
+               cudaStream_t st)
 {
     const unsigned nb = nblocks(g.N3, 128);
     switch (op) {
-    case OP_GRAD_S: NOVA_DISPATCH_H(h, (k_op_grad_s<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
-    case OP_GRAD_V: NOVA_DISPATCH_H(h, (k_op_grad_v<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
-    case OP_DIV_V: NOVA_DISPATCH_H(h, (k_op_div_v<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
-    case OP_CURL: NOVA_DISPATCH_H(h, (k_op_curl<HH><<<nb, 128, 0, st>>>(g, co, ia, a, out))); break;
-    case OP_DIV_VF: NOVA_DISPATCH_H(h, (k_op_div_vf<HH><<<nb, 128, 0, st>>>(g, co, ia, a, b, nc, out))); break;
-    default: NOVA_DISPATCH_H(h, (k_op_lap<HH><<<nb, 128, 0, st>>>(g, co, ia, corr2, nu, a, nc, out))); break;
+    case OP_GRAD_S: NOVA_DISPATCH_H(h, (k_op_grad_s<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, a, out))); break;
+    case OP_GRAD_V: NOVA_DISPATCH_H(h, (k_op_grad_v<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, a, out))); break;
+    case OP_DIV_V: NOVA_DISPATCH_H(h, (k_op_div_v<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, a, out))); break;
+    case OP_CURL: NOVA_DISPATCH_H(h, (k_op_curl<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, a, out))); break;
+    case OP_DIV_VF: NOVA_DISPATCH_H(h, (k_op_div_vf<HH><<<nb, 128, 0, st>>>(g, wa, wb, co, ia, a, b, nc, out))); break;
+    default: NOVA_DISPATCH_H(h, (k_op_lap<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, corr2, nu, a, nc, out))); break;
     }
 }
 
@@ -577,11 +712,26 @@ void launch_aos_to_soa(const Geo &g, int h, const int n[3], int nc, const double
     k_aos_to_soa<<<nblocks(g.N3, 256), 256, 0, st>>>(g, h, n[1], n[2], nc, aos, d64, hi, lo);
 }
 
-void launch_soa_to_aos(const Geo &g, int h, const int n[3], int nc, const double *d64, const float *hi,
-                       const float *lo, double *aos, cudaStream_t st)
+void launch_soa_to_aos(const Geo &g, const Walls<double> &wl, int h, const int n[3], int nc, const double *d64,
+                       const float *hi, const float *lo, double *aos, cudaStream_t st)
 {
     const long long tot = (long long)n[0] * n[1] * n[2];
-    k_soa_to_aos<<<nblocks(tot, 256), 256, 0, st>>>(g, h, n[0], n[1], n[2], nc, d64, hi, lo, aos);
+    k_soa_to_aos<<<nblocks(tot, 256), 256, 0, st>>>(g, wl, h, n[0], n[1], n[2], nc, d64, hi, lo, aos);
+}
+
+void launch_wall_fix64(const Geo &g, const WallFix &wf, double *f, cudaStream_t st)
+{
+    k_wall_fix<double><<<nblocks((long long)g.N0 * g.N2 * wf.nc, 256), 256, 0, st>>>(g, wf, f, nullptr);
+}
+
+void launch_wall_fix32(const Geo &g, const WallFix &wf, float *f, cudaStream_t st)
+{
+    k_wall_fix<float><<<nblocks((long long)g.N0 * g.N2 * wf.nc, 256), 256, 0, st>>>(g, wf, f, nullptr);
+}
+
+void launch_wall_fix_split(const Geo &g, const WallFix &wf, float *hi, float *lo, cudaStream_t st)
+{
+    k_wall_fix<float><<<nblocks((long long)g.N0 * g.N2 * wf.nc, 256), 256, 0, st>>>(g, wf, hi, lo);
 }
 
 void launch_split(long long n, const double *x, float *hi, float *lo, cudaStream_t st)

@@ -7,24 +7,38 @@ namespace nova {
 
 enum OpKind { OP_GRAD_S = 0, OP_GRAD_V = 1, OP_DIV_V = 2, OP_DIV_VF = 3, OP_LAP = 4, OP_CURL = 5 };
 
-void launch_div_proj(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64,
-                     const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st);
-void launch_scale(const Geo &g, void *spec, const double *kx2, const double *ky2, const double *kz2, double invN3,
-                  cudaStream_t st);
-void launch_correct(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,
-                    const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi, float *lo,
-                    cudaStream_t st);
+// wall-node overwrite per component: type 1 = Neumann, 2 = Dirichlet (0 = none)
+struct WallFix {
+    int on, nc;
+    double dy;
+    int type[2][9];   // [side: 0 south, 1 north][comp]
+    double val[2][9];
+};
+
+void launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
+                     const double *U64, const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st);
+// ny: y extent of the spectrum (the unique y nodes of the transform)
+void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const double *ky2, const double *kz2,
+                  double invN3, cudaStream_t st);
+void launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
+                    const double *p, double s, const double *Us64, double *U64, const float *Ushi, const float *Uslo,
+                    float *hi, float *lo, cudaStream_t st);
 int diag_blocks(const Geo &g);
-void launch_diag(int h, const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *Uhi,
-                 const float *Ulo, const double *B64, const float *Bhi, const float *Blo, int hasB, double *part,
-                 double step, double time, double *row, int *flag, cudaStream_t st);
+void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
+                 const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
+                 const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,
+                 cudaStream_t st);
 void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st);
-void launch_op(int op, int h, const Geo &g, const Coef<double> &co, const double *ia, const double *corr2,
-               const double *a, const double *b, int nc, double nu, double *out, cudaStream_t st);
+void launch_op(int op, int h, const Geo &g, const Walls<double> &wa, const Walls<double> &wb, const Coef<double> &co,
+               const double *ia, const double *corr2, const double *a, const double *b, int nc, double nu, double *out,
+               cudaStream_t st);
 void launch_aos_to_soa(const Geo &g, int h, const int n[3], int nc, const double *aos, double *d64, float *hi,
                        float *lo, cudaStream_t st);
-void launch_soa_to_aos(const Geo &g, int h, const int n[3], int nc, const double *d64, const float *hi,
-                       const float *lo, double *aos, cudaStream_t st);
+void launch_soa_to_aos(const Geo &g, const Walls<double> &wl, int h, const int n[3], int nc, const double *d64,
+                       const float *hi, const float *lo, double *aos, cudaStream_t st);
+void launch_wall_fix64(const Geo &g, const WallFix &wf, double *f, cudaStream_t st);
+void launch_wall_fix32(const Geo &g, const WallFix &wf, float *f, cudaStream_t st);
+void launch_wall_fix_split(const Geo &g, const WallFix &wf, float *hi, float *lo, cudaStream_t st);
 void launch_split(long long n, const double *x, float *hi, float *lo, cudaStream_t st);
 void launch_join(long long n, const float *hi, const float *lo, double *x, cudaStream_t st);
 

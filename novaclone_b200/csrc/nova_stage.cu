@@ -54,9 +54,9 @@ namespace nova {
 namespace {
 
 template <typename T, int H, int PHYS, int STAGE, bool STRETCH, class Args>
-__global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo g, Coef<T> co, const T *__restrict__ ia,
-                                                      const T *__restrict__ corr2, T dt, T visc, Args args,
-                                                      int ichunk)
+__global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo g, Walls<T> wl, Coef<T> co,
+                                                      const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
+                                                      T visc, Args args, int ichunk)
 {
     constexpr int NC = (PHYS == PHYS_NS) ? 3 : 6;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
     };
 
     tile_march<T, H, NC>(
-        g, sm, [&](int c, long long o) { return src[c][o]; }, ib, ie, pre,
+        g, wl, sm, [&](int c, long long o) { return src[c][o]; }, ib, ie, pre,
         [&](long long idx, auto &q, const auto &vx, const auto &vy, const auto &vz) {
             if constexpr (!kAhead) {
 #pragma unroll
@@ -254,8 +254,8 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
 constexpr int kH = 3;
 
 template <typename T, int PHYS, int STAGE, bool STRETCH, class Args>
-void launch_one(const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc, const Args &a,
-                cudaStream_t st)
+void launch_one(const Geo &g, const Walls<T> &wl, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
+                const Args &a, cudaStream_t st)
 {
     constexpr int NC = (PHYS == PHYS_NS) ? 3 : 6;
     constexpr size_t smem = tile_smem_bytes<T, kH, NC>();
@@ -267,53 +267,54 @@ void launch_one(const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T 
     }
     const int bps = stage_minb<T, PHYS>();
     const int ch = pick_ichunk(g, bps);
-    kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, corr2, dt, visc, a, ch);
+    kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, wl, co, ia, corr2, dt, visc, a, ch);
 }
 
 template <typename T, int PHYS, bool STRETCH, class Args>
-void launch_stage_t(int stage, const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
-                    const Args &a, cudaStream_t st)
+void launch_stage_t(int stage, const Geo &g, const Walls<T> &wl, const Coef<T> &co, const T *ia, const T *corr2, T dt,
+                    T visc, const Args &a, cudaStream_t st)
 {
     switch (stage) {
-    case 0: launch_one<T, PHYS, 0, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
-    case 1: launch_one<T, PHYS, 1, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
-    case 2: launch_one<T, PHYS, 2, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
-    case 3: launch_one<T, PHYS, 3, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
-    default: launch_one<T, PHYS, 4, STRETCH>(g, co, ia, corr2, dt, visc, a, st); break;
+    case 0: launch_one<T, PHYS, 0, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 1: launch_one<T, PHYS, 1, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 2: launch_one<T, PHYS, 2, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 3: launch_one<T, PHYS, 3, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    default: launch_one<T, PHYS, 4, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
     }
 }
 
 template <typename T, class Args>
-void launch_stage_any(int phys, int stage, bool stretch, const Geo &g, const Coef<T> &co, const T *ia,
-                      const T *corr2, T dt, T visc, const Args &a, cudaStream_t st)
+void launch_stage_any(int phys, int stage, bool stretch, const Geo &g, const Walls<T> &wl, const Coef<T> &co,
+                      const T *ia, const T *corr2, T dt, T visc, const Args &a, cudaStream_t st)
 {
     if (stretch) {
         switch (phys) {
-        case PHYS_NS: launch_stage_t<T, PHYS_NS, true>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, true>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-        default: launch_stage_t<T, PHYS_MHD_B, true>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        case PHYS_NS: launch_stage_t<T, PHYS_NS, true>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
+        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, true>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
+        default: launch_stage_t<T, PHYS_MHD_B, true>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
         }
     } else {
         switch (phys) {
-        case PHYS_NS: launch_stage_t<T, PHYS_NS, false>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, false>(stage, g, co, ia, corr2, dt, visc, a, st); break;
-        default: launch_stage_t<T, PHYS_MHD_B, false>(stage, g, co, ia, corr2, dt, visc, a, st); break;
+        case PHYS_NS: launch_stage_t<T, PHYS_NS, false>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
+        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, false>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
+        default: launch_stage_t<T, PHYS_MHD_B, false>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
         }
     }
 }
 
 }  // namespace
 
-void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
-                    const double *corr2, double dt, double visc, const StageArgs64 &a, cudaStream_t st)
+void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl, const Coef<double> &co,
+                    const double *ia, const double *corr2, double dt, double visc, const StageArgs64 &a,
+                    cudaStream_t st)
 {
-    launch_stage_any<double>(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, st);
+    launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
 }
 
-void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
-                    const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st)
+void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl, const Coef<float> &co,
+                    const float *ia, const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st)
 {
-    launch_stage_any<float>(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, st);
+    launch_stage_any<float>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
 }
 
 }  // namespace nova

@@ -6,7 +6,9 @@
 // of the NC input components in a register queue (the i-direction stencil);
 // the current plane plus its j/k halo is staged in shared memory (the j- and
 // k-direction stencils).  Every index is wrapped modulo the grid, which
-// synthesises the periodic ghosts (src/BC/periodicBC.hxx:1-66) at load time.
+// synthesises the periodic ghosts (src/BC/periodicBC.hxx:1-66) at load time;
+// with walls in y the j halo is mirrored with the Neumann/Dirichlet ghost
+// formulas instead (Walls<T>).
 //
 // Pipelining: the shared plane is double-buffered, so one barrier per plane
 // suffices; the global loads of the next plane (queue head, halo and, through
@@ -46,8 +48,8 @@ struct NoPre {
 // the thread's node, q the register queue and vx/vy/vz(c, s) the neighbour
 // accessors along i, j, k.
 template <typename T, int H, int NC, class Ld, class Pre, class Body>
-__device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm, const Ld &ld, int ib, int ie,
-                                           Pre &&pre, Body &&body)
+__device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, TileSmem<T, H, NC> &sm, const Ld &ld,
+                                           int ib, int ie, Pre &&pre, Body &&body)
 {
     constexpr int NJH = 2 * H * kTK;
     constexpr int NKH = 2 * H * kTJ;
@@ -58,9 +60,18 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
     const int k0 = blockIdx.x * kTK, j0 = blockIdx.y * kTJ;
     const int k = k0 + tx, j = j0 + ty;
     const bool valid = (k < g.N2) && (j < g.N1);
-    const int kw = wrapi(k, g.N2), jw = wrapi(j, g.N1);
+    const int kw = wrapi(k, g.N2);
+    // rows past the north wall hold mirrored ghosts (read as neighbours only)
+    int jw, tside = -1, tl = 0;
+    if (wl.on && j >= g.N1) {
+        tl = min(j - (g.N1 - 1), g.N1 - 1);
+        tside = 1;
+        jw = (g.N1 - 1) - tl;
+    } else {
+        jw = wrapi(j, g.N1);
+    }
 
-    int hrow[HS], hcol[HS];
+    int hrow[HS], hcol[HS], hside[HS], hl[HS];
     long long hoff[HS];
     bool hon[HS];
 #pragma unroll
@@ -81,8 +92,29 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
         if (!hon[s]) { row = 0; col = 0; }
         hrow[s] = row;
         hcol[s] = col;
-        hoff[s] = (long long)wrapi(j0 + row - H, g.N1) * g.N2 + wrapi(k0 + col - H, g.N2);
+        int jg = j0 + row - H;
+        hside[s] = -1;
+        hl[s] = 0;
+        if (wl.on) {  // mirror across the y walls
+            if (jg < 0) {
+                hside[s] = 0;
+                hl[s] = min(-jg, g.N1 - 1);
+                jg = hl[s];
+            } else if (jg >= g.N1) {
+                hside[s] = 1;
+                hl[s] = min(jg - (g.N1 - 1), g.N1 - 1);
+                jg = (g.N1 - 1) - hl[s];
+            }
+        } else {
+            jg = wrapi(jg, g.N1);
+        }
+        hoff[s] = (long long)jg * g.N2 + wrapi(k0 + col - H, g.N2);
     }
+    auto hload = [&](int s, int c, long long plane) -> T {
+        const T v = ld(c, plane + hoff[s]);
+        if (hside[s] < 0) return v;
+        return wl.sgn[hside[s]][c] * v + wl.off[hside[s]][c] * (T)hl[s];
+    };
 
     const long long colOff = (long long)jw * g.N2 + kw;
     T q[2 * H + 1][NC];
@@ -103,7 +135,7 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
 #pragma unroll
         for (int s = 0; s < HS; s++)
 #pragma unroll
-            for (int c = 0; c < NC; c++) hn[s][c] = hon[s] ? ld(c, plane + hoff[s]) : T(0);
+            for (int c = 0; c < NC; c++) hn[s][c] = hon[s] ? hload(s, c, plane) : T(0);
         if (valid) pre(plane + colOff, true);
     }
 
@@ -117,7 +149,7 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
 #pragma unroll
         for (int c = 0; c < NC; c++) {
             q[2 * H][c] = qn[c];
-            sm.v[b][c][ty + H][tx + H] = q[H][c];
+            sm.v[b][c][ty + H][tx + H] = (tside < 0) ? q[H][c] : wl.sgn[1][c] * q[H][c] + wl.off[1][c] * (T)tl;
         }
 #pragma unroll
         for (int s = 0; s < HS; s++)
@@ -136,7 +168,7 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
             for (int s = 0; s < HS; s++)
                 if (hon[s])
 #pragma unroll
-                    for (int c = 0; c < NC; c++) hn[s][c] = ld(c, nplane + hoff[s]);
+                    for (int c = 0; c < NC; c++) hn[s][c] = hload(s, c, nplane);
         }
         if (!valid) continue;
         pre(nplane + colOff, more);
@@ -148,10 +180,10 @@ __device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm,
 }
 
 template <typename T, int H, int NC, class Ld, class Body>
-__device__ __forceinline__ void tile_march(const Geo &g, TileSmem<T, H, NC> &sm, const Ld &ld, int ib, int ie,
-                                           Body &&body)
+__device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, TileSmem<T, H, NC> &sm, const Ld &ld,
+                                           int ib, int ie, Body &&body)
 {
-    tile_march<T, H, NC>(g, sm, ld, ib, ie, NoPre{}, body);
+    tile_march<T, H, NC>(g, wl, sm, ld, ib, ie, NoPre{}, body);
 }
 
 // grid shape of a tile march: k tiles x j tiles x i chunks

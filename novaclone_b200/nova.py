@@ -31,7 +31,8 @@ STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_
 # every symbol declared in include/nova_gpu.h
 EXPORTS = (
     "nova_create", "nova_destroy", "nova_last_error", "nova_set_stream", "nova_synchronize", "nova_mesh_local_n",
-    "nova_mesh_metrics", "nova_field_create", "nova_field_destroy", "nova_field_upload", "nova_field_download",
+    "nova_mesh_metrics", "nova_field_create", "nova_field_destroy", "nova_field_set_bc", "nova_field_get_bc",
+    "nova_field_upload", "nova_field_download",
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
     "nova_field_maxabs", "nova_advance", "nova_adjoint_grad", "nova_profile_enable", "nova_profile_read",
@@ -41,7 +42,7 @@ EXPORTS = (
 
 class MeshDesc(C.Structure):
     _fields_ = [("N", C.c_int * 3), ("L", C.c_double * 3), ("origin", C.c_double * 3), ("m", C.c_int),
-                ("hyperbolic_z", C.c_int), ("s1", C.c_double), ("s2", C.c_double)]
+                ("hyperbolic_z", C.c_int), ("s1", C.c_double), ("s2", C.c_double), ("walls", C.c_int * 3)]
 
 
 class BCDesc(C.Structure):
@@ -88,6 +89,8 @@ def load_library(path: str = LIB_PATH):
         "nova_mesh_metrics": [vp, dp, dp],
         "nova_field_create": [vp, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
         "nova_field_destroy": [vp, vp],
+        "nova_field_set_bc": [vp, vp, C.POINTER(BCDesc)],
+        "nova_field_get_bc": [vp, vp, C.POINTER(BCDesc)],
         "nova_field_upload": [vp, vp, dp, ip],
         "nova_field_download": [vp, vp, dp, ip, C.POINTER(BCDesc)],
         "nova_field_upload_soa": [vp, vp, dp],
@@ -129,9 +132,10 @@ def _iptr(a):
 class Mesh:
     """A nova_ctx: the reference's Mesh for one GPU (src/Mesh/Mesh.cpp:24-179)."""
 
-    def __init__(self, N, L=(2 * math.pi,) * 3, origin=(0.0, 0.0, 0.0), m=6, hyperbolic_z=None):
+    def __init__(self, N, L=(2 * math.pi,) * 3, origin=(0.0, 0.0, 0.0), m=6, hyperbolic_z=None, walls=(0, 0, 0)):
         self.lib = load_library()
         d = MeshDesc()
+        d.walls[:] = [int(v) for v in walls]
         d.N[:] = [int(v) for v in N]
         d.L[:] = [float(v) for v in L]
         d.origin[:] = [float(v) for v in origin]
@@ -147,6 +151,9 @@ class Mesh:
         self.L = tuple(float(v) for v in L)
         self.origin = tuple(float(v) for v in origin)
         self.m = int(m)
+        self.walls = tuple(int(v) for v in walls)
+        # stored nodes per axis: N (periodic) or N + 1 (walls)
+        self.shape = tuple(self.N[a] + self.walls[a] for a in range(3))
         n = np.zeros(3, np.int32)
         self.check(self.lib.nova_mesh_local_n(self.h, _iptr(n)))
         self.local_n = tuple(int(v) for v in n)
@@ -245,15 +252,24 @@ class Field:
         return out
 
     # device-native layout [c][i][j][k]
+    def set_bc(self, types, vals=None):
+        """types/vals: 18 entries indexed face + 6*comp (north, south, east, west, top, bottom)."""
+        b = BCDesc()
+        b.type[:] = [int(t) for t in types] + [0] * (18 - len(types))
+        v = list(vals) if vals is not None else [0.0] * len(types)
+        b.val[:] = [float(x) for x in v] + [0.0] * (18 - len(v))
+        self.mesh.check(self.mesh.lib.nova_field_set_bc(self.mesh.h, self.h, C.byref(b)))
+        return self
+
     def upload_soa(self, soa):
         a = np.ascontiguousarray(soa, np.float64)
-        if a.size != self.nc * int(np.prod(self.mesh.N)):
+        if a.size != self.nc * int(np.prod(self.mesh.shape)):
             raise ValueError("wrong size")
         self.mesh.check(self.mesh.lib.nova_field_upload_soa(self.mesh.h, self.h, _dptr(a)))
         return self
 
     def download_soa(self):
-        out = np.zeros((self.nc,) + self.mesh.N)
+        out = np.zeros((self.nc,) + self.mesh.shape)
         self.mesh.check(self.mesh.lib.nova_field_download_soa(self.mesh.h, self.h, _dptr(out)))
         return out
 

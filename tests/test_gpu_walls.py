@@ -1,0 +1,127 @@
+"""GPU parity with walls in y (config: temporal shear layer), against the
+oracle running the reference's Neumann/Dirichlet ghost fills
+(src/BC/neumannBC.hxx, src/BC/dirichletBC.hxx), its wall-node overwrites and
+the periodic FFT solve the reference's wall case uses (app/shearLayer/UEqn.H
+calls poisson::solve).  FP64: relative L2 <= 1e-11 per field."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2, rel_max
+
+pytestmark = pytest.mark.gpu
+
+N = (16, 12, 8)
+L = (2 * np.pi, 2 * np.pi, np.pi)
+# u, w Neumann / v Dirichlet on the y walls (north = high y, south = low y)
+UBC = {"north": [(1, 0.0), (2, 0.0), (1, 0.0)], "south": [(1, 0.0), (2, 0.0), (1, 0.0)]}
+PBC = {"north": (1, 0.0), "south": (1, 0.0)}
+# non-zero values exercise every ghost formula
+UBC_VALS = {"north": [(1, 0.3), (2, 0.1), (1, -0.2)], "south": [(1, -0.4), (2, 0.25), (2, 0.05)]}
+
+
+@pytest.fixture(scope="module")
+def nova():
+    from novaclone_b200 import nova
+    return nova
+
+
+def stored(OM, g):
+    """ghosted oracle field -> the stored nodes of a mesh with y walls: (nc, N0, N1+1, N2)"""
+    h = OM.h
+    u = g[h:h + OM.N[0], h:h + OM.N[1] + 1, h:h + OM.N[2]]
+    return np.ascontiguousarray(np.moveaxis(u, -1, 0))
+
+
+def gpu_mesh(nova):
+    return nova.Mesh(N, L=L, walls=(0, 1, 0))
+
+
+def set_bc(nova, f, spec, nc):
+    from oracle import oracle as O
+    t, v = O.bc_arrays(nc, spec)
+    f.set_bc(list(t) + [0] * (18 - len(t)), list(v) + [0.0] * (18 - len(v)))
+    return f
+
+
+def initial_field(oracle, OM, seed=0):
+    rng = np.random.default_rng(seed)
+    x = OM.origin[0] + np.arange(N[0]) * OM.d[0]
+    y = OM.origin[1] + np.arange(N[1] + 1) * OM.d[1]
+    z = OM.origin[2] + np.arange(N[2]) * OM.d[2]
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    U = np.stack([np.tanh(2.0 * (Y - np.pi)), 0.1 * np.sin(X) * np.sin(Y), 0.05 * np.cos(Z) * np.sin(Y)])
+    return U + 1e-3 * rng.standard_normal(U.shape)
+
+
+def ghosted_from_stored(oracle, OM, U, spec):
+    """stored nodes -> ghosted array with the reference's BCs applied"""
+    g = OM.zeros(U.shape[0])
+    h = OM.h
+    g[h:h + N[0], h:h + N[1] + 1, h:h + N[2]] = np.moveaxis(U, 0, -1)
+    return oracle.bc_apply(OM, g, spec)
+
+
+@pytest.mark.parametrize("spec", [UBC, UBC_VALS])
+def test_operators_with_walls(nova, oracle, spec):
+    OM = oracle.Mesh(N, L=L)
+    GM = gpu_mesh(nova)
+    Ug = ghosted_from_stored(oracle, OM, initial_field(oracle, OM), spec)
+    sg = ghosted_from_stored(oracle, OM, initial_field(oracle, OM, 1)[:1], {"north": (1, 0.1), "south": (2, -0.3)})
+    dU = set_bc(nova, nova.Field(GM, 3), spec, 3).upload(Ug)
+    ds = set_bc(nova, nova.Field(GM, 1), {"north": (1, 0.1), "south": (2, -0.3)}, 1).upload(sg)
+    cases = {"grad_s": (nova.ex.grad(ds), oracle.grad_s(OM, sg)), "div_v": (nova.ex.div(dU), oracle.div_v(OM, Ug)),
+             "div_vv": (nova.ex.div(dU, dU), oracle.div_vf(OM, Ug, Ug)),
+             "lap_v": (nova.ex.laplacian(0.02, dU), oracle.lap(OM, 0.02, Ug)),
+             "curl": (nova.ex.curl(dU), oracle.curl(OM, Ug))}
+    for name, (g, o) in cases.items():
+        assert rel_max(g.download_soa(), stored(OM, o)) < 1e-12, name
+    # downloads synthesise the wall ghosts with the field's own BC formulas
+    assert np.array_equal(dU.download(), Ug)
+
+
+@pytest.mark.parametrize("rk_mode", ["classical", "literal"])
+@pytest.mark.parametrize("spec", [UBC, UBC_VALS])
+def test_shear_layer_advance_with_walls(nova, oracle, rk_mode, spec):
+    OM = oracle.Mesh(N, L=L)
+    GM = gpu_mesh(nova)
+    U0 = initial_field(oracle, OM)
+    Ug = ghosted_from_stored(oracle, OM, U0, spec)
+    kw = dict(model="ns", rk_mode=rk_mode, nsteps=6, dt=0.01, nu=1e-2)
+    r = oracle.run(OM, Ug, bcU=spec, bcp=PBC, **kw)
+    U = set_bc(nova, nova.Field(GM, 3), spec, 3).upload(Ug)
+    p = set_bc(nova, nova.Field(GM, 1), PBC, 1)
+    kw.pop("nsteps")
+    hist = nova.advance(GM, nova.run_desc(**kw), U, p, nsteps=6)
+    got = U.download_soa()
+    ref = stored(OM, r[0])
+    for c in range(3):
+        assert rel_l2(got[c], ref[c]) < 1e-11, (c, rel_l2(got[c], ref[c]))
+    assert rel_l2(p.download_soa(), stored(OM, r[2])) < 1e-11
+    np.testing.assert_allclose(hist[:, 2], r[4][:, 2], rtol=1e-11)
+    assert np.abs(hist[:, 4] - r[4][:, 4]).max() < 1e-10 * max(1.0, np.abs(r[4][:, 4]).max())
+
+
+def test_walls_fp32_split_error_is_bounded(nova, oracle):
+    OM = oracle.Mesh(N, L=L)
+    GM = gpu_mesh(nova)
+    Ug = ghosted_from_stored(oracle, OM, initial_field(oracle, OM), UBC)
+    out = []
+    for prec in (nova.F64, nova.F32SPLIT):
+        U = set_bc(nova, nova.Field(GM, 3, prec), UBC, 3).upload(Ug)
+        p = set_bc(nova, nova.Field(GM, 1), PBC, 1)
+        nova.advance(GM, nova.run_desc(model="ns", rk_mode="classical", precision=prec, dt=0.01, nu=1e-2), U, p,
+                     nsteps=6)
+        out.append(U.download_soa())
+    for c in range(3):
+        assert rel_l2(out[1][c], out[0][c]) < 1e-5
+
+
+def test_wall_bc_validation(nova):
+    GM = gpu_mesh(nova)
+    f = nova.Field(GM, 3)
+    with pytest.raises(nova.NovaError) as e:
+        f.set_bc([0] * 18)  # periodic faces on the wall axis
+    assert e.value.status == nova.E_INVALID
+    with pytest.raises(nova.NovaError) as e:
+        nova.Mesh(N, L=L, walls=(1, 0, 0))
+    assert e.value.status == nova.E_UNSUPPORTED
