@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_adj_stage(Geo g, Coef<double> c
         return c < 3 ? a.Y[(long long)c * g.N3 + o] : a.G[(long long)(c - 3) * g.N3 + o] * gs;
     };
     const Walls<double> wl{};  // the adjoint is built for periodic meshes
-    tile_march<double, H, 6>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
+    tile_march<double, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
                                                       const auto &vz) {
         double mu[3], lam[3];
 #pragma unroll

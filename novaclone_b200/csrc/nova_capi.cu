@@ -99,19 +99,12 @@ void add_walls(const nova_ctx *ctx, const nova_field *f, Walls<T> &w, int c0)
 {
     if (!ctx->g.wallY || !f) return;
     w.on = 1;
-    const double dy = ctx->md.L[1] / ctx->md.N[1];
+    w.dy = (T)(ctx->md.L[1] / ctx->md.N[1]);
     for (int c = 0; c < f->nc && c0 + c < 9; c++) {
         for (int side = 0; side < 2; side++) {
             const int q = (side == 0 ? NOVA_SOUTH : NOVA_NORTH) + 6 * (c < 3 ? c : 0);
-            const int type = f->bc.type[q];
-            const double val = f->bc.val[q];
-            if (type == NOVA_BC_DIRICHLET) {
-                w.sgn[side][c0 + c] = T(-1);
-                w.off[side][c0 + c] = T(2.0 * val);
-            } else {
-                w.sgn[side][c0 + c] = T(1);
-                w.off[side][c0 + c] = T(-2.0 * val * dy);
-            }
+            w.dir[side][c0 + c] = f->bc.type[q] == NOVA_BC_DIRICHLET ? 1 : 0;
+            w.val[side][c0 + c] = (T)f->bc.val[q];
         }
     }
 }
@@ -930,6 +923,7 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     if (rd->rk_mode != NOVA_RK_LITERAL && rd->rk_mode != NOVA_RK_CLASSICAL)
         return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown rk_mode");
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: the fused kernels are built for m = 6");
+    if (mhd && ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: MHD is built for periodic meshes");
     if (!valid_field(st->U, 3) || !valid_field(st->p, 1) || st->p->prec != NOVA_F64 || st->U->prec != rd->precision)
         return fail(ctx, NOVA_E_INVALID, "nova_advance: U (3 comps, run precision) and p (FP64 scalar) required");
     if (mhd && (!valid_field(st->B, 3) || !valid_field(st->pB, 1) || st->pB->prec != NOVA_F64 ||

@@ -25,16 +25,35 @@ struct Geo {
     int wallY;
 };
 
-// Ghosts beyond the y walls of the halo'd components (src/BC/neumannBC.hxx,
-// src/BC/dirichletBC.hxx): ghost(l) = sgn * f(mirror l) + off * l, with
-//   Neumann:   sgn = +1, off = -2 val dy    (both faces, as the reference writes it)
-//   Dirichlet: sgn = -1, off = +2 val
+// Ghosts beyond the y walls of the halo'd components, evaluated with the
+// reference's own expressions (src/BC/neumannBC.hxx, src/BC/dirichletBC.hxx)
+// for the l-th ghost and its mirror node f:
+//   Neumann:   f - 2 l val dy     (both faces, as the reference writes it)
+//   Dirichlet: 2 l val - f
 // side 0 = south face (j = 0), side 1 = north face (j = N1 - 1).
 template <typename T> struct Walls {
     int on;
-    T sgn[2][9];
-    T off[2][9];
+    int dir[2][9];  // 1 = Dirichlet, 0 = Neumann
+    T val[2][9];
+    T dy;
 };
+
+// rounded like the reference's host code: every product and difference
+// rounded separately (no fused multiply-add)
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ T wall_ghost(const Walls<T> &w, int side, int c, int l, T f)
+{
+    // selects instead of a runtime index keep the parameters in the constant bank
+    const int dir = side == 0 ? w.dir[0][c] : w.dir[1][c];
+    const T val = side == 0 ? w.val[0][c] : w.val[1][c];
+    const T tv = rn_mul((T)2.0 * (T)l, val);
+    return dir ? rn_sub(tv, f) : rn_sub(f, rn_mul(tv, w.dy));
+}
 
 // First/second-derivative weights of src/settings/settings.cpp:25-31 for half
 // width H, per direction d: a[d][l] = c_l / (2 (l+1) delta_d) (grad.cpp:46),

@@ -49,7 +49,7 @@ __device__ __forceinline__ double at(const P &f, const Geo &g, int c, int i, int
             const int side = jj < 0 ? 0 : 1;
             const int l = side == 0 ? -jj : jj - (g.N1 - 1);
             const int jm = side == 0 ? l : (g.N1 - 1) - l;
-            return f.wl.sgn[side][c] * f(c, (long long)i * g.N12 + (long long)jm * g.N2 + k) + f.wl.off[side][c] * l;
+            return wall_ghost(f.wl, side, c, l, f(c, (long long)i * g.N12 + (long long)jm * g.N2 + k));
         }
         j = f.wl.on ? jj : wrapi(jj, g.N1);
     }
@@ -97,7 +97,7 @@ __global__ void k_scale(Geo g, int ny, cuDoubleComplex *__restrict__ spec, const
 
 // rhs = div(U*)/divisor and U = U* - s*grad(p): the 2.5-D march of nova_tile.cuh
 // (register queue along i, shared plane for j/k), one read of each input.
-template <int H, class LD>
+template <int H, class LD, bool WALLS>
 __global__ void __launch_bounds__(kThreads) k_div_tiled(Geo g, Coef<double> co, const double *__restrict__ ia, LD U,
                                                         double divisor, double *__restrict__ rhs, int ichunk)
 {
@@ -109,14 +109,14 @@ __global__ void __launch_bounds__(kThreads) k_div_tiled(Geo g, Coef<double> co, 
     double az[H];
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
-    tile_march<double, H, 3>(g, U.wl, sm, U, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy,
+    tile_march<double, H, 3, WALLS>(g, U.wl, sm, U, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy,
                                                           const auto &vz) {
         const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
         rhs[idx] = d / divisor;
     });
 }
 
-template <int H, bool SPLIT>
+template <int H, bool SPLIT, bool WALLS>
 __global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Walls<double> pw, Coef<double> co,
                                                             const double *__restrict__ ia, const double *__restrict__ p,
                                                             double s, const double *Us64, double *U64,
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Walls<double>
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
     auto ld = [&](int, long long o) { return p[o]; };
-    tile_march<double, H, 1>(g, pw, sm, ld, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy,
+    tile_march<double, H, 1, WALLS>(g, pw, sm, ld, ib, ie, [&](long long idx, auto &, const auto &vx, const auto &vy,
                                                           const auto &vz) {
         double us[3];
 #pragma unroll
@@ -193,7 +193,7 @@ __device__ __forceinline__ T block_reduce_max(T v, T *sh)
 // Energies sum the unique nodes as app/TG_Piosson/TG.cpp:148-166 does (the
 // stored north-wall row is the reference's last node and is skipped); the
 // divergence maxima cover every stored node (tools::maximum, src/Tools/Tools.h:19-36).
-template <int H, int NC, class LD>
+template <int H, int NC, class LD, bool WALLS>
 __global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl, Coef<double> co,
                                                          const double *__restrict__ ia, LD U, LD B, int ichunk,
                                                          double *__restrict__ part)
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl
     const int rows_e = g.N1 - g.wallY;
     double ek = 0.0, em = 0.0, mdu = 0.0, mdb = 0.0;
     auto ld = [&](int c, long long o) -> double { return c < 3 ? U(c, o) : B(c - 3, o); };
-    tile_march<double, H, NC>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
+    tile_march<double, H, NC, WALLS>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
                                                           const auto &vz) {
         const int j = (int)((idx % g.N12) / g.N2);
         const bool ce = j < rows_e;
@@ -510,7 +510,7 @@ __global__ void k_soa_to_aos(Geo g, Walls<double> wl, int h, int n0, int n1, int
     for (int c = 0; c < nc; c++) {
         const long long o = (long long)c * g.N3 + s;
         const double v = d64 ? d64[o] : (double)hi[o] + (double)lo[o];
-        aos[t * nc + c] = side < 0 ? v : wl.sgn[side][c] * v + wl.off[side][c] * l;
+        aos[t * nc + c] = side < 0 ? v : wall_ghost(wl, side, c, l, v);
     }
 }
 
@@ -590,17 +590,21 @@ void launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<do
 {
     const int ch = pick_ichunk(g, 3);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
+#define NOVA_DIV(LDT, LDV, W)                                                                             \
+    NOVA_DISPATCH_H(h, {                                                                                  \
+        constexpr size_t sb = tile_smem_bytes<double, HH, 3>();                                           \
+        k_div_tiled<HH, LDT, W><<<grid, block, sb, st>>>(g, co, ia, LDV, divisor, rhs, ch);                \
+    })
     if (U64) {
-        NOVA_DISPATCH_H(h, {
-            constexpr size_t sb = tile_smem_bytes<double, HH, 3>();
-            k_div_tiled<HH, Ld64><<<grid, block, sb, st>>>(g, co, ia, Ld64{U64, g.N3, wl}, divisor, rhs, ch);
-        });
+        if (wl.on) { NOVA_DIV(Ld64, (Ld64{U64, g.N3, wl}), true); } else { NOVA_DIV(Ld64, (Ld64{U64, g.N3, wl}), false); }
     } else {
-        NOVA_DISPATCH_H(h, {
-            constexpr size_t sb = tile_smem_bytes<double, HH, 3>();
-            k_div_tiled<HH, LdSplit><<<grid, block, sb, st>>>(g, co, ia, LdSplit{hi, lo, g.N3, wl}, divisor, rhs, ch);
-        });
+        if (wl.on) {
+            NOVA_DIV(LdSplit, (LdSplit{hi, lo, g.N3, wl}), true);
+        } else {
+            NOVA_DIV(LdSplit, (LdSplit{hi, lo, g.N3, wl}), false);
+        }
     }
+#undef NOVA_DIV
 }
 
 void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const double *ky2, const double *kz2,
@@ -616,19 +620,17 @@ void launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<dou
 {
     const int ch = pick_ichunk(g, 4);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
+#define NOVA_CORR(SPL, W)                                                                                 \
+    NOVA_DISPATCH_H(h, {                                                                                  \
+        constexpr size_t sb = tile_smem_bytes<double, HH, 1>();                                           \
+        k_correct_tiled<HH, SPL, W><<<grid, block, sb, st>>>(g, pw, co, ia, p, s, Us64, U64, Ushi, Uslo, hi, lo, ch); \
+    })
     if (U64) {
-        NOVA_DISPATCH_H(h, {
-            constexpr size_t sb = tile_smem_bytes<double, HH, 1>();
-            k_correct_tiled<HH, false><<<grid, block, sb, st>>>(g, pw, co, ia, p, s, Us64, U64, nullptr, nullptr,
-                                                                nullptr, nullptr, ch);
-        });
+        if (pw.on) { NOVA_CORR(false, true); } else { NOVA_CORR(false, false); }
     } else {
-        NOVA_DISPATCH_H(h, {
-            constexpr size_t sb = tile_smem_bytes<double, HH, 1>();
-            k_correct_tiled<HH, true><<<grid, block, sb, st>>>(g, pw, co, ia, p, s, nullptr, nullptr, Ushi, Uslo, hi, lo,
-                                                               ch);
-        });
+        if (pw.on) { NOVA_CORR(true, true); } else { NOVA_CORR(true, false); }
     }
+#undef NOVA_CORR
 }
 
 int diag_blocks(const Geo &g)
@@ -646,40 +648,29 @@ void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double
     const int ch = pick_ichunk(g, 2);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     const int nb = (int)(grid.x * grid.y * grid.z);
+#define NOVA_DIAG(NC, LDT, UU, BB, W)                                                                     \
+    NOVA_DISPATCH_H(h, {                                                                                  \
+        constexpr size_t sb = tile_smem_bytes<double, HH, NC>();                                          \
+        if (sb > 48 * 1024)                                                                               \
+            cudaFuncSetAttribute(k_diag_tiled<HH, NC, LDT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb); \
+        k_diag_tiled<HH, NC, LDT, W><<<grid, block, sb, st>>>(g, wl, co, ia, UU, BB, ch, part);            \
+    })
     if (U64) {
         Ld64 U{U64, g.N3, wl}, B{hasB ? B64 : U64, g.N3, wl};
         if (hasB) {
-            NOVA_DISPATCH_H(h, {
-                constexpr size_t sb = tile_smem_bytes<double, HH, 6>();
-                static bool attr = false;
-                if (!attr) {
-                    cudaFuncSetAttribute(k_diag_tiled<HH, 6, Ld64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-                    attr = true;
-                }
-                k_diag_tiled<HH, 6, Ld64><<<grid, block, sb, st>>>(g, wl, co, ia, U, B, ch, part);
-            });
+            if (wl.on) { NOVA_DIAG(6, Ld64, U, B, true); } else { NOVA_DIAG(6, Ld64, U, B, false); }
         } else {
-            NOVA_DISPATCH_H(h, (k_diag_tiled<HH, 3, Ld64><<<grid, block, tile_smem_bytes<double, HH, 3>(), st>>>(
-                                   g, wl, co, ia, U, B, ch, part)));
+            if (wl.on) { NOVA_DIAG(3, Ld64, U, B, true); } else { NOVA_DIAG(3, Ld64, U, B, false); }
         }
     } else {
         LdSplit U{Uhi, Ulo, g.N3, wl}, B{hasB ? Bhi : Uhi, hasB ? Blo : Ulo, g.N3, wl};
         if (hasB) {
-            NOVA_DISPATCH_H(h, {
-                constexpr size_t sb = tile_smem_bytes<double, HH, 6>();
-                static bool attr = false;
-                if (!attr) {
-                    cudaFuncSetAttribute(k_diag_tiled<HH, 6, LdSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sb);
-                    attr = true;
-                }
-                k_diag_tiled<HH, 6, LdSplit><<<grid, block, sb, st>>>(g, wl, co, ia, U, B, ch, part);
-            });
+            if (wl.on) { NOVA_DIAG(6, LdSplit, U, B, true); } else { NOVA_DIAG(6, LdSplit, U, B, false); }
         } else {
-            NOVA_DISPATCH_H(h, (k_diag_tiled<HH, 3, LdSplit><<<grid, block, tile_smem_bytes<double, HH, 3>(), st>>>(
-                                   g, wl, co, ia, U, B, ch, part)));
+            if (wl.on) { NOVA_DIAG(3, LdSplit, U, B, true); } else { NOVA_DIAG(3, LdSplit, U, B, false); }
         }
     }
+#undef NOVA_DIAG
     k_diag_final<<<1, 256, 0, st>>>(part, nb, 1.0 / (double)((long long)g.N0 * (g.N1 - g.wallY) * g.N2), step, time,
                                     row, flag);
 }

@@ -53,7 +53,7 @@ namespace nova {
 
 namespace {
 
-template <typename T, int H, int PHYS, int STAGE, bool STRETCH, class Args>
+template <typename T, int H, int PHYS, int STAGE, bool STRETCH, bool WALLS, class Args>
 __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo g, Walls<T> wl, Coef<T> co,
                                                       const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
                                                       T visc, Args args, int ichunk)
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
         }
     };
 
-    tile_march<T, H, NC>(
+    tile_march<T, H, NC, WALLS>(
         g, wl, sm, [&](int c, long long o) { return src[c][o]; }, ib, ie, pre,
         [&](long long idx, auto &q, const auto &vx, const auto &vy, const auto &vz) {
             if constexpr (!kAhead) {
@@ -253,13 +253,13 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
 
 constexpr int kH = 3;
 
-template <typename T, int PHYS, int STAGE, bool STRETCH, class Args>
+template <typename T, int PHYS, int STAGE, bool STRETCH, bool WALLS, class Args>
 void launch_one(const Geo &g, const Walls<T> &wl, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
                 const Args &a, cudaStream_t st)
 {
     constexpr int NC = (PHYS == PHYS_NS) ? 3 : 6;
     constexpr size_t smem = tile_smem_bytes<T, kH, NC>();
-    auto kern = k_stage<T, kH, PHYS, STAGE, STRETCH, Args>;
+    auto kern = k_stage<T, kH, PHYS, STAGE, STRETCH, WALLS, Args>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -270,16 +270,16 @@ void launch_one(const Geo &g, const Walls<T> &wl, const Coef<T> &co, const T *ia
     kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, wl, co, ia, corr2, dt, visc, a, ch);
 }
 
-template <typename T, int PHYS, bool STRETCH, class Args>
+template <typename T, int PHYS, bool STRETCH, bool WALLS, class Args>
 void launch_stage_t(int stage, const Geo &g, const Walls<T> &wl, const Coef<T> &co, const T *ia, const T *corr2, T dt,
                     T visc, const Args &a, cudaStream_t st)
 {
     switch (stage) {
-    case 0: launch_one<T, PHYS, 0, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
-    case 1: launch_one<T, PHYS, 1, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
-    case 2: launch_one<T, PHYS, 2, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
-    case 3: launch_one<T, PHYS, 3, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
-    default: launch_one<T, PHYS, 4, STRETCH>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 0: launch_one<T, PHYS, 0, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 1: launch_one<T, PHYS, 1, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 2: launch_one<T, PHYS, 2, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 3: launch_one<T, PHYS, 3, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    default: launch_one<T, PHYS, 4, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
     }
 }
 
@@ -287,19 +287,21 @@ template <typename T, class Args>
 void launch_stage_any(int phys, int stage, bool stretch, const Geo &g, const Walls<T> &wl, const Coef<T> &co,
                       const T *ia, const T *corr2, T dt, T visc, const Args &a, cudaStream_t st)
 {
-    if (stretch) {
-        switch (phys) {
-        case PHYS_NS: launch_stage_t<T, PHYS_NS, true>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
-        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, true>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
-        default: launch_stage_t<T, PHYS_MHD_B, true>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
+    // walls are built for the Navier-Stokes stage only (the C ABI refuses MHD with walls)
+    const bool walls = wl.on != 0;
+#define NOVA_STAGE_CASE(P, S, W) launch_stage_t<T, P, S, W>(stage, g, wl, co, ia, corr2, dt, visc, a, st)
+    if (phys == PHYS_NS) {
+        if (stretch) {
+            if (walls) NOVA_STAGE_CASE(PHYS_NS, true, true); else NOVA_STAGE_CASE(PHYS_NS, true, false);
+        } else {
+            if (walls) NOVA_STAGE_CASE(PHYS_NS, false, true); else NOVA_STAGE_CASE(PHYS_NS, false, false);
         }
+    } else if (phys == PHYS_MHD_U) {
+        if (stretch) NOVA_STAGE_CASE(PHYS_MHD_U, true, false); else NOVA_STAGE_CASE(PHYS_MHD_U, false, false);
     } else {
-        switch (phys) {
-        case PHYS_NS: launch_stage_t<T, PHYS_NS, false>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
-        case PHYS_MHD_U: launch_stage_t<T, PHYS_MHD_U, false>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
-        default: launch_stage_t<T, PHYS_MHD_B, false>(stage, g, wl, co, ia, corr2, dt, visc, a, st); break;
-        }
+        if (stretch) NOVA_STAGE_CASE(PHYS_MHD_B, true, false); else NOVA_STAGE_CASE(PHYS_MHD_B, false, false);
     }
+#undef NOVA_STAGE_CASE
 }
 
 }  // namespace

@@ -47,7 +47,7 @@ struct NoPre {
 // body(idx, q, vx, vy, vz) runs for valid threads once per plane, with idx
 // the thread's node, q the register queue and vx/vy/vz(c, s) the neighbour
 // accessors along i, j, k.
-template <typename T, int H, int NC, class Ld, class Pre, class Body>
+template <typename T, int H, int NC, bool WALLS, class Ld, class Pre, class Body>
 __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, TileSmem<T, H, NC> &sm, const Ld &ld,
                                            int ib, int ie, Pre &&pre, Body &&body)
 {
@@ -63,7 +63,7 @@ __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, Til
     const int kw = wrapi(k, g.N2);
     // rows past the north wall hold mirrored ghosts (read as neighbours only)
     int jw, tside = -1, tl = 0;
-    if (wl.on && j >= g.N1) {
+    if (WALLS && j >= g.N1) {
         tl = min(j - (g.N1 - 1), g.N1 - 1);
         tside = 1;
         jw = (g.N1 - 1) - tl;
@@ -95,7 +95,7 @@ __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, Til
         int jg = j0 + row - H;
         hside[s] = -1;
         hl[s] = 0;
-        if (wl.on) {  // mirror across the y walls
+        if constexpr (WALLS) {  // mirror across the y walls
             if (jg < 0) {
                 hside[s] = 0;
                 hl[s] = min(-jg, g.N1 - 1);
@@ -112,8 +112,11 @@ __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, Til
     }
     auto hload = [&](int s, int c, long long plane) -> T {
         const T v = ld(c, plane + hoff[s]);
-        if (hside[s] < 0) return v;
-        return wl.sgn[hside[s]][c] * v + wl.off[hside[s]][c] * (T)hl[s];
+        if constexpr (!WALLS) {
+            return v;
+        } else {
+            return hside[s] < 0 ? v : wall_ghost(wl, hside[s], c, hl[s], v);
+        }
     };
 
     const long long colOff = (long long)jw * g.N2 + kw;
@@ -149,7 +152,10 @@ __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, Til
 #pragma unroll
         for (int c = 0; c < NC; c++) {
             q[2 * H][c] = qn[c];
-            sm.v[b][c][ty + H][tx + H] = (tside < 0) ? q[H][c] : wl.sgn[1][c] * q[H][c] + wl.off[1][c] * (T)tl;
+            if constexpr (WALLS)
+                sm.v[b][c][ty + H][tx + H] = (tside < 0) ? q[H][c] : wall_ghost(wl, 1, c, tl, q[H][c]);
+            else
+                sm.v[b][c][ty + H][tx + H] = q[H][c];
         }
 #pragma unroll
         for (int s = 0; s < HS; s++)
@@ -179,11 +185,11 @@ __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, Til
     }
 }
 
-template <typename T, int H, int NC, class Ld, class Body>
+template <typename T, int H, int NC, bool WALLS, class Ld, class Body>
 __device__ __forceinline__ void tile_march(const Geo &g, const Walls<T> &wl, TileSmem<T, H, NC> &sm, const Ld &ld,
                                            int ib, int ie, Body &&body)
 {
-    tile_march<T, H, NC>(g, wl, sm, ld, ib, ie, NoPre{}, body);
+    tile_march<T, H, NC, WALLS>(g, wl, sm, ld, ib, ie, NoPre{}, body);
 }
 
 // grid shape of a tile march: k tiles x j tiles x i chunks

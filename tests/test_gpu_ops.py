@@ -139,10 +139,12 @@ def test_stretched_z_metrics_and_operators(nova, oracle):
     Ug, sg = OM.to_ghosted(U), OM.to_ghosted(s)
     dU = nova.Field(GM, 3).upload(Ug)
     ds = nova.Field(GM, 1).upload(sg)
+    # unique nodes only: the stretched metric is not periodic, so the reference's duplicate
+    # node N (which a periodic device field does not store) sees other d2z/dxi2 values
     for got, ref in ((nova.ex.grad(ds), oracle.grad_s(OM, sg)), (nova.ex.div(dU), oracle.div_v(OM, Ug)),
                      (nova.ex.div(dU, dU), oracle.div_vf(OM, Ug, Ug)),
                      (nova.ex.laplacian(0.1, dU), oracle.lap(OM, 0.1, Ug))):
-        assert rel_max(OM.interior(got.download()), OM.interior(ref)) < TOL
+        assert rel_max(got.download_soa(), OM.unique(ref)) < TOL
 
 
 def test_stretched_z_advance(nova, oracle):

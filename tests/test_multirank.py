@@ -20,7 +20,8 @@ dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
 r = dist.get_rank()
 v = bench.max_over_ranks(1.5 + r, dist, device="cpu")
 w = bench.max_over_ranks(-float(r), dist, device="cpu")
-print("RANK%%d %%r %%r" %% (r, v, w))
+with open(os.path.join(os.environ["OUT_DIR"], "rank%%d.txt" %% r), "w") as f:
+    f.write("%%r %%r" %% (v, w))
 dist.destroy_process_group()
 ''' % ROOT
 
@@ -42,14 +43,13 @@ def run_torchrun(tmp_path, script, args=(), nproc=2, env=None):
 
 
 def test_max_over_ranks_gloo(tmp_path):
-    r = run_torchrun(tmp_path, WORKER)
+    r = run_torchrun(tmp_path, WORKER, env={"OUT_DIR": str(tmp_path)})
     assert r.returncode == 0, r.stderr[-2000:]
     vals = {}
-    for line in r.stdout.splitlines():
-        if line.startswith("RANK"):
-            rank, v, w = line.split()
-            vals[rank] = (float(v), float(w))
-    assert vals == {"RANK0": (2.5, 0.0), "RANK1": (2.5, 0.0)}, r.stdout
+    for rank in (0, 1):
+        v, w = (tmp_path / ("rank%d.txt" % rank)).read_text().split()
+        vals[rank] = (float(v), float(w))
+    assert vals == {0: (2.5, 0.0), 1: (2.5, 0.0)}
 
 
 def test_reference_arm_prints_once_under_two_ranks(tmp_path):
