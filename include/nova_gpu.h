@@ -80,6 +80,11 @@ typedef struct {
 
 typedef enum { NOVA_MODEL_NS = 0, NOVA_MODEL_MHD = 1 } nova_model;
 typedef enum { NOVA_RK_LITERAL = 0, NOVA_RK_CLASSICAL = 1 } nova_rk_mode;
+/* Pressure solve on a mesh with y walls.  FFT: the reference's poisson::solve on the N
+ * unique y nodes as if y were periodic (what app/shearLayer does).  DCT: the inverse
+ * consistent with the node-based walls -- the even extension in y (a DCT-I), so that
+ * div(U) vanishes on the interior nodes after the projection. */
+typedef enum { NOVA_POISSON_FFT = 0, NOVA_POISSON_DCT = 1 } nova_poisson_mode;
 
 /* One nova_advance call = nsteps of the reference's per-step loop body. */
 typedef struct {
@@ -90,6 +95,8 @@ typedef struct {
     int diag_every;   /* diagnostics row every diag_every steps (0 = none) */
     double dt, nu, eta;
     double t0;        /* time of the state on entry (only reported in the history) */
+    int poisson;      /* nova_poisson_mode (meshes with y walls; periodic meshes ignore it) */
+    int reserved;
 } nova_run_desc;
 
 /* Fields advanced by nova_advance.  U (3 comps) and p (1) always; B, pB for MHD. */

@@ -55,6 +55,10 @@ struct nova_ctx {
     double *d_kx2 = nullptr, *d_ky2 = nullptr, *d_kz2 = nullptr;
     cufftHandle plan_f = 0, plan_b = 0;
     bool plans = false;
+    cufftHandle dct_f = 0, dct_b = 0;  // wall Poisson on the even extension in y
+    bool dct_plans = false;
+    double *d_ext = nullptr, *d_ky2e = nullptr;
+    void *d_spec2 = nullptr;
     void *d_spec = nullptr;
     double *d_rhs = nullptr;
     double *w64[3] = {nullptr, nullptr, nullptr};
@@ -345,6 +349,51 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
     return NOVA_OK;
 }
 
+// the wall Poisson of NOVA_POISSON_DCT: even extension in y, periodic solve on
+// the doubled domain (modified wavenumbers of period 2 L_y), restriction to
+// the stored rows
+nova_status poisson_device_dct(nova_ctx *ctx, const double *rhs, double *p)
+{
+    const Geo &g = ctx->g;
+    const int ny = ctx->md.N[1];
+    nova_status s;
+    if (!ctx->dct_plans) {
+        if ((s = fft_check(ctx, cufftPlan3d(&ctx->dct_f, g.N0, 2 * ny, g.N2, CUFFT_D2Z), "cufftPlan3d D2Z (walls)")) !=
+            NOVA_OK)
+            return s;
+        if ((s = fft_check(ctx, cufftPlan3d(&ctx->dct_b, g.N0, 2 * ny, g.N2, CUFFT_Z2D), "cufftPlan3d Z2D (walls)")) !=
+            NOVA_OK) {
+            cufftDestroy(ctx->dct_f);
+            return s;
+        }
+        ctx->dct_plans = true;
+        const size_t next = (size_t)g.N0 * 2 * ny * g.N2;
+        if ((s = dalloc(ctx, &ctx->d_ext, next)) != NOVA_OK) return s;
+        if ((s = dalloc(ctx, (double **)&ctx->d_spec2, 2 * (size_t)g.N0 * 2 * ny * (g.N2 / 2 + 1))) != NOVA_OK) return s;
+        const double *c = kCoef[(ctx->md.m - 2) / 2];
+        const double dy = ctx->md.L[1] / ny;
+        std::vector<double> ky2e = kp2_table(2 * ny, 2.0 * ctx->md.L[1], dy, ctx->h, c, true, 2 * ny);
+        if ((s = dalloc(ctx, &ctx->d_ky2e, ky2e.size())) != NOVA_OK) return s;
+        CK(cudaMemcpy(ctx->d_ky2e, ky2e.data(), sizeof(double) * ky2e.size(), cudaMemcpyHostToDevice));
+    }
+    ProfScope ps(ctx, NOVA_K_FFT);
+    cufftSetStream(ctx->dct_f, ctx->stream);
+    cufftSetStream(ctx->dct_b, ctx->stream);
+    launch_even_extend(g, ny, rhs, ctx->d_ext, ctx->stream);
+    if ((s = fft_check(ctx, cufftExecD2Z(ctx->dct_f, ctx->d_ext, (cufftDoubleComplex *)ctx->d_spec2), "cufftExecD2Z")) !=
+        NOVA_OK)
+        return s;
+    launch_scale(g, 2 * ny, ctx->d_spec2, ctx->d_kx2, ctx->d_ky2e, ctx->d_kz2,
+                 1.0 / ((double)g.N0 * 2.0 * ny * g.N2), ctx->stream);
+    if ((s = fft_check(ctx, cufftExecZ2D(ctx->dct_b, (cufftDoubleComplex *)ctx->d_spec2, ctx->d_ext), "cufftExecZ2D")) !=
+        NOVA_OK)
+        return s;
+    launch_restrict_rows(g, ny, ctx->d_ext, p, ctx->stream);
+    ctx->launches += 3;
+    CKL("wall poisson");
+    return NOVA_OK;
+}
+
 bool valid_field(const nova_field *f, int nc)
 {
     return f && f->nc == nc;
@@ -454,9 +503,13 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
         cufftDestroy(ctx->plan_f);
         cufftDestroy(ctx->plan_b);
     }
+    if (ctx->dct_plans) {
+        cufftDestroy(ctx->dct_f);
+        cufftDestroy(ctx->dct_b);
+    }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row};
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -793,6 +846,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
     const bool lit = rd->rk_mode == NOVA_RK_LITERAL;
     const bool str = ctx->md.hyperbolic_z != 0;
     const bool walls = g.wallY != 0;
+    const bool dct = walls && rd->poisson == NOVA_POISSON_DCT;
     const WallFix yfix = wall_fix_of(ctx, Y), pfix = wall_fix_of(ctx, p);
     const Walls<double> yw64 = walls_of<double>(ctx, Y), pw64 = walls_of<double>(ctx, p);
     auto fix64 = [&](double *f) {
@@ -833,9 +887,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             ctx->launches += 1;
         }
         CKL("k_div_tiled");
-        nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
+        nova_status s = dct ? poisson_device_dct(ctx, ctx->d_rhs, p->d64) : poisson_device(ctx, ctx->d_rhs, p->d64);
         if (s != NOVA_OK) return s;
-        if (walls) {
+        if (walls && !dct) {
             launch_wall_fix64(g, pfix, p->d64, st);
             ctx->launches += 1;
         }
@@ -895,9 +949,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             ctx->launches += 1;
         }
         CKL("k_div_tiled");
-        nova_status s = poisson_device(ctx, ctx->d_rhs, p->d64);
+        nova_status s = dct ? poisson_device_dct(ctx, ctx->d_rhs, p->d64) : poisson_device(ctx, ctx->d_rhs, p->d64);
         if (s != NOVA_OK) return s;
-        if (walls) {
+        if (walls && !dct) {
             launch_wall_fix64(g, pfix, p->d64, st);
             ctx->launches += 1;
         }
@@ -924,6 +978,12 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
         return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown rk_mode");
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: the fused kernels are built for m = 6");
     if (mhd && ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: MHD is built for periodic meshes");
+    if (rd->poisson != NOVA_POISSON_FFT && rd->poisson != NOVA_POISSON_DCT)
+        return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown poisson mode");
+    if (ctx->g.wallY && rd->poisson == NOVA_POISSON_DCT && st->p)
+        for (int face : {NOVA_NORTH, NOVA_SOUTH})
+            if (st->p->bc.type[face] != NOVA_BC_NEUMANN || st->p->bc.val[face] != 0.0)
+                return fail(ctx, NOVA_E_INVALID, "nova_advance: the DCT wall Poisson needs Neumann-0 pressure walls");
     if (!valid_field(st->U, 3) || !valid_field(st->p, 1) || st->p->prec != NOVA_F64 || st->U->prec != rd->precision)
         return fail(ctx, NOVA_E_INVALID, "nova_advance: U (3 comps, run precision) and p (FP64 scalar) required");
     if (mhd && (!valid_field(st->B, 3) || !valid_field(st->pB, 1) || st->pB->prec != NOVA_F64 ||

@@ -156,6 +156,35 @@ __global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Walls<double>
     });
 }
 
+// Wall Poisson by the even extension in y (a DCT-I of the N1+1 node-based
+// rows): ext has 2*ny rows, ext[j] = rhs[j] for j <= ny and ext[2 ny - j] =
+// rhs[j] for 0 < j < ny.  The mirror image of a field with Neumann-0 ghosts
+// is exactly this even extension, so the periodic solve on the doubled
+// domain inverts D.G with the wall ghosts the stencils use.
+__global__ void k_even_extend(Geo g, int ny, const double *__restrict__ rhs, double *__restrict__ ext)
+{
+    const long long tot = (long long)g.N0 * 2 * ny * g.N2;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= tot) return;
+    const int k = (int)(t % g.N2);
+    const long long r = t / g.N2;
+    const int jj = (int)(r % (2 * ny));
+    const int i = (int)(r / (2 * ny));
+    const int j = jj <= ny ? jj : 2 * ny - jj;
+    ext[t] = rhs[(long long)i * g.N12 + (long long)j * g.N2 + k];
+}
+
+__global__ void k_restrict_rows(Geo g, int ny, const double *__restrict__ ext, double *__restrict__ p)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    const int k = (int)(t % g.N2);
+    const long long r = t / g.N2;
+    const int j = (int)(r % g.N1);
+    const int i = (int)(r / g.N1);
+    p[t] = ext[((long long)i * 2 * ny + j) * g.N2 + k];
+}
+
 // ------------------------------------------------------------- diagnostics --
 constexpr int kRedThreads = 256;
 
@@ -723,6 +752,16 @@ void launch_wall_fix32(const Geo &g, const WallFix &wf, float *f, cudaStream_t s
 void launch_wall_fix_split(const Geo &g, const WallFix &wf, float *hi, float *lo, cudaStream_t st)
 {
     k_wall_fix<float><<<nblocks((long long)g.N0 * g.N2 * wf.nc, 256), 256, 0, st>>>(g, wf, hi, lo);
+}
+
+void launch_even_extend(const Geo &g, int ny, const double *rhs, double *ext, cudaStream_t st)
+{
+    k_even_extend<<<nblocks((long long)g.N0 * 2 * ny * g.N2, 256), 256, 0, st>>>(g, ny, rhs, ext);
+}
+
+void launch_restrict_rows(const Geo &g, int ny, const double *ext, double *p, cudaStream_t st)
+{
+    k_restrict_rows<<<nblocks(g.N3, 256), 256, 0, st>>>(g, ny, ext, p);
 }
 
 void launch_split(long long n, const double *x, float *hi, float *lo, cudaStream_t st)

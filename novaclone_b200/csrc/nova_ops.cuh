@@ -39,6 +39,8 @@ void launch_soa_to_aos(const Geo &g, const Walls<double> &wl, int h, const int n
 void launch_wall_fix64(const Geo &g, const WallFix &wf, double *f, cudaStream_t st);
 void launch_wall_fix32(const Geo &g, const WallFix &wf, float *f, cudaStream_t st);
 void launch_wall_fix_split(const Geo &g, const WallFix &wf, float *hi, float *lo, cudaStream_t st);
+void launch_even_extend(const Geo &g, int ny, const double *rhs, double *ext, cudaStream_t st);
+void launch_restrict_rows(const Geo &g, int ny, const double *ext, double *p, cudaStream_t st);
 void launch_split(long long n, const double *x, float *hi, float *lo, cudaStream_t st);
 void launch_join(long long n, const float *hi, const float *lo, double *x, cudaStream_t st);
 

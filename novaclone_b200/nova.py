@@ -18,6 +18,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libnova_b200.so")
 
 OK, E_INVALID, E_CUDA, E_OOM, E_NONFINITE, E_TIMEOUT, E_UNSUPPORTED = range(7)
+POISSON_FFT, POISSON_DCT = 0, 1
 F64, F32SPLIT = 0, 1
 PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
 MODEL_NS, MODEL_MHD = 0, 1
@@ -51,7 +52,8 @@ class BCDesc(C.Structure):
 
 class RunDesc(C.Structure):
     _fields_ = [("model", C.c_int), ("rk_mode", C.c_int), ("precision", C.c_int), ("diag_every", C.c_int),
-                ("dt", C.c_double), ("nu", C.c_double), ("eta", C.c_double), ("t0", C.c_double)]
+                ("dt", C.c_double), ("nu", C.c_double), ("eta", C.c_double), ("t0", C.c_double),
+                ("poisson", C.c_int), ("reserved", C.c_int)]
 
 
 class AdjDesc(C.Structure):
@@ -344,8 +346,10 @@ class tools:
         return v.value
 
 
-def run_desc(model="ns", rk_mode="classical", precision=F64, dt=0.01, nu=0.0, eta=0.0, diag_every=1, t0=0.0):
+def run_desc(model="ns", rk_mode="classical", precision=F64, dt=0.01, nu=0.0, eta=0.0, diag_every=1, t0=0.0,
+             poisson="fft"):
     r = RunDesc()
+    r.poisson = POISSON_DCT if poisson == "dct" else POISSON_FFT
     r.model = MODEL_MHD if model == "mhd" else MODEL_NS
     r.rk_mode = RK_CLASSICAL if rk_mode == "classical" else RK_LITERAL
     r.precision = precision

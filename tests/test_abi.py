@@ -48,7 +48,7 @@ def test_struct_layout_matches_header(tmp_path):
 #include "nova_gpu.h"
 int main(void) {
   printf("%zu %zu %zu %zu %zu\n", sizeof(nova_mesh_desc), offsetof(nova_mesh_desc, m), offsetof(nova_mesh_desc, s2), offsetof(nova_mesh_desc, walls), sizeof(nova_bc));
-  printf("%zu %zu %zu %zu\n", sizeof(nova_run_desc), offsetof(nova_run_desc, dt), offsetof(nova_run_desc, t0), sizeof(nova_state));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(nova_run_desc), offsetof(nova_run_desc, dt), offsetof(nova_run_desc, t0), offsetof(nova_run_desc, poisson), sizeof(nova_state));
   return 0; }
 ''')
     exe = tmp_path / "layout"
@@ -56,7 +56,8 @@ int main(void) {
     got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     want = [C.sizeof(nova.MeshDesc), nova.MeshDesc.m.offset, nova.MeshDesc.s2.offset, nova.MeshDesc.walls.offset,
             C.sizeof(nova.BCDesc),
-            C.sizeof(nova.RunDesc), nova.RunDesc.dt.offset, nova.RunDesc.t0.offset, C.sizeof(nova.State)]
+            C.sizeof(nova.RunDesc), nova.RunDesc.dt.offset, nova.RunDesc.t0.offset, nova.RunDesc.poisson.offset,
+            C.sizeof(nova.State)]
     assert [int(v) for v in got] == want
 
 

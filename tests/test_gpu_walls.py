@@ -125,3 +125,37 @@ def test_wall_bc_validation(nova):
     with pytest.raises(nova.NovaError) as e:
         nova.Mesh(N, L=L, walls=(1, 0, 0))
     assert e.value.status == nova.E_UNSUPPORTED
+
+
+def test_dct_wall_poisson_makes_interior_rows_divergence_free(nova, oracle):
+    """NOVA_POISSON_DCT solves div grad p = div U*/dt on the even extension of
+    the N1+1 wall-bounded rows, i.e. with the Neumann-0 mirror the pressure's
+    ghosts use, so with no-penetration U* the corrected field is discretely
+    divergence-free on every row between the walls.  The reference's periodic
+    solve (the FFT mode) leaves an O(dt) divergence there."""
+    OM = oracle.Mesh(N, L=L)
+    GM = gpu_mesh(nova)
+    Ug = ghosted_from_stored(oracle, OM, initial_field(oracle, OM), UBC)
+    divs = {}
+    for mode in ("dct", "fft"):
+        U = set_bc(nova, nova.Field(GM, 3), UBC, 3).upload(Ug)
+        p = set_bc(nova, nova.Field(GM, 1), PBC, 1)
+        nova.advance(GM, nova.run_desc(model="ns", rk_mode="classical", dt=0.01, nu=1e-2, poisson=mode), U, p,
+                     nsteps=3)
+        d = nova.ex.div(U).download_soa()[0]
+        divs[mode] = np.abs(d[:, 1:N[1], :]).max()
+        assert np.all(np.isfinite(U.download_soa()))
+    scale = 1.0 / OM.d[1]  # |D U| is O(|U|/dy) at most
+    assert divs["dct"] < 1e-12 * scale, divs
+    assert divs["fft"] > 1e4 * divs["dct"], divs
+
+
+def test_dct_wall_poisson_needs_neumann_zero_pressure(nova, oracle):
+    OM = oracle.Mesh(N, L=L)
+    GM = gpu_mesh(nova)
+    Ug = ghosted_from_stored(oracle, OM, initial_field(oracle, OM), UBC)
+    U = set_bc(nova, nova.Field(GM, 3), UBC, 3).upload(Ug)
+    p = set_bc(nova, nova.Field(GM, 1), {"north": (2, 0.0), "south": (1, 0.0)}, 1)
+    with pytest.raises(nova.NovaError) as e:
+        nova.advance(GM, nova.run_desc(model="ns", dt=0.01, nu=1e-2, poisson="dct"), U, p, nsteps=1)
+    assert e.value.status == nova.E_INVALID
