@@ -150,6 +150,25 @@ nova_status nova_laplacian(nova_ctx *ctx, double nu, const nova_field *f, nova_f
 /* poisson::rhs(rhs); poisson::solve(): p = L^-1 rhs on the unique nodes (mean mode 0) */
 nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, nova_field *p);
 nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *s, double *out);
+/* Allocation-free max|s| (no counterpart in the reference: tools::maximum
+ * allocates its reduction buffers).  Same result as nova_field_maxabs, computed
+ * in a fixed 64 KiB scratch that lives in the library image (a static device
+ * array, one per device) instead of memory the context allocates, so the call
+ * never invokes cudaMalloc/cudaFree or any pool allocator.  For callers that
+ * cannot allocate device memory when they check a field: a solver whose HBM is
+ * all handed out (fields sized to fill the device, or a framework's caching
+ * allocator holding the rest), or a monitor that must not add an allocation's
+ * implicit synchronisation to the running time steps.
+ * Limit: at most NOVA_MAXABS_NOALLOC_MAX_NODES stored nodes (N0*N1*N2, with y
+ * walls N0*(N1+1)*N2); larger fields return NOVA_E_INVALID (use
+ * nova_field_maxabs).  The scratch needs no zeroing: each call writes every
+ * slot before it reads it.  The first call on each device, with that device
+ * current, looks up the scratch address (cudaGetSymbolAddress, which may load
+ * the library's device code); make it before any stream capture.  Calls that
+ * overlap in time on one device (two streams, threads or contexts) share the
+ * scratch and race: serialise them. */
+#define NOVA_MAXABS_NOALLOC_MAX_NODES (1LL << 27)
+nova_status nova_field_maxabs_noalloc(nova_ctx *ctx, const nova_field *s, double *out);
 
 /* ---- fused time advance ---- */
 /* hist: nsteps x NOVA_HIST_COLS doubles (rows of steps without diagnostics are zero); may be NULL */

@@ -815,6 +815,27 @@ extern "C" nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *f, dou
     return NOVA_OK;
 }
 
+extern "C" nova_status nova_field_maxabs_noalloc(nova_ctx *ctx, const nova_field *f, double *out)
+{
+    if (!ctx || !f || !out) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs_noalloc: null argument");
+    if (f->nc != 1 || f->prec != NOVA_F64)
+        return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs_noalloc: FP64 scalar only");
+    const long long n = ctx->g.N3;
+    if (n < 1 || n > NOVA_MAXABS_NOALLOC_MAX_NODES)
+        return fail(ctx, NOVA_E_INVALID,
+                    "nova_field_maxabs_noalloc: " + std::to_string(n) +
+                        " stored nodes, more than its static scratch covers (NOVA_MAXABS_NOALLOC_MAX_NODES = " +
+                        std::to_string((long long)NOVA_MAXABS_NOALLOC_MAX_NODES) + "); use nova_field_maxabs");
+    double *scratch = nullptr;
+    CK(maxabs_noalloc_scratch(&scratch));
+    launch_maxabs_noalloc(n, f->d64, scratch, ctx->stream);
+    ctx->launches += 2;
+    CKL("maxabs_noalloc");
+    CK(cudaMemcpyAsync(out, scratch + kMaxabsStaticParts, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
 // ================================================================== advance ==
 namespace {
 

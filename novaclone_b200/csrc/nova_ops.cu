@@ -8,11 +8,14 @@
 //   U = U* - dt * grad(p)                    k_correct_tiled (src/ex/grad/grad.cpp:25-62)
 // k'^2 is built from 1-D tables of squared modified wavenumbers
 // (poisson::wavenumbersFFT_, poisson.cpp:337-396) summed in the reference's order.
+#include "nova_gpu.h"
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"
 #include "nova_tile.cuh"
 
 #include <cuComplex.h>
+
+#include <atomic>
 
 namespace nova {
 
@@ -329,6 +332,20 @@ __global__ void k_max_final(const double *__restrict__ part, int n, double *__re
     for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, part[q]);
     m = block_reduce_max(m, sh);
     if (threadIdx.x == 0) *out = m;
+}
+
+// one partial per fixed chunk of kMaxabsChunk nodes (no grid-stride loop, so the
+// number of partials is the size the static scratch has to hold)
+__global__ void __launch_bounds__(256) k_maxabs_chunks(long long n, const double *__restrict__ s,
+                                                       double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const long long b = (long long)blockIdx.x * kMaxabsChunk;
+    const long long e = min(b + (long long)kMaxabsChunk, n);
+    double m = 0.0;
+    for (long long t = b + threadIdx.x; t < e; t += blockDim.x) m = fmax(m, fabs(s[t]));
+    m = block_reduce_max(m, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
 }
 
 // --------------------------------------------------------------- operators --
@@ -709,6 +726,41 @@ void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cud
     const int nb = diag_blocks(g);
     k_maxabs_part<<<nb, 256, 0, st>>>(g.N3, Ld64{s, g.N3}, part);
     k_max_final<<<1, 256, 0, st>>>(part, nb, out);
+}
+
+// The allocation-free reduction's scratch: kMaxabsStaticParts partials, then
+// the result slot (64 KiB per device, part of the library image).  Nothing in
+// it has to start at zero: k_maxabs_chunks writes every partial that
+// k_max_final reads, and k_max_final writes the result before it is copied out.
+static __device__ __align__(256) double g_maxabs_scratch[kMaxabsStaticParts + 1];
+static_assert((long long)kMaxabsChunk * kMaxabsStaticParts == NOVA_MAXABS_NOALLOC_MAX_NODES,
+              "the static scratch must cover the advertised node limit");
+
+constexpr int kMaxabsDevices = 64;
+// per-device address, looked up once with that device current
+static std::atomic<double *> g_maxabs_scratch_ptr[kMaxabsDevices];
+
+cudaError_t maxabs_noalloc_scratch(double **scratch)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxabsDevices) return cudaErrorInvalidDevice;
+    double *q = g_maxabs_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!q) {
+        e = cudaGetSymbolAddress((void **)&q, g_maxabs_scratch);
+        if (e != cudaSuccess) return e;
+        g_maxabs_scratch_ptr[dev].store(q, std::memory_order_release);
+    }
+    *scratch = q;
+    return cudaSuccess;
+}
+
+void launch_maxabs_noalloc(long long n, const double *s, double *scratch, cudaStream_t st)
+{
+    const int np = (int)((n + kMaxabsChunk - 1) / kMaxabsChunk);
+    k_maxabs_chunks<<<np, 256, 0, st>>>(n, s, scratch);
+    k_max_final<<<1, 256, 0, st>>>(scratch, np, scratch + kMaxabsStaticParts);
 }
 
 void launch_op(int op, int h, const Geo &g, const Walls<double> &wa, const Walls<double> &wb, const Coef<double> &co,

@@ -41,6 +41,12 @@ void launch_wall_fix32(const Geo &g, const WallFix &wf, float *f, cudaStream_t s
 void launch_wall_fix_split(const Geo &g, const WallFix &wf, float *hi, float *lo, cudaStream_t st);
 void launch_even_extend(const Geo &g, int ny, const double *rhs, double *ext, cudaStream_t st);
 void launch_restrict_rows(const Geo &g, int ny, const double *ext, double *p, cudaStream_t st);
+// allocation-free max|s|: one block per kMaxabsChunk nodes, one partial each
+constexpr int kMaxabsChunk = 16384;
+constexpr int kMaxabsStaticParts = 8192;
+// address of this device's static scratch (kMaxabsStaticParts partials + the result)
+cudaError_t maxabs_noalloc_scratch(double **scratch);
+void launch_maxabs_noalloc(long long n, const double *s, double *scratch, cudaStream_t st);
 void launch_split(long long n, const double *x, float *hi, float *lo, cudaStream_t st);
 void launch_join(long long n, const float *hi, const float *lo, double *x, cudaStream_t st);
 

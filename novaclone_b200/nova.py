@@ -36,7 +36,7 @@ EXPORTS = (
     "nova_field_upload", "nova_field_download",
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
-    "nova_field_maxabs", "nova_advance", "nova_adjoint_grad", "nova_profile_enable", "nova_profile_read",
+    "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_profile_enable", "nova_profile_read",
     "nova_launch_count",
 )
 
@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH):
         "nova_laplacian": [vp, C.c_double, vp, vp],
         "nova_poisson_solve": [vp, vp, vp],
         "nova_field_maxabs": [vp, vp, dp],
+        "nova_field_maxabs_noalloc": [vp, vp, dp],
         "nova_advance": [vp, C.POINTER(RunDesc), C.POINTER(State), C.c_int, dp],
         "nova_adjoint_grad": [vp, C.POINTER(AdjDesc), C.POINTER(State), vp, vp, dp],
         "nova_profile_enable": [vp, C.c_int],
@@ -343,6 +344,16 @@ class tools:
         M = f.mesh
         v = C.c_double()
         M.check(M.lib.nova_field_maxabs(M.h, f.h, C.byref(v)))
+        return v.value
+
+    @staticmethod
+    def maximum_noalloc(f: Field) -> float:
+        """maximum() through the allocation-free entry point (fixed static
+        scratch, at most NOVA_MAXABS_NOALLOC_MAX_NODES stored nodes; calls on one
+        device must not overlap in time)."""
+        M = f.mesh
+        v = C.c_double()
+        M.check(M.lib.nova_field_maxabs_noalloc(M.h, f.h, C.byref(v)))
         return v.value
 
 
