@@ -9,6 +9,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -82,6 +83,7 @@ struct nova_ctx {
     double prof_ms[NOVA_K_COUNT] = {0};
     long prof_n[NOVA_K_COUNT] = {0};
     long launches = 0;
+    int stage_impl = STAGE_AUTO;  // NOVA_STAGE_IMPL=march|tma at nova_create
 };
 
 namespace {
@@ -323,8 +325,18 @@ nova_status ensure_red(nova_ctx *ctx)
     nova_status s;
     if ((s = dalloc(ctx, &ctx->d_part, (size_t)diag_blocks(ctx->g) * 4)) != NOVA_OK) return s;
     if ((s = dalloc(ctx, &ctx->d_scalar, 1)) != NOVA_OK) return s;
-    if ((s = dalloc(ctx, &ctx->d_flag, 1)) != NOVA_OK) return s;
+    // [0] non-finite diagnostics, [1] a stage pipeline wait timed out
+    if ((s = dalloc(ctx, &ctx->d_flag, 2)) != NOVA_OK) return s;
     return NOVA_OK;
+}
+
+nova_status stage_fail(nova_ctx *ctx, cudaError_t e)
+{
+    if (e == cudaErrorNotSupported)
+        return fail(ctx, NOVA_E_UNSUPPORTED,
+                    "NOVA_STAGE_IMPL=tma: the TMA stage kernel needs periodic y, N2 % 32 == 0, N1 % 8 == 0 and N1 >= 16");
+    if (e == cudaErrorInvalidValue) return fail(ctx, NOVA_E_CUDA, "stage kernel: cuTensorMapEncodeTiled failed");
+    return cuda_check(ctx, e, "stage kernel");
 }
 
 // rhs (device, N3 doubles) -> p: spectral inverse of div(grad(.)) (poisson::solve)
@@ -426,6 +438,10 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
     if (!ctx) return NOVA_E_OOM;
     ctx->md = *md;
     ctx->h = md->m / 2;
+    if (const char *impl = std::getenv("NOVA_STAGE_IMPL")) {
+        if (!std::strcmp(impl, "march")) ctx->stage_impl = STAGE_MARCH;
+        if (!std::strcmp(impl, "tma")) ctx->stage_impl = STAGE_TMA;
+    }
     for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
     Geo &g = ctx->g;
     g.wallY = md->walls[1];
@@ -880,9 +896,12 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         const Walls<double> sw = walls_of<double>(ctx, Y, X);
         fix64(Y->d64);
         double *Ustar;
+        nova_status sst = NOVA_OK;
         auto run64 = [&](int stage, const StageArgs64 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
-            launch_stage64(phys, stage, str, g, sw, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc, a, st);
+            const cudaError_t e = launch_stage64(phys, stage, str, g, sw, ctx->co64, ctx->d_ia64, ctx->d_corr64,
+                                                 rd->dt, visc, a, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
             ctx->launches += 1;
         };
         if (lit) {
@@ -901,6 +920,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             Ustar = Y->d64;
         }
         fix64(Ustar);
+        if (sst != NOVA_OK) return sst;
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
@@ -938,10 +958,13 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         };
         fixpair(Y->hi, Y->lo);
         const float *Ushi, *Uslo;
+        nova_status sst = NOVA_OK;
         auto run32 = [&](int stage, const StageArgs32 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
-            launch_stage32(phys, stage, str, g, sw, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt, (float)visc,
-                           a, st);
+            const cudaError_t e = launch_stage32(phys, stage, str, g, sw, ctx->co32, ctx->d_ia32, ctx->d_corr32,
+                                                 (float)rd->dt, (float)visc, a, st,
+                                                 StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
             ctx->launches += 1;
         };
         const float *Xp = X ? X->hi : nullptr;
@@ -963,6 +986,7 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             Ushi = Y->hi;
             Uslo = Y->lo;
         }
+        if (sst != NOVA_OK) return sst;
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
@@ -1023,7 +1047,7 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
         }
         CK(cudaMemsetAsync(ctx->d_hist, 0, sizeof(double) * nsteps * NOVA_HIST_COLS, ctx->stream));
     }
-    CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_flag, 0, 2 * sizeof(int), ctx->stream));
     for (int n = 0; n < nsteps; n++) {
         // app/TG_Piosson/RKLoop.H (NS) or app/OT_Poisson/UEqn.H then BEqn.H (MHD)
         s = evolve(ctx, rd, mhd ? PHYS_MHD_U : PHYS_NS, st->U, mhd ? st->B : nullptr, st->p, rd->nu, rd->dt, rd->dt);
@@ -1050,10 +1074,11 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     if (hist && rd->diag_every > 0)
         CK(cudaMemcpyAsync(hist, ctx->d_hist, sizeof(double) * nsteps * NOVA_HIST_COLS, cudaMemcpyDeviceToHost,
                            ctx->stream));
-    int flag = 0;
-    CK(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    int flag[2] = {0, 0};
+    CK(cudaMemcpyAsync(flag, ctx->d_flag, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (flag) return fail(ctx, NOVA_E_NONFINITE, "nova_advance: non-finite value in the diagnostics");
+    if (flag[1]) return fail(ctx, NOVA_E_CUDA, "nova_advance: a stage kernel pipeline wait timed out");
+    if (flag[0]) return fail(ctx, NOVA_E_NONFINITE, "nova_advance: non-finite value in the diagnostics");
     return NOVA_OK;
 }
 
@@ -1070,10 +1095,13 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
     cudaStream_t st = ctx->stream;
     double *A = ctx->w64[2];
     const bool str = ctx->md.hyperbolic_z != 0;
+    nova_status sst = NOVA_OK;
     auto run = [&](int stage, const StageArgs64 &a) {
         ProfScope ps(ctx, NOVA_K_STAGE);
-        launch_stage64(PHYS_NS, stage, str, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, rd->nu,
-                       a, st);
+        const cudaError_t e = launch_stage64(PHYS_NS, stage, str, g, Walls<double>{}, ctx->co64, ctx->d_ia64,
+                                             ctx->d_corr64, rd->dt, rd->nu, a, st,
+                                             StageExec{ctx->stage_impl, ctx->d_flag + 1});
+        if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
         ctx->launches += 1;
     };
     run(0, StageArgs64{Uin, nullptr, nullptr, A, Y2});
@@ -1084,6 +1112,7 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
         return NOVA_OK;
     }
     run(3, StageArgs64{Y4, nullptr, nullptr, A, Uout});
+    if (sst != NOVA_OK) return sst;
     CKL("stage kernel");
     launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt, ctx->d_rhs,
                     st);
@@ -1133,6 +1162,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: U and gradU must be FP64 3-component fields");
     nova_status s = ensure_work(ctx, NOVA_F64);
     if (s != NOVA_OK) return s;
+    CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
     const int N = ad->nsteps, K = ad->checkpoint_every;
     const int nck = (N + K - 1) / K;
     const int mmax = K < N ? K : N;
@@ -1204,7 +1234,10 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         }
     }
     CK(cudaMemcpyAsync(gradU->d64, lam, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    int perr = 0;
+    CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (perr) return fail(ctx, NOVA_E_CUDA, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
     if (objective) *objective = row[2];
     if (!std::isfinite(row[2])) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
     return NOVA_OK;

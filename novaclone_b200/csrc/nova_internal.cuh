@@ -157,13 +157,34 @@ void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const doubl
                         const AdjArgs &a, cudaStream_t st);
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);
 
+// Which kernel runs the Navier-Stokes stage: STAGE_AUTO = the TMA pipeline
+// (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits), else the
+// register-queue march (nova_stage.cu); STAGE_MARCH / STAGE_TMA force one
+// (STAGE_TMA on a mesh that does not fit is an error).  err: device word
+// raised by a pipeline wait that timed out.
+enum StageImpl { STAGE_AUTO = 0, STAGE_MARCH = 1, STAGE_TMA = 2 };
+struct StageExec {
+    int impl;
+    int *err;
+};
+bool stage_tma_fits(const Geo &g);
+cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
+                               const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
+                               cudaStream_t st);
+cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
+                               const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
+                               cudaStream_t st);
+
 // stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum)
 // stretch: apply the stretched-z Laplacian term (Mesh "hypz:"); on uniform
 // meshes d2zdxi2 is round-off (|.| < 1e-9) and the term is skipped
-void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl, const Coef<double> &co,
-                    const double *ia, const double *corr2, double dt, double visc, const StageArgs64 &a,
-                    cudaStream_t st);
-void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl, const Coef<float> &co,
-                    const float *ia, const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st);
+// Returns cudaErrorNotSupported when STAGE_TMA is forced on a mesh it does not
+// fit, cudaErrorInvalidValue when a tensor map cannot be encoded.
+cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl,
+                           const Coef<double> &co, const double *ia, const double *corr2, double dt, double visc,
+                           const StageArgs64 &a, cudaStream_t st, const StageExec &ex);
+cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl,
+                           const Coef<float> &co, const float *ia, const float *corr2, float dt, float visc,
+                           const StageArgs32 &a, cudaStream_t st, const StageExec &ex);
 
 }  // namespace nova

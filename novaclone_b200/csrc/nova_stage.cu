@@ -30,6 +30,7 @@
 // The FP32-split variant keeps A as an FP32 sum of increments and adds it to
 // the (hi, lo) base in FP64 at the last stage.
 #include "nova_internal.cuh"
+#include "nova_stage_math.cuh"
 #include "nova_tile.cuh"
 
 #include <type_traits>
@@ -124,22 +125,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
             T rhs[3];
             if constexpr (PHYS == PHYS_NS) {
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
-                T adv[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, div = 0, duz[3] = {0, 0, 0};
-                auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        adv[c] += adv1<T, H>(v, c, d, u0[d], a);
-                        lap[c] += lsum<T, H>(v, c, b);
-                        if (STRETCH && zdir) duz[c] = d1<T, H>(v, c, a);
-                    }
-                    div += d1<T, H>(v, d, a);
-                };
-                dir(vx, 0, co.a[0], co.b[0], false);
-                dir(vy, 1, co.a[1], co.b[1], false);
-                dir(vz, 2, az, bz, true);
-#pragma unroll
-                for (int c = 0; c < 3; c++)
-                    rhs[c] = T(-0.5) * fma(u0[c], div, adv[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c]);
+                ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, iak, c2k, visc, rhs);
             } else if constexpr (PHYS == PHYS_MHD_U) {
                 // comps 0-2: U (stage state), 3-5: B (frozen)
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
@@ -196,56 +182,15 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
             }
 
             if constexpr (std::is_same<T, double>::value) {
-                // RK4a weights (src/settings/settings.cpp:44-50)
-                const double w6 = 1.0 / 6.0, w3 = 1.0 / 3.0;
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const long long o = (long long)c * g.N3 + idx;
-                    const double du = dt * rhs[c];
-                    const double y0 = q[H][c];
-                    if constexpr (STAGE == 4) {
-                        args.Ynext[o] = (((y0 + du * w6) + du * w3) + du * w3) + du * w6;
-                    } else if constexpr (STAGE == 0) {
-                        args.Ynext[o] = y0 + du * 0.5;
-                        args.A[o] = y0 + du * w6;
-                    } else if constexpr (STAGE == 1) {
-                        args.Ynext[o] = e0[c] + du * 0.5;
-                        args.A[o] = e1[c] + du * w3;
-                    } else if constexpr (STAGE == 2) {
-                        args.Ynext[o] = e0[c] + du * 1.0;
-                        args.A[o] = e1[c] + du * w3;
-                    } else {
-                        args.Ynext[o] = e1[c] + du * w6;
-                    }
-                }
+                for (int c = 0; c < 3; c++)
+                    rk_store64<STAGE>(args, (long long)c * g.N3 + idx, q[H][c], e0[c], e1[c], dt * rhs[c]);
             } else {
-                const float w6 = 1.0f / 6.0f, w3 = 1.0f / 3.0f;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const long long o = (long long)c * g.N3 + idx;
-                    const float du = dt * rhs[c];
-                    if constexpr (STAGE == 4) {
-                        const float inc = ((du * w6 + du * w3) + du * w3) + du * w6;
-                        const double x = ((double)q[H][c] + (double)args.U0lo[o]) + (double)inc;
-                        const float hi = (float)x;
-                        args.outhi[o] = hi;
-                        args.outlo[o] = (float)(x - (double)hi);
-                    } else if constexpr (STAGE == 0) {
-                        args.Ynext[o] = q[H][c] + du * 0.5f;
-                        args.A[o] = du * w6;
-                    } else if constexpr (STAGE == 1) {
-                        args.Ynext[o] = e0[c] + du * 0.5f;
-                        args.A[o] = e1[c] + du * w3;
-                    } else if constexpr (STAGE == 2) {
-                        args.Ynext[o] = e0[c] + du;
-                        args.A[o] = e1[c] + du * w3;
-                    } else {
-                        const float inc = e1[c] + du * w6;
-                        const double x = ((double)e0[c] + (double)args.U0lo[o]) + (double)inc;
-                        const float hi = (float)x;
-                        args.outhi[o] = hi;
-                        args.outlo[o] = (float)(x - (double)hi);
-                    }
+                    const float lo = (STAGE == 3 || STAGE == 4) ? args.U0lo[o] : 0.0f;
+                    rk_store32<STAGE>(args, o, q[H][c], e0[c], e1[c], lo, dt * rhs[c]);
                 }
             }
         });
@@ -306,17 +251,26 @@ void launch_stage_any(int phys, int stage, bool stretch, const Geo &g, const Wal
 
 }  // namespace
 
-void launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl, const Coef<double> &co,
-                    const double *ia, const double *corr2, double dt, double visc, const StageArgs64 &a,
-                    cudaStream_t st)
+cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl,
+                           const Coef<double> &co, const double *ia, const double *corr2, double dt, double visc,
+                           const StageArgs64 &a, cudaStream_t st, const StageExec &ex)
 {
+    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g))
+        return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
+    if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
     launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
+    return cudaSuccess;
 }
 
-void launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl, const Coef<float> &co,
-                    const float *ia, const float *corr2, float dt, float visc, const StageArgs32 &a, cudaStream_t st)
+cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl,
+                           const Coef<float> &co, const float *ia, const float *corr2, float dt, float visc,
+                           const StageArgs32 &a, cudaStream_t st, const StageExec &ex)
 {
+    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g))
+        return launch_stage_tma32(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
+    if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
     launch_stage_any<float>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
+    return cudaSuccess;
 }
 
 }  // namespace nova

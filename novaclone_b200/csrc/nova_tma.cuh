@@ -1,0 +1,89 @@
+// sm_100a primitives of the TMA-fed stage pipeline: mbarriers in shared
+// memory and tiled bulk tensor loads (cp.async.bulk.tensor, no multicast).
+//
+// Every wait is bounded: after kWaitLimitNs (or 2^26 polls) without the phase
+// completing, or when another thread has already raised the error word, the
+// wait sets *err = 1 and returns false, and the caller leaves its pipeline.
+#pragma once
+
+#include <cuda.h>
+#include <cstdint>
+
+namespace nova {
+
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// makes the initialised barriers visible to the async (TMA) proxy
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// wait for the phase of parity `parity` to complete; false on timeout or when
+// *err is already raised (abandon = true: ignore *err, used while draining)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err, bool abandon = false)
+{
+    if (mbar_test(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 1; it < (1u << 26); it++) {
+        if (mbar_test(bar, parity)) return true;
+        if ((it & 255u) == 0) {
+            if (!abandon && *(volatile int *)err) return false;
+            if (global_ns() - t0 > kWaitLimitNs) break;
+        }
+    }
+    atomicExch(err, 1);
+    return false;
+}
+
+// 4-D tiled load of the tensor map's box at (c0..c3) into shared memory at
+// dst; completion is signalled on bar as transaction bytes
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
+}  // namespace nova

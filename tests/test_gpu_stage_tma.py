@@ -1,0 +1,104 @@
+"""The TMA-pipelined Navier-Stokes stage kernel against the register-queue
+march (NOVA_STAGE_IMPL=tma / march, read when a mesh context is created).
+Both run the same point arithmetic, so whole runs must agree bit for bit; the
+march itself is pinned to the oracle by test_gpu_advance.py, and meshes of
+32^3 and up (periodic y, N2 % 32 == 0, N1 % 8 == 0, N1 >= 16) take the TMA
+path by default, so those oracle tests cover it directly too."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nova():
+    from novaclone_b200 import nova
+    return nova
+
+
+def mesh_with(nova, impl, N, **kw):
+    old = os.environ.get("NOVA_STAGE_IMPL")
+    os.environ["NOVA_STAGE_IMPL"] = impl
+    try:
+        return nova.Mesh(N, **kw)
+    finally:
+        if old is None:
+            del os.environ["NOVA_STAGE_IMPL"]
+        else:
+            os.environ["NOVA_STAGE_IMPL"] = old
+
+
+# (33, 16, 32): i chunks of 16, 16 and 1 plane; (10, 24, 64): one chunk, two k tiles,
+# three j tiles (both wrap cases and an interior tile); (40, 16, 96): three k tiles
+SIZES = [(33, 16, 32), (10, 24, 64), (40, 16, 96)]
+
+
+def run(nova, impl, N, U0, prec, rk_mode, steps=3, **mesh_kw):
+    GM = mesh_with(nova, impl, N, **mesh_kw)
+    U = nova.Field(GM, 3, prec).upload_soa(U0)
+    p = nova.Field(GM, 1)
+    nova.advance(GM, nova.run_desc(model="ns", rk_mode=rk_mode, precision=prec, dt=2e-3, nu=0.01), U, p,
+                 nsteps=steps)
+    return U.download_soa(), p.download_soa()
+
+
+@pytest.mark.parametrize("N", SIZES)
+@pytest.mark.parametrize("rk_mode", ["classical", "literal"])
+def test_tma_equals_march_fp64(nova, N, rk_mode):
+    U0 = 0.3 * np.random.default_rng(5).standard_normal((3,) + N)
+    a = run(nova, "tma", N, U0, nova.F64, rk_mode)
+    b = run(nova, "march", N, U0, nova.F64, rk_mode)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("N", SIZES[:2])
+@pytest.mark.parametrize("rk_mode", ["classical", "literal"])
+def test_tma_equals_march_fp32_split(nova, N, rk_mode):
+    U0 = 0.3 * np.random.default_rng(6).standard_normal((3,) + N)
+    a = run(nova, "tma", N, U0, nova.F32SPLIT, rk_mode)
+    b = run(nova, "march", N, U0, nova.F32SPLIT, rk_mode)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_tma_equals_march_stretched_z(nova):
+    N, kw = (12, 16, 64), dict(L=(2 * np.pi, 2 * np.pi, 1.0), hyperbolic_z=(0.01, 0.01))
+    U0 = 0.3 * np.random.default_rng(7).standard_normal((3,) + N)
+    a = run(nova, "tma", N, U0, nova.F64, "classical", **kw)
+    b = run(nova, "march", N, U0, nova.F64, "classical", **kw)
+    assert np.array_equal(a[0], b[0])
+
+
+def test_tma_taylor_green_vs_oracle(nova, oracle):
+    N = (16, 16, 32)
+    OM = oracle.Mesh(N)
+    U0 = oracle.ic_taylor_green(OM)
+    got, _ = run(nova, "tma", N, U0, nova.F64, "classical", steps=4)
+    r = oracle.run(OM, OM.to_ghosted(U0), model="ns", rk_mode="classical", nsteps=4, dt=2e-3, nu=0.01)
+    ref = OM.unique(r[0])
+    for c in range(2):
+        assert rel_l2(got[c], ref[c]) < 1e-11
+
+
+def test_adjoint_through_tma_equals_march(nova):
+    N = (16, 16, 32)
+    U0 = 0.2 * np.random.default_rng(9).standard_normal((3,) + N)
+    out = []
+    for impl in ("tma", "march"):
+        GM = mesh_with(nova, impl, N)
+        J, grad = nova.adjoint_grad(GM, nova.run_desc(model="ns", dt=2e-3, nu=0.01), nova.Field(GM, 3).upload_soa(U0),
+                                    nsteps=4, checkpoint_every=2)
+        out.append((J, grad.download_soa()))
+    assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+
+
+def test_forcing_tma_on_a_mesh_it_does_not_fit_is_refused(nova):
+    GM = mesh_with(nova, "tma", (16, 12, 8))
+    U = nova.Field(GM, 3).upload_soa(np.zeros((3, 16, 12, 8)))
+    p = nova.Field(GM, 1)
+    with pytest.raises(nova.NovaError) as e:
+        nova.advance(GM, nova.run_desc(model="ns", dt=1e-3), U, p, nsteps=1)
+    assert e.value.status == nova.E_UNSUPPORTED
