@@ -334,7 +334,7 @@ nova_status stage_fail(nova_ctx *ctx, cudaError_t e)
 {
     if (e == cudaErrorNotSupported)
         return fail(ctx, NOVA_E_UNSUPPORTED,
-                    "NOVA_STAGE_IMPL=tma: the TMA stage kernel needs periodic y, N2 % 32 == 0, N1 % 8 == 0 and N1 >= 16");
+                    "NOVA_STAGE_IMPL=tma: the TMA stage kernel needs periodic y, N2 % 32 == 0 and N1 a multiple of 16 (FP64) or 8 (FP32), at least twice that");
     if (e == cudaErrorInvalidValue) return fail(ctx, NOVA_E_CUDA, "stage kernel: cuTensorMapEncodeTiled failed");
     return cuda_check(ctx, e, "stage kernel");
 }

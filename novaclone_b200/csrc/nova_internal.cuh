@@ -64,6 +64,25 @@ template <typename T> struct Coef {
     T b2[3];
 };
 
+// Per-launch weights of the fused advection-diffusion sum of the Navier-Stokes
+// stage (nova_stage_math.cuh): ha = a/2 per direction, vb = visc * b for x and
+// y (the z weights are scaled per node by the metric).
+template <typename T> struct StageCoef {
+    T ha[3][4];
+    T vb[2][4];
+};
+
+template <typename T> inline StageCoef<T> stage_coef(const Coef<T> &co, T visc)
+{
+    StageCoef<T> s{};
+    for (int d = 0; d < 3; d++)
+        for (int l = 0; l < 4; l++) {
+            s.ha[d][l] = co.a[d][l] * T(0.5);
+            if (d < 2) s.vb[d][l] = visc * co.b[d][l];
+        }
+    return s;
+}
+
 __host__ __device__ inline int wrapi(int x, int n)
 {
     int r = x % n;
@@ -158,7 +177,9 @@ void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const doubl
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);
 
 // Which kernel runs the Navier-Stokes stage: STAGE_AUTO = the TMA pipeline
-// (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits), else the
+// (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits: periodic y,
+// N2 % 32 == 0, N1 a multiple of the tile height 16 (FP64) or 8 (FP32) and
+// at least twice it), else the
 // register-queue march (nova_stage.cu); STAGE_MARCH / STAGE_TMA force one
 // (STAGE_TMA on a mesh that does not fit is an error).  err: device word
 // raised by a pipeline wait that timed out.
@@ -167,7 +188,7 @@ struct StageExec {
     int impl;
     int *err;
 };
-bool stage_tma_fits(const Geo &g);
+bool stage_tma_fits(const Geo &g, bool fp64);
 cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
                                const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
                                cudaStream_t st);

@@ -56,8 +56,8 @@ namespace {
 
 template <typename T, int H, int PHYS, int STAGE, bool STRETCH, bool WALLS, class Args>
 __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo g, Walls<T> wl, Coef<T> co,
-                                                      const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
-                                                      T visc, Args args, int ichunk)
+                                                      StageCoef<T> sc, const T *__restrict__ ia,
+                                                      const T *__restrict__ corr2, T dt, T visc, Args args, int ichunk)
 {
     constexpr int NC = (PHYS == PHYS_NS) ? 3 : 6;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
             T rhs[3];
             if constexpr (PHYS == PHYS_NS) {
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
-                ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, iak, c2k, visc, rhs);
+                ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
             } else if constexpr (PHYS == PHYS_MHD_U) {
                 // comps 0-2: U (stage state), 3-5: B (frozen)
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
@@ -212,7 +212,7 @@ void launch_one(const Geo &g, const Walls<T> &wl, const Coef<T> &co, const T *ia
     }
     const int bps = stage_minb<T, PHYS>();
     const int ch = pick_ichunk(g, bps);
-    kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, wl, co, ia, corr2, dt, visc, a, ch);
+    kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, wl, co, stage_coef(co, visc), ia, corr2, dt, visc, a, ch);
 }
 
 template <typename T, int PHYS, bool STRETCH, bool WALLS, class Args>
@@ -255,7 +255,7 @@ cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, cons
                            const Coef<double> &co, const double *ia, const double *corr2, double dt, double visc,
                            const StageArgs64 &a, cudaStream_t st, const StageExec &ex)
 {
-    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g))
+    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g, true))
         return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
     if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
     launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
@@ -266,7 +266,7 @@ cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, cons
                            const Coef<float> &co, const float *ia, const float *corr2, float dt, float visc,
                            const StageArgs32 &a, cudaStream_t st, const StageExec &ex)
 {
-    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g))
+    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g, false))
         return launch_stage_tma32(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
     if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
     launch_stage_any<float>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);

@@ -15,34 +15,72 @@
 
 namespace nova {
 
+// One direction of the fused sum  -1/2 A_d(U,U)_c + visc * lsum_d(U_c),
+// accumulated onto s[c]:
+//   s[c] += sum_l [ U_c(+l) W+_l + U_c(-l) W-_l ],
+//   W+_l = -a_l/2 (U_d(+l) + U_d(0)) + vb_l,   W-_l = a_l/2 (U_d(-l) + U_d(0)) + vb_l
+// The weights depend on the direction only, so the three components share
+// them: one product per neighbour instead of one for the advective and one for
+// the diffusive term.  dd += D_d U_d (the divergence term).
+template <typename T, int H, class V>
+__device__ __forceinline__ void ns_dir(const V &v, int d, T v0, const T *ha, const T *a, const T (&vb)[H], T (&s)[3],
+                                       T &dd)
+{
+    T wp[H], wm[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) {
+        const T p = v(d, l + 1), m = v(d, -l - 1);
+        wp[l] = fma(-ha[l], p + v0, vb[l]);
+        wm[l] = fma(ha[l], m + v0, vb[l]);
+        dd = fma(a[l], p - m, dd);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        T r = s[c];
+#pragma unroll
+        for (int l = 0; l < H; l++) {
+            r = fma(v(c, l + 1), wp[l], r);
+            r = fma(v(c, -l - 1), wm[l], r);
+        }
+        s[c] = r;
+    }
+}
+
 // vx/vy/vz(c, s): component c at offset s along i, j, k; u0 = U at the node;
-// iak = 1/dzdxi(k): the z sums run with the uniform weights co.a[2], co.b[2]
-// and are scaled by iak (first derivatives) or iak^2 (the Laplacian) once,
-// which keeps the per-thread z weights out of the registers
+// iak = 1/dzdxi(k): the z weights are a_l iak and b_l iak^2, applied as the
+// uniform weights with vb = visc iak b_l and the z sum scaled by iak (it is
+// evaluated first), so no per-node weight tables live in registers.
+// Algebraically the skew form and Laplacian above; rounding differs from the
+// term-by-term order at the level of a few ulps of the largest term.
 template <typename T, int H, bool STRETCH, class VX, class VY, class VZ>
 __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&u0)[3], const Coef<T> &co,
-                                       T iak, T c2k, T visc, T (&rhs)[3])
+                                       const StageCoef<T> &sc, T iak, T c2k, T visc, T (&rhs)[3])
 {
-    T adv[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, div = 0;
+    T s[3] = {0, 0, 0}, dv = 0;
+    {
+        T vb[H];
+        const T viak = visc * iak;
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = viak * co.b[2][l];
+        ns_dir<T, H>(vz, 2, u0[2], sc.ha[2], co.a[2], vb, s, dv);
+#pragma unroll
+        for (int c = 0; c < 3; c++) s[c] *= iak;
+        dv *= iak;
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = sc.vb[0][l];
+        ns_dir<T, H>(vx, 0, u0[0], sc.ha[0], co.a[0], vb, s, dv);
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = sc.vb[1][l];
+        ns_dir<T, H>(vy, 1, u0[1], sc.ha[1], co.a[1], vb, s, dv);
+    }
+    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * (iak * iak);
+    const T K = fma(T(-0.5), dv, -visc * bsum);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        adv[c] = adv1<T, H>(vx, c, 0, u0[0], co.a[0]) + adv1<T, H>(vy, c, 1, u0[1], co.a[1]);
-        lap[c] = lsum<T, H>(vx, c, co.b[0]) + lsum<T, H>(vy, c, co.b[1]);
+        T r = s[c];
+        if (STRETCH) r = fma(-visc * c2k, iak * d1<T, H>(vz, c, co.a[2]), r);
+        rhs[c] = fma(u0[c], K, r);
     }
-    div = d1<T, H>(vx, 0, co.a[0]) + d1<T, H>(vy, 1, co.a[1]);
-    const T iak2 = iak * iak;
-    T duz[3] = {0, 0, 0};
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        adv[c] = fma(iak, adv1<T, H>(vz, c, 2, u0[2], co.a[2]), adv[c]);
-        lap[c] = fma(iak2, lsum<T, H>(vz, c, co.b[2]), lap[c]);
-        if (STRETCH) duz[c] = iak * d1<T, H>(vz, c, co.a[2]);
-    }
-    div = fma(iak, d1<T, H>(vz, 2, co.a[2]), div);
-    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak2;
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-        rhs[c] = T(-0.5) * fma(u0[c], div, adv[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c]);
 }
 
 // Stage update of one component at node o (classical RK4 of

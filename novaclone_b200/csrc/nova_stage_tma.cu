@@ -2,29 +2,29 @@
 //
 // Same arithmetic and stage update as the register-queue march of
 // nova_stage.cu (nova_stage_math.cuh), different data movement.  A block owns
-// a kTK(k) x kTJ(j) column of the grid and walks it along i.  For every plane
-// one elected thread issues bulk tensor loads of
+// a kTK(k) x TJ(j) column of the grid and walks it along i.  A producer warp
+// issues, for every plane, bulk tensor loads of
 //   TCB: the tile's rows plus H halo rows on either side, all three
-//        components, laid out [row][c][k] (box 32 x 3 x 14), and
+//        components, laid out [row][c][k] (box 32 x 3 x (TJ + 6)), and
 //   L/R: the H-wide k halos left and right of the tile (boxes 4 x 8 x 3,
 //        [c][j][k], 4 wide to keep the 16-byte TMA alignment),
 // into a ring of kRing shared-memory slots, each completed by an mbarrier
 // transaction count, and the pointwise epilogue operands of the plane (RK base
-// and accumulator, box 32 x 3 x 8) into a second ring.  Periodic wrap needs
+// and accumulator, box 32 x 3 x TJ) into a second ring.  Periodic wrap needs
 // no ghost storage: in k the halo boxes start at the wrapped column (the tile
-// width divides N2), in j a boundary tile's rows arrive as two boxes (3 + 11
-// rows) that land back to back in the slot.
+// width divides N2), in j a boundary tile's rows arrive as two boxes (3 and
+// TJ + 3 rows) that land back to back in the slot.
 //
-// The consumer threads keep the i stencil in a register queue (the centre of
+// The consumer warps keep the i stencil in a register queue (the centre of
 // each arriving plane), read the j and k stencils from the slot of the plane
 // they are computing, and hand slots back through per-warp arrivals on the
-// slot's `empty` barrier.  The producer runs kLookS planes ahead of the queue
-// head (kLookS + H ahead of the plane being computed), so HBM latency is
-// covered by the ring instead of by the math of one plane.
+// slot's `empty` barrier; the producer refills a slot as soon as every warp
+// has released it, which keeps kRing - 2H - 1 planes in flight ahead of the
+// queue head.
 //
 // Every mbarrier wait is bounded (nova_tma.cuh); a wait that gives up raises
-// the error word and the block leaves its pipeline after the elected thread
-// has waited, again bounded, for the loads it still has in flight.
+// the error word and the block leaves its pipeline, the producer after waiting,
+// again bounded, for the loads it still has in flight.
 #include "nova_internal.cuh"
 #include "nova_stage_math.cuh"
 #include "nova_tile.cuh"
@@ -39,19 +39,28 @@ namespace nova {
 namespace {
 
 constexpr int kH = 3;
-constexpr int kRing = 6;   // stencil slots: planes p .. p+5 live at step p
-constexpr int kLookS = 2;  // stencil loads issued ahead of the queue head
-constexpr int kERing = 3;  // epilogue slots
-constexpr int kLookE = 2;  // epilogue loads issued ahead of the plane computed
-constexpr int kWarps = kThreads / 32;
-constexpr int kRowE = 3 * kTK;            // one halo'd row, three components
-constexpr int kTcbE = (kTJ + 2 * kH) * kRowE;
-constexpr int kLRE = 3 * kTJ * 4;         // one k-halo box
-constexpr int kSlotE = kTcbE + 2 * kLRE;  // elements per stencil slot
-constexpr int kEpiE = kTJ * kRowE;        // elements per epilogue field
-static_assert(kRing >= kLookS + 2 * kH - 2, "a slot is reused only after its plane was computed");
-static_assert(kERing >= kLookE + 1, "an epilogue slot is reused only after its plane was stored");
-static_assert(kTJ * 4 == kTK, "k-halo boxes share the component stride of the row boxes");
+constexpr int kRowE = 3 * kTK;  // one halo'd row, three components
+constexpr int kLRB = 8;         // rows of one k-halo box
+
+// Tile and ring configuration per precision.  FP64: a 32 x 16 tile, one block
+// per SM; FP32: a 32 x 8 tile, three blocks per SM.  Each block has one
+// consumer warp per tile row and one producer warp, whose elected lane issues
+// the loads in the order the consumers need them and blocks on the ring's
+// `empty` barriers alone, so it never delays the arithmetic.
+template <typename T> struct TmaCfg {
+    static constexpr int TJ = sizeof(T) == 8 ? 16 : 8;
+    static constexpr int kWarps = TJ;                  // consumer warps (one per tile row)
+    static constexpr int kThreads = kTK * (TJ + 1);    // plus the producer warp
+    static constexpr int kBlocksPerSM = sizeof(T) == 8 ? 1 : 3;
+    static constexpr int kRing = 7;   // stencil slots: the queue head runs kRing - 2H - 1 planes behind the loads
+    static constexpr int kERing = 3;  // epilogue slots
+    static constexpr int kTcbE = (TJ + 2 * kH) * kRowE;
+    static constexpr int kLRE = 3 * TJ * 4;           // the k-halo boxes of one side
+    static constexpr int kSlotE = kTcbE + 2 * kLRE;   // elements per stencil slot
+    static constexpr int kEpiE = TJ * kRowE;          // elements per epilogue field
+    static_assert(kRing >= 2 * kH + 1, "the queue and the plane computed fit in the ring");
+    static_assert(TJ % kLRB == 0 && kLRB * 4 == kTK, "k-halo boxes share the component stride of the row boxes");
+};
 
 // epilogue operands per stage, in load order
 //   FP64:  s=1,2: U0, A   s=3: A
@@ -66,45 +75,47 @@ template <typename T, int STAGE> __host__ __device__ constexpr int epi_fields()
 
 template <typename T, int NE> constexpr size_t tma_smem_bytes()
 {
-    return ((size_t)kRing * kSlotE + (size_t)kERing * NE * kEpiE) * sizeof(T) + 8 * (2 * kRing + 2 * kERing);
+    using C = TmaCfg<T>;
+    return ((size_t)C::kRing * C::kSlotE + (size_t)C::kERing * NE * C::kEpiE) * sizeof(T) +
+           8 * (2 * C::kRing + 2 * C::kERing);
 }
 
 struct StageMaps {
-    CUtensorMap tcb14, tcb3, tcb11;  // halo'd rows of the stencil field: 14, 3 or 11 rows
-    CUtensorMap lr;                  // k-halo boxes of the stencil field
-    CUtensorMap e[3];                // epilogue operands
+    CUtensorMap tcbA, tcb3, tcbB;  // halo'd rows of the stencil field: TJ+6, 3 or TJ+3 rows
+    CUtensorMap lr;                // k-halo boxes (4 x 8 x 3) of the stencil field
+    CUtensorMap e[3];              // epilogue operands
 };
 
-template <typename T, int STAGE>
+template <typename T, int STAGE, int EPI_E>
 __device__ __forceinline__ void epi_read(const T *se, int c, T &e0, T &e1, T &lo)
 {
     if constexpr (STAGE == 1 || STAGE == 2) {
         e0 = se[c * kTK];
-        e1 = se[kEpiE + c * kTK];
+        e1 = se[EPI_E + c * kTK];
     } else if constexpr (STAGE == 3) {
         if constexpr (sizeof(T) == 8) {
             e1 = se[c * kTK];
         } else {
             e0 = se[c * kTK];
-            e1 = se[kEpiE + c * kTK];
-            lo = se[2 * kEpiE + c * kTK];
+            e1 = se[EPI_E + c * kTK];
+            lo = se[2 * EPI_E + c * kTK];
         }
     } else if constexpr (STAGE == 4 && sizeof(T) == 4) {
         lo = se[c * kTK];
     }
 }
 
-// resident blocks per SM: FP64 two (registers), FP32 three (shared memory of the rings)
-template <typename T> __host__ __device__ constexpr int tma_blocks_per_sm() { return sizeof(T) == 8 ? 2 : 3; }
-
 template <typename T, int STAGE, bool STRETCH, class Args>
-__global__ void __launch_bounds__(kThreads, tma_blocks_per_sm<T>())
-    k_stage_tma(Geo g, Coef<T> co, const T *__restrict__ ia, const T *__restrict__ corr2, T dt, T visc, Args args,
-                const __grid_constant__ StageMaps maps, int ichunk, int *err)
+__global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
+    k_stage_tma(Geo g, Coef<T> co, StageCoef<T> sc, const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
+                T visc, Args args, const __grid_constant__ StageMaps maps, int ichunk, int *err)
 {
-    constexpr int H = kH;
+    using C = TmaCfg<T>;
+    constexpr int H = kH, TJ = C::TJ, kRing = C::kRing, kERing = C::kERing;
+    constexpr int kTcbE = C::kTcbE, kLRE = C::kLRE, kSlotE = C::kSlotE, kEpiE = C::kEpiE;
     constexpr int NE = epi_fields<T, STAGE>();
     constexpr uint32_t kSlotBytes = kSlotE * sizeof(T), kRowBytes = kRowE * sizeof(T), kEpiBytes = kEpiE * sizeof(T);
+    constexpr uint32_t kLRBoxBytes = 3 * kLRB * 4 * sizeof(T);
     extern __shared__ __align__(128) unsigned char smraw[];
     const T *ring = reinterpret_cast<const T *>(smraw);
     const T *ering = ring + kRing * kSlotE;
@@ -116,100 +127,104 @@ __global__ void __launch_bounds__(kThreads, tma_blocks_per_sm<T>())
     auto efull = [&](int r) { return bar0 + 8u * (2 * kRing + r); };
     auto eempty = [&](int r) { return bar0 + 8u * (2 * kRing + kERing + r); };
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTK + tx, lane = tid & 31;
-    const bool lead = tid == 0;
-    const int k0 = blockIdx.x * kTK, j0 = blockIdx.y * kTJ;
+    const int tx = threadIdx.x, ty = threadIdx.y, lane = tx;
+    const int k0 = blockIdx.x * kTK, j0 = blockIdx.y * TJ;
     const int ib = blockIdx.z * ichunk, ie = min(ib + ichunk, g.N0);
     const int nout = ie - ib, nld = nout + 2 * H;
 
-    if (lead) {
+    if (ty == TJ && lane == 0) {
         for (int r = 0; r < kRing; r++) {
             mbar_init(full(r), 1);
-            mbar_init(empty(r), kWarps);
+            mbar_init(empty(r), C::kWarps);
         }
         for (int r = 0; r < kERing; r++) {
             mbar_init(efull(r), 1);
-            mbar_init(eempty(r), kWarps);
+            mbar_init(eempty(r), C::kWarps);
         }
         mbar_init_fence();
     }
     __syncthreads();
 
-    // ---- producer (the elected thread) ----
-    const bool jlo = j0 < H, jhi = j0 + kTJ + H > g.N1;
-    const int kl = (k0 == 0 ? g.N2 : k0) - 4, kr = (k0 + kTK == g.N2) ? 0 : k0 + kTK;
-    int iss = 0, ise = 0;  // loads issued
-    bool ok = true;
-    auto issue_s = [&](int n) -> bool {  // stencil load n: plane ib - H + n
-        const int r = n % kRing;
-        if (n >= kRing && !mbar_wait(empty(r), ((n / kRing) + 1) & 1, err)) return false;
-        const uint32_t dst = s0 + r * kSlotBytes, bar = full(r);
-        mbar_expect_tx(bar, kSlotBytes);
-        const int plane = wrapi(ib - H + n, g.N0);
-        if (jlo) {
-            tma_load_4d(dst, &maps.tcb3, bar, k0, 0, g.N1 - H, plane);
-            tma_load_4d(dst + H * kRowBytes, &maps.tcb11, bar, k0, 0, 0, plane);
-        } else if (jhi) {
-            tma_load_4d(dst, &maps.tcb11, bar, k0, 0, j0 - H, plane);
-            tma_load_4d(dst + (kTJ + H) * kRowBytes, &maps.tcb3, bar, k0, 0, 0, plane);
-        } else {
-            tma_load_4d(dst, &maps.tcb14, bar, k0, 0, j0 - H, plane);
-        }
-        tma_load_4d(dst + kTcbE * sizeof(T), &maps.lr, bar, kl, j0, 0, plane);
-        tma_load_4d(dst + (kTcbE + kLRE) * sizeof(T), &maps.lr, bar, kr, j0, 0, plane);
-        return true;
-    };
-    auto issue_e = [&](int n) -> bool {  // epilogue load n: plane ib + n
-        const int r = n % kERing;
-        if (n >= kERing && !mbar_wait(eempty(r), ((n / kERing) + 1) & 1, err)) return false;
-        const uint32_t dst = e0addr + r * NE * kEpiBytes, bar = efull(r);
-        mbar_expect_tx(bar, NE * kEpiBytes);
-#pragma unroll
-        for (int f = 0; f < NE; f++) tma_load_4d(dst + f * kEpiBytes, &maps.e[f], bar, k0, 0, j0, ib + n);
-        return true;
-    };
-    auto produce = [&](int s_upto, int e_upto) {
-        while (ok && iss < min(s_upto, nld)) {
-            if (issue_s(iss)) iss++; else ok = false;
-        }
-        if constexpr (NE > 0) {
-            while (ok && ise < min(e_upto, nout)) {
-                if (issue_e(ise)) ise++; else ok = false;
+    // ---- producer warp: lane 0 issues every load of the block ----
+    if (ty == TJ) {
+        if (lane != 0) return;
+        const bool jlo = j0 < H, jhi = j0 + TJ + H > g.N1;
+        const int kl = (k0 == 0 ? g.N2 : k0) - 4, kr = (k0 + kTK == g.N2) ? 0 : k0 + kTK;
+        auto issue_s = [&](int n) -> bool {  // stencil load n: plane ib - H + n
+            const int r = n % kRing;
+            if (n >= kRing && !mbar_wait(empty(r), ((n / kRing) + 1) & 1, err)) return false;
+            const uint32_t dst = s0 + r * kSlotBytes, bar = full(r);
+            mbar_expect_tx(bar, kSlotBytes);
+            const int plane = wrapi(ib - H + n, g.N0);
+            if (jlo) {
+                tma_load_4d(dst, &maps.tcb3, bar, k0, 0, g.N1 - H, plane);
+                tma_load_4d(dst + H * kRowBytes, &maps.tcbB, bar, k0, 0, 0, plane);
+            } else if (jhi) {
+                tma_load_4d(dst, &maps.tcbB, bar, k0, 0, j0 - H, plane);
+                tma_load_4d(dst + (TJ + H) * kRowBytes, &maps.tcb3, bar, k0, 0, 0, plane);
+            } else {
+                tma_load_4d(dst, &maps.tcbA, bar, k0, 0, j0 - H, plane);
             }
+#pragma unroll
+            for (int b = 0; b < TJ / kLRB; b++) {
+                tma_load_4d(dst + kTcbE * sizeof(T) + b * kLRBoxBytes, &maps.lr, bar, kl, j0 + b * kLRB, 0, plane);
+                tma_load_4d(dst + (kTcbE + kLRE) * sizeof(T) + b * kLRBoxBytes, &maps.lr, bar, kr, j0 + b * kLRB, 0,
+                            plane);
+            }
+            return true;
+        };
+        auto issue_e = [&](int n) -> bool {  // epilogue load n: plane ib + n
+            const int r = n % kERing;
+            if (n >= kERing && !mbar_wait(eempty(r), ((n / kERing) + 1) & 1, err)) return false;
+            const uint32_t dst = e0addr + r * NE * kEpiBytes, bar = efull(r);
+            mbar_expect_tx(bar, NE * kEpiBytes);
+#pragma unroll
+            for (int f = 0; f < NE; f++) tma_load_4d(dst + f * kEpiBytes, &maps.e[f], bar, k0, 0, j0, ib + n);
+            return true;
+        };
+        // in the order of need: stencil load t + 2H is the queue head of step t,
+        // epilogue load t is read at step t
+        int iss = 0, ise = 0;
+        bool ok = true;
+        for (int t = -2 * H; t < nout && ok; t++) {
+            if ((ok = issue_s(t + 2 * H))) iss++;
+            if (NE > 0 && ok && t >= 0 && (ok = issue_e(t))) ise++;
         }
-    };
+        if (!ok) {
+            // the consumers may have left: wait, bounded, for the loads still landing in shared memory
+            for (int n = max(0, iss - kRing); n < iss; n++) mbar_wait(full(n % kRing), (n / kRing) & 1, err, true);
+            for (int n = max(0, ise - kERing); n < ise; n++)
+                mbar_wait(efull(n % kERing), (n / kERing) & 1, err, true);
+        }
+        return;
+    }
+
+    // ---- consumer warps ----
     auto release = [&](uint32_t bar) {
         __syncwarp();
         if (lane == 0) mbar_arrive(bar);
     };
-
-    // ---- consumers (all threads) ----
     const int kw = k0 + tx;
     const T iak = ia[kw];
     const T c2k = STRETCH ? corr2[kw] : T(0);
 
-    // slot offsets: centre, and the k neighbours at s = -3..-1, 1..3 (inside
-    // the row box or in the left/right halo box); component stride kTK in both
+    // slot offsets: centre, and the k neighbour at s (inside the row box or in
+    // the left/right halo boxes, [box][c][8 rows][4]); component stride kTK in both
     const int cen = (H + ty) * kRowE + tx;
-    int oz[2 * H];
-#pragma unroll
-    for (int u = 0; u < 2 * H; u++) {
-        const int s = u < H ? u - H : u - H + 1;
+    const int lrrow = (ty / kLRB) * 3 * kLRB * 4 + (ty % kLRB) * 4;
+    auto zoff = [&](int s) -> int {
         const int x = tx + s;
-        oz[u] = x < 0 ? kTcbE + ty * 4 + 4 + x : (x >= kTK ? kTcbE + kLRE + ty * 4 + (x - kTK) : cen + s);
-    }
+        return x < 0 ? kTcbE + lrrow + 4 + x : (x >= kTK ? kTcbE + kLRE + lrrow + (x - kTK) : cen + s);
+    };
 
     T q[2 * H + 1][3];
-    int cs = 0, ce = 0;  // loads waited for (the elected thread's drain bound)
-    if (lead) produce(kLookS + 1, kLookE);
+    bool ok = true;
     for (int n = 0; n < 2 * H; n++) {  // queue: planes ib-3 .. ib+2
-        if (lead) produce(n + kLookS + 1, kLookE);
-        ok = ok && mbar_wait(full(n % kRing), (n / kRing) & 1, err);
+        ok = mbar_wait(full(n % kRing), (n / kRing) & 1, err);
         if (!__all_sync(0xffffffffu, ok)) {
             ok = false;
             break;
         }
-        cs = n + 1;
         const T *sl = ring + (n % kRing) * kSlotE;
 #pragma unroll
         for (int c = 0; c < 3; c++) q[n + 1][c] = sl[cen + c * kTK];
@@ -218,13 +233,11 @@ __global__ void __launch_bounds__(kThreads, tma_blocks_per_sm<T>())
 
     for (int p = 0; p < nout && ok; p++) {
         const int hd = p + 2 * H;  // queue head: plane ib + p + 3
-        if (lead) produce(hd + kLookS + 1, p + kLookE + 1);
-        ok = ok && mbar_wait(full(hd % kRing), (hd / kRing) & 1, err);
+        ok = mbar_wait(full(hd % kRing), (hd / kRing) & 1, err);
         if (!__all_sync(0xffffffffu, ok)) {
             ok = false;
             break;
         }
-        cs = hd + 1;
 #pragma unroll
         for (int s = 0; s < 2 * H; s++)
 #pragma unroll
@@ -240,24 +253,21 @@ __global__ void __launch_bounds__(kThreads, tma_blocks_per_sm<T>())
         const T *sl = ring + (cur % kRing) * kSlotE;
         auto vx = [&](int c, int s) -> T { return q[H + s][c]; };
         auto vy = [&](int c, int s) -> T { return sl[cen + s * kRowE + c * kTK]; };
-        auto vz = [&](int c, int s) -> T {
-            return s == 0 ? sl[cen + c * kTK] : sl[oz[s < 0 ? s + H : s + H - 1] + c * kTK];
-        };
+        auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
         const T u0[3] = {q[H][0], q[H][1], q[H][2]};
         T rhs[3];
-        ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, iak, c2k, visc, rhs);
+        ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
 
         T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
         if constexpr (NE > 0) {
-            ok = ok && mbar_wait(efull(p % kERing), (p / kERing) & 1, err);
+            ok = mbar_wait(efull(p % kERing), (p / kERing) & 1, err);
             if (!__all_sync(0xffffffffu, ok)) {
                 ok = false;
                 break;
             }
-            ce = p + 1;
             const T *se = ering + (p % kERing) * NE * kEpiE + ty * kRowE + tx;
 #pragma unroll
-            for (int c = 0; c < 3; c++) epi_read<T, STAGE>(se, c, e0[c], e1[c], lo[c]);
+            for (int c = 0; c < 3; c++) epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
         }
         const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
 #pragma unroll
@@ -272,11 +282,6 @@ __global__ void __launch_bounds__(kThreads, tma_blocks_per_sm<T>())
         release(empty(cur % kRing));
     }
 
-    if (lead && !ok) {
-        // loads issued but not waited for are still landing in this block's shared memory
-        for (int n = cs; n < iss; n++) mbar_wait(full(n % kRing), (n / kRing) & 1, err, true);
-        for (int n = ce; n < ise; n++) mbar_wait(efull(n % kERing), (n / kERing) & 1, err, true);
-    }
 }
 
 // ------------------------------------------------------------------ host --
@@ -300,8 +305,8 @@ template <typename T> constexpr CUtensorMapDataType tmap_type()
     return sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
 }
 
-// a 3-component field [c][i][j][k]; rows != 0: dims (k, c, j, i), box kTK x 3 x rows;
-// rows == 0: dims (k, j, c, i), box 4 x kTJ x 3 (the k halos)
+// a 3-component field [c][i][j][k]; rows != 0: dims (k, c, j, i), box kTK x 3 x rows x 1;
+// rows == 0: dims (k, j, c, i), box 4 x kLRB x 3 x 1 (the k halos)
 template <typename T> bool encode(CUtensorMap *m, const T *base, const Geo &g, unsigned rows)
 {
     EncodeFn fn = encode_fn();
@@ -317,12 +322,23 @@ template <typename T> bool encode(CUtensorMap *m, const T *base, const Geo &g, u
     } else {
         const cuuint64_t d[4] = {(cuuint64_t)g.N2, (cuuint64_t)g.N1, 3, (cuuint64_t)g.N0};
         const cuuint64_t s[3] = {(cuuint64_t)g.N2 * es, (cuuint64_t)g.N3 * es, (cuuint64_t)g.N12 * es};
-        const cuuint32_t b[4] = {4, (cuuint32_t)kTJ, 3, 1};
+        const cuuint32_t b[4] = {4, (cuuint32_t)kLRB, 3, 1};
         memcpy(dims, d, sizeof d), memcpy(strides, s, sizeof s), memcpy(box, b, sizeof b);
     }
     return fn(m, tmap_type<T>(), 4, const_cast<T *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// i-chunk of a TMA stage launch: >= ~4 waves of resident blocks, the 2H-plane
+// warm-up kept small against the chunk length
+template <typename T> int tma_ichunk(const Geo &g)
+{
+    using C = TmaCfg<T>;
+    const long long tiles = (long long)(g.N2 / kTK) * (g.N1 / C::TJ);
+    int ch = g.N0;
+    while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * C::kBlocksPerSM * 4) ch /= 2;
+    return ch;
 }
 
 template <typename T, int STAGE, bool STRETCH, class Args>
@@ -332,9 +348,10 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     constexpr int NE = epi_fields<T, STAGE>();
     StageMaps maps;
     memset(&maps, 0, sizeof maps);
-    bool ok = encode(&maps.tcb14, Y, g, kTJ + 2 * kH) && encode(&maps.tcb3, Y, g, kH) &&
-              encode(&maps.tcb11, Y, g, kTJ + kH) && encode(&maps.lr, Y, g, 0);
-    for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, kTJ);
+    using Cf = TmaCfg<T>;
+    bool ok = encode(&maps.tcbA, Y, g, Cf::TJ + 2 * kH) && encode(&maps.tcb3, Y, g, kH) &&
+              encode(&maps.tcbB, Y, g, Cf::TJ + kH) && encode(&maps.lr, Y, g, 0);
+    for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, Cf::TJ);
     if (!ok) return cudaErrorInvalidValue;
     constexpr size_t smem = tma_smem_bytes<T, NE>();
     auto kern = k_stage_tma<T, STAGE, STRETCH, Args>;
@@ -344,8 +361,9 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         attr = true;
     }
-    const int ch = pick_ichunk(g, tma_blocks_per_sm<T>());
-    kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, corr2, dt, visc, a, maps, ch, err);
+    const int ch = tma_ichunk<T>(g);
+    const dim3 grid(g.N2 / kTK, g.N1 / Cf::TJ, (g.N0 + ch - 1) / ch);
+    kern<<<grid, dim3(kTK, Cf::TJ + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err);
     return cudaSuccess;
 }
 
@@ -364,11 +382,13 @@ cudaError_t launch_tma_stage(int stage, const Geo &g, const Coef<T> &co, const T
 
 }  // namespace
 
-bool stage_tma_fits(const Geo &g)
+bool stage_tma_fits(const Geo &g, bool fp64)
 {
     // tile width divides N2 (k halo boxes start at a wrapped column), tile
-    // height divides N1 with at most one wrap per tile in j, periodic y
-    return !g.wallY && g.N2 % kTK == 0 && g.N1 % kTJ == 0 && g.N1 >= 2 * kTJ;
+    // height (16 rows for FP64, 8 for FP32) divides N1 with at most one wrap
+    // per tile in j, periodic y
+    const int tj = fp64 ? TmaCfg<double>::TJ : TmaCfg<float>::TJ;
+    return !g.wallY && g.N2 % kTK == 0 && g.N1 % tj == 0 && g.N1 >= 2 * tj;
 }
 
 cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,

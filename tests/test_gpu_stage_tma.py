@@ -2,8 +2,9 @@
 march (NOVA_STAGE_IMPL=tma / march, read when a mesh context is created).
 Both run the same point arithmetic, so whole runs must agree bit for bit; the
 march itself is pinned to the oracle by test_gpu_advance.py, and meshes of
-32^3 and up (periodic y, N2 % 32 == 0, N1 % 8 == 0, N1 >= 16) take the TMA
-path by default, so those oracle tests cover it directly too."""
+32^3 and up (periodic y, N2 % 32 == 0, N1 a multiple of the tile height 16
+(FP64) or 8 (FP32) and at least twice it) take the TMA path by default, so
+those oracle tests cover it directly too."""
 import os
 
 import numpy as np
@@ -32,9 +33,11 @@ def mesh_with(nova, impl, N, **kw):
             os.environ["NOVA_STAGE_IMPL"] = old
 
 
-# (33, 16, 32): i chunks of 16, 16 and 1 plane; (10, 24, 64): one chunk, two k tiles,
-# three j tiles (both wrap cases and an interior tile); (40, 16, 96): three k tiles
-SIZES = [(33, 16, 32), (10, 24, 64), (40, 16, 96)]
+# FP64 tiles are 32 x 16, FP32-split tiles 32 x 8.  (33, 32, 32): i chunks of
+# 16, 16 and 1 plane; (10, 48, 64): two k tiles, three j tiles (both wrap
+# cases and an interior tile); (40, 32, 96): three k tiles.
+SIZES = [(33, 32, 32), (10, 48, 64), (40, 32, 96)]
+SIZES32 = [(33, 16, 32), (10, 24, 64)]
 
 
 def run(nova, impl, N, U0, prec, rk_mode, steps=3, **mesh_kw):
@@ -55,7 +58,7 @@ def test_tma_equals_march_fp64(nova, N, rk_mode):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
-@pytest.mark.parametrize("N", SIZES[:2])
+@pytest.mark.parametrize("N", SIZES32)
 @pytest.mark.parametrize("rk_mode", ["classical", "literal"])
 def test_tma_equals_march_fp32_split(nova, N, rk_mode):
     U0 = 0.3 * np.random.default_rng(6).standard_normal((3,) + N)
@@ -65,7 +68,7 @@ def test_tma_equals_march_fp32_split(nova, N, rk_mode):
 
 
 def test_tma_equals_march_stretched_z(nova):
-    N, kw = (12, 16, 64), dict(L=(2 * np.pi, 2 * np.pi, 1.0), hyperbolic_z=(0.01, 0.01))
+    N, kw = (12, 32, 64), dict(L=(2 * np.pi, 2 * np.pi, 1.0), hyperbolic_z=(0.01, 0.01))
     U0 = 0.3 * np.random.default_rng(7).standard_normal((3,) + N)
     a = run(nova, "tma", N, U0, nova.F64, "classical", **kw)
     b = run(nova, "march", N, U0, nova.F64, "classical", **kw)
@@ -73,7 +76,7 @@ def test_tma_equals_march_stretched_z(nova):
 
 
 def test_tma_taylor_green_vs_oracle(nova, oracle):
-    N = (16, 16, 32)
+    N = (16, 32, 32)
     OM = oracle.Mesh(N)
     U0 = oracle.ic_taylor_green(OM)
     got, _ = run(nova, "tma", N, U0, nova.F64, "classical", steps=4)
@@ -84,7 +87,7 @@ def test_tma_taylor_green_vs_oracle(nova, oracle):
 
 
 def test_adjoint_through_tma_equals_march(nova):
-    N = (16, 16, 32)
+    N = (16, 32, 32)
     U0 = 0.2 * np.random.default_rng(9).standard_normal((3,) + N)
     out = []
     for impl in ("tma", "march"):
