@@ -1185,9 +1185,19 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     auto Y4 = [&](int t) { return seg + V * (4 * (size_t)t + 3); };
     cudaStream_t st = ctx->stream;
 
-    // forward pass, keeping every K-th state (the running state lives in mu)
+    // forward pass, keeping every K-th state (the running state lives in mu);
+    // the last segment keeps its states and stage states as it goes, so the
+    // reverse sweep does not recompute it
+    const int c_last = nck - 1, n_last = c_last * K, m_last = N - n_last;
     CK(cudaMemcpyAsync(ck, init->U->d64, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
     for (int n = 0; n < N; n++) {
+        if (n >= n_last) {
+            const int t = n - n_last;
+            if (t == 0) CK(cudaMemcpyAsync(St(0), ck + V * c_last, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+            double *out = (t + 1 < m_last) ? St(t + 1) : mu;
+            if ((s = fwd_step64(ctx, rd, St(t), Y2(t), Y3(t), Y4(t), out, true)) != NOVA_OK) return s;
+            continue;
+        }
         const double *src = (n % K == 0) ? ck + V * (n / K) : mu;
         if ((s = fwd_step64(ctx, rd, src, ctx->w64[0], ctx->w64[1], ctx->w64[0], mu, true)) != NOVA_OK) return s;
         if ((n + 1) % K == 0 && n + 1 < N)
@@ -1209,11 +1219,14 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     for (int c = nck - 1; c >= 0; c--) {
         const int n0 = c * K;
         const int m = (N - n0) < K ? (N - n0) : K;
-        CK(cudaMemcpyAsync(St(0), ck + V * c, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
-        for (int t = 0; t < m; t++) {
-            const bool full = t + 1 < m;
-            if ((s = fwd_step64(ctx, rd, St(t), Y2(t), Y3(t), Y4(t), full ? St(t + 1) : nullptr, full)) != NOVA_OK)
-                return s;
+        if (c != c_last) {
+            CK(cudaMemcpyAsync(St(0), ck + V * c, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+            for (int t = 0; t < m; t++) {
+                const bool full = t + 1 < m;
+                if ((s = fwd_step64(ctx, rd, St(t), Y2(t), Y3(t), Y4(t), full ? St(t + 1) : nullptr, full)) !=
+                    NOVA_OK)
+                    return s;
+            }
         }
         for (int t = m - 1; t >= 0; t--) {
             {
