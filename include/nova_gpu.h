@@ -43,7 +43,7 @@ typedef enum {
     NOVA_E_CUDA = 2,        /* a CUDA or cuFFT call failed */
     NOVA_E_OOM = 3,         /* device allocation failed */
     NOVA_E_NONFINITE = 4,   /* a diagnostic reduction saw NaN/Inf in the state */
-    NOVA_E_TIMEOUT = 5,     /* reserved: a bounded device wait gave up */
+    NOVA_E_TIMEOUT = 5,     /* a bounded device wait (the stage pipeline's mbarriers) gave up */
     NOVA_E_UNSUPPORTED = 6  /* valid request this build does not implement */
 } nova_status;
 
@@ -188,6 +188,24 @@ typedef struct {
  * *objective receives J.  gradB is reserved for the MHD adjoint (pass NULL). */
 nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *adj, const nova_state *init, nova_field *gradU,
                               nova_field *gradB, double *objective);
+
+/* ---- restart checkpoints ----
+ * Lossless FP64 restart of a state (the reference restarts from its EnSight
+ * float output, src/Field/Field.hxx:404-516; this file keeps every bit).
+ * Layout, host byte order:
+ *   "NOVACKP1"; mesh: int32 N[3], m, walls[3], hyperbolic_z; double L[3],
+ *   origin[3], s1, s2; double t; int64 step; int32 nfields, reserved;
+ *   per field present (slot 0 U, 1 p, 2 B, 3 pB): int32 slot, ncomp, precision,
+ *   reserved; nova_bc (int32 type[18], double val[18]); ncomp * N0*N1*N2
+ *   doubles, component-major [c][i][j][k] over the stored nodes (N1 + 1 rows
+ *   with y walls); FP32-split fields as hi + lo.
+ * nova_checkpoint_write writes the fields of st that are non-NULL.
+ * nova_checkpoint_read refuses a file of another mesh (NOVA_E_INVALID), fills
+ * the non-NULL fields of st that the file holds (values and BCs; FP32-split
+ * targets get the FP64 values split into hi + lo) and leaves the others as
+ * they are; t and step may be NULL. */
+nova_status nova_checkpoint_write(nova_ctx *ctx, const char *path, const nova_state *st, double t, long long step);
+nova_status nova_checkpoint_read(nova_ctx *ctx, const char *path, nova_state *st, double *t, long long *step);
 
 /* ---- instrumentation: per-kernel CUDA-event timing of nova_advance ---- */
 typedef enum { NOVA_K_STAGE = 0, NOVA_K_DIV = 1, NOVA_K_FFT = 2, NOVA_K_CORRECT = 3, NOVA_K_DIAG = 4, NOVA_K_ADJ = 5,

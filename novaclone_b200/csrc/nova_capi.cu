@@ -1077,7 +1077,7 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     int flag[2] = {0, 0};
     CK(cudaMemcpyAsync(flag, ctx->d_flag, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (flag[1]) return fail(ctx, NOVA_E_CUDA, "nova_advance: a stage kernel pipeline wait timed out");
+    if (flag[1]) return fail(ctx, NOVA_E_TIMEOUT, "nova_advance: a stage kernel pipeline wait timed out");
     if (flag[0]) return fail(ctx, NOVA_E_NONFINITE, "nova_advance: non-finite value in the diagnostics");
     return NOVA_OK;
 }
@@ -1250,9 +1250,162 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     int perr = 0;
     CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (perr) return fail(ctx, NOVA_E_CUDA, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
+    if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
     if (objective) *objective = row[2];
     if (!std::isfinite(row[2])) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
+    return NOVA_OK;
+}
+
+// =============================================================== checkpoints ==
+namespace {
+
+const char kCkptMagic[8] = {'N', 'O', 'V', 'A', 'C', 'K', 'P', '1'};
+
+struct CkptFile {
+    std::FILE *fp = nullptr;
+    bool ok = true;
+    ~CkptFile()
+    {
+        if (fp) std::fclose(fp);
+    }
+    void put(const void *p, size_t n) { ok = ok && std::fwrite(p, 1, n, fp) == n; }
+    void get(void *p, size_t n) { ok = ok && std::fread(p, 1, n, fp) == n; }
+};
+
+struct CkptMesh {
+    int32_t N[3], m, walls[3], hyperbolic_z;
+    double L[3], origin[3], s1, s2;
+};
+
+CkptMesh ckpt_mesh(const nova_mesh_desc &md)
+{
+    CkptMesh c{};
+    for (int a = 0; a < 3; a++) {
+        c.N[a] = md.N[a];
+        c.walls[a] = md.walls[a];
+        c.L[a] = md.L[a];
+        c.origin[a] = md.origin[a];
+    }
+    c.m = md.m;
+    c.hyperbolic_z = md.hyperbolic_z;
+    c.s1 = md.hyperbolic_z ? md.s1 : 0.0;
+    c.s2 = md.hyperbolic_z ? md.s2 : 0.0;
+    return c;
+}
+
+void put_mesh(CkptFile &f, const CkptMesh &c)
+{
+    f.put(c.N, sizeof c.N), f.put(&c.m, 4), f.put(c.walls, sizeof c.walls), f.put(&c.hyperbolic_z, 4);
+    f.put(c.L, sizeof c.L), f.put(c.origin, sizeof c.origin), f.put(&c.s1, 8), f.put(&c.s2, 8);
+}
+
+void get_mesh(CkptFile &f, CkptMesh &c)
+{
+    f.get(c.N, sizeof c.N), f.get(&c.m, 4), f.get(c.walls, sizeof c.walls), f.get(&c.hyperbolic_z, 4);
+    f.get(c.L, sizeof c.L), f.get(c.origin, sizeof c.origin), f.get(&c.s1, 8), f.get(&c.s2, 8);
+}
+
+bool same_mesh(const CkptMesh &a, const CkptMesh &b)
+{
+    bool same = a.m == b.m && a.hyperbolic_z == b.hyperbolic_z && a.s1 == b.s1 && a.s2 == b.s2;
+    for (int d = 0; d < 3; d++)
+        same = same && a.N[d] == b.N[d] && a.walls[d] == b.walls[d] && a.L[d] == b.L[d] && a.origin[d] == b.origin[d];
+    return same;
+}
+
+const int kCkptComps[4] = {3, 1, 3, 1};  // U, p, B, pB
+
+}  // namespace
+
+extern "C" nova_status nova_checkpoint_write(nova_ctx *ctx, const char *path, const nova_state *st, double t,
+                                             long long step)
+{
+    if (!ctx || !path || !st) return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_write: null argument");
+    const nova_field *fs[4] = {st->U, st->p, st->B, st->pB};
+    int32_t nf = 0;
+    for (int q = 0; q < 4; q++) {
+        if (!fs[q]) continue;
+        if (!valid_field(fs[q], kCkptComps[q]))
+            return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_write: state field " + std::to_string(q) +
+                                                 " has the wrong component count");
+        nf++;
+    }
+    CkptFile f;
+    f.fp = std::fopen(path, "wb");
+    if (!f.fp) return fail(ctx, NOVA_E_INVALID, std::string("nova_checkpoint_write: cannot open ") + path);
+    f.put(kCkptMagic, 8);
+    put_mesh(f, ckpt_mesh(ctx->md));
+    const int64_t st64 = step;
+    const int32_t zero = 0;
+    f.put(&t, 8), f.put(&st64, 8), f.put(&nf, 4), f.put(&zero, 4);
+    std::vector<double> host;
+    for (int q = 0; q < 4 && f.ok; q++) {
+        const nova_field *fl = fs[q];
+        if (!fl) continue;
+        const int32_t hdr[4] = {q, fl->nc, fl->prec, 0};
+        f.put(hdr, sizeof hdr);
+        int32_t types[18];
+        for (int i = 0; i < 18; i++) types[i] = fl->bc.type[i];
+        f.put(types, sizeof types), f.put(fl->bc.val, sizeof fl->bc.val);
+        host.resize((size_t)fl->nc * ctx->g.N3);
+        nova_status s = soa_out(ctx, fl, host.data(), cudaMemcpyDeviceToHost);
+        if (s != NOVA_OK) return s;
+        CK(cudaStreamSynchronize(ctx->stream));
+        f.put(host.data(), sizeof(double) * host.size());
+    }
+    const bool closed = std::fclose(f.fp) == 0;
+    f.fp = nullptr;
+    if (!f.ok || !closed) return fail(ctx, NOVA_E_INVALID, std::string("nova_checkpoint_write: write failed: ") + path);
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_checkpoint_read(nova_ctx *ctx, const char *path, nova_state *st, double *t,
+                                            long long *step)
+{
+    if (!ctx || !path || !st) return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: null argument");
+    nova_field *fs[4] = {st->U, st->p, st->B, st->pB};
+    for (int q = 0; q < 4; q++)
+        if (fs[q] && !valid_field(fs[q], kCkptComps[q]))
+            return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: state field " + std::to_string(q) +
+                                                 " has the wrong component count");
+    CkptFile f;
+    f.fp = std::fopen(path, "rb");
+    if (!f.fp) return fail(ctx, NOVA_E_INVALID, std::string("nova_checkpoint_read: cannot open ") + path);
+    char magic[8];
+    f.get(magic, 8);
+    if (!f.ok || std::memcmp(magic, kCkptMagic, 8) != 0)
+        return fail(ctx, NOVA_E_INVALID, std::string("nova_checkpoint_read: not a checkpoint file: ") + path);
+    CkptMesh cm{};
+    get_mesh(f, cm);
+    if (!f.ok || !same_mesh(cm, ckpt_mesh(ctx->md)))
+        return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: the file holds another mesh");
+    double tt = 0.0;
+    int64_t st64 = 0;
+    int32_t nf = 0, reserved = 0;
+    f.get(&tt, 8), f.get(&st64, 8), f.get(&nf, 4), f.get(&reserved, 4);
+    if (!f.ok || nf < 0 || nf > 4) return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: corrupt header");
+    std::vector<double> host;
+    for (int i = 0; i < nf; i++) {
+        int32_t hdr[4];
+        f.get(hdr, sizeof hdr);
+        if (!f.ok || hdr[0] < 0 || hdr[0] > 3 || hdr[1] != kCkptComps[hdr[0]])
+            return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: corrupt field record");
+        int32_t types[18];
+        nova_bc bc;
+        f.get(types, sizeof types), f.get(bc.val, sizeof bc.val);
+        for (int k = 0; k < 18; k++) bc.type[k] = types[k];
+        host.resize((size_t)hdr[1] * ctx->g.N3);
+        f.get(host.data(), sizeof(double) * host.size());
+        if (!f.ok) return fail(ctx, NOVA_E_INVALID, std::string("nova_checkpoint_read: truncated file: ") + path);
+        nova_field *fl = fs[hdr[0]];
+        if (!fl) continue;
+        nova_status s = nova_field_set_bc(ctx, fl, &bc);
+        if (s != NOVA_OK) return s;
+        if ((s = soa_in(ctx, fl, host.data(), cudaMemcpyHostToDevice)) != NOVA_OK) return s;
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    if (t) *t = tt;
+    if (step) *step = st64;
     return NOVA_OK;
 }
 

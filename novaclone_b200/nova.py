@@ -36,7 +36,8 @@ EXPORTS = (
     "nova_field_upload", "nova_field_download",
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
-    "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_profile_enable", "nova_profile_read",
+    "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_checkpoint_write",
+    "nova_checkpoint_read", "nova_profile_enable", "nova_profile_read",
     "nova_launch_count",
 )
 
@@ -110,6 +111,8 @@ def load_library(path: str = LIB_PATH):
         "nova_field_maxabs_noalloc": [vp, vp, dp],
         "nova_advance": [vp, C.POINTER(RunDesc), C.POINTER(State), C.c_int, dp],
         "nova_adjoint_grad": [vp, C.POINTER(AdjDesc), C.POINTER(State), vp, vp, dp],
+        "nova_checkpoint_write": [vp, C.c_char_p, C.POINTER(State), C.c_double, C.c_longlong],
+        "nova_checkpoint_read": [vp, C.c_char_p, C.POINTER(State), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "nova_profile_enable": [vp, C.c_int],
         "nova_profile_read": [vp, C.c_int, dp, C.POINTER(C.c_long), C.c_int],
         "nova_launch_count": [vp, C.POINTER(C.c_long), C.c_int],
@@ -391,3 +394,21 @@ def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_eve
     J = C.c_double()
     mesh.check(mesh.lib.nova_adjoint_grad(mesh.h, C.byref(a), C.byref(st), grad.h, None, C.byref(J)))
     return J.value, grad
+
+
+def _state(U=None, p=None, B=None, pB=None):
+    return State(*(f.h if f is not None else None for f in (U, p, B, pB)))
+
+
+def checkpoint_write(mesh: Mesh, path: str, U=None, p=None, B=None, pB=None, t: float = 0.0, step: int = 0):
+    """Lossless FP64 restart file of the given fields (nova_checkpoint_write)."""
+    st = _state(U, p, B, pB)
+    mesh.check(mesh.lib.nova_checkpoint_write(mesh.h, os.fsencode(path), C.byref(st), float(t), int(step)))
+
+
+def checkpoint_read(mesh: Mesh, path: str, U=None, p=None, B=None, pB=None):
+    """Fill the given fields from a restart file of the same mesh; returns (t, step)."""
+    st = _state(U, p, B, pB)
+    t, step = C.c_double(), C.c_longlong()
+    mesh.check(mesh.lib.nova_checkpoint_read(mesh.h, os.fsencode(path), C.byref(st), C.byref(t), C.byref(step)))
+    return t.value, step.value
