@@ -14,6 +14,7 @@ src/Field/Field.h:82-85) and the unique-point component-major layout
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 import tempfile
@@ -259,7 +260,7 @@ def write_case(dirname, mesh, bc=None):
         f.write("N: %d %d %d\n" % mesh.N)
         f.write("L: %.17g %.17g %.17g\n" % mesh.L)
     bc = bc or {}
-    for name, nc in (("U", 3), ("p", 1), ("B", 3), ("pB", 1)):
+    for name, nc in (("U", 3), ("p", 1), ("B", 3), ("pB", 1), ("rho", 1), ("T", 1)):
         t, v = bc_arrays(nc, bc.get(name))
         with open(os.path.join(dirname, name + "BC"), "w") as f:
             for c in range(nc):
@@ -306,6 +307,156 @@ def ref_ops(mesh, U, s, nu):
         return {k: np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (nc,)) for k, nc in names.items()}
 
 
+# ------------------------------------------------- compressible loop bodies --
+# Restated with the pinned operators above and numpy point operations in the
+# reference's expression order; fields are ghosted AoS arrays.
+
+RK4W = (1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0)  # app/TG/TG.cpp:62, shearLayer.cpp:164
+
+
+def wc_eos_k(c, rho0):
+    """c*c/2.0/rho0 of app/shearLayerWC/pEqn.H:2."""
+    return c * c / 2.0 / rho0
+
+
+def _u_eqn(mesh, U, rho, p, T, dt, mu, gz, buoy, bcU):
+    """app/TG/UEqn.H:1-38, app/shearLayerWC/UEqn.H:1-42 (buoyancy -(rho*T)*g)."""
+    g = np.array([0.0, 0.0, gz])
+    rhoUc = rho * U
+    rhoUOld = rho * U
+    for rk in range(4):
+        e = -div_vf(mesh, rho * U, U)
+        e = e - grad_s(mesh, p)
+        e = e + lap(mesh, mu, U)
+        if buoy:
+            e = e - (rho * T) * g
+        drhoU = dt * e
+        rhoUc = rhoUc + RK4W[rk] * drhoU
+        if rk < 3:
+            U = rhoUOld / rho + (int(rk / 2) + 1) / 2.0 * (drhoU / rho)
+        else:
+            U = rhoUc / rho
+        U = bc_apply(mesh, U, bcU)
+    return U
+
+
+def _rho_eqn(mesh, U, rho, dt, bcr):
+    """app/TG/rhoEqn.H:1-37 (= app/shearLayerWC/rhoEqn.H)."""
+    rhoOld = rho.copy()
+    rhoc = rho.copy()
+    for rk in range(4):
+        drho = dt * (-div_v(mesh, rho * U))
+        rhoc = rhoc + RK4W[rk] * drho
+        rho = rhoOld + (int(rk / 2) + 1) / 2.0 * drho if rk < 3 else rhoc
+        rho = bc_apply(mesh, rho, bcr)
+    return rho
+
+
+def _t_eqn(mesh, U, rho, T, dt, ka, bcT):
+    """app/shearLayerWC/TEqn.H:1-38."""
+    rhoTc = rho * T
+    rhoTOld = rho * T
+    for rk in range(4):
+        drhoT = dt * (-div_vf(mesh, rho * U, T) + lap(mesh, ka, T))
+        rhoTc = rhoTc + RK4W[rk] * drhoT
+        if rk < 3:
+            T = rhoTOld / rho + (int(rk / 2) + 1) / 2.0 * (drhoT / rho)
+        else:
+            T = rhoTc / rho
+        T = bc_apply(mesh, T, bcT)
+    return T
+
+
+def wc_run(mesh, U, rho, p, T=None, *, order="shear", nsteps=1, dt=0.01, mu=0.0, ka=0.0, c=0.0, rho0=1.0,
+           gz=0.0, bc=None):
+    """The compressible time step on ghosted arrays.
+    order "tg":    app/TG/TG.cpp:73-75, rhoEqn.H, pEqn.H (p = 50 rho^2), UEqn.H;
+    order "shear": app/shearLayerWC/shearLayer.cpp:197-200, UEqn.H (with buoyancy),
+                   rhoEqn.H, pEqn.H (p = c^2/(2 rho0) rho^2), TEqn.H.
+    Returns (U, rho, p, T, hist[nsteps, 6]) with hist rows (step, t, Ek, 0, max|div U|, 0)."""
+    bc = bc or {}
+    U = bc_apply(mesh, np.array(U, np.float64), bc.get("U"))
+    rho = bc_apply(mesh, np.array(rho, np.float64), bc.get("rho"))
+    p = bc_apply(mesh, np.array(p, np.float64), bc.get("p"))
+    T = bc_apply(mesh, mesh.zeros(1) if T is None else np.array(T, np.float64), bc.get("T"))
+    K = wc_eos_k(c, rho0)
+    hist = np.zeros((nsteps, HIST_COLS))
+    h, N = mesh.h, mesh.N
+    for step in range(nsteps):
+        if order == "tg":
+            rho = _rho_eqn(mesh, U, rho, dt, bc.get("rho"))
+            p = 50.0 * (rho * rho)
+            U = _u_eqn(mesh, U, rho, p, T, dt, mu, gz, False, bc.get("U"))
+        else:
+            U = _u_eqn(mesh, U, rho, p, T, dt, mu, gz, True, bc.get("U"))
+            rho = _rho_eqn(mesh, U, rho, dt, bc.get("rho"))
+            p = (K * rho) * rho
+            T = _t_eqn(mesh, U, rho, T, dt, ka, bc.get("T"))
+        u = U[h:h + N[0], h:h + N[1], h:h + N[2]]
+        ek = 0.0
+        for v in (0.5 * (u[..., 0] * u[..., 0] + u[..., 1] * u[..., 1] + u[..., 2] * u[..., 2])).ravel():
+            ek += v
+        hist[step] = (step + 1, (step + 1) * dt, ek / u[..., 0].size, 0.0, maximum(mesh, div_v(mesh, U)), 0.0)
+    return U, rho, p, T, hist
+
+
+def wc_hydrostatic(mesh, T, *, c, rho0, gz):
+    """Initial p and rho of app/shearLayerWC/shearLayer.cpp:114-155 for a given T:
+    pEqn.H on rho = rho0, the column integral of hydrostaticP.H:1-38 (from the
+    top node down, T*dz*g_z*rho0, unique i and k, j including the duplicate
+    node), rho = (p/K)^0.5.  Returns ghosted (p, rho)."""
+    K = wc_eos_k(c, rho0)
+    T = bc_apply(mesh, np.array(T, np.float64))
+    rho = np.full(mesh.n + (1,), rho0)
+    p = (K * rho) * rho
+    h, n = mesh.h, mesh.n
+    dz = mesh.L[2] / mesh.N[2]
+    pHyd = mesh.zeros(1)
+    col = T[h:n[0] - h - 1, h:n[1] - h, h:n[2] - h - 1, 0]
+    terms = ((col * dz) * gz) * rho0
+    pHyd[h:n[0] - h - 1, h:n[1] - h, h:n[2] - h - 1, 0] = np.cumsum(terms[..., ::-1], axis=-1)[..., ::-1]
+    p = p + pHyd
+    # std::pow(x, 0.5) (C pow, not numpy's sqrt shortcut for the exponent 0.5)
+    q = p[h:n[0] - h, h:n[1] - h, h:n[2] - h] / K
+    rho[h:n[0] - h, h:n[1] - h, h:n[2] - h] = np.array([math.pow(v, 0.5) for v in q.ravel()]).reshape(q.shape)
+    return bc_apply(mesh, p), bc_apply(mesh, rho)
+
+
+def ref_wc_run(mesh, U, rho, p, T=None, *, order="shear", nsteps=1, dt=0.01, mu=0.0, ka=0.0, c=0.0, rho0=1.0,
+               gz=0.0, bc=None):
+    """The reference's own compressible loop bodies (oracle/_ref/nova_ref wc)."""
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        write_case(case, mesh, bc)
+        paths = {}
+        for name, a in (("U", U), ("rho", rho), ("p", p), ("T", T)):
+            if a is None:
+                paths[name] = "-"
+                continue
+            paths[name] = os.path.join(td, name + ".bin")
+            np.ascontiguousarray(a, np.float64).tofile(paths[name])
+        out = os.path.join(td, "out")
+        subprocess.run([REF_BIN, "wc", case, order, str(nsteps)] + [repr(float(v)) for v in (dt, mu, ka, c, rho0, gz)]
+                       + [paths["U"], paths["rho"], paths["p"], paths["T"], out, "-m", str(mesh.m)],
+                       check=True, stdout=subprocess.DEVNULL)
+        r = tuple(np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (nc,))
+                  for k, nc in (("U", 3), ("rho", 1), ("p", 1), ("T", 1)))
+        hist = np.fromfile(out + "_hist.bin").reshape(nsteps, HIST_COLS)
+    return r + (hist,)
+
+
+def ref_wc_init(mesh, T, *, c, rho0, gz):
+    """The reference's weakly-compressible initialisation (oracle/_ref/nova_ref wcinit)."""
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        write_case(case, mesh)
+        np.ascontiguousarray(T, np.float64).tofile(os.path.join(td, "T.bin"))
+        out = os.path.join(td, "out")
+        subprocess.run([REF_BIN, "wcinit", case, repr(float(c)), repr(float(rho0)), repr(float(gz)),
+                        os.path.join(td, "T.bin"), out, "-m", str(mesh.m)], check=True, stdout=subprocess.DEVNULL)
+        return tuple(np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (1,)) for k in ("p", "rho"))
+
+
 # ------------------------------------------------------------- initial data --
 
 def ic_taylor_green(mesh):
@@ -322,6 +473,46 @@ def ic_orszag_tang(mesh):
     U = np.stack([-2.0 * np.sin(Y), 2.0 * np.sin(X), np.zeros_like(X)])
     B = np.stack([-2.0 * np.sin(2.0 * Y) + np.sin(Z), 2.0 * np.sin(X) + np.sin(Z), np.zeros_like(X)])
     return U, B
+
+
+def wc_shear_params(mach=0.1):
+    """Constants of app/shearLayerWC/shearLayer.cpp:31-44 (Mach as a parameter)."""
+    Re0, Ri0, Pr, rho0, c = 1967.0, 0.08, 7.0, 999.57, 0.0417
+    u0 = c * mach
+    h0, t0 = 0.2, 0.1
+    mu = rho0 * u0 * h0 / Re0
+    return dict(rho0=rho0, c=c, u0=u0, h0=h0, t0=t0, mu=mu, ka=mu / Pr, gz=-Ri0 * u0 * u0 / t0 / h0)
+
+
+def ic_wc_shear(mesh, prm, seed=0):
+    """U, T of shearLayer.cpp:116-135 on the unique points with z = -7.5 h0 + k dz,
+    the reference's std::default_random_engine noise replaced by a seeded
+    uniform(-1, 1) generator."""
+    u0, h0, t0 = prm["u0"], prm["h0"], prm["t0"]
+    x, _, z = mesh.coords()
+    z = z - 7.5 * h0
+    X, _, Z = np.meshgrid(x, np.zeros(mesh.N[1]), z, indexing="ij")
+    rng = np.random.default_rng(seed)
+    k0 = 2.0 * 3.1415926536 / (14.0 * h0 / 2.0)
+    a, b = 0.005, 0.4177
+    th, ch = np.tanh(2.0 * Z / h0), np.cosh(2.0 * Z / h0)
+    U = np.zeros((3,) + mesh.N)
+    U[0] = u0 / 2.0 * th + a * u0 / 2.0 / k0 * (-np.cos(2 * k0 * X) + 2.0 * b * np.cos(k0 * X)) * th / ch
+    U[1] = a * u0 / 2.0 * rng.uniform(-1, 1, mesh.N) / ch / ch
+    U[2] = a * u0 / 2.0 * rng.uniform(-1, 1, mesh.N) / ch / ch
+    T = t0 / 2.0 * th + a * t0 / 2.0 * rng.uniform(-1, 1, mesh.N) / ch / ch
+    return U, T[None]
+
+
+def ic_tg_compressible(mesh):
+    """app/TG/TG.cpp:38-56 on the unique points (x = -pi + i dx): U of Taylor-Green,
+    p = 50 + (cos 2x + cos 2y)(cos 2z + 2)/16, rho = (p/50)^0.5."""
+    pi = np.pi
+    x, y, z = (c - pi for c in mesh.coords())
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    U = np.stack([np.sin(X) * np.cos(Y) * np.cos(Z), -np.cos(X) * np.sin(Y) * np.cos(Z), np.zeros_like(X)])
+    p = 50 + 1.0 / 16.0 * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2)
+    return U, np.power(p / 50.0, 0.5)[None], p[None]
 
 
 def cfl_dt(mesh, fields, cfl=0.3):

@@ -10,9 +10,17 @@
  *
  *   nova_ref run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U.bin> <B.bin|-> <out>
  *   nova_ref ops <case> <nu> <U.bin> <s.bin> <out>
- *   (either may end with the reference's `-m <order>` option)
+ *   nova_ref wc <case> <tg|shear> <nsteps> <dt> <mu> <ka> <c> <rho0> <gz> <U.bin> <rho.bin> <p.bin> <T.bin|-> <out>
+ *   nova_ref wcinit <case> <c> <rho0> <gz> <T.bin> <out>
+ *   (any may end with the reference's `-m <order>` option)
  *
- * <case> holds `mesh` and the BC files (UBC, pBC, BBC, pBBC).
+ * `wc` runs the compressible loop bodies: app/TG (rhoEqn.H, pEqn.H, UEqn.H in
+ * the order of app/TG/TG.cpp:73-75) or app/shearLayerWC (UEqn.H, rhoEqn.H,
+ * pEqn.H, TEqn.H in the order of shearLayer.cpp:197-200).  `wcinit` runs the
+ * weakly-compressible initialisation of shearLayer.cpp:114-155 (pEqn.H on
+ * rho = rho0, hydrostaticP.H, rho from the EOS) for a given T.
+ *
+ * <case> holds `mesh` and the BC files (UBC, pBC, BBC, pBBC, rhoBC, TBC).
  */
 #include <chrono>
 #include <cstdio>
@@ -203,13 +211,113 @@ static int ops(int argc, char **argv)
     return 0;
 }
 
+/* app/TG/TG.cpp:91-109 and the reference's max|div U| */
+static void wc_hist(std::vector<double> &hist, int step, const Mesh &mesh, const Time &time, Field<vector> &U)
+{
+    double row[6] = {double(step + 1), time.curTime(), ek_mean(mesh, U), 0.0, 0.0, 0.0};
+    auto d = ex::div(U);
+    row[4] = tools::maximum(d);
+    hist.insert(hist.end(), row, row + 6);
+}
+
+static int wc(int argc, char **argv)
+{
+    if (argc < 16) {
+        std::fprintf(stderr, "usage: wc <case> <tg|shear> <nsteps> <dt> <mu> <ka> <c> <rho0> <gz> <U> <rho> <p> <T|-> <out>\n");
+        return 2;
+    }
+    settings::zoneName() = argv[2];
+    const bool tg = std::string(argv[3]) == "tg";
+    const int nsteps = std::atoi(argv[4]);
+    const double dt = std::atof(argv[5]);
+    const scalar mu = std::atof(argv[6]);
+    const scalar ka = std::atof(argv[7]);
+    const scalar c = std::atof(argv[8]);
+    const scalar rho0 = std::atof(argv[9]);
+    vector g(0, 0, std::atof(argv[10]));
+    const std::string inT = argv[14], out = argv[15];
+    scalar RK4[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+
+    Time time(dt, dt * (nsteps + 0.5), 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+    Field<vector> U(mesh, vector(0, 0, 0), "U");
+    Field<scalar> rho(mesh, rho0, "rho");
+    Field<scalar> p(mesh, 0, "p");
+    Field<scalar> T(mesh, 0, "T");
+    load(U, argv[11]);
+    load(rho, argv[12]);
+    load(p, argv[13]);
+    if (inT != "-") load(T, inT);
+    U.correctBoundaryConditions();
+    p.correctBoundaryConditions();
+    rho.correctBoundaryConditions();
+    T.correctBoundaryConditions();
+
+    std::vector<double> hist;
+    for (int step = 0; step < nsteps; step++) {
+        time++;
+        if (tg) {
+#include "TG/rhoEqn.H"
+#include "TG/pEqn.H"
+#include "TG/UEqn.H"
+        } else {
+#include "shearLayerWC/UEqn.H"
+#include "shearLayerWC/rhoEqn.H"
+#include "shearLayerWC/pEqn.H"
+#include "shearLayerWC/TEqn.H"
+        }
+        wc_hist(hist, step, mesh, time, U);
+    }
+    save(U, out + "_U.bin");
+    save(rho, out + "_rho.bin");
+    save(p, out + "_p.bin");
+    save(T, out + "_T.bin");
+    FILE *fp = std::fopen((out + "_hist.bin").c_str(), "wb");
+    std::fwrite(hist.data(), sizeof(double), hist.size(), fp);
+    std::fclose(fp);
+    return 0;
+}
+
+static int wcinit(int argc, char **argv)
+{
+    if (argc < 8) { std::fprintf(stderr, "usage: wcinit <case> <c> <rho0> <gz> <T> <out>\n"); return 2; }
+    settings::zoneName() = argv[2];
+    const scalar c = std::atof(argv[3]);
+    const scalar rho0 = std::atof(argv[4]);
+    vector g(0, 0, std::atof(argv[5]));
+    const std::string out = argv[7];
+    Time time(0.01, 1.0, 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+    Field<scalar> T(mesh, 0, "T");
+    Field<scalar> p(mesh, 0, "p");
+    Field<scalar> pHyd(mesh, 0, "pHyd");
+    Field<scalar> rho(mesh, rho0, "rho");
+    load(T, argv[6]);
+    T.correctBoundaryConditions();
+#include "shearLayerWC/pEqn.H"
+#include "shearLayerWC/hydrostaticP.H"
+    for (int i = settings::m() / 2; i < mesh.ni() - settings::m() / 2; i++)
+        for (int j = settings::m() / 2; j < mesh.nj() - settings::m() / 2; j++)
+            for (int k = settings::m() / 2; k < mesh.nk() - settings::m() / 2; k++)
+                rho(i, j, k) = std::pow(p(i, j, k) / (c * c / 2.0 / rho0), 0.5); /* shearLayer.cpp:141-150 */
+    p.correctBoundaryConditions();
+    rho.correctBoundaryConditions();
+    save(p, out + "_p.bin");
+    save(rho, out + "_rho.bin");
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
-    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops ... [-m order]\n"); return 2; }
+    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit ... [-m order]\n"); return 2; }
     settings::process(argc, argv); /* the reference's own -m option (settings.cpp:53-78) */
     std::string mode = argv[1];
     if (mode == "run") return run(argc, argv);
     if (mode == "ops") return ops(argc, argv);
+    if (mode == "wc") return wc(argc, argv);
+    if (mode == "wcinit") return wcinit(argc, argv);
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;
 }

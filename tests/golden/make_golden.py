@@ -1,12 +1,13 @@
 """Generate the golden vectors in tests/golden/ from the reference itself.
 
 Runs oracle/_ref/nova_ref -- the reference's own sources (src/ex, src/poisson,
-src/BC, src/Field, app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H)
+src/BC, src/Field, app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H,
+the compressible app/TG and app/shearLayerWC loop bodies)
 compiled in place by `make -C oracle ref` -- on small seeded inputs and stores
 inputs and outputs as .npz.  Needs the reference tree (only present where the
 fixtures are generated); the tests only read the .npz files.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [name ...]
 """
 from __future__ import annotations
 
@@ -53,15 +54,51 @@ def run_case(name, N, model, rk_mode, nsteps, dt, nu, eta, L=None):
     np.savez_compressed(os.path.join(HERE, name), **res)
 
 
+def wc_tg_case(name, N, nsteps, dt, mu):
+    """compressible Taylor-Green (app/TG/TG.cpp): rhoEqn.H, pEqn.H, UEqn.H"""
+    M = O.Mesh(N)
+    U, rho, p = O.ic_tg_compressible(M)
+    r = O.ref_wc_run(M, M.to_ghosted(U), M.to_ghosted(rho), M.to_ghosted(p), order="tg", nsteps=nsteps, dt=dt,
+                     mu=mu)
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(M.L), nsteps=np.array(nsteps),
+                        dt=np.array(dt), mu=np.array(mu), U0=U, rho0=rho, p0=p, U=M.unique(r[0]),
+                        rho=M.unique(r[1]), p=M.unique(r[2]), hist=r[4])
+
+
+def wc_shear_case(name, N, nsteps, cfl=0.3, mach=0.1, seed=0):
+    """weakly-compressible shear layer (app/shearLayerWC): the hydrostatic
+    initialisation of shearLayer.cpp:114-155, then UEqn.H, rhoEqn.H, pEqn.H, TEqn.H"""
+    prm = O.wc_shear_params(mach)
+    h0 = prm["h0"]
+    M = O.Mesh(N, L=(14.0 * h0, 1.7 * h0, 15.0 * h0))
+    U, T = O.ic_wc_shear(M, prm, seed)
+    pi, rhoi = O.ref_wc_init(M, M.to_ghosted(T), c=prm["c"], rho0=prm["rho0"], gz=prm["gz"])
+    dt = cfl * min(M.d) / (prm["u0"] / mach + prm["u0"] / 2.0)  # shearLayer.cpp:182
+    kw = {k: prm[k] for k in ("mu", "ka", "c", "rho0", "gz")}
+    r = O.ref_wc_run(M, M.to_ghosted(U), rhoi, pi, M.to_ghosted(T), order="shear", nsteps=nsteps, dt=dt, **kw)
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(M.L), nsteps=np.array(nsteps),
+                        dt=np.array(dt), mach=np.array(mach), U0=U, T0=T, p_init=M.unique(pi),
+                        rho_init=M.unique(rhoi), U=M.unique(r[0]), rho=M.unique(r[1]), p=M.unique(r[2]),
+                        T=M.unique(r[3]), hist=r[4], **{k: np.array(v) for k, v in prm.items()})
+
+
+CASES = {
+    "ops_10x8x6.npz": lambda n: ops_case(n, (10, 8, 6), (2 * np.pi, 2.0, 3.0), 7, 0.01),
+    "ops_16x12x8_m4.npz": lambda n: ops_case(n, (16, 12, 8), (2 * np.pi,) * 3, 8, 0.02, m=4),
+    "tg_12_classical.npz": lambda n: run_case(n, (12, 12, 12), "ns", "classical", 6, 0.05, 1 / 1600, 0.0),
+    "tg_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "ns", "literal", 6, 0.05, 1 / 1600, 0.0),
+    "ot_12_classical.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "classical", 4, 0.01, 1e-3, 1e-3),
+    "ot_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "literal", 4, 0.01, 1e-3, 1e-3),
+    "wc_tg_12.npz": lambda n: wc_tg_case(n, (12, 12, 12), 5, 0.02, 1 / 1600),
+    "wc_shear_12x8x16.npz": lambda n: wc_shear_case(n, (12, 8, 16), 4),
+}
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("build the reference first: make -C oracle ref")
-    ops_case("ops_10x8x6.npz", (10, 8, 6), (2 * np.pi, 2.0, 3.0), 7, 0.01)
-    ops_case("ops_16x12x8_m4.npz", (16, 12, 8), (2 * np.pi,) * 3, 8, 0.02, m=4)
-    run_case("tg_12_classical.npz", (12, 12, 12), "ns", "classical", 6, 0.05, 1 / 1600, 0.0)
-    run_case("tg_12_literal.npz", (12, 12, 12), "ns", "literal", 6, 0.05, 1 / 1600, 0.0)
-    run_case("ot_12_classical.npz", (12, 12, 12), "mhd", "classical", 4, 0.01, 1e-3, 1e-3)
-    run_case("ot_12_literal.npz", (12, 12, 12), "mhd", "literal", 4, 0.01, 1e-3, 1e-3)
+    for name in sys.argv[1:] or CASES:
+        CASES[name](name)
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 
