@@ -189,6 +189,34 @@ typedef struct {
 nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *adj, const nova_state *init, nova_field *gradU,
                               nova_field *gradB, double *objective);
 
+/* ---- weakly-compressible time advance ----
+ * One call = nsteps of the compressible loop bodies on a periodic mesh, FP64:
+ *   NOVA_WC_TG:    app/TG/TG.cpp:73-75          rhoEqn.H, pEqn.H (p = K (rho rho), K = 50), UEqn.H
+ *   NOVA_WC_SHEAR: app/shearLayerWC/shearLayer.cpp:197-200
+ *                  UEqn.H (buoyancy -(rho T) g), rhoEqn.H, pEqn.H (p = (K rho) rho,
+ *                  K = c^2/(2 rho0)), TEqn.H
+ * Each loop is the reference's classical RK4 on rho*U, rho, rho*T.
+ * hist: nsteps x NOVA_HIST_COLS rows (step, t, mean 1/2|U|^2, 0, max|div U|, 0) or NULL. */
+typedef enum { NOVA_WC_TG = 0, NOVA_WC_SHEAR = 1 } nova_wc_case;
+typedef struct {
+    int wc_case;      /* nova_wc_case */
+    int diag_every;   /* diagnostics row every n steps (0: none) */
+    double dt;
+    double mu;        /* laplacian(mu, U) */
+    double ka;        /* laplacian(ka, T) (shear case) */
+    double eos_k;     /* K of the EOS */
+    double g[3];      /* gravity of the buoyancy term (shear case) */
+    double t0;        /* time before the first step (for the hist rows) */
+} nova_wc_desc;
+typedef struct {
+    nova_field *U, *rho, *p, *T;  /* T may be NULL for NOVA_WC_TG */
+} nova_wc_state;
+nova_status nova_advance_wc(nova_ctx *ctx, const nova_wc_desc *wd, nova_wc_state *st, int nsteps, double *hist);
+/* The initialisation of app/shearLayerWC/shearLayer.cpp:114-150: p = (K rho0) rho0 plus the column
+ * integral of T dz g_z rho0 from the top node down (hydrostaticP.H:1-38), rho = (p/K)^(1/2). */
+nova_status nova_wc_hydrostatic(nova_ctx *ctx, const nova_wc_desc *wd, double rho0, const nova_field *T,
+                                nova_field *p, nova_field *rho);
+
 /* ---- restart checkpoints ----
  * Lossless FP64 restart of a state (the reference restarts from its EnSight
  * float output, src/Field/Field.hxx:404-516; this file keeps every bit).

@@ -3,6 +3,7 @@
 #include "nova_gpu.h"
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"
+#include "nova_wc.cuh"
 
 #include <cuda_runtime.h>
 #include <cufft.h>
@@ -1253,6 +1254,103 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
     if (objective) *objective = row[2];
     if (!std::isfinite(row[2])) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
+    return NOVA_OK;
+}
+
+// ========================================================= weakly compressible ==
+extern "C" nova_status nova_advance_wc(nova_ctx *ctx, const nova_wc_desc *wd, nova_wc_state *st, int nsteps,
+                                       double *hist)
+{
+    if (!ctx || !wd || !st || nsteps < 0) return fail(ctx, NOVA_E_INVALID, "nova_advance_wc: bad arguments");
+    const bool shear = wd->wc_case == NOVA_WC_SHEAR;
+    if (wd->wc_case != NOVA_WC_TG && !shear) return fail(ctx, NOVA_E_INVALID, "nova_advance_wc: unknown case");
+    auto f64 = [](const nova_field *f, int nc) { return valid_field(f, nc) && f->prec == NOVA_F64; };
+    if (!f64(st->U, 3) || !f64(st->rho, 1) || !f64(st->p, 1) || (shear && !f64(st->T, 1)))
+        return fail(ctx, NOVA_E_INVALID, "nova_advance_wc: U, rho, p (and T for the shear case) must be FP64 fields");
+    if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance_wc: periodic meshes only");
+    if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance_wc: the fused kernels are built for m = 6");
+    nova_status s = ensure_work(ctx, NOVA_F64);
+    if (s != NOVA_OK) return s;
+    if (hist && wd->diag_every > 0) {
+        if (ctx->hist_cap < (long long)nsteps * NOVA_HIST_COLS) {
+            if (ctx->d_hist) cudaFree(ctx->d_hist);
+            ctx->d_hist = nullptr;
+            ctx->hist_cap = 0;
+            if ((s = dalloc(ctx, &ctx->d_hist, (size_t)nsteps * NOVA_HIST_COLS)) != NOVA_OK) return s;
+            ctx->hist_cap = (long long)nsteps * NOVA_HIST_COLS;
+        }
+        CK(cudaMemsetAsync(ctx->d_hist, 0, sizeof(double) * nsteps * NOVA_HIST_COLS, ctx->stream));
+    }
+    CK(cudaMemsetAsync(ctx->d_flag, 0, 2 * sizeof(int), ctx->stream));
+    const Geo &g = ctx->g;
+    const bool str = ctx->md.hyperbolic_z != 0;
+    double *w0 = ctx->w64[0], *w1 = ctx->w64[1], *acc = ctx->w64[2];
+    // one RK loop of the quantity q (stored in qf): stage states alternate w0/w1, the last stage writes qf
+    auto loop = [&](int which, double *qf, double visc) {
+        WcArgs a{};
+        a.U = st->U->d64;
+        a.rho = st->rho->d64;
+        a.T = st->T ? st->T->d64 : nullptr;
+        a.p = st->p->d64;
+        a.Q0 = qf;
+        a.acc = acc;
+        a.dt = wd->dt;
+        a.visc = visc;
+        a.eos_k = wd->eos_k;
+        for (int c = 0; c < 3; c++) a.g[c] = wd->g[c];
+        const double *ys[4] = {qf, w0, w1, w0};
+        double *yn[4] = {w0, w1, w0, qf};
+        for (int stage = 0; stage < 4; stage++) {
+            ProfScope ps(ctx, NOVA_K_STAGE);
+            a.Y = ys[stage];
+            a.Ynext = yn[stage];
+            launch_wc_stage(which, stage, wd->wc_case, str, g, ctx->co64, ctx->d_ia64, ctx->d_corr64, a, ctx->stream);
+            ctx->launches += 1;
+        }
+    };
+    for (int n = 0; n < nsteps; n++) {
+        if (shear) {
+            loop(WC_LOOP_U, st->U->d64, wd->mu);
+            loop(WC_LOOP_RHO, st->rho->d64, 0.0);
+            loop(WC_LOOP_T, st->T->d64, wd->ka);
+        } else {
+            loop(WC_LOOP_RHO, st->rho->d64, 0.0);
+            loop(WC_LOOP_U, st->U->d64, wd->mu);
+        }
+        CKL("weakly-compressible stage kernels");
+        if (hist && wd->diag_every > 0 && ((n + 1) % wd->diag_every == 0 || n + 1 == nsteps)) {
+            ProfScope ps(ctx, NOVA_K_DIAG);
+            launch_diag(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, st->U->d64, nullptr, nullptr, nullptr,
+                        nullptr, nullptr, 0, ctx->d_part, (double)(n + 1), wd->t0 + (n + 1) * wd->dt,
+                        ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag, ctx->stream);
+            ctx->launches += 2;
+            CKL("k_diag");
+        }
+    }
+    if (hist && wd->diag_every > 0)
+        CK(cudaMemcpyAsync(hist, ctx->d_hist, sizeof(double) * nsteps * NOVA_HIST_COLS, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    int flag[2] = {0, 0};
+    CK(cudaMemcpyAsync(flag, ctx->d_flag, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (flag[0]) return fail(ctx, NOVA_E_NONFINITE, "nova_advance_wc: non-finite value in the diagnostics");
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_wc_hydrostatic(nova_ctx *ctx, const nova_wc_desc *wd, double rho0, const nova_field *T,
+                                           nova_field *p, nova_field *rho)
+{
+    if (!ctx || !wd || !T || !p || !rho) return fail(ctx, NOVA_E_INVALID, "nova_wc_hydrostatic: null argument");
+    auto f64 = [](const nova_field *f) { return valid_field(f, 1) && f->prec == NOVA_F64; };
+    if (!f64(T) || !f64(p) || !f64(rho))
+        return fail(ctx, NOVA_E_INVALID, "nova_wc_hydrostatic: T, p, rho must be FP64 scalar fields");
+    if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_wc_hydrostatic: periodic meshes only");
+    if (!(wd->eos_k > 0.0)) return fail(ctx, NOVA_E_INVALID, "nova_wc_hydrostatic: eos_k must be positive");
+    launch_wc_hydrostatic(ctx->g, ctx->md.L[2] / ctx->md.N[2], wd->g[2], rho0, wd->eos_k, T->d64, p->d64, rho->d64,
+                          ctx->stream);
+    ctx->launches += 1;
+    CKL("k_wc_hydrostatic");
+    CK(cudaStreamSynchronize(ctx->stream));
     return NOVA_OK;
 }
 

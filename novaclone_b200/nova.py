@@ -26,6 +26,7 @@ RK_LITERAL, RK_CLASSICAL = 0, 1
 HIST_COLS = 6
 K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG, K_ADJ = range(6)
 OBJ_EKIN_FINAL = 0
+WC_TG, WC_SHEAR = 0, 1
 STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_OOM", 4: "NOVA_E_NONFINITE",
                 5: "NOVA_E_TIMEOUT", 6: "NOVA_E_UNSUPPORTED"}
 
@@ -36,8 +37,8 @@ EXPORTS = (
     "nova_field_upload", "nova_field_download",
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
-    "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_checkpoint_write",
-    "nova_checkpoint_read", "nova_profile_enable", "nova_profile_read",
+    "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_advance_wc",
+    "nova_wc_hydrostatic", "nova_checkpoint_write", "nova_checkpoint_read", "nova_profile_enable", "nova_profile_read",
     "nova_launch_count",
 )
 
@@ -63,6 +64,15 @@ class AdjDesc(C.Structure):
 
 class State(C.Structure):
     _fields_ = [("U", C.c_void_p), ("p", C.c_void_p), ("B", C.c_void_p), ("pB", C.c_void_p)]
+
+
+class WcDesc(C.Structure):
+    _fields_ = [("wc_case", C.c_int), ("diag_every", C.c_int), ("dt", C.c_double), ("mu", C.c_double),
+                ("ka", C.c_double), ("eos_k", C.c_double), ("g", C.c_double * 3), ("t0", C.c_double)]
+
+
+class WcState(C.Structure):
+    _fields_ = [("U", C.c_void_p), ("rho", C.c_void_p), ("p", C.c_void_p), ("T", C.c_void_p)]
 
 
 class NovaError(RuntimeError):
@@ -111,6 +121,8 @@ def load_library(path: str = LIB_PATH):
         "nova_field_maxabs_noalloc": [vp, vp, dp],
         "nova_advance": [vp, C.POINTER(RunDesc), C.POINTER(State), C.c_int, dp],
         "nova_adjoint_grad": [vp, C.POINTER(AdjDesc), C.POINTER(State), vp, vp, dp],
+        "nova_advance_wc": [vp, C.POINTER(WcDesc), C.POINTER(WcState), C.c_int, dp],
+        "nova_wc_hydrostatic": [vp, C.POINTER(WcDesc), C.c_double, vp, vp, vp],
         "nova_checkpoint_write": [vp, C.c_char_p, C.POINTER(State), C.c_double, C.c_longlong],
         "nova_checkpoint_read": [vp, C.c_char_p, C.POINTER(State), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "nova_profile_enable": [vp, C.c_int],
@@ -412,3 +424,25 @@ def checkpoint_read(mesh: Mesh, path: str, U=None, p=None, B=None, pB=None):
     t, step = C.c_double(), C.c_longlong()
     mesh.check(mesh.lib.nova_checkpoint_read(mesh.h, os.fsencode(path), C.byref(st), C.byref(t), C.byref(step)))
     return t.value, step.value
+
+
+def wc_desc(case="shear", dt=0.01, mu=0.0, ka=0.0, eos_k=50.0, g=(0.0, 0.0, 0.0), diag_every=1, t0=0.0):
+    """nova_wc_desc: case "tg" (app/TG) or "shear" (app/shearLayerWC)."""
+    d = WcDesc()
+    d.wc_case = WC_SHEAR if case == "shear" else WC_TG
+    d.diag_every, d.dt, d.mu, d.ka, d.eos_k, d.t0 = int(diag_every), dt, mu, ka, eos_k, t0
+    d.g[:] = [float(v) for v in g]
+    return d
+
+
+def advance_wc(mesh: Mesh, wd: WcDesc, U: Field, rho: Field, p: Field, T: Field = None, nsteps: int = 1):
+    """nsteps of the weakly-compressible loop bodies; returns the diagnostics rows."""
+    st = WcState(U.h, rho.h, p.h, T.h if T is not None else None)
+    hist = np.zeros((nsteps, HIST_COLS))
+    mesh.check(mesh.lib.nova_advance_wc(mesh.h, C.byref(wd), C.byref(st), int(nsteps), _dptr(hist)))
+    return hist
+
+
+def wc_hydrostatic(mesh: Mesh, wd: WcDesc, rho0: float, T: Field, p: Field, rho: Field):
+    """Initial p and rho of the weakly-compressible shear layer for a given T."""
+    mesh.check(mesh.lib.nova_wc_hydrostatic(mesh.h, C.byref(wd), float(rho0), T.h, p.h, rho.h))
