@@ -925,7 +925,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
-            launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, Ustar, nullptr, nullptr, divisor, ctx->d_rhs, st);
+            const cudaError_t e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, Ustar, nullptr, nullptr,
+                                                  divisor, ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            if (e != cudaSuccess) return stage_fail(ctx, e);
             ctx->launches += 1;
         }
         CKL("k_div_tiled");
@@ -937,8 +939,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         }
         {
             ProfScope ps(ctx, NOVA_K_CORRECT);
-            launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, Ustar, Y->d64, nullptr,
-                           nullptr, nullptr, nullptr, st);
+            const cudaError_t e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, Ustar,
+                                                 Y->d64, nullptr, nullptr, nullptr, nullptr, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            if (e != cudaSuccess) return stage_fail(ctx, e);
             ctx->launches += 1;
         }
         fix64(Y->d64);
@@ -991,7 +994,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
-            launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo, divisor, ctx->d_rhs, st);
+            const cudaError_t e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo,
+                                                  divisor, ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            if (e != cudaSuccess) return stage_fail(ctx, e);
             ctx->launches += 1;
         }
         CKL("k_div_tiled");
@@ -1003,8 +1008,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         }
         {
             ProfScope ps(ctx, NOVA_K_CORRECT);
-            launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, nullptr, nullptr, Ushi, Uslo,
-                           Y->hi, Y->lo, st);
+            const cudaError_t e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, nullptr,
+                                                 nullptr, Ushi, Uslo, Y->hi, Y->lo, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            if (e != cudaSuccess) return stage_fail(ctx, e);
             ctx->launches += 1;
         }
         fixpair(Y->hi, Y->lo);
@@ -1115,14 +1121,16 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
     run(3, StageArgs64{Y4, nullptr, nullptr, A, Uout});
     if (sst != NOVA_OK) return sst;
     CKL("stage kernel");
-    launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt, ctx->d_rhs,
-                    st);
+    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt,
+                                    ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+    if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, ctx->w64[1]);
     if (s != NOVA_OK) return s;
-    launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->w64[1], rd->dt, Uout, Uout, nullptr,
-                   nullptr, nullptr, nullptr, st);
+    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->w64[1], rd->dt, Uout, Uout, nullptr,
+                       nullptr, nullptr, nullptr, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+    if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_correct_tiled");
     return NOVA_OK;
@@ -1132,14 +1140,16 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
 nova_status project64(nova_ctx *ctx, const double *in, double *out, double *pbuf)
 {
     const Geo &g = ctx->g;
-    launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, in, nullptr, nullptr, 1.0, ctx->d_rhs,
-                    ctx->stream);
+    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, in, nullptr, nullptr, 1.0,
+                                    ctx->d_rhs, ctx->stream, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+    if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, pbuf);
     if (s != NOVA_OK) return s;
-    launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, 1.0, in, out, nullptr, nullptr, nullptr,
-                   nullptr, ctx->stream);
+    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, 1.0, in, out, nullptr, nullptr,
+                       nullptr, nullptr, ctx->stream, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+    if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_correct_tiled");
     return NOVA_OK;

@@ -631,9 +631,12 @@ inline unsigned nblocks(long long n, int b) { return (unsigned)((n + b - 1) / b)
     default: { constexpr int HH = 4; __VA_ARGS__; } break; \
     }
 
-void launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
-                     const double *U64, const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st)
+cudaError_t launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
+                            const double *U64, const float *hi, const float *lo, double divisor, double *rhs,
+                            cudaStream_t st, const StageExec &ex)
 {
+    if (ex.err && h == 3 && !wl.on && ex.impl != STAGE_MARCH && proj_tma_fits(g))
+        return launch_div_tma(g, co, ia, U64, hi, lo, divisor, rhs, ex.err, st);
     const int ch = pick_ichunk(g, 3);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
 #define NOVA_DIV(LDT, LDV, W)                                                                             \
@@ -651,6 +654,7 @@ void launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<do
         }
     }
 #undef NOVA_DIV
+    return cudaSuccess;
 }
 
 void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const double *ky2, const double *kz2,
@@ -660,10 +664,12 @@ void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const dou
     k_scale<<<nblocks(tot, 256), 256, 0, st>>>(g, ny, (cuDoubleComplex *)spec, kx2, ky2, kz2, invN3);
 }
 
-void launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
-                    const double *p, double s, const double *Us64, double *U64, const float *Ushi, const float *Uslo,
-                    float *hi, float *lo, cudaStream_t st)
+cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
+                           const double *p, double s, const double *Us64, double *U64, const float *Ushi,
+                           const float *Uslo, float *hi, float *lo, cudaStream_t st, const StageExec &ex)
 {
+    if (ex.err && h == 3 && !pw.on && ex.impl != STAGE_MARCH && proj_tma_fits(g))
+        return launch_correct_tma(g, co, ia, p, s, Us64, U64, Ushi, Uslo, hi, lo, ex.err, st);
     const int ch = pick_ichunk(g, 4);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
 #define NOVA_CORR(SPL, W)                                                                                 \
@@ -677,6 +683,7 @@ void launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<dou
         if (pw.on) { NOVA_CORR(true, true); } else { NOVA_CORR(true, false); }
     }
 #undef NOVA_CORR
+    return cudaSuccess;
 }
 
 int diag_blocks(const Geo &g)

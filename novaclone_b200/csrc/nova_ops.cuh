@@ -15,14 +15,27 @@ struct WallFix {
     double val[2][9];
 };
 
-void launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
-                     const double *U64, const float *hi, const float *lo, double divisor, double *rhs, cudaStream_t st);
+// ex: with a non-null error word (ex.err) the TMA-pipelined kernels of
+// nova_proj_tma.cu run where the mesh fits them (proj_tma_fits: periodic y,
+// N2 % 32 == 0, N1 % 16 == 0, N1 >= 32) and StageExec::impl is not
+// STAGE_MARCH; otherwise the tiled march kernels.  Returns
+// cudaErrorInvalidValue when a tensor map cannot be encoded.
+cudaError_t launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
+                            const double *U64, const float *hi, const float *lo, double divisor, double *rhs,
+                            cudaStream_t st, const StageExec &ex = StageExec{STAGE_MARCH, nullptr});
 // ny: y extent of the spectrum (the unique y nodes of the transform)
 void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const double *ky2, const double *kz2,
                   double invN3, cudaStream_t st);
-void launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
-                    const double *p, double s, const double *Us64, double *U64, const float *Ushi, const float *Uslo,
-                    float *hi, float *lo, cudaStream_t st);
+cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
+                           const double *p, double s, const double *Us64, double *U64, const float *Ushi,
+                           const float *Uslo, float *hi, float *lo, cudaStream_t st,
+                           const StageExec &ex = StageExec{STAGE_MARCH, nullptr});
+bool proj_tma_fits(const Geo &g);
+cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *hi,
+                           const float *lo, double divisor, double *rhs, int *err, cudaStream_t st);
+cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,
+                               const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi,
+                               float *lo, int *err, cudaStream_t st);
 int diag_blocks(const Geo &g);
 void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                  const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
