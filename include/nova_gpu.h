@@ -235,6 +235,28 @@ nova_status nova_wc_hydrostatic(nova_ctx *ctx, const nova_wc_desc *wd, double rh
 nova_status nova_checkpoint_write(nova_ctx *ctx, const char *path, const nova_state *st, double t, long long step);
 nova_status nova_checkpoint_read(nova_ctx *ctx, const char *path, nova_state *st, double *t, long long *step);
 
+/* ---- EnSight Gold output (and input) in the reference's layout ----
+ * The files the reference writes for post-processing (one rank, processor 0000):
+ *   <dir>/geom.p0000.geo          block rectilinear, N+1 nodes per axis, float32
+ *                                 coordinates (src/Mesh/Mesh.cpp:224-300)
+ *   <dir>/fd.p0000.case, <dir>/restart.p.0000.case   the case file with the
+ *                                 reference's variable list and the output times
+ *                                 (Mesh.cpp:302-355)
+ *   <dir>/<name>.0000.<num:05>.dat  float32 values over nodes 0..N of every axis
+ *                                 (periodic duplicate included), i fastest,
+ *                                 component by component (src/Field/Field.hxx:404-453)
+ * The host functions need no GPU: soa is the stored-node layout [c][i][j][k] of
+ * nova_field_download_soa.  nova_ensight_read_* is Field<T>::read
+ * (Field.hxx:456-485): it restores float32 values.  Errors: NOVA_E_INVALID. */
+nova_status nova_ensight_write_geometry(const nova_mesh_desc *md, const char *dir);
+nova_status nova_ensight_write_case(const char *dir, int ntimes, const double *times);
+nova_status nova_ensight_write_host(const nova_mesh_desc *md, const double *soa, int ncomp, const char *dir,
+                                    const char *name, int num);
+nova_status nova_ensight_read_host(const nova_mesh_desc *md, double *soa, int ncomp, const char *dir,
+                                   const char *name, int num);
+nova_status nova_ensight_write_field(nova_ctx *ctx, const nova_field *f, const char *dir, const char *name, int num);
+nova_status nova_ensight_read_field(nova_ctx *ctx, nova_field *f, const char *dir, const char *name, int num);
+
 /* ---- instrumentation: per-kernel CUDA-event timing of nova_advance ---- */
 typedef enum { NOVA_K_STAGE = 0, NOVA_K_DIV = 1, NOVA_K_FFT = 2, NOVA_K_CORRECT = 3, NOVA_K_DIAG = 4, NOVA_K_ADJ = 5,
                NOVA_K_COUNT = 6 } nova_kernel_class;

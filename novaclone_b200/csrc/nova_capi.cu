@@ -2,6 +2,7 @@
 // drop-in operators, the cuFFT projection and the fused time advance.
 #include "nova_gpu.h"
 #include "nova_internal.cuh"
+#include "nova_mesh.cuh"
 #include "nova_ops.cuh"
 #include "nova_wc.cuh"
 
@@ -180,21 +181,6 @@ nova_status dalloc(nova_ctx *ctx, T **p, size_t n)
     return cuda_check(ctx, cudaMalloc((void **)p, sizeof(T) * (n ? n : 1)), "cudaMalloc");
 }
 
-// Mesh::z (src/Mesh/Mesh.cpp:373-407) for a single rank
-double mesh_z(const nova_mesh_desc &m, int h, double bcoef, int k)
-{
-    const double dz = m.L[2] / m.N[2];
-    if (m.hyperbolic_z) {
-        const double A = std::pow(m.s1 / m.s2, 0.5);
-        const int globK = k - h + (int)(long)m.origin[2];
-        const int globN = m.N[2] + 1;
-        const double R = (double)globK / (double)(globN - 1) - 0.5;
-        const double U = 1.0 + std::tanh(bcoef * R) / std::tanh(bcoef / 2.0);
-        return U / (2.0 * A + (1 - A) * U) * m.L[2];
-    }
-    return (k - h) * dz + m.origin[2];
-}
-
 // Mesh::dzdxi_, d2zdxi2_ (src/Mesh/Mesh.cpp:146-179)
 void mesh_metrics(const nova_mesh_desc &m, std::vector<double> &dz1, std::vector<double> &dz2)
 {
@@ -202,11 +188,7 @@ void mesh_metrics(const nova_mesh_desc &m, std::vector<double> &dz1, std::vector
     const int nk = m.N[2] + 1 + m.m;
     const double *c = kCoef[(m.m - 2) / 2];
     const double dz = m.L[2] / m.N[2];
-    double b = 1.0;
-    if (m.hyperbolic_z) {
-        const int globN = m.N[2] + 1;
-        for (int i = 1; i < 10000; i++) b = std::asinh(b / ((globN - 1) * std::pow(m.s1 * m.s2, 0.5)));
-    }
+    const double b = mesh_hyp_b(m);
     dz1.assign(nk, 0.0);
     dz2.assign(nk, 0.0);
     for (int k = h; k < nk - h; k++) {
@@ -1514,6 +1496,32 @@ extern "C" nova_status nova_checkpoint_read(nova_ctx *ctx, const char *path, nov
     }
     if (t) *t = tt;
     if (step) *step = st64;
+    return NOVA_OK;
+}
+
+// =================================================================== EnSight ==
+extern "C" nova_status nova_ensight_write_field(nova_ctx *ctx, const nova_field *f, const char *dir, const char *name,
+                                                int num)
+{
+    if (!ctx || !f || !dir || !name) return fail(ctx, NOVA_E_INVALID, "nova_ensight_write_field: null argument");
+    std::vector<double> host((size_t)f->nc * ctx->g.N3);
+    nova_status s = soa_out(ctx, f, host.data(), cudaMemcpyDeviceToHost);
+    if (s != NOVA_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (nova_ensight_write_host(&ctx->md, host.data(), f->nc, dir, name, num) != NOVA_OK)
+        return fail(ctx, NOVA_E_INVALID, std::string("nova_ensight_write_field: cannot write ") + dir + "/" + name);
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_ensight_read_field(nova_ctx *ctx, nova_field *f, const char *dir, const char *name, int num)
+{
+    if (!ctx || !f || !dir || !name) return fail(ctx, NOVA_E_INVALID, "nova_ensight_read_field: null argument");
+    std::vector<double> host((size_t)f->nc * ctx->g.N3);
+    if (nova_ensight_read_host(&ctx->md, host.data(), f->nc, dir, name, num) != NOVA_OK)
+        return fail(ctx, NOVA_E_INVALID, std::string("nova_ensight_read_field: cannot read ") + dir + "/" + name);
+    nova_status s = soa_in(ctx, f, host.data(), cudaMemcpyHostToDevice);
+    if (s != NOVA_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream));
     return NOVA_OK;
 }
 

@@ -38,7 +38,9 @@ EXPORTS = (
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
     "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_advance_wc",
-    "nova_wc_hydrostatic", "nova_checkpoint_write", "nova_checkpoint_read", "nova_profile_enable", "nova_profile_read",
+    "nova_wc_hydrostatic", "nova_checkpoint_write", "nova_checkpoint_read", "nova_ensight_write_geometry",
+    "nova_ensight_write_case", "nova_ensight_write_host", "nova_ensight_read_host", "nova_ensight_write_field",
+    "nova_ensight_read_field", "nova_profile_enable", "nova_profile_read",
     "nova_launch_count",
 )
 
@@ -123,6 +125,12 @@ def load_library(path: str = LIB_PATH):
         "nova_adjoint_grad": [vp, C.POINTER(AdjDesc), C.POINTER(State), vp, vp, dp],
         "nova_advance_wc": [vp, C.POINTER(WcDesc), C.POINTER(WcState), C.c_int, dp],
         "nova_wc_hydrostatic": [vp, C.POINTER(WcDesc), C.c_double, vp, vp, vp],
+        "nova_ensight_write_geometry": [C.POINTER(MeshDesc), C.c_char_p],
+        "nova_ensight_write_case": [C.c_char_p, C.c_int, dp],
+        "nova_ensight_write_host": [C.POINTER(MeshDesc), dp, C.c_int, C.c_char_p, C.c_char_p, C.c_int],
+        "nova_ensight_read_host": [C.POINTER(MeshDesc), dp, C.c_int, C.c_char_p, C.c_char_p, C.c_int],
+        "nova_ensight_write_field": [vp, vp, C.c_char_p, C.c_char_p, C.c_int],
+        "nova_ensight_read_field": [vp, vp, C.c_char_p, C.c_char_p, C.c_int],
         "nova_checkpoint_write": [vp, C.c_char_p, C.POINTER(State), C.c_double, C.c_longlong],
         "nova_checkpoint_read": [vp, C.c_char_p, C.POINTER(State), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "nova_profile_enable": [vp, C.c_int],
@@ -446,3 +454,61 @@ def advance_wc(mesh: Mesh, wd: WcDesc, U: Field, rho: Field, p: Field, T: Field 
 def wc_hydrostatic(mesh: Mesh, wd: WcDesc, rho0: float, T: Field, p: Field, rho: Field):
     """Initial p and rho of the weakly-compressible shear layer for a given T."""
     mesh.check(mesh.lib.nova_wc_hydrostatic(mesh.h, C.byref(wd), float(rho0), T.h, p.h, rho.h))
+
+
+# ----------------------------------------------------------------- EnSight --
+class ensight:
+    """EnSight Gold files in the reference's layout (src/Mesh/Mesh.cpp:224-355,
+    src/Field/Field.hxx:404-485).  The host functions need no GPU."""
+
+    @staticmethod
+    def mesh_desc(N, L=(2 * math.pi,) * 3, origin=(0.0, 0.0, 0.0), m=6, hyperbolic_z=None, walls=(0, 0, 0)):
+        d = MeshDesc()
+        d.N[:] = [int(v) for v in N]
+        d.L[:] = [float(v) for v in L]
+        d.origin[:] = [float(v) for v in origin]
+        d.m = int(m)
+        d.hyperbolic_z = int(hyperbolic_z is not None)
+        d.s1, d.s2 = hyperbolic_z if hyperbolic_z is not None else (0.0, 0.0)
+        d.walls[:] = [int(v) for v in walls]
+        return d
+
+    @staticmethod
+    def _check(st, what):
+        if st != OK:
+            raise NovaError(st, what)
+
+    @staticmethod
+    def write_geometry(md: MeshDesc, dir: str):
+        ensight._check(load_library().nova_ensight_write_geometry(C.byref(md), os.fsencode(dir)), dir)
+
+    @staticmethod
+    def write_case(dir: str, times):
+        t = np.ascontiguousarray(times, np.float64)
+        ensight._check(load_library().nova_ensight_write_case(os.fsencode(dir), len(t), _dptr(t)), dir)
+
+    @staticmethod
+    def write_host(md: MeshDesc, soa, dir: str, name: str, num: int):
+        a = np.ascontiguousarray(soa, np.float64)
+        nc = a.shape[0] if a.ndim == 4 else 1
+        ensight._check(load_library().nova_ensight_write_host(C.byref(md), _dptr(a), nc, os.fsencode(dir),
+                                                              name.encode(), int(num)), name)
+
+    @staticmethod
+    def read_host(md: MeshDesc, nc: int, dir: str, name: str, num: int):
+        shape = (nc,) + tuple(md.N[a] + md.walls[a] for a in range(3))
+        out = np.zeros(shape)
+        ensight._check(load_library().nova_ensight_read_host(C.byref(md), _dptr(out), nc, os.fsencode(dir),
+                                                             name.encode(), int(num)), name)
+        return out
+
+    @staticmethod
+    def write_field(f: Field, dir: str, name: str, num: int):
+        M = f.mesh
+        M.check(M.lib.nova_ensight_write_field(M.h, f.h, os.fsencode(dir), name.encode(), int(num)))
+
+    @staticmethod
+    def read_field(f: Field, dir: str, name: str, num: int):
+        M = f.mesh
+        M.check(M.lib.nova_ensight_read_field(M.h, f.h, os.fsencode(dir), name.encode(), int(num)))
+        return f

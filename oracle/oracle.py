@@ -457,6 +457,39 @@ def ref_wc_init(mesh, T, *, c, rho0, gz):
         return tuple(np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (1,)) for k in ("p", "rho"))
 
 
+def ref_ensight(mesh, U, p, *, nsteps, dt, outdir):
+    """The reference's EnSight output (Mesh::write, Field<T>::write after each of
+    nsteps steps) of ghosted U and p into outdir (oracle/_ref/nova_ref ensight)."""
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        write_case(case, mesh)
+        np.ascontiguousarray(U, np.float64).tofile(os.path.join(td, "U.bin"))
+        np.ascontiguousarray(p, np.float64).tofile(os.path.join(td, "p.bin"))
+        subprocess.run([REF_BIN, "ensight", case, str(nsteps), repr(float(dt)), os.path.join(td, "U.bin"),
+                        os.path.join(td, "p.bin"), outdir, "-m", str(mesh.m)], check=True, stdout=subprocess.DEVNULL)
+
+
+def ensight_parse(path, kind, n=None, nc=1):
+    """EnSight Gold file -> dict of its content: header lines as text up to the
+    first NUL, integers and float32 arrays.  kind "geo" or "dat"; n = nodes per axis."""
+    b = open(path, "rb").read()
+    text = lambda o: b[o:o + 80].split(b"\0")[0].decode()
+    if kind == "geo":
+        lines = [text(80 * i) for i in range(6)]
+        o = 480
+        part = int(np.frombuffer(b, np.int32, 1, o)[0])
+        lines += [text(o + 4), text(o + 84)]
+        o += 164
+        dims = np.frombuffer(b, np.int32, 3, o)
+        o += 12
+        coords = np.frombuffer(b, np.float32, int(dims.sum()), o)
+        return {"lines": lines, "part": part, "dims": dims.copy(), "coords": coords.copy(), "size": len(b)}
+    lines = [text(0), text(80), text(164)]
+    part = int(np.frombuffer(b, np.int32, 1, 160)[0])
+    vals = np.frombuffer(b, np.float32, offset=244)
+    return {"lines": lines, "part": part, "values": vals.copy(), "size": len(b)}
+
+
 # ------------------------------------------------------------- initial data --
 
 def ic_taylor_green(mesh):

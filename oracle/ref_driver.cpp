@@ -12,6 +12,7 @@
  *   nova_ref ops <case> <nu> <U.bin> <s.bin> <out>
  *   nova_ref wc <case> <tg|shear> <nsteps> <dt> <mu> <ka> <c> <rho0> <gz> <U.bin> <rho.bin> <p.bin> <T.bin|-> <out>
  *   nova_ref wcinit <case> <c> <rho0> <gz> <T.bin> <out>
+ *   nova_ref ensight <case> <nsteps> <dt> <U.bin> <p.bin> <dir>
  *   (any may end with the reference's `-m <order>` option)
  *
  * `wc` runs the compressible loop bodies: app/TG (rhoEqn.H, pEqn.H, UEqn.H in
@@ -309,15 +310,42 @@ static int wcinit(int argc, char **argv)
     return 0;
 }
 
+/* the apps' output after each step: Mesh::write (geometry, case, restart) and Field<T>::write */
+static int ensight(int argc, char **argv)
+{
+    if (argc < 8) { std::fprintf(stderr, "usage: ensight <case> <nsteps> <dt> <U> <p> <dir>\n"); return 2; }
+    settings::zoneName() = argv[2];
+    const int nsteps = std::atoi(argv[3]);
+    const double dt = std::atof(argv[4]);
+    const std::string dir = argv[7];
+    Time time(dt, dt * (nsteps + 0.5), 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+    Field<vector> U(mesh, vector(0, 0, 0), "U");
+    Field<scalar> p(mesh, 0, "p");
+    load(U, argv[5]);
+    load(p, argv[6]);
+    U.correctBoundaryConditions();
+    p.correctBoundaryConditions();
+    for (int step = 0; step < nsteps; step++) {
+        time++;
+        mesh.write(dir);
+        U.write(dir, "U");
+        p.write(dir, "p");
+    }
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
-    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit ... [-m order]\n"); return 2; }
+    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit|ensight ... [-m order]\n"); return 2; }
     settings::process(argc, argv); /* the reference's own -m option (settings.cpp:53-78) */
     std::string mode = argv[1];
     if (mode == "run") return run(argc, argv);
     if (mode == "ops") return ops(argc, argv);
     if (mode == "wc") return wc(argc, argv);
     if (mode == "wcinit") return wcinit(argc, argv);
+    if (mode == "ensight") return ensight(argc, argv);
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;
 }

@@ -82,6 +82,52 @@ def wc_shear_case(name, N, nsteps, cfl=0.3, mach=0.1, seed=0):
                         T=M.unique(r[3]), hist=r[4], **{k: np.array(v) for k, v in prm.items()})
 
 
+def ensight_case(name, N, L, origin, seed, walls=False):
+    """the reference's EnSight output of seeded U and p (Mesh::write, Field<T>::write, 2 steps)"""
+    import tempfile
+    M = O.Mesh(N, L=L, origin=origin)
+    rng = np.random.default_rng(seed)
+    bc = None
+    if walls:
+        n1 = N[1] + 1  # the wall nodes are stored: seed the N1+1 rows, apply the reference's BCs
+        U = rng.standard_normal((3, N[0], n1, N[2]))
+        p = rng.standard_normal((1, N[0], n1, N[2]))
+        bc = {"U": {"north": [(1, 0.0), (2, 0.0), (1, 0.0)], "south": [(1, 0.0), (2, 0.0), (1, 0.0)]},
+              "p": {"north": (1, 0.0), "south": (1, 0.0)}}
+        Ug, pg = M.zeros(3), M.zeros(1)
+        h = M.h
+        Ug[h:h + N[0], h:h + n1, h:h + N[2]] = np.moveaxis(U, 0, -1)
+        pg[h:h + N[0], h:h + n1, h:h + N[2]] = np.moveaxis(p, 0, -1)
+        Ug, pg = O.bc_apply(M, Ug, bc["U"]), O.bc_apply(M, pg, bc["p"])
+        U = np.ascontiguousarray(np.moveaxis(Ug[h:h + N[0], h:h + n1, h:h + N[2]], -1, 0))
+        p = np.ascontiguousarray(np.moveaxis(pg[h:h + N[0], h:h + n1, h:h + N[2]], -1, 0))
+    else:
+        U = rng.standard_normal((3,) + M.N)
+        p = rng.standard_normal((1,) + M.N)
+        Ug, pg = M.to_ghosted(U), M.to_ghosted(p)
+    dt = 0.125
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        O.write_case(case, M, bc)
+        Ug.tofile(os.path.join(td, "U.bin"))
+        pg.tofile(os.path.join(td, "p.bin"))
+        out = os.path.join(td, "out")
+        os.makedirs(out)
+        import subprocess
+        subprocess.run([O.REF_BIN, "ensight", case, "2", repr(dt), os.path.join(td, "U.bin"), os.path.join(td, "p.bin"),
+                        out, "-m", str(M.m)], check=True, stdout=subprocess.DEVNULL)
+        geo = O.ensight_parse(os.path.join(out, "geom.p0000.geo"), "geo")
+        dat = {k: O.ensight_parse(os.path.join(out, "%s.0000.00002.dat" % k), "dat") for k in ("U", "p")}
+        case_text = open(os.path.join(out, "fd.p0000.case")).read()
+        restart_text = open(os.path.join(out, "restart.p.0000.case")).read()
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(L), origin=np.array(origin),
+                        walls=np.array(int(walls)), U=U, p=p, times=np.array([0.0, dt]),
+                        geo_lines=np.array(geo["lines"]), geo_dims=geo["dims"], geo_coords=geo["coords"],
+                        geo_size=np.array(geo["size"]), dat_lines=np.array(dat["U"]["lines"]),
+                        U_values=dat["U"]["values"], p_values=dat["p"]["values"], case_text=np.array(case_text),
+                        restart_text=np.array(restart_text))
+
+
 CASES = {
     "ops_10x8x6.npz": lambda n: ops_case(n, (10, 8, 6), (2 * np.pi, 2.0, 3.0), 7, 0.01),
     "ops_16x12x8_m4.npz": lambda n: ops_case(n, (16, 12, 8), (2 * np.pi,) * 3, 8, 0.02, m=4),
@@ -91,6 +137,8 @@ CASES = {
     "ot_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "literal", 4, 0.01, 1e-3, 1e-3),
     "wc_tg_12.npz": lambda n: wc_tg_case(n, (12, 12, 12), 5, 0.02, 1 / 1600),
     "wc_shear_12x8x16.npz": lambda n: wc_shear_case(n, (12, 8, 16), 4),
+    "ensight_7x5x6.npz": lambda n: ensight_case(n, (7, 5, 6), (2.0, 1.5, 3.0), (0.5, -1.0, 0.25), 11),
+    "ensight_walls_6x8x5.npz": lambda n: ensight_case(n, (6, 8, 5), (1.0, 2.0, 1.5), (0.0, 0.0, 0.0), 12, True),
 }
 
 

@@ -89,3 +89,13 @@ def test_a_checkpoint_of_another_mesh_is_refused(nova, tmp_path):
     with pytest.raises(nova.NovaError) as e:
         nova.checkpoint_read(M, str(tmp_path / "missing.nova"), U)
     assert e.value.status == nova.E_INVALID
+
+
+def test_ensight_field_round_trip(nova, tmp_path):
+    """nova_ensight_write_field / read_field: the reference's float32 restart path."""
+    M = nova.Mesh((16, 12, 8), walls=(0, 1, 0))
+    x = np.random.default_rng(4).standard_normal((3,) + M.shape)
+    U = nova.Field(M, 3).upload_soa(x)
+    nova.ensight.write_field(U, str(tmp_path), "U", 3)
+    V = nova.ensight.read_field(nova.Field(M, 3), str(tmp_path), "U", 3)
+    assert np.array_equal(V.download_soa(), x.astype(np.float32).astype(np.float64))
