@@ -149,6 +149,15 @@ nova_status nova_div_vf(nova_ctx *ctx, const nova_field *U, const nova_field *f,
 nova_status nova_laplacian(nova_ctx *ctx, double nu, const nova_field *f, nova_field *out);
 /* poisson::rhs(rhs); poisson::solve(): p = L^-1 rhs on the unique nodes (mean mode 0) */
 nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, nova_field *p);
+/* ex:: variants no app's time advance calls (FP64):
+ *   ex::div(Field<tensor>)              src/ex/div/div.hxx:258-285  -> nova_div_t (9 -> 3)
+ *   ex::div(Field<symmTensor>)          div.hxx:222-255             -> nova_div_t (6 -> 3; xx xy xz yy yz zz)
+ *   ex::div(Field<scalar>, Field<tensor>) div.hxx:173-207            -> nova_div_st (1 x 9 -> 3)
+ *   ex::laplacian(Field<scalar>, Field<T>) src/ex/laplacian/laplacian.hxx:64-127 -> nova_laplacian_f
+ * The tensor divergences carry no z metric, as in the reference. */
+nova_status nova_div_t(nova_ctx *ctx, const nova_field *T, nova_field *out);
+nova_status nova_div_st(nova_ctx *ctx, const nova_field *s, const nova_field *T, nova_field *out);
+nova_status nova_laplacian_f(nova_ctx *ctx, const nova_field *nu, const nova_field *f, nova_field *out);
 nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *s, double *out);
 /* Allocation-free max|s| (no counterpart in the reference: tools::maximum
  * allocates its reduction buffers).  Same result as nova_field_maxabs, computed

@@ -745,7 +745,7 @@ static nova_status op_common(nova_ctx *ctx, int op, const nova_field *a, const n
         return fail(ctx, NOVA_E_UNSUPPORTED, "operator: the ex:: entry points take FP64 fields");
     if (a == out || (b && b == out)) return fail(ctx, NOVA_E_INVALID, "operator: output aliases an input");
     launch_op(op, ctx->h, ctx->g, walls_of<double>(ctx, a), walls_of<double>(ctx, b), ctx->co64, ctx->d_ia64,
-              ctx->d_corr64, a->d64, b ? b->d64 : nullptr, (op == OP_DIV_VF) ? b->nc : a->nc, nu, out->d64,
+              ctx->d_corr64, a->d64, b ? b->d64 : nullptr, (op == OP_DIV_VF || op == OP_LAP_F) ? b->nc : a->nc, nu, out->d64,
               ctx->stream);
     ctx->launches += 1;
     CKL("operator kernel");
@@ -771,6 +771,27 @@ extern "C" nova_status nova_curl(nova_ctx *ctx, const nova_field *U, nova_field 
 extern "C" nova_status nova_div_v(nova_ctx *ctx, const nova_field *U, nova_field *out)
 {
     return op_common(ctx, OP_DIV_V, U, nullptr, out, 3, 1, 0.0);
+}
+
+extern "C" nova_status nova_div_t(nova_ctx *ctx, const nova_field *T, nova_field *out)
+{
+    if (!ctx || !T) return fail(ctx, NOVA_E_INVALID, "nova_div_t: null argument");
+    if (T->nc != 9 && T->nc != 6) return fail(ctx, NOVA_E_INVALID, "nova_div_t: a tensor (9) or symmTensor (6) field");
+    return op_common(ctx, OP_DIV_T, T, nullptr, out, 0, 3, 0.0);
+}
+
+extern "C" nova_status nova_div_st(nova_ctx *ctx, const nova_field *s, const nova_field *T, nova_field *out)
+{
+    if (!ctx || !s || !T) return fail(ctx, NOVA_E_INVALID, "nova_div_st: null argument");
+    if (T->nc != 9) return fail(ctx, NOVA_E_INVALID, "nova_div_st: T must be a tensor (9) field");
+    return op_common(ctx, OP_DIV_ST, s, T, out, 1, 3, 0.0);
+}
+
+extern "C" nova_status nova_laplacian_f(nova_ctx *ctx, const nova_field *nu, const nova_field *f, nova_field *out)
+{
+    if (!ctx || !nu || !f || !out) return fail(ctx, NOVA_E_INVALID, "nova_laplacian_f: null argument");
+    if (out->nc != f->nc) return fail(ctx, NOVA_E_INVALID, "nova_laplacian_f: out must have the components of f");
+    return op_common(ctx, OP_LAP_F, nu, f, out, 1, 0, 0.0);
 }
 
 extern "C" nova_status nova_div_vf(nova_ctx *ctx, const nova_field *U, const nova_field *f, nova_field *out)

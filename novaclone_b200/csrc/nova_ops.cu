@@ -503,6 +503,92 @@ __global__ void k_op_lap(Geo g, Walls<double> wa, Coef<double> co, const double 
     }
 }
 
+// ex::div(Field<tensor>) (src/ex/div/div.hxx:258-285) and ex::div(Field<symmTensor>)
+// (div.hxx:222-255; storage xx xy xz yy yz zz): out_c = sum_d D_d T[c*3+d],
+// without the z metric, as in the reference
+template <int H>
+__global__ void k_op_div_t(Geo g, Walls<double> wa, Coef<double> co, const double *__restrict__ T, int symm,
+                           double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 F{T, g.N3, wa};
+    const int S[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int c = 0; c < 3; c++) {
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) r += dd1<H>(F, g, symm ? S[c * 3 + d] : c * 3 + d, i, j, k, d, co.a[d]);
+        out[(long long)c * g.N3 + t] = r;
+    }
+}
+
+// ex::div(Field<scalar> s, Field<tensor> T) (div.hxx:173-207): sum_d D_d (s T[c*3+d])
+template <int H>
+__global__ void k_op_div_st(Geo g, Walls<double> wa, Walls<double> wb, Coef<double> co, const double *__restrict__ s,
+                            const double *__restrict__ T, double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 Sf{s, g.N3, wa}, F{T, g.N3, wb};
+    for (int c = 0; c < 3; c++) {
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double q = 0.0;
+#pragma unroll
+            for (int l = 0; l < H; l++)
+                q = fma(co.a[d][l],
+                        at(Sf, g, 0, i, j, k, d, l + 1) * at(F, g, c * 3 + d, i, j, k, d, l + 1)
+                            - at(Sf, g, 0, i, j, k, d, -l - 1) * at(F, g, c * 3 + d, i, j, k, d, -l - 1),
+                        q);
+            r += q;
+        }
+        out[(long long)c * g.N3 + t] = r;
+    }
+}
+
+// ex::laplacian(Field<scalar> nu, Field<T>) (src/ex/laplacian/laplacian.hxx:64-127):
+// the + neighbour at 1+l weighted by nu at offset l, the - neighbour at -1-l
+// by nu at -1-l, both against the centre; z terms over dzdxi^2 and the
+// stretched-z term -nu(0) D_z f d2zdxi2/dzdxi^3
+template <int H>
+__global__ void k_op_lap_f(Geo g, Walls<double> wa, Walls<double> wb, Coef<double> co, const double *__restrict__ ia,
+                           const double *__restrict__ corr2, const double *__restrict__ nu, const double *__restrict__ f,
+                           int nc, double *__restrict__ out)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.N3) return;
+    int i, j, k;
+    pt_index(g, t, i, j, k);
+    Ld64 NU{nu, g.N3, wa}, F{f, g.N3, wb};
+    const double i2 = ia[k] * ia[k];
+    double az[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[k];
+    const double nu0 = NU(0, t);
+    for (int c = 0; c < nc; c++) {
+        const double f0 = F(c, t);
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double m = (d == 2) ? i2 : 1.0;
+#pragma unroll
+            for (int l = 0; l < H; l++) {
+                const double np = l == 0 ? nu0 : at(NU, g, 0, i, j, k, d, l);
+                const double nm = at(NU, g, 0, i, j, k, d, -l - 1);
+                const double fp = at(F, g, c, i, j, k, d, l + 1), fm = at(F, g, c, i, j, k, d, -l - 1);
+                r = fma(co.b[d][l] * m, fma(np, fp - f0, nm * (fm - f0)), r);
+            }
+        }
+        const double dz = dd1<H>(F, g, c, i, j, k, 2, az);
+        out[(long long)c * g.N3 + t] = fma(-nu0 * corr2[k], dz, r);
+    }
+}
+
 // ------------------------------------------------------------------ layout --
 // reference ghosted AoS (n0, n1, n2, nc) -> unique SoA
 __global__ void k_aos_to_soa(Geo g, int h, int n1, int n2, int nc, const double *__restrict__ aos,
@@ -781,6 +867,11 @@ void launch_op(int op, int h, const Geo &g, const Walls<double> &wa, const Walls
     case OP_DIV_V: NOVA_DISPATCH_H(h, (k_op_div_v<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, a, out))); break;
     case OP_CURL: NOVA_DISPATCH_H(h, (k_op_curl<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, a, out))); break;
     case OP_DIV_VF: NOVA_DISPATCH_H(h, (k_op_div_vf<HH><<<nb, 128, 0, st>>>(g, wa, wb, co, ia, a, b, nc, out))); break;
+    case OP_DIV_T: NOVA_DISPATCH_H(h, (k_op_div_t<HH><<<nb, 128, 0, st>>>(g, wa, co, a, nc == 6, out))); break;
+    case OP_DIV_ST: NOVA_DISPATCH_H(h, (k_op_div_st<HH><<<nb, 128, 0, st>>>(g, wa, wb, co, a, b, out))); break;
+    case OP_LAP_F:
+        NOVA_DISPATCH_H(h, (k_op_lap_f<HH><<<nb, 128, 0, st>>>(g, wa, wb, co, ia, corr2, a, b, nc, out)));
+        break;
     default: NOVA_DISPATCH_H(h, (k_op_lap<HH><<<nb, 128, 0, st>>>(g, wa, co, ia, corr2, nu, a, nc, out))); break;
     }
 }

@@ -5,7 +5,12 @@
 
 namespace nova {
 
-enum OpKind { OP_GRAD_S = 0, OP_GRAD_V = 1, OP_DIV_V = 2, OP_DIV_VF = 3, OP_LAP = 4, OP_CURL = 5 };
+enum OpKind {
+    OP_GRAD_S = 0, OP_GRAD_V = 1, OP_DIV_V = 2, OP_DIV_VF = 3, OP_LAP = 4, OP_CURL = 5,
+    OP_DIV_T = 6,   // div(tensor) (a: 9 comps) or div(symmTensor) (a: 6 comps)
+    OP_DIV_ST = 7,  // div(scalar a, tensor b)
+    OP_LAP_F = 8    // laplacian(Field nu = a, f = b with nc comps)
+};
 
 // wall-node overwrite per component: type 1 = Neumann, 2 = Dirichlet (0 = none)
 struct WallFix {

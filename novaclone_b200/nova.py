@@ -37,6 +37,7 @@ EXPORTS = (
     "nova_field_upload", "nova_field_download",
     "nova_field_upload_soa", "nova_field_download_soa", "nova_field_copy_from_device", "nova_field_copy_to_device",
     "nova_grad_s", "nova_grad_v", "nova_curl", "nova_div_v", "nova_div_vf", "nova_laplacian", "nova_poisson_solve",
+    "nova_div_t", "nova_div_st", "nova_laplacian_f",
     "nova_field_maxabs", "nova_field_maxabs_noalloc", "nova_advance", "nova_adjoint_grad", "nova_advance_wc",
     "nova_wc_hydrostatic", "nova_checkpoint_write", "nova_checkpoint_read", "nova_ensight_write_geometry",
     "nova_ensight_write_case", "nova_ensight_write_host", "nova_ensight_read_host", "nova_ensight_write_field",
@@ -119,6 +120,9 @@ def load_library(path: str = LIB_PATH):
         "nova_div_vf": [vp, vp, vp, vp],
         "nova_laplacian": [vp, C.c_double, vp, vp],
         "nova_poisson_solve": [vp, vp, vp],
+        "nova_div_t": [vp, vp, vp],
+        "nova_div_st": [vp, vp, vp, vp],
+        "nova_laplacian_f": [vp, vp, vp, vp],
         "nova_field_maxabs": [vp, vp, dp],
         "nova_field_maxabs_noalloc": [vp, vp, dp],
         "nova_advance": [vp, C.POINTER(RunDesc), C.POINTER(State), C.c_int, dp],
@@ -322,10 +326,17 @@ class ex:
 
     @staticmethod
     def div(U: Field, f: Field = None) -> Field:
+        """div(vector), div(vector, T), div(tensor), div(symmTensor), div(scalar, tensor)."""
         M = U.mesh
-        if f is None:
+        if f is None and U.nc in (6, 9):
+            out = Field(M, 3)
+            M.check(M.lib.nova_div_t(M.h, U.h, out.h))
+        elif f is None:
             out = Field(M, 1)
             M.check(M.lib.nova_div_v(M.h, U.h, out.h))
+        elif U.nc == 1:
+            out = Field(M, 3)
+            M.check(M.lib.nova_div_st(M.h, U.h, f.h, out.h))
         else:
             out = Field(M, f.nc)
             M.check(M.lib.nova_div_vf(M.h, U.h, f.h, out.h))
@@ -339,10 +350,14 @@ class ex:
         return out
 
     @staticmethod
-    def laplacian(nu: float, f: Field) -> Field:
+    def laplacian(nu, f: Field) -> Field:
+        """laplacian(scalar nu, T) or laplacian(Field<scalar> nu, T)."""
         M = f.mesh
         out = Field(M, f.nc)
-        M.check(M.lib.nova_laplacian(M.h, float(nu), f.h, out.h))
+        if isinstance(nu, Field):
+            M.check(M.lib.nova_laplacian_f(M.h, nu.h, f.h, out.h))
+        else:
+            M.check(M.lib.nova_laplacian(M.h, float(nu), f.h, out.h))
         return out
 
 

@@ -421,6 +421,111 @@ void orc_lap(const orc_mesh *M, double nu, const double *f, int nc, double *out)
 #undef F
 }
 
+/* ex::div(Field<tensor>) (src/ex/div/div.hxx:258-285) and ex::div(Field<symmTensor>)
+ * (div.hxx:222-255, tensor(symm) of src/Types/tensor/tensor.cpp:43-46 with the
+ * storage xx xy xz yy yz zz): out_c = sum_l N - S + E - W + T - B of component
+ * [c*3 + d], no z metric.  T holds 9 (symm = 0) or 6 (symm = 1) components. */
+static double tens(const double *T, long p, int symm, int r)
+{
+    static const int S[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    return symm ? T[p * 6 + S[r]] : T[p * 9 + r];
+}
+
+void orc_div_t(const orc_mesh *M, const double *T, int symm, double *out)
+{
+    const int h = M->h;
+    const double dx = M->d[0], dy = M->d[1], dz = M->d[2];
+    const double *co = M->coef;
+    memset(out, 0, sizeof(double) * 3 * npts(M));
+    for (int i = h; i < M->n[0] - h; i++)
+        for (int j = h; j < M->n[1] - h; j++)
+            for (int k = h; k < M->n[2] - h; k++) {
+                double *o = out + IDX(M, i, j, k) * 3;
+                for (int l = 0; l < h; l++)
+                    for (int c = 0; c < 3; c++) {
+                        o[c] += co[l] / 2.0 / (l + 1) / dy * tens(T, IDX(M, i, j + 1 + l, k), symm, c * 3 + 1);
+                        o[c] += -co[l] / 2.0 / (l + 1) / dy * tens(T, IDX(M, i, j - 1 - l, k), symm, c * 3 + 1);
+                        o[c] += co[l] / 2.0 / (l + 1) / dx * tens(T, IDX(M, i + 1 + l, j, k), symm, c * 3);
+                        o[c] += -co[l] / 2.0 / (l + 1) / dx * tens(T, IDX(M, i - 1 - l, j, k), symm, c * 3);
+                        o[c] += co[l] / 2.0 / (l + 1) / dz * tens(T, IDX(M, i, j, k + 1 + l), symm, c * 3 + 2);
+                        o[c] += -co[l] / 2.0 / (l + 1) / dz * tens(T, IDX(M, i, j, k - 1 - l), symm, c * 3 + 2);
+                    }
+            }
+}
+
+/* ex::div(Field<scalar> s, Field<tensor> T) (div.hxx:173-207): the same sums of s*T */
+void orc_div_sT(const orc_mesh *M, const double *s, const double *T, double *out)
+{
+    const int h = M->h;
+    const double dx = M->d[0], dy = M->d[1], dz = M->d[2];
+    const double *co = M->coef;
+    memset(out, 0, sizeof(double) * 3 * npts(M));
+#define SV(i, j, k) s[IDX(M, i, j, k)]
+#define TV(i, j, k, r) T[IDX(M, i, j, k) * 9 + (r)]
+    for (int i = h; i < M->n[0] - h; i++)
+        for (int j = h; j < M->n[1] - h; j++)
+            for (int k = h; k < M->n[2] - h; k++) {
+                double *o = out + IDX(M, i, j, k) * 3;
+                for (int l = 0; l < h; l++)
+                    for (int c = 0; c < 3; c++) {
+                        o[c] += co[l] / 2.0 / (l + 1) / dy * SV(i, j + 1 + l, k) * TV(i, j + 1 + l, k, c * 3 + 1);
+                        o[c] += -co[l] / 2.0 / (l + 1) / dy * SV(i, j - 1 - l, k) * TV(i, j - 1 - l, k, c * 3 + 1);
+                        o[c] += co[l] / 2.0 / (l + 1) / dx * SV(i + 1 + l, j, k) * TV(i + 1 + l, j, k, c * 3);
+                        o[c] += -co[l] / 2.0 / (l + 1) / dx * SV(i - 1 - l, j, k) * TV(i - 1 - l, j, k, c * 3);
+                        o[c] += co[l] / 2.0 / (l + 1) / dz * SV(i, j, k + 1 + l) * TV(i, j, k + 1 + l, c * 3 + 2);
+                        o[c] += -co[l] / 2.0 / (l + 1) / dz * SV(i, j, k - 1 - l) * TV(i, j, k - 1 - l, c * 3 + 2);
+                    }
+            }
+#undef SV
+#undef TV
+}
+
+/* ex::laplacian(Field<scalar> nu, Field<T>) (src/ex/laplacian/laplacian.hxx:64-127):
+ * the + neighbour weighted by nu at offset l, the - neighbour by nu at -1-l */
+void orc_lap_f(const orc_mesh *M, const double *nu, const double *f, int nc, double *out)
+{
+    const int h = M->h;
+    const double dx = M->d[0], dy = M->d[1], dz = M->d[2];
+    const double *co = M->coef;
+    memset(out, 0, sizeof(double) * nc * npts(M));
+#define F(i, j, k, c) f[IDX(M, i, j, k) * nc + (c)]
+#define NU(i, j, k) nu[IDX(M, i, j, k)]
+    for (int l = 0; l < h; l++)
+        for (int i = h; i < M->n[0] - h; i++)
+            for (int j = h; j < M->n[1] - h; j++) {
+                double *lp = out + IDX(M, i, j, 0) * nc;
+                for (int k = h; k < M->n[2] - h; k++) {
+                    const double zz = pow(M->dzdxi[k], 2);
+                    const double nN = NU(i, j + l, k), nS = NU(i, j - 1 - l, k), nE = NU(i + l, j, k),
+                                 nW = NU(i - 1 - l, j, k), nT = NU(i, j, k + l), nB = NU(i, j, k - 1 - l);
+                    for (int c = 0; c < nc; c++)
+                        lp[k * nc + c] += (nN * co[l] / pow((l + 1) * dy, 2) * F(i, j + 1 + l, k, c)
+                                           + nS * co[l] / pow((l + 1) * dy, 2) * F(i, j - 1 - l, k, c)
+                                           + nE * co[l] / pow((l + 1) * dx, 2) * F(i + 1 + l, j, k, c)
+                                           + nW * co[l] / pow((l + 1) * dx, 2) * F(i - 1 - l, j, k, c)
+                                           + nT * co[l] / pow((l + 1) * dz, 2) * F(i, j, k + 1 + l, c) / zz
+                                           + nB * co[l] / pow((l + 1) * dz, 2) * F(i, j, k - 1 - l, c) / zz
+                                           + (-(nE + nW) * co[l] / pow((l + 1) * dx, 2)
+                                              - (nN + nS) * co[l] / pow((l + 1) * dy, 2)
+                                              - (nT + nB) * co[l] / pow((l + 1) * dz, 2) / zz) * F(i, j, k, c));
+                }
+            }
+    for (int l = 0; l < h; l++)
+        for (int i = h; i < M->n[0] - h; i++)
+            for (int j = h; j < M->n[1] - h; j++) {
+                double *lp = out + IDX(M, i, j, 0) * nc;
+                for (int k = h; k < M->n[2] - h; k++) {
+                    const double z3 = pow(M->dzdxi[k], 3);
+                    for (int c = 0; c < nc; c++)
+                        lp[k * nc + c] -= (co[l] / 2.0 / (l + 1) / dz * F(i, j, k + 1 + l, c)
+                                           - co[l] / 2.0 / (l + 1) / dz * F(i, j, k - 1 - l, c))
+                                          * NU(i, j, k) * M->d2zdxi2[k] / z3;
+                }
+            }
+#undef F
+#undef NU
+}
+
 /* tools::maximum (src/Tools/Tools.h:19-36) for a scalar field */
 double orc_maximum(const orc_mesh *M, const double *f)
 {

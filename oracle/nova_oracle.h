@@ -45,6 +45,9 @@ void orc_curl(const orc_mesh *mesh, const double *U, double *out);              
 void orc_div_v(const orc_mesh *mesh, const double *U, double *out);             /* 3 -> 1 */
 void orc_div_vf(const orc_mesh *mesh, const double *U, const double *f, int nc, double *out);
 void orc_lap(const orc_mesh *mesh, double nu, const double *f, int nc, double *out);
+void orc_div_t(const orc_mesh *mesh, const double *T, int symm, double *out);
+void orc_div_sT(const orc_mesh *mesh, const double *s, const double *T, double *out);
+void orc_lap_f(const orc_mesh *mesh, const double *nu, const double *f, int nc, double *out);
 double orc_maximum(const orc_mesh *mesh, const double *f);                     /* scalar field */
 
 /* poisson::rhs + poisson::solve: p's N0*N1*N2 unique interior nodes are written. */

@@ -69,6 +69,9 @@ def lib():
         L.orc_div_v.argtypes = [C.c_void_p, dp, dp]
         L.orc_div_vf.argtypes = [C.c_void_p, dp, dp, C.c_int, dp]
         L.orc_lap.argtypes = [C.c_void_p, C.c_double, dp, C.c_int, dp]
+        L.orc_div_t.argtypes = [C.c_void_p, dp, C.c_int, dp]
+        L.orc_div_sT.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_lap_f.argtypes = [C.c_void_p, dp, dp, C.c_int, dp]
         L.orc_maximum.restype = C.c_double
         L.orc_maximum.argtypes = [C.c_void_p, dp]
         L.orc_poisson_solve.argtypes = [C.c_void_p, dp, dp]
@@ -199,6 +202,29 @@ def lap(mesh, nu, f):
     nc = f.shape[-1]
     out = mesh.zeros(nc)
     lib().orc_lap(mesh._p, float(nu), np.ascontiguousarray(f), nc, out)
+    return out
+
+
+def div_t(mesh, T):
+    """ex::div(Field<tensor>) (9 components) or ex::div(Field<symmTensor>) (6)."""
+    nc = T.shape[-1]
+    out = mesh.zeros(3)
+    lib().orc_div_t(mesh._p, np.ascontiguousarray(T), int(nc == 6), out)
+    return out
+
+
+def div_sT(mesh, s, T):
+    """ex::div(Field<scalar>, Field<tensor>)."""
+    out = mesh.zeros(3)
+    lib().orc_div_sT(mesh._p, np.ascontiguousarray(s), np.ascontiguousarray(T), out)
+    return out
+
+
+def lap_f(mesh, nu, f):
+    """ex::laplacian(Field<scalar> nu, Field<T>)."""
+    nc = f.shape[-1]
+    out = mesh.zeros(nc)
+    lib().orc_lap_f(mesh._p, np.ascontiguousarray(nu), np.ascontiguousarray(f), nc, out)
     return out
 
 
@@ -488,6 +514,23 @@ def ensight_parse(path, kind, n=None, nc=1):
     part = int(np.frombuffer(b, np.int32, 1, 160)[0])
     vals = np.frombuffer(b, np.float32, offset=244)
     return {"lines": lines, "part": part, "values": vals.copy(), "size": len(b)}
+
+
+def ref_ops2(mesh, T, S, s, nu, U):
+    """The reference's div(tensor), div(symmTensor), div(scalar, tensor),
+    laplacian(Field nu, vector / scalar) on ghosted inputs (oracle/_ref/nova_ref ops2)."""
+    names = {"div_t": 3, "div_st": 3, "div_sT": 3, "lap_f_v": 3, "lap_f_s": 1}
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        write_case(case, mesh)
+        paths = []
+        for k, a in (("T", T), ("S", S), ("s", s), ("nu", nu), ("U", U)):
+            paths.append(os.path.join(td, k + ".bin"))
+            np.ascontiguousarray(a, np.float64).tofile(paths[-1])
+        out = os.path.join(td, "out")
+        subprocess.run([REF_BIN, "ops2", case] + paths + [out, "-m", str(mesh.m)], check=True,
+                       stdout=subprocess.DEVNULL)
+        return {k: np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (nc,)) for k, nc in names.items()}
 
 
 # ------------------------------------------------------------- initial data --

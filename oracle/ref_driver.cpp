@@ -13,6 +13,7 @@
  *   nova_ref wc <case> <tg|shear> <nsteps> <dt> <mu> <ka> <c> <rho0> <gz> <U.bin> <rho.bin> <p.bin> <T.bin|-> <out>
  *   nova_ref wcinit <case> <c> <rho0> <gz> <T.bin> <out>
  *   nova_ref ensight <case> <nsteps> <dt> <U.bin> <p.bin> <dir>
+ *   nova_ref ops2 <case> <T.bin> <S.bin> <s.bin> <nu.bin> <U.bin> <out>
  *   (any may end with the reference's `-m <order>` option)
  *
  * `wc` runs the compressible loop bodies: app/TG (rhoEqn.H, pEqn.H, UEqn.H in
@@ -310,6 +311,35 @@ static int wcinit(int argc, char **argv)
     return 0;
 }
 
+/* the ex:: variants no app of the time advance uses: div(tensor), div(symmTensor),
+ * div(scalar, tensor), laplacian(Field nu, vector / scalar); inputs are ghosted as given */
+static int ops2(int argc, char **argv)
+{
+    if (argc < 9) { std::fprintf(stderr, "usage: ops2 <case> <T> <S> <s> <nu> <U> <out>\n"); return 2; }
+    settings::zoneName() = argv[2];
+    const std::string out = argv[8];
+    Time time(0.01, 1.0, 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+    Field<tensor> T(mesh, tensor(0.0), "Tt");
+    Field<symmTensor> S(mesh, symmTensor(0.0), "Ss");
+    Field<scalar> s(mesh, 0, "ss");
+    Field<scalar> nu(mesh, 0, "nu");
+    Field<vector> U(mesh, vector(0, 0, 0), "Uu");
+    load(T, argv[3]);
+    load(S, argv[4]);
+    load(s, argv[5]);
+    load(nu, argv[6]);
+    load(U, argv[7]);
+    auto Tp = std::make_shared<Field<tensor> >(T);
+    save(*ex::div(T), out + "_div_t.bin");
+    save(*ex::div(S), out + "_div_st.bin");
+    save(*ex::div(s, Tp), out + "_div_sT.bin");
+    save(*ex::laplacian(nu, U), out + "_lap_f_v.bin");
+    save(*ex::laplacian(nu, s), out + "_lap_f_s.bin");
+    return 0;
+}
+
 /* the apps' output after each step: Mesh::write (geometry, case, restart) and Field<T>::write */
 static int ensight(int argc, char **argv)
 {
@@ -338,7 +368,7 @@ static int ensight(int argc, char **argv)
 
 int main(int argc, char **argv)
 {
-    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit|ensight ... [-m order]\n"); return 2; }
+    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit|ensight|ops2 ... [-m order]\n"); return 2; }
     settings::process(argc, argv); /* the reference's own -m option (settings.cpp:53-78) */
     std::string mode = argv[1];
     if (mode == "run") return run(argc, argv);
@@ -346,6 +376,7 @@ int main(int argc, char **argv)
     if (mode == "wc") return wc(argc, argv);
     if (mode == "wcinit") return wcinit(argc, argv);
     if (mode == "ensight") return ensight(argc, argv);
+    if (mode == "ops2") return ops2(argc, argv);
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;
 }

@@ -128,6 +128,18 @@ def ensight_case(name, N, L, origin, seed, walls=False):
                         restart_text=np.array(restart_text))
 
 
+def ops2_case(name, N, L, seed):
+    """the reference's div(tensor), div(symmTensor), div(scalar, tensor), laplacian(Field nu, .)"""
+    M = O.Mesh(N, L=L)
+    rng = np.random.default_rng(seed)
+    ins = {"T": rng.standard_normal((9,) + M.N), "S": rng.standard_normal((6,) + M.N),
+           "s": rng.standard_normal((1,) + M.N), "nu": 0.5 + rng.random((1,) + M.N),
+           "U": rng.standard_normal((3,) + M.N)}
+    out = O.ref_ops2(M, *(M.to_ghosted(ins[k]) for k in ("T", "S", "s", "nu", "U")))
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(L), **ins,
+                        **{"out_" + k: M.interior(v) for k, v in out.items()})
+
+
 CASES = {
     "ops_10x8x6.npz": lambda n: ops_case(n, (10, 8, 6), (2 * np.pi, 2.0, 3.0), 7, 0.01),
     "ops_16x12x8_m4.npz": lambda n: ops_case(n, (16, 12, 8), (2 * np.pi,) * 3, 8, 0.02, m=4),
@@ -137,6 +149,7 @@ CASES = {
     "ot_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "literal", 4, 0.01, 1e-3, 1e-3),
     "wc_tg_12.npz": lambda n: wc_tg_case(n, (12, 12, 12), 5, 0.02, 1 / 1600),
     "wc_shear_12x8x16.npz": lambda n: wc_shear_case(n, (12, 8, 16), 4),
+    "ops2_7x6x5.npz": lambda n: ops2_case(n, (7, 6, 5), (2.0, 1.5, 3.0), 13),
     "ensight_7x5x6.npz": lambda n: ensight_case(n, (7, 5, 6), (2.0, 1.5, 3.0), (0.5, -1.0, 0.25), 11),
     "ensight_walls_6x8x5.npz": lambda n: ensight_case(n, (6, 8, 5), (1.0, 2.0, 1.5), (0.0, 0.0, 0.0), 12, True),
 }

@@ -161,3 +161,56 @@ def test_stretched_z_advance(nova, oracle):
     ref = OM.unique(r[0])
     for c in range(3):
         assert np.linalg.norm(U.download_soa()[c] - ref[c]) / np.linalg.norm(ref[c]) < 1e-11
+
+
+def test_tensor_divergences_and_field_nu_laplacian_vs_reference_golden(nova, oracle):
+    """nova_div_t (tensor, symmTensor), nova_div_st, nova_laplacian_f against the
+    reference's own operators (src/ex/div/div.hxx:173-285, laplacian.hxx:64-127)."""
+    g = load_golden("ops2_7x6x5.npz")
+    N, L = tuple(int(v) for v in g["N"]), tuple(g["L"])
+    OM = oracle.Mesh(N, L=L)
+    GM = nova.Mesh(N, L=L)
+    F = {k: nova.Field(GM, g[k].shape[0]).upload_soa(g[k]) for k in ("T", "S", "s", "nu", "U")}
+    got = {"div_t": nova.ex.div(F["T"]), "div_st": nova.ex.div(F["S"]), "div_sT": nova.ex.div(F["s"], F["T"]),
+           "lap_f_v": nova.ex.laplacian(F["nu"], F["U"]), "lap_f_s": nova.ex.laplacian(F["nu"], F["s"])}
+    for k, f in got.items():
+        assert rel_max(OM.interior(f.download()), g["out_" + k]) < TOL, k
+
+
+def test_field_nu_laplacian_stretched_z_and_walls_vs_oracle(nova, oracle):
+    rng = np.random.default_rng(14)
+    N, L, hz = (10, 8, 16), (2 * np.pi, 2.0, 1.0), (0.03, 0.03)
+    OM = oracle.Mesh(N, L=L, hyperbolic_z=hz)
+    GM = nova.Mesh(N, L=L, hyperbolic_z=hz)
+    nu = 0.5 + rng.random((1,) + N)
+    U = rng.standard_normal((3,) + N)
+    ref = oracle.lap_f(OM, OM.to_ghosted(nu), OM.to_ghosted(U))
+    got = nova.ex.laplacian(nova.Field(GM, 1).upload_soa(nu), nova.Field(GM, 3).upload_soa(U))
+    assert rel_max(got.download_soa(), OM.unique(ref)) < TOL
+
+    # y walls: nu Neumann, U with Dirichlet v and Neumann u, w (the ghosts of src/BC)
+    N = (12, 10, 8)
+    OM = oracle.Mesh(N, L=(2 * np.pi, 2.0, 1.5))
+    GM = nova.Mesh(N, L=(2 * np.pi, 2.0, 1.5), walls=(0, 1, 0))
+    spec_u = {"north": [(1, 0.0), (2, 0.3), (1, 0.0)], "south": [(1, 0.1), (2, 0.0), (1, 0.0)]}
+    spec_n = {"north": (1, 0.0), "south": (1, 0.0)}
+    h = OM.h
+
+    def ghosted(x, spec):
+        gg = OM.zeros(x.shape[0])
+        gg[h:h + N[0], h:h + N[1] + 1, h:h + N[2]] = np.moveaxis(x, 0, -1)
+        return oracle.bc_apply(OM, gg, spec)
+
+    nu = 0.5 + rng.random((1, N[0], N[1] + 1, N[2]))
+    U = rng.standard_normal((3, N[0], N[1] + 1, N[2]))
+    nug, Ug = ghosted(nu, spec_n), ghosted(U, spec_u)
+    ref = oracle.lap_f(OM, nug, Ug)
+    fn = nova.Field(GM, 1)
+    t, v = oracle.bc_arrays(1, spec_n)
+    fn.set_bc(list(t), list(v))
+    fu = nova.Field(GM, 3)
+    t, v = oracle.bc_arrays(3, spec_u)
+    fu.set_bc(list(t), list(v))
+    got = nova.ex.laplacian(fn.upload(nug), fu.upload(Ug))
+    stored = np.ascontiguousarray(np.moveaxis(ref[h:h + N[0], h:h + N[1] + 1, h:h + N[2]], -1, 0))
+    assert rel_max(got.download_soa(), stored) < TOL

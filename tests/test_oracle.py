@@ -150,3 +150,15 @@ def test_weakly_compressible_shear_bitwise_vs_reference_golden(oracle):
         assert np.array_equal(M.unique(a), g[name]), name
     assert np.array_equal(hist, g["hist"])
     assert np.abs(g["rho"] - g["rho_init"]).max() > 0  # the density really evolves
+
+
+def test_tensor_operators_and_field_nu_laplacian_bitwise_vs_reference_golden(oracle):
+    """ex::div(tensor), div(symmTensor), div(scalar, tensor), laplacian(Field nu, .)."""
+    g = load_golden("ops2_7x6x5.npz")
+    M = oracle.Mesh(tuple(int(v) for v in g["N"]), L=tuple(g["L"]))
+    G = {k: M.to_ghosted(g[k]) for k in ("T", "S", "s", "nu", "U")}
+    mine = {"div_t": oracle.div_t(M, G["T"]), "div_st": oracle.div_t(M, G["S"]),
+            "div_sT": oracle.div_sT(M, G["s"], G["T"]), "lap_f_v": oracle.lap_f(M, G["nu"], G["U"]),
+            "lap_f_s": oracle.lap_f(M, G["nu"], G["s"])}
+    for k, v in mine.items():
+        assert np.array_equal(M.interior(v), g["out_" + k]), k
