@@ -184,12 +184,17 @@ nova_status nova_field_maxabs_noalloc(nova_ctx *ctx, const nova_field *s, double
 nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *run, nova_state *state, int nsteps, double *hist);
 
 /* ---- discrete adjoint (no counterpart in the reference: added capability) ---- */
-typedef enum { NOVA_OBJ_EKIN_FINAL = 0 } nova_objective;
+/* NOVA_OBJ_EKIN_FINAL:         J = Ek(N), Ek = mean(1/2 |U|^2) over the unique nodes
+ * NOVA_OBJ_DISSIPATION_WINDOW: J = sum over steps n0+1..N of eps_n dt, eps_n = -(Ek(n) - Ek(n-1))/dt
+ *                              the dissipation rate the apps print (app/TG/TG.cpp:113-115),
+ *                              i.e. J = Ek(n0) - Ek(N), n0 = window_start */
+typedef enum { NOVA_OBJ_EKIN_FINAL = 0, NOVA_OBJ_DISSIPATION_WINDOW = 1 } nova_objective;
 typedef struct {
     nova_run_desc run;     /* forward run: NS, classical RK4, FP64 */
     int nsteps;            /* steps of the forward solve */
     int checkpoint_every;  /* K: states kept every K steps, segments recomputed in reverse */
-    int objective;         /* nova_objective: J = mean(1/2 |U|^2) at the final step */
+    int objective;         /* nova_objective */
+    int window_start;      /* n0 of NOVA_OBJ_DISSIPATION_WINDOW, 0 <= n0 < nsteps */
 } nova_adj_desc;
 /* Gradient of J(U(T)) with respect to the initial velocity by the hand-written
  * discrete adjoint of the fused stage, the RK4 loop and the (self-adjoint)

@@ -125,7 +125,18 @@ __global__ void k_axpby(long long n, double a, const double *__restrict__ x, dou
     if (t < n) y[t] = a * x[t];
 }
 
+__global__ void k_axpy(long long n, double a, const double *__restrict__ x, double *__restrict__ y)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < n) y[t] = fma(a, x[t], y[t]);
+}
+
 }  // namespace
+
+void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t st)
+{
+    k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, x, y);
+}
 
 void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                         const AdjArgs &a, cudaStream_t st)

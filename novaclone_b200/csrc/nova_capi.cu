@@ -1167,7 +1167,11 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     const nova_run_desc *rd = &ad->run;
     if (rd->model != NOVA_MODEL_NS || rd->rk_mode != NOVA_RK_CLASSICAL || rd->precision != NOVA_F64 || gradB)
         return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: built for FP64 Navier-Stokes, classical RK4");
-    if (ad->objective != NOVA_OBJ_EKIN_FINAL) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: objective");
+    const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
+    if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window)
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective");
+    if (window && (ad->window_start < 0 || ad->window_start >= ad->nsteps))
+        return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: window_start must lie in [0, nsteps)");
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: the fused kernels are built for m = 6");
     if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: periodic meshes only");
     if (ad->nsteps < 1 || ad->checkpoint_every < 1 || !(rd->dt > 0.0))
@@ -1204,7 +1208,17 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     // reverse sweep does not recompute it
     const int c_last = nck - 1, n_last = c_last * K, m_last = N - n_last;
     CK(cudaMemcpyAsync(ck, init->U->d64, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    if ((s = dalloc(ctx, &ctx->d_row, 2 * NOVA_HIST_COLS)) != NOVA_OK) return s;
+    const int n0w = window ? ad->window_start : -1;
+    auto ekin = [&](const double *u, double *row_dev) {  // diagnostics row of the state u
+        launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, u, nullptr, nullptr, nullptr, nullptr,
+                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
+        ctx->launches += 2;
+    };
     for (int n = 0; n < N; n++) {
+        if (n == n0w)  // Ek(n0) of the window: the state before step n0
+            ekin(n >= n_last ? (n == n_last ? ck + V * c_last : St(n - n_last)) : (n % K == 0 ? ck + V * (n / K) : mu),
+                 ctx->d_row + NOVA_HIST_COLS);
         if (n >= n_last) {
             const int t = n - n_last;
             if (t == 0) CK(cudaMemcpyAsync(St(0), ck + V * c_last, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
@@ -1217,15 +1231,11 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         if ((n + 1) % K == 0 && n + 1 < N)
             CK(cudaMemcpyAsync(ck + V * ((n + 1) / K), mu, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
     }
-    // J = mean 1/2 |U_N|^2 and lambda_N = U_N / N^3
-    if ((s = dalloc(ctx, &ctx->d_row, NOVA_HIST_COLS)) != NOVA_OK) return s;
-    launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, mu, nullptr, nullptr, nullptr, nullptr,
-                nullptr, 0,
-                ctx->d_part, (double)N, N * rd->dt, ctx->d_row, ctx->d_flag, st);
-    ctx->launches += 2;
-    double row[NOVA_HIST_COLS];
+    // Ek(N); lambda_N = dJ/dU_N = +-U_N / N^3 (the unique nodes are the N^3 entries)
+    ekin(mu, ctx->d_row);
+    double row[2 * NOVA_HIST_COLS];
     CK(cudaMemcpyAsync(row, ctx->d_row, sizeof(row), cudaMemcpyDeviceToHost, st));
-    launch_scale_copy((long long)V, 1.0 / (double)ctx->g.N3, mu, lam, st);
+    launch_scale_copy((long long)V, (window ? -1.0 : 1.0) / (double)ctx->g.N3, mu, lam, st);
     ctx->launches += 1;
     CKL("adjoint seed");
 
@@ -1258,6 +1268,10 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
             adj(2, AdjArgs{Y2(t), gB, mu, Lam, gA, Lam});
             adj(1, AdjArgs{St(t), gA, mu, Lam, lam, nullptr});
             CKL("k_adj_stage");
+            if (n0 + t == n0w) {  // lambda is dJ/dU_n0: add dEk(n0)/dU_n0
+                launch_axpy((long long)V, 1.0 / (double)ctx->g.N3, St(t), lam, st);
+                ctx->launches += 1;
+            }
         }
     }
     CK(cudaMemcpyAsync(gradU->d64, lam, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
@@ -1265,8 +1279,9 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
-    if (objective) *objective = row[2];
-    if (!std::isfinite(row[2])) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
+    const double J = window ? row[NOVA_HIST_COLS + 2] - row[2] : row[2];
+    if (objective) *objective = J;
+    if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
     return NOVA_OK;
 }
 

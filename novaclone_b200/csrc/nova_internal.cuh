@@ -174,7 +174,8 @@ struct AdjArgs {
 };
 void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                         const AdjArgs &a, cudaStream_t st);
-void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);
+void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);  // y = a x
+void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t st);        // y += a x
 
 // Which kernel runs the Navier-Stokes stage: STAGE_AUTO = the TMA pipeline
 // (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits: periodic y,

@@ -25,7 +25,7 @@ MODEL_NS, MODEL_MHD = 0, 1
 RK_LITERAL, RK_CLASSICAL = 0, 1
 HIST_COLS = 6
 K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG, K_ADJ = range(6)
-OBJ_EKIN_FINAL = 0
+OBJ_EKIN_FINAL, OBJ_DISSIPATION_WINDOW = 0, 1
 WC_TG, WC_SHEAR = 0, 1
 STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_OOM", 4: "NOVA_E_NONFINITE",
                 5: "NOVA_E_TIMEOUT", 6: "NOVA_E_UNSUPPORTED"}
@@ -62,7 +62,8 @@ class RunDesc(C.Structure):
 
 
 class AdjDesc(C.Structure):
-    _fields_ = [("run", RunDesc), ("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("objective", C.c_int)]
+    _fields_ = [("run", RunDesc), ("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("objective", C.c_int),
+                ("window_start", C.c_int)]
 
 
 class State(C.Structure):
@@ -417,13 +418,16 @@ def advance(mesh: Mesh, rd: RunDesc, U: Field, p: Field, B: Field = None, pB: Fi
     return hist
 
 
-def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_every: int = 20):
-    """dJ/dU0 for J = mean(1/2 |U(nsteps)|^2) by the discrete adjoint; returns (J, grad Field)."""
+def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_every: int = 20,
+                 window_start: int = None):
+    """dJ/dU0 by the discrete adjoint; returns (J, grad Field).  J = Ek(nsteps), or with
+    window_start = n0 the dissipation over steps n0+1..nsteps, Ek(n0) - Ek(nsteps)."""
     a = AdjDesc()
     a.run = rd
     a.nsteps = int(nsteps)
     a.checkpoint_every = int(checkpoint_every)
-    a.objective = OBJ_EKIN_FINAL
+    a.objective = OBJ_EKIN_FINAL if window_start is None else OBJ_DISSIPATION_WINDOW
+    a.window_start = 0 if window_start is None else int(window_start)
     grad = Field(mesh, 3)
     st = State(U0.h, None, None, None)
     J = C.c_double()

@@ -103,3 +103,35 @@ def test_adjoint_unsupported_modes(nova):
     with pytest.raises(nova.NovaError) as e:
         nova.adjoint_grad(GM, nova.run_desc(rk_mode="literal", dt=0.01), U, 2)
     assert e.value.status == nova.E_UNSUPPORTED
+
+
+def ek_after(nova, N, U0, dt, nu, nsteps):
+    return forward_J(nova, N, U0, dt, nu, nsteps) if nsteps > 0 else 0.5 * float(np.sum(U0 * U0)) / float(np.prod(N))
+
+
+def test_dissipation_window_objective(nova, oracle):
+    """J = sum of the dissipation eps_n dt over steps n0+1..N = Ek(n0) - Ek(N)."""
+    N = (16, 16, 16)
+    nsteps, n0, nu = 9, 4, 1e-2
+    U0, dt = base_state(oracle, N, seed=2)
+    GM = nova.Mesh(N)
+    U = nova.Field(GM, 3).upload_soa(U0)
+    rd = nova.run_desc(model="ns", rk_mode="classical", dt=dt, nu=nu)
+
+    def Jf(u):
+        return ek_after(nova, N, u, dt, nu, n0) - ek_after(nova, N, u, dt, nu, nsteps)
+
+    J, grad = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=3, window_start=n0)
+    g = grad.download_soa()
+    assert J == pytest.approx(Jf(U0), rel=1e-12)
+    rng = np.random.default_rng(7)
+    eps = 1e-6
+    for _ in range(3):
+        v = smooth_direction(rng, N)
+        fd = (Jf(U0 + eps * v) - Jf(U0 - eps * v)) / (2 * eps)
+        ad = float(np.sum(g * v))
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+    # window from step 0: dJ/dU0 = U0/N^3 - dEk(N)/dU0
+    _, g0 = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=4, window_start=0)
+    _, gk = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=4)
+    assert rel_l2(g0.download_soa(), U0 / np.prod(N) - gk.download_soa()) < 1e-13
