@@ -185,21 +185,29 @@ nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *run, nova_state *st
 
 /* ---- discrete adjoint (no counterpart in the reference: added capability) ---- */
 /* NOVA_OBJ_EKIN_FINAL:         J = Ek(N), Ek = mean(1/2 |U|^2) over the unique nodes
- * NOVA_OBJ_DISSIPATION_WINDOW: J = sum over steps n0+1..N of eps_n dt, eps_n = -(Ek(n) - Ek(n-1))/dt
+ * NOVA_OBJ_DISSIPATION_WINDOW: J = sum over steps n0+1..N of eps_n dt, eps_n = -(E(n) - E(n-1))/dt
  *                              the dissipation rate the apps print (app/TG/TG.cpp:113-115),
- *                              i.e. J = Ek(n0) - Ek(N), n0 = window_start */
-typedef enum { NOVA_OBJ_EKIN_FINAL = 0, NOVA_OBJ_DISSIPATION_WINDOW = 1 } nova_objective;
+ *                              i.e. J = E(n0) - E(N), n0 = window_start; E = Ek (Navier-Stokes)
+ *                              or Ek + Em (MHD; the apps print Ek, Em and their rates, app/OT_Poisson/OT.cpp:135-180)
+ * NOVA_OBJ_ETOT_FINAL:         J = Ek(N) + Em(N), Em = mean(1/2 |B|^2) (MHD only) */
+typedef enum {
+    NOVA_OBJ_EKIN_FINAL = 0,
+    NOVA_OBJ_DISSIPATION_WINDOW = 1,
+    NOVA_OBJ_ETOT_FINAL = 2
+} nova_objective;
 typedef struct {
-    nova_run_desc run;     /* forward run: NS, classical RK4, FP64 */
+    nova_run_desc run;     /* forward run: NS or MHD, classical RK4, FP64, periodic uniform mesh */
     int nsteps;            /* steps of the forward solve */
     int checkpoint_every;  /* K: states kept every K steps, segments recomputed in reverse */
     int objective;         /* nova_objective */
     int window_start;      /* n0 of NOVA_OBJ_DISSIPATION_WINDOW, 0 <= n0 < nsteps */
 } nova_adj_desc;
-/* Gradient of J(U(T)) with respect to the initial velocity by the hand-written
- * discrete adjoint of the fused stage, the RK4 loop and the (self-adjoint)
- * projection.  init->U is not modified; gradU receives dJ/dU0 (FP64, 3 comps);
- * *objective receives J.  gradB is reserved for the MHD adjoint (pass NULL). */
+/* Gradient of J with respect to the initial fields by the hand-written
+ * discrete adjoint of the fused stages, the RK4 loops and the (self-adjoint)
+ * projection.  init is not modified; gradU receives dJ/dU0 (FP64, 3 comps);
+ * for MHD (run.model NOVA_MODEL_MHD, the U loop then the B loop of each step
+ * as nova_advance runs them) gradB receives dJ/dB0 (FP64, 3 comps; required);
+ * for Navier-Stokes gradB must be NULL.  *objective receives J. */
 nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *adj, const nova_state *init, nova_field *gradU,
                               nova_field *gradB, double *objective);
 

@@ -75,7 +75,7 @@ struct nova_ctx {
     size_t stage_cap = 0;
     double *adj_pool = nullptr;  // adjoint checkpoints, segment states, adjoint fields
     size_t adj_cap = 0;
-    double *d_row = nullptr;     // one diagnostics row
+    double *d_row = nullptr;     // two diagnostics rows (adjoint objectives)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::string err;
@@ -1095,11 +1095,13 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
 // ================================================================== adjoint ==
 namespace {
 
-// One classical RK4 step + projection of an FP64 Navier-Stokes state:
-// Uin -> Uout (may alias), stage states into Y2, Y3, Y4 (Y4 may alias Y2).
-// Without `full` only the stage states are produced.
-nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin, double *Y2, double *Y3, double *Y4,
-                       double *Uout, bool full)
+// One classical RK4 loop of the evolved FP64 field Yin with the frozen field X
+// (physics phys, viscosity visc), stage states into S2, S3, S4 (S4 may alias
+// S2); with `full` the stage-3 result and its projection (rhs divisor and
+// correction scale `div`) into out (may alias Yin).  Without `full` only the
+// stage states are produced.
+nova_status rk_loop64(nova_ctx *ctx, const nova_run_desc *rd, int phys, double visc, double div, const double *Yin,
+                      const double *X, double *S2, double *S3, double *S4, double *out, bool full)
 {
     const Geo &g = ctx->g;
     cudaStream_t st = ctx->stream;
@@ -1108,35 +1110,45 @@ nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin
     nova_status sst = NOVA_OK;
     auto run = [&](int stage, const StageArgs64 &a) {
         ProfScope ps(ctx, NOVA_K_STAGE);
-        const cudaError_t e = launch_stage64(PHYS_NS, stage, str, g, Walls<double>{}, ctx->co64, ctx->d_ia64,
-                                             ctx->d_corr64, rd->dt, rd->nu, a, st,
+        const cudaError_t e = launch_stage64(phys, stage, str, g, Walls<double>{}, ctx->co64, ctx->d_ia64,
+                                             ctx->d_corr64, rd->dt, visc, a, st,
                                              StageExec{ctx->stage_impl, ctx->d_flag + 1});
         if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
         ctx->launches += 1;
     };
-    run(0, StageArgs64{Uin, nullptr, nullptr, A, Y2});
-    run(1, StageArgs64{Y2, nullptr, Uin, A, Y3});
-    run(2, StageArgs64{Y3, nullptr, Uin, A, Y4});
+    run(0, StageArgs64{Yin, X, nullptr, A, S2});
+    run(1, StageArgs64{S2, X, Yin, A, S3});
+    run(2, StageArgs64{S3, X, Yin, A, S4});
     if (!full) {
+        if (sst != NOVA_OK) return sst;
         CKL("stage kernel");
         return NOVA_OK;
     }
-    run(3, StageArgs64{Y4, nullptr, nullptr, A, Uout});
+    run(3, StageArgs64{S4, X, nullptr, A, out});
     if (sst != NOVA_OK) return sst;
     CKL("stage kernel");
-    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, Uout, nullptr, nullptr, rd->dt,
+    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, out, nullptr, nullptr, div,
                                     ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
     if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, ctx->w64[1]);
     if (s != NOVA_OK) return s;
-    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->w64[1], rd->dt, Uout, Uout, nullptr,
+    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, ctx->w64[1], div, out, out, nullptr,
                        nullptr, nullptr, nullptr, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
     if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_correct_tiled");
     return NOVA_OK;
+}
+
+// One classical RK4 step + projection of an FP64 Navier-Stokes state:
+// Uin -> Uout (may alias), stage states into Y2, Y3, Y4 (Y4 may alias Y2).
+// Without `full` only the stage states are produced.
+nova_status fwd_step64(nova_ctx *ctx, const nova_run_desc *rd, const double *Uin, double *Y2, double *Y3, double *Y4,
+                       double *Uout, bool full)
+{
+    return rk_loop64(ctx, rd, PHYS_NS, rd->nu, rd->dt, Uin, nullptr, Y2, Y3, Y4, Uout, full);
 }
 
 // out = P in = in - G L^-1 D in (the projection is symmetric: its own adjoint)
@@ -1158,6 +1170,21 @@ nova_status project64(nova_ctx *ctx, const double *in, double *out, double *pbuf
     return NOVA_OK;
 }
 
+// the adjoint's device pool: `need` doubles, grown on demand
+nova_status adj_pool(nova_ctx *ctx, size_t need)
+{
+    if (ctx->adj_cap >= need) return NOVA_OK;
+    if (ctx->adj_pool) cudaFree(ctx->adj_pool);
+    ctx->adj_pool = nullptr;
+    ctx->adj_cap = 0;
+    const nova_status s = dalloc(ctx, &ctx->adj_pool, need);
+    if (s == NOVA_OK) ctx->adj_cap = need;
+    return s;
+}
+
+nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
+                        nova_field *gradB, double *objective);
+
 }  // namespace
 
 extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init,
@@ -1165,19 +1192,28 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
 {
     if (!ctx || !ad || !init || !gradU) return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: null argument");
     const nova_run_desc *rd = &ad->run;
-    if (rd->model != NOVA_MODEL_NS || rd->rk_mode != NOVA_RK_CLASSICAL || rd->precision != NOVA_F64 || gradB)
-        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: built for FP64 Navier-Stokes, classical RK4");
+    const bool mhd = rd->model == NOVA_MODEL_MHD;
+    if ((rd->model != NOVA_MODEL_NS && !mhd) || rd->rk_mode != NOVA_RK_CLASSICAL || rd->precision != NOVA_F64)
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: built for FP64 Navier-Stokes and MHD, classical RK4");
     const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
-    if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window)
-        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective");
+    if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window && !(mhd && ad->objective == NOVA_OBJ_ETOT_FINAL))
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective for this model");
     if (window && (ad->window_start < 0 || ad->window_start >= ad->nsteps))
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: window_start must lie in [0, nsteps)");
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: the fused kernels are built for m = 6");
-    if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: periodic meshes only");
+    if (ctx->g.wallY || ctx->md.hyperbolic_z)
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: periodic uniform meshes only");
     if (ad->nsteps < 1 || ad->checkpoint_every < 1 || !(rd->dt > 0.0))
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: nsteps, checkpoint_every and dt must be positive");
     if (!valid_field(init->U, 3) || init->U->prec != NOVA_F64 || !valid_field(gradU, 3) || gradU->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: U and gradU must be FP64 3-component fields");
+    if (mhd) {
+        if (!valid_field(init->B, 3) || init->B->prec != NOVA_F64 || !gradB || !valid_field(gradB, 3) ||
+            gradB->prec != NOVA_F64)
+            return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: MHD needs FP64 3-component B and gradB");
+        return adjoint_mhd(ctx, ad, init, gradU, gradB, objective);
+    }
+    if (gradB) return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: gradB is for MHD runs (pass NULL)");
     nova_status s = ensure_work(ctx, NOVA_F64);
     if (s != NOVA_OK) return s;
     CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
@@ -1187,13 +1223,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     const size_t V = 3 * (size_t)ctx->g.N3;
     // layout: nck checkpoints | 4*mmax segment fields | lam, mu, gA, gB, Lam
     const size_t need = V * ((size_t)nck + 4 * (size_t)mmax + 5);
-    if (ctx->adj_cap < need) {
-        if (ctx->adj_pool) cudaFree(ctx->adj_pool);
-        ctx->adj_pool = nullptr;
-        ctx->adj_cap = 0;
-        if ((s = dalloc(ctx, &ctx->adj_pool, need)) != NOVA_OK) return s;
-        ctx->adj_cap = need;
-    }
+    if ((s = adj_pool(ctx, need)) != NOVA_OK) return s;
     double *ck = ctx->adj_pool;
     double *seg = ck + V * nck;
     double *lam = seg + V * 4 * mmax, *mu = lam + V, *gA = mu + V, *gB = gA + V, *Lam = gB + V;
@@ -1284,6 +1314,183 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
     return NOVA_OK;
 }
+
+namespace {
+
+// Discrete adjoint of the MHD step of nova_advance (app/OT_Poisson: UEqn.H then
+// BEqn.H): U^{n+1} = P Phi_U(U^n; B^n), then B^{n+1} = P Phi_B(B^n; U^{n+1}),
+// Phi the classical RK4 loops, P the projection.  Reverse of one step, given
+// lamU = dJ/dU^{n+1}, lamB = dJ/dB^{n+1}:
+//   B loop: mu = P lamB; stages S = 4..1 of Phi_B (frozen U^{n+1}, stage states
+//           Z_S): the recursion of k_adj_stage with xi = dt dF_B/dB^T g_S gives
+//           lamB <- dJ/dB^n through the B loop, and lamU += dt dF_B/dU^T g_S;
+//   U loop: mu = P lamU; stages S = 4..1 of Phi_U (frozen B^n, stage states
+//           Y_S): the Navier-Stokes recursion gives lamU <- dJ/dU^n, and
+//           lamB += dt dF_U/dB^T g_S.
+nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
+                        nova_field *gradB, double *objective)
+{
+    const nova_run_desc *rd = &ad->run;
+    const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
+    const bool etot = window || ad->objective == NOVA_OBJ_ETOT_FINAL;
+    nova_status s = ensure_work(ctx, NOVA_F64);
+    if (s != NOVA_OK) return s;
+    CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
+    const int N = ad->nsteps, K = ad->checkpoint_every;
+    const int nck = (N + K - 1) / K;
+    const int mmax = K < N ? K : N;
+    const size_t V = 3 * (size_t)ctx->g.N3;
+    // layout: nck U and nck B checkpoints | 8*mmax + 1 segment fields | lamU, lamB, mu, gA, gB, Lam
+    if ((s = adj_pool(ctx, V * (2 * (size_t)nck + 8 * (size_t)mmax + 1 + 6))) != NOVA_OK) return s;
+    double *ckU = ctx->adj_pool, *ckB = ckU + V * nck;
+    double *seg = ckB + V * nck;
+    double *lamU = seg + V * (8 * (size_t)mmax + 1), *lamB = lamU + V, *mu = lamB + V, *gA = mu + V, *gB = gA + V,
+           *Lam = gB + V;
+    // per step t of a segment: U^n, Y2, Y3, Y4 (U loop), B^n, Z2, Z3, Z4 (B loop); U^{n+1} is slot t + 1
+    auto slot = [&](int t, int f) { return seg + V * (8 * (size_t)t + f); };
+    auto St = [&](int t) { return slot(t, 0); };
+    auto SB = [&](int t) { return slot(t, 4); };
+    cudaStream_t st = ctx->stream;
+    double *w0 = ctx->w64[0], *w1 = ctx->w64[1];
+    double *runU = mu, *runB = Lam;  // running state of the forward pass
+
+    // one step; the B loop is projected only when bout is set
+    auto step = [&](const double *u, const double *b, double *y2, double *y3, double *y4, double *uout, double *z2,
+                    double *z3, double *z4, double *bout) {
+        nova_status r = rk_loop64(ctx, rd, PHYS_MHD_U, rd->nu, rd->dt, u, b, y2, y3, y4, uout, true);
+        if (r != NOVA_OK) return r;
+        return rk_loop64(ctx, rd, PHYS_MHD_B, rd->eta, 1.0, b, uout, z2, z3, z4, bout, bout != nullptr);
+    };
+    auto seg_step = [&](int t, int m, double *blast) {
+        return step(St(t), SB(t), slot(t, 1), slot(t, 2), slot(t, 3), St(t + 1), slot(t, 5), slot(t, 6), slot(t, 7),
+                    t + 1 < m ? SB(t + 1) : blast);
+    };
+    auto energy = [&](const double *u, const double *b, double *row_dev) {  // diagnostics row of (u, b)
+        launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, u, nullptr, nullptr, b, nullptr,
+                    nullptr, 1, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
+        ctx->launches += 2;
+    };
+    auto copy = [&](double *dst, const double *src) {
+        return cudaMemcpyAsync(dst, src, sizeof(double) * V, cudaMemcpyDeviceToDevice, st);
+    };
+
+    // forward pass, keeping (U, B) every K steps; the last segment keeps its
+    // states and stage states as it goes
+    const int c_last = nck - 1, n_last = c_last * K, m_last = N - n_last;
+    CK(copy(ckU, init->U->d64));
+    CK(copy(ckB, init->B->d64));
+    if ((s = dalloc(ctx, &ctx->d_row, 2 * NOVA_HIST_COLS)) != NOVA_OK) return s;
+    const int n0w = window ? ad->window_start : -1;
+    for (int n = 0; n < N; n++) {
+        if (n == n0w) {  // E(n0) of the window: the state before step n0
+            const bool ck = n == n_last || (n < n_last && n % K == 0);
+            const double *u = ck ? ckU + V * (n / K) : (n > n_last ? St(n - n_last) : runU);
+            const double *b = ck ? ckB + V * (n / K) : (n > n_last ? SB(n - n_last) : runB);
+            energy(u, b, ctx->d_row + NOVA_HIST_COLS);
+        }
+        if (n >= n_last) {
+            const int t = n - n_last;
+            if (t == 0) {
+                CK(copy(St(0), ckU + V * c_last));
+                CK(copy(SB(0), ckB + V * c_last));
+            }
+            if ((s = seg_step(t, m_last, runB)) != NOVA_OK) return s;
+            continue;
+        }
+        const bool ck = n % K == 0;
+        if ((s = step(ck ? ckU + V * (n / K) : runU, ck ? ckB + V * (n / K) : runB, w0, w1, w0, runU, w0, w1, w0,
+                      runB)) != NOVA_OK)
+            return s;
+        if ((n + 1) % K == 0 && n + 1 < N) {
+            CK(copy(ckU + V * ((n + 1) / K), runU));
+            CK(copy(ckB + V * ((n + 1) / K), runB));
+        }
+    }
+    // E(N); lamU = dJ/dU_N = +-U_N / N^3, lamB = +-B_N / N^3 (or 0 for Ek alone)
+    const double *UN = St(m_last);
+    energy(UN, runB, ctx->d_row);
+    double row[2 * NOVA_HIST_COLS];
+    CK(cudaMemcpyAsync(row, ctx->d_row, sizeof(row), cudaMemcpyDeviceToHost, st));
+    const double seed = (window ? -1.0 : 1.0) / (double)ctx->g.N3;
+    launch_scale_copy((long long)V, seed, UN, lamU, st);
+    ctx->launches += 1;
+    if (etot) {
+        launch_scale_copy((long long)V, seed, runB, lamB, st);
+        ctx->launches += 1;
+    } else {
+        CK(cudaMemsetAsync(lamB, 0, sizeof(double) * V, st));
+    }
+    CKL("adjoint seed");
+
+    const double dt = rd->dt;
+    auto adj_u = [&](int stage, const AdjArgs &a) {
+        ProfScope ps(ctx, NOVA_K_ADJ);
+        launch_adj_stage64(stage, ctx->g, ctx->co64, ctx->d_ia64, dt, rd->nu, a, st);
+        ctx->launches += 1;
+    };
+    auto adj_mhd = [&](int kind, int stage, const AdjArgs &a, double *acc) {
+        ProfScope ps(ctx, NOVA_K_ADJ);
+        launch_adj_mhd(kind, stage, ctx->g, ctx->co64, ctx->d_ia64, dt, rd->eta, a, acc, st);
+        ctx->launches += 1;
+    };
+    auto proj = [&](const double *in) {
+        ProfScope ps(ctx, NOVA_K_DIV);
+        return project64(ctx, in, mu, gB);
+    };
+    enum { UB = 0, BU = 1, BB = 2 };
+    for (int c = nck - 1; c >= 0; c--) {
+        const int n0 = c * K;
+        const int m = (N - n0) < K ? (N - n0) : K;
+        if (c != c_last) {
+            CK(copy(St(0), ckU + V * c));
+            CK(copy(SB(0), ckB + V * c));
+            for (int t = 0; t < m; t++)
+                if ((s = seg_step(t, m, nullptr)) != NOVA_OK) return s;
+        }
+        for (int t = m - 1; t >= 0; t--) {
+            // B loop: frozen U^{n+1} = St(t + 1), stage states Z_S
+            if ((s = proj(lamB)) != NOVA_OK) return s;
+            const double *Up = St(t + 1);
+            adj_mhd(BB, 4, AdjArgs{Up, mu, mu, nullptr, gA, Lam}, nullptr);
+            adj_mhd(BU, 4, AdjArgs{slot(t, 7), mu, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BB, 3, AdjArgs{Up, gA, mu, Lam, gB, Lam}, nullptr);
+            adj_mhd(BU, 3, AdjArgs{slot(t, 6), gA, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BB, 2, AdjArgs{Up, gB, mu, Lam, gA, Lam}, nullptr);
+            adj_mhd(BU, 2, AdjArgs{slot(t, 5), gB, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BB, 1, AdjArgs{Up, gA, mu, Lam, lamB, nullptr}, nullptr);
+            adj_mhd(BU, 1, AdjArgs{SB(t), gA, nullptr, nullptr, nullptr, nullptr}, lamU);
+            // U loop: frozen B^n = SB(t), stage states Y_S
+            if ((s = proj(lamU)) != NOVA_OK) return s;
+            adj_u(4, AdjArgs{slot(t, 3), mu, mu, nullptr, gA, Lam});
+            adj_mhd(UB, 4, AdjArgs{SB(t), mu, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_u(3, AdjArgs{slot(t, 2), gA, mu, Lam, gB, Lam});
+            adj_mhd(UB, 3, AdjArgs{SB(t), gA, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_u(2, AdjArgs{slot(t, 1), gB, mu, Lam, gA, Lam});
+            adj_mhd(UB, 2, AdjArgs{SB(t), gB, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_u(1, AdjArgs{St(t), gA, mu, Lam, lamU, nullptr});
+            adj_mhd(UB, 1, AdjArgs{SB(t), gA, nullptr, nullptr, nullptr, nullptr}, lamB);
+            CKL("k_adj_mhd");
+            if (n0 + t == n0w) {  // add dE(n0)/d(U, B)_n0
+                launch_axpy((long long)V, 1.0 / (double)ctx->g.N3, St(t), lamU, st);
+                launch_axpy((long long)V, 1.0 / (double)ctx->g.N3, SB(t), lamB, st);
+                ctx->launches += 2;
+            }
+        }
+    }
+    CK(copy(gradU->d64, lamU));
+    CK(copy(gradB->d64, lamB));
+    int perr = 0;
+    CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
+    const double E = row[2] + (etot ? row[3] : 0.0);
+    const double J = window ? (row[NOVA_HIST_COLS + 2] + row[NOVA_HIST_COLS + 3]) - E : E;
+    if (objective) *objective = J;
+    if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
+    return NOVA_OK;
+}
+
+}  // namespace
 
 // ========================================================= weakly compressible ==
 extern "C" nova_status nova_advance_wc(nova_ctx *ctx, const nova_wc_desc *wd, nova_wc_state *st, int nsteps,

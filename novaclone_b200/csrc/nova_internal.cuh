@@ -174,6 +174,11 @@ struct AdjArgs {
 };
 void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                         const AdjArgs &a, cudaStream_t st);
+// MHD adjoint stage pieces (nova_adjoint.cu): kind 0 = dF_U/dB (lambda_B += ...),
+// 1 = dF_B/dU (lambda_U += ...), 2 = dF_B/dB with the reverse RK4 recursion;
+// a.Y = the field in the transpose (B^n, Z_S or U^{n+1}), a.G = g_S
+void launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double visc,
+                    const AdjArgs &a, double *acc, cudaStream_t st);
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);  // y = a x
 void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t st);        // y += a x
 

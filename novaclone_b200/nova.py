@@ -25,7 +25,7 @@ MODEL_NS, MODEL_MHD = 0, 1
 RK_LITERAL, RK_CLASSICAL = 0, 1
 HIST_COLS = 6
 K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG, K_ADJ = range(6)
-OBJ_EKIN_FINAL, OBJ_DISSIPATION_WINDOW = 0, 1
+OBJ_EKIN_FINAL, OBJ_DISSIPATION_WINDOW, OBJ_ETOT_FINAL = 0, 1, 2
 WC_TG, WC_SHEAR = 0, 1
 STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_OOM", 4: "NOVA_E_NONFINITE",
                 5: "NOVA_E_TIMEOUT", 6: "NOVA_E_UNSUPPORTED"}
@@ -419,20 +419,27 @@ def advance(mesh: Mesh, rd: RunDesc, U: Field, p: Field, B: Field = None, pB: Fi
 
 
 def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_every: int = 20,
-                 window_start: int = None):
-    """dJ/dU0 by the discrete adjoint; returns (J, grad Field).  J = Ek(nsteps), or with
-    window_start = n0 the dissipation over steps n0+1..nsteps, Ek(n0) - Ek(nsteps)."""
+                 window_start: int = None, B0: Field = None, total_energy: bool = False):
+    """Gradient of J by the discrete adjoint.  J = Ek(nsteps); with total_energy
+    (MHD) Ek + Em; with window_start = n0 the dissipation over steps n0+1..nsteps,
+    E(n0) - E(nsteps) (E = Ek, or Ek + Em for MHD).  Returns (J, dJ/dU0) for
+    Navier-Stokes and (J, dJ/dU0, dJ/dB0) for MHD (rd.model MHD, B0 given)."""
     a = AdjDesc()
     a.run = rd
     a.nsteps = int(nsteps)
     a.checkpoint_every = int(checkpoint_every)
-    a.objective = OBJ_EKIN_FINAL if window_start is None else OBJ_DISSIPATION_WINDOW
+    if window_start is not None:
+        a.objective = OBJ_DISSIPATION_WINDOW
+    else:
+        a.objective = OBJ_ETOT_FINAL if total_energy else OBJ_EKIN_FINAL
     a.window_start = 0 if window_start is None else int(window_start)
     grad = Field(mesh, 3)
-    st = State(U0.h, None, None, None)
+    gradB = Field(mesh, 3) if B0 is not None else None
+    st = State(U0.h, None, B0.h if B0 is not None else None, None)
     J = C.c_double()
-    mesh.check(mesh.lib.nova_adjoint_grad(mesh.h, C.byref(a), C.byref(st), grad.h, None, C.byref(J)))
-    return J.value, grad
+    mesh.check(mesh.lib.nova_adjoint_grad(mesh.h, C.byref(a), C.byref(st), grad.h,
+                                          gradB.h if gradB is not None else None, C.byref(J)))
+    return (J.value, grad) if gradB is None else (J.value, grad, gradB)
 
 
 def _state(U=None, p=None, B=None, pB=None):

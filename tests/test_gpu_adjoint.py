@@ -1,10 +1,11 @@
 """GPU checks of the hand-written discrete adjoint (nova_adjoint_grad).
 
-The gradient of J = mean(1/2 |U(T)|^2) with respect to U(0) is compared with
-central finite differences of the forward solver (nova_advance) along seeded
-random directions of unit RMS amplitude, eps = 1e-6: agreement <= 1e-6
-relative.  The result must not depend on the checkpoint interval, and the
-adjoint's own forward pass must reproduce the forward solver's J."""
+The gradient of J = mean(1/2 |U(T)|^2) (MHD: also + mean(1/2 |B(T)|^2)) with
+respect to U(0) (and B(0)) is compared with central finite differences of the
+forward solver (nova_advance) along seeded random directions of unit RMS
+amplitude, eps = 1e-6: agreement <= 1e-6 relative.  The result must not depend
+on the checkpoint interval, and the adjoint's own forward pass must reproduce
+the forward solver's J."""
 import numpy as np
 import pytest
 
@@ -96,12 +97,22 @@ def test_adjoint_zero_steps_is_identity_gradient(nova, oracle):
 
 def test_adjoint_unsupported_modes(nova):
     GM = nova.Mesh((8, 8, 8))
-    U = nova.Field(GM, 3)
-    with pytest.raises(nova.NovaError) as e:
+    U, B = nova.Field(GM, 3), nova.Field(GM, 3)
+    with pytest.raises(nova.NovaError) as e:  # MHD needs B0 and gradB
         nova.adjoint_grad(GM, nova.run_desc(model="mhd", dt=0.01), U, 2)
-    assert e.value.status == nova.E_UNSUPPORTED
+    assert e.value.status == nova.E_INVALID
     with pytest.raises(nova.NovaError) as e:
         nova.adjoint_grad(GM, nova.run_desc(rk_mode="literal", dt=0.01), U, 2)
+    assert e.value.status == nova.E_UNSUPPORTED
+    with pytest.raises(nova.NovaError) as e:
+        nova.adjoint_grad(GM, nova.run_desc(model="mhd", rk_mode="literal", dt=0.01), U, 2, B0=B)
+    assert e.value.status == nova.E_UNSUPPORTED
+    with pytest.raises(nova.NovaError) as e:  # Em has no meaning without B
+        nova.adjoint_grad(GM, nova.run_desc(dt=0.01), U, 2, total_energy=True)
+    assert e.value.status == nova.E_UNSUPPORTED
+    SM = nova.Mesh((8, 8, 16), hyperbolic_z=(0.02, 0.02))
+    with pytest.raises(nova.NovaError) as e:  # the transposes assume a uniform mesh
+        nova.adjoint_grad(SM, nova.run_desc(dt=0.01), nova.Field(SM, 3), 2)
     assert e.value.status == nova.E_UNSUPPORTED
 
 
@@ -135,3 +146,94 @@ def test_dissipation_window_objective(nova, oracle):
     _, g0 = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=4, window_start=0)
     _, gk = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=4)
     assert rel_l2(g0.download_soa(), U0 / np.prod(N) - gk.download_soa()) < 1e-13
+
+
+# ------------------------------------------------------------------ MHD ----
+def energies(u, b, N):
+    n = float(np.prod(N))
+    return 0.5 * float(np.sum(u * u)) / n, 0.5 * float(np.sum(b * b)) / n
+
+
+def mhd_forward(nova, N, U0, B0, dt, nu, eta, nsteps):
+    """(Ek, Em) after nsteps of the MHD loop body (U loop, then B loop)."""
+    if nsteps == 0:
+        return energies(U0, B0, N)
+    GM = nova.Mesh(N)
+    U, B = nova.Field(GM, 3).upload_soa(U0), nova.Field(GM, 3).upload_soa(B0)
+    nova.advance(GM, nova.run_desc(model="mhd", rk_mode="classical", dt=dt, nu=nu, eta=eta, diag_every=0), U,
+                 nova.Field(GM, 1), B, nova.Field(GM, 1), nsteps=nsteps, history=False)
+    return energies(U.download_soa(), B.download_soa(), N)
+
+
+def mhd_base(oracle, N, seed):
+    OM = oracle.Mesh(N)
+    rng = np.random.default_rng(seed)
+    U0, B0 = oracle.ic_orszag_tang(OM)
+    U0 = U0 + 0.05 * smooth_direction(rng, N)
+    B0 = B0 + 0.05 * smooth_direction(rng, N)
+    return U0, B0, oracle.cfl_dt(OM, [U0, B0])
+
+
+@pytest.mark.parametrize("total", [True, False])
+def test_mhd_adjoint_matches_central_differences(nova, oracle, total):
+    """Orszag-Tang + perturbations, 6 steps: directions in U alone, B alone and both."""
+    N = (16, 16, 16)
+    nsteps, nu, eta = 6, 1e-2, 2e-2
+    U0, B0, dt = mhd_base(oracle, N, seed=4)
+    GM = nova.Mesh(N)
+    U, B = nova.Field(GM, 3).upload_soa(U0), nova.Field(GM, 3).upload_soa(B0)
+    rd = nova.run_desc(model="mhd", rk_mode="classical", dt=dt, nu=nu, eta=eta)
+    J, gU, gB = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=4, B0=B, total_energy=total)
+    gu, gb = gU.download_soa(), gB.download_soa()
+
+    def Jf(u, b):
+        ek, em = mhd_forward(nova, N, u, b, dt, nu, eta, nsteps)
+        return ek + em if total else ek
+
+    assert J == pytest.approx(Jf(U0, B0), rel=1e-13)
+    assert np.abs(gb).max() > 1e-3 * np.abs(gu).max()  # the coupling really carries gradient into B
+    rng = np.random.default_rng(99)
+    eps = 1e-6
+    for wu, wb in ((1.0, 0.0), (0.0, 1.0), (1.0, 1.0)):
+        v, w = wu * smooth_direction(rng, N), wb * smooth_direction(rng, N)
+        fd = (Jf(U0 + eps * v, B0 + eps * w) - Jf(U0 - eps * v, B0 - eps * w)) / (2 * eps)
+        ad = float(np.sum(gu * v) + np.sum(gb * w))
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (wu, wb, fd, ad)
+    assert np.array_equal(U.download_soa(), U0) and np.array_equal(B.download_soa(), B0)
+
+
+def test_mhd_adjoint_independent_of_checkpoint_interval(nova, oracle):
+    N = (12, 16, 20)
+    U0, B0, dt = mhd_base(oracle, N, seed=5)
+    GM = nova.Mesh(N)
+    U, B = nova.Field(GM, 3).upload_soa(U0), nova.Field(GM, 3).upload_soa(B0)
+    rd = nova.run_desc(model="mhd", rk_mode="classical", dt=dt, nu=5e-3, eta=5e-3)
+    runs = [nova.adjoint_grad(GM, rd, U, 7, checkpoint_every=k, B0=B, total_energy=True) for k in (1, 3, 7, 50)]
+    for r in runs[1:]:
+        assert r[0] == runs[0][0]
+        assert rel_l2(r[1].download_soa(), runs[0][1].download_soa()) < 1e-14
+        assert rel_l2(r[2].download_soa(), runs[0][2].download_soa()) < 1e-14
+
+
+def test_mhd_dissipation_window_objective(nova, oracle):
+    """J = E(n0) - E(N), E = Ek + Em: the total-energy dissipation over the window."""
+    N = (16, 16, 16)
+    nsteps, n0, nu, eta = 7, 3, 1e-2, 1e-2
+    U0, B0, dt = mhd_base(oracle, N, seed=6)
+    GM = nova.Mesh(N)
+    U, B = nova.Field(GM, 3).upload_soa(U0), nova.Field(GM, 3).upload_soa(B0)
+    rd = nova.run_desc(model="mhd", rk_mode="classical", dt=dt, nu=nu, eta=eta)
+
+    def Jf(u, b):
+        return sum(mhd_forward(nova, N, u, b, dt, nu, eta, n0)) - sum(mhd_forward(nova, N, u, b, dt, nu, eta, nsteps))
+
+    J, gU, gB = nova.adjoint_grad(GM, rd, U, nsteps, checkpoint_every=2, window_start=n0, B0=B)
+    assert J == pytest.approx(Jf(U0, B0), rel=1e-12)
+    gu, gb = gU.download_soa(), gB.download_soa()
+    rng = np.random.default_rng(11)
+    eps = 1e-6
+    for _ in range(2):
+        v, w = smooth_direction(rng, N), smooth_direction(rng, N)
+        fd = (Jf(U0 + eps * v, B0 + eps * w) - Jf(U0 - eps * v, B0 - eps * w)) / (2 * eps)
+        ad = float(np.sum(gu * v) + np.sum(gb * w))
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
