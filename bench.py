@@ -39,6 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "Mpoint-steps/s at 256^3: FP64 vs FP32-split (stated err); adjoint/fwd time ratio"
 UNIT = "Mpoint-steps/s"
 NU = 1.0 / 1600.0
+MHD_NU = 1.0 / 1000.0
 CFL = 0.3
 # algorithmic HBM bytes per grid point for one classical RK4 step of the NS
 # stage kernels (3 components): FP64 stages 72 + 120 + 120 + 72; FP32-split
@@ -66,6 +67,15 @@ def tg_field(n):
     return np.stack([u, v, np.zeros_like(u)])
 
 
+def ot_fields(n):
+    """Orszag-Tang: u = (-2 sin y, 2 sin x, 0), B = (-2 sin 2y + sin z, 2 sin x + sin z, 0)."""
+    x = np.arange(n) * (2 * math.pi / n)
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    U = np.stack([-2.0 * np.sin(Y), 2.0 * np.sin(X), np.zeros_like(X)])
+    B = np.stack([-2.0 * np.sin(2.0 * Y) + np.sin(Z), 2.0 * np.sin(X) + np.sin(Z), np.zeros_like(X)])
+    return U, B
+
+
 def ghosted(U, h=3):
     """(3, n, n, n) unique nodes -> the reference's ghosted AoS Field<vector> layout (periodic images)."""
     n = U.shape[1]
@@ -74,8 +84,9 @@ def ghosted(U, h=3):
     return np.ascontiguousarray(np.moveaxis(g, 0, -1))
 
 
-def cfl_dt(n, U):
-    return CFL * (2 * math.pi / n) / float(np.abs(U).sum(axis=0).max())
+def cfl_dt(n, U, B=None):
+    s = np.abs(U).sum(axis=0) + (0.0 if B is None else np.abs(B).sum(axis=0))
+    return CFL * (2 * math.pi / n) / float(s.max())
 
 
 def max_over_ranks(x, dist, device="cuda"):
@@ -280,6 +291,74 @@ def time_e2e(nova, torch, GM, U, p, rd, U0_aos_pinned, out_pinned, steps, dist):
     return sec, h2d, d2h
 
 
+def mhd_legs(args, nova, torch, dist, world):
+    """Secondary MHD numbers: Orszag-Tang at args.mhd_n^3 (U loop then B loop with
+    its cleaning projection, classical RK4, nu = eta = 1/1000), FP64 and
+    FP32-split, and the MHD adjoint / forward ratio at args.mhd_adj_n^3."""
+    def maxover(x):
+        return max_over_ranks(x, dist)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return maxover(e0.elapsed_time(e1) / 1e3), r
+
+    n, steps = args.mhd_n, args.mhd_steps
+    U0, B0 = ot_fields(n)
+    dt = cfl_dt(n, U0, B0)
+    GM = nova.Mesh((n, n, n))
+    GM.set_stream(torch.cuda.current_stream().cuda_stream)
+    p, pB = nova.Field(GM, 1), nova.Field(GM, 1)
+    out, finals = {}, {}
+    for prec_name, prec in (("f64", nova.F64), ("f32split", nova.F32SPLIT)):
+        U, B = nova.Field(GM, 3, prec).upload_soa(U0), nova.Field(GM, 3, prec).upload_soa(B0)
+        rd = nova.run_desc(model="mhd", rk_mode="classical", precision=prec, dt=dt, nu=MHD_NU, eta=MHD_NU,
+                           diag_every=0)
+        nova.advance(GM, rd, U, p, B, pB, nsteps=3, history=False)
+        GM.launch_count(reset=True)
+        sec, _ = timed(lambda: nova.advance(GM, rd, U, p, B, pB, nsteps=steps, history=False))
+        out[prec_name] = {"value": world * n ** 3 * steps / sec / 1e6, "unit": UNIT,
+                          "ms_per_step": 1e3 * sec / steps, "gpu_launches": GM.launch_count(reset=True)}
+        finals[prec_name] = np.concatenate([U.download_soa(), B.download_soa()])
+        U.close()
+        B.close()
+    out["f32split"]["rel_l2_vs_fp64"] = float(np.linalg.norm(finals["f32split"] - finals["f64"]) /
+                                              np.linalg.norm(finals["f64"]))
+    out["f32split"]["speedup_vs_fp64"] = out["f64"]["ms_per_step"] / out["f32split"]["ms_per_step"]
+    p.close()
+    pB.close()
+    res = {"workload": "Orszag-Tang, periodic [0,2pi]^3, %d^3, classical RK4 U loop + FFT projection, then B "
+                       "loop + cleaning projection, nu=eta=1/1000, CFL 0.3 on |u|+|B|; %d timed steps after 3"
+                       % (n, steps), **out}
+    if not args.no_adjoint:
+        na, M, K = args.mhd_adj_n, args.adj_steps, args.adj_checkpoint
+        U0, B0 = ot_fields(na)
+        dt = cfl_dt(na, U0, B0)
+        AM = nova.Mesh((na, na, na))
+        AM.set_stream(torch.cuda.current_stream().cuda_stream)
+        U, B = nova.Field(AM, 3).upload_soa(U0), nova.Field(AM, 3).upload_soa(B0)
+        p, pB = nova.Field(AM, 1), nova.Field(AM, 1)
+        rd = nova.run_desc(model="mhd", rk_mode="classical", dt=dt, nu=MHD_NU, eta=MHD_NU, diag_every=0)
+        for r in nova.adjoint_grad(AM, rd, U, 2, checkpoint_every=1, B0=B, total_energy=True)[1:]:
+            r.close()  # allocate and warm the path
+        t_fwd, _ = timed(lambda: nova.advance(AM, rd, U, p, B, pB, nsteps=M, history=False))
+        U.upload_soa(U0)
+        B.upload_soa(B0)
+        t_adj, r = timed(lambda: nova.adjoint_grad(AM, rd, U, M, checkpoint_every=K, B0=B, total_energy=True))
+        for f in list(r[1:]) + [U, B, p, pB]:
+            f.close()
+        res["adjoint"] = {"ratio": t_adj / t_fwd, "forward_s": t_fwd, "adjoint_s": t_adj, "grid": [na] * 3,
+                          "steps": M, "checkpoint_every": K, "objective": "E_kin + E_mag at the final step",
+                          "gradients": "dJ/dU0 and dJ/dB0", "dtype": "f64", "J": r[0]}
+    return res
+
+
 def our_arm(args, rank, world, dist):
     import torch
     from novaclone_b200 import nova
@@ -361,6 +440,8 @@ def our_arm(args, rank, world, dist):
                               "ms_per_step": 1e3 * sec / args.steps}
             U.close()
 
+    mhd = None if args.no_mhd else mhd_legs(args, nova, torch, dist, world)
+
     if rank != 0:
         return 0
 
@@ -410,6 +491,7 @@ def our_arm(args, rank, world, dist):
                       "e2e": e2e.get("f32split"), "gpu_launches": f32["launches"], "clocks": f32["clocks"]},
         "adjoint_fwd_ratio": None if adj is None else adj["ratio"],
         "adjoint": adj,
+        "mhd": mhd,
     }
     print(json.dumps(line))
     return 0
@@ -428,8 +510,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--adj-steps", type=int, default=40)
+    ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--adj-checkpoint", type=int, default=20)
+    ap.add_argument("--no-mhd", action="store_true")
+    ap.add_argument("--mhd-n", type=int, default=256)
+    ap.add_argument("--mhd-steps", type=int, default=20)
+    ap.add_argument("--mhd-adj-n", type=int, default=128)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

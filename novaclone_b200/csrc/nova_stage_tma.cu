@@ -33,6 +33,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstring>
+#include <type_traits>
 
 namespace nova {
 
@@ -217,69 +218,157 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
         return x < 0 ? kTcbE + lrrow + 4 + x : (x >= kTK ? kTcbE + kLRE + lrrow + (x - kTK) : cen + s);
     };
 
-    T q[2 * H + 1][3];
-    bool ok = true;
-    for (int n = 0; n < 2 * H; n++) {  // queue: planes ib-3 .. ib+2
-        ok = mbar_wait(full(n % kRing), (n / kRing) & 1, err);
-        if (!__all_sync(0xffffffffu, ok)) {
-            ok = false;
-            break;
-        }
-        const T *sl = ring + (n % kRing) * kSlotE;
-#pragma unroll
-        for (int c = 0; c < 3; c++) q[n + 1][c] = sl[cen + c * kTK];
-        if (n < H || n >= H + nout) release(empty(n % kRing));  // queue-only plane
-    }
-
-    for (int p = 0; p < nout && ok; p++) {
-        const int hd = p + 2 * H;  // queue head: plane ib + p + 3
-        ok = mbar_wait(full(hd % kRing), (hd / kRing) & 1, err);
-        if (!__all_sync(0xffffffffu, ok)) {
-            ok = false;
-            break;
-        }
-#pragma unroll
-        for (int s = 0; s < 2 * H; s++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) q[s][c] = q[s + 1][c];
-        {
-            const T *sh = ring + (hd % kRing) * kSlotE;
-#pragma unroll
-            for (int c = 0; c < 3; c++) q[2 * H][c] = sh[cen + c * kTK];
-            if (hd >= H + nout) release(empty(hd % kRing));
-        }
-
-        const int cur = p + H;
-        const T *sl = ring + (cur % kRing) * kSlotE;
-        auto vx = [&](int c, int s) -> T { return q[H + s][c]; };
-        auto vy = [&](int c, int s) -> T { return sl[cen + s * kRowE + c * kTK]; };
-        auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
-        const T u0[3] = {q[H][0], q[H][1], q[H][2]};
-        T rhs[3];
-        ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
-
-        T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
-        if constexpr (NE > 0) {
-            ok = mbar_wait(efull(p % kERing), (p / kERing) & 1, err);
+    // i-stencil queue of the centre values of planes cur-3 .. cur+3.
+    // FP64: the queue shifts by one plane per step (q[s] = logical s); the
+    // unrolled form below exceeds the FP64 kernel's 96-register budget.
+    // FP32: plane ib - H + x lives in q[x % 7], so logical plane s (0..2H,
+    // centre H) of step p is q[(p + s) % 7]; the loop is unrolled by 7
+    // (= 2H + 1 = kRing) so that the rotation is register renaming and every
+    // ring slot index is a compile-time constant of the unrolled step.
+    if constexpr (sizeof(T) == 8) {
+        T q[2 * H + 1][3];
+        bool ok = true;
+        for (int n = 0; n < 2 * H; n++) {  // queue: planes ib-3 .. ib+2
+            ok = mbar_wait(full(n % kRing), (n / kRing) & 1, err);
             if (!__all_sync(0xffffffffu, ok)) {
                 ok = false;
                 break;
             }
-            const T *se = ering + (p % kERing) * NE * kEpiE + ty * kRowE + tx;
+            const T *sl = ring + (n % kRing) * kSlotE;
 #pragma unroll
-            for (int c = 0; c < 3; c++) epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
+            for (int c = 0; c < 3; c++) q[n + 1][c] = sl[cen + c * kTK];
+            if (n < H || n >= H + nout) release(empty(n % kRing));  // queue-only plane
         }
-        const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
+
+        for (int p = 0; p < nout && ok; p++) {
+            const int hd = p + 2 * H;  // queue head: plane ib + p + 3
+            ok = mbar_wait(full(hd % kRing), (hd / kRing) & 1, err);
+            if (!__all_sync(0xffffffffu, ok)) {
+                ok = false;
+                break;
+            }
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const long long o = (long long)c * g.N3 + idx;
-            if constexpr (sizeof(T) == 8)
-                rk_store64<STAGE>(args, o, q[H][c], e0[c], e1[c], dt * rhs[c]);
-            else
-                rk_store32<STAGE>(args, o, q[H][c], e0[c], e1[c], lo[c], dt * rhs[c]);
+            for (int s = 0; s < 2 * H; s++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) q[s][c] = q[s + 1][c];
+            {
+                const T *sh = ring + (hd % kRing) * kSlotE;
+#pragma unroll
+                for (int c = 0; c < 3; c++) q[2 * H][c] = sh[cen + c * kTK];
+                if (hd >= H + nout) release(empty(hd % kRing));
+            }
+
+            const int cur = p + H;
+            const T *sl = ring + (cur % kRing) * kSlotE;
+            auto vx = [&](int c, int s) -> T { return q[H + s][c]; };
+            auto vy = [&](int c, int s) -> T { return sl[cen + s * kRowE + c * kTK]; };
+            auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
+            const T u0[3] = {q[H][0], q[H][1], q[H][2]};
+            T rhs[3];
+            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+
+            T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
+            if constexpr (NE > 0) {
+                ok = mbar_wait(efull(p % kERing), (p / kERing) & 1, err);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    ok = false;
+                    break;
+                }
+                const T *se = ering + (p % kERing) * NE * kEpiE + ty * kRowE + tx;
+#pragma unroll
+                for (int c = 0; c < 3; c++) epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
+            }
+            const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const long long o = (long long)c * g.N3 + idx;
+                if constexpr (sizeof(T) == 8)
+                    rk_store64<STAGE>(args, o, q[H][c], e0[c], e1[c], dt * rhs[c]);
+                else
+                    rk_store32<STAGE>(args, o, q[H][c], e0[c], e1[c], lo[c], dt * rhs[c]);
+            }
+            if constexpr (NE > 0) release(eempty(p % kERing));
+            release(empty(cur % kRing));
         }
-        if constexpr (NE > 0) release(eempty(p % kERing));
-        release(empty(cur % kRing));
+    } else {
+        static_assert(kRing == 2 * H + 1, "queue rotation and ring slots share one period");
+        T q[2 * H + 1][3];
+        bool ok = true;
+        for (int n = 0; n < 2 * H; n++) {  // queue: planes ib-3 .. ib+2
+            ok = mbar_wait(full(n % kRing), (n / kRing) & 1, err);
+            if (!__all_sync(0xffffffffu, ok)) {
+                ok = false;
+                break;
+            }
+            const T *sl = ring + (n % kRing) * kSlotE;
+#pragma unroll
+            for (int c = 0; c < 3; c++) q[n][c] = sl[cen + c * kTK];
+            if (n < H || n >= H + nout) release(empty(n % kRing));  // queue-only plane
+        }
+
+        int es = 0, eph = 0;  // epilogue ring slot and phase of step p
+        // step p = 7 m + R: queue head plane hd = p + 2H, centre plane cur = p + H
+        auto step = [&](auto Rc, int m, int p) -> bool {
+            constexpr int R = decltype(Rc)::value;
+            const int hd = p + 2 * H;
+            constexpr int sHd = (R + 2 * H) % kRing, sCur = (R + H) % kRing;
+            if (!__all_sync(0xffffffffu, mbar_wait(full(sHd), (m + (R + 2 * H) / kRing) & 1, err))) return false;
+            {
+                // the new head, plane ib + p + H, replaces plane ib + p - H - 1
+                constexpr int kQ = (R + 2 * H) % (2 * H + 1);
+                const T *sh = ring + sHd * kSlotE;
+#pragma unroll
+                for (int c = 0; c < 3; c++) q[kQ][c] = sh[cen + c * kTK];
+                if (hd >= H + nout) release(empty(sHd));
+            }
+            const T *sl = ring + sCur * kSlotE;
+            auto vx = [&](int c, int s) -> T { return q[(R + H + s + 2 * H + 1) % (2 * H + 1)][c]; };
+            auto vy = [&](int c, int s) -> T { return sl[cen + s * kRowE + c * kTK]; };
+            auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
+            constexpr int kC = (R + H) % (2 * H + 1);
+            const T u0[3] = {q[kC][0], q[kC][1], q[kC][2]};
+            T rhs[3];
+            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+
+            T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
+            if constexpr (NE > 0) {
+                if (!__all_sync(0xffffffffu, mbar_wait(efull(es), eph, err))) return false;
+                const T *se = ering + es * NE * kEpiE + ty * kRowE + tx;
+#pragma unroll
+                for (int c = 0; c < 3; c++) epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
+            }
+            const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const long long o = (long long)c * g.N3 + idx;
+                if constexpr (sizeof(T) == 8)
+                    rk_store64<STAGE>(args, o, u0[c], e0[c], e1[c], dt * rhs[c]);
+                else
+                    rk_store32<STAGE>(args, o, u0[c], e0[c], e1[c], lo[c], dt * rhs[c]);
+            }
+            if constexpr (NE > 0) {
+                release(eempty(es));
+                if (++es == kERing) {
+                    es = 0;
+                    eph ^= 1;
+                }
+            }
+            release(empty(sCur));
+            return true;
+        };
+        using I0 = std::integral_constant<int, 0>;
+        using I1 = std::integral_constant<int, 1>;
+        using I2 = std::integral_constant<int, 2>;
+        using I3 = std::integral_constant<int, 3>;
+        using I4 = std::integral_constant<int, 4>;
+        using I5 = std::integral_constant<int, 5>;
+        using I6 = std::integral_constant<int, 6>;
+        for (int m = 0, p = 0; ok && p < nout; m++, p += kRing) {
+            ok = step(I0{}, m, p) && (p + 1 >= nout || (step(I1{}, m, p + 1) && (p + 2 >= nout ||
+                 (step(I2{}, m, p + 2) && (p + 3 >= nout || (step(I3{}, m, p + 3) && (p + 4 >= nout ||
+                 (step(I4{}, m, p + 4) && (p + 5 >= nout || (step(I5{}, m, p + 5) && (p + 6 >= nout ||
+                 step(I6{}, m, p + 6))))))))))));
+        }
     }
 
 }
