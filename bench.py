@@ -345,8 +345,8 @@ def mhd_legs(args, nova, torch, dist, world):
         U, B = nova.Field(AM, 3).upload_soa(U0), nova.Field(AM, 3).upload_soa(B0)
         p, pB = nova.Field(AM, 1), nova.Field(AM, 1)
         rd = nova.run_desc(model="mhd", rk_mode="classical", dt=dt, nu=MHD_NU, eta=MHD_NU, diag_every=0)
-        for r in nova.adjoint_grad(AM, rd, U, 2, checkpoint_every=1, B0=B, total_energy=True)[1:]:
-            r.close()  # allocate and warm the path
+        for r in nova.adjoint_grad(AM, rd, U, M, checkpoint_every=K, B0=B, total_energy=True)[1:]:
+            r.close()  # warm-up: the same call, which also sizes the checkpoint pool
         t_fwd, _ = timed(lambda: nova.advance(AM, rd, U, p, B, pB, nsteps=M, history=False))
         U.upload_soa(U0)
         B.upload_soa(B0)
@@ -394,31 +394,44 @@ def our_arm(args, rank, world, dist):
 
     err = float(np.linalg.norm(finals["f32split"] - finals["f64"]) / np.linalg.norm(finals["f64"]))
 
-    # adjoint / forward wall-time ratio (FP64): gradient of E_kin after M steps
-    # with checkpoints every K steps, against an M-step forward solve
+    # adjoint / forward wall-time ratio: gradient of E_kin after M steps with
+    # checkpoints every K steps, against an M-step forward solve of the same
+    # precision (FP64, then FP32-split, whose gradient is compared with FP64's)
     adj = None
     if not args.no_adjoint:
         M, K = args.adj_steps, args.adj_checkpoint
-        U = nova.Field(GM, 3).upload_soa(U0)
-        rd = nova.run_desc(model="ns", rk_mode="classical", precision=nova.F64, dt=dt, nu=NU, diag_every=0)
-        nova.adjoint_grad(GM, rd, U, 2, checkpoint_every=1)  # allocate and warm the path
-        torch.cuda.synchronize()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        e[0].record()
-        nova.advance(GM, rd, U, p, nsteps=M, history=False)
-        e[1].record()
-        U.upload_soa(U0)
-        torch.cuda.synchronize()
-        e[2].record()
-        J, grad = nova.adjoint_grad(GM, rd, U, M, checkpoint_every=K)
-        e[3].record()
-        torch.cuda.synchronize()
-        t_fwd = e[0].elapsed_time(e[1]) / 1e3
-        t_adj = e[2].elapsed_time(e[3]) / 1e3
-        adj = {"ratio": maxover(t_adj) / maxover(t_fwd), "forward_s": t_fwd, "adjoint_s": t_adj, "steps": M,
-               "checkpoint_every": K, "objective": "E_kin at the final step", "dtype": "f64", "J": J}
-        grad.close()
-        U.close()
+        adj_runs = {}
+        for prec_name, prec in (("f64", nova.F64), ("f32split", nova.F32SPLIT)):
+            U = nova.Field(GM, 3, prec).upload_soa(U0)
+            rd = nova.run_desc(model="ns", rk_mode="classical", precision=prec, dt=dt, nu=NU, diag_every=0)
+            # warm-up: the same call, which also sizes the checkpoint pool (a
+            # one-time device allocation of about (M/K + 4K + 5) fields)
+            nova.adjoint_grad(GM, rd, U, M, checkpoint_every=K)[1].close()
+            torch.cuda.synchronize()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record()
+            nova.advance(GM, rd, U, p, nsteps=M, history=False)
+            e[1].record()
+            U.upload_soa(U0)
+            torch.cuda.synchronize()
+            e[2].record()
+            J, grad = nova.adjoint_grad(GM, rd, U, M, checkpoint_every=K)
+            e[3].record()
+            torch.cuda.synchronize()
+            t_fwd = maxover(e[0].elapsed_time(e[1]) / 1e3)
+            t_adj = maxover(e[2].elapsed_time(e[3]) / 1e3)
+            adj_runs[prec_name] = {"ratio": t_adj / t_fwd, "forward_s": t_fwd, "adjoint_s": t_adj, "J": J,
+                                   "grad": grad.download_soa()}
+            grad.close()
+            U.close()
+        f, s32 = adj_runs["f64"], adj_runs["f32split"]
+        adj = {"ratio": f["ratio"], "forward_s": f["forward_s"], "adjoint_s": f["adjoint_s"], "steps": M,
+               "checkpoint_every": K, "objective": "E_kin at the final step", "dtype": "f64", "J": f["J"],
+               "f32split": {"ratio": s32["ratio"], "forward_s": s32["forward_s"], "adjoint_s": s32["adjoint_s"],
+                            "J": s32["J"], "grad_rel_l2_vs_fp64": float(np.linalg.norm(s32["grad"] - f["grad"]) /
+                                                                        np.linalg.norm(f["grad"])),
+                            "dtype": "f32 adjoint stages and stage states, f64 adjoint state and projection"}}
+        del adj_runs
     t_end = (args.warmup + args.steps) * dt
 
     # e2e through the reference-layout ABI (ghosted AoS host buffers, pinned)

@@ -26,58 +26,61 @@ namespace nova {
 
 namespace {
 
-template <int H, int S>
-__global__ void __launch_bounds__(kThreads, 1) k_adj_stage(Geo g, Coef<double> co, const double *__restrict__ ia,
-                                                           double dt, double nu, AdjArgs a, int ichunk)
+// T: the arithmetic and storage type of the stage states, the directions g
+// and the running sum Lam (double, or float for the FP32-split adjoint, A =
+// AdjArgs32); mu and the resulting dJ/dU are FP64 in both.
+template <typename T, int H, int S, class A>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
+    k_adj_stage(Geo g, Coef<T> co, const T *__restrict__ ia, T dt, T nu, A a, int ichunk)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    auto &sm = *reinterpret_cast<TileSmem<double, H, 6> *>(smraw);
+    auto &sm = *reinterpret_cast<TileSmem<T, H, 6> *>(smraw);
     const int ib = blockIdx.z * ichunk;
     const int ie = min(ib + ichunk, g.N0);
     const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
-    const double iak = ia[kw];
-    double az[H], bz[H];
+    const T iak = ia[kw];
+    T az[H], bz[H];
 #pragma unroll
     for (int l = 0; l < H; l++) {
         az[l] = co.a[2][l] * iak;
         bz[l] = co.b[2][l] * iak * iak;
     }
-    const double bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
+    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
     // comps 0-2: forward stage state Y, 3-5: adjoint stage direction g (= mu/6 at s=4)
-    const double gs = (S == 4) ? 1.0 / 6.0 : 1.0;
-    auto ld = [&](int c, long long o) -> double {
-        return c < 3 ? a.Y[(long long)c * g.N3 + o] : a.G[(long long)(c - 3) * g.N3 + o] * gs;
+    auto ld = [&](int c, long long o) -> T {
+        if (c < 3) return a.Y[(long long)c * g.N3 + o];
+        if constexpr (S == 4) return (T)(a.mu[(long long)(c - 3) * g.N3 + o] * (1.0 / 6.0));
+        return a.G[(long long)(c - 3) * g.N3 + o];
     };
-    const Walls<double> wl{};  // the adjoint is built for periodic meshes
-    tile_march<double, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
-                                                      const auto &vz) {
-        double mu[3], lam[3];
+    const Walls<T> wl{};  // the adjoint is built for periodic meshes
+    tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
+                                                  const auto &vz) {
+        double mu[3];
+        T lam[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             mu[c] = a.mu[(long long)c * g.N3 + idx];
             if (S != 4) lam[c] = a.Lam[(long long)c * g.N3 + idx];
         }
-        const double y0[3] = {q[H][0], q[H][1], q[H][2]};
-        const double g0[3] = {q[H][3], q[H][4], q[H][5]};
-        double At[3] = {0, 0, 0};   // the e = d terms
-        double Bt[3] = {0, 0, 0};   // - sum_d A_d(Y,g)_e
-        double lap[3] = {0, 0, 0};
-        double divY = 0.0;
-        auto dir = [&](const auto &v, int d, const double *aa, const double *bb) {
-            double dY[3], dG[3];
+        const T y0[3] = {q[H][0], q[H][1], q[H][2]};
+        const T g0[3] = {q[H][3], q[H][4], q[H][5]};
+        T At[3] = {0, 0, 0};   // the e = d terms
+        T Bt[3] = {0, 0, 0};   // - sum_d A_d(Y,g)_e
+        T lap[3] = {0, 0, 0};
+        T divY = 0;
+        auto dir = [&](const auto &v, int d, const T *aa, const T *bb) {
+            T dY[3], dG[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                dY[c] = d1<double, H>(v, c, aa);
-                dG[c] = d1<double, H>(v, 3 + c, aa);
-                Bt[c] -= adv1<double, H>(v, 3 + c, d, y0[d], aa);
-                lap[c] += lsum<double, H>(v, 3 + c, bb);
+                dY[c] = d1<T, H>(v, c, aa);
+                dG[c] = d1<T, H>(v, 3 + c, aa);
+                Bt[c] -= adv1<T, H>(v, 3 + c, d, y0[d], aa);
+                lap[c] += lsum<T, H>(v, 3 + c, bb);
             }
             divY += dY[d];
             // D_d(sum_c Y_c g_c)
-            auto sdot = [&](int, int s) -> double {
-                return v(0, s) * v(3, s) + v(1, s) * v(4, s) + v(2, s) * v(5, s);
-            };
-            const double ds = d1<double, H>(sdot, 0, aa);
+            auto sdot = [&](int, int s) -> T { return v(0, s) * v(3, s) + v(1, s) * v(4, s) + v(2, s) * v(5, s); };
+            const T ds = d1<T, H>(sdot, 0, aa);
             At[d] = -(y0[0] * dG[0] + y0[1] * dG[1] + y0[2] * dG[2]) + (g0[0] * dY[0] + g0[1] * dY[1] + g0[2] * dY[2])
                     - ds;
         };
@@ -86,37 +89,49 @@ __global__ void __launch_bounds__(kThreads, 1) k_adj_stage(Geo g, Coef<double> c
         dir(vz, 2, az, bz);
 #pragma unroll
         for (int e = 0; e < 3; e++) {
-            const double ntg = 0.5 * (At[e] + fma(g0[e], divY, Bt[e]));
-            const double xi = dt * (-ntg + nu * fma(-bsum, g0[e], lap[e]));
+            const T ntg = T(0.5) * (At[e] + fma(g0[e], divY, Bt[e]));
+            const T xi = dt * (-ntg + nu * fma(-bsum, g0[e], lap[e]));
             const long long o = (long long)e * g.N3 + idx;
             if constexpr (S == 4) {
-                a.Gout[o] = mu[e] * (1.0 / 3.0) + xi;
+                a.Gout[o] = (T)(mu[e] * (1.0 / 3.0)) + xi;
                 a.LamOut[o] = xi;
             } else if constexpr (S == 3) {
-                a.Gout[o] = mu[e] * (1.0 / 3.0) + 0.5 * xi;
+                a.Gout[o] = (T)(mu[e] * (1.0 / 3.0)) + T(0.5) * xi;
                 a.LamOut[o] = lam[e] + xi;
             } else if constexpr (S == 2) {
-                a.Gout[o] = mu[e] * (1.0 / 6.0) + 0.5 * xi;
+                a.Gout[o] = (T)(mu[e] * (1.0 / 6.0)) + T(0.5) * xi;
                 a.LamOut[o] = lam[e] + xi;
-            } else {
+            } else if constexpr (sizeof(T) == 8) {
                 a.Gout[o] = mu[e] + (lam[e] + xi);
+            } else {
+                a.lam[o] = mu[e] + (double)(lam[e] + xi);
             }
         }
     });
 }
 
-template <int S>
-void launch_s(const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu, const AdjArgs &a,
-              cudaStream_t st)
+template <typename T, int S, class A>
+void launch_s(const Geo &g, const Coef<T> &co, const T *ia, T dt, T nu, const A &a, cudaStream_t st)
 {
-    constexpr size_t smem = tile_smem_bytes<double, 3, 6>();
+    constexpr size_t smem = tile_smem_bytes<T, 3, 6>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_adj_stage<3, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_adj_stage<T, 3, S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    const int ch = pick_ichunk(g, 1);
-    k_adj_stage<3, S><<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, dt, nu, a, ch);
+    const int ch = pick_ichunk(g, sizeof(T) == 8 ? 1 : 2);
+    k_adj_stage<T, 3, S, A><<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, dt, nu, a, ch);
+}
+
+template <typename T, class A>
+void launch_adj(int s, const Geo &g, const Coef<T> &co, const T *ia, T dt, T nu, const A &a, cudaStream_t st)
+{
+    switch (s) {
+    case 4: launch_s<T, 4>(g, co, ia, dt, nu, a, st); break;
+    case 3: launch_s<T, 3>(g, co, ia, dt, nu, a, st); break;
+    case 2: launch_s<T, 2>(g, co, ia, dt, nu, a, st); break;
+    default: launch_s<T, 1>(g, co, ia, dt, nu, a, st); break;
+    }
 }
 
 // ----------------------------------------------------------- MHD adjoint --
@@ -260,12 +275,13 @@ void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t
 void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                         const AdjArgs &a, cudaStream_t st)
 {
-    switch (s) {
-    case 4: launch_s<4>(g, co, ia, dt, nu, a, st); break;
-    case 3: launch_s<3>(g, co, ia, dt, nu, a, st); break;
-    case 2: launch_s<2>(g, co, ia, dt, nu, a, st); break;
-    default: launch_s<1>(g, co, ia, dt, nu, a, st); break;
-    }
+    launch_adj<double>(s, g, co, ia, dt, nu, a, st);
+}
+
+void launch_adj_stage32(int s, const Geo &g, const Coef<float> &co, const float *ia, float dt, float nu,
+                        const AdjArgs32 &a, cudaStream_t st)
+{
+    launch_adj<float>(s, g, co, ia, dt, nu, a, st);
 }
 
 void launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double visc,

@@ -1142,6 +1142,48 @@ nova_status rk_loop64(nova_ctx *ctx, const nova_run_desc *rd, int phys, double v
     return NOVA_OK;
 }
 
+// One classical RK4 step + projection of an FP32-split Navier-Stokes state,
+// the launches of the split path of nova_advance: (hi, lo) -> (ohi, olo) (may
+// alias), FP32 stage states into S2, S3, S4 (S4 may alias S2), the pressure
+// into pbuf (FP64).  Without `full` only the stage states are produced.
+nova_status rk_loop32(nova_ctx *ctx, const nova_run_desc *rd, const float *hi, const float *lo, float *S2, float *S3,
+                      float *S4, float *ohi, float *olo, double *pbuf, bool full)
+{
+    const Geo &g = ctx->g;
+    cudaStream_t st = ctx->stream;
+    float *A = ctx->w32[2];
+    const bool str = ctx->md.hyperbolic_z != 0;
+    nova_status sst = NOVA_OK;
+    auto run = [&](int stage, const StageArgs32 &a) {
+        ProfScope ps(ctx, NOVA_K_STAGE);
+        const cudaError_t e = launch_stage32(PHYS_NS, stage, str, g, Walls<float>{}, ctx->co32, ctx->d_ia32,
+                                             ctx->d_corr32, (float)rd->dt, (float)rd->nu, a, st,
+                                             StageExec{ctx->stage_impl, ctx->d_flag + 1});
+        if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
+        ctx->launches += 1;
+    };
+    run(0, StageArgs32{hi, nullptr, nullptr, nullptr, A, S2, nullptr, nullptr});
+    run(1, StageArgs32{S2, nullptr, hi, nullptr, A, S3, nullptr, nullptr});
+    run(2, StageArgs32{S3, nullptr, hi, nullptr, A, S4, nullptr, nullptr});
+    if (full) run(3, StageArgs32{S4, nullptr, hi, lo, A, nullptr, ohi, olo});
+    if (sst != NOVA_OK) return sst;
+    CKL("stage kernel");
+    if (!full) return NOVA_OK;
+    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, ohi, olo, rd->dt,
+                                    ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+    if (e != cudaSuccess) return stage_fail(ctx, e);
+    ctx->launches += 1;
+    CKL("k_div_tiled");
+    nova_status s = poisson_device(ctx, ctx->d_rhs, pbuf);
+    if (s != NOVA_OK) return s;
+    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, rd->dt, nullptr, nullptr, ohi, olo,
+                       ohi, olo, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+    if (e != cudaSuccess) return stage_fail(ctx, e);
+    ctx->launches += 1;
+    CKL("k_correct_tiled");
+    return NOVA_OK;
+}
+
 // One classical RK4 step + projection of an FP64 Navier-Stokes state:
 // Uin -> Uout (may alias), stage states into Y2, Y3, Y4 (Y4 may alias Y2).
 // Without `full` only the stage states are produced.
@@ -1184,6 +1226,8 @@ nova_status adj_pool(nova_ctx *ctx, size_t need)
 
 nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
                         nova_field *gradB, double *objective);
+nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
+                          double *objective);
 
 }  // namespace
 
@@ -1193,8 +1237,11 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     if (!ctx || !ad || !init || !gradU) return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: null argument");
     const nova_run_desc *rd = &ad->run;
     const bool mhd = rd->model == NOVA_MODEL_MHD;
-    if ((rd->model != NOVA_MODEL_NS && !mhd) || rd->rk_mode != NOVA_RK_CLASSICAL || rd->precision != NOVA_F64)
-        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: built for FP64 Navier-Stokes and MHD, classical RK4");
+    const bool split = rd->precision == NOVA_F32SPLIT;
+    if ((rd->model != NOVA_MODEL_NS && !mhd) || rd->rk_mode != NOVA_RK_CLASSICAL ||
+        (rd->precision != NOVA_F64 && !(split && !mhd)))
+        return fail(ctx, NOVA_E_UNSUPPORTED,
+                    "nova_adjoint_grad: built for classical RK4: FP64 or FP32-split Navier-Stokes, FP64 MHD");
     const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
     if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window && !(mhd && ad->objective == NOVA_OBJ_ETOT_FINAL))
         return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective for this model");
@@ -1205,8 +1252,10 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: periodic uniform meshes only");
     if (ad->nsteps < 1 || ad->checkpoint_every < 1 || !(rd->dt > 0.0))
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: nsteps, checkpoint_every and dt must be positive");
-    if (!valid_field(init->U, 3) || init->U->prec != NOVA_F64 || !valid_field(gradU, 3) || gradU->prec != NOVA_F64)
-        return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: U and gradU must be FP64 3-component fields");
+    if (!valid_field(init->U, 3) || init->U->prec != rd->precision || !valid_field(gradU, 3) ||
+        gradU->prec != NOVA_F64)
+        return fail(ctx, NOVA_E_INVALID,
+                    "nova_adjoint_grad: U (3 comps, run precision) and gradU (3 comps, FP64) required");
     if (mhd) {
         if (!valid_field(init->B, 3) || init->B->prec != NOVA_F64 || !gradB || !valid_field(gradB, 3) ||
             gradB->prec != NOVA_F64)
@@ -1214,6 +1263,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return adjoint_mhd(ctx, ad, init, gradU, gradB, objective);
     }
     if (gradB) return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: gradB is for MHD runs (pass NULL)");
+    if (split) return adjoint_split(ctx, ad, init, gradU, objective);
     nova_status s = ensure_work(ctx, NOVA_F64);
     if (s != NOVA_OK) return s;
     CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
@@ -1485,6 +1535,142 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
     if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
     const double E = row[2] + (etot ? row[3] : 0.0);
     const double J = window ? (row[NOVA_HIST_COLS + 2] + row[NOVA_HIST_COLS + 3]) - E : E;
+    if (objective) *objective = J;
+    if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
+    return NOVA_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// FP32-split adjoint: the trajectory of the split path of nova_advance (FP32
+// stage states, (hi, lo) state, FP64 projection) and the adjoint stage
+// kernels in FP32 (stage states, directions g, running sum Lam); the adjoint
+// lam = dJ/dU between steps and its projection mu = P lam stay FP64, and the
+// last reverse stage forms lam = mu + (Lam + xi) in FP64.  Checkpoints keep
+// the (hi, lo) pairs, so the recomputed segments repeat the forward pass bit
+// for bit.
+nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
+                          double *objective)
+{
+    const nova_run_desc *rd = &ad->run;
+    const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
+    nova_status s = ensure_work(ctx, NOVA_F32SPLIT);
+    if (s != NOVA_OK) return s;
+    CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
+    const int N = ad->nsteps, K = ad->checkpoint_every;
+    const int nck = (N + K - 1) / K;
+    const int mmax = K < N ? K : N;
+    const size_t V = 3 * (size_t)ctx->g.N3;
+    const size_t Vf = (V + 63) / 64 * 64;  // float field stride (256-byte aligned starts)
+    // layout: FP64 lam, mu, pbuf | FP32: nck (hi, lo) checkpoints, mmax + 1 step states (hi),
+    // 3 mmax stage states, lo_run, lo_n0, gA, gB, Lam
+    const size_t nf = 2 * (size_t)nck + (mmax + 1) + 3 * (size_t)mmax + 5;
+    if ((s = adj_pool(ctx, 3 * V + (nf * Vf + 1) / 2)) != NOVA_OK) return s;
+    double *lam = ctx->adj_pool, *mu = lam + V, *pbuf = mu + V;
+    float *fl = reinterpret_cast<float *>(pbuf + V);
+    auto F = [&](size_t i) { return fl + Vf * i; };
+    auto ckhi = [&](int c) { return F(2 * (size_t)c); };
+    auto cklo = [&](int c) { return F(2 * (size_t)c + 1); };
+    const size_t b1 = 2 * (size_t)nck, b2 = b1 + mmax + 1, b3 = b2 + 3 * (size_t)mmax;
+    auto Y1 = [&](int t) { return F(b1 + t); };
+    auto Ys = [&](int t, int st) { return F(b2 + 3 * (size_t)t + (st - 2)); };  // stage states 2, 3, 4
+    float *lo_run = F(b3), *lo_n0 = F(b3 + 1), *gA = F(b3 + 2), *gB = F(b3 + 3), *Lam = F(b3 + 4);
+    float *runhi = gA, *runlo = gB;  // running state of the forward pass outside the kept segment
+    float *w0 = ctx->w32[0], *w1 = ctx->w32[1];
+    cudaStream_t st = ctx->stream;
+    auto copyf = [&](float *dst, const float *src) {
+        return cudaMemcpyAsync(dst, src, sizeof(float) * V, cudaMemcpyDeviceToDevice, st);
+    };
+    auto energy = [&](const float *hi, const float *lo, double *row_dev) {
+        launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, hi, lo, nullptr, nullptr,
+                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
+        ctx->launches += 2;
+    };
+
+    const int c_last = nck - 1, n_last = c_last * K, m_last = N - n_last;
+    CK(copyf(ckhi(0), init->U->hi));
+    CK(copyf(cklo(0), init->U->lo));
+    if ((s = dalloc(ctx, &ctx->d_row, 2 * NOVA_HIST_COLS)) != NOVA_OK) return s;
+    const int n0w = window ? ad->window_start : -1;
+    for (int n = 0; n < N; n++) {
+        const bool kept = n >= n_last;
+        const int t = n - n_last;
+        if (kept && t == 0) {
+            CK(copyf(Y1(0), ckhi(c_last)));
+            CK(copyf(lo_run, cklo(c_last)));
+        }
+        const bool ck = !kept && n % K == 0;
+        const float *hi = kept ? Y1(t) : (ck ? ckhi(n / K) : runhi);
+        const float *lo = kept ? lo_run : (ck ? cklo(n / K) : runlo);
+        if (n == n0w) {  // E(n0) of the window: the state before step n0
+            energy(hi, lo, ctx->d_row + NOVA_HIST_COLS);
+            CK(copyf(lo_n0, lo));
+        }
+        if (kept) {
+            if ((s = rk_loop32(ctx, rd, Y1(t), lo_run, Ys(t, 2), Ys(t, 3), Ys(t, 4), Y1(t + 1), lo_run, pbuf,
+                               true)) != NOVA_OK)
+                return s;
+            continue;
+        }
+        if ((s = rk_loop32(ctx, rd, hi, lo, w0, w1, w0, runhi, runlo, pbuf, true)) != NOVA_OK) return s;
+        if ((n + 1) % K == 0 && n + 1 < N) {
+            CK(copyf(ckhi((n + 1) / K), runhi));
+            CK(copyf(cklo((n + 1) / K), runlo));
+        }
+    }
+    // E(N); lam_N = +-U_N / N^3 with U_N = hi + lo
+    energy(Y1(m_last), lo_run, ctx->d_row);
+    double row[2 * NOVA_HIST_COLS];
+    CK(cudaMemcpyAsync(row, ctx->d_row, sizeof(row), cudaMemcpyDeviceToHost, st));
+    launch_join((long long)V, Y1(m_last), lo_run, lam, st);
+    launch_scale_copy((long long)V, (window ? -1.0 : 1.0) / (double)ctx->g.N3, lam, lam, st);
+    ctx->launches += 2;
+    CKL("adjoint seed");
+
+    const float dt = (float)rd->dt, nu = (float)rd->nu;
+    auto adj = [&](int stage, const AdjArgs32 &a) {
+        ProfScope ps(ctx, NOVA_K_ADJ);
+        launch_adj_stage32(stage, ctx->g, ctx->co32, ctx->d_ia32, dt, nu, a, st);
+        ctx->launches += 1;
+    };
+    for (int c = nck - 1; c >= 0; c--) {
+        const int n0 = c * K;
+        const int m = (N - n0) < K ? (N - n0) : K;
+        if (c != c_last) {
+            CK(copyf(Y1(0), ckhi(c)));
+            CK(copyf(lo_run, cklo(c)));
+            for (int t = 0; t < m; t++) {
+                if (n0 + t == n0w) CK(copyf(lo_n0, lo_run));
+                if ((s = rk_loop32(ctx, rd, Y1(t), lo_run, Ys(t, 2), Ys(t, 3), Ys(t, 4), Y1(t + 1), lo_run, pbuf,
+                                   t + 1 < m)) != NOVA_OK)
+                    return s;
+            }
+        }
+        for (int t = m - 1; t >= 0; t--) {
+            {
+                ProfScope ps(ctx, NOVA_K_DIV);
+                if ((s = project64(ctx, lam, mu, pbuf)) != NOVA_OK) return s;
+            }
+            adj(4, AdjArgs32{Ys(t, 4), nullptr, mu, nullptr, gA, Lam, nullptr});
+            adj(3, AdjArgs32{Ys(t, 3), gA, mu, Lam, gB, Lam, nullptr});
+            adj(2, AdjArgs32{Ys(t, 2), gB, mu, Lam, gA, Lam, nullptr});
+            adj(1, AdjArgs32{Y1(t), gA, mu, Lam, nullptr, nullptr, lam});
+            CKL("k_adj_stage");
+            if (n0 + t == n0w) {  // lam is dJ/dU_n0: add dEk(n0)/dU_n0 = U_n0 / N^3
+                launch_join((long long)V, Y1(t), lo_n0, pbuf, st);
+                launch_axpy((long long)V, 1.0 / (double)ctx->g.N3, pbuf, lam, st);
+                ctx->launches += 2;
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(gradU->d64, lam, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    int perr = 0;
+    CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
+    const double J = window ? row[NOVA_HIST_COLS + 2] - row[2] : row[2];
     if (objective) *objective = J;
     if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
     return NOVA_OK;

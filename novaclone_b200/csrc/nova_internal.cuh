@@ -174,6 +174,19 @@ struct AdjArgs {
 };
 void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                         const AdjArgs &a, cudaStream_t st);
+// FP32-split adjoint stage: FP32 stage states, directions and running sum;
+// mu (and dJ/dU, written to `lam` at s = 1) in FP64
+struct AdjArgs32 {
+    const float *Y;
+    const float *G;      // g_s (s < 4)
+    const double *mu;    // projected adjoint of U*
+    const float *Lam;
+    float *Gout;         // g_{s-1} (s > 1)
+    float *LamOut;
+    double *lam;         // dJ/dU (s = 1)
+};
+void launch_adj_stage32(int s, const Geo &g, const Coef<float> &co, const float *ia, float dt, float nu,
+                        const AdjArgs32 &a, cudaStream_t st);
 // MHD adjoint stage pieces (nova_adjoint.cu): kind 0 = dF_U/dB (lambda_B += ...),
 // 1 = dF_B/dU (lambda_U += ...), 2 = dF_B/dB with the reverse RK4 recursion;
 // a.Y = the field in the transpose (B^n, Z_S or U^{n+1}), a.G = g_S

@@ -423,7 +423,9 @@ def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_eve
     """Gradient of J by the discrete adjoint.  J = Ek(nsteps); with total_energy
     (MHD) Ek + Em; with window_start = n0 the dissipation over steps n0+1..nsteps,
     E(n0) - E(nsteps) (E = Ek, or Ek + Em for MHD).  Returns (J, dJ/dU0) for
-    Navier-Stokes and (J, dJ/dU0, dJ/dB0) for MHD (rd.model MHD, B0 given)."""
+    Navier-Stokes and (J, dJ/dU0, dJ/dB0) for MHD (rd.model MHD, B0 given).
+    With rd.precision F32SPLIT (Navier-Stokes; U0 a split field) the trajectory is
+    the split path's and the adjoint stages run in FP32; the gradient is FP64."""
     a = AdjDesc()
     a.run = rd
     a.nsteps = int(nsteps)
