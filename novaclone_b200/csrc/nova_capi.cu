@@ -58,6 +58,10 @@ struct nova_ctx {
     double *d_kx2 = nullptr, *d_ky2 = nullptr, *d_kz2 = nullptr;
     cufftHandle plan_f = 0, plan_b = 0;
     bool plans = false;
+    // periodic meshes with N0 = 64 or 256: plan_f/plan_b are batched 2-D (j, k)
+    // transforms and the i direction runs fused with the scale (k_pois_i)
+    bool pois_i = false;
+    double *d_twN = nullptr;  // W_N0^m, m = 0..N0-1 (re, im)
     cufftHandle dct_f = 0, dct_b = 0;  // wall Poisson on the even extension in y
     bool dct_plans = false;
     double *d_ext = nullptr, *d_ky2e = nullptr;
@@ -284,19 +288,37 @@ nova_status ensure_fft(nova_ctx *ctx)
     // the transform runs over the N[1] unique y nodes of poisson::rhs (poisson.cpp:167-181),
     // which with walls are the first N[1] of the N[1]+1 stored rows
     const int ny = ctx->md.N[1];
-    int n[3] = {g.N0, ny, g.N2};
-    int rembed[3] = {g.N0, g.N1, g.N2};
-    int cembed[3] = {g.N0, ny, g.N2 / 2 + 1};
-    const int rdist = g.N0 * g.N1 * g.N2, cdist = g.N0 * ny * (g.N2 / 2 + 1);
-    if ((s = fft_check(ctx, cufftPlanMany(&ctx->plan_f, 3, n, rembed, 1, rdist, cembed, 1, cdist, CUFFT_D2Z, 1),
+    const bool pi = pois_i_fits(g);
+    if (pi) {
+        // W_N0^m = exp(-2 pi i m / N0), rounded from extended precision
+        std::vector<double> tw(2 * (size_t)g.N0);
+        const long double pi_l = 3.141592653589793238462643383279502884L;
+        for (int m = 0; m < g.N0; m++) {
+            const long double a = 2.0L * pi_l * (long double)m / (long double)g.N0;
+            tw[2 * m] = (double)cosl(a);
+            tw[2 * m + 1] = (double)-sinl(a);
+        }
+        if ((s = dalloc(ctx, &ctx->d_twN, tw.size())) != NOVA_OK) return s;
+        CK(cudaMemcpy(ctx->d_twN, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice));
+    }
+    // 3-D transform, or for k_pois_i the (j, k) planes batched over i; both
+    // give the half spectrum [i][j][kz]
+    const int rank = pi ? 2 : 3, batch = pi ? g.N0 : 1;
+    int n3d[3] = {g.N0, ny, g.N2}, n2d[2] = {ny, g.N2};
+    int rembed3[3] = {g.N0, g.N1, g.N2}, rembed2[2] = {g.N1, g.N2};
+    int cembed3[3] = {g.N0, ny, g.N2 / 2 + 1}, cembed2[2] = {ny, g.N2 / 2 + 1};
+    int *n = pi ? n2d : n3d, *rembed = pi ? rembed2 : rembed3, *cembed = pi ? cembed2 : cembed3;
+    const int rdist = (pi ? 1 : g.N0) * g.N1 * g.N2, cdist = (pi ? 1 : g.N0) * ny * (g.N2 / 2 + 1);
+    if ((s = fft_check(ctx, cufftPlanMany(&ctx->plan_f, rank, n, rembed, 1, rdist, cembed, 1, cdist, CUFFT_D2Z, batch),
                        "cufftPlanMany D2Z")) != NOVA_OK)
         return s;
-    if ((s = fft_check(ctx, cufftPlanMany(&ctx->plan_b, 3, n, cembed, 1, cdist, rembed, 1, rdist, CUFFT_Z2D, 1),
+    if ((s = fft_check(ctx, cufftPlanMany(&ctx->plan_b, rank, n, cembed, 1, cdist, rembed, 1, rdist, CUFFT_Z2D, batch),
                        "cufftPlanMany Z2D")) != NOVA_OK) {
         cufftDestroy(ctx->plan_f);
         return s;
     }
     ctx->plans = true;
+    ctx->pois_i = pi;
     const size_t nspec = (size_t)g.N0 * ny * (g.N2 / 2 + 1);
     if ((s = dalloc(ctx, (double **)&ctx->d_spec, 2 * nspec)) != NOVA_OK) return s;
     if ((s = dalloc(ctx, &ctx->d_rhs, (size_t)g.N3)) != NOVA_OK) return s;
@@ -334,10 +356,17 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
                        "cufftExecD2Z")) != NOVA_OK)
         return s;
     const long long nuniq = (long long)ctx->g.N0 * ctx->md.N[1] * ctx->g.N2;
-    launch_scale(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2, 1.0 / (double)nuniq,
-                 ctx->stream);
-    ctx->launches += 1;
-    CKL("k_scale");
+    if (ctx->pois_i) {
+        launch_pois_i(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_twN, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
+                      1.0 / (double)nuniq, ctx->stream);
+        ctx->launches += 1;
+        CKL("k_pois_i");
+    } else {
+        launch_scale(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2, 1.0 / (double)nuniq,
+                     ctx->stream);
+        ctx->launches += 1;
+        CKL("k_scale");
+    }
     if ((s = fft_check(ctx, cufftExecZ2D(ctx->plan_b, (cufftDoubleComplex *)ctx->d_spec, (cufftDoubleReal *)p),
                        "cufftExecZ2D")) != NOVA_OK)
         return s;
@@ -508,7 +537,7 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
     }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2};
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

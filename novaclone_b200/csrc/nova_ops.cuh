@@ -31,6 +31,12 @@ cudaError_t launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const 
 // ny: y extent of the spectrum (the unique y nodes of the transform)
 void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const double *ky2, const double *kz2,
                   double invN3, cudaStream_t st);
+// the i direction of the periodic spectral solve fused with the scale
+// (nova_pois_i.cu): in place on the half spectrum [i][j][kz] of the 2-D
+// (j, k) transforms; twN = W_N0^m, m = 0..N0-1 (interleaved re, im)
+bool pois_i_fits(const Geo &g);
+void launch_pois_i(const Geo &g, int ny, void *spec, const double *twN, const double *kx2, const double *ky2,
+                   const double *kz2, double invN3, cudaStream_t st);
 cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
                            const double *p, double s, const double *Us64, double *U64, const float *Ushi,
                            const float *Uslo, float *hi, float *lo, cudaStream_t st,

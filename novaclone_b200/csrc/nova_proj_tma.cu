@@ -321,11 +321,14 @@ template <typename T> bool encode_rows(ProjMaps &pm, int ms, const T *f, const G
            encode3(&pm.m[ms + M_RB], f, g, kTK, TJ + kH);
 }
 
+// i-chunk: >= ~2 waves of the 2 resident blocks per SM; longer chunks than the
+// stage kernel's carry fewer warm-up planes (whose whole slot is loaded for
+// the queue's component), measured 7% faster than 4 waves at 256^3
 int proj_ichunk(const Geo &g)
 {
     const long long tiles = (long long)(g.N2 / kTK) * (g.N1 / TJ);
     int ch = g.N0;
-    while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * 2 * 4) ch /= 2;
+    while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * 2 * 2) ch /= 2;
     return ch;
 }
 

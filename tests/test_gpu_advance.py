@@ -55,9 +55,11 @@ def check_hist(h_gpu, h_ref, rtol=1e-11, divtol=1e-11):
     assert np.abs(h_gpu[:, 4:6] - h_ref[:, 4:6]).max() < divtol
 
 
-@pytest.mark.parametrize("rk_mode", ["classical", "literal"])
-def test_taylor_green_fp64_vs_oracle(nova, oracle, rk_mode):
-    OM = oracle.Mesh((32, 32, 32))
+@pytest.mark.parametrize("rk_mode,N", [("classical", (32, 32, 32)), ("literal", (32, 32, 32)),
+                                        ("classical", (64, 16, 32))])
+def test_taylor_green_fp64_vs_oracle(nova, oracle, rk_mode, N):
+    """(64, 16, 32): TMA stage kernels and the i-direction solve fused with the scale."""
+    OM = oracle.Mesh(N)
     U0 = oracle.ic_taylor_green(OM)
     dt = oracle.cfl_dt(OM, [U0])
     kw = dict(model="ns", rk_mode=rk_mode, nsteps=20, dt=dt, nu=1 / 1600)

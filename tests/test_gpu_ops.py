@@ -72,7 +72,9 @@ def test_operators_vs_reference_golden(nova, oracle, name):
     assert rel_max(p.download_soa(), ref_p) < TOL
 
 
-@pytest.mark.parametrize("N", [(16, 16, 16), (24, 12, 18), (9, 6, 15)])
+# N0 = 64 and 256 run the i-direction FFT fused with the scale (k_pois_i);
+# N2 = 10 and 18 leave a ragged last group of kz columns
+@pytest.mark.parametrize("N", [(16, 16, 16), (24, 12, 18), (9, 6, 15), (64, 12, 18), (256, 8, 10), (64, 32, 64)])
 def test_poisson_vs_oracle(nova, oracle, N):
     rng = np.random.default_rng(2)
     OM = oracle.Mesh(N)
