@@ -908,8 +908,11 @@ nova_status ensure_work(nova_ctx *ctx, int prec)
 // wall-node overwrites land where the reference calls correctBoundaryConditions:
 // on every refreshed stage state (CLASSICAL: U = Ustar; U.correctBC), on U*
 // before the projection, on p after the solve and on U after the correction.
+// dg: diagnostics of Y as it enters this sweep (the previous step's history
+// row), taken by the first stage kernel where it can (FP64 TMA stage), else
+// by the diagnostics kernel right after that stage, which leaves Y unchanged.
 nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field *Y, const nova_field *X,
-                   nova_field *p, double visc, double divisor, double corr_scale)
+                   nova_field *p, double visc, double divisor, double corr_scale, const StageDiag *dg = nullptr)
 {
     const Geo &g = ctx->g;
     cudaStream_t st = ctx->stream;
@@ -932,10 +935,18 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         nova_status sst = NOVA_OK;
         auto run64 = [&](int stage, const StageArgs64 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
+            const bool first = stage == 0 || stage == 4;
+            bool taken = false;
             const cudaError_t e = launch_stage64(phys, stage, str, g, sw, ctx->co64, ctx->d_ia64, ctx->d_corr64,
-                                                 rd->dt, visc, a, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+                                                 rd->dt, visc, a, st, StageExec{ctx->stage_impl, ctx->d_flag + 1},
+                                                 first ? dg : nullptr, &taken);
             if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
-            ctx->launches += 1;
+            ctx->launches += taken ? 2 : 1;
+            if (first && dg && !taken) {
+                launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, Y->d64, nullptr, nullptr,
+                            nullptr, nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st);
+                ctx->launches += 2;
+            }
         };
         if (lit) {
             run64(4, StageArgs64{Y->d64, X ? X->d64 : nullptr, nullptr, nullptr, ctx->w64[1]});
@@ -993,6 +1004,11 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             }
         };
         fixpair(Y->hi, Y->lo);
+        if (dg) {
+            launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, nullptr, Y->hi, Y->lo, nullptr,
+                        nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st);
+            ctx->launches += 2;
+        }
         const float *Ushi, *Uslo;
         nova_status sst = NOVA_OK;
         auto run32 = [&](int stage, const StageArgs32 &a) {
@@ -1087,9 +1103,20 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
         CK(cudaMemsetAsync(ctx->d_hist, 0, sizeof(double) * nsteps * NOVA_HIST_COLS, ctx->stream));
     }
     CK(cudaMemsetAsync(ctx->d_flag, 0, 2 * sizeof(int), ctx->stream));
+    // FP64 Navier-Stokes on a uniform periodic mesh: the history row of a step
+    // is taken by the first stage kernel of the next step, which reads the same
+    // state with its halos and forms its divergence anyway (the last step's row
+    // by the diagnostics kernel)
+    const bool defer_diag = hist && rd->diag_every > 0 && !mhd && rd->precision == NOVA_F64 && !ctx->g.wallY &&
+                            !ctx->md.hyperbolic_z && ctx->h == 3 && ctx->stage_impl != STAGE_MARCH &&
+                            stage_tma_fits(ctx->g, true);
+    StageDiag pend{};
+    bool have = false;
     for (int n = 0; n < nsteps; n++) {
         // app/TG_Piosson/RKLoop.H (NS) or app/OT_Poisson/UEqn.H then BEqn.H (MHD)
-        s = evolve(ctx, rd, mhd ? PHYS_MHD_U : PHYS_NS, st->U, mhd ? st->B : nullptr, st->p, rd->nu, rd->dt, rd->dt);
+        s = evolve(ctx, rd, mhd ? PHYS_MHD_U : PHYS_NS, st->U, mhd ? st->B : nullptr, st->p, rd->nu, rd->dt, rd->dt,
+                   have ? &pend : nullptr);
+        have = false;
         if (s != NOVA_OK) return s;
         if (mhd) {
             // B loop is always the refreshed RK4 (BEqn.H:86-87); B cleaning has no 1/dt (BEqn.H:91-94)
@@ -1098,7 +1125,12 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
             s = evolve(ctx, &rb, PHYS_MHD_B, st->B, st->U, st->pB, rd->eta, 1.0, 1.0);
             if (s != NOVA_OK) return s;
         }
-        if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps)) {
+        if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps) && defer_diag &&
+            n + 1 < nsteps) {
+            pend = StageDiag{ctx->d_part, diag_blocks(ctx->g), ctx->d_hist + (long long)n * NOVA_HIST_COLS,
+                             ctx->d_flag, (double)(n + 1), rd->t0 + (n + 1) * rd->dt, 1.0 / (double)ctx->g.N3};
+            have = true;
+        } else if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps)) {
             ProfScope ps(ctx, NOVA_K_DIAG);
             const nova_field *U = st->U, *B = mhd ? st->B : nullptr;
             launch_diag(ctx->h, ctx->g, walls_of<double>(ctx, U, B), ctx->co64, ctx->d_ia64, U->d64, U->hi, U->lo,

@@ -208,9 +208,20 @@ struct StageExec {
     int *err;
 };
 bool stage_tma_fits(const Geo &g, bool fp64);
+// diagnostics of a stage's input state taken by the stage itself (FP64 TMA
+// stage 0 or literal stage 4, uniform periodic mesh): per-block partials into
+// part (room for cap blocks), then the history row (k_diag_final)
+struct StageDiag {
+    double *part;
+    int cap;
+    double *row;
+    int *flag;
+    double step, time, invN3;
+};
 cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
                                const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
-                               cudaStream_t st);
+                               cudaStream_t st, const StageDiag *dg = nullptr,
+                               bool *dg_done = nullptr);
 cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
                                const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
                                cudaStream_t st);
@@ -222,7 +233,8 @@ cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef
 // fit, cudaErrorInvalidValue when a tensor map cannot be encoded.
 cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl,
                            const Coef<double> &co, const double *ia, const double *corr2, double dt, double visc,
-                           const StageArgs64 &a, cudaStream_t st, const StageExec &ex);
+                           const StageArgs64 &a, cudaStream_t st, const StageExec &ex, const StageDiag *dg = nullptr,
+                           bool *dg_done = nullptr);
 cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, const Walls<float> &wl,
                            const Coef<float> &co, const float *ia, const float *corr2, float dt, float visc,
                            const StageArgs32 &a, cudaStream_t st, const StageExec &ex);

@@ -814,6 +814,12 @@ void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double
                                     row, flag);
 }
 
+void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
+                       cudaStream_t st)
+{
+    k_diag_final<<<1, 256, 0, st>>>(part, nb, invN3, step, time, row, flag);
+}
+
 void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st)
 {
     const int nb = diag_blocks(g);

@@ -48,6 +48,9 @@ cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const doubl
                                const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi,
                                float *lo, int *err, cudaStream_t st);
 int diag_blocks(const Geo &g);
+// the history row from nb blocks of partials (Ek, Em, max|div U|, max|div B| per block)
+void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
+                       cudaStream_t st);
 void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                  const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
                  const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,

@@ -122,10 +122,10 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
                     if constexpr (kE1) e1[c] = e1p[o];
                 }
             }
-            T rhs[3];
+            T rhs[3], divu;
             if constexpr (PHYS == PHYS_NS) {
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
-                ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+                ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs, divu);
             } else if constexpr (PHYS == PHYS_MHD_U) {
                 // comps 0-2: U (stage state), 3-5: B (frozen)
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
@@ -253,10 +253,11 @@ void launch_stage_any(int phys, int stage, bool stretch, const Geo &g, const Wal
 
 cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, const Walls<double> &wl,
                            const Coef<double> &co, const double *ia, const double *corr2, double dt, double visc,
-                           const StageArgs64 &a, cudaStream_t st, const StageExec &ex)
+                           const StageArgs64 &a, cudaStream_t st, const StageExec &ex, const StageDiag *dg,
+                           bool *dg_done)
 {
     if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g, true))
-        return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
+        return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st, dg, dg_done);
     if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
     launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;

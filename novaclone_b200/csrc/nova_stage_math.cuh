@@ -47,6 +47,7 @@ __device__ __forceinline__ void ns_dir(const V &v, int d, T v0, const T *ha, con
 }
 
 // vx/vy/vz(c, s): component c at offset s along i, j, k; u0 = U at the node;
+// divu receives sum_d D_d U_d at the node (the divergence of the stage state);
 // iak = 1/dzdxi(k): the z weights are a_l iak and b_l iak^2, applied as the
 // uniform weights with vb = visc iak b_l and the z sum scaled by iak (it is
 // evaluated first), so no per-node weight tables live in registers.
@@ -54,7 +55,7 @@ __device__ __forceinline__ void ns_dir(const V &v, int d, T v0, const T *ha, con
 // term-by-term order at the level of a few ulps of the largest term.
 template <typename T, int H, bool STRETCH, class VX, class VY, class VZ>
 __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&u0)[3], const Coef<T> &co,
-                                       const StageCoef<T> &sc, T iak, T c2k, T visc, T (&rhs)[3])
+                                       const StageCoef<T> &sc, T iak, T c2k, T visc, T (&rhs)[3], T &divu)
 {
     T s[3] = {0, 0, 0}, dv = 0;
     {
@@ -73,6 +74,7 @@ __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz,
         for (int l = 0; l < H; l++) vb[l] = sc.vb[1][l];
         ns_dir<T, H>(vy, 1, u0[1], sc.ha[1], co.a[1], vb, s, dv);
     }
+    divu = dv;
     const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * (iak * iak);
     const T K = fma(T(-0.5), dv, -visc * bsum);
 #pragma unroll

@@ -26,6 +26,7 @@
 // the error word and the block leaves its pipeline, the producer after waiting,
 // again bounded, for the loads it still has in flight.
 #include "nova_internal.cuh"
+#include "nova_ops.cuh"
 #include "nova_stage_math.cuh"
 #include "nova_tile.cuh"
 #include "nova_tma.cuh"
@@ -74,11 +75,13 @@ template <typename T, int STAGE> __host__ __device__ constexpr int epi_fields()
         return (STAGE == 1 || STAGE == 2) ? 2 : (STAGE == 3 ? 3 : (STAGE == 4 ? 1 : 0));
 }
 
+// ring data, the ring barriers, then 2 doubles per consumer warp for the
+// diagnostics reduction (DIAG launches)
 template <typename T, int NE> constexpr size_t tma_smem_bytes()
 {
     using C = TmaCfg<T>;
     return ((size_t)C::kRing * C::kSlotE + (size_t)C::kERing * NE * C::kEpiE) * sizeof(T) +
-           8 * (2 * C::kRing + 2 * C::kERing);
+           8 * (2 * C::kRing + 2 * C::kERing) + 16 * C::kWarps;
 }
 
 struct StageMaps {
@@ -106,11 +109,16 @@ __device__ __forceinline__ void epi_read(const T *se, int c, T &e0, T &e1, T &lo
     }
 }
 
-template <typename T, int STAGE, bool STRETCH, class Args>
+// DIAG (FP64, stages that read U itself: 0 and the literal 4): the block also
+// sums 1/2 |U|^2 and takes max |div U| over its nodes, the divergence being the
+// one the stage arithmetic forms anyway, and writes them to dpart[block * 4]
+// (the layout of the diagnostics partials: Ek, Em = 0, max|div U|, max|div B| = 0)
+template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG>
 __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     k_stage_tma(Geo g, Coef<T> co, StageCoef<T> sc, const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
-                T visc, Args args, const __grid_constant__ StageMaps maps, int ichunk, int *err)
+                T visc, Args args, const __grid_constant__ StageMaps maps, int ichunk, int *err, double *dpart)
 {
+    static_assert(!DIAG || (sizeof(T) == 8 && (STAGE == 0 || STAGE == 4)), "diagnostics of an FP64 state only");
     using C = TmaCfg<T>;
     constexpr int H = kH, TJ = C::TJ, kRing = C::kRing, kERing = C::kERing;
     constexpr int kTcbE = C::kTcbE, kLRE = C::kLRE, kSlotE = C::kSlotE, kEpiE = C::kEpiE;
@@ -225,6 +233,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     // centre H) of step p is q[(p + s) % 7]; the loop is unrolled by 7
     // (= 2H + 1 = kRing) so that the rotation is register renaming and every
     // ring slot index is a compile-time constant of the unrolled step.
+    double ek = 0.0, mdu = 0.0;  // DIAG
     if constexpr (sizeof(T) == 8) {
         T q[2 * H + 1][3];
         bool ok = true;
@@ -264,8 +273,12 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             auto vy = [&](int c, int s) -> T { return sl[cen + s * kRowE + c * kTK]; };
             auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
             const T u0[3] = {q[H][0], q[H][1], q[H][2]};
-            T rhs[3];
-            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+            T rhs[3], divu;
+            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs, divu);
+            if constexpr (DIAG) {
+                ek += 0.5 * (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]);
+                mdu = fmax(mdu, fabs(divu));
+            }
 
             T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
             if constexpr (NE > 0) {
@@ -327,8 +340,8 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
             constexpr int kC = (R + H) % (2 * H + 1);
             const T u0[3] = {q[kC][0], q[kC][1], q[kC][2]};
-            T rhs[3];
-            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+            T rhs[3], divu;
+            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs, divu);
 
             T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
             if constexpr (NE > 0) {
@@ -371,6 +384,32 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
         }
     }
 
+    if constexpr (DIAG) {
+        // consumer warps only (the producer has returned): fixed-order sums
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ek += __shfl_down_sync(0xffffffffu, ek, o);
+            mdu = fmax(mdu, __shfl_down_sync(0xffffffffu, mdu, o));
+        }
+        double *red = reinterpret_cast<double *>(smraw + (bar0 - s0) + 8 * (2 * kRing + 2 * kERing));
+        if (lane == 0) {
+            red[2 * ty] = ek;
+            red[2 * ty + 1] = mdu;
+        }
+        asm volatile("bar.sync 1, %0;" ::"n"(C::kWarps * 32) : "memory");
+        if (ty == 0 && lane == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < C::kWarps; w++) {
+                a += red[2 * w];
+                b = fmax(b, red[2 * w + 1]);
+            }
+            const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            dpart[blk * 4 + 0] = a;
+            dpart[blk * 4 + 1] = 0.0;
+            dpart[blk * 4 + 2] = b;
+            dpart[blk * 4 + 3] = 0.0;
+        }
+    }
 }
 
 // ------------------------------------------------------------------ host --
@@ -430,9 +469,9 @@ template <typename T> int tma_ichunk(const Geo &g)
     return ch;
 }
 
-template <typename T, int STAGE, bool STRETCH, class Args>
+template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG = false>
 cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc, const Args &a,
-                       const T *Y, const T *const *ef, int *err, cudaStream_t st)
+                       const T *Y, const T *const *ef, int *err, cudaStream_t st, double *dpart = nullptr)
 {
     constexpr int NE = epi_fields<T, STAGE>();
     StageMaps maps;
@@ -443,7 +482,7 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, Cf::TJ);
     if (!ok) return cudaErrorInvalidValue;
     constexpr size_t smem = tma_smem_bytes<T, NE>();
-    auto kern = k_stage_tma<T, STAGE, STRETCH, Args>;
+    auto kern = k_stage_tma<T, STAGE, STRETCH, Args, DIAG>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -452,7 +491,8 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     }
     const int ch = tma_ichunk<T>(g);
     const dim3 grid(g.N2 / kTK, g.N1 / Cf::TJ, (g.N0 + ch - 1) / ch);
-    kern<<<grid, dim3(kTK, Cf::TJ + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err);
+    kern<<<grid, dim3(kTK, Cf::TJ + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err,
+                                                     dpart);
     return cudaSuccess;
 }
 
@@ -482,7 +522,7 @@ bool stage_tma_fits(const Geo &g, bool fp64)
 
 cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
                                const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
-                               cudaStream_t st)
+                               cudaStream_t st, const StageDiag *dg, bool *dg_done)
 {
     const double *ef[3] = {nullptr, nullptr, nullptr};
     if (stage == 1 || stage == 2) {
@@ -490,6 +530,22 @@ cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef
         ef[1] = a.A;
     } else if (stage == 3) {
         ef[0] = a.A;
+    }
+    if (dg && !stretch && (stage == 0 || stage == 4)) {
+        using Cf = TmaCfg<double>;
+        const int ch = tma_ichunk<double>(g);
+        const long long nb = (long long)(g.N2 / kTK) * (g.N1 / Cf::TJ) * ((g.N0 + ch - 1) / ch);
+        if (nb <= dg->cap) {
+            const cudaError_t e =
+                stage == 0 ? launch_tma<double, 0, false, StageArgs64, true>(g, co, ia, corr2, dt, visc, a, a.Y, ef,
+                                                                             err, st, dg->part)
+                           : launch_tma<double, 4, false, StageArgs64, true>(g, co, ia, corr2, dt, visc, a, a.Y, ef,
+                                                                             err, st, dg->part);
+            if (e != cudaSuccess) return e;
+            launch_diag_final(dg->part, (int)nb, dg->invN3, dg->step, dg->time, dg->row, dg->flag, st);
+            if (dg_done) *dg_done = true;
+            return cudaSuccess;
+        }
     }
     return stretch ? launch_tma_stage<double, true>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st)
                    : launch_tma_stage<double, false>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st);

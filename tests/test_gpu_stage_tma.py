@@ -105,3 +105,24 @@ def test_forcing_tma_on_a_mesh_it_does_not_fit_is_refused(nova):
     with pytest.raises(nova.NovaError) as e:
         nova.advance(GM, nova.run_desc(model="ns", dt=1e-3), U, p, nsteps=1)
     assert e.value.status == nova.E_UNSUPPORTED
+
+
+@pytest.mark.parametrize("rk_mode", ["classical", "literal"])
+def test_history_rows_from_the_stage_kernel(nova, rk_mode):
+    """FP64 TMA runs take each step's history row (Ek, max|div U|) inside the next
+    step's first stage kernel, the march runs from the diagnostics kernel: same
+    state, same divergence up to the order of the sums."""
+    N = (40, 32, 64)
+    U0 = 0.3 * np.random.default_rng(11).standard_normal((3,) + N)
+    hist = {}
+    for impl in ("tma", "march"):
+        GM = mesh_with(nova, impl, N)
+        U = nova.Field(GM, 3).upload_soa(U0)
+        rd = nova.run_desc(model="ns", rk_mode=rk_mode, dt=2e-3, nu=0.01, diag_every=2)
+        hist[impl] = nova.advance(GM, rd, U, nova.Field(GM, 1), nsteps=7)
+    a, b = hist["tma"], hist["march"]
+    assert np.array_equal(a[:, :2], b[:, :2])  # step, time; zero rows where no diagnostics were due
+    assert np.array_equal(a[:, 3], b[:, 3]) and np.array_equal(a[:, 5], b[:, 5])
+    assert np.all(a[[1, 3, 5, 6], 2] > 0)
+    np.testing.assert_allclose(a[:, 2], b[:, 2], rtol=1e-13)
+    np.testing.assert_allclose(a[:, 4], b[:, 4], rtol=1e-12, atol=1e-14)
