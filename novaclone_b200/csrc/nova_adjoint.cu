@@ -1,24 +1,9 @@
 // Discrete adjoint of the Navier-Stokes stage: xi = dt * J_F(Y)^T g, fused
-// with the reverse recursion of the classical RK4 stage loop.
-//
-// Forward right-hand side (app/TG_Piosson/RKLoop.H:17-22):
-//   F(U)_c = -N(U)_c + nu L U_c,
-//   N(U)_c = 1/2 sum_d [ D_d(U_d U_c) + U_d D_d U_c + U_c D_d U_d ]   (src/ex/div/div.hxx:84-172)
-// With periodic central differences D_d^T = -D_d and L^T = L, so for an
-// adjoint direction g the transpose of the linearisation N'(Y) is
-//   (N'(Y)^T g)_e = 1/2 [ - sum_c Y_c D_e g_c + sum_c g_c D_e Y_c - D_e(sum_c Y_c g_c)
-//                         - sum_d ( Y_d D_d g_e + D_d(Y_d g_e) ) + g_e sum_d D_d Y_d ]
-// and Y_d D_d g_e + D_d(Y_d g_e) is the A_d(Y,g)_e form of the forward kernel.
-// The z metric enters as in the forward operator; on a uniform mesh it is a
-// constant 1 up to round-off, which keeps the transpose exact to ~1e-14.
-//
-// Reverse RK4 (forward stages k_s = dt F(Y_s), Y1 = U, Y2 = U + k1/2,
-// Y3 = U + k2/2, Y4 = U + k3, U* = U + (k1 + 2k2 + 2k3 + k4)/6), given
-// mu = dJ/dU*:
-//   s=4: g4 = mu/6        xi4 -> g3 = mu/3 + xi4        Lam = xi4
-//   s=3:                  xi3 -> g2 = mu/3 + xi3/2      Lam += xi3
-//   s=2:                  xi2 -> g1 = mu/6 + xi2/2      Lam += xi2
-//   s=1:                  xi1 -> dJ/dU = mu + Lam + xi1
+// with the reverse recursion of the classical RK4 stage loop (the point
+// arithmetic and the recursion are in nova_adj_math.cuh); tiled march, used
+// where the TMA pipeline of nova_adj_tma.cu does not fit the mesh and for the
+// FP32-split adjoint.  The MHD coupling transposes follow below.
+#include "nova_adj_math.cuh"
 #include "nova_internal.cuh"
 #include "nova_tile.cuh"
 
@@ -38,14 +23,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
     const int ib = blockIdx.z * ichunk;
     const int ie = min(ib + ichunk, g.N0);
     const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
-    const T iak = ia[kw];
-    T az[H], bz[H];
-#pragma unroll
-    for (int l = 0; l < H; l++) {
-        az[l] = co.a[2][l] * iak;
-        bz[l] = co.b[2][l] * iak * iak;
-    }
-    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
+    T az[H], bz[H], bsum;
+    adj_zweights<T, H>(co, ia[kw], az, bz, bsum);
     // comps 0-2: forward stage state Y, 3-5: adjoint stage direction g (= mu/6 at s=4)
     auto ld = [&](int c, long long o) -> T {
         if (c < 3) return a.Y[(long long)c * g.N3 + o];
@@ -56,7 +35,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
     tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
                                                   const auto &vz) {
         double mu[3];
-        T lam[3];
+        T lam[3] = {0, 0, 0};
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             mu[c] = a.mu[(long long)c * g.N3 + idx];
@@ -64,49 +43,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
         }
         const T y0[3] = {q[H][0], q[H][1], q[H][2]};
         const T g0[3] = {q[H][3], q[H][4], q[H][5]};
-        T At[3] = {0, 0, 0};   // the e = d terms
-        T Bt[3] = {0, 0, 0};   // - sum_d A_d(Y,g)_e
-        T lap[3] = {0, 0, 0};
-        T divY = 0;
-        auto dir = [&](const auto &v, int d, const T *aa, const T *bb) {
-            T dY[3], dG[3];
+        T xi[3];
+        adj_xi<T, H>(vx, vy, vz, y0, g0, co, az, bz, nu, dt, bsum, xi);
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                dY[c] = d1<T, H>(v, c, aa);
-                dG[c] = d1<T, H>(v, 3 + c, aa);
-                Bt[c] -= adv1<T, H>(v, 3 + c, d, y0[d], aa);
-                lap[c] += lsum<T, H>(v, 3 + c, bb);
-            }
-            divY += dY[d];
-            // D_d(sum_c Y_c g_c)
-            auto sdot = [&](int, int s) -> T { return v(0, s) * v(3, s) + v(1, s) * v(4, s) + v(2, s) * v(5, s); };
-            const T ds = d1<T, H>(sdot, 0, aa);
-            At[d] = -(y0[0] * dG[0] + y0[1] * dG[1] + y0[2] * dG[2]) + (g0[0] * dY[0] + g0[1] * dY[1] + g0[2] * dY[2])
-                    - ds;
-        };
-        dir(vx, 0, co.a[0], co.b[0]);
-        dir(vy, 1, co.a[1], co.b[1]);
-        dir(vz, 2, az, bz);
-#pragma unroll
-        for (int e = 0; e < 3; e++) {
-            const T ntg = T(0.5) * (At[e] + fma(g0[e], divY, Bt[e]));
-            const T xi = dt * (-ntg + nu * fma(-bsum, g0[e], lap[e]));
-            const long long o = (long long)e * g.N3 + idx;
-            if constexpr (S == 4) {
-                a.Gout[o] = (T)(mu[e] * (1.0 / 3.0)) + xi;
-                a.LamOut[o] = xi;
-            } else if constexpr (S == 3) {
-                a.Gout[o] = (T)(mu[e] * (1.0 / 3.0)) + T(0.5) * xi;
-                a.LamOut[o] = lam[e] + xi;
-            } else if constexpr (S == 2) {
-                a.Gout[o] = (T)(mu[e] * (1.0 / 6.0)) + T(0.5) * xi;
-                a.LamOut[o] = lam[e] + xi;
-            } else if constexpr (sizeof(T) == 8) {
-                a.Gout[o] = mu[e] + (lam[e] + xi);
-            } else {
-                a.lam[o] = mu[e] + (double)(lam[e] + xi);
-            }
-        }
+        for (int e = 0; e < 3; e++) adj_store<T, S>(a, (long long)e * g.N3 + idx, mu[e], lam[e], xi[e]);
     });
 }
 
@@ -272,10 +212,12 @@ void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t
     k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, x, y);
 }
 
-void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
-                        const AdjArgs &a, cudaStream_t st)
+cudaError_t launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
+                               const AdjArgs &a, cudaStream_t st, int *err)
 {
+    if (err && adj_tma_fits(g)) return launch_adj_tma64(s, g, co, ia, dt, nu, a, err, st);
     launch_adj<double>(s, g, co, ia, dt, nu, a, st);
+    return cudaSuccess;
 }
 
 void launch_adj_stage32(int s, const Geo &g, const Coef<float> &co, const float *ia, float dt, float nu,

@@ -1381,6 +1381,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     CKL("adjoint seed");
 
     // reverse sweep, segment by segment
+    cudaError_t aerr = cudaSuccess;
     for (int c = nck - 1; c >= 0; c--) {
         const int n0 = c * K;
         const int m = (N - n0) < K ? (N - n0) : K;
@@ -1401,7 +1402,9 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
             const double dt = rd->dt, nu = rd->nu;
             auto adj = [&](int stage, const AdjArgs &a) {
                 ProfScope ps(ctx, NOVA_K_ADJ);
-                launch_adj_stage64(stage, ctx->g, ctx->co64, ctx->d_ia64, dt, nu, a, st);
+                const cudaError_t e = launch_adj_stage64(stage, ctx->g, ctx->co64, ctx->d_ia64, dt, nu, a, st,
+                                                         ctx->stage_impl != STAGE_MARCH ? ctx->d_flag + 1 : nullptr);
+                if (e != cudaSuccess && aerr == cudaSuccess) aerr = e;
                 ctx->launches += 1;
             };
             adj(4, AdjArgs{Y4(t), mu, mu, nullptr, gA, Lam});
@@ -1415,6 +1418,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
             }
         }
     }
+    if (aerr != cudaSuccess) return stage_fail(ctx, aerr);
     CK(cudaMemcpyAsync(gradU->d64, lam, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
     int perr = 0;
     CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1534,9 +1538,12 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
     CKL("adjoint seed");
 
     const double dt = rd->dt;
+    cudaError_t aerr = cudaSuccess;
     auto adj_u = [&](int stage, const AdjArgs &a) {
         ProfScope ps(ctx, NOVA_K_ADJ);
-        launch_adj_stage64(stage, ctx->g, ctx->co64, ctx->d_ia64, dt, rd->nu, a, st);
+        const cudaError_t e = launch_adj_stage64(stage, ctx->g, ctx->co64, ctx->d_ia64, dt, rd->nu, a, st,
+                                                 ctx->stage_impl != STAGE_MARCH ? ctx->d_flag + 1 : nullptr);
+        if (e != cudaSuccess && aerr == cudaSuccess) aerr = e;
         ctx->launches += 1;
     };
     auto adj_mhd = [&](int kind, int stage, const AdjArgs &a, double *acc) {
@@ -1588,6 +1595,7 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
             }
         }
     }
+    if (aerr != cudaSuccess) return stage_fail(ctx, aerr);
     CK(copy(gradU->d64, lamU));
     CK(copy(gradB->d64, lamB));
     int perr = 0;

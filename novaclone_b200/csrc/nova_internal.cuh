@@ -7,6 +7,7 @@
 // index wrapping (src/BC/periodicBC.hxx:1-66 becomes address arithmetic).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -172,8 +173,13 @@ struct AdjArgs {
     double *Gout;       // g_{s-1}, or dJ/dU at s = 1
     double *LamOut;     // updated running sum (s > 1)
 };
-void launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
-                        const AdjArgs &a, cudaStream_t st);
+// err: the pipeline error word; with it, meshes that fit the TMA adjoint
+// (nova_adj_tma.cu: periodic, N2 % 32 == 0, N1 a multiple of 8 and >= 16) run it
+cudaError_t launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
+                               const AdjArgs &a, cudaStream_t st, int *err = nullptr);
+bool adj_tma_fits(const Geo &g);
+cudaError_t launch_adj_tma64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
+                             const AdjArgs &a, int *err, cudaStream_t st);
 // FP32-split adjoint stage: FP32 stage states, directions and running sum;
 // mu (and dJ/dU, written to `lam` at s = 1) in FP64
 struct AdjArgs32 {
@@ -208,6 +214,10 @@ struct StageExec {
     int *err;
 };
 bool stage_tma_fits(const Geo &g, bool fp64);
+// tensor map of a 3-component FP64 field [c][i][j][k] (nova_stage_tma.cu):
+// rows > 0: box kTK(k) x 3(c) x rows(j) x 1(i), landing [row][c][k];
+// rows = 0: the 4-wide k-halo box 4(k) x 8(j) x 3(c) x 1(i), landing [c][j][k]
+bool tma_encode_field(CUtensorMap *m, const double *base, const Geo &g, unsigned rows);
 // diagnostics of a stage's input state taken by the stage itself (FP64 TMA
 // stage 0 or literal stage 4, uniform periodic mesh): per-block partials into
 // part (room for cap blocks), then the history row (k_diag_final)

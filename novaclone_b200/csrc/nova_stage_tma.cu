@@ -511,6 +511,11 @@ cudaError_t launch_tma_stage(int stage, const Geo &g, const Coef<T> &co, const T
 
 }  // namespace
 
+bool tma_encode_field(CUtensorMap *m, const double *base, const Geo &g, unsigned rows)
+{
+    return encode<double>(m, base, g, rows);
+}
+
 bool stage_tma_fits(const Geo &g, bool fp64)
 {
     // tile width divides N2 (k halo boxes start at a wrapped column), tile

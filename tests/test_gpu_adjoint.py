@@ -50,8 +50,9 @@ def base_state(oracle, N, seed=0):
     return U0, oracle.cfl_dt(OM, [U0])
 
 
-def test_adjoint_gradient_matches_central_differences(nova, oracle):
-    N = (24, 24, 24)
+@pytest.mark.parametrize("N", [(24, 24, 24), (16, 16, 32)])
+def test_adjoint_gradient_matches_central_differences(nova, oracle, N):
+    """(16, 16, 32) runs the TMA-fed adjoint stage, (24, 24, 24) the tiled one."""
     nsteps, nu = 12, 1e-2
     U0, dt = base_state(oracle, N)
     GM = nova.Mesh(N)
@@ -286,3 +287,41 @@ def test_split_adjoint_checkpoint_interval_and_window(nova, oracle):
     J64, w64 = nova.adjoint_grad(GM, rd64, U64, nsteps, checkpoint_every=3, window_start=n0)
     assert J32 == pytest.approx(J64, rel=1e-5)
     assert rel_l2(w32.download_soa(), w64.download_soa()) < SPLIT_TOL
+
+
+@pytest.mark.parametrize("N,model", [((16, 16, 32), "ns"), ((12, 24, 64), "ns"), ((16, 16, 32), "mhd")])
+def test_tma_adjoint_equals_tiled(nova, oracle, N, model):
+    """The TMA-fed adjoint stage (meshes with N2 % 32 == 0, N1 % 8 == 0, N1 >= 16)
+    against the tiled one (NOVA_STAGE_IMPL=march): the same arithmetic up to the
+    place of the 1/6 of the first reverse stage."""
+    import os
+    rng = np.random.default_rng(21)
+    U0 = 0.5 * smooth_direction(rng, N)
+    B0 = 0.5 * smooth_direction(rng, N)
+    OM = oracle.Mesh(N)
+    dt = oracle.cfl_dt(OM, [U0, B0])
+    grads = {}
+    for impl in ("auto", "march"):  # auto: the TMA adjoint wherever the mesh fits it
+        old = os.environ.get("NOVA_STAGE_IMPL")
+        if impl == "auto":
+            os.environ.pop("NOVA_STAGE_IMPL", None)
+        else:
+            os.environ["NOVA_STAGE_IMPL"] = impl
+        try:
+            GM = nova.Mesh(N)
+        finally:
+            if old is None:
+                os.environ.pop("NOVA_STAGE_IMPL", None)
+            else:
+                os.environ["NOVA_STAGE_IMPL"] = old
+        U = nova.Field(GM, 3).upload_soa(U0)
+        rd = nova.run_desc(model=model, rk_mode="classical", dt=dt, nu=1e-2, eta=1e-2)
+        if model == "mhd":
+            B = nova.Field(GM, 3).upload_soa(B0)
+            r = nova.adjoint_grad(GM, rd, U, 5, checkpoint_every=2, B0=B, total_energy=True)
+            grads[impl] = [r[1].download_soa(), r[2].download_soa()]
+        else:
+            r = nova.adjoint_grad(GM, rd, U, 5, checkpoint_every=2)
+            grads[impl] = [r[1].download_soa()]
+    for a, b in zip(grads["auto"], grads["march"]):
+        assert rel_l2(a, b) < 1e-13, rel_l2(a, b)

@@ -87,6 +87,9 @@ def test_tma_taylor_green_vs_oracle(nova, oracle):
 
 
 def test_adjoint_through_tma_equals_march(nova):
+    """The forward passes agree bit for bit (J); the reverse stages of the TMA
+    adjoint apply the first stage's 1/6 to xi instead of to g, so the gradients
+    agree to rounding."""
     N = (16, 32, 32)
     U0 = 0.2 * np.random.default_rng(9).standard_normal((3,) + N)
     out = []
@@ -95,7 +98,8 @@ def test_adjoint_through_tma_equals_march(nova):
         J, grad = nova.adjoint_grad(GM, nova.run_desc(model="ns", dt=2e-3, nu=0.01), nova.Field(GM, 3).upload_soa(U0),
                                     nsteps=4, checkpoint_every=2)
         out.append((J, grad.download_soa()))
-    assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+    assert out[0][0] == out[1][0]
+    assert rel_l2(out[0][1], out[1][1]) < 1e-13
 
 
 def test_forcing_tma_on_a_mesh_it_does_not_fit_is_refused(nova):
