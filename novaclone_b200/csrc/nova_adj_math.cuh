@@ -21,15 +21,27 @@
 
 namespace nova {
 
-// vx/vy/vz(c, s): component c (0-2: Y, 3-5: g) at offset s along i, j, k;
-// az, bz: the z weights a_l / dzdxi, b_l / dzdxi^2; bsum: the centre weight of
-// the three second differences
-template <typename T, int H, class VX, class VY, class VZ>
-__device__ __forceinline__ void adj_xi(const VX &vx, const VY &vy, const VZ &vz, const T (&y0)[3], const T (&g0)[3],
-                                       const Coef<T> &co, const T *az, const T *bz, T nu, T dt, T bsum, T (&xi)[3])
+// adjoint stage kinds: the MHD coupling transposes (numbered as launch_adj_mhd's
+// kind) and the Navier-Stokes stage
+enum AdjKind { ADJ_UB = 0, ADJ_BU = 1, ADJ_BB = 2, ADJ_NS = 3 };
+
+// Building blocks at one node for a field P (comps 0-2 of vx/vy/vz, the
+// forward stage state Y of the Navier-Stokes stage) and a direction g (comps
+// 3-5), each vx/vy/vz(c, s) the component c at offset s along i, j, k:
+//   Sx_e   = sum_d sum_l [ g_e(+l) V+_l + g_e(-l) V-_l ],  V+-_l = +-(a_l/2)(P_d(+-l) + P_d(0)) + nu b_l
+//            (1/2 sum_d A_d(P, g)_e + nu lap(g)_e without its centre term)
+//   At_d   = -sum_c P_c D_d g_c + sum_c g_c D_d P_c - D_d(P.g)
+//   divP   = sum_d D_d P_d,  divG = sum_d D_d g_d (with DIVG)
+// az, bz: the z weights a_l / dzdxi, b_l / dzdxi^2
+template <typename T, int H, bool DIVG, class VX, class VY, class VZ>
+__device__ __forceinline__ void adj_terms(const VX &vx, const VY &vy, const VZ &vz, const T (&p0)[3], const T (&g0)[3],
+                                          const Coef<T> &co, const T *az, const T *bz, T nu, T (&Sx)[3], T (&At)[3],
+                                          T &divP, T &divG)
 {
-    T Sx[3] = {0, 0, 0}, At[3] = {0, 0, 0};
-    T divY = 0;
+    divP = 0;
+    divG = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) Sx[c] = 0;
     auto dir = [&](const auto &v, int d, const T *aa, const T *bb) {
         T vp[H], vm[H];
         T at = 0;
@@ -37,15 +49,16 @@ __device__ __forceinline__ void adj_xi(const VX &vx, const VY &vy, const VZ &vz,
         for (int l = 0; l < H; l++) {
             const T p = v(d, l + 1), m = v(d, -l - 1);
             const T ha = T(0.5) * aa[l], nb = nu * bb[l];
-            vp[l] = fma(ha, y0[d] + p, nb);
-            vm[l] = fma(-ha, y0[d] + m, nb);
-            divY = fma(aa[l], p - m, divY);
+            vp[l] = fma(ha, p0[d] + p, nb);
+            vm[l] = fma(-ha, p0[d] + m, nb);
+            divP = fma(aa[l], p - m, divP);
+            if (DIVG) divG = fma(aa[l], v(3 + d, l + 1) - v(3 + d, -l - 1), divG);
             T t = 0;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const T yp = v(c, l + 1), ym = v(c, -l - 1), gp = v(3 + c, l + 1), gm = v(3 + c, -l - 1);
-                t = fma(-gp, y0[c] + yp, t);
-                t = fma(gm, y0[c] + ym, t);
+                t = fma(-gp, p0[c] + yp, t);
+                t = fma(gm, p0[c] + ym, t);
                 t = fma(g0[c], yp - ym, t);
             }
             at = fma(aa[l], t, at);
@@ -65,6 +78,15 @@ __device__ __forceinline__ void adj_xi(const VX &vx, const VY &vy, const VZ &vz,
     dir(vx, 0, co.a[0], co.b[0]);
     dir(vy, 1, co.a[1], co.b[1]);
     dir(vz, 2, az, bz);
+}
+
+// the Navier-Stokes stage: xi = dt [ Sx - 1/2 At - 1/2 g divY - nu bsum g ] (P = Y)
+template <typename T, int H, class VX, class VY, class VZ>
+__device__ __forceinline__ void adj_xi(const VX &vx, const VY &vy, const VZ &vz, const T (&y0)[3], const T (&g0)[3],
+                                       const Coef<T> &co, const T *az, const T *bz, T nu, T dt, T bsum, T (&xi)[3])
+{
+    T Sx[3], At[3], divY, divG;
+    adj_terms<T, H, false>(vx, vy, vz, y0, g0, co, az, bz, nu, Sx, At, divY, divG);
 #pragma unroll
     for (int e = 0; e < 3; e++) xi[e] = dt * (Sx[e] - T(0.5) * fma(g0[e], divY, At[e]) - nu * bsum * g0[e]);
 }

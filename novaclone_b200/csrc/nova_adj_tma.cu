@@ -1,18 +1,26 @@
-// Navier-Stokes adjoint stage (FP64) fed by a TMA pipeline, the data movement
-// of the forward stage kernel (nova_stage_tma.cu) for the six halo'd
-// components of the adjoint (forward stage state Y and direction g), with the
-// point arithmetic and the reverse RK4 recursion of nova_adj_math.cuh.
+// Adjoint stage kernels (FP64) fed by a TMA pipeline, the data movement of
+// the forward stage kernel (nova_stage_tma.cu) for six halo'd components: a
+// field P (the forward stage state Y of the Navier-Stokes stage, or the field
+// frozen in or evolved by an MHD loop) and the adjoint direction g, with the
+// building blocks of nova_adj_math.cuh combined per kind:
+//   ADJ_NS: xi = dt [ Sx - 1/2 At - 1/2 g divP - nu bsum g ]     (reverse RK4 recursion)
+//   ADJ_BB: xi = dt [ Sx + 1/2 At - 1/2 g divP - eta bsum g ]    (B loop, dF_B/dB; recursion)
+//   ADJ_UB: acc += dt [ 1/2 g divP - Sx + 1/2 At + P divG ]      (dF_U/dB, P = B^n)
+//   ADJ_BU: acc += dt [ 1/2 g divP - Sx - 1/2 At ]               (dF_B/dU, P = the B stage state)
+// (Sx with the Laplacian weight nu for NS, eta for BB, none for UB and BU);
+// the MHD right-hand sides are app/OT_Poisson/UEqn.H:16-23 and BEqn.H:72-78.
 //
 // A block owns a kTK(k) x 8(j) column and walks it along i: one producer warp
 // (lane 0) loads, per plane, each of the two 3-component fields as its halo'd
 // rows (box 32 x 3 x 14, [row][c][k]; a j-boundary tile as two boxes) and its
 // 4-wide k halos (box 4 x 8 x 3) into a 7-slot ring, and the epilogue
-// operands (mu, Lam) into a 3-slot ring.  Eight consumer warps, one per tile
-// row, keep the i stencil of the six components in a register queue; the
-// loop is unrolled by the queue period 7 = 2H + 1 = ring size, so the queue
-// rotates by register renaming.  At s = 4 the g field is mu itself: xi is
-// linear in g, so the kernel works on mu and scales xi by 1/6, and the centre
-// mu of the store comes from the queue.
+// operands (mu and Lam, or the accumulated adjoint) into a 3-slot ring.
+// Eight consumer warps, one per tile row, keep the i stencil of the six
+// components in a register queue; the loop is unrolled by the queue period
+// 7 = 2H + 1 = ring size, so the queue rotates by register renaming.  At
+// s = 4 the g field is mu itself: every combination is linear in g, so the
+// kernel works on mu and scales the result by 1/6, and the centre mu of the
+// recursion comes from the queue.
 //
 // Every mbarrier wait is bounded (nova_tma.cuh); a wait that gives up raises
 // the error word, and the producer drains its loads in flight, bounded, before
@@ -44,7 +52,11 @@ constexpr int kEpiE = TJ * kRowE;            // one epilogue field
 static_assert(kRing == 2 * kH + 1, "queue rotation and ring slots share one period");
 static_assert(TJ == kLRB && kLRB * 4 == kTK, "one k-halo box per side, component stride kTK");
 
-template <int S> __host__ __device__ constexpr int adj_epi() { return S == 4 ? 0 : 2; }  // mu, Lam
+// epilogue fields: mu, Lam (recursion kinds below s = 4) or the accumulated adjoint
+template <int KIND, int S> __host__ __device__ constexpr int adj_epi()
+{
+    return (KIND == ADJ_NS || KIND == ADJ_BB) ? (S == 4 ? 0 : 2) : 1;
+}
 
 template <int NE> constexpr size_t adj_smem_bytes()
 {
@@ -53,15 +65,16 @@ template <int NE> constexpr size_t adj_smem_bytes()
 
 struct AdjMaps {
     CUtensorMap f[2][4];  // per field: rows TJ+6, 3, TJ+3, k halos
-    CUtensorMap e[2];     // mu, Lam
+    CUtensorMap e[2];     // mu, Lam (or the accumulated adjoint)
 };
 
-template <int S>
+template <int KIND, int S>
 __global__ void __launch_bounds__(kThreads, 1)
     k_adj_tma(Geo g, Coef<double> co, const double *__restrict__ ia, double dt, double nu, AdjArgs args,
-              const __grid_constant__ AdjMaps maps, int ichunk, int *err)
+              double *__restrict__ acc, const __grid_constant__ AdjMaps maps, int ichunk, int *err)
 {
-    constexpr int H = kH, NE = adj_epi<S>();
+    constexpr int H = kH, NE = adj_epi<KIND, S>();
+    constexpr bool kRec = KIND == ADJ_NS || KIND == ADJ_BB;  // reverse RK4 recursion kinds
     constexpr uint32_t kSlotBytes = kSlotE * 8, kRowBytes = kRowE * 8, kEpiBytes = kEpiE * 8;
     constexpr uint32_t kFieldBytes = kFieldE * 8, kLRBytes = kLRE * 8;
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -199,30 +212,47 @@ __global__ void __launch_bounds__(kThreads, 1)
         auto vy = [&](int c, int s) -> double { return sl[fo(c) + cen + s * kRowE]; };
         auto vz = [&](int c, int s) -> double { return sl[fo(c) + zoff(s)]; };
         constexpr int kC = (R + H) % (2 * H + 1);
-        const double y0[3] = {q[kC][0], q[kC][1], q[kC][2]};
+        const double p0[3] = {q[kC][0], q[kC][1], q[kC][2]};
         const double g0[3] = {q[kC][3], q[kC][4], q[kC][5]};
-        double xi[3];
-        adj_xi<double, H>(vx, vy, vz, y0, g0, co, az, bz, nu, dt, bsum, xi);
+        double Sx[3], At[3], divP, divG;
+        adj_terms<double, H, KIND == ADJ_UB>(vx, vy, vz, p0, g0, co, az, bz, kRec ? nu : 0.0, Sx, At, divP, divG);
+        constexpr double gs = S == 4 ? 1.0 / 6.0 : 1.0;  // g4 = mu / 6
+        double r[3];
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            if constexpr (KIND == ADJ_NS)
+                r[e] = dt * (Sx[e] - 0.5 * fma(g0[e], divP, At[e]) - nu * bsum * g0[e]);
+            else if constexpr (KIND == ADJ_BB)
+                r[e] = dt * (Sx[e] + 0.5 * fma(-g0[e], divP, At[e]) - nu * bsum * g0[e]);
+            else if constexpr (KIND == ADJ_UB)
+                r[e] = dt * (fma(0.5 * g0[e], divP, -Sx[e]) + fma(0.5, At[e], p0[e] * divG));
+            else
+                r[e] = dt * (fma(0.5 * g0[e], divP, -Sx[e]) - 0.5 * At[e]);
+            if constexpr (S == 4) r[e] *= gs;
+        }
 
-        double mu[3], lam[3] = {0, 0, 0};
+        double e0[3], e1[3] = {0, 0, 0};
         if constexpr (NE > 0) {
             if (!__all_sync(0xffffffffu, mbar_wait(efull(es), eph, err))) return false;
             const double *se = ering + es * NE * kEpiE + ty * kRowE + tx;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                mu[c] = se[c * kTK];
-                lam[c] = se[kEpiE + c * kTK];
+                e0[c] = se[c * kTK];
+                if constexpr (NE > 1) e1[c] = se[kEpiE + c * kTK];
             }
         } else {
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                mu[c] = g0[c];             // the g field is mu at s = 4
-                xi[c] *= (1.0 / 6.0);      // g4 = mu / 6
-            }
+            for (int c = 0; c < 3; c++) e0[c] = g0[c];  // mu: the g field at s = 4
         }
         const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
 #pragma unroll
-        for (int e = 0; e < 3; e++) adj_store<double, S>(args, (long long)e * g.N3 + idx, mu[e], lam[e], xi[e]);
+        for (int e = 0; e < 3; e++) {
+            const long long o = (long long)e * g.N3 + idx;
+            if constexpr (kRec)
+                adj_store<double, S>(args, o, e0[e], e1[e], r[e]);
+            else
+                acc[o] = e0[e] + r[e];
+        }
         if constexpr (NE > 0) {
             release(eempty(es));
             if (++es == kERing) {
@@ -257,45 +287,61 @@ int adj_ichunk(const Geo &g)
     return ch;
 }
 
-template <int S>
+template <int KIND, int S>
 cudaError_t launch_adj_s(const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
-                         const AdjArgs &a, int *err, cudaStream_t st)
+                         const AdjArgs &a, double *acc, int *err, cudaStream_t st)
 {
-    constexpr int NE = adj_epi<S>();
+    constexpr int NE = adj_epi<KIND, S>();
     AdjMaps maps;
     memset(&maps, 0, sizeof maps);
-    const double *fld[2] = {a.Y, S == 4 ? a.mu : a.G};
+    const double *fld[2] = {a.Y, a.G};  // at s = 4 the drivers pass mu as g
     bool ok = true;
     for (int f = 0; f < 2; f++)
         ok = ok && tma_encode_field(&maps.f[f][0], fld[f], g, TJ + 2 * kH) &&
              tma_encode_field(&maps.f[f][1], fld[f], g, kH) && tma_encode_field(&maps.f[f][2], fld[f], g, TJ + kH) &&
              tma_encode_field(&maps.f[f][3], fld[f], g, 0);
-    if (NE > 0) ok = ok && tma_encode_field(&maps.e[0], a.mu, g, TJ) && tma_encode_field(&maps.e[1], a.Lam, g, TJ);
+    if (KIND == ADJ_NS || KIND == ADJ_BB) {
+        if (NE > 0) ok = ok && tma_encode_field(&maps.e[0], a.mu, g, TJ) && tma_encode_field(&maps.e[1], a.Lam, g, TJ);
+    } else {
+        ok = ok && tma_encode_field(&maps.e[0], acc, g, TJ);
+    }
     if (!ok) return cudaErrorInvalidValue;
     constexpr size_t smem = adj_smem_bytes<NE>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_adj_tma<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_adj_tma<KIND, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
     const int ch = adj_ichunk(g);
     const dim3 grid(g.N2 / kTK, g.N1 / TJ, (g.N0 + ch - 1) / ch);
-    k_adj_tma<S><<<grid, dim3(kTK, TJ + 1), smem, st>>>(g, co, ia, dt, nu, a, maps, ch, err);
+    k_adj_tma<KIND, S><<<grid, dim3(kTK, TJ + 1), smem, st>>>(g, co, ia, dt, nu, a, acc, maps, ch, err);
     return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t launch_adj_k(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
+                         const AdjArgs &a, double *acc, int *err, cudaStream_t st)
+{
+    switch (s) {
+    case 4: return launch_adj_s<KIND, 4>(g, co, ia, dt, nu, a, acc, err, st);
+    case 3: return launch_adj_s<KIND, 3>(g, co, ia, dt, nu, a, acc, err, st);
+    case 2: return launch_adj_s<KIND, 2>(g, co, ia, dt, nu, a, acc, err, st);
+    default: return launch_adj_s<KIND, 1>(g, co, ia, dt, nu, a, acc, err, st);
+    }
 }
 
 }  // namespace
 
 bool adj_tma_fits(const Geo &g) { return !g.wallY && g.N2 % kTK == 0 && g.N1 % TJ == 0 && g.N1 >= 2 * TJ; }
 
-cudaError_t launch_adj_tma64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
-                             const AdjArgs &a, int *err, cudaStream_t st)
+cudaError_t launch_adj_tma64(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt,
+                             double nu, const AdjArgs &a, double *acc, int *err, cudaStream_t st)
 {
-    switch (s) {
-    case 4: return launch_adj_s<4>(g, co, ia, dt, nu, a, err, st);
-    case 3: return launch_adj_s<3>(g, co, ia, dt, nu, a, err, st);
-    case 2: return launch_adj_s<2>(g, co, ia, dt, nu, a, err, st);
-    default: return launch_adj_s<1>(g, co, ia, dt, nu, a, err, st);
+    switch (kind) {
+    case ADJ_UB: return launch_adj_k<ADJ_UB>(s, g, co, ia, dt, nu, a, acc, err, st);
+    case ADJ_BU: return launch_adj_k<ADJ_BU>(s, g, co, ia, dt, nu, a, acc, err, st);
+    case ADJ_BB: return launch_adj_k<ADJ_BB>(s, g, co, ia, dt, nu, a, acc, err, st);
+    default: return launch_adj_k<ADJ_NS>(s, g, co, ia, dt, nu, a, acc, err, st);
     }
 }
 

@@ -215,7 +215,7 @@ void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t
 cudaError_t launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                                const AdjArgs &a, cudaStream_t st, int *err)
 {
-    if (err && adj_tma_fits(g)) return launch_adj_tma64(s, g, co, ia, dt, nu, a, err, st);
+    if (err && adj_tma_fits(g)) return launch_adj_tma64(ADJ_NS, s, g, co, ia, dt, nu, a, nullptr, err, st);
     launch_adj<double>(s, g, co, ia, dt, nu, a, st);
     return cudaSuccess;
 }
@@ -226,15 +226,17 @@ void launch_adj_stage32(int s, const Geo &g, const Coef<float> &co, const float 
     launch_adj<float>(s, g, co, ia, dt, nu, a, st);
 }
 
-void launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double visc,
-                    const AdjArgs &a, double *acc, cudaStream_t st)
+cudaError_t launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt,
+                           double visc, const AdjArgs &a, double *acc, cudaStream_t st, int *err)
 {
+    if (err && adj_tma_fits(g)) return launch_adj_tma64(kind, s, g, co, ia, dt, visc, a, acc, err, st);
     if (kind == 0)
         launch_mhd_k<KIND_UB>(s, g, co, ia, dt, visc, a, acc, st);
     else if (kind == 1)
         launch_mhd_k<KIND_BU>(s, g, co, ia, dt, visc, a, acc, st);
     else
         launch_mhd_k<KIND_BB>(s, g, co, ia, dt, visc, a, acc, st);
+    return cudaSuccess;
 }
 
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st)

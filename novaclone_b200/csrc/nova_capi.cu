@@ -1548,7 +1548,9 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
     };
     auto adj_mhd = [&](int kind, int stage, const AdjArgs &a, double *acc) {
         ProfScope ps(ctx, NOVA_K_ADJ);
-        launch_adj_mhd(kind, stage, ctx->g, ctx->co64, ctx->d_ia64, dt, rd->eta, a, acc, st);
+        const cudaError_t e = launch_adj_mhd(kind, stage, ctx->g, ctx->co64, ctx->d_ia64, dt, rd->eta, a, acc, st,
+                                             ctx->stage_impl != STAGE_MARCH ? ctx->d_flag + 1 : nullptr);
+        if (e != cudaSuccess && aerr == cudaSuccess) aerr = e;
         ctx->launches += 1;
     };
     auto proj = [&](const double *in) {

@@ -178,8 +178,10 @@ struct AdjArgs {
 cudaError_t launch_adj_stage64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
                                const AdjArgs &a, cudaStream_t st, int *err = nullptr);
 bool adj_tma_fits(const Geo &g);
-cudaError_t launch_adj_tma64(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double nu,
-                             const AdjArgs &a, int *err, cudaStream_t st);
+// kind: 0, 1, 2 = the MHD pieces of launch_adj_mhd (acc: the adjoint they add
+// into), 3 = the Navier-Stokes stage
+cudaError_t launch_adj_tma64(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt,
+                             double nu, const AdjArgs &a, double *acc, int *err, cudaStream_t st);
 // FP32-split adjoint stage: FP32 stage states, directions and running sum;
 // mu (and dJ/dU, written to `lam` at s = 1) in FP64
 struct AdjArgs32 {
@@ -196,8 +198,8 @@ void launch_adj_stage32(int s, const Geo &g, const Coef<float> &co, const float 
 // MHD adjoint stage pieces (nova_adjoint.cu): kind 0 = dF_U/dB (lambda_B += ...),
 // 1 = dF_B/dU (lambda_U += ...), 2 = dF_B/dB with the reverse RK4 recursion;
 // a.Y = the field in the transpose (B^n, Z_S or U^{n+1}), a.G = g_S
-void launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double visc,
-                    const AdjArgs &a, double *acc, cudaStream_t st);
+cudaError_t launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt,
+                           double visc, const AdjArgs &a, double *acc, cudaStream_t st, int *err = nullptr);
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);  // y = a x
 void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t st);        // y += a x
 
