@@ -76,6 +76,57 @@ def ot_fields(n):
     return U, B
 
 
+def unit_directions(n, count, seed):
+    """Seeded random smooth vector fields of unit RMS amplitude on the n^3 grid
+    (three low Fourier modes per component), one at a time."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(n) * (2 * math.pi / n)
+    for _ in range(count):
+        v = np.zeros((3, n, n, n))
+        for c in range(3):
+            for _ in range(3):
+                k = rng.integers(-3, 4, size=3)
+                ph, amp = rng.uniform(0, 2 * math.pi), rng.standard_normal()
+                e = (np.exp(1j * k[0] * x)[:, None, None] * np.exp(1j * k[1] * x)[None, :, None] *
+                     np.exp(1j * (k[2] * x + ph))[None, None, :])
+                v[c] += amp * e.real
+        yield v / math.sqrt(float(np.mean(v * v)))
+
+
+def final_energy(nova, GM, rd, U0, nsteps, B0=None):
+    """E_kin (+ E_mag with B0) after nsteps, from the solver's own diagnostics row."""
+    U = nova.Field(GM, 3).upload_soa(U0)
+    p = nova.Field(GM, 1)
+    B = pB = None
+    if B0 is not None:
+        B, pB = nova.Field(GM, 3).upload_soa(B0), nova.Field(GM, 1)
+    rd.diag_every = nsteps
+    h = nova.advance(GM, rd, U, p, B, pB, nsteps=nsteps, history=True)
+    rd.diag_every = 0
+    for f in (U, p, B, pB):
+        if f is not None:
+            f.close()
+    return float(h[-1, 2] + (h[-1, 3] if B0 is not None else 0.0))
+
+
+def fd_check(nova, GM, rd, U0, grads, nsteps, count, eps=1e-6, B0=None, seed=2024):
+    """Central finite differences of the objective along `count` seeded unit
+    directions (in U, and in B for MHD) against the adjoint gradient."""
+    errs = []
+    n = U0.shape[1]
+    dirs = unit_directions(n, count * (2 if B0 is not None else 1), seed)
+    for _ in range(count):
+        v = next(dirs)
+        w = next(dirs) if B0 is not None else None
+        plus = final_energy(nova, GM, rd, U0 + eps * v, nsteps, None if B0 is None else B0 + eps * w)
+        minus = final_energy(nova, GM, rd, U0 - eps * v, nsteps, None if B0 is None else B0 - eps * w)
+        fd = (plus - minus) / (2 * eps)
+        ad = float(np.sum(grads[0] * v)) + (float(np.sum(grads[1] * w)) if B0 is not None else 0.0)
+        errs.append(abs(fd - ad) / abs(ad))
+    return {"directions": count, "eps": eps, "max_rel_err": max(errs), "rel_errs": errs,
+            "objective_from": "the solver's diagnostics row after the same steps"}
+
+
 def ghosted(U, h=3):
     """(3, n, n, n) unique nodes -> the reference's ghosted AoS Field<vector> layout (periodic images)."""
     n = U.shape[1]
@@ -292,9 +343,10 @@ def time_e2e(nova, torch, GM, U, p, rd, U0_aos_pinned, out_pinned, steps, dist):
 
 
 def mhd_legs(args, nova, torch, dist, world):
-    """Secondary MHD numbers: Orszag-Tang at args.mhd_n^3 (U loop then B loop with
-    its cleaning projection, classical RK4, nu = eta = 1/1000), FP64 and
-    FP32-split, and the MHD adjoint / forward ratio at args.mhd_adj_n^3."""
+    """Secondary MHD numbers: Orszag-Tang at args.mhd_n^3 for args.mhd_steps steps
+    (U loop then B loop with its cleaning projection, classical RK4, nu = eta =
+    1/1000), FP64 and FP32-split with the split error at the end, and the MHD
+    adjoint / forward ratio at args.mhd_adj_n^3 with its finite-difference check."""
     def maxover(x):
         return max_over_ranks(x, dist)
 
@@ -351,11 +403,13 @@ def mhd_legs(args, nova, torch, dist, world):
         U.upload_soa(U0)
         B.upload_soa(B0)
         t_adj, r = timed(lambda: nova.adjoint_grad(AM, rd, U, M, checkpoint_every=K, B0=B, total_energy=True))
+        grads = [r[1].download_soa(), r[2].download_soa()]
         for f in list(r[1:]) + [U, B, p, pB]:
             f.close()
+        fd = fd_check(nova, AM, rd, U0, grads, M, args.fd_dirs, B0=B0) if args.fd_dirs > 0 else None
         res["adjoint"] = {"ratio": t_adj / t_fwd, "forward_s": t_fwd, "adjoint_s": t_adj, "grid": [na] * 3,
                           "steps": M, "checkpoint_every": K, "objective": "E_kin + E_mag at the final step",
-                          "gradients": "dJ/dU0 and dJ/dB0", "dtype": "f64", "J": r[0]}
+                          "gradients": "dJ/dU0 and dJ/dB0", "dtype": "f64", "J": r[0], "fd_check": fd}
     return res
 
 
@@ -425,8 +479,13 @@ def our_arm(args, rank, world, dist):
             grad.close()
             U.close()
         f, s32 = adj_runs["f64"], adj_runs["f32split"]
+        fd = None
+        if args.fd_dirs > 0:
+            rd = nova.run_desc(model="ns", rk_mode="classical", precision=nova.F64, dt=dt, nu=NU, diag_every=0)
+            fd = fd_check(nova, GM, rd, U0, [f["grad"]], M, args.fd_dirs)
         adj = {"ratio": f["ratio"], "forward_s": f["forward_s"], "adjoint_s": f["adjoint_s"], "steps": M,
                "checkpoint_every": K, "objective": "E_kin at the final step", "dtype": "f64", "J": f["J"],
+               "fd_check": fd,
                "f32split": {"ratio": s32["ratio"], "forward_s": s32["forward_s"], "adjoint_s": s32["adjoint_s"],
                             "J": s32["J"], "grad_rel_l2_vs_fp64": float(np.linalg.norm(s32["grad"] - f["grad"]) /
                                                                         np.linalg.norm(f["grad"])),
@@ -526,9 +585,10 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--adj-checkpoint", type=int, default=20)
     ap.add_argument("--no-mhd", action="store_true")
-    ap.add_argument("--mhd-n", type=int, default=256)
-    ap.add_argument("--mhd-steps", type=int, default=20)
+    ap.add_argument("--mhd-n", type=int, default=128)
+    ap.add_argument("--mhd-steps", type=int, default=200)
     ap.add_argument("--mhd-adj-n", type=int, default=128)
+    ap.add_argument("--fd-dirs", type=int, default=8, help="finite-difference checks of each FP64 adjoint")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
