@@ -551,6 +551,20 @@ def ic_orszag_tang(mesh):
     return U, B
 
 
+def ic_mhd_jet(mesh, seed=1, noise=1e-3):
+    """MHD jet (x, y in [-4, 4] about the axis, z periodic): u_z = 0.5 (1 - tanh((r - 1)/0.1)),
+    B_z = 0.5, B_theta = 0.2 r exp(-r^2), white noise of amplitude `noise` on u."""
+    x, y, z = mesh.coords()
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    r = np.sqrt(X * X + Y * Y)
+    zero = np.zeros_like(X)
+    U = np.stack([zero, zero, 0.5 * (1.0 - np.tanh((r - 1.0) / 0.1))])
+    U = U + noise * np.random.default_rng(seed).standard_normal(U.shape)
+    e = 0.2 * np.exp(-r * r)  # B_theta / r
+    B = np.stack([-e * Y, e * X, np.full_like(X, 0.5)])
+    return U, B
+
+
 def wc_shear_params(mach=0.1):
     """Constants of app/shearLayerWC/shearLayer.cpp:31-44 (Mach as a parameter)."""
     Re0, Ri0, Pr, rho0, c = 1967.0, 0.08, 7.0, 999.57, 0.0417

@@ -133,6 +133,25 @@ def test_fp32_split_error_is_bounded(nova, oracle):
     assert g32["hist"][-1, 4] < 1e-10  # the FP64 projection still removes the divergence
 
 
+def test_mhd_jet_vs_oracle_and_split_error(nova, oracle):
+    """The MHD jet configuration on a small mesh (x, y in [-4, 4], z in [0, 16],
+    the reference app's scheme: literal U loop, refreshed B loop): FP64 against
+    the oracle, FP32-split against FP64."""
+    OM = oracle.Mesh((24, 24, 48), L=(8.0, 8.0, 16.0), origin=(-4.0, -4.0, 0.0))
+    U0, B0 = oracle.ic_mhd_jet(OM)
+    dt = oracle.cfl_dt(OM, [U0, B0])
+    kw = dict(model="mhd", rk_mode="literal", nsteps=10, dt=dt, nu=1 / 1500, eta=1 / 1500)
+    g = gpu_run(nova, OM, U0, B0, **kw)
+    o = oracle_run(oracle, OM, U0, B0, **kw)
+    for f in ("U", "B"):
+        assert rel_l2(g[f], o[f]) < TOL64, (f, rel_l2(g[f], o[f]))
+    assert rel_l2(g["p"], o["p"]) < TOL64
+    check_hist(g["hist"], o["hist"])
+    s = gpu_run(nova, OM, U0, B0, precision=nova.F32SPLIT, **kw)
+    for f in ("U", "B"):
+        assert rel_l2(s[f], g[f]) < 1e-5
+
+
 def test_fp32_split_mhd_error_is_bounded(nova, oracle):
     OM = oracle.Mesh((24, 24, 24))
     U0, B0 = oracle.ic_orszag_tang(OM)
