@@ -426,6 +426,24 @@ def mhd_legs(args, nova, torch, dist, world):
         res["adjoint"] = {"ratio": t_adj / t_fwd, "forward_s": t_fwd, "adjoint_s": t_adj, "grid": [na] * 3,
                           "steps": M, "checkpoint_every": K, "objective": "E_kin + E_mag at the final step",
                           "gradients": "dJ/dU0 and dJ/dB0", "dtype": "f64", "J": r[0], "fd_check": fd}
+        # the FP32-split adjoint of the same case against its own forward solve and the FP64 gradients
+        U, B = nova.Field(AM, 3, nova.F32SPLIT).upload_soa(U0), nova.Field(AM, 3, nova.F32SPLIT).upload_soa(B0)
+        p, pB = nova.Field(AM, 1), nova.Field(AM, 1)
+        rd = nova.run_desc(model="mhd", rk_mode="classical", precision=nova.F32SPLIT, dt=dt, nu=MHD_NU, eta=MHD_NU,
+                           diag_every=0)
+        for f in nova.adjoint_grad(AM, rd, U, M, checkpoint_every=K, B0=B, total_energy=True)[1:]:
+            f.close()
+        t_fwd, _ = timed(lambda: nova.advance(AM, rd, U, p, B, pB, nsteps=M, history=False))
+        U.upload_soa(U0)
+        B.upload_soa(B0)
+        t_adj, r = timed(lambda: nova.adjoint_grad(AM, rd, U, M, checkpoint_every=K, B0=B, total_energy=True))
+        g32 = [r[1].download_soa(), r[2].download_soa()]
+        for f in list(r[1:]) + [U, B, p, pB]:
+            f.close()
+        res["adjoint"]["f32split"] = {
+            "ratio": t_adj / t_fwd, "forward_s": t_fwd, "adjoint_s": t_adj, "J": r[0],
+            "grad_rel_l2_vs_fp64": [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(g32, grads)],
+            "dtype": "f32 adjoint stages and stage states, f64 adjoint state and projections"}
     return res
 
 

@@ -196,7 +196,7 @@ typedef enum {
     NOVA_OBJ_ETOT_FINAL = 2
 } nova_objective;
 typedef struct {
-    nova_run_desc run;     /* forward run: NS or MHD, classical RK4, FP64, periodic uniform mesh */
+    nova_run_desc run;     /* forward run: NS or MHD, classical RK4, FP64 or FP32-split, periodic uniform mesh */
     int nsteps;            /* steps of the forward solve */
     int checkpoint_every;  /* K: states kept every K steps, segments recomputed in reverse */
     int objective;         /* nova_objective */
@@ -204,7 +204,9 @@ typedef struct {
 } nova_adj_desc;
 /* Gradient of J with respect to the initial fields by the hand-written
  * discrete adjoint of the fused stages, the RK4 loops and the (self-adjoint)
- * projection.  init is not modified; gradU receives dJ/dU0 (FP64, 3 comps);
+ * projection.  init is not modified (its fields in the run's precision; for
+ * FP32-split the trajectory is the split path's and the adjoint stages run in
+ * FP32 with the adjoint state in FP64); gradU receives dJ/dU0 (FP64, 3 comps);
  * for MHD (run.model NOVA_MODEL_MHD, the U loop then the B loop of each step
  * as nova_advance runs them) gradB receives dJ/dB0 (FP64, 3 comps; required);
  * for Navier-Stokes gradB must be NULL.  *objective receives J. */

@@ -75,122 +75,93 @@ void launch_adj(int s, const Geo &g, const Coef<T> &co, const T *ia, T dt, T nu,
 }
 
 // ----------------------------------------------------------- MHD adjoint --
-// Building blocks for div(V,F)_c = 1/2 sum_d [D_d(V_d F_c) + V_d D_d F_c + F_c D_d V_d]
-// with D_d^T = -D_d (periodic central differences), for an adjoint direction g:
-//   T_F(V; g)_c = (d div(V,F)/dF)^T g = 1/2 [ -sum_d A_d(V,g)_c + g_c sum_d D_d V_d ]
-//   T_V(F; g)_e = (d div(V,F)/dV)^T g = 1/2 [ -sum_c F_c D_e g_c + sum_c g_c D_e F_c - D_e(sum_c F_c g_c) ]
-// (for the Navier-Stokes term div(U,U) the transpose is T_F(U) + T_V(U), k_adj_stage).
 // MHD right-hand sides (app/OT_Poisson/UEqn.H:16-23, BEqn.H:72-78):
 //   F_U = -div(U,U) + nu L U + div(B,B) - grad(1/2 |B|^2)   (B frozen in the U loop)
 //   F_B = -div(U,B) + div(B,U) + eta L B                    (U frozen in the B loop)
-// with (d grad(1/2|B|^2)/dB)^T g = -B_e div g, the kernels compute, for the
-// stage direction g_S and the field P in comps 0-2 of the march:
-//   KIND_UB: lambda_B += dt [T_F(B) + T_V(B) + B div g]     P = B^n (dF_U/dB)
-//   KIND_BU: lambda_U += dt [T_F(B) - T_V(B)]               P = Z_S, the B stage state (dF_B/dU)
-//   KIND_BB: xi = dt [-T_F(U') + T_V(U') + eta L g]          P = U^{n+1} (dF_B/dB; F_B is linear in B)
-//            with the reverse RK4 recursion of k_adj_stage in the epilogue
-enum AdjMhdKind { KIND_UB = 0, KIND_BU = 1, KIND_BB = 2 };
-
-template <int KIND, int S>
-__global__ void __launch_bounds__(kThreads, 1) k_adj_mhd(Geo g, Coef<double> co, const double *__restrict__ ia,
-                                                         double dt, double visc, AdjArgs a, double *acc, int ichunk)
+// The coupling transposes, from the building blocks of nova_adj_math.cuh for
+// the field P in comps 0-2 and the stage direction g_S in comps 3-5
+// ((d grad(1/2|B|^2)/dB)^T g = -B div g):
+//   ADJ_UB: acc += dt [ 1/2 g divP - Sx + 1/2 At + P divG ]   P = B^n        (dF_U/dB into lambda_B)
+//   ADJ_BU: acc += dt [ 1/2 g divP - Sx - 1/2 At ]            P = Z_S        (dF_B/dU into lambda_U)
+//   ADJ_BB: xi   = dt [ Sx + 1/2 At - 1/2 g divP - eta bsum g ] P = U^{n+1}  (dF_B/dB, with the recursion)
+// (Sx with the Laplacian weight eta for BB only).  Tiled march; T = float with
+// A = AdjArgs32 for the FP32-split adjoint (acc and mu stay FP64).  At s = 4
+// the direction is mu/6, read from a.mu.
+template <typename T, int KIND, int S, class A>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
+    k_adj_mhd(Geo g, Coef<T> co, const T *__restrict__ ia, T dt, T visc, A a, double *acc, int ichunk)
 {
     constexpr int H = 3;
     extern __shared__ __align__(16) unsigned char smraw[];
-    auto &sm = *reinterpret_cast<TileSmem<double, H, 6> *>(smraw);
+    auto &sm = *reinterpret_cast<TileSmem<T, H, 6> *>(smraw);
     const int ib = blockIdx.z * ichunk;
     const int ie = min(ib + ichunk, g.N0);
     const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
-    const double iak = ia[kw];
-    double az[H], bz[H];
-#pragma unroll
-    for (int l = 0; l < H; l++) {
-        az[l] = co.a[2][l] * iak;
-        bz[l] = co.b[2][l] * iak * iak;
-    }
-    const double bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
-    const double gs = (S == 4) ? 1.0 / 6.0 : 1.0;
-    auto ld = [&](int c, long long o) -> double {
-        return c < 3 ? a.Y[(long long)c * g.N3 + o] : a.G[(long long)(c - 3) * g.N3 + o] * gs;
+    T az[H], bz[H], bsum;
+    adj_zweights<T, H>(co, ia[kw], az, bz, bsum);
+    auto ld = [&](int c, long long o) -> T {
+        if (c < 3) return a.Y[(long long)c * g.N3 + o];
+        if constexpr (S == 4) return (T)(a.mu[(long long)(c - 3) * g.N3 + o] * (1.0 / 6.0));
+        return a.G[(long long)(c - 3) * g.N3 + o];
     };
-    const Walls<double> wl{};
-    tile_march<double, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
-                                                          const auto &vz) {
-        const double p0[3] = {q[H][0], q[H][1], q[H][2]};
-        const double g0[3] = {q[H][3], q[H][4], q[H][5]};
-        double At[3] = {0, 0, 0}, Bt[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, divP = 0.0, divg = 0.0;
-        auto dir = [&](const auto &v, int d, const double *aa, const double *bb) {
-            double dP[3], dG[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                dP[c] = d1<double, H>(v, c, aa);
-                dG[c] = d1<double, H>(v, 3 + c, aa);
-                Bt[c] -= adv1<double, H>(v, 3 + c, d, p0[d], aa);
-                if (KIND == KIND_BB) lap[c] += lsum<double, H>(v, 3 + c, bb);
-            }
-            divP += dP[d];
-            divg += dG[d];
-            auto sdot = [&](int, int s) -> double {
-                return v(0, s) * v(3, s) + v(1, s) * v(4, s) + v(2, s) * v(5, s);
-            };
-            At[d] = -(p0[0] * dG[0] + p0[1] * dG[1] + p0[2] * dG[2]) + (g0[0] * dP[0] + g0[1] * dP[1] + g0[2] * dP[2])
-                    - d1<double, H>(sdot, 0, aa);
-        };
-        dir(vx, 0, co.a[0], co.b[0]);
-        dir(vy, 1, co.a[1], co.b[1]);
-        dir(vz, 2, az, bz);
+    const Walls<T> wl{};
+    tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
+                                                  const auto &vz) {
+        const T p0[3] = {q[H][0], q[H][1], q[H][2]};
+        const T g0[3] = {q[H][3], q[H][4], q[H][5]};
+        T Sx[3], At[3], divP, divG;
+        adj_terms<T, H, KIND == ADJ_UB>(vx, vy, vz, p0, g0, co, az, bz, KIND == ADJ_BB ? visc : T(0), Sx, At, divP,
+                                        divG);
 #pragma unroll
         for (int e = 0; e < 3; e++) {
-            const double TF = 0.5 * fma(g0[e], divP, Bt[e]), TV = 0.5 * At[e];
             const long long o = (long long)e * g.N3 + idx;
-            if constexpr (KIND == KIND_UB) {
-                acc[o] += dt * (TF + TV + p0[e] * divg);
-            } else if constexpr (KIND == KIND_BU) {
-                acc[o] += dt * (TF - TV);
+            if constexpr (KIND == ADJ_BB) {
+                const T xi = dt * (Sx[e] + T(0.5) * fma(-g0[e], divP, At[e]) - visc * bsum * g0[e]);
+                adj_store<T, S>(a, o, a.mu[o], S == 4 ? T(0) : a.Lam[o], xi);
+            } else if constexpr (KIND == ADJ_UB) {
+                acc[o] += (double)(dt * (fma(T(0.5) * g0[e], divP, -Sx[e]) + fma(T(0.5), At[e], p0[e] * divG)));
             } else {
-                const double xi = dt * (-TF + TV + visc * fma(-bsum, g0[e], lap[e]));
-                const double mu = a.mu[o];
-                if constexpr (S == 4) {
-                    a.Gout[o] = mu * (1.0 / 3.0) + xi;
-                    a.LamOut[o] = xi;
-                } else if constexpr (S == 3) {
-                    a.Gout[o] = mu * (1.0 / 3.0) + 0.5 * xi;
-                    a.LamOut[o] = a.Lam[o] + xi;
-                } else if constexpr (S == 2) {
-                    a.Gout[o] = mu * (1.0 / 6.0) + 0.5 * xi;
-                    a.LamOut[o] = a.Lam[o] + xi;
-                } else {
-                    a.Gout[o] = mu + (a.Lam[o] + xi);
-                }
+                acc[o] += (double)(dt * (fma(T(0.5) * g0[e], divP, -Sx[e]) - T(0.5) * At[e]));
             }
         }
     });
 }
 
-template <int KIND, int S>
-void launch_mhd_s(const Geo &g, const Coef<double> &co, const double *ia, double dt, double visc, const AdjArgs &a,
-                  double *acc, cudaStream_t st)
+template <typename T, int KIND, int S, class A>
+void launch_mhd_s(const Geo &g, const Coef<T> &co, const T *ia, T dt, T visc, const A &a, double *acc, cudaStream_t st)
 {
-    constexpr size_t smem = tile_smem_bytes<double, 3, 6>();
+    constexpr size_t smem = tile_smem_bytes<T, 3, 6>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_adj_mhd<KIND, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_adj_mhd<T, KIND, S, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    const int ch = pick_ichunk(g, 1);
-    k_adj_mhd<KIND, S><<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, dt, visc, a, acc, ch);
+    const int ch = pick_ichunk(g, sizeof(T) == 8 ? 1 : 2);
+    k_adj_mhd<T, KIND, S, A><<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, dt, visc, a, acc, ch);
 }
 
-template <int KIND>
-void launch_mhd_k(int s, const Geo &g, const Coef<double> &co, const double *ia, double dt, double visc,
-                  const AdjArgs &a, double *acc, cudaStream_t st)
+template <typename T, int KIND, class A>
+void launch_mhd_k(int s, const Geo &g, const Coef<T> &co, const T *ia, T dt, T visc, const A &a, double *acc,
+                  cudaStream_t st)
 {
     switch (s) {
-    case 4: launch_mhd_s<KIND, 4>(g, co, ia, dt, visc, a, acc, st); break;
-    case 3: launch_mhd_s<KIND, 3>(g, co, ia, dt, visc, a, acc, st); break;
-    case 2: launch_mhd_s<KIND, 2>(g, co, ia, dt, visc, a, acc, st); break;
-    default: launch_mhd_s<KIND, 1>(g, co, ia, dt, visc, a, acc, st); break;
+    case 4: launch_mhd_s<T, KIND, 4>(g, co, ia, dt, visc, a, acc, st); break;
+    case 3: launch_mhd_s<T, KIND, 3>(g, co, ia, dt, visc, a, acc, st); break;
+    case 2: launch_mhd_s<T, KIND, 2>(g, co, ia, dt, visc, a, acc, st); break;
+    default: launch_mhd_s<T, KIND, 1>(g, co, ia, dt, visc, a, acc, st); break;
     }
+}
+
+template <typename T, class A>
+void launch_mhd_any(int kind, int s, const Geo &g, const Coef<T> &co, const T *ia, T dt, T visc, const A &a,
+                    double *acc, cudaStream_t st)
+{
+    if (kind == ADJ_UB)
+        launch_mhd_k<T, ADJ_UB>(s, g, co, ia, dt, visc, a, acc, st);
+    else if (kind == ADJ_BU)
+        launch_mhd_k<T, ADJ_BU>(s, g, co, ia, dt, visc, a, acc, st);
+    else
+        launch_mhd_k<T, ADJ_BB>(s, g, co, ia, dt, visc, a, acc, st);
 }
 
 __global__ void k_axpby(long long n, double a, const double *__restrict__ x, double *__restrict__ y)
@@ -230,13 +201,14 @@ cudaError_t launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co
                            double visc, const AdjArgs &a, double *acc, cudaStream_t st, int *err)
 {
     if (err && adj_tma_fits(g)) return launch_adj_tma64(kind, s, g, co, ia, dt, visc, a, acc, err, st);
-    if (kind == 0)
-        launch_mhd_k<KIND_UB>(s, g, co, ia, dt, visc, a, acc, st);
-    else if (kind == 1)
-        launch_mhd_k<KIND_BU>(s, g, co, ia, dt, visc, a, acc, st);
-    else
-        launch_mhd_k<KIND_BB>(s, g, co, ia, dt, visc, a, acc, st);
+    launch_mhd_any<double>(kind, s, g, co, ia, dt, visc, a, acc, st);
     return cudaSuccess;
+}
+
+void launch_adj_mhd32(int kind, int s, const Geo &g, const Coef<float> &co, const float *ia, float dt, float visc,
+                      const AdjArgs32 &a, double *acc, cudaStream_t st)
+{
+    launch_mhd_any<float>(kind, s, g, co, ia, dt, visc, a, acc, st);
 }
 
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st)

@@ -1203,12 +1203,15 @@ nova_status rk_loop64(nova_ctx *ctx, const nova_run_desc *rd, int phys, double v
     return NOVA_OK;
 }
 
-// One classical RK4 step + projection of an FP32-split Navier-Stokes state,
-// the launches of the split path of nova_advance: (hi, lo) -> (ohi, olo) (may
-// alias), FP32 stage states into S2, S3, S4 (S4 may alias S2), the pressure
-// into pbuf (FP64).  Without `full` only the stage states are produced.
-nova_status rk_loop32(nova_ctx *ctx, const nova_run_desc *rd, const float *hi, const float *lo, float *S2, float *S3,
-                      float *S4, float *ohi, float *olo, double *pbuf, bool full)
+// One classical RK4 loop + projection of an FP32-split state (physics phys,
+// viscosity visc, frozen field X given by its hi part, rhs divisor and
+// correction scale div), the launches of the split path of nova_advance:
+// (hi, lo) -> (ohi, olo) (may alias), FP32 stage states into S2, S3, S4 (S4
+// may alias S2), the pressure into pbuf (FP64).  Without `full` only the
+// stage states are produced.
+nova_status rk_loop32(nova_ctx *ctx, const nova_run_desc *rd, int phys, double visc, double div, const float *hi,
+                      const float *lo, const float *X, float *S2, float *S3, float *S4, float *ohi, float *olo,
+                      double *pbuf, bool full)
 {
     const Geo &g = ctx->g;
     cudaStream_t st = ctx->stream;
@@ -1217,27 +1220,27 @@ nova_status rk_loop32(nova_ctx *ctx, const nova_run_desc *rd, const float *hi, c
     nova_status sst = NOVA_OK;
     auto run = [&](int stage, const StageArgs32 &a) {
         ProfScope ps(ctx, NOVA_K_STAGE);
-        const cudaError_t e = launch_stage32(PHYS_NS, stage, str, g, Walls<float>{}, ctx->co32, ctx->d_ia32,
-                                             ctx->d_corr32, (float)rd->dt, (float)rd->nu, a, st,
+        const cudaError_t e = launch_stage32(phys, stage, str, g, Walls<float>{}, ctx->co32, ctx->d_ia32,
+                                             ctx->d_corr32, (float)rd->dt, (float)visc, a, st,
                                              StageExec{ctx->stage_impl, ctx->d_flag + 1});
         if (e != cudaSuccess && sst == NOVA_OK) sst = stage_fail(ctx, e);
         ctx->launches += 1;
     };
-    run(0, StageArgs32{hi, nullptr, nullptr, nullptr, A, S2, nullptr, nullptr});
-    run(1, StageArgs32{S2, nullptr, hi, nullptr, A, S3, nullptr, nullptr});
-    run(2, StageArgs32{S3, nullptr, hi, nullptr, A, S4, nullptr, nullptr});
-    if (full) run(3, StageArgs32{S4, nullptr, hi, lo, A, nullptr, ohi, olo});
+    run(0, StageArgs32{hi, X, nullptr, nullptr, A, S2, nullptr, nullptr});
+    run(1, StageArgs32{S2, X, hi, nullptr, A, S3, nullptr, nullptr});
+    run(2, StageArgs32{S3, X, hi, nullptr, A, S4, nullptr, nullptr});
+    if (full) run(3, StageArgs32{S4, X, hi, lo, A, nullptr, ohi, olo});
     if (sst != NOVA_OK) return sst;
     CKL("stage kernel");
     if (!full) return NOVA_OK;
-    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, ohi, olo, rd->dt,
+    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, ohi, olo, div,
                                     ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
     if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, pbuf);
     if (s != NOVA_OK) return s;
-    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, rd->dt, nullptr, nullptr, ohi, olo,
+    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, div, nullptr, nullptr, ohi, olo,
                        ohi, olo, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
     if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
@@ -1289,6 +1292,8 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
                         nova_field *gradB, double *objective);
 nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
                           double *objective);
+nova_status adjoint_mhd_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
+                              nova_field *gradB, double *objective);
 
 }  // namespace
 
@@ -1300,9 +1305,9 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     const bool mhd = rd->model == NOVA_MODEL_MHD;
     const bool split = rd->precision == NOVA_F32SPLIT;
     if ((rd->model != NOVA_MODEL_NS && !mhd) || rd->rk_mode != NOVA_RK_CLASSICAL ||
-        (rd->precision != NOVA_F64 && !(split && !mhd)))
+        (rd->precision != NOVA_F64 && !split))
         return fail(ctx, NOVA_E_UNSUPPORTED,
-                    "nova_adjoint_grad: built for classical RK4: FP64 or FP32-split Navier-Stokes, FP64 MHD");
+                    "nova_adjoint_grad: built for classical RK4 Navier-Stokes and MHD, FP64 or FP32-split");
     const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
     if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window && !(mhd && ad->objective == NOVA_OBJ_ETOT_FINAL))
         return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective for this model");
@@ -1318,10 +1323,12 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return fail(ctx, NOVA_E_INVALID,
                     "nova_adjoint_grad: U (3 comps, run precision) and gradU (3 comps, FP64) required");
     if (mhd) {
-        if (!valid_field(init->B, 3) || init->B->prec != NOVA_F64 || !gradB || !valid_field(gradB, 3) ||
+        if (!valid_field(init->B, 3) || init->B->prec != rd->precision || !gradB || !valid_field(gradB, 3) ||
             gradB->prec != NOVA_F64)
-            return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: MHD needs FP64 3-component B and gradB");
-        return adjoint_mhd(ctx, ad, init, gradU, gradB, objective);
+            return fail(ctx, NOVA_E_INVALID,
+                        "nova_adjoint_grad: MHD needs B (3 comps, run precision) and gradB (3 comps, FP64)");
+        return split ? adjoint_mhd_split(ctx, ad, init, gradU, gradB, objective)
+                     : adjoint_mhd(ctx, ad, init, gradU, gradB, objective);
     }
     if (gradB) return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: gradB is for MHD runs (pass NULL)");
     if (split) return adjoint_split(ctx, ad, init, gradU, objective);
@@ -1572,7 +1579,7 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
             if ((s = proj(lamB)) != NOVA_OK) return s;
             const double *Up = St(t + 1);
             adj_mhd(BB, 4, AdjArgs{Up, mu, mu, nullptr, gA, Lam}, nullptr);
-            adj_mhd(BU, 4, AdjArgs{slot(t, 7), mu, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BU, 4, AdjArgs{slot(t, 7), mu, mu, nullptr, nullptr, nullptr}, lamU);
             adj_mhd(BB, 3, AdjArgs{Up, gA, mu, Lam, gB, Lam}, nullptr);
             adj_mhd(BU, 3, AdjArgs{slot(t, 6), gA, nullptr, nullptr, nullptr, nullptr}, lamU);
             adj_mhd(BB, 2, AdjArgs{Up, gB, mu, Lam, gA, Lam}, nullptr);
@@ -1582,7 +1589,7 @@ nova_status adjoint_mhd(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state
             // U loop: frozen B^n = SB(t), stage states Y_S
             if ((s = proj(lamU)) != NOVA_OK) return s;
             adj_u(4, AdjArgs{slot(t, 3), mu, mu, nullptr, gA, Lam});
-            adj_mhd(UB, 4, AdjArgs{SB(t), mu, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_mhd(UB, 4, AdjArgs{SB(t), mu, mu, nullptr, nullptr, nullptr}, lamB);
             adj_u(3, AdjArgs{slot(t, 2), gA, mu, Lam, gB, Lam});
             adj_mhd(UB, 3, AdjArgs{SB(t), gA, nullptr, nullptr, nullptr, nullptr}, lamB);
             adj_u(2, AdjArgs{slot(t, 1), gB, mu, Lam, gA, Lam});
@@ -1680,12 +1687,14 @@ nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_sta
             CK(copyf(lo_n0, lo));
         }
         if (kept) {
-            if ((s = rk_loop32(ctx, rd, Y1(t), lo_run, Ys(t, 2), Ys(t, 3), Ys(t, 4), Y1(t + 1), lo_run, pbuf,
-                               true)) != NOVA_OK)
+            if ((s = rk_loop32(ctx, rd, PHYS_NS, rd->nu, rd->dt, Y1(t), lo_run, nullptr, Ys(t, 2), Ys(t, 3),
+                               Ys(t, 4), Y1(t + 1), lo_run, pbuf, true)) != NOVA_OK)
                 return s;
             continue;
         }
-        if ((s = rk_loop32(ctx, rd, hi, lo, w0, w1, w0, runhi, runlo, pbuf, true)) != NOVA_OK) return s;
+        if ((s = rk_loop32(ctx, rd, PHYS_NS, rd->nu, rd->dt, hi, lo, nullptr, w0, w1, w0, runhi, runlo, pbuf,
+                           true)) != NOVA_OK)
+            return s;
         if ((n + 1) % K == 0 && n + 1 < N) {
             CK(copyf(ckhi((n + 1) / K), runhi));
             CK(copyf(cklo((n + 1) / K), runlo));
@@ -1714,8 +1723,8 @@ nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_sta
             CK(copyf(lo_run, cklo(c)));
             for (int t = 0; t < m; t++) {
                 if (n0 + t == n0w) CK(copyf(lo_n0, lo_run));
-                if ((s = rk_loop32(ctx, rd, Y1(t), lo_run, Ys(t, 2), Ys(t, 3), Ys(t, 4), Y1(t + 1), lo_run, pbuf,
-                                   t + 1 < m)) != NOVA_OK)
+                if ((s = rk_loop32(ctx, rd, PHYS_NS, rd->nu, rd->dt, Y1(t), lo_run, nullptr, Ys(t, 2), Ys(t, 3),
+                                   Ys(t, 4), Y1(t + 1), lo_run, pbuf, t + 1 < m)) != NOVA_OK)
                     return s;
             }
         }
@@ -1742,6 +1751,203 @@ nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_sta
     CK(cudaStreamSynchronize(st));
     if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
     const double J = window ? row[NOVA_HIST_COLS + 2] - row[2] : row[2];
+    if (objective) *objective = J;
+    if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
+    return NOVA_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// FP32-split MHD adjoint: the split MHD step of nova_advance (U loop with B's
+// hi part frozen, then the B loop with the new U's hi part frozen, FP64
+// projections), (hi, lo) checkpoints and FP32 stage states; the stage
+// recursions and the coupling transposes in FP32; lamU, lamB and both
+// projections in FP64.  The reverse of a step is that of adjoint_mhd.
+nova_status adjoint_mhd_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_state *init, nova_field *gradU,
+                              nova_field *gradB, double *objective)
+{
+    const nova_run_desc *rd = &ad->run;
+    const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
+    const bool etot = window || ad->objective == NOVA_OBJ_ETOT_FINAL;
+    nova_status s = ensure_work(ctx, NOVA_F32SPLIT);
+    if (s != NOVA_OK) return s;
+    CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
+    const int N = ad->nsteps, K = ad->checkpoint_every;
+    const int nck = (N + K - 1) / K;
+    const int mmax = K < N ? K : N;
+    const size_t V = 3 * (size_t)ctx->g.N3;
+    const size_t Vf = (V + 63) / 64 * 64;
+    // layout: FP64 lamU, lamB, mu, pbuf | FP32: nck (U hi, U lo, B hi, B lo) checkpoints,
+    // per step t: U hi, Y2, Y3, Y4, B hi, Z2, Z3, Z4, then U hi of step mmax,
+    // loU, loB, loU0, loB0, gA, gB, Lam, one more running field
+    const size_t nf = 4 * (size_t)nck + 8 * (size_t)mmax + 1 + 8;
+    if ((s = adj_pool(ctx, 4 * V + (nf * Vf + 1) / 2)) != NOVA_OK) return s;
+    double *lamU = ctx->adj_pool, *lamB = lamU + V, *mu = lamB + V, *pbuf = mu + V;
+    float *fl = reinterpret_cast<float *>(pbuf + V);
+    auto F = [&](size_t i) { return fl + Vf * i; };
+    auto ck = [&](int c, int f) { return F(4 * (size_t)c + f); };  // f: 0 U hi, 1 U lo, 2 B hi, 3 B lo
+    const size_t b1 = 4 * (size_t)nck, b2 = b1 + 8 * (size_t)mmax + 1;
+    auto slot = [&](int t, int f) { return F(b1 + 8 * (size_t)t + f); };
+    auto Uh = [&](int t) { return slot(t, 0); };
+    auto Bh = [&](int t) { return slot(t, 4); };
+    float *loU = F(b2), *loB = F(b2 + 1), *loU0 = F(b2 + 2), *loB0 = F(b2 + 3), *gA = F(b2 + 4), *gB = F(b2 + 5),
+          *Lam = F(b2 + 6), *extra = F(b2 + 7);
+    float *rUh = gA, *rUl = gB, *rBh = Lam, *rBl = extra;  // running state of the forward pass
+    float *w0 = ctx->w32[0], *w1 = ctx->w32[1];
+    cudaStream_t st = ctx->stream;
+    auto copyf = [&](float *dst, const float *src) {
+        return cudaMemcpyAsync(dst, src, sizeof(float) * V, cudaMemcpyDeviceToDevice, st);
+    };
+    auto energy = [&](const float *uh, const float *ul, const float *bh, const float *bl, double *row_dev) {
+        launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, uh, ul, nullptr, bh, bl, 1,
+                    ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
+        ctx->launches += 2;
+    };
+    // one step of the kept or recomputed segment; the B loop is projected
+    // (into bhi, lo in place) unless this is a recomputed segment's last step
+    auto seg_step = [&](int t, int m, float *blast) {
+        nova_status r = rk_loop32(ctx, rd, PHYS_MHD_U, rd->nu, rd->dt, Uh(t), loU, Bh(t), slot(t, 1), slot(t, 2),
+                                  slot(t, 3), Uh(t + 1), loU, pbuf, true);
+        if (r != NOVA_OK) return r;
+        float *bh = t + 1 < m ? Bh(t + 1) : blast;
+        return rk_loop32(ctx, rd, PHYS_MHD_B, rd->eta, 1.0, Bh(t), loB, Uh(t + 1), slot(t, 5), slot(t, 6),
+                         slot(t, 7), bh, loB, pbuf, bh != nullptr);
+    };
+
+    const int c_last = nck - 1, n_last = c_last * K, m_last = N - n_last;
+    CK(copyf(ck(0, 0), init->U->hi));
+    CK(copyf(ck(0, 1), init->U->lo));
+    CK(copyf(ck(0, 2), init->B->hi));
+    CK(copyf(ck(0, 3), init->B->lo));
+    if ((s = dalloc(ctx, &ctx->d_row, 2 * NOVA_HIST_COLS)) != NOVA_OK) return s;
+    const int n0w = window ? ad->window_start : -1;
+    for (int n = 0; n < N; n++) {
+        const bool kept = n >= n_last;
+        const int t = n - n_last;
+        if (kept && t == 0) {
+            CK(copyf(Uh(0), ck(c_last, 0)));
+            CK(copyf(loU, ck(c_last, 1)));
+            CK(copyf(Bh(0), ck(c_last, 2)));
+            CK(copyf(loB, ck(c_last, 3)));
+        }
+        const bool isck = !kept && n % K == 0;
+        const float *uh = kept ? Uh(t) : (isck ? ck(n / K, 0) : rUh);
+        const float *ul = kept ? loU : (isck ? ck(n / K, 1) : rUl);
+        const float *bh = kept ? Bh(t) : (isck ? ck(n / K, 2) : rBh);
+        const float *bl = kept ? loB : (isck ? ck(n / K, 3) : rBl);
+        if (n == n0w) {  // E(n0) of the window: the state before step n0
+            energy(uh, ul, bh, bl, ctx->d_row + NOVA_HIST_COLS);
+            CK(copyf(loU0, ul));
+            CK(copyf(loB0, bl));
+        }
+        if (kept) {
+            if ((s = seg_step(t, m_last, rBh)) != NOVA_OK) return s;
+            continue;
+        }
+        if ((s = rk_loop32(ctx, rd, PHYS_MHD_U, rd->nu, rd->dt, uh, ul, bh, w0, w1, w0, rUh, rUl, pbuf, true)) !=
+            NOVA_OK)
+            return s;
+        if ((s = rk_loop32(ctx, rd, PHYS_MHD_B, rd->eta, 1.0, bh, bl, rUh, w0, w1, w0, rBh, rBl, pbuf, true)) !=
+            NOVA_OK)
+            return s;
+        if ((n + 1) % K == 0 && n + 1 < N) {
+            CK(copyf(ck((n + 1) / K, 0), rUh));
+            CK(copyf(ck((n + 1) / K, 1), rUl));
+            CK(copyf(ck((n + 1) / K, 2), rBh));
+            CK(copyf(ck((n + 1) / K, 3), rBl));
+        }
+    }
+    // E(N); lamU = +-U_N / N^3, lamB = +-B_N / N^3 (or 0 for Ek alone); U_N = (Uh(m_last), loU), B_N = (rBh, loB)
+    energy(Uh(m_last), loU, rBh, loB, ctx->d_row);
+    double row[2 * NOVA_HIST_COLS];
+    CK(cudaMemcpyAsync(row, ctx->d_row, sizeof(row), cudaMemcpyDeviceToHost, st));
+    const double seed = (window ? -1.0 : 1.0) / (double)ctx->g.N3;
+    launch_join((long long)V, Uh(m_last), loU, lamU, st);
+    launch_scale_copy((long long)V, seed, lamU, lamU, st);
+    ctx->launches += 2;
+    if (etot) {
+        launch_join((long long)V, rBh, loB, lamB, st);
+        launch_scale_copy((long long)V, seed, lamB, lamB, st);
+        ctx->launches += 2;
+    } else {
+        CK(cudaMemsetAsync(lamB, 0, sizeof(double) * V, st));
+    }
+    CKL("adjoint seed");
+
+    const float dt = (float)rd->dt;
+    auto adj_u = [&](int stage, const AdjArgs32 &a) {
+        ProfScope ps(ctx, NOVA_K_ADJ);
+        launch_adj_stage32(stage, ctx->g, ctx->co32, ctx->d_ia32, dt, (float)rd->nu, a, st);
+        ctx->launches += 1;
+    };
+    auto adj_mhd = [&](int kind, int stage, const AdjArgs32 &a, double *acc) {
+        ProfScope ps(ctx, NOVA_K_ADJ);
+        launch_adj_mhd32(kind, stage, ctx->g, ctx->co32, ctx->d_ia32, dt, (float)rd->eta, a, acc, st);
+        ctx->launches += 1;
+    };
+    auto proj = [&](const double *in) {
+        ProfScope ps(ctx, NOVA_K_DIV);
+        return project64(ctx, in, mu, pbuf);
+    };
+    enum { UB = 0, BU = 1, BB = 2 };
+    for (int c = nck - 1; c >= 0; c--) {
+        const int n0 = c * K;
+        const int m = (N - n0) < K ? (N - n0) : K;
+        if (c != c_last) {
+            CK(copyf(Uh(0), ck(c, 0)));
+            CK(copyf(loU, ck(c, 1)));
+            CK(copyf(Bh(0), ck(c, 2)));
+            CK(copyf(loB, ck(c, 3)));
+            for (int t = 0; t < m; t++) {
+                if (n0 + t == n0w) {
+                    CK(copyf(loU0, loU));
+                    CK(copyf(loB0, loB));
+                }
+                if ((s = seg_step(t, m, nullptr)) != NOVA_OK) return s;
+            }
+        }
+        for (int t = m - 1; t >= 0; t--) {
+            // B loop: frozen U^{n+1} (its hi part, Uh(t + 1)), stage states Z_S
+            if ((s = proj(lamB)) != NOVA_OK) return s;
+            const float *Up = Uh(t + 1);
+            adj_mhd(BB, 4, AdjArgs32{Up, nullptr, mu, nullptr, gA, Lam, nullptr}, nullptr);
+            adj_mhd(BU, 4, AdjArgs32{slot(t, 7), nullptr, mu, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BB, 3, AdjArgs32{Up, gA, mu, Lam, gB, Lam, nullptr}, nullptr);
+            adj_mhd(BU, 3, AdjArgs32{slot(t, 6), gA, mu, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BB, 2, AdjArgs32{Up, gB, mu, Lam, gA, Lam, nullptr}, nullptr);
+            adj_mhd(BU, 2, AdjArgs32{slot(t, 5), gB, mu, nullptr, nullptr, nullptr, nullptr}, lamU);
+            adj_mhd(BB, 1, AdjArgs32{Up, gA, mu, Lam, nullptr, nullptr, lamB}, nullptr);
+            adj_mhd(BU, 1, AdjArgs32{Bh(t), gA, mu, nullptr, nullptr, nullptr, nullptr}, lamU);
+            // U loop: frozen B^n (its hi part, Bh(t)), stage states Y_S
+            if ((s = proj(lamU)) != NOVA_OK) return s;
+            adj_u(4, AdjArgs32{slot(t, 3), nullptr, mu, nullptr, gA, Lam, nullptr});
+            adj_mhd(UB, 4, AdjArgs32{Bh(t), nullptr, mu, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_u(3, AdjArgs32{slot(t, 2), gA, mu, Lam, gB, Lam, nullptr});
+            adj_mhd(UB, 3, AdjArgs32{Bh(t), gA, mu, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_u(2, AdjArgs32{slot(t, 1), gB, mu, Lam, gA, Lam, nullptr});
+            adj_mhd(UB, 2, AdjArgs32{Bh(t), gB, mu, nullptr, nullptr, nullptr, nullptr}, lamB);
+            adj_u(1, AdjArgs32{Uh(t), gA, mu, Lam, nullptr, nullptr, lamU});
+            adj_mhd(UB, 1, AdjArgs32{Bh(t), gA, mu, nullptr, nullptr, nullptr, nullptr}, lamB);
+            CKL("k_adj_mhd");
+            if (n0 + t == n0w) {  // add dE(n0)/d(U, B)_n0 = (U, B)_n0 / N^3
+                launch_join((long long)V, Uh(t), loU0, pbuf, st);
+                launch_axpy((long long)V, 1.0 / (double)ctx->g.N3, pbuf, lamU, st);
+                launch_join((long long)V, Bh(t), loB0, pbuf, st);
+                launch_axpy((long long)V, 1.0 / (double)ctx->g.N3, pbuf, lamB, st);
+                ctx->launches += 4;
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(gradU->d64, lamU, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(gradB->d64, lamB, sizeof(double) * V, cudaMemcpyDeviceToDevice, st));
+    int perr = 0;
+    CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (perr) return fail(ctx, NOVA_E_TIMEOUT, "nova_adjoint_grad: a stage kernel pipeline wait timed out");
+    const double E = row[2] + (etot ? row[3] : 0.0);
+    const double J = window ? (row[NOVA_HIST_COLS + 2] + row[NOVA_HIST_COLS + 3]) - E : E;
     if (objective) *objective = J;
     if (!std::isfinite(J)) return fail(ctx, NOVA_E_NONFINITE, "nova_adjoint_grad: non-finite objective");
     return NOVA_OK;

@@ -195,9 +195,13 @@ struct AdjArgs32 {
 };
 void launch_adj_stage32(int s, const Geo &g, const Coef<float> &co, const float *ia, float dt, float nu,
                         const AdjArgs32 &a, cudaStream_t st);
-// MHD adjoint stage pieces (nova_adjoint.cu): kind 0 = dF_U/dB (lambda_B += ...),
-// 1 = dF_B/dU (lambda_U += ...), 2 = dF_B/dB with the reverse RK4 recursion;
-// a.Y = the field in the transpose (B^n, Z_S or U^{n+1}), a.G = g_S
+// FP32 MHD coupling transposes (tiled): kind 0, 1, 2 as launch_adj_mhd; acc FP64
+void launch_adj_mhd32(int kind, int s, const Geo &g, const Coef<float> &co, const float *ia, float dt, float visc,
+                      const AdjArgs32 &a, double *acc, cudaStream_t st);
+// MHD adjoint stage pieces (nova_adjoint.cu, nova_adj_tma.cu): kind 0 = dF_U/dB
+// (lambda_B += ...), 1 = dF_B/dU (lambda_U += ...), 2 = dF_B/dB with the
+// reverse RK4 recursion; a.Y = the field in the transpose (B^n, Z_S or
+// U^{n+1}), a.G = g_S; at s = 4 the direction is mu/6 and a.mu and a.G are mu
 cudaError_t launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co, const double *ia, double dt,
                            double visc, const AdjArgs &a, double *acc, cudaStream_t st, int *err = nullptr);
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);  // y = a x

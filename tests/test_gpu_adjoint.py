@@ -325,3 +325,53 @@ def test_tma_adjoint_equals_tiled(nova, oracle, N, model):
             grads[impl] = [r[1].download_soa()]
     for a, b in zip(grads["auto"], grads["march"]):
         assert rel_l2(a, b) < 1e-13, rel_l2(a, b)
+
+
+def split_mhd_energies(nova, N, U0, B0, dt, nu, eta, nsteps):
+    GM = nova.Mesh(N)
+    U, B = nova.Field(GM, 3, nova.F32SPLIT).upload_soa(U0), nova.Field(GM, 3, nova.F32SPLIT).upload_soa(B0)
+    nova.advance(GM, nova.run_desc(model="mhd", rk_mode="classical", precision=nova.F32SPLIT, dt=dt, nu=nu, eta=eta,
+                                   diag_every=0), U, nova.Field(GM, 1), B, nova.Field(GM, 1), nsteps=nsteps,
+                 history=False)
+    return energies(U.download_soa(), B.download_soa(), N)
+
+
+@pytest.mark.parametrize("N", [(16, 16, 16), (16, 16, 32)])
+def test_split_mhd_adjoint_matches_fp64(nova, oracle, N):
+    nsteps, nu, eta = 6, 1e-2, 2e-2
+    U0, B0, dt = mhd_base(oracle, N, seed=12)
+    GM = nova.Mesh(N)
+    kw = dict(model="mhd", rk_mode="classical", dt=dt, nu=nu, eta=eta)
+    U64, B64 = nova.Field(GM, 3).upload_soa(U0), nova.Field(GM, 3).upload_soa(B0)
+    U32, B32 = (nova.Field(GM, 3, nova.F32SPLIT).upload_soa(U0), nova.Field(GM, 3, nova.F32SPLIT).upload_soa(B0))
+    J64, gu64, gb64 = nova.adjoint_grad(GM, nova.run_desc(**kw), U64, nsteps, checkpoint_every=4, B0=B64,
+                                        total_energy=True)
+    J32, gu32, gb32 = nova.adjoint_grad(GM, nova.run_desc(precision=nova.F32SPLIT, **kw), U32, nsteps,
+                                        checkpoint_every=4, B0=B32, total_energy=True)
+    assert J32 == pytest.approx(sum(split_mhd_energies(nova, N, U0, B0, dt, nu, eta, nsteps)), rel=1e-13)
+    assert J32 == pytest.approx(J64, rel=1e-6)
+    for a, b in ((gu32, gu64), (gb32, gb64)):
+        e = rel_l2(a.download_soa(), b.download_soa())
+        assert 1e-12 < e < SPLIT_TOL, e
+
+
+def test_split_mhd_adjoint_checkpoints_and_window(nova, oracle):
+    N = (16, 16, 32)
+    nsteps, n0 = 7, 3
+    U0, B0, dt = mhd_base(oracle, N, seed=13)
+    GM = nova.Mesh(N)
+    kw = dict(model="mhd", rk_mode="classical", dt=dt, nu=1e-2, eta=1e-2)
+    U32, B32 = (nova.Field(GM, 3, nova.F32SPLIT).upload_soa(U0), nova.Field(GM, 3, nova.F32SPLIT).upload_soa(B0))
+    rd32 = nova.run_desc(precision=nova.F32SPLIT, **kw)
+    runs = [nova.adjoint_grad(GM, rd32, U32, nsteps, checkpoint_every=k, B0=B32) for k in (1, 3, 50)]
+    for r in runs[1:]:
+        assert r[0] == runs[0][0]
+        assert rel_l2(r[1].download_soa(), runs[0][1].download_soa()) < 1e-14
+        assert rel_l2(r[2].download_soa(), runs[0][2].download_soa()) < 1e-14
+    U64, B64 = nova.Field(GM, 3).upload_soa(U0), nova.Field(GM, 3).upload_soa(B0)
+    J32, u32, b32 = nova.adjoint_grad(GM, rd32, U32, nsteps, checkpoint_every=2, window_start=n0, B0=B32)
+    J64, u64, b64 = nova.adjoint_grad(GM, nova.run_desc(**kw), U64, nsteps, checkpoint_every=2, window_start=n0,
+                                      B0=B64)
+    assert J32 == pytest.approx(J64, rel=1e-5)
+    assert rel_l2(u32.download_soa(), u64.download_soa()) < SPLIT_TOL
+    assert rel_l2(b32.download_soa(), b64.download_soa()) < SPLIT_TOL
