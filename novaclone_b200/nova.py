@@ -424,8 +424,8 @@ def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_eve
     (MHD) Ek + Em; with window_start = n0 the dissipation over steps n0+1..nsteps,
     E(n0) - E(nsteps) (E = Ek, or Ek + Em for MHD).  Returns (J, dJ/dU0) for
     Navier-Stokes and (J, dJ/dU0, dJ/dB0) for MHD (rd.model MHD, B0 given).
-    With rd.precision F32SPLIT (Navier-Stokes; U0 a split field) the trajectory is
-    the split path's and the adjoint stages run in FP32; the gradient is FP64."""
+    With rd.precision F32SPLIT (U0, B0 split fields) the trajectory is the split
+    path's and the adjoint stages run in FP32; the gradients are FP64."""
     a = AdjDesc()
     a.run = rd
     a.nsteps = int(nsteps)
