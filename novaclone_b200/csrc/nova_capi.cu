@@ -944,7 +944,8 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             ctx->launches += taken ? 2 : 1;
             if (first && dg && !taken) {
                 launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, Y->d64, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st);
+                            nullptr, nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st,
+                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
                 ctx->launches += 2;
             }
         };
@@ -1006,7 +1007,8 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         fixpair(Y->hi, Y->lo);
         if (dg) {
             launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, nullptr, Y->hi, Y->lo, nullptr,
-                        nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st);
+                        nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st,
+                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
             ctx->launches += 2;
         }
         const float *Ushi, *Uslo;
@@ -1137,7 +1139,8 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
                         B ? B->d64 : nullptr,
                         B ? B->hi : nullptr, B ? B->lo : nullptr, mhd ? 1 : 0, ctx->d_part, (double)(n + 1),
                         rd->t0 + (n + 1) * rd->dt, ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag,
-                        ctx->stream);
+                        ctx->stream,
+                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
             ctx->launches += 2;
             CKL("k_diag");
         }
@@ -1360,7 +1363,8 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     const int n0w = window ? ad->window_start : -1;
     auto ekin = [&](const double *u, double *row_dev) {  // diagnostics row of the state u
         launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, u, nullptr, nullptr, nullptr, nullptr,
-                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
+                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st,
+                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
         ctx->launches += 2;
     };
     for (int n = 0; n < N; n++) {
@@ -1663,7 +1667,8 @@ nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_sta
     };
     auto energy = [&](const float *hi, const float *lo, double *row_dev) {
         launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, hi, lo, nullptr, nullptr,
-                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
+                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st,
+                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
         ctx->launches += 2;
     };
 

@@ -782,8 +782,16 @@ int diag_blocks(const Geo &g)
 void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                  const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
                  const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,
-                 cudaStream_t st)
+                 cudaStream_t st, const StageExec &ex)
 {
+    const double invN3 = 1.0 / (double)((long long)g.N0 * (g.N1 - g.wallY) * g.N2);
+    if (ex.err && h == 3 && !wl.on && !hasB && ex.impl != STAGE_MARCH && proj_tma_fits(g)) {
+        const int nb = launch_diag_tma(g, co, ia, U64, Uhi, Ulo, part, diag_blocks(g), ex.err, st);
+        if (nb > 0) {
+            k_diag_final<<<1, 256, 0, st>>>(part, nb, invN3, step, time, row, flag);
+            return;
+        }
+    }
     const int ch = pick_ichunk(g, 2);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     const int nb = (int)(grid.x * grid.y * grid.z);

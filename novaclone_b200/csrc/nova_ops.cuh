@@ -51,10 +51,16 @@ int diag_blocks(const Geo &g);
 // the history row from nb blocks of partials (Ek, Em, max|div U|, max|div B| per block)
 void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
                        cudaStream_t st);
+// ex: with its error word, a Navier-Stokes field on a mesh the TMA projection
+// kernels fit takes the TMA diagnostics pass (nova_proj_tma.cu)
 void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                  const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
                  const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,
-                 cudaStream_t st);
+                 cudaStream_t st, const StageExec &ex = StageExec{STAGE_MARCH, nullptr});
+// Ek and max|div U| partials of one field by the TMA divergence loads: the
+// number of blocks written, 0 where the grid exceeds cap blocks (nothing launched)
+int launch_diag_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *hi,
+                    const float *lo, double *part, int cap, int *err, cudaStream_t st);
 void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st);
 void launch_op(int op, int h, const Geo &g, const Walls<double> &wa, const Walls<double> &wb, const Coef<double> &co,
                const double *ia, const double *corr2, const double *a, const double *b, int nc, double nu, double *out,

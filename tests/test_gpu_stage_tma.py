@@ -87,9 +87,10 @@ def test_tma_taylor_green_vs_oracle(nova, oracle):
 
 
 def test_adjoint_through_tma_equals_march(nova):
-    """The forward passes agree bit for bit (J); the reverse stages of the TMA
-    adjoint apply the first stage's 1/6 to xi instead of to g, so the gradients
-    agree to rounding."""
+    """The forward passes agree bit for bit; J comes from the TMA or the tiled
+    diagnostics reduction (different summation order), and the reverse stages
+    of the TMA adjoint apply the first stage's 1/6 to xi instead of to g, so J
+    and the gradients agree to rounding."""
     N = (16, 32, 32)
     U0 = 0.2 * np.random.default_rng(9).standard_normal((3,) + N)
     out = []
@@ -98,7 +99,7 @@ def test_adjoint_through_tma_equals_march(nova):
         J, grad = nova.adjoint_grad(GM, nova.run_desc(model="ns", dt=2e-3, nu=0.01), nova.Field(GM, 3).upload_soa(U0),
                                     nsteps=4, checkpoint_every=2)
         out.append((J, grad.download_soa()))
-    assert out[0][0] == out[1][0]
+    assert out[0][0] == pytest.approx(out[1][0], rel=1e-14)
     assert rel_l2(out[0][1], out[1][1]) < 1e-13
 
 
