@@ -213,6 +213,50 @@ typedef struct {
 nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *adj, const nova_state *init, nova_field *gradU,
                               nova_field *gradB, double *objective);
 
+/* ---- implicit operators (src/im) ----
+ * nova_fdm is the reference's fdMatrix<scalar> (src/im/fdMatrix/fdMatrix.h:33-77)
+ * on a periodic uniform mesh: per-node coefficients al[0..5] of the neighbours
+ * j+1, j-1, i+1, i-1, k+1, k-1 (N, S, E, W, T, B), the centre ap and the
+ * source b, for A x = b with (A x)_n = ap x_n + sum_l al_l x_{n+l}, and the
+ * transported FP64 scalar field x it solves for (kept by pointer, as the
+ * reference keeps its shared_ptr). */
+typedef struct nova_fdm nova_fdm;
+/* im::laplacian(mu, x) (src/im/laplacian/laplacian.hxx:24-58): al = mu/d^2,
+ * ap = -2 mu sum 1/d^2, b = -ex::laplacian(mu, x) + A x (the deferred
+ * correction, src/im/fdMatrix/fdMatrix.hxx:201-225) */
+nova_status nova_im_laplacian(nova_ctx *ctx, double mu, nova_field *x, nova_fdm **out);
+/* a += alpha b, coefficients and source (operator+= / -=, fdMatrix.hxx:311-339; operator+ / binary operator-, 359-369, 383-393) */
+nova_status nova_fdm_add(nova_ctx *ctx, nova_fdm *a, double alpha, const nova_fdm *b);
+/* a *= b node by node, coefficients and source (operator*=, fdMatrix.hxx:341-354) */
+nova_status nova_fdm_mul(nova_ctx *ctx, nova_fdm *a, const nova_fdm *b);
+/* coefficients and source times s (s = -1: the unary operator-, fdMatrix.hxx:395-413) */
+nova_status nova_fdm_scale(nova_ctx *ctx, nova_fdm *a, double s);
+/* b += alpha f (operator== with alpha = 1, fdMatrix.hxx:371-381); f: FP64 scalar */
+nova_status nova_fdm_add_source(nova_ctx *ctx, nova_fdm *a, double alpha, const nova_field *f);
+/* ap += d (Field arithmetic on fdMatrix::ap()) */
+nova_status nova_fdm_add_diagonal(nova_ctx *ctx, nova_fdm *a, double d);
+/* fdMatrix::relax(urf) (fdMatrix.hxx:227-232): b += (1 - urf)/urf ap x, ap /= urf; urf > 0 */
+nova_status nova_fdm_relax(nova_ctx *ctx, nova_fdm *a, double urf);
+/* fdMatrix::setReference (fdMatrix.hxx:235-246) at the unique node (i, j, k): b += 1e15 val, ap *= 1e15 */
+nova_status nova_fdm_set_reference(nova_ctx *ctx, nova_fdm *a, int i, int j, int k, double val);
+/* fdMatrix::residual (fdMatrix.hxx:249-290): the RMS of b - A x over the
+ * (N0+1)(N1+1)(N2+1) nodes the reference counts (the duplicate periodic
+ * nodes included) */
+nova_status nova_fdm_residual(nova_ctx *ctx, const nova_fdm *a, double *res);
+/* fdMatrix::solve(tol, max_its) (fdMatrix.hxx:59-198): per iteration the
+ * residual check (stop when not above tol), then line sweeps along j, i and k
+ * on x.  Every line of a sweep is solved at once as a periodic tridiagonal
+ * system with the neighbours off the line taken at the sweep's start, where
+ * the reference solves the lines one after another (Gauss-Seidel across
+ * lines), each as a Dirichlet problem whose ghost and duplicate end nodes keep
+ * their values from the last ghost refresh (once per iteration): a different
+ * iteration with the same fixed point.  its, res (the last residual checked)
+ * may be NULL. */
+nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, int max_its, int *its, double *res);
+/* the eight fields to the host, SoA over the unique nodes: al0..al5, ap, b (8 x N0 N1 N2 doubles) */
+nova_status nova_fdm_download(nova_ctx *ctx, const nova_fdm *a, double *host);
+nova_status nova_fdm_destroy(nova_fdm *a);
+
 /* ---- weakly-compressible time advance ----
  * One call = nsteps of the compressible loop bodies on a periodic mesh, FP64:
  *   NOVA_WC_TG:    app/TG/TG.cpp:73-75          rhoEqn.H, pEqn.H (p = K (rho rho), K = 50), UEqn.H

@@ -1960,6 +1960,210 @@ nova_status adjoint_mhd_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova
 
 }  // namespace
 
+// ======================================================= implicit operators ==
+// fdMatrix<scalar> of src/im (kernels in nova_im.cu): coef = [al0..al5 | ap | b]
+struct nova_fdm {
+    nova_ctx *ctx = nullptr;
+    nova_field *x = nullptr;     // the transported field (not owned)
+    double *coef = nullptr;      // 8 x N3
+    double *scratch = nullptr;   // the solve's line scratch (3 N3) and its second x buffer (N3)
+};
+
+namespace {
+
+nova_status fdm_check(nova_ctx *ctx, const nova_fdm *a, const char *what)
+{
+    if (!ctx || !a || a->ctx != ctx || !a->coef) return fail(ctx, NOVA_E_INVALID, what);
+    return NOVA_OK;
+}
+
+bool fdm_mesh_ok(const nova_ctx *ctx) { return !ctx->g.wallY && !ctx->md.hyperbolic_z; }
+
+}  // namespace
+
+extern "C" nova_status nova_im_laplacian(nova_ctx *ctx, double mu, nova_field *x, nova_fdm **out)
+{
+    if (!ctx || !x || !out) return fail(ctx, NOVA_E_INVALID, "nova_im_laplacian: null argument");
+    *out = nullptr;
+    if (!valid_field(x, 1) || x->prec != NOVA_F64)
+        return fail(ctx, NOVA_E_INVALID, "nova_im_laplacian: x must be an FP64 scalar field");
+    if (!fdm_mesh_ok(ctx)) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_im_laplacian: periodic uniform meshes only");
+    const Geo &g = ctx->g;
+    if (g.N0 < 3 || g.N1 < 3 || g.N2 < 3)
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_im_laplacian: at least 3 nodes per direction");
+    nova_fdm *a = new (std::nothrow) nova_fdm;
+    if (!a) return fail(ctx, NOVA_E_OOM, "nova_im_laplacian: out of host memory");
+    a->ctx = ctx;
+    a->x = x;
+    nova_status s = dalloc(ctx, &a->coef, 8 * (size_t)g.N3);
+    if (s != NOVA_OK) {
+        delete a;
+        return s;
+    }
+    const double dx = ctx->md.L[0] / ctx->md.N[0], dy = ctx->md.L[1] / ctx->md.N[1],
+                 dz = ctx->md.L[2] / ctx->md.N[2];
+    // the deferred correction's ex::laplacian goes through the source slot (read, then overwritten per node)
+    launch_fdm_laplacian(g, ctx->co64, ctx->d_ia64, ctx->d_corr64, ctx->h, mu, dx, dy, dz, x->d64,
+                         a->coef + 7 * (size_t)g.N3, a->coef, ctx->stream);
+    ctx->launches += 3;
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(a->coef);
+        delete a;
+        return cuda_check(ctx, e, "nova_im_laplacian");
+    }
+    *out = a;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_add(nova_ctx *ctx, nova_fdm *a, double alpha, const nova_fdm *b)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_add: bad matrix")) != NOVA_OK) return s;
+    if ((s = fdm_check(ctx, b, "nova_fdm_add: bad matrix")) != NOVA_OK) return s;
+    launch_fdm_algebra(ctx->g, 0, alpha, a->coef, b->coef, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_mul(nova_ctx *ctx, nova_fdm *a, const nova_fdm *b)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_mul: bad matrix")) != NOVA_OK) return s;
+    if ((s = fdm_check(ctx, b, "nova_fdm_mul: bad matrix")) != NOVA_OK) return s;
+    launch_fdm_algebra(ctx->g, 1, 0.0, a->coef, b->coef, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_scale(nova_ctx *ctx, nova_fdm *a, double sc)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_scale: bad matrix")) != NOVA_OK) return s;
+    launch_fdm_algebra(ctx->g, 2, sc, a->coef, nullptr, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_add_source(nova_ctx *ctx, nova_fdm *a, double alpha, const nova_field *f)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_add_source: bad matrix")) != NOVA_OK) return s;
+    if (!valid_field(f, 1) || f->prec != NOVA_F64)
+        return fail(ctx, NOVA_E_INVALID, "nova_fdm_add_source: f must be an FP64 scalar field");
+    launch_fdm_point(ctx->g, 0, alpha, a->coef, f->d64, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_add_diagonal(nova_ctx *ctx, nova_fdm *a, double d)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_add_diagonal: bad matrix")) != NOVA_OK) return s;
+    launch_fdm_point(ctx->g, 1, d, a->coef, nullptr, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_relax(nova_ctx *ctx, nova_fdm *a, double urf)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_relax: bad matrix")) != NOVA_OK) return s;
+    if (!(urf > 0.0)) return fail(ctx, NOVA_E_INVALID, "nova_fdm_relax: urf must be positive");
+    launch_fdm_point(ctx->g, 2, urf, a->coef, a->x->d64, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_set_reference(nova_ctx *ctx, nova_fdm *a, int i, int j, int k, double val)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_set_reference: bad matrix")) != NOVA_OK) return s;
+    const Geo &g = ctx->g;
+    if (i < 0 || i >= g.N0 || j < 0 || j >= g.N1 || k < 0 || k >= g.N2)
+        return fail(ctx, NOVA_E_INVALID, "nova_fdm_set_reference: node outside the mesh");
+    launch_fdm_setref(g, a->coef, ((long long)i * g.N1 + j) * g.N2 + k, val, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+namespace {
+
+nova_status fdm_res(nova_ctx *ctx, const nova_fdm *a, const double *x, double *res)
+{
+    nova_status s = ensure_red(ctx);
+    if (s != NOVA_OK) return s;
+    const int nb = 592;  // <= the partials the diagnostics reserve (diag_blocks(g) * 4 >= 1184 * 4)
+    launch_fdm_residual(ctx->g, a->coef, x, ctx->d_part, nb, ctx->d_scalar, ctx->stream);
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(res, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+}  // namespace
+
+extern "C" nova_status nova_fdm_residual(nova_ctx *ctx, const nova_fdm *a, double *res)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_residual: bad matrix")) != NOVA_OK) return s;
+    if (!res) return fail(ctx, NOVA_E_INVALID, "nova_fdm_residual: null argument");
+    return fdm_res(ctx, a, a->x->d64, res);
+}
+
+extern "C" nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, int max_its, int *its, double *res)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_solve: bad matrix")) != NOVA_OK) return s;
+    if (max_its < 0) return fail(ctx, NOVA_E_INVALID, "nova_fdm_solve: max_its must not be negative");
+    const Geo &g = ctx->g;
+    if ((s = dalloc(ctx, &a->scratch, 4 * (size_t)g.N3)) != NOVA_OK) return s;
+    double *x = a->x->d64, *xt = a->scratch + 3 * (size_t)g.N3;
+    double r = 0.0;
+    int n = 0;
+    if ((s = fdm_res(ctx, a, x, &r)) != NOVA_OK) return s;
+    while (n < max_its) {
+        if ((s = fdm_res(ctx, a, x, &r)) != NOVA_OK) return s;
+        if (!(r > tol)) break;
+        n++;
+        launch_fdm_sweep(1, g, a->coef, x, xt, a->scratch, ctx->stream);   // j lines
+        launch_fdm_sweep(0, g, a->coef, xt, x, a->scratch, ctx->stream);   // i lines
+        launch_fdm_sweep(2, g, a->coef, x, xt, a->scratch, ctx->stream);   // k lines
+        CK(cudaMemcpyAsync(x, xt, sizeof(double) * g.N3, cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->launches += 3;
+        CKL("k_fdm_sweep");
+    }
+    if (its) *its = n;
+    if (res) *res = r;
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_download(nova_ctx *ctx, const nova_fdm *a, double *host)
+{
+    nova_status s;
+    if ((s = fdm_check(ctx, a, "nova_fdm_download: bad matrix")) != NOVA_OK) return s;
+    if (!host) return fail(ctx, NOVA_E_INVALID, "nova_fdm_download: null argument");
+    CK(cudaMemcpyAsync(host, a->coef, sizeof(double) * 8 * ctx->g.N3, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return NOVA_OK;
+}
+
+extern "C" nova_status nova_fdm_destroy(nova_fdm *a)
+{
+    if (!a) return NOVA_OK;
+    if (a->coef) cudaFree(a->coef);
+    if (a->scratch) cudaFree(a->scratch);
+    delete a;
+    return NOVA_OK;
+}
+
 // ========================================================= weakly compressible ==
 extern "C" nova_status nova_advance_wc(nova_ctx *ctx, const nova_wc_desc *wd, nova_wc_state *st, int nsteps,
                                        double *hist)

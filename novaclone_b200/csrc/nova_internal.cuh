@@ -165,6 +165,38 @@ struct StageArgs32 {
 enum Physics { PHYS_NS = 0, PHYS_MHD_U = 1, PHYS_MHD_B = 2 };
 
 // reverse RK4 stage of the discrete adjoint (nova_adjoint.cu)
+// block-wide sum / max (blockDim.x a multiple of 32, sh >= 32 entries); the
+// result is valid in thread 0
+template <typename T>
+__device__ __forceinline__ T block_reduce_sum(T v, T *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    T r = 0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) r += sh[q];
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_reduce_max(T v, T *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    T r = 0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) r = fmax(r, sh[q]);
+    return r;
+}
+
 struct AdjArgs {
     const double *Y;    // forward stage state Y_s (3 comps, halo'd)
     const double *G;    // adjoint stage direction g_s (halo'd); mu itself at s = 4

@@ -191,35 +191,6 @@ __global__ void k_restrict_rows(Geo g, int ny, const double *__restrict__ ext, d
 // ------------------------------------------------------------- diagnostics --
 constexpr int kRedThreads = 256;
 
-template <typename T>
-__device__ __forceinline__ T block_reduce_sum(T v, T *sh)
-{
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    __syncthreads();
-    if (lane == 0) sh[w] = v;
-    __syncthreads();
-    T r = 0;
-    if (threadIdx.x == 0)
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) r += sh[q];
-    return r;
-}
-
-template <typename T>
-__device__ __forceinline__ T block_reduce_max(T v, T *sh)
-{
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    __syncthreads();
-    if (lane == 0) sh[w] = v;
-    __syncthreads();
-    T r = 0;
-    if (threadIdx.x == 0)
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) r = fmax(r, sh[q]);
-    return r;
-}
 
 // per-block partials: [0] sum 1/2|U|^2, [1] sum 1/2|B|^2, [2] max|div U|, [3] max|div B|
 // Energies sum the unique nodes as app/TG_Piosson/TG.cpp:148-166 does (the

@@ -48,6 +48,20 @@ cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const doubl
                                const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi,
                                float *lo, int *err, cudaStream_t st);
 int diag_blocks(const Geo &g);
+// implicit operators (nova_im.cu): coef = 8 FP64 fields [al0..al5 | ap | b]
+void launch_fdm_laplacian(const Geo &g, const Coef<double> &co, const double *ia, const double *corr2, int h,
+                          double mu, double dx, double dy, double dz, const double *x, double *hoa, double *coef,
+                          cudaStream_t st);
+// mode 0: a += alpha b, 1: a *= b, 2: a *= alpha (all eight fields)
+void launch_fdm_algebra(const Geo &g, int mode, double alpha, double *a, const double *b, cudaStream_t st);
+// mode 0: b += v f, 1: ap += v, 2: relax with urf = v (f = x)
+void launch_fdm_point(const Geo &g, int mode, double v, double *coef, const double *f, cudaStream_t st);
+void launch_fdm_setref(const Geo &g, double *coef, long long n, double val, cudaStream_t st);
+void launch_fdm_residual(const Geo &g, const double *coef, const double *x, double *part, int nb, double *out,
+                         cudaStream_t st);
+// one sweep of periodic tridiagonal line solves along axis; scratch: 3 N3 doubles
+void launch_fdm_sweep(int axis, const Geo &g, const double *coef, const double *xin, double *xout, double *scratch,
+                      cudaStream_t st);
 // the history row from nb blocks of partials (Ek, Em, max|div U|, max|div B| per block)
 void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
                        cudaStream_t st);

@@ -42,7 +42,9 @@ EXPORTS = (
     "nova_wc_hydrostatic", "nova_checkpoint_write", "nova_checkpoint_read", "nova_ensight_write_geometry",
     "nova_ensight_write_case", "nova_ensight_write_host", "nova_ensight_read_host", "nova_ensight_write_field",
     "nova_ensight_read_field", "nova_profile_enable", "nova_profile_read",
-    "nova_launch_count",
+    "nova_launch_count", "nova_im_laplacian", "nova_fdm_add", "nova_fdm_mul", "nova_fdm_scale",
+    "nova_fdm_add_source", "nova_fdm_add_diagonal", "nova_fdm_relax", "nova_fdm_set_reference",
+    "nova_fdm_residual", "nova_fdm_solve", "nova_fdm_download", "nova_fdm_destroy",
 )
 
 
@@ -141,6 +143,18 @@ def load_library(path: str = LIB_PATH):
         "nova_profile_enable": [vp, C.c_int],
         "nova_profile_read": [vp, C.c_int, dp, C.POINTER(C.c_long), C.c_int],
         "nova_launch_count": [vp, C.POINTER(C.c_long), C.c_int],
+        "nova_im_laplacian": [vp, C.c_double, vp, C.POINTER(C.c_void_p)],
+        "nova_fdm_add": [vp, vp, C.c_double, vp],
+        "nova_fdm_mul": [vp, vp, vp],
+        "nova_fdm_scale": [vp, vp, C.c_double],
+        "nova_fdm_add_source": [vp, vp, C.c_double, vp],
+        "nova_fdm_add_diagonal": [vp, vp, C.c_double],
+        "nova_fdm_relax": [vp, vp, C.c_double],
+        "nova_fdm_set_reference": [vp, vp, C.c_int, C.c_int, C.c_int, C.c_double],
+        "nova_fdm_residual": [vp, vp, dp],
+        "nova_fdm_solve": [vp, vp, C.c_double, C.c_int, ip, dp],
+        "nova_fdm_download": [vp, vp, dp],
+        "nova_fdm_destroy": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -375,6 +389,83 @@ class poisson:
     def solve(self):
         M = self.p.mesh
         M.check(M.lib.nova_poisson_solve(M.h, self._rhs.h, self.p.h))
+
+
+class FdMatrix:
+    """The reference's fdMatrix<scalar> (src/im/fdMatrix): per-node coefficients
+    al[0..5] (neighbours j+1, j-1, i+1, i-1, k+1, k-1), ap and the source b of
+    A x = b, and the transported field x that solve() updates in place."""
+
+    def __init__(self, mesh: Mesh, x: Field, h):
+        self.mesh, self.x, self.h = mesh, x, h
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.mesh.lib is not None:
+            self.mesh.lib.nova_fdm_destroy(self.h)
+            self.h = None
+
+    def add(self, other: "FdMatrix", alpha: float = 1.0) -> "FdMatrix":
+        """self += alpha other (operator+ / operator-)"""
+        self.mesh.check(self.mesh.lib.nova_fdm_add(self.mesh.h, self.h, float(alpha), other.h))
+        return self
+
+    def mul(self, other: "FdMatrix") -> "FdMatrix":
+        """self *= other node by node (operator*=)"""
+        self.mesh.check(self.mesh.lib.nova_fdm_mul(self.mesh.h, self.h, other.h))
+        return self
+
+    def scale(self, s: float) -> "FdMatrix":
+        """coefficients and source times s (s = -1: unary operator-)"""
+        self.mesh.check(self.mesh.lib.nova_fdm_scale(self.mesh.h, self.h, float(s)))
+        return self
+
+    def eq(self, f: Field, alpha: float = 1.0) -> "FdMatrix":
+        """operator==: the source += alpha f"""
+        self.mesh.check(self.mesh.lib.nova_fdm_add_source(self.mesh.h, self.h, float(alpha), f.h))
+        return self
+
+    def add_diagonal(self, d: float) -> "FdMatrix":
+        """ap() += d"""
+        self.mesh.check(self.mesh.lib.nova_fdm_add_diagonal(self.mesh.h, self.h, float(d)))
+        return self
+
+    def relax(self, urf: float) -> "FdMatrix":
+        self.mesh.check(self.mesh.lib.nova_fdm_relax(self.mesh.h, self.h, float(urf)))
+        return self
+
+    def set_reference(self, i: int, j: int, k: int, val: float) -> "FdMatrix":
+        self.mesh.check(self.mesh.lib.nova_fdm_set_reference(self.mesh.h, self.h, int(i), int(j), int(k),
+                                                             float(val)))
+        return self
+
+    def residual(self) -> float:
+        r = C.c_double()
+        self.mesh.check(self.mesh.lib.nova_fdm_residual(self.mesh.h, self.h, C.byref(r)))
+        return r.value
+
+    def solve(self, tol: float, max_its: int):
+        """Line relaxation on x until the residual is not above tol; returns (iterations, residual)."""
+        its, r = C.c_int(), C.c_double()
+        self.mesh.check(self.mesh.lib.nova_fdm_solve(self.mesh.h, self.h, float(tol), int(max_its), C.byref(its),
+                                                     C.byref(r)))
+        return its.value, r.value
+
+    def download(self):
+        """(al (6, N0, N1, N2), ap, b) on the unique nodes"""
+        out = np.zeros((8,) + tuple(self.mesh.N))
+        self.mesh.check(self.mesh.lib.nova_fdm_download(self.mesh.h, self.h, _dptr(out)))
+        return out[:6], out[6], out[7]
+
+
+class im:
+    """The reference's implicit operators (src/im)."""
+
+    @staticmethod
+    def laplacian(mu: float, x: Field) -> FdMatrix:
+        M = x.mesh
+        h = C.c_void_p()
+        M.check(M.lib.nova_im_laplacian(M.h, float(mu), x.h, C.byref(h)))
+        return FdMatrix(M, x, h)
 
 
 class tools:

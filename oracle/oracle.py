@@ -533,6 +533,135 @@ def ref_ops2(mesh, T, S, s, nu, U):
         return {k: np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (nc,)) for k, nc in names.items()}
 
 
+# ------------------------------------------------------- implicit operators --
+
+def im_laplacian(mesh, mu, xg):
+    """im::laplacian(mu, x) (src/im/laplacian/laplacian.hxx:24-58) for a ghosted
+    scalar x (periodic images filled): the 7-point coefficients al[0..5] (the
+    neighbours j+1, j-1, i+1, i-1, k+1, k-1) and ap on the interior nodes, and
+    the source of the deferred correction (src/im/fdMatrix/fdMatrix.hxx:201-225)
+    src = -ex::laplacian(mu, x) + sum_l al_l x(neighbour l) + ap x, summed in that
+    order.  Ghost entries are 0, as in the reference's pooled fields."""
+    n, h = mesh.n, mesh.h
+    dx, dy, dz = mesh.d
+    x = xg[..., 0] if xg.ndim == 4 else xg
+    I, J, K = slice(h, n[0] - h), slice(h, n[1] - h), slice(h, n[2] - h)
+    al = np.zeros((6,) + n)
+    ap = np.zeros(n)
+    src = np.zeros(n)
+    for l, d in ((0, dy), (1, dy), (2, dx), (3, dx), (4, dz), (5, dz)):
+        al[l][I, J, K] = mu / (d * d)
+    ap[I, J, K] = -2.0 * mu / (dx * dx) - 2.0 * mu / (dy * dy) - 2.0 * mu / (dz * dz)
+    hoa = lap(mesh, mu, x[..., None])[..., 0]
+
+    def sh(di, dj, dk):
+        return x[h + di:n[0] - h + di, h + dj:n[1] - h + dj, h + dk:n[2] - h + dk]
+    c = [a[I, J, K] for a in al]
+    src[I, J, K] = (((((((-hoa[I, J, K] + c[0] * sh(0, 1, 0)) + c[1] * sh(0, -1, 0)) + c[2] * sh(1, 0, 0)) +
+                        c[3] * sh(-1, 0, 0)) + c[4] * sh(0, 0, 1)) + c[5] * sh(0, 0, -1)) + ap[I, J, K] * sh(0, 0, 0))
+    return al, ap, src
+
+
+def fdm_residual(mesh, al, ap, src, xg):
+    """fdMatrix::residual (fdMatrix.hxx:249-290) for a scalar: the RMS of
+    src - sum_l al_l x(neighbour l) - ap x over the interior nodes, the duplicate
+    periodic nodes included."""
+    n, h = mesh.n, mesh.h
+    x = xg[..., 0] if xg.ndim == 4 else xg
+    I, J, K = slice(h, n[0] - h), slice(h, n[1] - h), slice(h, n[2] - h)
+
+    def sh(di, dj, dk):
+        return x[h + di:n[0] - h + di, h + dj:n[1] - h + dj, h + dk:n[2] - h + dk]
+    r = ((((((src[I, J, K] - al[0][I, J, K] * sh(0, 1, 0)) - al[1][I, J, K] * sh(0, -1, 0)) -
+            al[2][I, J, K] * sh(1, 0, 0)) - al[3][I, J, K] * sh(-1, 0, 0)) - al[4][I, J, K] * sh(0, 0, 1)) -
+         al[5][I, J, K] * sh(0, 0, -1)) - ap[I, J, K] * sh(0, 0, 0)
+    cnt = r.size
+    return float(np.sqrt(float(np.sum(r * r)) / cnt))
+
+
+def _tdma(a, b, c, d):
+    """tools::tdma (src/Tools/Tools.cpp:43-62), Python floats."""
+    m = len(a)
+    cp, dp, x = [0.0] * m, [0.0] * m, [0.0] * m
+    cp[0] = c[0] / b[0]
+    dp[0] = d[0] / b[0]
+    for i in range(1, m):
+        cp[i] = c[i] / (b[i] - a[i] * cp[i - 1])
+        dp[i] = (d[i] - a[i] * dp[i - 1]) / (b[i] - a[i] * cp[i - 1])
+    x[m - 1] = dp[m - 1]
+    for i in range(m - 2, -1, -1):
+        x[i] = dp[i] - cp[i] * x[i + 1]
+    return x
+
+
+def fdm_solve(mesh, al, ap, src, xg, tol, max_its):
+    """fdMatrix::solve(tol, maxIts) (fdMatrix.hxx:59-198) for a scalar on a
+    periodic mesh, in the reference's order: per iteration the residual check,
+    then line sweeps along j (lines in i-then-k order), along i, along k, each
+    line a tridiagonal solve over the whole ghosted line with the ghost rows and
+    the last (duplicate) node held at their current values, Gauss-Seidel across
+    lines; then the periodic ghost refresh.  Small meshes only (Python loops).
+    Returns (x ghosted, iterations, residual)."""
+    n, h = mesh.n, mesh.h
+    x = (xg[..., 0] if xg.ndim == 4 else xg).copy()
+    its, res = 0, fdm_residual(mesh, al, ap, src, x)
+    while its < max_its:
+        res = fdm_residual(mesh, al, ap, src, x)
+        if not res > tol:
+            break
+        its += 1
+        for axis in (1, 0, 2):
+            m = n[axis]
+            # sub- and super-diagonal coefficients (S, N), (W, E), (B, T) and the
+            # off-line neighbours moved to the right-hand side, (l, di, dj, dk), in the
+            # reference's order (fdMatrix.hxx:103-108, 138-143, 173-178)
+            lo, hi = {0: (3, 2), 1: (1, 0), 2: (5, 4)}[axis]
+            others = [ax for ax in (0, 1, 2) if ax != axis]
+            offs = {0: ((0, 0, 1, 0), (1, 0, -1, 0), (4, 0, 0, 1), (5, 0, 0, -1)),
+                    1: ((2, 1, 0, 0), (3, -1, 0, 0), (4, 0, 0, 1), (5, 0, 0, -1)),
+                    2: ((2, 1, 0, 0), (3, -1, 0, 0), (0, 0, 1, 0), (1, 0, -1, 0))}[axis]
+            for p in range(h, n[others[0]] - h):
+                for q in range(h, n[others[1]] - h):
+                    a, b, c, d = [0.0] * m, [0.0] * m, [0.0] * m, [0.0] * m
+                    for t in range(m):
+                        idx = [0, 0, 0]
+                        idx[axis], idx[others[0]], idx[others[1]] = t, p, q
+                        i, j, k = idx
+                        if t < h or t >= m - h - 1:
+                            a[t], b[t], c[t], d[t] = 0.0, 1.0, 0.0, float(x[i, j, k])
+                            continue
+                        a[t], b[t], c[t] = float(al[lo][i, j, k]), float(ap[i, j, k]), float(al[hi][i, j, k])
+                        v = float(src[i, j, k])
+                        for l, di, dj, dk in offs:
+                            v = v - float(al[l][i, j, k]) * float(x[i + di, j + dj, k + dk])
+                        d[t] = v
+                    sol = _tdma(a, b, c, d)
+                    for t in range(h, m - h):
+                        idx = [0, 0, 0]
+                        idx[axis], idx[others[0]], idx[others[1]] = t, p, q
+                        x[tuple(idx)] = sol[t]
+        x = bc_apply(mesh, x[..., None])[..., 0]
+    return x, its, res
+
+
+def ref_im(mesh, mu, c, xg, fg, tol, max_its):
+    """The reference's im::laplacian(mu, x), ap -= c, (M == f).solve(tol, max_its)
+    (oracle/_ref/nova_ref im): coefficients and source as built, x after the
+    solve, and the residual after it."""
+    with tempfile.TemporaryDirectory() as td:
+        case = os.path.join(td, "case")
+        write_case(case, mesh)
+        px, pf = os.path.join(td, "x.bin"), os.path.join(td, "f.bin")
+        np.ascontiguousarray(xg, np.float64).tofile(px)
+        np.ascontiguousarray(fg, np.float64).tofile(pf)
+        out = os.path.join(td, "out")
+        subprocess.run([REF_BIN, "im", case, repr(float(mu)), repr(float(c)), px, pf, repr(float(tol)),
+                        str(int(max_its)), out, "-m", str(mesh.m)], check=True, stdout=subprocess.DEVNULL)
+        rd = lambda k: np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n)
+        return {"al": np.stack([rd("al%d" % l) for l in range(6)]), "ap": rd("ap"), "src": rd("src"),
+                "x": rd("x"), "res": float(open(out + "_res.txt").read())}
+
+
 # ------------------------------------------------------------- initial data --
 
 def ic_taylor_green(mesh):

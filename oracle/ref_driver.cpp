@@ -14,6 +14,7 @@
  *   nova_ref wcinit <case> <c> <rho0> <gz> <T.bin> <out>
  *   nova_ref ensight <case> <nsteps> <dt> <U.bin> <p.bin> <dir>
  *   nova_ref ops2 <case> <T.bin> <S.bin> <s.bin> <nu.bin> <U.bin> <out>
+ *   nova_ref im <case> <mu> <c> <x.bin> <f.bin> <tol> <maxits> <out>
  *   (any may end with the reference's `-m <order>` option)
  *
  * `wc` runs the compressible loop bodies: app/TG (rhoEqn.H, pEqn.H, UEqn.H in
@@ -40,6 +41,7 @@
 #include "ex/div/div.h"
 #include "ex/grad/grad.h"
 #include "ex/laplacian/laplacian.h"
+#include "im/laplacian/laplacian.h" /* after ex/laplacian, which it uses */
 #include "parallelCom/parallelCom.h"
 #include "poisson/poisson.h"
 #include "settings/settings.h"
@@ -340,6 +342,40 @@ static int ops2(int argc, char **argv)
     return 0;
 }
 
+/* the implicit Laplacian (src/im): M = im::laplacian(mu, x) (7-point coefficients and the
+ * deferred correction against ex::laplacian), M.ap() -= c, then (M == f).solve(tol, maxits)
+ * on x (the reference's line relaxation, fdMatrix.hxx:59-198); saves the coefficients and the
+ * source as built, x after the solve and the residual */
+static int im_solve(int argc, char **argv)
+{
+    if (argc < 10) { std::fprintf(stderr, "usage: im <case> <mu> <c> <x> <f> <tol> <maxits> <out>\n"); return 2; }
+    settings::zoneName() = argv[2];
+    const double mu = std::atof(argv[3]), c = std::atof(argv[4]), tol = std::atof(argv[7]);
+    const int maxits = std::atoi(argv[8]);
+    const std::string out = argv[9];
+    Time time(0.01, 1.0, 1);
+    parallelCom::decompose(settings::zoneName() + "/" + "mesh");
+    Mesh mesh(settings::zoneName() + "/" + "mesh", time);
+    auto x = std::make_shared<Field<scalar> >(mesh, 0, "p");  // the scalar BCs of the case (pBC)
+    auto f = std::make_shared<Field<scalar> >(mesh, 0, "p");
+    load(*x, argv[5]);
+    load(*f, argv[6]);
+    x->correctBoundaryConditions();
+    auto M = im::laplacian(mu, x);
+    for (int l = 0; l < 6; l++) save(M->al(l), out + "_al" + std::to_string(l) + ".bin");
+    save(M->ap(), out + "_ap.bin");
+    save(*dynamic_cast<Field<scalar> *>(M.get()), out + "_src.bin");
+    M->ap() -= c;
+    auto S = (M == f);
+    S->solve(tol, maxits);
+    save(*x, out + "_x.bin");
+    const scalar res = S->residual();
+    std::FILE *fp = std::fopen((out + "_res.txt").c_str(), "w");
+    std::fprintf(fp, "%.17g\n", res);
+    std::fclose(fp);
+    return 0;
+}
+
 /* the apps' output after each step: Mesh::write (geometry, case, restart) and Field<T>::write */
 static int ensight(int argc, char **argv)
 {
@@ -368,7 +404,7 @@ static int ensight(int argc, char **argv)
 
 int main(int argc, char **argv)
 {
-    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit|ensight|ops2 ... [-m order]\n"); return 2; }
+    if (argc < 2) { std::fprintf(stderr, "usage: nova_ref run|ops|wc|wcinit|ensight|ops2|im ... [-m order]\n"); return 2; }
     settings::process(argc, argv); /* the reference's own -m option (settings.cpp:53-78) */
     std::string mode = argv[1];
     if (mode == "run") return run(argc, argv);
@@ -377,6 +413,7 @@ int main(int argc, char **argv)
     if (mode == "wcinit") return wcinit(argc, argv);
     if (mode == "ensight") return ensight(argc, argv);
     if (mode == "ops2") return ops2(argc, argv);
+    if (mode == "im") return im_solve(argc, argv);
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;
 }

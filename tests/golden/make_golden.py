@@ -1,8 +1,8 @@
 """Generate the golden vectors in tests/golden/ from the reference itself.
 
 Runs oracle/_ref/nova_ref -- the reference's own sources (src/ex, src/poisson,
-src/BC, src/Field, app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H,
-the compressible app/TG and app/shearLayerWC loop bodies)
+src/BC, src/Field, src/im, app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H +
+BEqn.H, the compressible app/TG and app/shearLayerWC loop bodies)
 compiled in place by `make -C oracle ref` -- on small seeded inputs and stores
 inputs and outputs as .npz.  Needs the reference tree (only present where the
 fixtures are generated); the tests only read the .npz files.
@@ -140,6 +140,22 @@ def ops2_case(name, N, L, seed):
                         **{"out_" + k: M.interior(v) for k, v in out.items()})
 
 
+def im_case(name, N, L, seed, mu, c, tol, max_its):
+    """the reference's im::laplacian(mu, x) (coefficients, deferred-correction
+    source), ap -= c, and (M == f).solve(tol, max_its) on x"""
+    M = O.Mesh(N, L=L)
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((1,) + M.N)
+    f = rng.standard_normal((1,) + M.N)
+    out = O.ref_im(M, mu, c, M.to_ghosted(x), M.to_ghosted(f), tol, max_its)
+    h = M.h
+    inner = (slice(h, h + N[0]), slice(h, h + N[1]), slice(h, h + N[2]))
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(L), mu=np.array(mu), c=np.array(c),
+                        tol=np.array(tol), max_its=np.array(max_its), x=x, f=f,
+                        al=np.stack([a[inner] for a in out["al"]]), ap=out["ap"][inner], src=out["src"][inner],
+                        x_solved=out["x"][inner][None], res=np.array(out["res"]))
+
+
 CASES = {
     "ops_10x8x6.npz": lambda n: ops_case(n, (10, 8, 6), (2 * np.pi, 2.0, 3.0), 7, 0.01),
     "ops_16x12x8_m4.npz": lambda n: ops_case(n, (16, 12, 8), (2 * np.pi,) * 3, 8, 0.02, m=4),
@@ -152,6 +168,7 @@ CASES = {
     "ops2_7x6x5.npz": lambda n: ops2_case(n, (7, 6, 5), (2.0, 1.5, 3.0), 13),
     "ensight_7x5x6.npz": lambda n: ensight_case(n, (7, 5, 6), (2.0, 1.5, 3.0), (0.5, -1.0, 0.25), 11),
     "ensight_walls_6x8x5.npz": lambda n: ensight_case(n, (6, 8, 5), (1.0, 2.0, 1.5), (0.0, 0.0, 0.0), 12, True),
+    "im_7x6x8.npz": lambda n: im_case(n, (7, 6, 8), (2.0, 1.5, 3.0), 17, 0.7, 6.0, 1e-14, 400),
 }
 
 

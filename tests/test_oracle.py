@@ -162,3 +162,22 @@ def test_tensor_operators_and_field_nu_laplacian_bitwise_vs_reference_golden(ora
             "lap_f_s": oracle.lap_f(M, G["nu"], G["s"])}
     for k, v in mine.items():
         assert np.array_equal(M.interior(v), g["out_" + k]), k
+
+
+def test_im_laplacian_and_line_relaxation_match_the_reference(oracle):
+    """im::laplacian (coefficients, deferred-correction source) and fdMatrix::solve
+    restated against the reference's own run (tests/golden/im_7x6x8.npz): bit for bit,
+    the solve's iterations included."""
+    g = load_golden("im_7x6x8.npz")
+    N = tuple(int(v) for v in g["N"])
+    M = oracle.Mesh(N, L=tuple(g["L"]))
+    xg = M.to_ghosted(g["x"])
+    al, ap, src = oracle.im_laplacian(M, float(g["mu"]), xg)
+    h = M.h
+    inner = (slice(h, h + N[0]), slice(h, h + N[1]), slice(h, h + N[2]))
+    assert np.array_equal(np.stack([a[inner] for a in al]), g["al"])
+    assert np.array_equal(ap[inner], g["ap"]) and np.array_equal(src[inner], g["src"])
+    ap2, src2 = ap - float(g["c"]), src + M.to_ghosted(g["f"])[..., 0]
+    x, its, _ = oracle.fdm_solve(M, al, ap2, src2, xg, float(g["tol"]), int(g["max_its"]))
+    assert np.array_equal(x[inner][None], g["x_solved"])
+    assert oracle.fdm_residual(M, al, ap2, src2, x) == float(g["res"])
