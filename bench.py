@@ -46,6 +46,11 @@ CFL = 0.3
 # stages 36 + 60 + 60 + 72 (see the stage-kernel epilogue in nova_stage.cu)
 STAGE_BYTES = {"f64": 384.0, "f32split": 228.0}
 STAGE_LAUNCHES_PER_STEP = 4
+# fdMatrix::solve, FP64 bytes per node per iteration that the algorithm must
+# move: the residual reads the 8 matrix fields and x (72); each of the three
+# line sweeps reads the 8 matrix fields (source, ap, the two coefficients along
+# the line, the four off it) and x, and writes x (80)
+IM_BYTES = 72.0 + 3 * 80.0
 
 
 def workload_config(n, extra=None):
@@ -447,6 +452,60 @@ def mhd_legs(args, nova, torch, dist, world):
     return res
 
 
+def im_leg(args, nova, torch, dist, world):
+    """The implicit Laplacian of src/im: im::laplacian(mu, x), ap -= c, (M == f)
+    and fdMatrix::solve with tol = 0, so that exactly args.im_its iterations run
+    (residual check, then line sweeps along j, i, k), on a periodic args.im_n^3
+    mesh; beside it the reference's own solve on the host (serial, as written)."""
+    n, its = args.im_n, args.im_its
+    mu, c = 1e-3, 1.0
+    rng = np.random.default_rng(11)
+    x0, f0 = rng.standard_normal((1, n, n, n)), rng.standard_normal((1, n, n, n))
+    GM = nova.Mesh((n, n, n))
+    GM.set_stream(torch.cuda.current_stream().cuda_stream)
+    x, f = nova.Field(GM, 1).upload_soa(x0), nova.Field(GM, 1).upload_soa(f0)
+    A = nova.im.laplacian(mu, x)
+    A.add_diagonal(-c)
+    A.eq(f)
+    A.solve(0.0, 3)  # warm-up: scratch and line factors
+    res0 = A.residual()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    GM.launch_count(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    done, _ = A.solve(0.0, its)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+    launches = GM.launch_count(reset=True)
+    res1 = A.residual()
+    A.close()
+    x.close()
+    f.close()
+    peak, peak_kind = measured_peaks()
+    achieved = IM_BYTES * n ** 3 * its / sec / 1e9
+    out = {"workload": "im::laplacian(1e-3, x) - 1 == f on a periodic [0,2pi]^3 %d^3 mesh, random x and f; "
+                       "fdMatrix::solve(tol=0, %d) timed after 3 iterations" % (n, its),
+           "value": world * n ** 3 * its / sec / 1e6, "unit": "Mnode-iterations/s", "iterations": done,
+           "ms_per_iteration": 1e3 * sec / its, "gpu_launches": launches, "dtype": "f64",
+           "residual_before_after": [res0, res1],
+           "roofline": {"bound": "hbm", "kernel": "one solve iteration (residual + three line sweeps)",
+                        "alg_bytes_per_node_iteration": IM_BYTES, "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind}}
+    if world == 1 and not args.no_cpu_baseline and reference_bin()[0] is not None:
+        from oracle import oracle as O
+        nc, ic = args.im_cpu_n, args.im_cpu_its
+        M = O.Mesh((nc, nc, nc), L=(2 * np.pi,) * 3)
+        r = O.ref_im(M, mu, c, M.to_ghosted(x0[:, :nc, :nc, :nc]), M.to_ghosted(f0[:, :nc, :nc, :nc]), 0.0, ic)
+        out["cpu_baseline"] = {"value": nc ** 3 * ic / r["solve_s"] / 1e6, "unit": "Mnode-iterations/s",
+                               "cores": 1, "kind": "reference",
+                               "sample": "the reference's fdMatrix::solve (serial as written), %d^3, %d iterations"
+                                         % (nc, ic)}
+    return out
+
+
 def our_arm(args, rank, world, dist):
     import torch
     from novaclone_b200 import nova
@@ -557,6 +616,7 @@ def our_arm(args, rank, world, dist):
             U.close()
 
     mhd = None if args.no_mhd else mhd_legs(args, nova, torch, dist, world)
+    im = None if args.no_im else im_leg(args, nova, torch, dist, world)
 
     if rank != 0:
         return 0
@@ -609,6 +669,7 @@ def our_arm(args, rank, world, dist):
         "adjoint_fwd_ratio": None if adj is None else adj["ratio"],
         "adjoint": adj,
         "mhd": mhd,
+        "im": im,
     }
     print(json.dumps(line))
     return 0
@@ -633,6 +694,11 @@ def main():
     ap.add_argument("--mhd-n", type=int, default=128)
     ap.add_argument("--mhd-steps", type=int, default=200)
     ap.add_argument("--mhd-adj-n", type=int, default=128)
+    ap.add_argument("--no-im", action="store_true")
+    ap.add_argument("--im-n", type=int, default=256)
+    ap.add_argument("--im-its", type=int, default=20)
+    ap.add_argument("--im-cpu-n", type=int, default=128)
+    ap.add_argument("--im-cpu-its", type=int, default=30)
     ap.add_argument("--fd-dirs", type=int, default=8, help="finite-difference checks of each FP64 adjoint")
     args = ap.parse_args()
     if args.warmup < 3:

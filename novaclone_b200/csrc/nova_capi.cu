@@ -1966,7 +1966,9 @@ struct nova_fdm {
     nova_ctx *ctx = nullptr;
     nova_field *x = nullptr;     // the transported field (not owned)
     double *coef = nullptr;      // 8 x N3
-    double *scratch = nullptr;   // the solve's line scratch (3 N3) and its second x buffer (N3)
+    double *scratch = nullptr;   // the solve's second x buffer (N3)
+    double *fac = nullptr;       // line factors along i, j, k: 3 x 4 N3, then the per-line scalars
+    bool factored = false;       // fac matches the coefficients (the source does not enter it)
 };
 
 namespace {
@@ -2021,6 +2023,7 @@ extern "C" nova_status nova_fdm_add(nova_ctx *ctx, nova_fdm *a, double alpha, co
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_add: bad matrix")) != NOVA_OK) return s;
     if ((s = fdm_check(ctx, b, "nova_fdm_add: bad matrix")) != NOVA_OK) return s;
+    a->factored = false;
     launch_fdm_algebra(ctx->g, 0, alpha, a->coef, b->coef, ctx->stream);
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2032,6 +2035,7 @@ extern "C" nova_status nova_fdm_mul(nova_ctx *ctx, nova_fdm *a, const nova_fdm *
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_mul: bad matrix")) != NOVA_OK) return s;
     if ((s = fdm_check(ctx, b, "nova_fdm_mul: bad matrix")) != NOVA_OK) return s;
+    a->factored = false;
     launch_fdm_algebra(ctx->g, 1, 0.0, a->coef, b->coef, ctx->stream);
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2042,6 +2046,7 @@ extern "C" nova_status nova_fdm_scale(nova_ctx *ctx, nova_fdm *a, double sc)
 {
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_scale: bad matrix")) != NOVA_OK) return s;
+    a->factored = false;
     launch_fdm_algebra(ctx->g, 2, sc, a->coef, nullptr, ctx->stream);
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2064,6 +2069,7 @@ extern "C" nova_status nova_fdm_add_diagonal(nova_ctx *ctx, nova_fdm *a, double 
 {
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_add_diagonal: bad matrix")) != NOVA_OK) return s;
+    a->factored = false;
     launch_fdm_point(ctx->g, 1, d, a->coef, nullptr, ctx->stream);
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2075,6 +2081,7 @@ extern "C" nova_status nova_fdm_relax(nova_ctx *ctx, nova_fdm *a, double urf)
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_relax: bad matrix")) != NOVA_OK) return s;
     if (!(urf > 0.0)) return fail(ctx, NOVA_E_INVALID, "nova_fdm_relax: urf must be positive");
+    a->factored = false;
     launch_fdm_point(ctx->g, 2, urf, a->coef, a->x->d64, ctx->stream);
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2088,6 +2095,7 @@ extern "C" nova_status nova_fdm_set_reference(nova_ctx *ctx, nova_fdm *a, int i,
     const Geo &g = ctx->g;
     if (i < 0 || i >= g.N0 || j < 0 || j >= g.N1 || k < 0 || k >= g.N2)
         return fail(ctx, NOVA_E_INVALID, "nova_fdm_set_reference: node outside the mesh");
+    a->factored = false;
     launch_fdm_setref(g, a->coef, ((long long)i * g.N1 + j) * g.N2 + k, val, ctx->stream);
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2100,7 +2108,7 @@ nova_status fdm_res(nova_ctx *ctx, const nova_fdm *a, const double *x, double *r
 {
     nova_status s = ensure_red(ctx);
     if (s != NOVA_OK) return s;
-    const int nb = 592;  // <= the partials the diagnostics reserve (diag_blocks(g) * 4 >= 1184 * 4)
+    const int nb = 592;  // 4 blocks per SM (k_fdm_res launch bounds); <= the partials reserved (diag_blocks(g) * 4)
     launch_fdm_residual(ctx->g, a->coef, x, ctx->d_part, nb, ctx->d_scalar, ctx->stream);
     ctx->launches += 2;
     CK(cudaMemcpyAsync(res, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -2124,21 +2132,45 @@ extern "C" nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, in
     if ((s = fdm_check(ctx, a, "nova_fdm_solve: bad matrix")) != NOVA_OK) return s;
     if (max_its < 0) return fail(ctx, NOVA_E_INVALID, "nova_fdm_solve: max_its must not be negative");
     const Geo &g = ctx->g;
-    if ((s = dalloc(ctx, &a->scratch, 4 * (size_t)g.N3)) != NOVA_OK) return s;
-    double *x = a->x->d64, *xt = a->scratch + 3 * (size_t)g.N3;
+    if ((s = dalloc(ctx, &a->scratch, (size_t)g.N3)) != NOVA_OK) return s;
+    // factors of the three line directions (4 N3 each) and their per-line scalars (2 per line)
+    const size_t lines[3] = {(size_t)g.N1 * g.N2, (size_t)g.N0 * g.N2, (size_t)g.N0 * g.N1};
+    if ((s = dalloc(ctx, &a->fac, 12 * (size_t)g.N3 + 2 * (lines[0] + lines[1] + lines[2]))) != NOVA_OK) return s;
+    double *fac[3], *ls[3];
+    {
+        double *q = a->fac + 12 * (size_t)g.N3;
+        for (int ax = 0; ax < 3; ax++) {
+            fac[ax] = a->fac + 4 * (size_t)ax * g.N3;
+            ls[ax] = q;
+            q += 2 * lines[ax];
+        }
+    }
+    if (!a->factored && max_its > 0) {
+        for (int ax = 0; ax < 3; ax++) launch_fdm_factor(ax, g, a->coef, fac[ax], ls[ax], ctx->stream);
+        ctx->launches += 3;
+        CKL("k_fdm_factor");
+        a->factored = true;
+    }
+    // x and the second buffer swap roles every sweep; cur holds the iterate
+    double *cur = a->x->d64, *other = a->scratch;
     double r = 0.0;
     int n = 0;
-    if ((s = fdm_res(ctx, a, x, &r)) != NOVA_OK) return s;
+    if (max_its == 0 && (s = fdm_res(ctx, a, cur, &r)) != NOVA_OK) return s;
     while (n < max_its) {
-        if ((s = fdm_res(ctx, a, x, &r)) != NOVA_OK) return s;
+        // the residual checked before each iteration, as the reference reports it
+        if ((s = fdm_res(ctx, a, cur, &r)) != NOVA_OK) return s;
         if (!(r > tol)) break;
         n++;
-        launch_fdm_sweep(1, g, a->coef, x, xt, a->scratch, ctx->stream);   // j lines
-        launch_fdm_sweep(0, g, a->coef, xt, x, a->scratch, ctx->stream);   // i lines
-        launch_fdm_sweep(2, g, a->coef, x, xt, a->scratch, ctx->stream);   // k lines
-        CK(cudaMemcpyAsync(x, xt, sizeof(double) * g.N3, cudaMemcpyDeviceToDevice, ctx->stream));
+        for (const int ax : {1, 0, 2}) {  // j lines, i lines, k lines
+            launch_fdm_line(ax, g, a->coef, fac[ax], ls[ax], cur, other, ctx->stream);
+            std::swap(cur, other);
+        }
         ctx->launches += 3;
-        CKL("k_fdm_sweep");
+        CKL("k_fdm_line");
+    }
+    if (cur != a->x->d64) {
+        CK(cudaMemcpyAsync(a->x->d64, cur, sizeof(double) * g.N3, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
     }
     if (its) *its = n;
     if (res) *res = r;
@@ -2160,6 +2192,7 @@ extern "C" nova_status nova_fdm_destroy(nova_fdm *a)
     if (!a) return NOVA_OK;
     if (a->coef) cudaFree(a->coef);
     if (a->scratch) cudaFree(a->scratch);
+    if (a->fac) cudaFree(a->fac);
     delete a;
     return NOVA_OK;
 }

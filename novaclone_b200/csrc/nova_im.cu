@@ -97,27 +97,42 @@ __global__ void k_fdm_setref(double *ap, double *b, long long n, double val)
     ap[n] = ap[n] * 1e15;
 }
 
-// partial sums of (b - A x)^2 over the (N0+1)(N1+1)(N2+1) nodes (indices wrap)
-__global__ void k_fdm_res(Geo g, const double *__restrict__ coef, const double *__restrict__ x, double *part)
+// partial sums of (b - A x)^2 over the (N0+1)(N1+1)(N2+1) nodes the reference
+// loops over: its duplicate periodic node N of each direction is node 0 here,
+// so node 0 of a direction counts twice.  A block takes whole (i, j) rows, two
+// at a time so that both rows' loads are in flight together, its threads
+// along k.
+__device__ __forceinline__ double fdm_res_node(const Geo &g, const double *__restrict__ coef,
+                                               const double *__restrict__ x, int row, int k)
+{
+    const long long N3 = g.N3;
+    const int i = row / g.N1, j = row - i * g.N1;
+    const long long base = (long long)row * g.N2, n = base + k;
+    double r = coef[7 * N3 + n];
+    r = __dsub_rn(r, __dmul_rn(coef[0 * N3 + n], x[nidx(g, i, wrapi(j + 1, g.N1), k)]));
+    r = __dsub_rn(r, __dmul_rn(coef[1 * N3 + n], x[nidx(g, i, wrapi(j - 1, g.N1), k)]));
+    r = __dsub_rn(r, __dmul_rn(coef[2 * N3 + n], x[nidx(g, wrapi(i + 1, g.N0), j, k)]));
+    r = __dsub_rn(r, __dmul_rn(coef[3 * N3 + n], x[nidx(g, wrapi(i - 1, g.N0), j, k)]));
+    r = __dsub_rn(r, __dmul_rn(coef[4 * N3 + n], x[base + wrapi(k + 1, g.N2)]));
+    r = __dsub_rn(r, __dmul_rn(coef[5 * N3 + n], x[base + wrapi(k - 1, g.N2)]));
+    r = __dsub_rn(r, __dmul_rn(coef[6 * N3 + n], x[n]));
+    const double w = (i == 0 ? 2.0 : 1.0) * (j == 0 ? 2.0 : 1.0) * (k == 0 ? 2.0 : 1.0);
+    return __dmul_rn(w, __dmul_rn(r, r));
+}
+
+__global__ void __launch_bounds__(256, 4) k_fdm_res(Geo g, const double *__restrict__ coef,
+                                                    const double *__restrict__ x, double *part)
 {
     __shared__ double sh[32];
-    const long long tot = (long long)(g.N0 + 1) * (g.N1 + 1) * (g.N2 + 1);
-    const long long N3 = g.N3;
+    const int rows = g.N0 * g.N1;
     double acc = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t % (g.N2 + 1)) % g.N2, j = (int)((t / (g.N2 + 1)) % (g.N1 + 1)) % g.N1;
-        const int i = (int)(t / ((long long)(g.N1 + 1) * (g.N2 + 1))) % g.N0;
-        const long long n = nidx(g, i, j, k);
-        double r = coef[7 * N3 + n];
-        r = __dsub_rn(r, __dmul_rn(coef[0 * N3 + n], x[nidx(g, i, wrapi(j + 1, g.N1), k)]));
-        r = __dsub_rn(r, __dmul_rn(coef[1 * N3 + n], x[nidx(g, i, wrapi(j - 1, g.N1), k)]));
-        r = __dsub_rn(r, __dmul_rn(coef[2 * N3 + n], x[nidx(g, wrapi(i + 1, g.N0), j, k)]));
-        r = __dsub_rn(r, __dmul_rn(coef[3 * N3 + n], x[nidx(g, wrapi(i - 1, g.N0), j, k)]));
-        r = __dsub_rn(r, __dmul_rn(coef[4 * N3 + n], x[nidx(g, i, j, wrapi(k + 1, g.N2))]));
-        r = __dsub_rn(r, __dmul_rn(coef[5 * N3 + n], x[nidx(g, i, j, wrapi(k - 1, g.N2))]));
-        r = __dsub_rn(r, __dmul_rn(coef[6 * N3 + n], x[n]));
-        acc = __dadd_rn(acc, __dmul_rn(r, r));
+    for (int row = blockIdx.x; row < rows; row += 2 * gridDim.x) {
+        const int row2 = row + gridDim.x;
+        for (int k = threadIdx.x; k < g.N2; k += blockDim.x) {
+            const double a = fdm_res_node(g, coef, x, row, k);
+            const double b = row2 < rows ? fdm_res_node(g, coef, x, row2, k) : 0.0;
+            acc = __dadd_rn(acc, __dadd_rn(a, b));
+        }
     }
     acc = block_reduce_sum(acc, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -132,58 +147,69 @@ __global__ void k_fdm_res_final(const double *__restrict__ part, int nb, double 
     if (threadIdx.x == 0) out[0] = sqrt(a / count);
 }
 
-// One line per thread along AXIS (0: i, 1: j, 2: k): a_t x_{t-1} + b_t x_t +
-// c_t x_{t+1} = d_t with periodic wrap, the off-line neighbours from xin.
-// Scratch: cp, yv, zv (one element per node of the line).
+// Lines along AXIS (0: i, 1: j, 2: k) and their numbering: i-lines by (j, k),
+// j-lines by (i, k), k-lines by (i, j), the fastest coordinate last; LO and HI
+// are the coefficients below and above the diagonal along AXIS
+// (fdMatrix.hxx:99-101, 134-136, 169-171).
 template <int AXIS>
-__global__ void k_fdm_sweep(Geo g, const double *__restrict__ coef, const double *__restrict__ xin, double *xout,
-                            double *cp, double *yv, double *zv)
+struct LineGeo {
+    static constexpr int LO = AXIS == 0 ? 3 : (AXIS == 1 ? 1 : 5), HI = AXIS == 0 ? 2 : (AXIS == 1 ? 0 : 4);
+    static __device__ __forceinline__ int len(const Geo &g) { return AXIS == 0 ? g.N0 : (AXIS == 1 ? g.N1 : g.N2); }
+    // (i, j, k) of node t on line (slow, fast): the line's two fixed coordinates,
+    // slowest first (j, k for i-lines; i, k for j-lines; i, j for k-lines)
+    static __device__ __forceinline__ void coords(int slow, int fast, int t, int &i, int &j, int &k)
+    {
+        if (AXIS == 0) {
+            i = t;
+            j = slow;
+            k = fast;
+        } else if (AXIS == 1) {
+            i = slow;
+            j = t;
+            k = fast;
+        } else {
+            i = slow;
+            j = fast;
+            k = t;
+        }
+    }
+    // the extent of the fastest fixed coordinate: line number = slow * nfast(g) + fast
+    static __device__ __forceinline__ int nfast(const Geo &g) { return AXIS == 2 ? g.N1 : g.N2; }
+};
+
+// Factors of the periodic tridiagonal system of every line along AXIS, one
+// line per thread.  The line's rows a_t x_{t-1} + b_t x_t + c_t x_{t+1} = d_t
+// wrap around (x_{-1} = x_{n-1}, x_n = x_0).  Folding the two corner entries
+// into the diagonal with gamma = -b_0 gives the open tridiagonal T' with
+// T = T' + u v^T, u = (gamma, 0.., c_{n-1}), v = (1, 0.., a_0/gamma), so
+// (Sherman-Morrison) x = y - z (v.y)/(1 + v.z) with T' y = d, T' z = u.
+// Stored per node (fac = [w | cp | P | z], 4 N3 per axis): the inverse Thomas
+// pivots w_t, the eliminated super-diagonal cp_t, z, and
+// P_t = prod_{s<t} (-cp_s), so that the back-substituted y_0 is the sum of
+// P_t yhat_t over the forward-eliminated yhat; per line (ls = [q | h]):
+// q = a_0/gamma, h = 1/(1 + v.z).  The coefficients do not change while a
+// solve runs, so this runs once per solve, and again only after they change.
+template <int AXIS>
+__global__ void k_fdm_factor(Geo g, const double *__restrict__ coef, double *fac, double *ls)
 {
+    using LG = LineGeo<AXIS>;
+    constexpr int LO = LG::LO, HI = LG::HI;
     const long long N3 = g.N3;
-    const int n = AXIS == 0 ? g.N0 : (AXIS == 1 ? g.N1 : g.N2);
+    const int n = LG::len(g), nf = LG::nfast(g);
     const long long lines = N3 / n;
     const long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (line >= lines) return;
-    // the line's fixed indices: i-lines by (j, k), j-lines by (i, k), k-lines by (i, j), the fastest last
-    int i0 = 0, j0 = 0, k0 = 0;
-    if (AXIS == 0) {
-        j0 = (int)(line / g.N2);
-        k0 = (int)(line % g.N2);
-    } else if (AXIS == 1) {
-        i0 = (int)(line / g.N2);
-        k0 = (int)(line % g.N2);
-    } else {
-        i0 = (int)(line / g.N1);
-        j0 = (int)(line % g.N1);
-    }
-    auto node = [&](int t) -> long long {
-        return AXIS == 0 ? nidx(g, t, j0, k0) : (AXIS == 1 ? nidx(g, i0, t, k0) : nidx(g, i0, j0, t));
+    const int slow = (int)(line / nf), fast = (int)(line % nf);
+    auto node = [&](int t) {
+        int i, j, k;
+        LG::coords(slow, fast, t, i, j, k);
+        return nidx(g, i, j, k);
     };
-    // sub/super-diagonal coefficients and the off-line neighbours (fdMatrix.hxx:99-108, 134-143, 169-178)
-    constexpr int LO = AXIS == 0 ? 3 : (AXIS == 1 ? 1 : 5), HI = AXIS == 0 ? 2 : (AXIS == 1 ? 0 : 4);
-    auto rhs = [&](int t, long long o) -> double {
-        const int i = AXIS == 0 ? t : i0, j = AXIS == 1 ? t : j0, k = AXIS == 2 ? t : k0;
-        double d = coef[7 * N3 + o];
-        if (AXIS != 1) {
-            d = d - coef[0 * N3 + o] * xin[nidx(g, i, wrapi(j + 1, g.N1), k)];
-            d = d - coef[1 * N3 + o] * xin[nidx(g, i, wrapi(j - 1, g.N1), k)];
-        }
-        if (AXIS != 0) {
-            d = d - coef[2 * N3 + o] * xin[nidx(g, wrapi(i + 1, g.N0), j, k)];
-            d = d - coef[3 * N3 + o] * xin[nidx(g, wrapi(i - 1, g.N0), j, k)];
-        }
-        if (AXIS != 2) {
-            d = d - coef[4 * N3 + o] * xin[nidx(g, i, j, wrapi(k + 1, g.N2))];
-            d = d - coef[5 * N3 + o] * xin[nidx(g, i, j, wrapi(k - 1, g.N2))];
-        }
-        return d;
-    };
-    // Sherman-Morrison: T' = T - u v^T with the corners folded into the
-    // diagonal, gamma = -b_0, u = (gamma, 0.., c_{n-1}), v = (1, 0.., a_0/gamma)
+    double *W = fac, *CP = fac + N3, *P = fac + 2 * N3, *Z = fac + 3 * N3;
     const long long o0 = node(0), on = node(n - 1);
     const double a0 = coef[LO * N3 + o0], cn = coef[HI * N3 + on];
     const double gam = -coef[6 * N3 + o0];
-    double cprev = 0.0, yprev = 0.0, zprev = 0.0;
+    double cprev = 0.0, zprev = 0.0, pprev = 1.0;
     for (int t = 0; t < n; t++) {
         const long long o = node(t);
         const double a = t == 0 ? 0.0 : coef[LO * N3 + o];
@@ -192,41 +218,177 @@ __global__ void k_fdm_sweep(Geo g, const double *__restrict__ coef, const double
         if (t == 0) b -= gam;
         if (t == n - 1) b -= cn * a0 / gam;
         const double u = t == 0 ? gam : (t == n - 1 ? cn : 0.0);
-        const double den = b - a * cprev;
-        const double cc = c / den;
-        const double yy = (rhs(t, o) - a * yprev) / den;
-        const double zz = (u - a * zprev) / den;
-        cp[o] = cc;
-        yv[o] = yy;
-        zv[o] = zz;
+        const double w = 1.0 / (b - a * cprev);
+        const double p = t == 0 ? 1.0 : pprev * -cprev;
+        const double cc = c * w;
+        const double zz = (u - a * zprev) * w;
+        W[o] = w;
+        CP[o] = cc;
+        P[o] = p;
+        Z[o] = zz;
         cprev = cc;
-        yprev = yy;
         zprev = zz;
+        pprev = p;
     }
-    // back substitution (y and z), then x = y - z (v.y)/(1 + v.z)
-    double ynext = 0.0, znext = 0.0, y0 = 0.0, z0 = 0.0, yn = 0.0, zn = 0.0;
+    double znext = 0.0, z0 = 0.0, zn = 0.0;
     for (int t = n - 1; t >= 0; t--) {
         const long long o = node(t);
-        const double yy = t == n - 1 ? yv[o] : yv[o] - cp[o] * ynext;
-        const double zz = t == n - 1 ? zv[o] : zv[o] - cp[o] * znext;
-        yv[o] = yy;
-        zv[o] = zz;
-        ynext = yy;
+        const double zz = Z[o] - CP[o] * znext;
+        Z[o] = zz;
         znext = zz;
-        if (t == n - 1) {
-            yn = yy;
-            zn = zz;
+        if (t == n - 1) zn = zz;
+        if (t == 0) z0 = zz;
+    }
+    const double q = a0 / gam;
+    ls[line] = q;
+    ls[lines + line] = 1.0 / (1.0 + z0 + q * zn);
+}
+
+// One sweep along AXIS with the factors of k_fdm_factor: every line solved at
+// once, the neighbours off the line read from xin, the result in xout.  A
+// block takes FDM_LT lines with consecutive values of the fastest fixed
+// coordinate, in chunks of FDM_TT nodes along them.  Each chunk's tiles pass
+// through shared memory so that every global access is coalesced: across the
+// lines for i- and j-lines (consecutive k), along the line for k-lines.
+// Warp 0 runs the recurrences, lane l on line l:
+//   forward   yhat_t = (d_t - a_t yhat_{t-1}) w_t,  Y0 += P_t yhat_t   (yhat into xout)
+//   f = (Y0 + q yhat_{n-1}) h                                            (= (v.y)/(1 + v.z))
+//   backward  y_t = yhat_t - cp_t y_{t+1},  x_t = y_t - f z_t           (xout in place)
+constexpr int FDM_LT = 32, FDM_TT = 16, FDM_LINE_THREADS = 256;
+constexpr int FDM_PER = FDM_LT * FDM_TT / FDM_LINE_THREADS;  // tile elements per thread
+static_assert(FDM_LT * FDM_TT % FDM_LINE_THREADS == 0, "tile elements split evenly over the threads");
+
+template <int AXIS>
+__global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const double *__restrict__ coef,
+                                                                const double *__restrict__ fac,
+                                                                const double *__restrict__ ls,
+                                                                const double *__restrict__ xin, double *xout)
+{
+    using LG = LineGeo<AXIS>;
+    constexpr int LO = LG::LO, LT = FDM_LT, TT = FDM_TT;
+    __shared__ double sm[4][LT][TT + 1];
+    const long long N3 = g.N3;
+    const int n = LG::len(g), nf = LG::nfast(g);
+    const long long lines = N3 / n;
+    const int groups = (nf + LT - 1) / LT;
+    const int slow = (int)(blockIdx.x / groups), f0 = (int)(blockIdx.x % groups) * LT;
+    const int nl = min(LT, nf - f0);
+    const long long line0 = (long long)slow * nf + f0;
+    const double *W = fac, *CP = fac + N3, *P = fac + 2 * N3, *Z = fac + 3 * N3;
+    const int tid = threadIdx.x;
+    // element e of a tile, (line l, node tt of the chunk): consecutive threads on consecutive addresses
+    auto elem = [&](int e, int &l, int &tt) {
+        if (AXIS == 2) {
+            l = e / TT;
+            tt = e % TT;
+        } else {
+            l = e % LT;
+            tt = e / LT;
         }
-        if (t == 0) {
-            y0 = yy;
-            z0 = zz;
+    };
+    auto node = [&](int l, int t) {
+        int i, j, k;
+        LG::coords(slow, f0 + l, t, i, j, k);
+        return nidx(g, i, j, k);
+    };
+    const int nch = (n + TT - 1) / TT;
+    double yh = 0.0, Y0 = 0.0;  // warp 0, lane l: line l's last yhat and the sum for y_0
+
+    // forward elimination, chunk by chunk; a thread stores the previous chunk's
+    // yhat of its own tile elements before it loads the next chunk into them
+    for (int c = 0; c < nch; c++) {
+        const int t0 = c * TT, nt = min(TT, n - t0);
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            if (c > 0 && l < nl) xout[node(l, t0 - TT + tt)] = sm[0][l][tt];  // chunks before the last are full
+            // elements past the lines' or the chunk's end read node (0, t0) and store nothing
+            const bool in = l < nl && tt < nt;
+            const int t = in ? t0 + tt : t0;
+            int i, j, k;
+            LG::coords(slow, f0 + (in ? l : 0), t, i, j, k);
+            const long long o = nidx(g, i, j, k);
+            double d = coef[7 * N3 + o];
+            if (AXIS != 1) {
+                d -= coef[0 * N3 + o] * xin[nidx(g, i, wrapi(j + 1, g.N1), k)];
+                d -= coef[1 * N3 + o] * xin[nidx(g, i, wrapi(j - 1, g.N1), k)];
+            }
+            if (AXIS != 0) {
+                d -= coef[2 * N3 + o] * xin[nidx(g, wrapi(i + 1, g.N0), j, k)];
+                d -= coef[3 * N3 + o] * xin[nidx(g, wrapi(i - 1, g.N0), j, k)];
+            }
+            if (AXIS != 2) {
+                d -= coef[4 * N3 + o] * xin[nidx(g, i, j, wrapi(k + 1, g.N2))];
+                d -= coef[5 * N3 + o] * xin[nidx(g, i, j, wrapi(k - 1, g.N2))];
+            }
+            const double lo = t == 0 ? 0.0 : coef[LO * N3 + o], w = W[o], p = P[o];
+            if (in) {
+                sm[0][l][tt] = d;
+                sm[1][l][tt] = lo;
+                sm[2][l][tt] = w;
+                sm[3][l][tt] = p;
+            }
+        }
+        __syncthreads();
+        if (tid < nl) {
+            const int l = tid;
+#pragma unroll 8
+            for (int tt = 0; tt < nt; tt++) {
+                yh = (sm[0][l][tt] - sm[1][l][tt] * yh) * sm[2][l][tt];
+                Y0 += sm[3][l][tt] * yh;
+                sm[0][l][tt] = yh;
+            }
+        }
+        __syncthreads();
+    }
+    {  // the last chunk's yhat
+        const int t0 = (nch - 1) * TT, nt = n - t0;
+        for (int e = tid; e < LT * TT; e += FDM_LINE_THREADS) {
+            int l, tt;
+            elem(e, l, tt);
+            if (l >= nl || tt >= nt) continue;
+            xout[node(l, t0 + tt)] = sm[0][l][tt];
         }
     }
-    const double vy = y0 + a0 / gam * yn, vz = z0 + a0 / gam * zn;
-    const double f = vy / (1.0 + vz);
-    for (int t = 0; t < n; t++) {
-        const long long o = node(t);
-        xout[o] = yv[o] - f * zv[o];
+    double f = 0.0, ynext = 0.0;
+    if (tid < nl) f = (Y0 + ls[line0 + tid] * yh) * ls[lines + line0 + tid];
+    __syncthreads();
+
+    // back substitution and the correction, from the last chunk to the first
+    for (int c = nch - 1; c >= 0; c--) {
+        const int t0 = c * TT, nt = min(TT, n - t0);
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            const bool in = l < nl && tt < nt;
+            const long long o = in ? node(l, t0 + tt) : node(0, t0);
+            const double yv = xout[o], cp = CP[o], z = Z[o];
+            if (in) {
+                sm[0][l][tt] = yv;
+                sm[1][l][tt] = cp;
+                sm[2][l][tt] = z;
+            }
+        }
+        __syncthreads();
+        if (tid < nl) {
+            const int l = tid;
+#pragma unroll 8
+            for (int tt = nt - 1; tt >= 0; tt--) {
+                const double y = sm[0][l][tt] - sm[1][l][tt] * ynext;
+                sm[0][l][tt] = y - f * sm[2][l][tt];
+                ynext = y;
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < LT * TT; e += FDM_LINE_THREADS) {
+            int l, tt;
+            elem(e, l, tt);
+            if (l >= nl || tt >= nt) continue;
+            xout[node(l, t0 + tt)] = sm[0][l][tt];
+        }
+        __syncthreads();
     }
 }
 
@@ -269,18 +431,30 @@ void launch_fdm_residual(const Geo &g, const double *coef, const double *x, doub
     k_fdm_res_final<<<1, 256, 0, st>>>(part, nb, count, out);
 }
 
-void launch_fdm_sweep(int axis, const Geo &g, const double *coef, const double *xin, double *xout, double *scratch,
-                      cudaStream_t st)
+void launch_fdm_factor(int axis, const Geo &g, const double *coef, double *fac, double *ls, cudaStream_t st)
 {
-    double *cp = scratch, *yv = scratch + g.N3, *zv = scratch + 2 * g.N3;
     const int n = axis == 0 ? g.N0 : (axis == 1 ? g.N1 : g.N2);
     const unsigned nb = blocks_for(g.N3 / n, 128);
     if (axis == 0)
-        k_fdm_sweep<0><<<nb, 128, 0, st>>>(g, coef, xin, xout, cp, yv, zv);
+        k_fdm_factor<0><<<nb, 128, 0, st>>>(g, coef, fac, ls);
     else if (axis == 1)
-        k_fdm_sweep<1><<<nb, 128, 0, st>>>(g, coef, xin, xout, cp, yv, zv);
+        k_fdm_factor<1><<<nb, 128, 0, st>>>(g, coef, fac, ls);
     else
-        k_fdm_sweep<2><<<nb, 128, 0, st>>>(g, coef, xin, xout, cp, yv, zv);
+        k_fdm_factor<2><<<nb, 128, 0, st>>>(g, coef, fac, ls);
+}
+
+void launch_fdm_line(int axis, const Geo &g, const double *coef, const double *fac, const double *ls,
+                     const double *xin, double *xout, cudaStream_t st)
+{
+    // one block per FDM_LT consecutive values of the fastest fixed coordinate
+    const int fast = axis == 2 ? g.N1 : g.N2, slow = axis == 0 ? g.N1 : g.N0;
+    const unsigned nb = (unsigned)slow * (unsigned)((fast + FDM_LT - 1) / FDM_LT);
+    if (axis == 0)
+        k_fdm_line<0><<<nb, FDM_LINE_THREADS, 0, st>>>(g, coef, fac, ls, xin, xout);
+    else if (axis == 1)
+        k_fdm_line<1><<<nb, FDM_LINE_THREADS, 0, st>>>(g, coef, fac, ls, xin, xout);
+    else
+        k_fdm_line<2><<<nb, FDM_LINE_THREADS, 0, st>>>(g, coef, fac, ls, xin, xout);
 }
 
 }  // namespace nova

@@ -59,9 +59,12 @@ void launch_fdm_point(const Geo &g, int mode, double v, double *coef, const doub
 void launch_fdm_setref(const Geo &g, double *coef, long long n, double val, cudaStream_t st);
 void launch_fdm_residual(const Geo &g, const double *coef, const double *x, double *part, int nb, double *out,
                          cudaStream_t st);
-// one sweep of periodic tridiagonal line solves along axis; scratch: 3 N3 doubles
-void launch_fdm_sweep(int axis, const Geo &g, const double *coef, const double *xin, double *xout, double *scratch,
-                      cudaStream_t st);
+// the factors of the periodic tridiagonal line systems along axis: fac 4 N3
+// doubles, ls 2 x (lines along axis) doubles
+void launch_fdm_factor(int axis, const Geo &g, const double *coef, double *fac, double *ls, cudaStream_t st);
+// one sweep of line solves along axis with those factors, xin -> xout (distinct)
+void launch_fdm_line(int axis, const Geo &g, const double *coef, const double *fac, const double *ls,
+                     const double *xin, double *xout, cudaStream_t st);
 // the history row from nb blocks of partials (Ek, Em, max|div U|, max|div B| per block)
 void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
                        cudaStream_t st);

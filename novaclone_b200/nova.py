@@ -399,10 +399,14 @@ class FdMatrix:
     def __init__(self, mesh: Mesh, x: Field, h):
         self.mesh, self.x, self.h = mesh, x, h
 
-    def __del__(self):
+    def close(self):
+        """release the matrix's device memory now"""
         if getattr(self, "h", None) and self.mesh.lib is not None:
             self.mesh.lib.nova_fdm_destroy(self.h)
-            self.h = None
+        self.h = None
+
+    def __del__(self):
+        self.close()
 
     def add(self, other: "FdMatrix", alpha: float = 1.0) -> "FdMatrix":
         """self += alpha other (operator+ / operator-)"""

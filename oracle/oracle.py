@@ -647,7 +647,7 @@ def fdm_solve(mesh, al, ap, src, xg, tol, max_its):
 def ref_im(mesh, mu, c, xg, fg, tol, max_its):
     """The reference's im::laplacian(mu, x), ap -= c, (M == f).solve(tol, max_its)
     (oracle/_ref/nova_ref im): coefficients and source as built, x after the
-    solve, and the residual after it."""
+    solve, the residual after it and the solve's wall seconds."""
     with tempfile.TemporaryDirectory() as td:
         case = os.path.join(td, "case")
         write_case(case, mesh)
@@ -659,7 +659,8 @@ def ref_im(mesh, mu, c, xg, fg, tol, max_its):
                         str(int(max_its)), out, "-m", str(mesh.m)], check=True, stdout=subprocess.DEVNULL)
         rd = lambda k: np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n)
         return {"al": np.stack([rd("al%d" % l) for l in range(6)]), "ap": rd("ap"), "src": rd("src"),
-                "x": rd("x"), "res": float(open(out + "_res.txt").read())}
+                "x": rd("x"), "res": float(open(out + "_res.txt").read()),
+                "solve_s": float(open(out + "_time.txt").read())}
 
 
 # ------------------------------------------------------------- initial data --

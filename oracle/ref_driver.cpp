@@ -345,7 +345,7 @@ static int ops2(int argc, char **argv)
 /* the implicit Laplacian (src/im): M = im::laplacian(mu, x) (7-point coefficients and the
  * deferred correction against ex::laplacian), M.ap() -= c, then (M == f).solve(tol, maxits)
  * on x (the reference's line relaxation, fdMatrix.hxx:59-198); saves the coefficients and the
- * source as built, x after the solve and the residual */
+ * source as built, x after the solve, the residual and the solve's wall time */
 static int im_solve(int argc, char **argv)
 {
     if (argc < 10) { std::fprintf(stderr, "usage: im <case> <mu> <c> <x> <f> <tol> <maxits> <out>\n"); return 2; }
@@ -367,11 +367,16 @@ static int im_solve(int argc, char **argv)
     save(*dynamic_cast<Field<scalar> *>(M.get()), out + "_src.bin");
     M->ap() -= c;
     auto S = (M == f);
+    const auto t0 = std::chrono::steady_clock::now();
     S->solve(tol, maxits);
+    const double solve_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     save(*x, out + "_x.bin");
     const scalar res = S->residual();
     std::FILE *fp = std::fopen((out + "_res.txt").c_str(), "w");
     std::fprintf(fp, "%.17g\n", res);
+    std::fclose(fp);
+    fp = std::fopen((out + "_time.txt").c_str(), "w");  /* wall seconds of the solve call */
+    std::fprintf(fp, "%.9g\n", solve_s);
     std::fclose(fp);
     return 0;
 }
