@@ -251,7 +251,10 @@ nova_status nova_fdm_residual(nova_ctx *ctx, const nova_fdm *a, double *res);
  * lines), each as a Dirichlet problem whose ghost and duplicate end nodes keep
  * their values from the last ghost refresh (once per iteration): a different
  * iteration with the same fixed point.  its, res (the last residual checked)
- * may be NULL. */
+ * may be NULL.  The first call allocates the solve's device storage, kept
+ * until nova_fdm_destroy: a second x buffer and the factors of the three
+ * line directions, 13 N0 N1 N2 doubles plus two per line; the factors are
+ * recomputed only after a call that changes the coefficients. */
 nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, int max_its, int *its, double *res);
 /* the eight fields to the host, SoA over the unique nodes: al0..al5, ap, b (8 x N0 N1 N2 doubles) */
 nova_status nova_fdm_download(nova_ctx *ctx, const nova_fdm *a, double *host);

@@ -11,12 +11,13 @@
 //     reference counts, (N0+1)(N1+1)(N2+1) with the duplicate periodic nodes;
 //   solve (fdMatrix.hxx:59-198): line sweeps along j, i, k per iteration.
 //     The reference sweeps the lines of a direction one after another
-//     (Gauss-Seidel across lines) and holds the duplicate node of each line
-//     at its value from the last ghost refresh; here every line of a sweep is
-//     solved at once, the neighbours off the line taken at the sweep's start,
-//     as an exactly periodic tridiagonal system (Thomas' algorithm with the
-//     Sherman-Morrison correction for the two corner entries).  Both are
-//     iterations with the same fixed point, A x = b with periodic wrap.
+//     (Gauss-Seidel across lines) and holds the ghost and duplicate end
+//     nodes of each line at their values from the last ghost refresh; here
+//     every line of a sweep is solved at once, the neighbours off the line
+//     taken at the sweep's start, as an exactly periodic tridiagonal system
+//     (Thomas' algorithm with the Sherman-Morrison correction for the two
+//     corner entries).  Both are iterations with the same fixed point,
+//     A x = b with periodic wrap.
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"
 
