@@ -178,10 +178,10 @@ struct LineGeo {
     static __device__ __forceinline__ int nfast(const Geo &g) { return AXIS == 2 ? g.N1 : g.N2; }
 };
 
-// Factors of the periodic tridiagonal system of every line along AXIS, one
-// line per thread.  The line's rows a_t x_{t-1} + b_t x_t + c_t x_{t+1} = d_t
-// wrap around (x_{-1} = x_{n-1}, x_n = x_0).  Folding the two corner entries
-// into the diagonal with gamma = -b_0 gives the open tridiagonal T' with
+// Factors of the periodic tridiagonal system of every line along AXIS.  The
+// line's rows a_t x_{t-1} + b_t x_t + c_t x_{t+1} = d_t wrap around
+// (x_{-1} = x_{n-1}, x_n = x_0).  Folding the two corner entries into the
+// diagonal with gamma = -b_0 gives the open tridiagonal T' with
 // T = T' + u v^T, u = (gamma, 0.., c_{n-1}), v = (1, 0.., a_0/gamma), so
 // (Sherman-Morrison) x = y - z (v.y)/(1 + v.z) with T' y = d, T' z = u.
 // Stored per node (fac = [w | cp | P | z], 4 N3 per axis): the inverse Thomas
@@ -190,59 +190,160 @@ struct LineGeo {
 // P_t yhat_t over the forward-eliminated yhat; per line (ls = [q | h]):
 // q = a_0/gamma, h = 1/(1 + v.z).  The coefficients do not change while a
 // solve runs, so this runs once per solve, and again only after they change.
+// Blocks, tiles and warp 0's recurrences are those of k_fdm_line below: the
+// forward pass turns a chunk's (a, b, c) into (w, cp, P, zhat) in place, the
+// backward pass zhat into z.
+constexpr int FDM_LT = 32, FDM_TT = 16, FDM_LINE_THREADS = 256;
+constexpr int FDM_PER = FDM_LT * FDM_TT / FDM_LINE_THREADS;  // tile elements per thread
+static_assert(FDM_LT * FDM_TT % FDM_LINE_THREADS == 0, "tile elements split evenly over the threads");
+
 template <int AXIS>
-__global__ void k_fdm_factor(Geo g, const double *__restrict__ coef, double *fac, double *ls)
+__global__ void __launch_bounds__(FDM_LINE_THREADS, 4) k_fdm_factor(Geo g, const double *__restrict__ coef,
+                                                                     double *fac, double *ls)
 {
     using LG = LineGeo<AXIS>;
-    constexpr int LO = LG::LO, HI = LG::HI;
+    constexpr int LO = LG::LO, HI = LG::HI, LT = FDM_LT, TT = FDM_TT;
+    __shared__ double sm[4][LT][TT + 1];
     const long long N3 = g.N3;
     const int n = LG::len(g), nf = LG::nfast(g);
     const long long lines = N3 / n;
-    const long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (line >= lines) return;
-    const int slow = (int)(line / nf), fast = (int)(line % nf);
-    auto node = [&](int t) {
+    const int groups = (nf + LT - 1) / LT;
+    const int slow = (int)(blockIdx.x / groups), f0 = (int)(blockIdx.x % groups) * LT;
+    const int nl = min(LT, nf - f0);
+    const long long line0 = (long long)slow * nf + f0;
+    double *W = fac, *CP = fac + N3, *P = fac + 2 * N3, *Z = fac + 3 * N3;
+    const int tid = threadIdx.x;
+    auto elem = [&](int e, int &l, int &tt) {
+        if (AXIS == 2) {
+            l = e / TT;
+            tt = e % TT;
+        } else {
+            l = e % LT;
+            tt = e / LT;
+        }
+    };
+    auto node = [&](int l, int t) {
         int i, j, k;
-        LG::coords(slow, fast, t, i, j, k);
+        LG::coords(slow, f0 + l, t, i, j, k);
         return nidx(g, i, j, k);
     };
-    double *W = fac, *CP = fac + N3, *P = fac + 2 * N3, *Z = fac + 3 * N3;
-    const long long o0 = node(0), on = node(n - 1);
-    const double a0 = coef[LO * N3 + o0], cn = coef[HI * N3 + on];
-    const double gam = -coef[6 * N3 + o0];
-    double cprev = 0.0, zprev = 0.0, pprev = 1.0;
-    for (int t = 0; t < n; t++) {
-        const long long o = node(t);
-        const double a = t == 0 ? 0.0 : coef[LO * N3 + o];
-        const double c = t == n - 1 ? 0.0 : coef[HI * N3 + o];
-        double b = coef[6 * N3 + o];
-        if (t == 0) b -= gam;
-        if (t == n - 1) b -= cn * a0 / gam;
-        const double u = t == 0 ? gam : (t == n - 1 ? cn : 0.0);
-        const double w = 1.0 / (b - a * cprev);
-        const double p = t == 0 ? 1.0 : pprev * -cprev;
-        const double cc = c * w;
-        const double zz = (u - a * zprev) * w;
-        W[o] = w;
-        CP[o] = cc;
-        P[o] = p;
-        Z[o] = zz;
-        cprev = cc;
-        zprev = zz;
-        pprev = p;
+    const int nch = (n + TT - 1) / TT;
+    // warp 0, lane l: line l's corner entries and running values
+    double a0 = 0.0, cn = 0.0, gam = 1.0, cprev = 0.0, zprev = 0.0, pprev = 1.0;
+    if (tid < nl) {
+        a0 = coef[LO * N3 + node(tid, 0)];
+        cn = coef[HI * N3 + node(tid, n - 1)];
+        gam = -coef[6 * N3 + node(tid, 0)];
     }
+
+    // forward elimination: slots (a, b, c) in, (w, cp, P, zhat) out
+    for (int c = 0; c < nch; c++) {
+        const int t0 = c * TT, nt = min(TT, n - t0);
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            if (c > 0 && l < nl) {  // the previous (full) chunk's factors
+                const long long o = node(l, t0 - TT + tt);
+                W[o] = sm[0][l][tt];
+                CP[o] = sm[1][l][tt];
+                P[o] = sm[2][l][tt];
+                Z[o] = sm[3][l][tt];
+            }
+            const bool in = l < nl && tt < nt;
+            const int t = in ? t0 + tt : t0;
+            const long long o = node(in ? l : 0, t);
+            const double av = t == 0 ? 0.0 : coef[LO * N3 + o], bv = coef[6 * N3 + o],
+                         cv = t == n - 1 ? 0.0 : coef[HI * N3 + o];
+            if (in) {
+                sm[0][l][tt] = av;
+                sm[1][l][tt] = bv;
+                sm[2][l][tt] = cv;
+            }
+        }
+        __syncthreads();
+        if (tid < nl) {
+            const int l = tid;
+            for (int tt = 0; tt < nt; tt++) {
+                const int t = t0 + tt;
+                const double a = sm[0][l][tt], cc = sm[2][l][tt];
+                double bb = sm[1][l][tt];
+                if (t == 0) bb -= gam;
+                if (t == n - 1) bb -= cn * a0 / gam;
+                const double u = t == 0 ? gam : (t == n - 1 ? cn : 0.0);
+                const double w = 1.0 / (bb - a * cprev);
+                const double p = t == 0 ? 1.0 : pprev * -cprev;
+                const double cpv = cc * w;
+                const double zz = (u - a * zprev) * w;
+                sm[0][l][tt] = w;
+                sm[1][l][tt] = cpv;
+                sm[2][l][tt] = p;
+                sm[3][l][tt] = zz;
+                cprev = cpv;
+                zprev = zz;
+                pprev = p;
+            }
+        }
+        __syncthreads();
+    }
+    {  // the last chunk's factors
+        const int t0 = (nch - 1) * TT, nt = n - t0;
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            if (l >= nl || tt >= nt) continue;
+            const long long o = node(l, t0 + tt);
+            W[o] = sm[0][l][tt];
+            CP[o] = sm[1][l][tt];
+            P[o] = sm[2][l][tt];
+            Z[o] = sm[3][l][tt];
+        }
+    }
+    __syncthreads();
+
+    // z = zhat back-substituted, from the last chunk to the first
     double znext = 0.0, z0 = 0.0, zn = 0.0;
-    for (int t = n - 1; t >= 0; t--) {
-        const long long o = node(t);
-        const double zz = Z[o] - CP[o] * znext;
-        Z[o] = zz;
-        znext = zz;
-        if (t == n - 1) zn = zz;
-        if (t == 0) z0 = zz;
+    for (int c = nch - 1; c >= 0; c--) {
+        const int t0 = c * TT, nt = min(TT, n - t0);
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            const bool in = l < nl && tt < nt;
+            const long long o = in ? node(l, t0 + tt) : node(0, t0);
+            const double cpv = CP[o], zh = Z[o];
+            if (in) {
+                sm[1][l][tt] = cpv;
+                sm[3][l][tt] = zh;
+            }
+        }
+        __syncthreads();
+        if (tid < nl) {
+            const int l = tid;
+            for (int tt = nt - 1; tt >= 0; tt--) {
+                const double zz = sm[3][l][tt] - sm[1][l][tt] * znext;
+                sm[3][l][tt] = zz;
+                znext = zz;
+                if (t0 + tt == n - 1) zn = zz;
+                if (t0 + tt == 0) z0 = zz;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            if (l >= nl || tt >= nt) continue;
+            Z[node(l, t0 + tt)] = sm[3][l][tt];
+        }
+        __syncthreads();
     }
-    const double q = a0 / gam;
-    ls[line] = q;
-    ls[lines + line] = 1.0 / (1.0 + z0 + q * zn);
+    if (tid < nl) {
+        const double q = a0 / gam;
+        ls[line0 + tid] = q;
+        ls[lines + line0 + tid] = 1.0 / (1.0 + z0 + q * zn);
+    }
 }
 
 // One sweep along AXIS with the factors of k_fdm_factor: every line solved at
@@ -255,10 +356,6 @@ __global__ void k_fdm_factor(Geo g, const double *__restrict__ coef, double *fac
 //   forward   yhat_t = (d_t - a_t yhat_{t-1}) w_t,  Y0 += P_t yhat_t   (yhat into xout)
 //   f = (Y0 + q yhat_{n-1}) h                                            (= (v.y)/(1 + v.z))
 //   backward  y_t = yhat_t - cp_t y_{t+1},  x_t = y_t - f z_t           (xout in place)
-constexpr int FDM_LT = 32, FDM_TT = 16, FDM_LINE_THREADS = 256;
-constexpr int FDM_PER = FDM_LT * FDM_TT / FDM_LINE_THREADS;  // tile elements per thread
-static_assert(FDM_LT * FDM_TT % FDM_LINE_THREADS == 0, "tile elements split evenly over the threads");
-
 template <int AXIS>
 __global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const double *__restrict__ coef,
                                                                 const double *__restrict__ fac,
@@ -434,14 +531,15 @@ void launch_fdm_residual(const Geo &g, const double *coef, const double *x, doub
 
 void launch_fdm_factor(int axis, const Geo &g, const double *coef, double *fac, double *ls, cudaStream_t st)
 {
-    const int n = axis == 0 ? g.N0 : (axis == 1 ? g.N1 : g.N2);
-    const unsigned nb = blocks_for(g.N3 / n, 128);
+    // the blocks of k_fdm_line
+    const int fast = axis == 2 ? g.N1 : g.N2, slow = axis == 0 ? g.N1 : g.N0;
+    const unsigned nb = (unsigned)slow * (unsigned)((fast + FDM_LT - 1) / FDM_LT);
     if (axis == 0)
-        k_fdm_factor<0><<<nb, 128, 0, st>>>(g, coef, fac, ls);
+        k_fdm_factor<0><<<nb, FDM_LINE_THREADS, 0, st>>>(g, coef, fac, ls);
     else if (axis == 1)
-        k_fdm_factor<1><<<nb, 128, 0, st>>>(g, coef, fac, ls);
+        k_fdm_factor<1><<<nb, FDM_LINE_THREADS, 0, st>>>(g, coef, fac, ls);
     else
-        k_fdm_factor<2><<<nb, 128, 0, st>>>(g, coef, fac, ls);
+        k_fdm_factor<2><<<nb, FDM_LINE_THREADS, 0, st>>>(g, coef, fac, ls);
 }
 
 void launch_fdm_line(int axis, const Geo &g, const double *coef, const double *fac, const double *ls,
