@@ -356,8 +356,11 @@ __global__ void __launch_bounds__(FDM_LINE_THREADS, 4) k_fdm_factor(Geo g, const
 //   forward   yhat_t = (d_t - a_t yhat_{t-1}) w_t,  Y0 += P_t yhat_t   (yhat into xout)
 //   f = (Y0 + q yhat_{n-1}) h                                            (= (v.y)/(1 + v.z))
 //   backward  y_t = yhat_t - cp_t y_{t+1},  x_t = y_t - f z_t           (xout in place)
+// Every thread loads its tile elements of the next chunk into registers
+// before the block waits for warp 0, so those loads are in flight during the
+// recurrences and the barriers.
 template <int AXIS>
-__global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const double *__restrict__ coef,
+__global__ void __launch_bounds__(FDM_LINE_THREADS, 3) k_fdm_line(Geo g, const double *__restrict__ coef,
                                                                 const double *__restrict__ fac,
                                                                 const double *__restrict__ ls,
                                                                 const double *__restrict__ xin, double *xout)
@@ -390,10 +393,56 @@ __global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const d
         return nidx(g, i, j, k);
     };
     const int nch = (n + TT - 1) / TT;
+
+    // a thread's forward operands of one tile element, as loaded: the source,
+    // the four coefficients off the line and their neighbours (in the order
+    // they are subtracted), the coefficient below the diagonal, w and P;
+    // elements past the lines' or the chunk's end load node (0, t0)
+    struct Fwd {
+        double b, c[4], x[4], lo, w, p;
+    };
+    Fwd R[FDM_PER];
+    auto load_fwd = [&](int c) {
+        const int t0 = c * TT, nt = min(TT, n - t0);
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            const bool in = l < nl && tt < nt;
+            const int t = in ? t0 + tt : t0;
+            int i, j, k;
+            LG::coords(slow, f0 + (in ? l : 0), t, i, j, k);
+            const long long o = nidx(g, i, j, k);
+            R[m].b = coef[7 * N3 + o];
+            int q = 0;
+            if (AXIS != 1) {
+                R[m].c[q] = coef[0 * N3 + o];
+                R[m].x[q++] = xin[nidx(g, i, wrapi(j + 1, g.N1), k)];
+                R[m].c[q] = coef[1 * N3 + o];
+                R[m].x[q++] = xin[nidx(g, i, wrapi(j - 1, g.N1), k)];
+            }
+            if (AXIS != 0) {
+                R[m].c[q] = coef[2 * N3 + o];
+                R[m].x[q++] = xin[nidx(g, wrapi(i + 1, g.N0), j, k)];
+                R[m].c[q] = coef[3 * N3 + o];
+                R[m].x[q++] = xin[nidx(g, wrapi(i - 1, g.N0), j, k)];
+            }
+            if (AXIS != 2) {
+                R[m].c[q] = coef[4 * N3 + o];
+                R[m].x[q++] = xin[nidx(g, i, j, wrapi(k + 1, g.N2))];
+                R[m].c[q] = coef[5 * N3 + o];
+                R[m].x[q++] = xin[nidx(g, i, j, wrapi(k - 1, g.N2))];
+            }
+            R[m].lo = t == 0 ? 0.0 : coef[LO * N3 + o];
+            R[m].w = W[o];
+            R[m].p = P[o];
+        }
+    };
     double yh = 0.0, Y0 = 0.0;  // warp 0, lane l: line l's last yhat and the sum for y_0
 
-    // forward elimination, chunk by chunk; a thread stores the previous chunk's
-    // yhat of its own tile elements before it loads the next chunk into them
+    // forward elimination; a thread stores the previous chunk's yhat of its own
+    // tile elements before it puts the next chunk's operands into them
+    load_fwd(0);
     for (int c = 0; c < nch; c++) {
         const int t0 = c * TT, nt = min(TT, n - t0);
 #pragma unroll
@@ -401,33 +450,17 @@ __global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const d
             int l, tt;
             elem(tid + m * FDM_LINE_THREADS, l, tt);
             if (c > 0 && l < nl) xout[node(l, t0 - TT + tt)] = sm[0][l][tt];  // chunks before the last are full
-            // elements past the lines' or the chunk's end read node (0, t0) and store nothing
-            const bool in = l < nl && tt < nt;
-            const int t = in ? t0 + tt : t0;
-            int i, j, k;
-            LG::coords(slow, f0 + (in ? l : 0), t, i, j, k);
-            const long long o = nidx(g, i, j, k);
-            double d = coef[7 * N3 + o];
-            if (AXIS != 1) {
-                d -= coef[0 * N3 + o] * xin[nidx(g, i, wrapi(j + 1, g.N1), k)];
-                d -= coef[1 * N3 + o] * xin[nidx(g, i, wrapi(j - 1, g.N1), k)];
-            }
-            if (AXIS != 0) {
-                d -= coef[2 * N3 + o] * xin[nidx(g, wrapi(i + 1, g.N0), j, k)];
-                d -= coef[3 * N3 + o] * xin[nidx(g, wrapi(i - 1, g.N0), j, k)];
-            }
-            if (AXIS != 2) {
-                d -= coef[4 * N3 + o] * xin[nidx(g, i, j, wrapi(k + 1, g.N2))];
-                d -= coef[5 * N3 + o] * xin[nidx(g, i, j, wrapi(k - 1, g.N2))];
-            }
-            const double lo = t == 0 ? 0.0 : coef[LO * N3 + o], w = W[o], p = P[o];
-            if (in) {
+            if (l < nl && tt < nt) {
+                double d = R[m].b;
+#pragma unroll
+                for (int q = 0; q < 4; q++) d -= R[m].c[q] * R[m].x[q];
                 sm[0][l][tt] = d;
-                sm[1][l][tt] = lo;
-                sm[2][l][tt] = w;
-                sm[3][l][tt] = p;
+                sm[1][l][tt] = R[m].lo;
+                sm[2][l][tt] = R[m].w;
+                sm[3][l][tt] = R[m].p;
             }
         }
+        if (c + 1 < nch) load_fwd(c + 1);
         __syncthreads();
         if (tid < nl) {
             const int l = tid;
@@ -440,21 +473,13 @@ __global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const d
         }
         __syncthreads();
     }
-    {  // the last chunk's yhat
-        const int t0 = (nch - 1) * TT, nt = n - t0;
-        for (int e = tid; e < LT * TT; e += FDM_LINE_THREADS) {
-            int l, tt;
-            elem(e, l, tt);
-            if (l >= nl || tt >= nt) continue;
-            xout[node(l, t0 + tt)] = sm[0][l][tt];
-        }
-    }
-    double f = 0.0, ynext = 0.0;
-    if (tid < nl) f = (Y0 + ls[line0 + tid] * yh) * ls[lines + line0 + tid];
-    __syncthreads();
 
-    // back substitution and the correction, from the last chunk to the first
-    for (int c = nch - 1; c >= 0; c--) {
+    // a thread's backward operands of one tile element: yhat, cp, z
+    struct Bwd {
+        double y, cp, z;
+    };
+    Bwd S[FDM_PER];
+    auto load_bwd = [&](int c) {
         const int t0 = c * TT, nt = min(TT, n - t0);
 #pragma unroll
         for (int m = 0; m < FDM_PER; m++) {
@@ -462,13 +487,41 @@ __global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const d
             elem(tid + m * FDM_LINE_THREADS, l, tt);
             const bool in = l < nl && tt < nt;
             const long long o = in ? node(l, t0 + tt) : node(0, t0);
-            const double yv = xout[o], cp = CP[o], z = Z[o];
-            if (in) {
-                sm[0][l][tt] = yv;
-                sm[1][l][tt] = cp;
-                sm[2][l][tt] = z;
+            S[m].y = xout[o];
+            S[m].cp = CP[o];
+            S[m].z = Z[o];
+        }
+    };
+    {  // the last chunk's yhat, then the backward operands of that chunk
+        const int t0 = (nch - 1) * TT, nt = n - t0;
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            if (l < nl && tt < nt) xout[node(l, t0 + tt)] = sm[0][l][tt];
+        }
+        load_bwd(nch - 1);
+    }
+    double f = 0.0, ynext = 0.0;
+    if (tid < nl) f = (Y0 + ls[line0 + tid] * yh) * ls[lines + line0 + tid];
+
+    // back substitution and the correction, from the last chunk to the first;
+    // a thread stores the previous chunk's x of its own tile elements before it
+    // puts the next chunk's operands into them
+    for (int c = nch - 1; c >= 0; c--) {
+        const int t0 = c * TT, nt = min(TT, n - t0);
+#pragma unroll
+        for (int m = 0; m < FDM_PER; m++) {
+            int l, tt;
+            elem(tid + m * FDM_LINE_THREADS, l, tt);
+            if (c + 1 < nch && l < nl && t0 + TT + tt < n) xout[node(l, t0 + TT + tt)] = sm[0][l][tt];
+            if (l < nl && tt < nt) {
+                sm[0][l][tt] = S[m].y;
+                sm[1][l][tt] = S[m].cp;
+                sm[2][l][tt] = S[m].z;
             }
         }
+        if (c > 0) load_bwd(c - 1);
         __syncthreads();
         if (tid < nl) {
             const int l = tid;
@@ -480,13 +533,12 @@ __global__ void __launch_bounds__(FDM_LINE_THREADS, 6) k_fdm_line(Geo g, const d
             }
         }
         __syncthreads();
-        for (int e = tid; e < LT * TT; e += FDM_LINE_THREADS) {
-            int l, tt;
-            elem(e, l, tt);
-            if (l >= nl || tt >= nt) continue;
-            xout[node(l, t0 + tt)] = sm[0][l][tt];
-        }
-        __syncthreads();
+    }
+#pragma unroll
+    for (int m = 0; m < FDM_PER; m++) {  // chunk 0's x
+        int l, tt;
+        elem(tid + m * FDM_LINE_THREADS, l, tt);
+        if (l < nl && tt < min(TT, n)) xout[node(l, tt)] = sm[0][l][tt];
     }
 }
 
