@@ -3,7 +3,8 @@
 // ghosted array-of-structs storage of src/Field/Field.h:56-157,
 // correctBoundaryConditions(), ex::grad/div/curl/laplacian returning
 // std::shared_ptr<Field<T>> (src/ex/*/ *.h), poisson(p).rhs(f).solve()
-// (src/poisson/poisson.h:36-115) and tools::maximum (src/Tools/Tools.h:19-36).
+// (src/poisson/poisson.h:36-115), tools::maximum (src/Tools/Tools.h:19-36) and
+// im::laplacian with its fdMatrix (src/im).
 // Each call runs on the GPU through the C ABI; host Fields are the caller's
 // buffers in the reference layout, uploaded and downloaded per call.  The
 // fused path replaces a whole loop body (RKLoop.H / UEqn.H + BEqn.H) with
@@ -17,6 +18,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "nova_gpu.h"
@@ -217,6 +219,131 @@ inline scalar maximum(const std::shared_ptr<Field<scalar>> &f)
     return v;
 }
 }  // namespace tools
+
+// fdMatrix<scalar> (src/im/fdMatrix/fdMatrix.h:33-77): the matrix lives on the
+// device (nova_fdm); the transported field stays the caller's Field<scalar>,
+// uploaded before every call that reads it and downloaded after solve().
+// Like the reference's operators, these change the matrix in place.
+template <class T> class fdMatrix {
+    static_assert(std::is_same<T, scalar>::value, "the implicit operators are built for scalar fields");
+    std::shared_ptr<Field<T>> x_;
+    std::shared_ptr<nova_fdm> m_;
+    nova_ctx *ctx() const { return x_->mesh().ctx(); }
+
+public:
+    fdMatrix(std::shared_ptr<Field<T>> x, nova_fdm *m) : x_(std::move(x)), m_(m, nova_fdm_destroy) {}
+    nova_fdm *dev() const { return m_.get(); }
+
+    // ap() += d / ap() -= d, the Field arithmetic apps apply to fdMatrix::ap()
+    class Diagonal {
+        fdMatrix &a_;
+
+    public:
+        explicit Diagonal(fdMatrix &a) : a_(a) {}
+        Diagonal &operator+=(scalar d)
+        {
+            check(a_.ctx(), nova_fdm_add_diagonal(a_.ctx(), a_.dev(), d), "nova_fdm_add_diagonal");
+            return *this;
+        }
+        Diagonal &operator-=(scalar d) { return *this += -d; }
+    };
+    Diagonal ap() { return Diagonal(*this); }
+
+    // fdMatrix::solve (fdMatrix.hxx:59-198): x is the initial guess and the result
+    void solve(scalar tol, int maxIts)
+    {
+        x_->toDevice();
+        check(ctx(), nova_fdm_solve(ctx(), dev(), tol, maxIts, nullptr, nullptr), "nova_fdm_solve");
+        x_->fromDevice();
+    }
+    T residual()
+    {
+        x_->toDevice();
+        double r = 0.0;
+        check(ctx(), nova_fdm_residual(ctx(), dev(), &r), "nova_fdm_residual");
+        return r;
+    }
+    void relax(const scalar &urf)
+    {
+        x_->toDevice();
+        check(ctx(), nova_fdm_relax(ctx(), dev(), urf), "nova_fdm_relax");
+    }
+    // (i, j, k) index the ghosted field as in the reference (m/2 ghost nodes
+    // first); the node is taken modulo the periodic length, so the duplicate
+    // end node N is node 0
+    void setReference(int i, int j, int k, scalar val)
+    {
+        const nova_mesh_desc &d = x_->mesh().desc();
+        const int h = d.m / 2, idx[3] = {i, j, k};
+        int u[3];
+        for (int a = 0; a < 3; a++) u[a] = ((idx[a] - h) % d.N[a] + d.N[a]) % d.N[a];
+        check(ctx(), nova_fdm_set_reference(ctx(), dev(), u[0], u[1], u[2], val), "nova_fdm_set_reference");
+    }
+    fdMatrix &operator+=(const fdMatrix &r)
+    {
+        check(ctx(), nova_fdm_add(ctx(), dev(), 1.0, r.dev()), "nova_fdm_add");
+        return *this;
+    }
+    fdMatrix &operator-=(const fdMatrix &r)
+    {
+        check(ctx(), nova_fdm_add(ctx(), dev(), -1.0, r.dev()), "nova_fdm_add");
+        return *this;
+    }
+    fdMatrix &operator*=(const fdMatrix &r)
+    {
+        check(ctx(), nova_fdm_mul(ctx(), dev(), r.dev()), "nova_fdm_mul");
+        return *this;
+    }
+    // the source += f
+    void operator==(const Field<T> &f)
+    {
+        f.toDevice();
+        check(ctx(), nova_fdm_add_source(ctx(), dev(), 1.0, f.dev()), "nova_fdm_add_source");
+    }
+    void negate() { check(ctx(), nova_fdm_scale(ctx(), dev(), -1.0), "nova_fdm_scale"); }
+};
+
+// the global operators of fdMatrix.hxx:359-413: the left operand, changed in place
+template <class T>
+std::shared_ptr<fdMatrix<T>> operator+(std::shared_ptr<fdMatrix<T>> a, const std::shared_ptr<fdMatrix<T>> &b)
+{
+    *a += *b;
+    return a;
+}
+template <class T>
+std::shared_ptr<fdMatrix<T>> operator-(std::shared_ptr<fdMatrix<T>> a, const std::shared_ptr<fdMatrix<T>> &b)
+{
+    *a -= *b;
+    return a;
+}
+template <class T> std::shared_ptr<fdMatrix<T>> operator-(std::shared_ptr<fdMatrix<T>> a)
+{
+    a->negate();
+    return a;
+}
+template <class T>
+std::shared_ptr<fdMatrix<T>> operator==(std::shared_ptr<fdMatrix<T>> a, const std::shared_ptr<Field<T>> &f)
+{
+    *a == *f;
+    return a;
+}
+
+namespace im {
+// im::laplacian(mu, x) (src/im/laplacian/laplacian.hxx:24-58)
+template <class T> std::shared_ptr<fdMatrix<T>> laplacian(const scalar mu, std::shared_ptr<Field<T>> x)
+{
+    static_assert(std::is_same<T, scalar>::value, "the implicit operators are built for scalar fields");
+    x->toDevice();
+    nova_fdm *m = nullptr;
+    check(x->mesh().ctx(), nova_im_laplacian(x->mesh().ctx(), mu, x->dev(), &m), "nova_im_laplacian");
+    return std::make_shared<fdMatrix<T>>(std::move(x), m);
+}
+// im::laplacian(x) = im::laplacian(1, x) (laplacian.hxx:61-68)
+template <class T> std::shared_ptr<fdMatrix<T>> laplacian(std::shared_ptr<Field<T>> x)
+{
+    return laplacian(scalar(1.0), std::move(x));
+}
+}  // namespace im
 
 // The fused loop body: state resident on the device between calls.
 class Advance {

@@ -61,10 +61,12 @@ int main(void) {
     assert [int(v) for v in got] == want
 
 
-def test_cpp_adapter_compiles():
+@pytest.mark.parametrize("prog", ["tg_driver.cpp", "im_driver.cpp"])
+def test_cpp_adapter_compiles(prog):
     """The header-only C++ adapter (include/nova/nova.hpp) builds against the C ABI."""
-    src = os.path.join(ROOT, "tests", "cpp", "tg_driver.cpp")
-    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I" + os.path.join(ROOT, "include"), src], check=True)
+    src = os.path.join(ROOT, "tests", "cpp", prog)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I" + os.path.join(ROOT, "include"),
+                    src], check=True)
 
 
 def test_invalid_arguments_rejected_without_gpu(lib):

@@ -141,3 +141,31 @@ def test_iterations_match_line_model(nova, its):
     xa = x.download_soa()[0]
     A.solve(0.0, 2)
     assert rel_l2(x.download_soa()[0], line_jacobi_model(al, ap, b, xa, 2)) < 1e-13
+
+
+def test_cpp_adapter_im_driver(tmp_path):
+    """The reference-style C++ program (tests/cpp/im_driver.cpp) through
+    include/nova/nova.hpp: (im::laplacian(mu, x) - c) == f, solve, on the golden
+    case, against the reference's own solution."""
+    import os
+    import subprocess
+    from oracle import oracle as O
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "novaclone_b200")
+    exe = tmp_path / "im_driver"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "im_driver.cpp"), "-L" + libdir, "-lnova_b200",
+                    "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    g = load_golden("im_7x6x8.npz")
+    OM = O.Mesh(tuple(int(v) for v in g["N"]), L=tuple(g["L"]))
+    case = tmp_path / "case"
+    O.write_case(str(case), OM)
+    OM.to_ghosted(g["x"]).tofile(str(tmp_path / "x.bin"))
+    OM.to_ghosted(g["f"]).tofile(str(tmp_path / "f.bin"))
+    out = tmp_path / "out.bin"
+    res = subprocess.run([str(exe), str(case), repr(float(g["mu"])), repr(float(g["c"])), str(tmp_path / "x.bin"),
+                          str(tmp_path / "f.bin"), repr(float(g["tol"])), str(int(g["max_its"])), str(out)],
+                         capture_output=True, text=True, check=True)
+    assert float(res.stdout.split()[-1]) <= float(g["tol"])
+    x = OM.unique(np.fromfile(str(out)).reshape(OM.n + (1,)))
+    assert rel_l2(x, g["x_solved"]) < 1e-12
