@@ -2131,6 +2131,13 @@ extern "C" nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, in
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_solve: bad matrix")) != NOVA_OK) return s;
     if (max_its < 0) return fail(ctx, NOVA_E_INVALID, "nova_fdm_solve: max_its must not be negative");
+    if (max_its == 0) {  // no iteration: only the residual of x, and nothing to allocate
+        double r = 0.0;
+        if ((s = fdm_res(ctx, a, a->x->d64, &r)) != NOVA_OK) return s;
+        if (its) *its = 0;
+        if (res) *res = r;
+        return NOVA_OK;
+    }
     const Geo &g = ctx->g;
     if ((s = dalloc(ctx, &a->scratch, (size_t)g.N3)) != NOVA_OK) return s;
     // factors of the three line directions (4 N3 each) and their per-line scalars (2 per line)
@@ -2145,7 +2152,7 @@ extern "C" nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, in
             q += 2 * lines[ax];
         }
     }
-    if (!a->factored && max_its > 0) {
+    if (!a->factored) {
         for (int ax = 0; ax < 3; ax++) launch_fdm_factor(ax, g, a->coef, fac[ax], ls[ax], ctx->stream);
         ctx->launches += 3;
         CKL("k_fdm_factor");
@@ -2155,7 +2162,6 @@ extern "C" nova_status nova_fdm_solve(nova_ctx *ctx, nova_fdm *a, double tol, in
     double *cur = a->x->d64, *other = a->scratch;
     double r = 0.0;
     int n = 0;
-    if (max_its == 0 && (s = fdm_res(ctx, a, cur, &r)) != NOVA_OK) return s;
     while (n < max_its) {
         // the residual checked before each iteration, as the reference reports it
         if ((s = fdm_res(ctx, a, cur, &r)) != NOVA_OK) return s;

@@ -80,6 +80,22 @@ def test_invalid_arguments_rejected_without_gpu(lib):
     assert lib.nova_advance(None, None, None, 1, None) == nova.E_INVALID
 
 
+def test_implicit_operators_reject_null_handles(lib):
+    """Every nova_fdm_* entry point (and nova_im_laplacian) refuses a missing
+    context, matrix or field with NOVA_E_INVALID before touching the device."""
+    from novaclone_b200 import nova
+    h = C.c_void_p()
+    its, res = C.c_int(), C.c_double()
+    assert lib.nova_im_laplacian(None, 1.0, None, C.byref(h)) == nova.E_INVALID
+    calls = [lib.nova_fdm_add(None, None, 1.0, None), lib.nova_fdm_mul(None, None, None),
+             lib.nova_fdm_scale(None, None, -1.0), lib.nova_fdm_add_source(None, None, 1.0, None),
+             lib.nova_fdm_add_diagonal(None, None, 1.0), lib.nova_fdm_relax(None, None, 0.5),
+             lib.nova_fdm_set_reference(None, None, 0, 0, 0, 1.0), lib.nova_fdm_residual(None, None, C.byref(res)),
+             lib.nova_fdm_solve(None, None, 0.0, 1, C.byref(its), C.byref(res)), lib.nova_fdm_download(None, None, None)]
+    assert calls == [nova.E_INVALID] * len(calls)
+    assert lib.nova_fdm_destroy(None) == nova.OK
+
+
 def test_no_silent_cpu_fallback(lib):
     """On a machine without a GPU, creating a context fails with a CUDA error."""
     import torch

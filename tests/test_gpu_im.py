@@ -120,6 +120,18 @@ def test_refusals(nova):
     with pytest.raises(nova.NovaError) as e:
         A.relax(0.0)
     assert e.value.status == nova.E_INVALID
+    with pytest.raises(nova.NovaError) as e:
+        A.solve(0.0, -1)
+    assert e.value.status == nova.E_INVALID
+
+
+def test_solve_without_iterations_reports_the_residual(nova):
+    N = (8, 10, 12)
+    x0 = np.random.default_rng(9).standard_normal((1,) + N)
+    M, x, A = build(nova, N, (1.0, 2.0, 3.0), 0.4, x0)
+    A.add_diagonal(-2.0)
+    assert A.solve(0.0, 0) == (0, A.residual())
+    assert np.array_equal(x.download_soa(), x0)
 
 
 @pytest.mark.parametrize("its", [1, 2, 3])
