@@ -140,17 +140,18 @@ def ops2_case(name, N, L, seed):
                         **{"out_" + k: M.interior(v) for k, v in out.items()})
 
 
-def im_case(name, N, L, seed, mu, c, tol, max_its):
+def im_case(name, N, L, seed, mu, c, tol, max_its, m=6):
     """the reference's im::laplacian(mu, x) (coefficients, deferred-correction
-    source), ap -= c, and (M == f).solve(tol, max_its) on x"""
-    M = O.Mesh(N, L=L)
+    source), ap -= c, and (M == f).solve(tol, max_its) on x, stencil order m"""
+    M = O.Mesh(N, L=L, m=m)
     rng = np.random.default_rng(seed)
     x = rng.standard_normal((1,) + M.N)
     f = rng.standard_normal((1,) + M.N)
     out = O.ref_im(M, mu, c, M.to_ghosted(x), M.to_ghosted(f), tol, max_its)
     h = M.h
     inner = (slice(h, h + N[0]), slice(h, h + N[1]), slice(h, h + N[2]))
-    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(L), mu=np.array(mu), c=np.array(c),
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(L), m=np.array(m), mu=np.array(mu),
+                        c=np.array(c),
                         tol=np.array(tol), max_its=np.array(max_its), x=x, f=f,
                         al=np.stack([a[inner] for a in out["al"]]), ap=out["ap"][inner], src=out["src"][inner],
                         x_solved=out["x"][inner][None], res=np.array(out["res"]))
@@ -169,6 +170,7 @@ CASES = {
     "ensight_7x5x6.npz": lambda n: ensight_case(n, (7, 5, 6), (2.0, 1.5, 3.0), (0.5, -1.0, 0.25), 11),
     "ensight_walls_6x8x5.npz": lambda n: ensight_case(n, (6, 8, 5), (1.0, 2.0, 1.5), (0.0, 0.0, 0.0), 12, True),
     "im_7x6x8.npz": lambda n: im_case(n, (7, 6, 8), (2.0, 1.5, 3.0), 17, 0.7, 6.0, 1e-14, 400),
+    "im_9x5x6_m4.npz": lambda n: im_case(n, (9, 5, 6), (1.5, 1.0, 2.5), 23, 0.35, 4.0, 1e-14, 600, m=4),
 }
 
 

@@ -1,8 +1,9 @@
 """The fixed point of the GPU's implicit solve iteration (tests/fdm_model.py)
 against the reference's own fdMatrix::solve on the golden case
-(tests/golden/im_7x6x8.npz): the two iterations differ, their converged
+(tests/golden/im_*.npz): the two iterations differ, their converged
 solutions must not.  CPU only."""
 import numpy as np
+import pytest
 
 from conftest import load_golden, rel_l2
 from fdm_model import line_jacobi_model
@@ -21,8 +22,9 @@ def residual(al, ap, b, x):
     return float(np.sqrt(np.sum(w * r * r) / np.prod([n + 1 for n in x.shape])))
 
 
-def test_line_model_converges_to_the_reference_solution():
-    g = load_golden("im_7x6x8.npz")
+@pytest.mark.parametrize("case", ["im_7x6x8.npz", "im_9x5x6_m4.npz"])
+def test_line_model_converges_to_the_reference_solution(case):
+    g = load_golden(case)
     al, ap, b = g["al"], g["ap"] - float(g["c"]), g["src"] + g["f"][0]
     tol, max_its = float(g["tol"]), int(g["max_its"])
     x, its = g["x"][0].copy(), 0

@@ -1,6 +1,6 @@
 """The implicit operators of src/im on the GPU (nova_im_laplacian, nova_fdm_*)
-against the reference's own run (tests/golden/im_7x6x8.npz, made by
-tests/golden/make_golden.py from im::laplacian and fdMatrix::solve) and, on a
+against the reference's own runs (tests/golden/im_*.npz, 6th and 4th order, made
+by tests/golden/make_golden.py from im::laplacian and fdMatrix::solve) and, on a
 larger mesh, against an exact spectral solve of the same periodic 7-point
 system.  The reference relaxes the lines of a sweep one after another, the GPU
 all at once: the iterations differ, the converged solutions agree."""
@@ -19,26 +19,35 @@ def nova():
     return nova
 
 
-def build(nova, N, L, mu, x0):
-    M = nova.Mesh(N, L=L)
+def build(nova, N, L, mu, x0, m=6):
+    M = nova.Mesh(N, L=L, m=m)
     x = nova.Field(M, 1).upload_soa(x0)
     return M, x, nova.im.laplacian(mu, x)
 
 
-def test_coefficients_and_source_vs_reference(nova):
-    g = load_golden("im_7x6x8.npz")
+CASES = ["im_7x6x8.npz", "im_9x5x6_m4.npz"]
+
+
+def order(g):
+    return int(g["m"]) if "m" in g else 6
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_coefficients_and_source_vs_reference(nova, case):
+    g = load_golden(case)
     N = tuple(int(v) for v in g["N"])
-    M, x, A = build(nova, N, tuple(g["L"]), float(g["mu"]), g["x"])
+    M, x, A = build(nova, N, tuple(g["L"]), float(g["mu"]), g["x"], order(g))
     al, ap, b = A.download()
     assert np.array_equal(al, g["al"]) and np.array_equal(ap, g["ap"])
     # b = -ex::laplacian(mu, x) + A x: the 6th-order Laplacian is the GPU's own (parity 1e-12)
     assert rel_l2(b, g["src"]) < 1e-13
 
 
-def test_solve_vs_reference(nova):
-    g = load_golden("im_7x6x8.npz")
+@pytest.mark.parametrize("case", CASES)
+def test_solve_vs_reference(nova, case):
+    g = load_golden(case)
     N = tuple(int(v) for v in g["N"])
-    M, x, A = build(nova, N, tuple(g["L"]), float(g["mu"]), g["x"])
+    M, x, A = build(nova, N, tuple(g["L"]), float(g["mu"]), g["x"], order(g))
     A.add_diagonal(-float(g["c"]))
     f = nova.Field(M, 1).upload_soa(g["f"])
     its, res = A.eq(f).solve(float(g["tol"]), int(g["max_its"]))

@@ -164,13 +164,14 @@ def test_tensor_operators_and_field_nu_laplacian_bitwise_vs_reference_golden(ora
         assert np.array_equal(M.interior(v), g["out_" + k]), k
 
 
-def test_im_laplacian_and_line_relaxation_match_the_reference(oracle):
+@pytest.mark.parametrize("case", ["im_7x6x8.npz", "im_9x5x6_m4.npz"])
+def test_im_laplacian_and_line_relaxation_match_the_reference(oracle, case):
     """im::laplacian (coefficients, deferred-correction source) and fdMatrix::solve
-    restated against the reference's own run (tests/golden/im_7x6x8.npz): bit for bit,
-    the solve's iterations included."""
-    g = load_golden("im_7x6x8.npz")
+    restated against the reference's own runs (tests/golden/im_*.npz, 6th and 4th
+    order): bit for bit, the solve's iterations included."""
+    g = load_golden(case)
     N = tuple(int(v) for v in g["N"])
-    M = oracle.Mesh(N, L=tuple(g["L"]))
+    M = oracle.Mesh(N, L=tuple(g["L"]), m=int(g["m"]) if "m" in g else 6)
     xg = M.to_ghosted(g["x"])
     al, ap, src = oracle.im_laplacian(M, float(g["mu"]), xg)
     h = M.h
