@@ -93,6 +93,7 @@ class Mesh:
         self.h = self.m // 2
         hz = hyperbolic_z is not None
         s1, s2 = hyperbolic_z if hz else (0.0, 0.0)
+        self.hyperbolic_z = (float(s1), float(s2)) if hz else None
         self._p = lib().orc_mesh_new(np.array(self.N, np.int32), np.array(self.L), np.array(self.origin),
                                      self.m, int(hz), float(s1), float(s2))
         if not self._p:
@@ -285,6 +286,8 @@ def write_case(dirname, mesh, bc=None):
         f.write("origin: %.17g %.17g %.17g\n" % mesh.origin)
         f.write("N: %d %d %d\n" % mesh.N)
         f.write("L: %.17g %.17g %.17g\n" % mesh.L)
+        if mesh.hyperbolic_z is not None:
+            f.write("hypz: %.17g %.17g\n" % mesh.hyperbolic_z)
     bc = bc or {}
     for name, nc in (("U", 3), ("p", 1), ("B", 3), ("pB", 1), ("rho", 1), ("T", 1)):
         t, v = bc_arrays(nc, bc.get(name))

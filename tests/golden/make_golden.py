@@ -22,13 +22,15 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from oracle import oracle as O  # noqa: E402
 
 
-def ops_case(name, N, L, seed, nu, m=6):
-    M = O.Mesh(N, L=L, m=m)
+def ops_case(name, N, L, seed, nu, m=6, hyperbolic_z=None):
+    M = O.Mesh(N, L=L, m=m, hyperbolic_z=hyperbolic_z)
     rng = np.random.default_rng(seed)
     U = rng.standard_normal((3,) + M.N)
     s = rng.standard_normal((1,) + M.N)
     out = O.ref_ops(M, M.to_ghosted(U), M.to_ghosted(s), nu)
     res = {"N": np.array(N), "L": np.array(L), "m": np.array(m), "nu": np.array(nu), "U": U, "s": s}
+    if hyperbolic_z is not None:
+        res["hypz"] = np.array(hyperbolic_z)
     for k, v in out.items():
         res["out_" + k] = M.interior(v)  # incl. the duplicate node, as the reference stores it
     np.savez_compressed(os.path.join(HERE, name), **res)
@@ -160,6 +162,8 @@ def im_case(name, N, L, seed, mu, c, tol, max_its, m=6):
 CASES = {
     "ops_10x8x6.npz": lambda n: ops_case(n, (10, 8, 6), (2 * np.pi, 2.0, 3.0), 7, 0.01),
     "ops_16x12x8_m4.npz": lambda n: ops_case(n, (16, 12, 8), (2 * np.pi,) * 3, 8, 0.02, m=4),
+    "ops_hypz_12x10x16.npz": lambda n: ops_case(n, (12, 10, 16), (2 * np.pi, 2 * np.pi, 1.0), 29, 0.02,
+                                                hyperbolic_z=(0.03, 0.03)),
     "tg_12_classical.npz": lambda n: run_case(n, (12, 12, 12), "ns", "classical", 6, 0.05, 1 / 1600, 0.0),
     "tg_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "ns", "literal", 6, 0.05, 1 / 1600, 0.0),
     "ot_12_classical.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "classical", 4, 0.01, 1e-3, 1e-3),

@@ -22,10 +22,14 @@ def test_fft_matches_numpy():
             assert np.abs(got - ref).max() / np.abs(ref).max() < 5e-15
 
 
-@pytest.mark.parametrize("name", ["ops_10x8x6.npz", "ops_16x12x8_m4.npz"])
+@pytest.mark.parametrize("name", ["ops_10x8x6.npz", "ops_16x12x8_m4.npz", "ops_hypz_12x10x16.npz"])
 def test_operators_bitwise_vs_reference_golden(oracle, name):
+    """Every operator against the reference's own output, bit for bit: 6th and
+    4th order, and a 'hypz:' stretched z (Mesh.cpp:373-407), whose metrics the
+    operators carry"""
     g = load_golden(name)
-    M = oracle.Mesh(tuple(g["N"]), L=tuple(g["L"]), m=int(g["m"]))
+    hz = tuple(float(v) for v in g["hypz"]) if "hypz" in g else None
+    M = oracle.Mesh(tuple(g["N"]), L=tuple(g["L"]), m=int(g["m"]), hyperbolic_z=hz)
     U = M.to_ghosted(g["U"])
     s = M.to_ghosted(g["s"])
     nu = float(g["nu"])
