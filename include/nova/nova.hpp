@@ -41,9 +41,24 @@ struct vector {
     scalar &operator[](int d) { return v_[d]; }
 };
 
+// layout-compatible with the reference's tensor (scalar v_[9], xx xy xz yx ..., src/Types/tensor/tensor.h:25)
+// and symmTensor (scalar v_[6], xx xy xz yy yz zz, src/Types/symmTensor/symmTensor.h:19)
+struct tensor {
+    scalar v_[9];
+    tensor() : v_{0, 0, 0, 0, 0, 0, 0, 0, 0} {}
+    scalar &operator[](int c) { return v_[c]; }
+};
+struct symmTensor {
+    scalar v_[6];
+    symmTensor() : v_{0, 0, 0, 0, 0, 0} {}
+    scalar &operator[](int c) { return v_[c]; }
+};
+
 template <class T> struct nComp;
 template <> struct nComp<scalar> { static constexpr int value = 1; };
 template <> struct nComp<vector> { static constexpr int value = 3; };
+template <> struct nComp<symmTensor> { static constexpr int value = 6; };
+template <> struct nComp<tensor> { static constexpr int value = 9; };
 
 class Error : public std::runtime_error {
 public:
@@ -155,6 +170,40 @@ inline std::shared_ptr<Field<vector>> grad(const Field<scalar> &f)
     return out;
 }
 
+// ex::grad(const Field<vector>&) (src/ex/grad/grad.h:43-46, the Q1 stencil of grad.cpp:65-102)
+inline std::shared_ptr<Field<tensor>> grad(const Field<vector> &U)
+{
+    auto out = std::make_shared<Field<tensor>>(U.mesh());
+    U.toDevice();
+    check(U.mesh().ctx(), nova_grad_v(U.mesh().ctx(), U.dev(), out->dev()), "nova_grad_v");
+    out->fromDevice();
+    return out;
+}
+
+// ex::div(const Field<tensor>&), ex::div(const Field<symmTensor>&) (src/ex/div/div.hxx:222-285)
+template <class T>
+typename std::enable_if<std::is_same<T, tensor>::value || std::is_same<T, symmTensor>::value,
+                        std::shared_ptr<Field<vector>>>::type
+div(const Field<T> &t)
+{
+    auto out = std::make_shared<Field<vector>>(t.mesh());
+    t.toDevice();
+    check(t.mesh().ctx(), nova_div_t(t.mesh().ctx(), t.dev(), out->dev()), "nova_div_t");
+    out->fromDevice();
+    return out;
+}
+
+// ex::div(const Field<scalar>&, std::shared_ptr<Field<tensor>>) (src/ex/div/div.hxx:173-207)
+inline std::shared_ptr<Field<vector>> div(const Field<scalar> &s, const std::shared_ptr<Field<tensor>> &t)
+{
+    auto out = std::make_shared<Field<vector>>(s.mesh());
+    s.toDevice();
+    t->toDevice();
+    check(s.mesh().ctx(), nova_div_st(s.mesh().ctx(), s.dev(), t->dev(), out->dev()), "nova_div_st");
+    out->fromDevice();
+    return out;
+}
+
 inline std::shared_ptr<Field<scalar>> div(const Field<vector> &U)
 {
     auto out = std::make_shared<Field<scalar>>(U.mesh());
@@ -188,6 +237,17 @@ template <class T> std::shared_ptr<Field<T>> laplacian(const scalar &nu, const F
     auto out = std::make_shared<Field<T>>(f.mesh());
     f.toDevice();
     check(f.mesh().ctx(), nova_laplacian(f.mesh().ctx(), nu, f.dev(), out->dev()), "nova_laplacian");
+    out->fromDevice();
+    return out;
+}
+
+// ex::laplacian(const Field<scalar>& nu, const Field<T>&) (src/ex/laplacian/laplacian.hxx:64-127)
+template <class T> std::shared_ptr<Field<T>> laplacian(const Field<scalar> &nu, const Field<T> &f)
+{
+    auto out = std::make_shared<Field<T>>(f.mesh());
+    nu.toDevice();
+    f.toDevice();
+    check(f.mesh().ctx(), nova_laplacian_f(f.mesh().ctx(), nu.dev(), f.dev(), out->dev()), "nova_laplacian_f");
     out->fromDevice();
     return out;
 }

@@ -61,7 +61,7 @@ int main(void) {
     assert [int(v) for v in got] == want
 
 
-@pytest.mark.parametrize("prog", ["tg_driver.cpp", "im_driver.cpp"])
+@pytest.mark.parametrize("prog", ["tg_driver.cpp", "im_driver.cpp", "ops2_driver.cpp"])
 def test_cpp_adapter_compiles(prog):
     """The header-only C++ adapter (include/nova/nova.hpp) builds against the C ABI."""
     src = os.path.join(ROOT, "tests", "cpp", prog)

@@ -216,3 +216,32 @@ def test_field_nu_laplacian_stretched_z_and_walls_vs_oracle(nova, oracle):
     got = nova.ex.laplacian(fn.upload(nug), fu.upload(Ug))
     stored = np.ascontiguousarray(np.moveaxis(ref[h:h + N[0], h:h + N[1] + 1, h:h + N[2]], -1, 0))
     assert rel_max(got.download_soa(), stored) < TOL
+
+
+def test_cpp_adapter_tensor_operators(oracle, tmp_path):
+    """The reference-style C++ program (tests/cpp/ops2_driver.cpp) through
+    include/nova/nova.hpp, with its tensor and symmTensor types: the operators
+    against the reference's own outputs (tests/golden/ops2_7x6x5.npz), grad of
+    a vector against the oracle."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "novaclone_b200")
+    exe = tmp_path / "ops2_driver"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "ops2_driver.cpp"), "-L" + libdir, "-lnova_b200",
+                    "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    g = load_golden("ops2_7x6x5.npz")
+    OM = oracle.Mesh(tuple(int(v) for v in g["N"]), L=tuple(g["L"]))
+    case = tmp_path / "case"
+    oracle.write_case(str(case), OM)
+    for k in ("T", "S", "s", "nu", "U"):
+        OM.to_ghosted(g[k]).tofile(str(tmp_path / ("in_" + k + ".bin")))
+    subprocess.run([str(exe), str(case), str(tmp_path / "in_"), str(tmp_path / "out_")], check=True)
+
+    def read(name, nc):
+        return OM.interior(np.fromfile(str(tmp_path / ("out_" + name + ".bin"))).reshape(OM.n + (nc,)))
+    for k, nc in (("div_t", 3), ("div_st", 3), ("div_sT", 3), ("lap_f_v", 3), ("lap_f_s", 1)):
+        assert rel_max(read(k, nc), g["out_" + k]) < TOL, k
+    want = OM.interior(oracle.grad_v(OM, OM.to_ghosted(g["U"])))
+    assert rel_max(read("grad_v", 9), want) < TOL
