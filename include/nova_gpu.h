@@ -27,6 +27,16 @@
  *   tools::maximum(shared_ptr<Field<T>>)      src/Tools/Tools.h:19-36      -> nova_field_maxabs
  *   the loop bodies app/TG_Piosson/RKLoop.H:1-54, app/OT_Poisson/UEqn.H:1-54 and
  *   app/OT_Poisson/BEqn.H:1-110 (one time step each)           -> nova_advance
+ *   ex::div(tensor / symmTensor / scalar, tensor), ex::laplacian(Field nu, .)
+ *                                             src/ex/div/div.hxx:173-285, laplacian.hxx:64-127
+ *                                                        -> nova_div_t, nova_div_st, nova_laplacian_f
+ *   im::laplacian, fdMatrix<scalar> and its operators, relax, setReference, residual, solve
+ *                                             src/im/laplacian/laplacian.hxx:24-68,
+ *                                             src/im/fdMatrix/fdMatrix.hxx:19-413
+ *                                                        -> nova_im_laplacian, nova_fdm_*
+ *   Field<T>::write / read, Mesh::write (EnSight Gold)
+ *                                             src/Field/Field.hxx:404-516, src/Mesh/Mesh.cpp:224-369
+ *                                                        -> nova_ensight_*
  */
 #ifndef NOVA_GPU_H
 #define NOVA_GPU_H
