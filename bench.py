@@ -179,15 +179,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per grid point per stage launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "stage_kernel_ns_f64.md")
+def profiled_value(name, key):
+    """A 'key: value' line of a committed ncu summary under profiles/, if any."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_point_per_launch:"):
+        if line.startswith(key + ":"):
             return float(line.split(":")[1])
     return None
+
+
+def profiled_traffic():
+    """DRAM bytes per grid point per stage launch from the committed ncu summary, if any."""
+    return profiled_value("stage_kernel_ns_f64.md", "dram_bytes_per_point_per_launch")
 
 
 class ClockSampler:
@@ -486,6 +491,7 @@ def im_leg(args, nova, torch, dist, world):
     f.close()
     peak, peak_kind = measured_peaks()
     achieved = IM_BYTES * n ** 3 * its / sec / 1e9
+    tr = profiled_value("fdm_solve_256.md", "dram_bytes_per_node_iteration")
     out = {"workload": "im::laplacian(1e-3, x) - 1 == f on a periodic [0,2pi]^3 %d^3 mesh, random x and f; "
                        "fdMatrix::solve(tol=0, %d) timed after 3 iterations" % (n, its),
            "value": world * n ** 3 * its / sec / 1e6, "unit": "Mnode-iterations/s", "iterations": done,
@@ -493,7 +499,9 @@ def im_leg(args, nova, torch, dist, world):
            "residual_before_after": [res0, res1],
            "roofline": {"bound": "hbm", "kernel": "one solve iteration (residual + three line sweeps)",
                         "alg_bytes_per_node_iteration": IM_BYTES, "achieved": achieved, "peak": peak,
-                        "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind}}
+                        "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                        "traffic": None if tr is None else tr * n ** 3,
+                        "traffic_per": "iteration (DRAM bytes from the committed ncu summary)"}}
     if world == 1 and not args.no_cpu_baseline and reference_bin()[0] is not None:
         from oracle import oracle as O
         nc, ic = args.im_cpu_n, args.im_cpu_its
