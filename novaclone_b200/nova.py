@@ -434,15 +434,18 @@ class FdMatrix:
         return self
 
     def relax(self, urf: float) -> "FdMatrix":
+        """fdMatrix::relax(urf): source += (1 - urf)/urf ap x, then ap /= urf (urf > 0)"""
         self.mesh.check(self.mesh.lib.nova_fdm_relax(self.mesh.h, self.h, float(urf)))
         return self
 
     def set_reference(self, i: int, j: int, k: int, val: float) -> "FdMatrix":
+        """fdMatrix::setReference at the unique node (i, j, k): source += 1e15 val, ap *= 1e15"""
         self.mesh.check(self.mesh.lib.nova_fdm_set_reference(self.mesh.h, self.h, int(i), int(j), int(k),
                                                              float(val)))
         return self
 
     def residual(self) -> float:
+        """fdMatrix::residual: the RMS of b - A x over the reference's (N0+1)(N1+1)(N2+1) nodes"""
         r = C.c_double()
         self.mesh.check(self.mesh.lib.nova_fdm_residual(self.mesh.h, self.h, C.byref(r)))
         return r.value
