@@ -25,8 +25,10 @@
  *                                                        -> nova_laplacian
  *   poisson::rhs(...) + poisson::solve()      src/poisson/poisson.h:111-113 -> nova_poisson_solve
  *   tools::maximum(shared_ptr<Field<T>>)      src/Tools/Tools.h:19-36      -> nova_field_maxabs
- *   the loop bodies app/TG_Piosson/RKLoop.H:1-54, app/OT_Poisson/UEqn.H:1-54 and
- *   app/OT_Poisson/BEqn.H:1-110 (one time step each)           -> nova_advance
+ *   the loop bodies app/TG_Piosson/RKLoop.H:1-54, app/OT_Poisson/UEqn.H:1-54,
+ *   app/OT_Poisson/BEqn.H:1-110 and app/shearLayer/UEqn.H:1-54 (one time step each),
+ *   with the per-step diagnostics of app/OT_Poisson/OT.cpp:132-176 and
+ *   tools::CFL (src/Tools/Tools.cpp:9-41)                     -> nova_advance
  *   ex::div(tensor / symmTensor / scalar, tensor), ex::laplacian(Field nu, .)
  *                                             src/ex/div/div.hxx:173-285, laplacian.hxx:64-127
  *                                                        -> nova_div_t, nova_div_st, nova_laplacian_f
@@ -89,7 +91,14 @@ typedef struct {
 } nova_bc;
 
 typedef enum { NOVA_MODEL_NS = 0, NOVA_MODEL_MHD = 1 } nova_model;
-typedef enum { NOVA_RK_LITERAL = 0, NOVA_RK_CLASSICAL = 1 } nova_rk_mode;
+/* LITERAL: app/TG_Piosson/RKLoop.H and app/OT_Poisson/UEqn.H as written (U not refreshed
+ * between stages); CLASSICAL: the same loop with the stage state refreshed (RK4);
+ * SHEARLAYER: app/shearLayer/UEqn.H:14-38 -- per stage rk, U* = UOld + RK4[rk] dt F(U)
+ * with RK4 = {1/6, 1/3, 1/3, 1/6}, then a projection with rhs div(U*)/dt/RK4c[rk] and
+ * U = U* - RK4c[rk] dt grad(p), so U is refreshed by a projected stage value (for MHD
+ * the U loop runs with the Lorentz terms of a frozen B, and B is not advanced, as in
+ * that app, whose BEqn.H is not included). */
+typedef enum { NOVA_RK_LITERAL = 0, NOVA_RK_CLASSICAL = 1, NOVA_RK_SHEARLAYER = 2 } nova_rk_mode;
 /* Pressure solve on a mesh with y walls.  FFT: the reference's poisson::solve on the N
  * unique y nodes as if y were periodic (what app/shearLayer does).  DCT: the inverse
  * consistent with the node-based walls -- the even extension in y (a DCT-I), so that
@@ -114,7 +123,19 @@ typedef struct {
     nova_field *U, *p, *B, *pB;
 } nova_state;
 
-#define NOVA_HIST_COLS 6 /* step, t, Ek, Em, max|div U|, max|div B| */
+/* One history row (the diagnostics the apps compute after each step):
+ *   0 step, 1 t, 2 Ek = <1/2|U|^2>, 3 Em = <1/2|B|^2>, 4 max|div U|, 5 max|div B|
+ *     (tools::maximum of ex::div, app/TG_Piosson/RKLoop.H:42-51, app/OT_Poisson/BEqn.H:46-54),
+ *   6 omega = <|ex::curl(U)|>, 7 Jav = <|ex::curl(B)|>, 8 Jmax = max|ex::curl(B)|,
+ *   9 epsilon = -nu omega^2 - eta Jav^2, 10 Umax = max|U|   (app/OT_Poisson/OT.cpp:132-176),
+ *   11-13 cfl_x, cfl_y, cfl_z of tools::CFL (src/Tools/Tools.cpp:9-41, as written: signed
+ *     velocities, and cfl_y, cfl_z compared against cfl_x at the loop's last node only),
+ *   14 1/2 <|curl U|^2>, 15 1/2 <|curl B|^2> with the central 6th-order curl (the enstrophy;
+ *     ex::curl is the reference's Q1 stencil of ex::grad(vector), which 6-8 keep).
+ * <.> and the maxima of 8 and 10 run over the unique nodes, the divergence maxima and
+ * cfl_x over every stored node.  nova_advance_wc fills the columns of U (0-2, 4, 6, 9-14;
+ * epsilon with its mu). */
+#define NOVA_HIST_COLS 16
 
 /* ---- context ---- */
 nova_status nova_create(const nova_mesh_desc *mesh, nova_ctx **out);
@@ -169,23 +190,24 @@ nova_status nova_div_t(nova_ctx *ctx, const nova_field *T, nova_field *out);
 nova_status nova_div_st(nova_ctx *ctx, const nova_field *s, const nova_field *T, nova_field *out);
 nova_status nova_laplacian_f(nova_ctx *ctx, const nova_field *nu, const nova_field *f, nova_field *out);
 nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *s, double *out);
-/* Allocation-free max|s| (no counterpart in the reference: tools::maximum
- * allocates its reduction buffers).  Same result as nova_field_maxabs, computed
- * in a fixed 64 KiB scratch that lives in the library image (a static device
- * array, one per device) instead of memory the context allocates, so the call
- * never invokes cudaMalloc/cudaFree or any pool allocator.  For callers that
- * cannot allocate device memory when they check a field: a solver whose HBM is
- * all handed out (fields sized to fill the device, or a framework's caching
- * allocator holding the rest), or a monitor that must not add an allocation's
- * implicit synchronisation to the running time steps.
+/* Allocation-free max|s|: the same result as nova_field_maxabs, which keeps its
+ * per-block partials in memory the context allocates on first use (no
+ * counterpart in the reference).  Here the partials live in a fixed 64 KiB
+ * scratch in the library image (a static device array, one per device that
+ * loads the library, held until the process exits), so the call never invokes
+ * cudaMalloc/cudaFree or any pool allocator.  For callers that cannot allocate
+ * device memory when they check a field: a solver whose HBM is all handed out
+ * (fields sized to fill the device, or a framework's caching allocator holding
+ * the rest), or a monitor that must not add an allocation's implicit
+ * synchronisation to the running time steps.
  * Limit: at most NOVA_MAXABS_NOALLOC_MAX_NODES stored nodes (N0*N1*N2, with y
  * walls N0*(N1+1)*N2); larger fields return NOVA_E_INVALID (use
  * nova_field_maxabs).  The scratch needs no zeroing: each call writes every
- * slot before it reads it.  The first call on each device, with that device
- * current, looks up the scratch address (cudaGetSymbolAddress, which may load
- * the library's device code); make it before any stream capture.  Calls that
- * overlap in time on one device (two streams, threads or contexts) share the
- * scratch and race: serialise them. */
+ * slot before it reads it.  Each call looks up the scratch address with the
+ * caller's device current (cudaGetSymbolAddress); the first call on a device
+ * may load the library's device code, so make it before any stream capture.
+ * Calls that overlap in time on one device (two streams, threads or contexts)
+ * share the scratch and race: serialise them. */
 #define NOVA_MAXABS_NOALLOC_MAX_NODES (1LL << 27)
 nova_status nova_field_maxabs_noalloc(nova_ctx *ctx, const nova_field *s, double *out);
 
@@ -277,7 +299,7 @@ nova_status nova_fdm_destroy(nova_fdm *a);
  *                  UEqn.H (buoyancy -(rho T) g), rhoEqn.H, pEqn.H (p = (K rho) rho,
  *                  K = c^2/(2 rho0)), TEqn.H
  * Each loop is the reference's classical RK4 on rho*U, rho, rho*T.
- * hist: nsteps x NOVA_HIST_COLS rows (step, t, mean 1/2|U|^2, 0, max|div U|, 0) or NULL. */
+ * hist: nsteps x NOVA_HIST_COLS rows (the columns of U; B's are zero) or NULL. */
 typedef enum { NOVA_WC_TG = 0, NOVA_WC_SHEAR = 1 } nova_wc_case;
 typedef struct {
     int wc_case;      /* nova_wc_case */

@@ -70,6 +70,7 @@ struct nova_ctx {
     double *d_rhs = nullptr;
     double *w64[3] = {nullptr, nullptr, nullptr};
     float *w32[3] = {nullptr, nullptr, nullptr};
+    float *w32x = nullptr;  // the shear-layer loop's FP32-split U* (lo part)
     double *d_part = nullptr;
     double *d_scalar = nullptr;
     int *d_flag = nullptr;
@@ -328,7 +329,7 @@ nova_status ensure_fft(nova_ctx *ctx)
 nova_status ensure_red(nova_ctx *ctx)
 {
     nova_status s;
-    if ((s = dalloc(ctx, &ctx->d_part, (size_t)diag_blocks(ctx->g) * 4)) != NOVA_OK) return s;
+    if ((s = dalloc(ctx, &ctx->d_part, (size_t)diag_blocks(ctx->g) * kDiagParts)) != NOVA_OK) return s;
     if ((s = dalloc(ctx, &ctx->d_scalar, 1)) != NOVA_OK) return s;
     // [0] non-finite diagnostics, [1] a stage pipeline wait timed out
     if ((s = dalloc(ctx, &ctx->d_flag, 2)) != NOVA_OK) return s;
@@ -418,9 +419,17 @@ nova_status poisson_device_dct(nova_ctx *ctx, const double *rhs, double *p)
     return NOVA_OK;
 }
 
-bool valid_field(const nova_field *f, int nc)
+// a field of this context's mesh: its buffers hold the context's N3 nodes per
+// component (a field made by a context of another mesh would be read or
+// written past its end)
+bool on_mesh(const nova_ctx *ctx, const nova_field *f)
 {
-    return f && f->nc == nc;
+    return f && f->n3 == ctx->g.N3;
+}
+
+bool valid_field(const nova_ctx *ctx, const nova_field *f, int nc)
+{
+    return on_mesh(ctx, f) && f->nc == nc;
 }
 
 nova_status ensure_stage(nova_ctx *ctx, size_t n)
@@ -537,7 +546,7 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
     }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN};
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->w32x};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -666,6 +675,7 @@ static nova_status check_local_n(nova_ctx *ctx, const int local_n[3])
 extern "C" nova_status nova_field_upload(nova_ctx *ctx, nova_field *f, const double *host, const int local_n[3])
 {
     if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_upload: null argument");
+    if (!on_mesh(ctx, f)) return fail(ctx, NOVA_E_INVALID, "nova_field_upload: field of another mesh");
     nova_status s = check_local_n(ctx, local_n);
     if (s != NOVA_OK) return s;
     const size_t n = (size_t)local_n[0] * local_n[1] * local_n[2] * f->nc;
@@ -682,6 +692,7 @@ extern "C" nova_status nova_field_download(nova_ctx *ctx, const nova_field *f, d
                                            const nova_bc *bc)
 {
     if (!ctx || !f || !host) return fail(ctx, NOVA_E_INVALID, "nova_field_download: null argument");
+    if (!on_mesh(ctx, f)) return fail(ctx, NOVA_E_INVALID, "nova_field_download: field of another mesh");
     nova_status s = check_local_n(ctx, local_n);
     if (s != NOVA_OK) return s;
     nova_field tmp = *f;  // ghosts from the given BCs, or the field's own
@@ -703,6 +714,7 @@ extern "C" nova_status nova_field_download(nova_ctx *ctx, const nova_field *f, d
 
 static nova_status soa_in(nova_ctx *ctx, nova_field *f, const double *src, cudaMemcpyKind kind)
 {
+    if (!on_mesh(ctx, f)) return fail(ctx, NOVA_E_INVALID, "field upload: field of another mesh");
     const size_t n = (size_t)f->nc * f->n3;
     if (f->prec == NOVA_F64) {
         CK(cudaMemcpyAsync(f->d64, src, sizeof(double) * n, kind, ctx->stream));
@@ -719,6 +731,7 @@ static nova_status soa_in(nova_ctx *ctx, nova_field *f, const double *src, cudaM
 
 static nova_status soa_out(nova_ctx *ctx, const nova_field *f, double *dst, cudaMemcpyKind kind)
 {
+    if (!on_mesh(ctx, f)) return fail(ctx, NOVA_E_INVALID, "field download: field of another mesh");
     const size_t n = (size_t)f->nc * f->n3;
     if (f->prec == NOVA_F64) {
         CK(cudaMemcpyAsync(dst, f->d64, sizeof(double) * n, kind, ctx->stream));
@@ -768,6 +781,8 @@ static nova_status op_common(nova_ctx *ctx, int op, const nova_field *a, const n
                              int nc_in, int nc_out, double nu)
 {
     if (!ctx || !a || !out) return fail(ctx, NOVA_E_INVALID, "operator: null argument");
+    if (!on_mesh(ctx, a) || !on_mesh(ctx, out) || (b && !on_mesh(ctx, b)))
+        return fail(ctx, NOVA_E_INVALID, "operator: field of another mesh");
     if ((nc_in && a->nc != nc_in) || (nc_out && out->nc != nc_out))
         return fail(ctx, NOVA_E_INVALID, "operator: wrong number of components");
     if (a->prec != NOVA_F64 || out->prec != NOVA_F64 || (b && b->prec != NOVA_F64))
@@ -840,6 +855,7 @@ extern "C" nova_status nova_laplacian(nova_ctx *ctx, double nu, const nova_field
 extern "C" nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, nova_field *p)
 {
     if (!ctx || !rhs || !p) return fail(ctx, NOVA_E_INVALID, "nova_poisson_solve: null argument");
+    if (!on_mesh(ctx, rhs) || !on_mesh(ctx, p)) return fail(ctx, NOVA_E_INVALID, "nova_poisson_solve: field of another mesh");
     if (rhs->nc != 1 || p->nc != 1 || rhs->prec != NOVA_F64 || p->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID, "nova_poisson_solve: needs FP64 scalar fields");
     nova_status s = ensure_fft(ctx);
@@ -853,6 +869,7 @@ extern "C" nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, 
 extern "C" nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *f, double *out)
 {
     if (!ctx || !f || !out) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs: null argument");
+    if (!on_mesh(ctx, f)) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs: field of another mesh");
     if (f->nc != 1 || f->prec != NOVA_F64) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs: FP64 scalar only");
     nova_status s = ensure_red(ctx);
     if (s != NOVA_OK) return s;
@@ -867,6 +884,7 @@ extern "C" nova_status nova_field_maxabs(nova_ctx *ctx, const nova_field *f, dou
 extern "C" nova_status nova_field_maxabs_noalloc(nova_ctx *ctx, const nova_field *f, double *out)
 {
     if (!ctx || !f || !out) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs_noalloc: null argument");
+    if (!on_mesh(ctx, f)) return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs_noalloc: field of another mesh");
     if (f->nc != 1 || f->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID, "nova_field_maxabs_noalloc: FP64 scalar only");
     const long long n = ctx->g.N3;
@@ -887,6 +905,24 @@ extern "C" nova_status nova_field_maxabs_noalloc(nova_ctx *ctx, const nova_field
 
 // ================================================================== advance ==
 namespace {
+
+// app/shearLayer: the RK4 weights used as stage coefficients (shearLayer.cpp:164)
+// and settings::RK4c_ (src/settings/settings.cpp:51), the projection's scale per stage
+const double kShearW[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+const double kRK4c[4] = {0.5, 0.5, 1.0, 1.0};
+
+// the physical parameters of a history row of a run (epsilon's viscosities,
+// tools::CFL's dt and the mesh spacing Mesh::dx_, dy_, dz_)
+DiagPhys phys_of(const nova_ctx *ctx, const nova_run_desc *rd)
+{
+    return DiagPhys{rd->nu, rd->model == NOVA_MODEL_MHD ? rd->eta : 0.0, rd->dt, ctx->md.L[0] / ctx->md.N[0],
+                    ctx->md.L[1] / ctx->md.N[1], ctx->md.L[2] / ctx->md.N[2]};
+}
+
+DiagPhys phys_of(const DiagFinal &f)
+{
+    return DiagPhys{f.nu, f.eta, f.dt, f.dx, f.dy, f.dz};
+}
 
 nova_status ensure_work(nova_ctx *ctx, int prec)
 {
@@ -928,6 +964,95 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             ctx->launches += 1;
         }
     };
+    const StageExec ex{ctx->stage_impl, ctx->d_flag + 1};
+    if (rd->rk_mode == NOVA_RK_SHEARLAYER) {
+        // app/shearLayer/UEqn.H:14-38: per stage rk, U* = UOld + RK4[rk] dt F(U),
+        // rhs = div(U*)/dt/RK4c[rk], U = U* - RK4c[rk] dt grad(p), with the
+        // wall-node overwrites of U*.correctBC, p.correctBC and U.correctBC
+        const bool f64 = Y->prec == NOVA_F64;
+        if (dg) {
+            launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, Y->d64, Y->hi, Y->lo, nullptr,
+                        nullptr, nullptr, 0, dg->part, dg->fin.step, dg->fin.time, dg->row, dg->flag, st,
+                        phys_of(dg->fin));
+            ctx->launches += 2;
+        }
+        const size_t n3 = 3 * (size_t)g.N3;
+        double *Old64 = ctx->w64[2], *Us64 = ctx->w64[1];
+        float *Oh = ctx->w32[0], *Ol = ctx->w32[1], *Sh = ctx->w32[2], *Sl = ctx->w32x;
+        const Walls<double> sw64 = walls_of<double>(ctx, Y, X);
+        const Walls<float> sw32 = walls_of<float>(ctx, Y, X);
+        if (walls) {
+            if (f64)
+                launch_wall_fix64(g, yfix, Y->d64, st);
+            else
+                launch_wall_fix_split(g, yfix, Y->hi, Y->lo, st);
+            ctx->launches += 1;
+        }
+        if (f64) {
+            CK(cudaMemcpyAsync(Old64, Y->d64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+        } else {
+            CK(cudaMemcpyAsync(Oh, Y->hi, sizeof(float) * n3, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(Ol, Y->lo, sizeof(float) * n3, cudaMemcpyDeviceToDevice, st));
+        }
+        for (int rk = 0; rk < 4; rk++) {
+            cudaError_t e;
+            {
+                ProfScope ps(ctx, NOVA_K_STAGE);
+                if (f64)
+                    e = launch_stage64(phys, 5, str, g, sw64, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc,
+                                       StageArgs64{Y->d64, X ? X->d64 : nullptr, Old64, nullptr, Us64, kShearW[rk]},
+                                       st, ex);
+                else
+                    e = launch_stage32(phys, 5, str, g, sw32, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt,
+                                       (float)visc,
+                                       StageArgs32{Y->hi, X ? X->hi : nullptr, Oh, Ol, nullptr, nullptr, Sh, Sl,
+                                                   (float)kShearW[rk]},
+                                       st, ex);
+                ctx->launches += 1;
+            }
+            if (e != cudaSuccess) return stage_fail(ctx, e);
+            if (walls) {
+                if (f64)
+                    launch_wall_fix64(g, yfix, Us64, st);
+                else
+                    launch_wall_fix_split(g, yfix, Sh, Sl, st);
+                ctx->launches += 1;
+            }
+            CKL("stage kernel");
+            {
+                ProfScope ps(ctx, NOVA_K_DIV);
+                e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, f64 ? Us64 : nullptr, f64 ? nullptr : Sh,
+                                    f64 ? nullptr : Sl, divisor * kRK4c[rk], ctx->d_rhs, st, ex);
+                if (e != cudaSuccess) return stage_fail(ctx, e);
+                ctx->launches += 1;
+            }
+            CKL("divergence kernel");
+            nova_status s =
+                dct ? poisson_device_dct(ctx, ctx->d_rhs, p->d64) : poisson_device(ctx, ctx->d_rhs, p->d64);
+            if (s != NOVA_OK) return s;
+            if (walls && !dct) {
+                launch_wall_fix64(g, pfix, p->d64, st);
+                ctx->launches += 1;
+            }
+            {
+                ProfScope ps(ctx, NOVA_K_CORRECT);
+                e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, kRK4c[rk] * corr_scale,
+                                   f64 ? Us64 : nullptr, f64 ? Y->d64 : nullptr, f64 ? nullptr : Sh,
+                                   f64 ? nullptr : Sl, f64 ? nullptr : Y->hi, f64 ? nullptr : Y->lo, st, ex);
+                if (e != cudaSuccess) return stage_fail(ctx, e);
+                ctx->launches += 1;
+            }
+            if (walls) {
+                if (f64)
+                    launch_wall_fix64(g, yfix, Y->d64, st);
+                else
+                    launch_wall_fix_split(g, yfix, Y->hi, Y->lo, st);
+                ctx->launches += 1;
+            }
+            CKL("correction kernel");
+        }
+        return NOVA_OK;
+    }
     if (Y->prec == NOVA_F64) {
         const Walls<double> sw = walls_of<double>(ctx, Y, X);
         fix64(Y->d64);
@@ -944,8 +1069,8 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             ctx->launches += taken ? 2 : 1;
             if (first && dg && !taken) {
                 launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, Y->d64, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st,
-                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
+                            nullptr, nullptr, nullptr, 0, dg->part, dg->fin.step, dg->fin.time, dg->row, dg->flag, st,
+                            phys_of(dg->fin));
                 ctx->launches += 2;
             }
         };
@@ -1007,8 +1132,8 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         fixpair(Y->hi, Y->lo);
         if (dg) {
             launch_diag(ctx->h, g, walls_of<double>(ctx, Y), ctx->co64, ctx->d_ia64, nullptr, Y->hi, Y->lo, nullptr,
-                        nullptr, nullptr, 0, dg->part, dg->step, dg->time, dg->row, dg->flag, st,
-                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
+                        nullptr, nullptr, 0, dg->part, dg->fin.step, dg->fin.time, dg->row, dg->flag, st,
+                        phys_of(dg->fin));
             ctx->launches += 2;
         }
         const float *Ushi, *Uslo;
@@ -1076,8 +1201,9 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     if (!ctx || !rd || !st || nsteps < 0) return fail(ctx, NOVA_E_INVALID, "nova_advance: bad arguments");
     const bool mhd = rd->model == NOVA_MODEL_MHD;
     if (rd->model != NOVA_MODEL_NS && !mhd) return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown model");
-    if (rd->rk_mode != NOVA_RK_LITERAL && rd->rk_mode != NOVA_RK_CLASSICAL)
+    if (rd->rk_mode != NOVA_RK_LITERAL && rd->rk_mode != NOVA_RK_CLASSICAL && rd->rk_mode != NOVA_RK_SHEARLAYER)
         return fail(ctx, NOVA_E_INVALID, "nova_advance: unknown rk_mode");
+    const bool shear = rd->rk_mode == NOVA_RK_SHEARLAYER;
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: the fused kernels are built for m = 6");
     if (mhd && ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance: MHD is built for periodic meshes");
     if (rd->poisson != NOVA_POISSON_FFT && rd->poisson != NOVA_POISSON_DCT)
@@ -1086,14 +1212,16 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
         for (int face : {NOVA_NORTH, NOVA_SOUTH})
             if (st->p->bc.type[face] != NOVA_BC_NEUMANN || st->p->bc.val[face] != 0.0)
                 return fail(ctx, NOVA_E_INVALID, "nova_advance: the DCT wall Poisson needs Neumann-0 pressure walls");
-    if (!valid_field(st->U, 3) || !valid_field(st->p, 1) || st->p->prec != NOVA_F64 || st->U->prec != rd->precision)
+    if (!valid_field(ctx, st->U, 3) || !valid_field(ctx, st->p, 1) || st->p->prec != NOVA_F64 || st->U->prec != rd->precision)
         return fail(ctx, NOVA_E_INVALID, "nova_advance: U (3 comps, run precision) and p (FP64 scalar) required");
-    if (mhd && (!valid_field(st->B, 3) || !valid_field(st->pB, 1) || st->pB->prec != NOVA_F64 ||
+    if (mhd && (!valid_field(ctx, st->B, 3) || !valid_field(ctx, st->pB, 1) || st->pB->prec != NOVA_F64 ||
                 st->B->prec != rd->precision))
         return fail(ctx, NOVA_E_INVALID, "nova_advance: MHD needs B (3 comps) and pB (FP64 scalar)");
     if (!(rd->dt > 0.0)) return fail(ctx, NOVA_E_INVALID, "nova_advance: dt must be positive");
     nova_status s = ensure_work(ctx, rd->precision);
     if (s != NOVA_OK) return s;
+    if (shear && rd->precision == NOVA_F32SPLIT && (s = dalloc(ctx, &ctx->w32x, 3 * (size_t)ctx->g.N3)) != NOVA_OK)
+        return s;
     if (hist && rd->diag_every > 0) {
         if (ctx->hist_cap < (long long)nsteps * NOVA_HIST_COLS) {
             if (ctx->d_hist) cudaFree(ctx->d_hist);
@@ -1109,7 +1237,7 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     // is taken by the first stage kernel of the next step, which reads the same
     // state with its halos and forms its divergence anyway (the last step's row
     // by the diagnostics kernel)
-    const bool defer_diag = hist && rd->diag_every > 0 && !mhd && rd->precision == NOVA_F64 && !ctx->g.wallY &&
+    const bool defer_diag = hist && rd->diag_every > 0 && !mhd && !shear && rd->precision == NOVA_F64 && !ctx->g.wallY &&
                             !ctx->md.hyperbolic_z && ctx->h == 3 && ctx->stage_impl != STAGE_MARCH &&
                             stage_tma_fits(ctx->g, true);
     StageDiag pend{};
@@ -1120,7 +1248,7 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
                    have ? &pend : nullptr);
         have = false;
         if (s != NOVA_OK) return s;
-        if (mhd) {
+        if (mhd && !shear) {
             // B loop is always the refreshed RK4 (BEqn.H:86-87); B cleaning has no 1/dt (BEqn.H:91-94)
             nova_run_desc rb = *rd;
             rb.rk_mode = NOVA_RK_CLASSICAL;
@@ -1130,7 +1258,9 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
         if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps) && defer_diag &&
             n + 1 < nsteps) {
             pend = StageDiag{ctx->d_part, diag_blocks(ctx->g), ctx->d_hist + (long long)n * NOVA_HIST_COLS,
-                             ctx->d_flag, (double)(n + 1), rd->t0 + (n + 1) * rd->dt, 1.0 / (double)ctx->g.N3};
+                             ctx->d_flag,
+                             diag_final_of(ctx->g, phys_of(ctx, rd), (double)(n + 1), rd->t0 + (n + 1) * rd->dt,
+                                           st->U->d64, nullptr, nullptr)};
             have = true;
         } else if (hist && rd->diag_every > 0 && ((n + 1) % rd->diag_every == 0 || n + 1 == nsteps)) {
             ProfScope ps(ctx, NOVA_K_DIAG);
@@ -1139,8 +1269,7 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
                         B ? B->d64 : nullptr,
                         B ? B->hi : nullptr, B ? B->lo : nullptr, mhd ? 1 : 0, ctx->d_part, (double)(n + 1),
                         rd->t0 + (n + 1) * rd->dt, ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag,
-                        ctx->stream,
-                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
+                        ctx->stream, phys_of(ctx, rd));
             ctx->launches += 2;
             CKL("k_diag");
         }
@@ -1321,12 +1450,12 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: periodic uniform meshes only");
     if (ad->nsteps < 1 || ad->checkpoint_every < 1 || !(rd->dt > 0.0))
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: nsteps, checkpoint_every and dt must be positive");
-    if (!valid_field(init->U, 3) || init->U->prec != rd->precision || !valid_field(gradU, 3) ||
+    if (!valid_field(ctx, init->U, 3) || init->U->prec != rd->precision || !valid_field(ctx, gradU, 3) ||
         gradU->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID,
                     "nova_adjoint_grad: U (3 comps, run precision) and gradU (3 comps, FP64) required");
     if (mhd) {
-        if (!valid_field(init->B, 3) || init->B->prec != rd->precision || !gradB || !valid_field(gradB, 3) ||
+        if (!valid_field(ctx, init->B, 3) || init->B->prec != rd->precision || !gradB || !valid_field(ctx, gradB, 3) ||
             gradB->prec != NOVA_F64)
             return fail(ctx, NOVA_E_INVALID,
                         "nova_adjoint_grad: MHD needs B (3 comps, run precision) and gradB (3 comps, FP64)");
@@ -1363,8 +1492,7 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     const int n0w = window ? ad->window_start : -1;
     auto ekin = [&](const double *u, double *row_dev) {  // diagnostics row of the state u
         launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, u, nullptr, nullptr, nullptr, nullptr,
-                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st,
-                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
+                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
         ctx->launches += 2;
     };
     for (int n = 0; n < N; n++) {
@@ -1667,8 +1795,7 @@ nova_status adjoint_split(nova_ctx *ctx, const nova_adj_desc *ad, const nova_sta
     };
     auto energy = [&](const float *hi, const float *lo, double *row_dev) {
         launch_diag(ctx->h, ctx->g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, hi, lo, nullptr, nullptr,
-                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st,
-                        StageExec{ctx->stage_impl, ctx->d_flag + 1});
+                    nullptr, 0, ctx->d_part, 0.0, 0.0, row_dev, ctx->d_flag, st);
         ctx->launches += 2;
     };
 
@@ -1987,7 +2114,7 @@ extern "C" nova_status nova_im_laplacian(nova_ctx *ctx, double mu, nova_field *x
 {
     if (!ctx || !x || !out) return fail(ctx, NOVA_E_INVALID, "nova_im_laplacian: null argument");
     *out = nullptr;
-    if (!valid_field(x, 1) || x->prec != NOVA_F64)
+    if (!valid_field(ctx, x, 1) || x->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID, "nova_im_laplacian: x must be an FP64 scalar field");
     if (!fdm_mesh_ok(ctx)) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_im_laplacian: periodic uniform meshes only");
     const Geo &g = ctx->g;
@@ -2057,7 +2184,7 @@ extern "C" nova_status nova_fdm_add_source(nova_ctx *ctx, nova_fdm *a, double al
 {
     nova_status s;
     if ((s = fdm_check(ctx, a, "nova_fdm_add_source: bad matrix")) != NOVA_OK) return s;
-    if (!valid_field(f, 1) || f->prec != NOVA_F64)
+    if (!valid_field(ctx, f, 1) || f->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID, "nova_fdm_add_source: f must be an FP64 scalar field");
     launch_fdm_point(ctx->g, 0, alpha, a->coef, f->d64, ctx->stream);
     ctx->launches += 1;
@@ -2210,7 +2337,7 @@ extern "C" nova_status nova_advance_wc(nova_ctx *ctx, const nova_wc_desc *wd, no
     if (!ctx || !wd || !st || nsteps < 0) return fail(ctx, NOVA_E_INVALID, "nova_advance_wc: bad arguments");
     const bool shear = wd->wc_case == NOVA_WC_SHEAR;
     if (wd->wc_case != NOVA_WC_TG && !shear) return fail(ctx, NOVA_E_INVALID, "nova_advance_wc: unknown case");
-    auto f64 = [](const nova_field *f, int nc) { return valid_field(f, nc) && f->prec == NOVA_F64; };
+    auto f64 = [ctx](const nova_field *f, int nc) { return valid_field(ctx, f, nc) && f->prec == NOVA_F64; };
     if (!f64(st->U, 3) || !f64(st->rho, 1) || !f64(st->p, 1) || (shear && !f64(st->T, 1)))
         return fail(ctx, NOVA_E_INVALID, "nova_advance_wc: U, rho, p (and T for the shear case) must be FP64 fields");
     if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_advance_wc: periodic meshes only");
@@ -2268,7 +2395,9 @@ extern "C" nova_status nova_advance_wc(nova_ctx *ctx, const nova_wc_desc *wd, no
             ProfScope ps(ctx, NOVA_K_DIAG);
             launch_diag(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, st->U->d64, nullptr, nullptr, nullptr,
                         nullptr, nullptr, 0, ctx->d_part, (double)(n + 1), wd->t0 + (n + 1) * wd->dt,
-                        ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag, ctx->stream);
+                        ctx->d_hist + (long long)n * NOVA_HIST_COLS, ctx->d_flag, ctx->stream,
+                        DiagPhys{wd->mu, 0.0, wd->dt, ctx->md.L[0] / ctx->md.N[0], ctx->md.L[1] / ctx->md.N[1],
+                                 ctx->md.L[2] / ctx->md.N[2]});
             ctx->launches += 2;
             CKL("k_diag");
         }
@@ -2287,7 +2416,7 @@ extern "C" nova_status nova_wc_hydrostatic(nova_ctx *ctx, const nova_wc_desc *wd
                                            nova_field *p, nova_field *rho)
 {
     if (!ctx || !wd || !T || !p || !rho) return fail(ctx, NOVA_E_INVALID, "nova_wc_hydrostatic: null argument");
-    auto f64 = [](const nova_field *f) { return valid_field(f, 1) && f->prec == NOVA_F64; };
+    auto f64 = [ctx](const nova_field *f) { return valid_field(ctx, f, 1) && f->prec == NOVA_F64; };
     if (!f64(T) || !f64(p) || !f64(rho))
         return fail(ctx, NOVA_E_INVALID, "nova_wc_hydrostatic: T, p, rho must be FP64 scalar fields");
     if (ctx->g.wallY) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_wc_hydrostatic: periodic meshes only");
@@ -2369,7 +2498,7 @@ extern "C" nova_status nova_checkpoint_write(nova_ctx *ctx, const char *path, co
     int32_t nf = 0;
     for (int q = 0; q < 4; q++) {
         if (!fs[q]) continue;
-        if (!valid_field(fs[q], kCkptComps[q]))
+        if (!valid_field(ctx, fs[q], kCkptComps[q]))
             return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_write: state field " + std::to_string(q) +
                                                  " has the wrong component count");
         nf++;
@@ -2409,7 +2538,7 @@ extern "C" nova_status nova_checkpoint_read(nova_ctx *ctx, const char *path, nov
     if (!ctx || !path || !st) return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: null argument");
     nova_field *fs[4] = {st->U, st->p, st->B, st->pB};
     for (int q = 0; q < 4; q++)
-        if (fs[q] && !valid_field(fs[q], kCkptComps[q]))
+        if (fs[q] && !valid_field(ctx, fs[q], kCkptComps[q]))
             return fail(ctx, NOVA_E_INVALID, "nova_checkpoint_read: state field " + std::to_string(q) +
                                                  " has the wrong component count");
     CkptFile f;

@@ -147,19 +147,21 @@ __device__ __forceinline__ T lsum(const V &v, int c, const T *b)
 struct StageArgs64 {
     const double *Y;   // halo'd stage state (3 comps)
     const double *X;   // second halo'd field (MHD), else nullptr
-    const double *U0;  // RK base (stages 1, 2)
+    const double *U0;  // RK base (stages 1, 2, 5)
     double *A;         // RK accumulator
-    double *Ynext;     // next stage state, or U* after the last stage
+    double *Ynext;     // next stage state, or U* after the last stage (stage 5: U*)
+    double w;          // stage 5: the stage's weight
 };
 
 struct StageArgs32 {
     const float *Y;      // halo'd stage state (3 comps, FP32)
     const float *X;      // second halo'd field hi part (MHD)
     const float *U0hi;   // base hi
-    const float *U0lo;   // base lo (last stage / literal)
+    const float *U0lo;   // base lo (last stage / literal / stage 5)
     float *A;            // FP32 increment accumulator
     float *Ynext;        // next stage state (FP32)
-    float *outhi, *outlo;  // U* (last stage / literal)
+    float *outhi, *outlo;  // U* (last stage / literal / stage 5)
+    float w;             // stage 5: the stage's weight
 };
 
 enum Physics { PHYS_NS = 0, PHYS_MHD_U = 1, PHYS_MHD_B = 2 };
@@ -256,6 +258,28 @@ bool stage_tma_fits(const Geo &g, bool fp64);
 // rows > 0: box kTK(k) x 3(c) x rows(j) x 1(i), landing [row][c][k];
 // rows = 0: the 4-wide k-halo box 4(k) x 8(j) x 3(c) x 1(i), landing [c][j][k]
 bool tma_encode_field(CUtensorMap *m, const double *base, const Geo &g, unsigned rows);
+// The per-block diagnostics partials, kDiagParts doubles per block: sums over
+// the unique nodes of 1/2|U|^2, 1/2|B|^2, |ex::curl(U)|, |ex::curl(B)| and the
+// central 1/2|curl U|^2, 1/2|curl B|^2; maxima of |div U| and |div B| over
+// every stored node, of |ex::curl(B)| and |U| over the unique nodes, and of
+// U_x (from 0, signed) over every stored node (tools::CFL's cfl_x).
+enum DiagPart {
+    DP_EK = 0, DP_EM, DP_OMEGA, DP_JAV, DP_ENSU, DP_ENSB,  // sums
+    DP_DIVU, DP_DIVB, DP_JMAX, DP_UMAX, DP_UX, DP_SPARE,  // maxima
+    kDiagParts
+};
+// What the history row needs besides the partials (k_diag_final): the row's
+// step and time, 1/(number of unique nodes), the viscosities of epsilon, and
+// dt and the mesh spacing with the state itself for tools::CFL (the last node
+// of its loop, (N0, N1, N2) of the reference's interior, is the stored node
+// `last`).
+struct DiagFinal {
+    double invN3, step, time;
+    double nu, eta, dt, dx, dy, dz;
+    const double *U64;
+    const float *Uhi, *Ulo;
+    long long N3, last;
+};
 // diagnostics of a stage's input state taken by the stage itself (FP64 TMA
 // stage 0 or literal stage 4, uniform periodic mesh): per-block partials into
 // part (room for cap blocks), then the history row (k_diag_final)
@@ -264,7 +288,7 @@ struct StageDiag {
     int cap;
     double *row;
     int *flag;
-    double step, time, invN3;
+    DiagFinal fin;
 };
 cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
                                const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
@@ -274,7 +298,9 @@ cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef
                                const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
                                cudaStream_t st);
 
-// stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum)
+// stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum),
+// 5 = the shear-layer loop's stage U* = U0 + w dU (app/shearLayer/UEqn.H:28-29;
+// always the register-queue march)
 // stretch: apply the stretched-z Laplacian term (Mesh "hypz:"); on uniform
 // meshes d2zdxi2 is round-off (|.| < 1e-9) and the term is skipped
 // Returns cudaErrorNotSupported when STAGE_TMA is forced on a mesh it does not

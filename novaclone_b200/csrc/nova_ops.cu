@@ -10,12 +10,12 @@
 // (poisson::wavenumbersFFT_, poisson.cpp:337-396) summed in the reference's order.
 #include "nova_gpu.h"
 #include "nova_internal.cuh"
+#include "nova_diag.cuh"
 #include "nova_ops.cuh"
 #include "nova_tile.cuh"
 
 #include <cuComplex.h>
 
-#include <atomic>
 
 namespace nova {
 
@@ -192,10 +192,11 @@ __global__ void k_restrict_rows(Geo g, int ny, const double *__restrict__ ext, d
 constexpr int kRedThreads = 256;
 
 
-// per-block partials: [0] sum 1/2|U|^2, [1] sum 1/2|B|^2, [2] max|div U|, [3] max|div B|
-// Energies sum the unique nodes as app/TG_Piosson/TG.cpp:148-166 does (the
-// stored north-wall row is the reference's last node and is skipped); the
-// divergence maxima cover every stored node (tools::maximum, src/Tools/Tools.h:19-36).
+// The history row's per-block partials (DiagPart, kDiagParts per block).
+// Means and |U|, |curl B| maxima cover the unique nodes as app/OT_Poisson/OT.cpp:136-155
+// does (the stored north-wall row is the reference's last node and is skipped);
+// the divergence maxima and U_x cover every stored node (tools::maximum,
+// src/Tools/Tools.h:19-36; tools::CFL, src/Tools/Tools.cpp:15-25).
 template <int H, int NC, class LD, bool WALLS>
 __global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl, Coef<double> co,
                                                          const double *__restrict__ ia, LD U, LD B, int ichunk,
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     auto &sm = *reinterpret_cast<TileSmem<double, H, NC> *>(smraw);
-    __shared__ double red[4][kThreads / 32];
+    __shared__ double red[kDiagParts][kThreads / 32];
     const int ib = blockIdx.z * ichunk;
     const int ie = min(ib + ichunk, g.N0);
     const int kw = wrapi(blockIdx.x * kTK + threadIdx.x, g.N2);
@@ -211,77 +212,82 @@ __global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl
 #pragma unroll
     for (int l = 0; l < H; l++) az[l] = co.a[2][l] * ia[kw];
     const int rows_e = g.N1 - g.wallY;
-    double ek = 0.0, em = 0.0, mdu = 0.0, mdb = 0.0;
+    DiagAcc acc;
     auto ld = [&](int c, long long o) -> double { return c < 3 ? U(c, o) : B(c - 3, o); };
     tile_march<double, H, NC, WALLS>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
                                                           const auto &vz) {
         const int j = (int)((idx % g.N12) / g.N2);
         const bool ce = j < rows_e;
-        const double u = q[H][0], v = q[H][1], w = q[H][2];
-        if (ce) ek += 0.5 * (u * u + v * v + w * w);
+        const double u[3] = {q[H][0], q[H][1], q[H][2]};
         const double du = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
-        mdu = fmax(mdu, fabs(du));
+        double q1, hs;
+        curl_terms<H>(vx, vy, vz, 0, co.a[0], co.a[1], az, 1.0, q1, hs);
+        acc.add_u(u, du, q1, hs, ce);
         if constexpr (NC == 6) {
-            const double bx = q[H][3], by = q[H][4], bz = q[H][5];
-            if (ce) em += 0.5 * (bx * bx + by * by + bz * bz);
+            const double b[3] = {q[H][3], q[H][4], q[H][5]};
             const double db = d1<double, H>(vx, 3, co.a[0]) + d1<double, H>(vy, 4, co.a[1]) + d1<double, H>(vz, 5, az);
-            mdb = fmax(mdb, fabs(db));
+            curl_terms<H>(vx, vy, vz, 3, co.a[0], co.a[1], az, 1.0, q1, hs);
+            acc.add_b(b, db, q1, hs, ce);
         }
     });
     const int tid = threadIdx.y * kTK + threadIdx.x, lane = tid & 31, w = tid >> 5;
+    acc.warp_reduce();
+    if (lane == 0)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        ek += __shfl_down_sync(0xffffffffu, ek, o);
-        em += __shfl_down_sync(0xffffffffu, em, o);
-        mdu = fmax(mdu, __shfl_down_sync(0xffffffffu, mdu, o));
-        mdb = fmax(mdb, __shfl_down_sync(0xffffffffu, mdb, o));
-    }
-    if (lane == 0) {
-        red[0][w] = ek;
-        red[1][w] = em;
-        red[2][w] = mdu;
-        red[3][w] = mdb;
-    }
+        for (int q = 0; q < kDiagParts; q++) red[q][w] = acc.v[q];
     __syncthreads();
-    if (tid == 0) {
-        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        for (int q = 0; q < kThreads / 32; q++) {
-            a0 += red[0][q];
-            a1 += red[1][q];
-            a2 = fmax(a2, red[2][q]);
-            a3 = fmax(a3, red[3][q]);
-        }
+    if (tid < kDiagParts) {
+        double a = 0.0;
+        for (int x = 0; x < kThreads / 32; x++) a = tid >= DP_DIVU ? fmax(a, red[tid][x]) : a + red[tid][x];
         const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        part[blk * 4 + 0] = a0;
-        part[blk * 4 + 1] = a1;
-        part[blk * 4 + 2] = a2;
-        part[blk * 4 + 3] = a3;
+        part[blk * kDiagParts + tid] = a;
     }
 }
 
-__global__ void k_diag_final(const double *__restrict__ part, int nblk, double invN3, double step, double time,
-                             double *__restrict__ row, int *__restrict__ flag)
+// std::max(a, b) of the reference: b only when a < b
+__device__ __forceinline__ double ref_max(double a, double b) { return a < b ? b : a; }
+
+__global__ void k_diag_final(const double *__restrict__ part, int nblk, DiagFinal fin, double *__restrict__ row,
+                             int *__restrict__ flag)
 {
     __shared__ double sh[32];
-    double a = 0, b = 0, c = 0, d = 0;
-    for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
-        a += part[q * 4 + 0];
-        b += part[q * 4 + 1];
-        c = fmax(c, part[q * 4 + 2]);
-        d = fmax(d, part[q * 4 + 3]);
+    double tot[kDiagParts];
+#pragma unroll
+    for (int q = 0; q < kDiagParts; q++) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+            a = q >= DP_DIVU ? fmax(a, part[(long long)b * kDiagParts + q]) : a + part[(long long)b * kDiagParts + q];
+        tot[q] = q >= DP_DIVU ? block_reduce_max(a, sh) : block_reduce_sum(a, sh);
     }
-    a = block_reduce_sum(a, sh);
-    b = block_reduce_sum(b, sh);
-    c = block_reduce_max(c, sh);
-    d = block_reduce_max(d, sh);
     if (threadIdx.x == 0) {
-        row[0] = step;
-        row[1] = time;
-        row[2] = a * invN3;
-        row[3] = b * invN3;
-        row[4] = c;
-        row[5] = d;
-        if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(d)) atomicExch(flag, 1);
+        const double n = fin.invN3;
+        const double om = tot[DP_OMEGA] * n, jav = tot[DP_JAV] * n;
+        // tools::CFL: cfl_x = max over the nodes of U_x dt / dx (from 0); cfl_y,
+        // cfl_z = std::max(cfl_x, U dt / d) at the loop's last node
+        auto last = [&](int c) -> double {
+            const long long o = (long long)c * fin.N3 + fin.last;
+            return fin.U64 ? fin.U64[o] : (double)fin.Uhi[o] + (double)fin.Ulo[o];
+        };
+        const double cx = tot[DP_UX] * fin.dt / fin.dx;
+        row[0] = fin.step;
+        row[1] = fin.time;
+        row[2] = tot[DP_EK] * n;
+        row[3] = tot[DP_EM] * n;
+        row[4] = tot[DP_DIVU];
+        row[5] = tot[DP_DIVB];
+        row[6] = om;
+        row[7] = jav;
+        row[8] = tot[DP_JMAX];
+        row[9] = -fin.nu * (om * om) - fin.eta * (jav * jav);
+        row[10] = tot[DP_UMAX];
+        row[11] = cx;
+        row[12] = ref_max(cx, last(1) * fin.dt / fin.dy);
+        row[13] = ref_max(cx, last(2) * fin.dt / fin.dz);
+        row[14] = tot[DP_ENSU] * n;
+        row[15] = tot[DP_ENSB] * n;
+        bool bad = false;
+        for (int q = 0; q < kDiagParts; q++) bad = bad || !isfinite(tot[q]);
+        if (bad) atomicExch(flag, 1);
     }
 }
 
@@ -750,19 +756,34 @@ int diag_blocks(const Geo &g)
     return (int)(tiled > 1184 ? tiled : 1184);
 }
 
+DiagFinal diag_final_of(const Geo &g, const DiagPhys &ph, double step, double time, const double *U64,
+                        const float *Uhi, const float *Ulo)
+{
+    DiagFinal f{};
+    f.invN3 = 1.0 / (double)((long long)g.N0 * (g.N1 - g.wallY) * g.N2);
+    f.step = step;
+    f.time = time;
+    f.nu = ph.nu;
+    f.eta = ph.eta;
+    f.dt = ph.dt;
+    f.dx = ph.dx;
+    f.dy = ph.dy;
+    f.dz = ph.dz;
+    f.U64 = U64;
+    f.Uhi = Uhi;
+    f.Ulo = Ulo;
+    f.N3 = g.N3;
+    // the reference's interior node (N0, N1, N2): periodic axes wrap to 0, a
+    // wall axis stores it (the north wall row)
+    f.last = g.wallY ? (long long)(g.N1 - 1) * g.N2 : 0;
+    return f;
+}
+
 void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                  const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
                  const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,
-                 cudaStream_t st, const StageExec &ex)
+                 cudaStream_t st, const DiagPhys &ph)
 {
-    const double invN3 = 1.0 / (double)((long long)g.N0 * (g.N1 - g.wallY) * g.N2);
-    if (ex.err && h == 3 && !wl.on && !hasB && ex.impl != STAGE_MARCH && proj_tma_fits(g)) {
-        const int nb = launch_diag_tma(g, co, ia, U64, Uhi, Ulo, part, diag_blocks(g), ex.err, st);
-        if (nb > 0) {
-            k_diag_final<<<1, 256, 0, st>>>(part, nb, invN3, step, time, row, flag);
-            return;
-        }
-    }
     const int ch = pick_ichunk(g, 2);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
     const int nb = (int)(grid.x * grid.y * grid.z);
@@ -789,14 +810,12 @@ void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double
         }
     }
 #undef NOVA_DIAG
-    k_diag_final<<<1, 256, 0, st>>>(part, nb, 1.0 / (double)((long long)g.N0 * (g.N1 - g.wallY) * g.N2), step, time,
-                                    row, flag);
+    k_diag_final<<<1, 256, 0, st>>>(part, nb, diag_final_of(g, ph, step, time, U64, Uhi, Ulo), row, flag);
 }
 
-void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
-                       cudaStream_t st)
+void launch_diag_final(const double *part, int nb, const DiagFinal &fin, double *row, int *flag, cudaStream_t st)
 {
-    k_diag_final<<<1, 256, 0, st>>>(part, nb, invN3, step, time, row, flag);
+    k_diag_final<<<1, 256, 0, st>>>(part, nb, fin, row, flag);
 }
 
 void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st)
@@ -814,22 +833,15 @@ static __device__ __align__(256) double g_maxabs_scratch[kMaxabsStaticParts + 1]
 static_assert((long long)kMaxabsChunk * kMaxabsStaticParts == NOVA_MAXABS_NOALLOC_MAX_NODES,
               "the static scratch must cover the advertised node limit");
 
-constexpr int kMaxabsDevices = 64;
-// per-device address, looked up once with that device current
-static std::atomic<double *> g_maxabs_scratch_ptr[kMaxabsDevices];
-
+// The scratch's device address, looked up on every call with the caller's
+// device current: a cached address would go stale when the primary context
+// is destroyed and made again (cudaDeviceReset), and the lookup is cheap once
+// the module is loaded.
 cudaError_t maxabs_noalloc_scratch(double **scratch)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    double *q = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void **)&q, g_maxabs_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxabsDevices) return cudaErrorInvalidDevice;
-    double *q = g_maxabs_scratch_ptr[dev].load(std::memory_order_acquire);
-    if (!q) {
-        e = cudaGetSymbolAddress((void **)&q, g_maxabs_scratch);
-        if (e != cudaSuccess) return e;
-        g_maxabs_scratch_ptr[dev].store(q, std::memory_order_release);
-    }
     *scratch = q;
     return cudaSuccess;
 }

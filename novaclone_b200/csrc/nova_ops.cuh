@@ -65,19 +65,21 @@ void launch_fdm_factor(int axis, const Geo &g, const double *coef, double *fac, 
 // one sweep of line solves along axis with those factors, xin -> xout (distinct)
 void launch_fdm_line(int axis, const Geo &g, const double *coef, const double *fac, const double *ls,
                      const double *xin, double *xout, cudaStream_t st);
-// the history row from nb blocks of partials (Ek, Em, max|div U|, max|div B| per block)
-void launch_diag_final(const double *part, int nb, double invN3, double step, double time, double *row, int *flag,
-                       cudaStream_t st);
-// ex: with its error word, a Navier-Stokes field on a mesh the TMA projection
-// kernels fit takes the TMA diagnostics pass (nova_proj_tma.cu)
+// the history row from nb blocks of partials (kDiagParts per block)
+void launch_diag_final(const double *part, int nb, const DiagFinal &fin, double *row, int *flag, cudaStream_t st);
+// the physical parameters of a history row (epsilon, tools::CFL); zeros where
+// only the energies are wanted
+struct DiagPhys {
+    double nu, eta, dt, dx, dy, dz;
+};
+// the DiagFinal of a row of the state (U64 or Uhi/Ulo) on mesh g
+DiagFinal diag_final_of(const Geo &g, const DiagPhys &ph, double step, double time, const double *U64,
+                        const float *Uhi, const float *Ulo);
+// the history row of the state U (and B where hasB) by the tiled diagnostics kernel
 void launch_diag(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                  const double *U64, const float *Uhi, const float *Ulo, const double *B64, const float *Bhi,
                  const float *Blo, int hasB, double *part, double step, double time, double *row, int *flag,
-                 cudaStream_t st, const StageExec &ex = StageExec{STAGE_MARCH, nullptr});
-// Ek and max|div U| partials of one field by the TMA divergence loads: the
-// number of blocks written, 0 where the grid exceeds cap blocks (nothing launched)
-int launch_diag_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *hi,
-                    const float *lo, double *part, int cap, int *err, cudaStream_t st);
+                 cudaStream_t st, const DiagPhys &ph = DiagPhys{0, 0, 0, 1, 1, 1});
 void launch_maxabs(const Geo &g, const double *s, double *part, double *out, cudaStream_t st);
 void launch_op(int op, int h, const Geo &g, const Walls<double> &wa, const Walls<double> &wb, const Coef<double> &co,
                const double *ia, const double *corr2, const double *a, const double *b, int nc, double nu, double *out,

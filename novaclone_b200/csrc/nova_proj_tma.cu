@@ -33,9 +33,7 @@ constexpr int kRowsE = (TJ + 2 * kH) * kTK;  // a component's rows with the j ha
 constexpr int kTileE = TJ * kTK;             // a component's tile rows
 constexpr int kLRE = TJ * 4;                 // one side's k halo of a component
 
-// PROJ_DIAG: the loads of PROJ_DIV; per block, sum 1/2 |U|^2 and max |div U| into
-// the diagnostics partials (Ek, Em = 0, max|div U|, max|div B| = 0)
-enum ProjMode { PROJ_DIV = 0, PROJ_CORR = 1, PROJ_DIAG = 2 };
+enum ProjMode { PROJ_DIV = 0, PROJ_CORR = 1 };
 
 // map indices
 enum {
@@ -54,7 +52,7 @@ struct ProjMaps {
 };
 
 template <int MODE, bool SPLIT> struct ProjCfg {
-    static constexpr bool kDivLoads = MODE == PROJ_DIV || MODE == PROJ_DIAG;
+    static constexpr bool kDivLoads = MODE == PROJ_DIV;
     using TS = typename std::conditional<kDivLoads && SPLIT, float, double>::type;  // stencil element
     using TE = typename std::conditional<SPLIT, float, double>::type;              // U* element
     static constexpr int kSets = (kDivLoads && SPLIT) ? 2 : 1;
@@ -71,7 +69,6 @@ template <int MODE, bool SPLIT> struct ProjCfg {
 
 struct ProjArgs {
     double divisor, s;
-    double *part;               // DIAG output (4 doubles per block)
     double *rhs;                // DIV output
     double *U64;                // CORR output (FP64)
     float *hi, *lo;             // CORR output (split)
@@ -214,7 +211,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     };
 
     double q[2 * H + 1];
-    double ek = 0.0, mdu = 0.0;  // DIAG
     bool ok = true;
     for (int n = 0; n < 2 * H; n++) {
         ok = mbar_wait(full(n % kRing), (n / kRing) & 1, err);
@@ -246,11 +242,6 @@ __global__ void __launch_bounds__(kThreads, 2)
         if constexpr (MODE == PROJ_DIV) {
             const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
             a.rhs[idx] = d / a.divisor;
-        } else if constexpr (MODE == PROJ_DIAG) {
-            const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
-            const double u = q[H], v = val(sl, yoff), w = val(sl, oZ + ty * kTK + tx);
-            ek += 0.5 * (u * u + v * v + w * w);
-            mdu = fmax(mdu, fabs(d));
         } else {
             const double gr[3] = {d1<double, H>(vx, 0, co.a[0]), d1<double, H>(vy, 0, co.a[1]),
                                   d1<double, H>(vz, 0, az)};
@@ -279,32 +270,6 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
         }
         release(empty(cur % kRing));
-    }
-    if constexpr (MODE == PROJ_DIAG) {
-        // consumer warps only (the producer has returned): fixed-order sums
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            ek += __shfl_down_sync(0xffffffffu, ek, o);
-            mdu = fmax(mdu, __shfl_down_sync(0xffffffffu, mdu, o));
-        }
-        double *red = reinterpret_cast<double *>(smraw + (bar0 - s0) + 8 * 2 * (kRing + kERing));
-        if (lane == 0) {
-            red[2 * ty] = ek;
-            red[2 * ty + 1] = mdu;
-        }
-        asm volatile("bar.sync 1, %0;" ::"n"(kWarps * 32) : "memory");
-        if (ty == 0 && lane == 0) {
-            double s_ = 0.0, m_ = 0.0;
-            for (int w = 0; w < kWarps; w++) {
-                s_ += red[2 * w];
-                m_ = fmax(m_, red[2 * w + 1]);
-            }
-            const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-            a.part[blk * 4 + 0] = s_;
-            a.part[blk * 4 + 1] = 0.0;
-            a.part[blk * 4 + 2] = m_;
-            a.part[blk * 4 + 3] = 0.0;
-        }
     }
 }
 
@@ -413,31 +378,6 @@ cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const double *i
     const bool ok = set_maps(0, hi) && set_maps(M_SET, lo);
     if (!ok) return cudaErrorInvalidValue;
     return launch<PROJ_DIV, true>(g, co, ia, a, pm, err, st);
-}
-
-int launch_diag_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *hi,
-                    const float *lo, double *part, int cap, int *err, cudaStream_t st)
-{
-    const int ch = proj_ichunk(g);
-    const long long nb = (long long)(g.N2 / kTK) * (g.N1 / TJ) * ((g.N0 + ch - 1) / ch);
-    if (nb > cap) return 0;
-    ProjMaps pm;
-    memset(&pm, 0, sizeof pm);
-    ProjArgs a{};
-    a.part = part;
-    auto set_maps = [&](int ms, const auto *f) {
-        return encode3(&pm.m[ms + M_C0], f, g, kTK, TJ) && encode_rows(pm, ms, f + g.N3, g) &&
-               encode3(&pm.m[ms + M_C2], f + 2 * g.N3, g, kTK, TJ) &&
-               encode3(&pm.m[ms + M_LR], f + 2 * g.N3, g, 4, kLRB);
-    };
-    if (U64) {
-        if (!set_maps(0, U64)) return 0;
-        launch<PROJ_DIAG, false>(g, co, ia, a, pm, err, st);
-    } else {
-        if (!(set_maps(0, hi) && set_maps(M_SET, lo))) return 0;
-        launch<PROJ_DIAG, true>(g, co, ia, a, pm, err, st);
-    }
-    return (int)nb;
 }
 
 cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,

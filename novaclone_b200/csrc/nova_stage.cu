@@ -27,6 +27,7 @@
 //   s=3: U* = A  + dU*1/6
 //   s=4 (the reference loop as written, U not refreshed between stages, so
 //        all four dU are equal): U* = (((U0 + dU/6) + dU/3) + dU/3) + dU/6
+//   s=5 (app/shearLayer/UEqn.H:28-29): U* = U0 + dU*w, w the stage's weight
 // The FP32-split variant keeps A as an FP32 sum of increments and adds it to
 // the (hi, lo) base in FP64 at the last stage.
 #include "nova_internal.cuh"
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
     // pointwise epilogue operands (base, accumulator): prefetched one plane
     // ahead in FP64; the FP32 kernels load them at the start of the plane
     // (measured faster there: fewer live registers)
-    constexpr bool kE0 = (STAGE == 1 || STAGE == 2) || (!std::is_same<T, double>::value && STAGE == 3);
+    constexpr bool kE0 = (STAGE == 1 || STAGE == 2 || STAGE == 5) || (!std::is_same<T, double>::value && STAGE == 3);
     constexpr bool kE1 = (STAGE >= 1 && STAGE <= 3);
     constexpr bool kAhead = std::is_same<T, double>::value;
     const T *e0p = nullptr, *e1p = nullptr;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const long long o = (long long)c * g.N3 + idx;
-                    const float lo = (STAGE == 3 || STAGE == 4) ? args.U0lo[o] : 0.0f;
+                    const float lo = (STAGE >= 3) ? args.U0lo[o] : 0.0f;
                     rk_store32<STAGE>(args, o, q[H][c], e0[c], e1[c], lo, dt * rhs[c]);
                 }
             }
@@ -224,6 +225,7 @@ void launch_stage_t(int stage, const Geo &g, const Walls<T> &wl, const Coef<T> &
     case 1: launch_one<T, PHYS, 1, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
     case 2: launch_one<T, PHYS, 2, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
     case 3: launch_one<T, PHYS, 3, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
+    case 5: launch_one<T, PHYS, 5, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
     default: launch_one<T, PHYS, 4, STRETCH, WALLS>(g, wl, co, ia, corr2, dt, visc, a, st); break;
     }
 }
@@ -256,9 +258,9 @@ cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, cons
                            const StageArgs64 &a, cudaStream_t st, const StageExec &ex, const StageDiag *dg,
                            bool *dg_done)
 {
-    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g, true))
+    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage <= 4 && stage_tma_fits(g, true))
         return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st, dg, dg_done);
-    if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
+    if (phys == PHYS_NS && ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
     launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;
 }
@@ -267,9 +269,9 @@ cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, cons
                            const Coef<float> &co, const float *ia, const float *corr2, float dt, float visc,
                            const StageArgs32 &a, cudaStream_t st, const StageExec &ex)
 {
-    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage_tma_fits(g, false))
+    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage <= 4 && stage_tma_fits(g, false))
         return launch_stage_tma32(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
-    if (phys == PHYS_NS && ex.impl == STAGE_TMA) return cudaErrorNotSupported;
+    if (phys == PHYS_NS && ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
     launch_stage_any<float>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;
 }

@@ -92,12 +92,15 @@ __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz,
 //   s=1: Y2 = U0 + dU*1/2   A = A  + dU*1/3
 //   s=2: Y3 = U0 + dU       A = A  + dU*1/3
 //   s=3: U* = A  + dU*1/6
-// y0: the stage state at the node; e0: U0 (stages 1, 2); e1: A (stages 1-3)
+//   s=5: U* = U0 + dU*w   (app/shearLayer/UEqn.H:28-29, w = RK4[rk] of the stage)
+// y0: the stage state at the node; e0: U0 (stages 1, 2, 5); e1: A (stages 1-3)
 template <int STAGE>
 __device__ __forceinline__ void rk_store64(const StageArgs64 &a, long long o, double y0, double e0, double e1, double du)
 {
     const double w6 = 1.0 / 6.0, w3 = 1.0 / 3.0;
-    if constexpr (STAGE == 4) {
+    if constexpr (STAGE == 5) {
+        a.Ynext[o] = e0 + du * a.w;
+    } else if constexpr (STAGE == 4) {
         a.Ynext[o] = (((y0 + du * w6) + du * w3) + du * w3) + du * w6;
     } else if constexpr (STAGE == 0) {
         a.Ynext[o] = y0 + du * 0.5;
@@ -114,13 +117,18 @@ __device__ __forceinline__ void rk_store64(const StageArgs64 &a, long long o, do
 }
 
 // FP32-split: A is an FP32 sum of increments; the last stage adds it to the
-// (hi, lo) base in FP64.  e0: U0hi (stages 1-3), e1: A, lo: U0lo (stages 3, 4)
+// (hi, lo) base in FP64.  e0: U0hi (stages 1-3, 5), e1: A, lo: U0lo (stages 3-5)
 template <int STAGE>
 __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, float y0, float e0, float e1, float lo,
                                            float du)
 {
     const float w6 = 1.0f / 6.0f, w3 = 1.0f / 3.0f;
-    if constexpr (STAGE == 4) {
+    if constexpr (STAGE == 5) {
+        const double x = ((double)e0 + (double)lo) + (double)(du * a.w);
+        const float hi = (float)x;
+        a.outhi[o] = hi;
+        a.outlo[o] = (float)(x - (double)hi);
+    } else if constexpr (STAGE == 4) {
         const float inc = ((du * w6 + du * w3) + du * w3) + du * w6;
         const double x = ((double)y0 + (double)lo) + (double)inc;
         const float hi = (float)x;

@@ -25,6 +25,7 @@
 // Every mbarrier wait is bounded (nova_tma.cuh); a wait that gives up raises
 // the error word and the block leaves its pipeline, the producer after waiting,
 // again bounded, for the loads it still has in flight.
+#include "nova_diag.cuh"
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"
 #include "nova_stage_math.cuh"
@@ -75,13 +76,14 @@ template <typename T, int STAGE> __host__ __device__ constexpr int epi_fields()
         return (STAGE == 1 || STAGE == 2) ? 2 : (STAGE == 3 ? 3 : (STAGE == 4 ? 1 : 0));
 }
 
-// ring data, the ring barriers, then 2 doubles per consumer warp for the
-// diagnostics reduction (DIAG launches)
-template <typename T, int NE> constexpr size_t tma_smem_bytes()
+// ring data, the ring barriers, then (DIAG launches) kDiagParts doubles per
+// consumer warp for the block's reduction and six per consumer thread for the
+// running diagnostics
+template <typename T, int NE, bool DIAG = false> constexpr size_t tma_smem_bytes()
 {
     using C = TmaCfg<T>;
     return ((size_t)C::kRing * C::kSlotE + (size_t)C::kERing * NE * C::kEpiE) * sizeof(T) +
-           8 * (2 * C::kRing + 2 * C::kERing) + 16 * C::kWarps;
+           8 * (2 * C::kRing + 2 * C::kERing) + (DIAG ? 8 * (kDiagParts + 6 * kTK) * C::kWarps : 0);
 }
 
 struct StageMaps {
@@ -109,10 +111,11 @@ __device__ __forceinline__ void epi_read(const T *se, int c, T &e0, T &e1, T &lo
     }
 }
 
-// DIAG (FP64, stages that read U itself: 0 and the literal 4): the block also
-// sums 1/2 |U|^2 and takes max |div U| over its nodes, the divergence being the
-// one the stage arithmetic forms anyway, and writes them to dpart[block * 4]
-// (the layout of the diagnostics partials: Ek, Em = 0, max|div U|, max|div B| = 0)
+// DIAG (FP64, stages that read U itself: 0 and the literal 4, uniform
+// periodic mesh): the block also reduces the history row's terms of U over its
+// nodes (nova_diag.cuh: energy, |U|, U_x, the divergence the stage arithmetic
+// forms anyway, and the two curls from the stencil values it holds) into
+// dpart[block * kDiagParts] (the B terms zero)
 template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG>
 __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     k_stage_tma(Geo g, Coef<T> co, StageCoef<T> sc, const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
@@ -233,7 +236,10 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     // centre H) of step p is q[(p + s) % 7]; the loop is unrolled by 7
     // (= 2H + 1 = kRing) so that the rotation is register renaming and every
     // ring slot index is a compile-time constant of the unrolled step.
-    double ek = 0.0, mdu = 0.0;  // DIAG
+    // DIAG: the running diagnostics in shared memory (the registers hold the queue)
+    double *dred = reinterpret_cast<double *>(smraw + (bar0 - s0) + 8 * (2 * kRing + 2 * kERing));
+    DiagAccSm dacc{dred + kDiagParts * C::kWarps + ty * kTK + tx, C::kWarps * kTK};
+    if constexpr (DIAG) dacc.init();
     if constexpr (sizeof(T) == 8) {
         T q[2 * H + 1][3];
         bool ok = true;
@@ -276,8 +282,9 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             T rhs[3], divu;
             ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs, divu);
             if constexpr (DIAG) {
-                ek += 0.5 * (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]);
-                mdu = fmax(mdu, fabs(divu));
+                double q1, hs;
+                curl_terms<H>(vx, vy, vz, 0, co.a[0], co.a[1], co.a[2], iak, q1, hs);
+                dacc.add(u0, divu, q1, hs);
             }
 
             T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
@@ -386,28 +393,19 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
 
     if constexpr (DIAG) {
         // consumer warps only (the producer has returned): fixed-order sums
+        DiagAccU acc = dacc.load();
+        acc.warp_reduce();
+        double *red = dred;
+        if (lane == 0)
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            ek += __shfl_down_sync(0xffffffffu, ek, o);
-            mdu = fmax(mdu, __shfl_down_sync(0xffffffffu, mdu, o));
-        }
-        double *red = reinterpret_cast<double *>(smraw + (bar0 - s0) + 8 * (2 * kRing + 2 * kERing));
-        if (lane == 0) {
-            red[2 * ty] = ek;
-            red[2 * ty + 1] = mdu;
-        }
+            for (int q = 0; q < kDiagParts; q++) red[q * C::kWarps + ty] = acc.part(q);
         asm volatile("bar.sync 1, %0;" ::"n"(C::kWarps * 32) : "memory");
-        if (ty == 0 && lane == 0) {
-            double a = 0.0, b = 0.0;
-            for (int w = 0; w < C::kWarps; w++) {
-                a += red[2 * w];
-                b = fmax(b, red[2 * w + 1]);
-            }
+        if (ty == 0 && lane < kDiagParts) {
+            double a = 0.0;
+            for (int w = 0; w < C::kWarps; w++)
+                a = lane >= DP_DIVU ? fmax(a, red[lane * C::kWarps + w]) : a + red[lane * C::kWarps + w];
             const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-            dpart[blk * 4 + 0] = a;
-            dpart[blk * 4 + 1] = 0.0;
-            dpart[blk * 4 + 2] = b;
-            dpart[blk * 4 + 3] = 0.0;
+            dpart[blk * kDiagParts + lane] = a;
         }
     }
 }
@@ -481,7 +479,7 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
               encode(&maps.tcbB, Y, g, Cf::TJ + kH) && encode(&maps.lr, Y, g, 0);
     for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, Cf::TJ);
     if (!ok) return cudaErrorInvalidValue;
-    constexpr size_t smem = tma_smem_bytes<T, NE>();
+    constexpr size_t smem = tma_smem_bytes<T, NE, DIAG>();
     auto kern = k_stage_tma<T, STAGE, STRETCH, Args, DIAG>;
     static bool attr = false;
     if (!attr) {
@@ -547,7 +545,7 @@ cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef
                            : launch_tma<double, 4, false, StageArgs64, true>(g, co, ia, corr2, dt, visc, a, a.Y, ef,
                                                                              err, st, dg->part);
             if (e != cudaSuccess) return e;
-            launch_diag_final(dg->part, (int)nb, dg->invN3, dg->step, dg->time, dg->row, dg->flag, st);
+            launch_diag_final(dg->part, (int)nb, dg->fin, dg->row, dg->flag, st);
             if (dg_done) *dg_done = true;
             return cudaSuccess;
         }

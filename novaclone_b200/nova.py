@@ -22,8 +22,12 @@ POISSON_FFT, POISSON_DCT = 0, 1
 F64, F32SPLIT = 0, 1
 PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
 MODEL_NS, MODEL_MHD = 0, 1
-RK_LITERAL, RK_CLASSICAL = 0, 1
-HIST_COLS = 6
+RK_LITERAL, RK_CLASSICAL, RK_SHEARLAYER = 0, 1, 2
+# history row (nova_gpu.h NOVA_HIST_COLS): step, t, Ek, Em, max|div U|, max|div B|, omega, Jav,
+# Jmax, epsilon, Umax, cfl_x, cfl_y, cfl_z, 1/2<|curl U|^2>, 1/2<|curl B|^2>
+HIST_COLS = 16
+HIST_NAMES = ("step", "t", "Ek", "Em", "max_div_U", "max_div_B", "omega", "Jav", "Jmax", "epsilon", "Umax",
+              "cfl_x", "cfl_y", "cfl_z", "enstrophy_U", "enstrophy_B")
 K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG, K_ADJ = range(6)
 OBJ_EKIN_FINAL, OBJ_DISSIPATION_WINDOW, OBJ_ETOT_FINAL = 0, 1, 2
 WC_TG, WC_SHEAR = 0, 1
@@ -499,7 +503,7 @@ def run_desc(model="ns", rk_mode="classical", precision=F64, dt=0.01, nu=0.0, et
     r = RunDesc()
     r.poisson = POISSON_DCT if poisson == "dct" else POISSON_FFT
     r.model = MODEL_MHD if model == "mhd" else MODEL_NS
-    r.rk_mode = RK_CLASSICAL if rk_mode == "classical" else RK_LITERAL
+    r.rk_mode = {"literal": RK_LITERAL, "classical": RK_CLASSICAL, "shear": RK_SHEARLAYER}[rk_mode]
     r.precision = precision
     r.diag_every = diag_every
     r.dt, r.nu, r.eta, r.t0 = float(dt), float(nu), float(eta), float(t0)
@@ -508,7 +512,7 @@ def run_desc(model="ns", rk_mode="classical", precision=F64, dt=0.01, nu=0.0, et
 
 def advance(mesh: Mesh, rd: RunDesc, U: Field, p: Field, B: Field = None, pB: Field = None, nsteps: int = 1,
             history: bool = True):
-    """nsteps of the reference loop body; returns the (nsteps, 6) history or None."""
+    """nsteps of the reference loop body; returns the (nsteps, HIST_COLS) history or None."""
     st = State(U.h, p.h, B.h if B is not None else None, pB.h if pB is not None else None)
     hist = np.zeros((max(nsteps, 1), HIST_COLS)) if history else None
     mesh.check(mesh.lib.nova_advance(mesh.h, C.byref(rd), C.byref(st), int(nsteps),

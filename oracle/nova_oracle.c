@@ -3,6 +3,11 @@
  * See nova_oracle.h.  Each function names the reference lines it restates.
  * Build with -ffp-contract=off: the expressions below keep the reference's
  * association order so the result matches the reference bit for bit.
+ *
+ * With OpenMP the node loops are split across threads by i (inside each `l`
+ * pass where the reference sweeps l outermost), so every node still receives
+ * its terms in the reference's order and the result does not depend on the
+ * thread count; the reductions of the diagnostics stay serial.
  */
 #include "nova_oracle.h"
 #include "orc_fft.h"
@@ -227,6 +232,7 @@ void orc_grad_s(const orc_mesh *M, const double *f, double *g)
     const double *co = M->coef;
     memset(g, 0, sizeof(double) * 3 * npts(M));
     for (int l = 0; l < h; l++)
+#pragma omp parallel for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++)
                 for (int k = h; k < M->n[2] - h; k++) {
@@ -250,6 +256,7 @@ void orc_grad_v(const orc_mesh *M, const double *U, double *T)
     const int h = M->h;
     const double *co = M->coef;
     memset(T, 0, sizeof(double) * 9 * npts(M));
+#pragma omp parallel for schedule(static)
     for (int i = h; i < M->n[0] - h; i++)
         for (int j = h; j < M->n[1] - h; j++)
             for (int k = h; k < M->n[2] - h; k++) {
@@ -275,6 +282,7 @@ void orc_curl(const orc_mesh *M, const double *U, double *out)
     double *T = (double *)malloc(sizeof(double) * 9 * npts(M));
     orc_grad_v(M, U, T);
     memset(out, 0, sizeof(double) * 3 * npts(M));
+#pragma omp parallel for schedule(static)
     for (int i = h; i < M->n[0] - h; i++)
         for (int j = h; j < M->n[1] - h; j++)
             for (int k = h; k < M->n[2] - h; k++) {
@@ -293,10 +301,13 @@ void orc_div_v(const orc_mesh *M, const double *U, double *out)
     const int h = M->h, nk = M->n[2];
     const double dx = M->d[0], dy = M->d[1], dz = M->d[2];
     const double *co = M->coef;
+    memset(out, 0, sizeof(double) * npts(M));
+#pragma omp parallel
+    {
     double *Up = (double *)malloc(sizeof(double) * 6 * nk);
     double *Um = Up + nk, *Vp = Up + 2 * nk, *Vm = Up + 3 * nk, *Wp = Up + 4 * nk, *Wm = Up + 5 * nk;
-    memset(out, 0, sizeof(double) * npts(M));
     for (int l = 0; l < h; l++)
+#pragma omp for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++) {
                 double *dp = out + IDX(M, i, j, 0);
@@ -318,6 +329,7 @@ void orc_div_v(const orc_mesh *M, const double *U, double *out)
                               - co[l] / 2.0 / (l + 1) / dz * Wm[k] / M->dzdxi[k]);
             }
     free(Up);
+    }
 }
 
 /* ex::div(Field<vector> U, Field<T> f): skew-symmetric advective form
@@ -328,11 +340,14 @@ void orc_div_vf(const orc_mesh *M, const double *U, const double *f, int nc, dou
     const int h = M->h, nk = M->n[2];
     const double dx = M->d[0], dy = M->d[1], dz = M->d[2];
     const double *co = M->coef;
-    double *Up = (double *)malloc(sizeof(double) * 6 * nk);
-    double *Um = Up + nk, *Vp = Up + 2 * nk, *Vm = Up + 3 * nk, *Wp = Up + 4 * nk, *Wm = Up + 5 * nk;
     memset(out, 0, sizeof(double) * nc * npts(M));
 #define F(i, j, k, c) f[IDX(M, i, j, k) * nc + (c)]
+#pragma omp parallel
+    {
+    double *Up = (double *)malloc(sizeof(double) * 6 * nk);
+    double *Um = Up + nk, *Vp = Up + 2 * nk, *Vm = Up + 3 * nk, *Wp = Up + 4 * nk, *Wm = Up + 5 * nk;
     for (int l = 0; l < h; l++)
+#pragma omp for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++) {
                 double *dp = out + IDX(M, i, j, 0) * nc;
@@ -375,8 +390,9 @@ void orc_div_vf(const orc_mesh *M, const double *U, const double *f, int nc, dou
                                            - f0 * (co[l] / 2.0 / (l + 1) / dz * Wm[k]) / M->dzdxi[k]);
                     }
             }
-#undef F
     free(Up);
+    }
+#undef F
 }
 
 /* ex::laplacian(scalar nu, Field<T>) incl. the stretched-z correction
@@ -389,6 +405,7 @@ void orc_lap(const orc_mesh *M, double nu, const double *f, int nc, double *out)
     memset(out, 0, sizeof(double) * nc * npts(M));
 #define F(i, j, k, c) f[IDX(M, i, j, k) * nc + (c)]
     for (int l = 0; l < h; l++)
+#pragma omp parallel for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++) {
                 double *lp = out + IDX(M, i, j, 0) * nc;
@@ -407,6 +424,7 @@ void orc_lap(const orc_mesh *M, double nu, const double *f, int nc, double *out)
                 }
             }
     for (int l = 0; l < h; l++)
+#pragma omp parallel for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++) {
                 double *lp = out + IDX(M, i, j, 0) * nc;
@@ -437,6 +455,7 @@ void orc_div_t(const orc_mesh *M, const double *T, int symm, double *out)
     const double dx = M->d[0], dy = M->d[1], dz = M->d[2];
     const double *co = M->coef;
     memset(out, 0, sizeof(double) * 3 * npts(M));
+#pragma omp parallel for schedule(static)
     for (int i = h; i < M->n[0] - h; i++)
         for (int j = h; j < M->n[1] - h; j++)
             for (int k = h; k < M->n[2] - h; k++) {
@@ -462,6 +481,7 @@ void orc_div_sT(const orc_mesh *M, const double *s, const double *T, double *out
     memset(out, 0, sizeof(double) * 3 * npts(M));
 #define SV(i, j, k) s[IDX(M, i, j, k)]
 #define TV(i, j, k, r) T[IDX(M, i, j, k) * 9 + (r)]
+#pragma omp parallel for schedule(static)
     for (int i = h; i < M->n[0] - h; i++)
         for (int j = h; j < M->n[1] - h; j++)
             for (int k = h; k < M->n[2] - h; k++) {
@@ -491,6 +511,7 @@ void orc_lap_f(const orc_mesh *M, const double *nu, const double *f, int nc, dou
 #define F(i, j, k, c) f[IDX(M, i, j, k) * nc + (c)]
 #define NU(i, j, k) nu[IDX(M, i, j, k)]
     for (int l = 0; l < h; l++)
+#pragma omp parallel for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++) {
                 double *lp = out + IDX(M, i, j, 0) * nc;
@@ -511,6 +532,7 @@ void orc_lap_f(const orc_mesh *M, const double *nu, const double *f, int nc, dou
                 }
             }
     for (int l = 0; l < h; l++)
+#pragma omp parallel for schedule(static)
         for (int i = h; i < M->n[0] - h; i++)
             for (int j = h; j < M->n[1] - h; j++) {
                 double *lp = out + IDX(M, i, j, 0) * nc;
@@ -548,10 +570,11 @@ void orc_poisson_k2(const orc_mesh *M, double *k2)
     const int ni = M->N[0], nj = M->N[1], nk = M->N[2];
     const double eps = 1.0e-16, pi = M_PI;
     const double *co = M->coef;
-    long l = 0;
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < nk; k++)
         for (int j = 0; j < nj; j++)
             for (int i = 0; i < ni; i++) {
+                const long l = ((long)k * nj + j) * ni + i;
                 double kx, ky, kz;
                 if (2 * (i) < M->N[0])
                     kx = 2.0 * pi * (i) / M->L[0];
@@ -572,7 +595,7 @@ void orc_poisson_k2(const orc_mesh *M, double *k2)
                 if (kz > eps)
                     for (int ll = 0; ll < M->h; ll++)
                         kpz += kz * co[ll] / (ll + 1) * sin((ll + 1) * kz * M->d[2]) / (kz * M->d[2]);
-                k2[l++] = kpx * kpx + kpy * kpy + kpz * kpz;
+                k2[l] = kpx * kpx + kpy * kpy + kpz * kpz;
             }
 }
 
@@ -595,6 +618,7 @@ void orc_poisson_solve(const orc_mesh *M, const double *rhs, double *p)
             }
     orc_fft3d(M->N, phi, -1);
     const double eps = 1.0e-16;
+#pragma omp parallel for schedule(static)
     for (l = 0; l < tot; l++) {
         if (k2[l] < eps) {
             phi[l].re = 0.0;
@@ -621,20 +645,137 @@ void orc_poisson_solve(const orc_mesh *M, const double *rhs, double *p)
 
 /* -------------------------------------------------------- time advance -- */
 
-static double ek_mean(const orc_mesh *M, const double *U)
+/* one component of a vector field as a scalar field, ghosts included */
+static void component(const orc_mesh *M, const double *U, int c, double *out)
 {
-    /* app/TG_Piosson/TG.cpp:148-166: unique nodes only */
+    const long n = npts(M);
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < n; q++) out[q] = U[3 * q + c];
+}
+
+/* the central curl of U from grad(scalar) of its components (src/ex/grad/grad.cpp:25-62
+ * applied to U.x, U.y, U.z); g: 9*npts scratch (grad of component c at 3*c) */
+static void central_curl(const orc_mesh *M, const double *U, double *s, double *g, double *w)
+{
+    const long n = npts(M);
+    for (int c = 0; c < 3; c++) {
+        component(M, U, c, s);
+        orc_grad_s(M, s, g + 3 * n * c);
+    }
+    const double *gu = g, *gv = g + 3 * n, *gw = g + 6 * n;
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < n; q++) {
+        w[3 * q + 0] = gw[3 * q + 1] - gv[3 * q + 2]; /* dw/dy - dv/dz */
+        w[3 * q + 1] = gu[3 * q + 2] - gw[3 * q + 0]; /* du/dz - dw/dx */
+        w[3 * q + 2] = gv[3 * q + 0] - gu[3 * q + 1]; /* dv/dx - du/dy */
+    }
+}
+
+/* mean of 1/2 |w|^2 over the unique nodes, summed in the order of the apps' energy loops */
+static double half_sq_mean(const orc_mesh *M, const double *w)
+{
     const int h = M->h;
-    double Ek = 0.0;
+    double e = 0.0;
     int n = 0;
     for (int i = h; i < M->n[0] - h - 1; i++)
         for (int j = h; j < M->n[1] - h - 1; j++)
             for (int k = h; k < M->n[2] - h - 1; k++) {
-                const double *u = U + IDX(M, i, j, k) * 3;
-                Ek += 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+                const double *v = w + IDX(M, i, j, k) * 3;
+                e += 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
                 n++;
             }
-    return Ek / n;
+    return e / n;
+}
+
+/* One history row: the diagnostics of app/OT_Poisson/OT.cpp:132-176 (Ek, Em,
+ * Jav, Jmax, omega, epsilon and Umax over the unique nodes, in its loop
+ * order; J = ex::curl(B), omega from ex::curl(U) -- the Q1 stencil of
+ * grad(vector) -- and epsilon = -mu omega^2 - eta Jav^2 from the means),
+ * tools::CFL (src/Tools/Tools.cpp:9-41: cfl_y and cfl_z take std::max with
+ * cfl_x, and keep only the last node's value), tools::maximum of div U and
+ * div B (app/TG_Piosson/RKLoop.H:42-51, app/OT_Poisson/BEqn.H:46-54), plus
+ * 1/2 <|curl U|^2> and 1/2 <|curl B|^2> with the central 6th-order curl. */
+static void diag_row(const orc_mesh *M, const orc_run_desc *rd, int step, double t, const double *U,
+                     const double *B, double *row, double *w1, double *w2, double *g9, double *s)
+{
+    const int h = M->h;
+    const int mhd = rd->model == 1;
+    const double mu = rd->nu, eta = mhd ? rd->eta : 0.0;
+    row[0] = step + 1;
+    row[1] = t;
+    orc_curl(M, U, w1); /* omegav = ex::curl(U) */
+    if (mhd) orc_curl(M, B, w2); else memset(w2, 0, sizeof(double) * 3 * npts(M)); /* J = ex::curl(B) */
+    double Ek = 0.0, Em = 0.0, Jmax = 0.0, Umax = 0.0, Jav = 0.0, omega = 0.0;
+    int n = 0;
+    for (int i = h; i < M->n[0] - h - 1; i++)
+        for (int j = h; j < M->n[1] - h - 1; j++)
+            for (int k = h; k < M->n[2] - h - 1; k++) {
+                const long p = IDX(M, i, j, k) * 3;
+                const double *u = U + p, *J = w2 + p, *o = w1 + p;
+                Ek += 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+                if (mhd) {
+                    const double *b = B + p;
+                    Em += 0.5 * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+                }
+                const double jm = sqrt(J[0] * J[0] + J[1] * J[1] + J[2] * J[2]);
+                Jmax = Jmax < jm ? jm : Jmax; /* std::max(Jmax, .) */
+                const double um = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+                Umax = Umax < um ? um : Umax;
+                omega += sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+                Jav += sqrt(J[0] * J[0] + J[1] * J[1] + J[2] * J[2]);
+                n++;
+            }
+    Ek /= n;
+    Em /= n;
+    Jav /= n;
+    omega /= n;
+    row[2] = Ek;
+    row[3] = Em;
+    row[6] = omega;
+    row[7] = Jav;
+    row[8] = Jmax;
+    row[9] = -mu * (omega * omega) - eta * (Jav * Jav);
+    row[10] = Umax;
+    /* tools::CFL over [m/2, n - m/2) (duplicate nodes included) */
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+    for (int i = h; i < M->n[0] - h; i++)
+        for (int j = h; j < M->n[1] - h; j++)
+            for (int k = h; k < M->n[2] - h; k++) {
+                const double *u = U + IDX(M, i, j, k) * 3;
+                const double vx = u[0] * rd->dt / M->d[0], vy = u[1] * rd->dt / M->d[1], vz = u[2] * rd->dt / M->d[2];
+                cx = cx < vx ? vx : cx;
+                cy = cx < vy ? vy : cx;
+                cz = cx < vz ? vz : cx;
+            }
+    row[11] = cx;
+    row[12] = cy;
+    row[13] = cz;
+    orc_div_v(M, U, s);
+    row[4] = orc_maximum(M, s);
+    if (mhd) {
+        orc_div_v(M, B, s);
+        row[5] = orc_maximum(M, s);
+    } else {
+        row[5] = 0.0;
+    }
+    central_curl(M, U, s, g9, w1);
+    row[14] = half_sq_mean(M, w1);
+    if (mhd) {
+        central_curl(M, B, s, g9, w1);
+        row[15] = half_sq_mean(M, w1);
+    } else {
+        row[15] = 0.0;
+    }
+}
+
+void orc_diag_row(const orc_mesh *M, const orc_run_desc *rd, int step, double t, const double *U, const double *B,
+                  double *row)
+{
+    const long n = npts(M);
+    double *mem = (double *)calloc((size_t)(n * 16), sizeof(double));
+    if (!mem) return;
+    diag_row(M, rd, step, t, U, B, row, mem, mem + 3 * n, mem + 6 * n, mem + 15 * n);
+    free(mem);
 }
 
 /* one evaluation of dt*(RHS) of app/TG_Piosson/RKLoop.H:17-22 (model 0) or
@@ -646,18 +787,23 @@ static void u_rhs(const orc_mesh *M, const orc_run_desc *rd, const double *U, co
     const long n = npts(M);
     orc_div_vf(M, U, U, 3, t1);                               /* ex::div(U,U) */
     orc_lap(M, rd->nu, U, 3, t2);                             /* ex::laplacian(mu,U) */
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < 3 * n; q++) dU[q] = -t1[q] + t2[q];  /* -a + b */
     if (rd->model == 1) {
         orc_div_vf(M, B, B, 3, t1);                           /* + ex::div(B,B) */
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < 3 * n; q++) dU[q] = dU[q] + t1[q];
+#pragma omp parallel for schedule(static)
         for (long p = 0; p < n; p++) {                        /* 0.5*(B&B) */
             const double *b = B + 3 * p;
             s1[p] = (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * 0.5;
         }
         orc_grad_s(M, s1, t1);                                /* - ex::grad(...) */
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < 3 * n; q++) dU[q] = dU[q] - t1[q];
     }
     (void)s2;
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < 3 * n; q++) dU[q] = dU[q] * rd->dt; /* time.dt() * (...) */
 }
 
@@ -668,10 +814,25 @@ static void b_rhs(const orc_mesh *M, const orc_run_desc *rd, const double *U, co
     const long n = npts(M);
     orc_div_vf(M, U, B, 3, t1);
     orc_div_vf(M, B, U, 3, t2);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < 3 * n; q++) dB[q] = -t1[q] + t2[q];
     orc_lap(M, rd->eta, B, 3, t1);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < 3 * n; q++) dB[q] = (dB[q] + t1[q]) * rd->dt;
 }
+
+/* x[q] = x[q] + y[q] * a */
+static void axpy_(long n, double *x, const double *y, double a)
+{
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < n; q++) x[q] = x[q] + y[q] * a;
+}
+
+/* app/shearLayer/UEqn.H:14-38: RK4 weights used as stage coefficients,
+ * Ustar = UOld + RK4[rk]*dU with the stage state U refreshed by a projection
+ * after every stage (rhs div(Ustar)/dt/RK4c[rk], correction RK4c[rk]*dt*grad p) */
+static const double RK4W[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0}; /* shearLayer.cpp:164 */
+static const double RK4C[4] = {0.5, 0.5, 1.0, 1.0};                         /* settings::RK4c_ */
 
 int orc_run(const orc_mesh *M, const orc_run_desc *rd, double *U, double *B, double *p,
             double *pB, double *hist)
@@ -688,13 +849,32 @@ int orc_run(const orc_mesh *M, const orc_run_desc *rd, double *U, double *B, dou
     double t = 0.0;
     for (int step = 0; step < rd->nsteps; step++) {
         t += rd->dt;
+        if (rd->rk_mode == 2) {
+            /* ---- U equation: app/shearLayer/UEqn.H:1-54 (B frozen, BEqn.H not included) ---- */
+            memcpy(UOld, U, sizeof(double) * v);
+            for (int rk = 0; rk < 4; rk++) {
+                u_rhs(M, rd, U, B, dU[0], t1, t2, s1, s2);
+                memcpy(Ustar, UOld, sizeof(double) * v);
+                axpy_(v, Ustar, dU[0], RK4W[rk]);
+                orc_bc_apply(M, Ustar, 3, rd->bcU_type, rd->bcU_val);
+                orc_div_v(M, Ustar, s3);
+#pragma omp parallel for schedule(static)
+                for (long q = 0; q < n; q++) s3[q] = s3[q] / rd->dt / RK4C[rk];
+                orc_poisson_solve(M, s3, p);
+                orc_bc_apply(M, p, 1, rd->bcp_type, rd->bcp_val);
+                orc_grad_s(M, p, t1);
+                const double cs = RK4C[rk] * rd->dt;
+#pragma omp parallel for schedule(static)
+                for (long q = 0; q < v; q++) U[q] = Ustar[q] - cs * t1[q];
+                orc_bc_apply(M, U, 3, rd->bcU_type, rd->bcU_val);
+            }
+        } else {
         /* ---- U equation: app/TG_Piosson/RKLoop.H:1-38, app/OT_Poisson/UEqn.H:1-39 ---- */
         memcpy(UOld, U, sizeof(double) * v);
         for (int rk = 0; rk < 4; rk++) {
             u_rhs(M, rd, U, B, dU[rk], t1, t2, s1, s2);
             memcpy(Ustar, UOld, sizeof(double) * v);
-            for (int j = 0; j <= rk; j++)
-                for (long q = 0; q < v; q++) Ustar[q] = Ustar[q] + dU[j][q] * RK4A[rk][j];
+            for (int j = 0; j <= rk; j++) axpy_(v, Ustar, dU[j], RK4A[rk][j]);
             if (rd->rk_mode == 1) {
                 /* classical RK4: the stage state is refreshed, as the reference's own B loop does */
                 memcpy(U, Ustar, sizeof(double) * v);
@@ -703,10 +883,12 @@ int orc_run(const orc_mesh *M, const orc_run_desc *rd, double *U, double *B, dou
         }
         orc_bc_apply(M, Ustar, 3, rd->bcU_type, rd->bcU_val);
         orc_div_v(M, Ustar, s3);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < n; q++) s3[q] = s3[q] / rd->dt;
         orc_poisson_solve(M, s3, p);
         orc_bc_apply(M, p, 1, rd->bcp_type, rd->bcp_val);
         orc_grad_s(M, p, t1);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < v; q++) U[q] = Ustar[q] - t1[q] * rd->dt;
         orc_bc_apply(M, U, 3, rd->bcU_type, rd->bcU_val);
 
@@ -716,8 +898,7 @@ int orc_run(const orc_mesh *M, const orc_run_desc *rd, double *U, double *B, dou
             for (int rk = 0; rk < 4; rk++) {
                 b_rhs(M, rd, U, B, dU[rk], t1, t2);
                 memcpy(Bstar, Bold, sizeof(double) * v);
-                for (int j = 0; j <= rk; j++)
-                    for (long q = 0; q < v; q++) Bstar[q] = Bstar[q] + dU[j][q] * RK4A[rk][j];
+                for (int j = 0; j <= rk; j++) axpy_(v, Bstar, dU[j], RK4A[rk][j]);
                 memcpy(B, Bstar, sizeof(double) * v);
                 orc_bc_apply(M, B, 3, rd->bcB_type, rd->bcB_val);
             }
@@ -725,24 +906,16 @@ int orc_run(const orc_mesh *M, const orc_run_desc *rd, double *U, double *B, dou
             orc_poisson_solve(M, s3, pB);
             orc_bc_apply(M, pB, 1, rd->bcpB_type, rd->bcpB_val);
             orc_grad_s(M, pB, t3);
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < v; q++) B[q] -= t3[q];
             orc_bc_apply(M, B, 3, rd->bcB_type, rd->bcB_val);
         }
+        }
 
         if (hist && rd->diag_every > 0 && ((step + 1) % rd->diag_every == 0 || step + 1 == rd->nsteps)) {
-            double *row = hist + (long)step * ORC_HIST_COLS;
-            row[0] = step + 1;
-            row[1] = t;
-            row[2] = ek_mean(M, U);
-            row[3] = (rd->model == 1) ? ek_mean(M, B) : 0.0;
-            orc_div_v(M, U, s4);
-            row[4] = orc_maximum(M, s4);
-            if (rd->model == 1) {
-                orc_div_v(M, B, s4);
-                row[5] = orc_maximum(M, s4);
-            } else {
-                row[5] = 0.0;
-            }
+            /* dU[0..3] (4 vector fields, 12 npts) and s4 serve as the row's scratch */
+            diag_row(M, rd, step, t, U, (rd->model == 1) ? B : NULL, hist + (long)step * ORC_HIST_COLS, dU[0], dU[1],
+                     dU[2], s4);
         }
     }
     free(mem);

@@ -57,7 +57,9 @@ void orc_poisson_k2(const orc_mesh *mesh, double *k2);
 
 typedef struct {
     int model;      /* 0 = incompressible NS (TG_Piosson), 1 = incompressible MHD (OT_Poisson) */
-    int rk_mode;    /* 0 = literal reference loop, 1 = classical RK4 (U refreshed per stage) */
+    int rk_mode;    /* 0 = literal reference loop, 1 = classical RK4 (U refreshed per stage),
+                       2 = app/shearLayer/UEqn.H (RK4 weights as stage coefficients, a projection
+                       per stage; with model 1 the B terms enter the U loop and B stays frozen) */
     int nsteps;
     int diag_every; /* write a history row every diag_every steps (0 = never) */
     double dt, nu, eta;
@@ -71,11 +73,17 @@ typedef struct {
     double bcpB_val[6];
 } orc_run_desc;
 
-#define ORC_HIST_COLS 6 /* step, t, Ek, Em, max|div U|, max|div B| */
+/* History row: 0 step, 1 t, 2 Ek, 3 Em, 4 max|div U|, 5 max|div B|, 6 omega = mean|ex::curl(U)|,
+ * 7 Jav = mean|ex::curl(B)|, 8 Jmax, 9 epsilon = -nu omega^2 - eta Jav^2, 10 Umax,
+ * 11-13 tools::CFL x, y, z, 14 1/2<|curl U|^2>, 15 1/2<|curl B|^2> (central curl) */
+#define ORC_HIST_COLS 16
 
 /* Advance U (and B) by nsteps; p/pB hold the last pressures. hist: nsteps rows. */
 int orc_run(const orc_mesh *mesh, const orc_run_desc *rd, double *U, double *B,
             double *p, double *pB, double *hist);
+/* one history row of the state (U, B ghost-filled; B NULL for model 0) after step+1 steps at time t */
+void orc_diag_row(const orc_mesh *mesh, const orc_run_desc *rd, int step, double t, const double *U,
+                  const double *B, double *row);
 
 #ifdef __cplusplus
 }

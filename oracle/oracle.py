@@ -28,7 +28,8 @@ REF_BIN = os.path.join(HERE, "_ref", "nova_ref")
 PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
 # src/BC/BCenums.h:8
 FACES = ("north", "south", "east", "west", "top", "bottom")
-HIST_COLS = 6
+# history row columns (nova_oracle.h ORC_HIST_COLS)
+HIST_COLS = 16
 
 
 class RunDesc(C.Structure):
@@ -78,6 +79,8 @@ def lib():
         L.orc_poisson_k2.argtypes = [C.c_void_p, dp]
         L.orc_run.restype = C.c_int
         L.orc_run.argtypes = [C.c_void_p, C.POINTER(RunDesc), dp, dp, dp, dp, dp]
+        L.orc_diag_row.restype = None
+        L.orc_diag_row.argtypes = [C.c_void_p, C.POINTER(RunDesc), C.c_int, C.c_double, dp, C.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -248,10 +251,11 @@ def poisson_k2(mesh):
 def run(mesh, U, B=None, *, model="ns", rk_mode="classical", nsteps=1, dt=0.01, nu=0.0, eta=0.0,
         diag_every=1, bcU=None, bcp=None, bcB=None, bcpB=None):
     """Advance ghosted U (and B) in place by nsteps with the restated loop bodies.
-    Returns (U, B, p, pB, hist[nsteps, 6])."""
+    rk_mode: "literal", "classical" or "shear" (app/shearLayer/UEqn.H).
+    Returns (U, B, p, pB, hist[nsteps, HIST_COLS])."""
     rd = RunDesc()
     rd.model = 1 if model == "mhd" else 0
-    rd.rk_mode = 1 if rk_mode == "classical" else 0
+    rd.rk_mode = {"literal": 0, "classical": 1, "shear": 2}[rk_mode]
     rd.nsteps = nsteps
     rd.diag_every = diag_every
     rd.dt, rd.nu, rd.eta = dt, nu, eta
@@ -271,6 +275,18 @@ def run(mesh, U, B=None, *, model="ns", rk_mode="classical", nsteps=1, dt=0.01, 
     if rc != 0:
         raise RuntimeError("orc_run failed")
     return U, B, p, pB, hist
+
+
+def diag_row(mesh, U, B=None, *, model="ns", dt=0.01, nu=0.0, eta=0.0, step=0, t=0.0):
+    """One history row (nova_oracle.h ORC_HIST_COLS) of ghosted U (and B for "mhd")."""
+    rd = RunDesc()
+    rd.model = 1 if model == "mhd" else 0
+    rd.dt, rd.nu, rd.eta = dt, nu, eta
+    U = np.ascontiguousarray(U, np.float64)
+    Bc = None if B is None else np.ascontiguousarray(B, np.float64)
+    row = np.zeros(HIST_COLS)
+    lib().orc_diag_row(mesh._p, C.byref(rd), int(step), float(t), U, None if Bc is None else Bc.ctypes.data, row)
+    return row
 
 
 # ------------------------------------------------------ reference in place --
@@ -402,7 +418,7 @@ def wc_run(mesh, U, rho, p, T=None, *, order="shear", nsteps=1, dt=0.01, mu=0.0,
     order "tg":    app/TG/TG.cpp:73-75, rhoEqn.H, pEqn.H (p = 50 rho^2), UEqn.H;
     order "shear": app/shearLayerWC/shearLayer.cpp:197-200, UEqn.H (with buoyancy),
                    rhoEqn.H, pEqn.H (p = c^2/(2 rho0) rho^2), TEqn.H.
-    Returns (U, rho, p, T, hist[nsteps, 6]) with hist rows (step, t, Ek, 0, max|div U|, 0)."""
+    Returns (U, rho, p, T, hist[nsteps, HIST_COLS]) with hist rows (step, t, Ek, 0, max|div U|, 0, 0...)."""
     bc = bc or {}
     U = bc_apply(mesh, np.array(U, np.float64), bc.get("U"))
     rho = bc_apply(mesh, np.array(rho, np.float64), bc.get("rho"))
@@ -425,7 +441,7 @@ def wc_run(mesh, U, rho, p, T=None, *, order="shear", nsteps=1, dt=0.01, mu=0.0,
         ek = 0.0
         for v in (0.5 * (u[..., 0] * u[..., 0] + u[..., 1] * u[..., 1] + u[..., 2] * u[..., 2])).ravel():
             ek += v
-        hist[step] = (step + 1, (step + 1) * dt, ek / u[..., 0].size, 0.0, maximum(mesh, div_v(mesh, U)), 0.0)
+        hist[step, :6] = (step + 1, (step + 1) * dt, ek / u[..., 0].size, 0.0, maximum(mesh, div_v(mesh, U)), 0.0)
     return U, rho, p, T, hist
 
 
@@ -470,7 +486,8 @@ def ref_wc_run(mesh, U, rho, p, T=None, *, order="shear", nsteps=1, dt=0.01, mu=
                        check=True, stdout=subprocess.DEVNULL)
         r = tuple(np.fromfile("%s_%s.bin" % (out, k)).reshape(mesh.n + (nc,))
                   for k, nc in (("U", 3), ("rho", 1), ("p", 1), ("T", 1)))
-        hist = np.fromfile(out + "_hist.bin").reshape(nsteps, HIST_COLS)
+        hist = np.zeros((nsteps, HIST_COLS))
+        hist[:, :6] = np.fromfile(out + "_hist.bin").reshape(nsteps, 6)
     return r + (hist,)
 
 
@@ -696,6 +713,36 @@ def ic_mhd_jet(mesh, seed=1, noise=1e-3):
     e = 0.2 * np.exp(-r * r)  # B_theta / r
     B = np.stack([-e * Y, e * X, np.full_like(X, 0.5)])
     return U, B
+
+
+def ic_temporal_shear(mesh, seed=0, noise=1e-3, walls=True, delta=28.0):
+    """Temporal shear layer: u = tanh(delta (y - pi)), v = w = 0, plus seed-`seed`
+    Gaussian noise of amplitude `noise` on every component, on the stored nodes
+    (N1 + 1 rows when y is bounded by walls)."""
+    x, y, z = mesh.coords()
+    if walls:
+        y = mesh.origin[1] + np.arange(mesh.N[1] + 1) * mesh.d[1]
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    zero = np.zeros_like(X)
+    U = np.stack([np.tanh(delta * (Y - np.pi)), zero, zero])
+    return U + noise * np.random.default_rng(seed).standard_normal(U.shape)
+
+
+def ghosted_from_stored(mesh, U, spec=None):
+    """stored nodes (nc, N0, N1 + 1, N2) of a mesh with y walls -> the ghosted
+    reference layout with the BCs of `spec` applied"""
+    g = mesh.zeros(U.shape[0])
+    h = mesh.h
+    N = mesh.N
+    g[h:h + N[0], h:h + N[1] + 1, h:h + N[2]] = np.moveaxis(U, 0, -1)
+    return bc_apply(mesh, g, spec)
+
+
+def stored_of(mesh, g):
+    """ghosted -> the stored nodes of a mesh with y walls: (nc, N0, N1 + 1, N2)"""
+    h = mesh.h
+    u = g[h:h + mesh.N[0], h:h + mesh.N[1] + 1, h:h + mesh.N[2]]
+    return np.ascontiguousarray(np.moveaxis(u, -1, 0))
 
 
 def wc_shear_params(mach=0.1):

@@ -6,7 +6,7 @@
  * recursively and combined with an O(p^2) DFT butterfly.  Twiddles are read
  * from one table of exp(sign*2*pi*i*t/n) for the top-level n, built with
  * exact values on the axes, so sub-transforms index it with a stride.
- * Accuracy is checked against numpy.fft in tests/test_oracle_fft.py.
+ * Accuracy is checked against numpy.fft in tests/test_oracle.py.
  */
 #include "orc_fft.h"
 
@@ -101,17 +101,24 @@ static void fft_lines(int n, orc_cplx *base, long stride, long nlines,
 {
     if (n <= 1) return;
     orc_cplx *W = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
-    orc_cplx *in = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
-    orc_cplx *out = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
-    orc_cplx *scr = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
     for (int t = 0; t < n; t++) W[t] = twiddle(t, n, sign);
-    for (long L = 0; L < nlines; L++) {
-        orc_cplx *d = base + line_off[L];
-        for (int j = 0; j < n; j++) in[j] = d[(long)j * stride];
-        fft_rec(n, in, 1, out, W, n, 1, scr);
-        for (int j = 0; j < n; j++) d[(long)j * stride] = out[j];
+    /* lines are independent: with OpenMP each thread transforms its own lines
+     * with private buffers (identical arithmetic per line) */
+#pragma omp parallel
+    {
+        orc_cplx *in = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
+        orc_cplx *out = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
+        orc_cplx *scr = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
+#pragma omp for schedule(static)
+        for (long L = 0; L < nlines; L++) {
+            orc_cplx *d = base + line_off[L];
+            for (int j = 0; j < n; j++) in[j] = d[(long)j * stride];
+            fft_rec(n, in, 1, out, W, n, 1, scr);
+            for (int j = 0; j < n; j++) d[(long)j * stride] = out[j];
+        }
+        free(in); free(out); free(scr);
     }
-    free(W); free(in); free(out); free(scr);
+    free(W);
 }
 
 void orc_fft3d(const int n[3], orc_cplx *data, int sign)

@@ -4,11 +4,12 @@
  * Field, poisson objects exactly as app/TG_Piosson/TG.cpp and
  * app/OT_Poisson/OT.cpp do, then runs the reference's own loop bodies
  * (app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H) for the literal
- * mode, or the same loop with the stage state refreshed for the classical
- * RK4 mode.  I/O is raw little-endian float64 in the Field<T> layout; the wall
+ * mode, the same loop with the stage state refreshed for the classical RK4
+ * mode, or app/shearLayer/UEqn.H (shear mode).  Each step's history row is
+ * the diagnostics of app/OT_Poisson/OT.cpp:132-176 and tools::CFL.  I/O is raw little-endian float64 in the Field<T> layout; the wall
  * time of each step's loop body goes to <out>_time.txt, one line per step.
  *
- *   nova_ref run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U.bin> <B.bin|-> <out>
+ *   nova_ref run <case> <ns|mhd> <literal|classical|shear> <nsteps> <dt> <nu> <eta> <U.bin> <B.bin|-> <out>
  *   nova_ref ops <case> <nu> <U.bin> <s.bin> <out>
  *   nova_ref wc <case> <tg|shear> <nsteps> <dt> <mu> <ka> <c> <rho0> <gz> <U.bin> <rho.bin> <p.bin> <T.bin|-> <out>
  *   nova_ref wcinit <case> <c> <rho0> <gz> <T.bin> <out>
@@ -26,7 +27,10 @@
  * <case> holds `mesh` and the BC files (UBC, pBC, BBC, pBBC, rhoBC, TBC).
  */
 #include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <iostream>
+#include <sstream>
 #include <cstdlib>
 #include <memory>
 #include <string>
@@ -64,6 +68,101 @@ template <class T> static void save(const Field<T> &f, const std::string &path)
     std::fclose(fp);
 }
 
+/* tools::CFL (src/Tools/Tools.cpp:9-41) prints its three values; run it with
+ * std::cout redirected and at full precision, and read them back */
+static void cfl_of(const Field<vector> &U, const Mesh &mesh, double out[3])
+{
+    std::ostringstream os;
+    os.precision(17);
+    std::streambuf *old = std::cout.rdbuf(os.rdbuf());
+    const std::streamsize prec = std::cout.precision(17);
+    tools::CFL(U, mesh);
+    std::cout.precision(prec);
+    std::cout.rdbuf(old);
+    const std::string txt = os.str();
+    const char *keys[3] = {"CFL x:", "CFL y:", "CFL z:"};
+    for (int a = 0; a < 3; a++) {
+        const size_t at = txt.find(keys[a]);
+        out[a] = at == std::string::npos ? std::nan("") : std::strtod(txt.c_str() + at + 6, nullptr);
+    }
+}
+
+/* 1/2 <|curl V|^2> over the unique nodes with the central curl built from the
+ * reference's ex::grad of each component (the ghosts of V copied along) */
+static double central_enstrophy(Mesh &mesh, const Field<vector> &V)
+{
+    std::shared_ptr<Field<vector> > g[3];
+    for (int c = 0; c < 3; c++) {
+        Field<scalar> s(mesh, 0, "p");
+        for (int i = 0; i < mesh.ni(); i++)
+            for (int j = 0; j < mesh.nj(); j++)
+                for (int k = 0; k < mesh.nk(); k++) s(i, j, k) = V(i, j, k)[c];
+        g[c] = ex::grad(s);
+    }
+    scalar e = 0.0;
+    int n = 0;
+    for (int i = settings::m() / 2; i < mesh.ni() - settings::m() / 2 - 1; i++)
+        for (int j = settings::m() / 2; j < mesh.nj() - settings::m() / 2 - 1; j++)
+            for (int k = settings::m() / 2; k < mesh.nk() - settings::m() / 2 - 1; k++) {
+                const scalar wx = (*g[2])(i, j, k).y() - (*g[1])(i, j, k).z();
+                const scalar wy = (*g[0])(i, j, k).z() - (*g[2])(i, j, k).x();
+                const scalar wz = (*g[1])(i, j, k).x() - (*g[0])(i, j, k).y();
+                e += 0.5 * (wx * wx + wy * wy + wz * wz);
+                n++;
+            }
+    return e / n;
+}
+
+/* The history row of a step: the diagnostics loop of app/OT_Poisson/OT.cpp:132-176
+ * (omegav = ex::curl(U), J = ex::curl(B)), tools::CFL, tools::maximum of the
+ * divergences, and the central-curl enstrophies.  Columns as ORC_HIST_COLS. */
+static void hist_row(Mesh &mesh, const Time &time, int step, bool mhd, scalar mu, scalar eta,
+                     Field<vector> &U, Field<vector> &B, double row[16])
+{
+    for (int q = 0; q < 16; q++) row[q] = 0.0;
+    row[0] = double(step + 1);
+    row[1] = time.curTime();
+    auto omegav = ex::curl(U);
+    auto Jp = ex::curl(B);
+    const Field<vector> &J = *Jp;
+    scalar Ek = 0.0, Em = 0.0, Jmax = 0.0, Umax = 0.0, Jav = 0.0, omega = 0.0;
+    int n = 0;
+    for (int i = settings::m() / 2; i < mesh.ni() - settings::m() / 2 - 1; i++)
+        for (int j = settings::m() / 2; j < mesh.nj() - settings::m() / 2 - 1; j++)
+            for (int k = settings::m() / 2; k < mesh.nk() - settings::m() / 2 - 1; k++) {
+                Ek += 0.5 * (U(i, j, k).x() * U(i, j, k).x() + U(i, j, k).y() * U(i, j, k).y() + U(i, j, k).z() * U(i, j, k).z());
+                Em += 0.5 * (B(i, j, k).x() * B(i, j, k).x() + B(i, j, k).y() * B(i, j, k).y() + B(i, j, k).z() * B(i, j, k).z());
+                Jmax = std::max(Jmax, sqrt(J(i, j, k).x() * J(i, j, k).x() + J(i, j, k).y() * J(i, j, k).y() + J(i, j, k).z() * J(i, j, k).z()));
+                Umax = std::max(Umax, sqrt(U(i, j, k).x() * U(i, j, k).x() + U(i, j, k).y() * U(i, j, k).y() + U(i, j, k).z() * U(i, j, k).z()));
+                omega += sqrt((*omegav)(i, j, k).x() * (*omegav)(i, j, k).x() + (*omegav)(i, j, k).y() * (*omegav)(i, j, k).y()
+                              + (*omegav)(i, j, k).z() * (*omegav)(i, j, k).z());
+                Jav += sqrt(J(i, j, k).x() * J(i, j, k).x() + J(i, j, k).y() * J(i, j, k).y() + J(i, j, k).z() * J(i, j, k).z());
+                n++;
+            }
+    Ek /= n;
+    Em /= n;
+    Jav /= n;
+    omega /= n;
+    row[2] = Ek;
+    row[3] = mhd ? Em : 0.0;
+    row[6] = omega;
+    row[7] = Jav;
+    row[8] = Jmax;
+    row[9] = -mu * (omega * omega) - (mhd ? eta : 0.0) * (Jav * Jav);
+    row[10] = Umax;
+    cfl_of(U, mesh, row + 11);
+    {
+        auto d = ex::div(U);
+        row[4] = tools::maximum(d);
+    }
+    if (mhd) {
+        auto d = ex::div(B);
+        row[5] = tools::maximum(d);
+    }
+    row[14] = central_enstrophy(mesh, U);
+    if (mhd) row[15] = central_enstrophy(mesh, B);
+}
+
 /* app/TG_Piosson/TG.cpp:148-166 */
 static double ek_mean(const Mesh &mesh, const Field<vector> &U)
 {
@@ -81,10 +180,12 @@ static double ek_mean(const Mesh &mesh, const Field<vector> &U)
 
 static int run(int argc, char **argv)
 {
-    if (argc < 12) { std::fprintf(stderr, "usage: run <case> <ns|mhd> <literal|classical> <nsteps> <dt> <nu> <eta> <U> <B|-> <out>\n"); return 2; }
+    if (argc < 12) { std::fprintf(stderr, "usage: run <case> <ns|mhd> <literal|classical|shear> <nsteps> <dt> <nu> <eta> <U> <B|-> <out>\n"); return 2; }
     settings::zoneName() = argv[2];
     const bool mhd = std::string(argv[3]) == "mhd";
     const bool classical = std::string(argv[4]) == "classical";
+    const bool shear = std::string(argv[4]) == "shear";
+    scalar RK4[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0}; /* app/shearLayer/shearLayer.cpp:164 */
     const int nsteps = std::atoi(argv[5]);
     const double dt = std::atof(argv[6]);
     const scalar mu = std::atof(argv[7]);
@@ -121,7 +222,11 @@ static int run(int argc, char **argv)
     for (int step = 0; step < nsteps; step++) {
         const auto t0 = std::chrono::steady_clock::now();
         time++;
-        if (!mhd && !classical) {
+        if (shear) {
+            /* app/shearLayer: the U loop only (BEqn.H is not included there), B frozen; with
+             * the ns model B stays zero and its terms add zeros */
+#include "shearLayer/UEqn.H"
+        } else if (!mhd && !classical) {
 #include "TG_Piosson/RKLoop.H"
         } else if (mhd && !classical) {
 #include "OT_Poisson/UEqn.H"
@@ -157,16 +262,9 @@ static int run(int argc, char **argv)
             }
         }
         step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
-        double row[6] = {double(step + 1), time.curTime(), ek_mean(mesh, U), mhd ? ek_mean(mesh, B) : 0.0, 0.0, 0.0};
-        {
-            auto d = ex::div(U);
-            row[4] = tools::maximum(d);
-        }
-        if (mhd) {
-            auto d = ex::div(B);
-            row[5] = tools::maximum(d);
-        }
-        hist.insert(hist.end(), row, row + 6);
+        double row[16];
+        hist_row(mesh, time, step, mhd, mu, eta, U, B, row);
+        hist.insert(hist.end(), row, row + 16);
     }
 
     save(U, out + "_U.bin");

@@ -2,7 +2,9 @@
 
 Runs oracle/_ref/nova_ref -- the reference's own sources (src/ex, src/poisson,
 src/BC, src/Field, src/im, app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H +
-BEqn.H, the compressible app/TG and app/shearLayerWC loop bodies)
+BEqn.H, app/shearLayer/UEqn.H, the compressible app/TG and app/shearLayerWC
+loop bodies, and the per-step diagnostics of app/OT_Poisson/OT.cpp with
+tools::CFL)
 compiled in place by `make -C oracle ref` -- on small seeded inputs and stores
 inputs and outputs as .npz.  Needs the reference tree (only present where the
 fixtures are generated); the tests only read the .npz files.
@@ -54,6 +56,24 @@ def run_case(name, N, model, rk_mode, nsteps, dt, nu, eta, L=None):
         res["B"] = M.unique(r[1])
         res["pB"] = M.unique(r[3])
     np.savez_compressed(os.path.join(HERE, name), **res)
+
+
+# the wall BCs of the temporal shear layer: u, w Neumann-0 and v Dirichlet-0 on
+# the y walls, p Neumann-0
+SHEAR_BC = {"U": {"north": [(1, 0.0), (2, 0.0), (1, 0.0)], "south": [(1, 0.0), (2, 0.0), (1, 0.0)]},
+            "p": {"north": (1, 0.0), "south": (1, 0.0)}}
+
+
+def shear_case(name, N, L, nsteps, dt, nu, seed=0):
+    """app/shearLayer/UEqn.H (RK4 weights as stage coefficients, a projection per
+    stage) on a mesh with y walls, the temporal shear layer's initial field"""
+    M = O.Mesh(N, L=L)
+    U = O.ic_temporal_shear(M, seed=seed, noise=1e-2, delta=2.0)
+    Ug = O.ghosted_from_stored(M, U, SHEAR_BC["U"])
+    r = O.ref_run(M, Ug, model="ns", rk_mode="shear", nsteps=nsteps, dt=dt, nu=nu, bc=SHEAR_BC)
+    np.savez_compressed(os.path.join(HERE, name), N=np.array(N), L=np.array(L), nsteps=np.array(nsteps),
+                        dt=np.array(dt), nu=np.array(nu), U0=U, U=O.stored_of(M, r[0]), p=O.stored_of(M, r[2]),
+                        hist=r[4])
 
 
 def wc_tg_case(name, N, nsteps, dt, mu):
@@ -168,6 +188,9 @@ CASES = {
     "tg_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "ns", "literal", 6, 0.05, 1 / 1600, 0.0),
     "ot_12_classical.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "classical", 4, 0.01, 1e-3, 1e-3),
     "ot_12_literal.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "literal", 4, 0.01, 1e-3, 1e-3),
+    "tg_12_shear.npz": lambda n: run_case(n, (12, 12, 12), "ns", "shear", 6, 0.05, 1 / 1600, 0.0),
+    "ot_12_shear.npz": lambda n: run_case(n, (12, 12, 12), "mhd", "shear", 4, 0.01, 1e-3, 1e-3),
+    "shear_walls_12x10x8.npz": lambda n: shear_case(n, (12, 10, 8), (2 * np.pi, 2 * np.pi, np.pi), 6, 0.01, 1e-2),
     "wc_tg_12.npz": lambda n: wc_tg_case(n, (12, 12, 12), 5, 0.02, 1 / 1600),
     "wc_shear_12x8x16.npz": lambda n: wc_shear_case(n, (12, 8, 16), 4),
     "ops2_7x6x5.npz": lambda n: ops2_case(n, (7, 6, 5), (2.0, 1.5, 3.0), 13),

@@ -1,0 +1,128 @@
+"""GPU runs at the benchmark configurations' own sizes.
+
+FP64 parity against the oracle (the reference's algorithm restated bit for
+bit, run here on the host's cores) with every history column overlaid step
+by step:
+  * Taylor-Green 64^3, 100 steps, nu = 1/1600, dt from CFL 0.3 on the initial
+    field, in the classical and the literal (app/TG_Piosson/RKLoop.H as
+    written) modes: relative L2 <= 1e-11 per field;
+  * Orszag-Tang MHD 128^3, 20 steps, nu = eta = 1/1000, CFL 0.3 on |u| + |B|,
+    literal (app/OT_Poisson as written) and classical.
+FP32-split error statements against the FP64 GPU path at full size:
+  * the temporal shear layer 256 x 256 x 128 with y walls (DCT Poisson), the
+    shear-layer loop of app/shearLayer/UEqn.H, 500 steps;
+  * the MHD jet 192 x 192 x 384, 200 steps (t = 200 dt, dt from CFL 0.3).
+"""
+import numpy as np
+import pytest
+
+from conftest import check_history, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-11
+
+
+@pytest.fixture(scope="module")
+def nova():
+    from novaclone_b200 import nova
+    return nova
+
+
+def run_gpu(nova, GM, U0, B0=None, precision=0, bcU=None, bcp=None, **kw):
+    def field(nc, prec, spec=None):
+        f = nova.Field(GM, nc, prec)
+        if spec:
+            from oracle import oracle as O
+            t, v = O.bc_arrays(nc, spec)
+            f.set_bc(list(t) + [0] * (18 - len(t)), list(v) + [0.0] * (18 - len(v)))
+        return f
+    U = field(3, precision, bcU).upload_soa(U0)
+    p = field(1, nova.F64, bcp)
+    B = pB = None
+    if B0 is not None:
+        B = field(3, precision).upload_soa(B0)
+        pB = field(1, nova.F64)
+    nsteps = kw.pop("nsteps")
+    hist = nova.advance(GM, nova.run_desc(precision=precision, **kw), U, p, B, pB, nsteps=nsteps)
+    out = {"U": U.download_soa(), "p": p.download_soa(), "hist": hist}
+    if B is not None:
+        out["B"] = B.download_soa()
+    return out
+
+
+def compare_fields(got, ref, names):
+    for f in names:
+        for c in range(ref[f].shape[0]):
+            if np.abs(ref[f][c]).max() > 1e-8:
+                e = rel_l2(got[f][c], ref[f][c])
+                assert e < TOL64, (f, c, e)
+
+
+@pytest.mark.parametrize("rk_mode", ["classical", "literal"])
+def test_taylor_green_64_100_steps_vs_oracle(nova, oracle, rk_mode):
+    OM = oracle.Mesh((64, 64, 64))
+    U0 = oracle.ic_taylor_green(OM)
+    dt = oracle.cfl_dt(OM, [U0])
+    kw = dict(model="ns", rk_mode=rk_mode, nsteps=100, dt=dt, nu=1 / 1600)
+    g = run_gpu(nova, nova.Mesh(OM.N), U0, **kw)
+    r = oracle.run(OM, OM.to_ghosted(U0), **kw)
+    o = {"U": OM.unique(r[0]), "p": OM.unique(r[2])}
+    compare_fields(g, o, ("U", "p"))
+    check_history(g["hist"], r[4])
+    assert g["hist"][-1, 2] < g["hist"][0, 2]  # the kinetic energy decays
+
+
+@pytest.mark.parametrize("rk_mode", ["literal", "classical"])
+def test_orszag_tang_128_20_steps_vs_oracle(nova, oracle, rk_mode):
+    OM = oracle.Mesh((128, 128, 128))
+    U0, B0 = oracle.ic_orszag_tang(OM)
+    dt = oracle.cfl_dt(OM, [U0, B0])
+    kw = dict(model="mhd", rk_mode=rk_mode, nsteps=20, dt=dt, nu=1e-3, eta=1e-3)
+    g = run_gpu(nova, nova.Mesh(OM.N), U0, B0, **kw)
+    r = oracle.run(OM, OM.to_ghosted(U0), OM.to_ghosted(B0), **kw)
+    o = {"U": OM.unique(r[0]), "B": OM.unique(r[1]), "p": OM.unique(r[2])}
+    compare_fields(g, o, ("U", "B", "p"))
+    check_history(g["hist"], r[4])
+
+
+# u, w Neumann-0 and v Dirichlet-0 on the y walls; p Neumann-0
+SHEAR_UBC = {"north": [(1, 0.0), (2, 0.0), (1, 0.0)], "south": [(1, 0.0), (2, 0.0), (1, 0.0)]}
+SHEAR_PBC = {"north": (1, 0.0), "south": (1, 0.0)}
+
+
+def test_shear_layer_256x256x128_500_steps_split_vs_fp64(nova, oracle):
+    """u = tanh(28 (y - pi)) + seed-0 noise 1e-3, nu = 1/2000, y walls with the DCT
+    Poisson, x in [0, 2 pi), z in [0, pi) (isotropic spacing 2 pi/256), the
+    shear-layer loop, 500 steps at CFL 0.3: FP32-split against FP64."""
+    N = (256, 256, 128)
+    L = (2 * np.pi, 2 * np.pi, np.pi)
+    OM = oracle.Mesh(N, L=L)
+    GM = nova.Mesh(N, L=L, walls=(0, 1, 0))
+    U0 = oracle.ic_temporal_shear(OM, seed=0, noise=1e-3)
+    dt = 0.3 * min(OM.d) / float(np.abs(U0).sum(axis=0).max())
+    kw = dict(model="ns", rk_mode="shear", nsteps=500, dt=dt, nu=1 / 2000, poisson="dct", bcU=SHEAR_UBC,
+              bcp=SHEAR_PBC)
+    g64 = run_gpu(nova, GM, U0, precision=nova.F64, **dict(kw))
+    g32 = run_gpu(nova, GM, U0, precision=nova.F32SPLIT, **dict(kw))
+    err = rel_l2(g32["U"], g64["U"])
+    print("shear layer 256x256x128, 500 steps, t = %.4f: FP32-split rel. L2 vs FP64 = %.3e" % (500 * dt, err))
+    assert 0 < err < 1e-5
+    assert np.all(np.isfinite(g64["hist"])) and g64["hist"][-1, 4] < 1e-9 * g64["hist"][-1, 10] / min(OM.d)
+
+
+def test_mhd_jet_192x192x384_split_vs_fp64(nova, oracle):
+    """The MHD jet (x, y in [-4, 4), z in [0, 16), spacing 1/24; u_z = 0.5 (1 -
+    tanh((r - 1)/0.1)), B_z = 0.5, B_theta = 0.2 r exp(-r^2), seed-1 noise 1e-3 on
+    u; nu = eta = 1/1500; the app's scheme), 200 steps: FP32-split against FP64."""
+    N = (192, 192, 384)
+    OM = oracle.Mesh(N, L=(8.0, 8.0, 16.0), origin=(-4.0, -4.0, 0.0))
+    U0, B0 = oracle.ic_mhd_jet(OM)
+    dt = oracle.cfl_dt(OM, [U0, B0])
+    kw = dict(model="mhd", rk_mode="literal", nsteps=200, dt=dt, nu=1 / 1500, eta=1 / 1500)
+    GM = nova.Mesh(N, L=(8.0, 8.0, 16.0), origin=(-4.0, -4.0, 0.0))
+    g64 = run_gpu(nova, GM, U0, B0, precision=nova.F64, **dict(kw))
+    g32 = run_gpu(nova, GM, U0, B0, precision=nova.F32SPLIT, **dict(kw))
+    eu, eb = rel_l2(g32["U"], g64["U"]), rel_l2(g32["B"], g64["B"])
+    print("MHD jet 192x192x384, 200 steps, t = %.4f: FP32-split rel. L2 vs FP64: U %.3e, B %.3e" % (200 * dt, eu, eb))
+    assert 0 < eu < 1e-5 and 0 < eb < 1e-5

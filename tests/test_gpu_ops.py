@@ -245,3 +245,30 @@ def test_cpp_adapter_tensor_operators(oracle, tmp_path):
         assert rel_max(read(k, nc), g["out_" + k]) < TOL, k
     want = OM.interior(oracle.grad_v(OM, OM.to_ghosted(g["U"])))
     assert rel_max(read("grad_v", 9), want) < TOL
+
+
+def test_fields_of_another_mesh_are_refused(nova):
+    """A field made by a context of a smaller mesh, passed with a larger
+    context, is refused with NOVA_E_INVALID by every entry point that reads or
+    writes its nodes (its buffers hold fewer nodes than the context's mesh)."""
+    import ctypes as C
+    small, big = nova.Mesh((8, 8, 8)), nova.Mesh((16, 16, 16))
+    s1, s3 = nova.Field(small, 1), nova.Field(small, 3)
+    b1, b3 = nova.Field(big, 1), nova.Field(big, 3)
+    L, h = big.lib, big.h
+    v = C.c_double()
+    host = np.zeros(3 * 16 ** 3)
+    calls = {
+        "maxabs": L.nova_field_maxabs(h, s1.h, C.byref(v)),
+        "maxabs_noalloc": L.nova_field_maxabs_noalloc(h, s1.h, C.byref(v)),
+        "grad_s": L.nova_grad_s(h, s1.h, b3.h),
+        "grad_s out": L.nova_grad_s(h, b1.h, s3.h),
+        "div_vf": L.nova_div_vf(h, b3.h, s3.h, b3.h),
+        "poisson": L.nova_poisson_solve(h, s1.h, b1.h),
+        "upload_soa": L.nova_field_upload_soa(h, s3.h, nova._dptr(host)),
+        "download_soa": L.nova_field_download_soa(h, s3.h, nova._dptr(host)),
+    }
+    st = nova.State(s3.h, b1.h, None, None)
+    rd = nova.run_desc(dt=1e-3)
+    calls["advance"] = L.nova_advance(h, C.byref(rd), C.byref(st), 1, None)
+    assert calls == {k: nova.E_INVALID for k in calls}, calls

@@ -101,6 +101,60 @@ def test_shear_layer_advance_with_walls(nova, oracle, rk_mode, spec):
     assert np.abs(hist[:, 4] - r[4][:, 4]).max() < 1e-10 * max(1.0, np.abs(r[4][:, 4]).max())
 
 
+@pytest.mark.parametrize("rk_mode", ["shear", "classical"])
+def test_shear_layer_golden_with_walls(nova, oracle, rk_mode):
+    """The wall-bounded shear layer against the reference's own run
+    (tests/golden/shear_walls_12x10x8.npz: app/shearLayer/UEqn.H, the RK4
+    weights as stage coefficients with a projection per stage) and, in the
+    classical mode, against the oracle."""
+    from conftest import check_history, load_golden
+    g = load_golden("shear_walls_12x10x8.npz")
+    N_ = tuple(int(v) for v in g["N"])
+    OM = oracle.Mesh(N_, L=tuple(g["L"]))
+    GM = nova.Mesh(N_, L=tuple(g["L"]), walls=(0, 1, 0))
+    kw = dict(model="ns", rk_mode=rk_mode, dt=float(g["dt"]), nu=float(g["nu"]))
+    U = set_bc(nova, nova.Field(GM, 3), UBC, 3).upload_soa(g["U0"])
+    p = set_bc(nova, nova.Field(GM, 1), PBC, 1)
+    hist = nova.advance(GM, nova.run_desc(**kw), U, p, nsteps=int(g["nsteps"]))
+    if rk_mode == "shear":
+        ref_U, ref_p, ref_h = g["U"], g["p"], g["hist"]
+    else:
+        r = oracle.run(OM, oracle.ghosted_from_stored(OM, g["U0"], UBC), bcU=UBC, bcp=PBC, nsteps=int(g["nsteps"]),
+                       **kw)
+        ref_U, ref_p, ref_h = oracle.stored_of(OM, r[0]), oracle.stored_of(OM, r[2]), r[4]
+    got = U.download_soa()
+    for c in range(3):
+        assert rel_l2(got[c], ref_U[c]) < 1e-11, (c, rel_l2(got[c], ref_U[c]))
+    assert rel_l2(p.download_soa(), ref_p) < 1e-11
+    check_history(hist, ref_h, divtol=1e-10 * max(1.0, np.abs(ref_h[:, 4]).max()))
+
+
+def test_shear_layer_loop_with_walls_vs_oracle(nova, oracle):
+    """The shear-layer loop on a 32 x 24 x 16 wall mesh over 12 steps, FP64 against
+    the oracle (the periodic solve of the app), and FP32-split against FP64."""
+    from conftest import check_history
+    N_ = (32, 24, 16)
+    Lw = (2 * np.pi, 2 * np.pi, np.pi)
+    OM = oracle.Mesh(N_, L=Lw)
+    GM = nova.Mesh(N_, L=Lw, walls=(0, 1, 0))
+    U0 = oracle.ic_temporal_shear(OM, seed=0, noise=1e-2, delta=4.0)
+    kw = dict(model="ns", rk_mode="shear", dt=0.01, nu=1 / 2000)
+    r = oracle.run(OM, oracle.ghosted_from_stored(OM, U0, UBC), bcU=UBC, bcp=PBC, nsteps=12, **kw)
+    out = {}
+    for prec in (nova.F64, nova.F32SPLIT):
+        U = set_bc(nova, nova.Field(GM, 3, prec), UBC, 3).upload_soa(U0)
+        p = set_bc(nova, nova.Field(GM, 1), PBC, 1)
+        h = nova.advance(GM, nova.run_desc(precision=prec, **kw), U, p, nsteps=12)
+        out[prec] = (U.download_soa(), p.download_soa(), h)
+    got, gp, gh = out[nova.F64]
+    ref = oracle.stored_of(OM, r[0])
+    for c in range(3):
+        assert rel_l2(got[c], ref[c]) < 1e-11, (c, rel_l2(got[c], ref[c]))
+    assert rel_l2(gp, oracle.stored_of(OM, r[2])) < 1e-11
+    check_history(gh, r[4], divtol=1e-10 * max(1.0, np.abs(r[4][:, 4]).max()))
+    assert 0 < rel_l2(out[nova.F32SPLIT][0], got) < 1e-5
+
+
 def test_walls_fp32_split_error_is_bounded(nova, oracle):
     OM = oracle.Mesh(N, L=L)
     GM = gpu_mesh(nova)

@@ -41,8 +41,12 @@ def test_operators_bitwise_vs_reference_golden(oracle, name):
 
 
 @pytest.mark.parametrize("name", ["tg_12_classical.npz", "tg_12_literal.npz", "ot_12_classical.npz",
-                                  "ot_12_literal.npz"])
+                                  "ot_12_literal.npz", "tg_12_shear.npz", "ot_12_shear.npz"])
 def test_time_loop_bitwise_vs_reference_golden(oracle, name):
+    """The loop bodies (app/TG_Piosson/RKLoop.H, app/OT_Poisson/UEqn.H + BEqn.H,
+    app/shearLayer/UEqn.H) and every history column (app/OT_Poisson/OT.cpp:132-176,
+    tools::CFL, tools::maximum of the divergences, the central-curl enstrophies)
+    against the reference's own run, bit for bit"""
     g = load_golden(name)
     M = oracle.Mesh(tuple(g["N"]), L=tuple(g["L"]))
     model = str(g["model"])
@@ -52,10 +56,49 @@ def test_time_loop_bitwise_vs_reference_golden(oracle, name):
                                    eta=float(g["eta"]))
     assert np.array_equal(M.unique(U), g["U"])
     assert np.array_equal(M.unique(p), g["p"])
+    assert hist.shape == (int(g["nsteps"]), oracle.HIST_COLS)
     assert np.array_equal(hist, g["hist"])
     if model == "mhd":
         assert np.array_equal(M.unique(B), g["B"])
         assert np.array_equal(M.unique(pB), g["pB"])
+        assert np.all(hist[:, 7] > 0) and np.all(hist[:, 15] > 0)  # J terms present
+    assert np.all(hist[:, 6] > 0) and np.all(hist[:, 14] > 0) and np.all(hist[:, 11] > 0)
+
+
+def test_shear_layer_loop_with_walls_bitwise_vs_reference_golden(oracle):
+    """app/shearLayer/UEqn.H with Neumann/Dirichlet y walls and the periodic solve
+    the app calls (Q8), against the reference's own run"""
+    g = load_golden("shear_walls_12x10x8.npz")
+    M = oracle.Mesh(tuple(int(v) for v in g["N"]), L=tuple(g["L"]))
+    bc = {"north": [(1, 0.0), (2, 0.0), (1, 0.0)], "south": [(1, 0.0), (2, 0.0), (1, 0.0)]}
+    pbc = {"north": (1, 0.0), "south": (1, 0.0)}
+    Ug = oracle.ghosted_from_stored(M, g["U0"], bc)
+    U, B, p, pB, hist = oracle.run(M, Ug, model="ns", rk_mode="shear", nsteps=int(g["nsteps"]), dt=float(g["dt"]),
+                                   nu=float(g["nu"]), bcU=bc, bcp=pbc)
+    assert np.array_equal(oracle.stored_of(M, U), g["U"])
+    assert np.array_equal(oracle.stored_of(M, p), g["p"])
+    assert np.array_equal(hist, g["hist"])
+
+
+def test_history_columns_of_the_taylor_green_field(oracle):
+    """Known values of a history row at t = 0 for u = sin x cos y cos z,
+    v = -cos x sin y cos z: Ek = 1/8, Umax = 1 and the central curl's enstrophy
+    from the modified wavenumber k' of the 6th-order first derivative (all three
+    curl components are products of one sine or cosine per axis, each
+    differentiated once)"""
+    N = 16
+    M = oracle.Mesh((N, N, N))
+    Ug = M.to_ghosted(oracle.ic_taylor_green(M))
+    row = oracle.diag_row(M, Ug, dt=0.1, nu=0.01, t=0.5)
+    h = 2 * np.pi / N
+    kp = sum(c / (l + 1) * np.sin((l + 1) * h) / h for l, c in enumerate((1.5, -0.6, 0.1)))
+    # w = (-cos x sin y sin z D_z', -sin x cos y sin z D_z', 2 sin x sin y cos z D') k' up to signs:
+    # 1/2 <|w|^2> = 1/2 k'^2 (1/8 + 1/8 + 4/8) = 3 k'^2 / 8
+    assert abs(row[2] - 0.125) < 1e-14
+    assert abs(row[10] - 1.0) < 1e-12
+    assert abs(row[14] - 3 * kp * kp / 8) < 1e-12
+    assert row[4] < 1e-13
+    assert abs(row[11] - 0.1 / h) < 1e-12 and abs(row[12] - row[11]) < 1e-15
 
 
 def test_live_reference_matches_restatement_with_walls(oracle):
@@ -136,7 +179,7 @@ def test_compressible_taylor_green_bitwise_vs_reference_golden(oracle):
                                        order="tg", nsteps=int(g["nsteps"]), dt=float(g["dt"]), mu=float(g["mu"]))
     for name, a in (("U", U), ("rho", rho), ("p", p)):
         assert np.array_equal(M.unique(a), g[name]), name
-    assert np.array_equal(hist, g["hist"])
+    assert np.array_equal(hist[:, :6], g["hist"])
 
 
 def test_weakly_compressible_shear_bitwise_vs_reference_golden(oracle):
@@ -152,7 +195,7 @@ def test_weakly_compressible_shear_bitwise_vs_reference_golden(oracle):
                                        nsteps=int(g["nsteps"]), dt=float(g["dt"]), **prm)
     for name, a in (("U", U), ("rho", rho), ("p", p), ("T", T)):
         assert np.array_equal(M.unique(a), g[name]), name
-    assert np.array_equal(hist, g["hist"])
+    assert np.array_equal(hist[:, :6], g["hist"])
     assert np.abs(g["rho"] - g["rho_init"]).max() > 0  # the density really evolves
 
 
