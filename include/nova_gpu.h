@@ -221,11 +221,16 @@ nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *run, nova_state *st
  *                              the dissipation rate the apps print (app/TG/TG.cpp:113-115),
  *                              i.e. J = E(n0) - E(N), n0 = window_start; E = Ek (Navier-Stokes)
  *                              or Ek + Em (MHD; the apps print Ek, Em and their rates, app/OT_Poisson/OT.cpp:135-180)
- * NOVA_OBJ_ETOT_FINAL:         J = Ek(N) + Em(N), Em = mean(1/2 |B|^2) (MHD only) */
+ * NOVA_OBJ_ETOT_FINAL:         J = Ek(N) + Em(N), Em = mean(1/2 |B|^2) (MHD only)
+ * NOVA_OBJ_LINEAR_FINAL:       J = <w, U(N)> / (N0 N1 N2), w = the weight field (Navier-Stokes,
+ *                              FP64): the gradient is the adjoint of the linearised N-step map
+ *                              applied to w / (N0 N1 N2), for the dot-product test
+ *                              <D Phi v, w> = <v, D Phi^T w> */
 typedef enum {
     NOVA_OBJ_EKIN_FINAL = 0,
     NOVA_OBJ_DISSIPATION_WINDOW = 1,
-    NOVA_OBJ_ETOT_FINAL = 2
+    NOVA_OBJ_ETOT_FINAL = 2,
+    NOVA_OBJ_LINEAR_FINAL = 3
 } nova_objective;
 typedef struct {
     nova_run_desc run;     /* forward run: NS or MHD, classical RK4, FP64 or FP32-split, periodic uniform mesh */
@@ -233,6 +238,7 @@ typedef struct {
     int checkpoint_every;  /* K: states kept every K steps, segments recomputed in reverse */
     int objective;         /* nova_objective */
     int window_start;      /* n0 of NOVA_OBJ_DISSIPATION_WINDOW, 0 <= n0 < nsteps */
+    const nova_field *weight;  /* w of NOVA_OBJ_LINEAR_FINAL (3 comps, FP64); else ignored */
 } nova_adj_desc;
 /* Gradient of J with respect to the initial fields by the hand-written
  * discrete adjoint of the fused stages, the RK4 loops and the (self-adjoint)

@@ -216,4 +216,35 @@ void launch_scale_copy(long long n, double a, const double *x, double *y, cudaSt
     k_axpby<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, x, y);
 }
 
+namespace {
+
+__global__ void k_dot_part(long long n, const double *__restrict__ x, const double *__restrict__ y,
+                           double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    double a = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a = fma(x[t], y[t], a);
+    a = block_reduce_sum(a, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
+__global__ void k_sum_final(const double *__restrict__ part, int nb, double scale, double *__restrict__ out)
+{
+    __shared__ double sh[32];
+    double a = 0.0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) a += part[q];
+    a = block_reduce_sum(a, sh);
+    if (threadIdx.x == 0) *out = a * scale;
+}
+
+}  // namespace
+
+void launch_dot(long long n, const double *x, const double *y, double scale, double *part, int nb, double *out,
+                cudaStream_t st)
+{
+    k_dot_part<<<nb, 256, 0, st>>>(n, x, y, part);
+    k_sum_final<<<1, 256, 0, st>>>(part, nb, scale, out);
+}
+
 }  // namespace nova

@@ -1441,8 +1441,12 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
         return fail(ctx, NOVA_E_UNSUPPORTED,
                     "nova_adjoint_grad: built for classical RK4 Navier-Stokes and MHD, FP64 or FP32-split");
     const bool window = ad->objective == NOVA_OBJ_DISSIPATION_WINDOW;
-    if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window && !(mhd && ad->objective == NOVA_OBJ_ETOT_FINAL))
-        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective for this model");
+    const bool linear = ad->objective == NOVA_OBJ_LINEAR_FINAL;
+    if (ad->objective != NOVA_OBJ_EKIN_FINAL && !window && !(mhd && ad->objective == NOVA_OBJ_ETOT_FINAL) &&
+        !(linear && !mhd && !split))
+        return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: unknown objective for this model and precision");
+    if (linear && (!valid_field(ctx, ad->weight, 3) || ad->weight->prec != NOVA_F64))
+        return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: the linear objective needs a 3-component FP64 weight");
     if (window && (ad->window_start < 0 || ad->window_start >= ad->nsteps))
         return fail(ctx, NOVA_E_INVALID, "nova_adjoint_grad: window_start must lie in [0, nsteps)");
     if (ctx->h != 3) return fail(ctx, NOVA_E_UNSUPPORTED, "nova_adjoint_grad: the fused kernels are built for m = 6");
@@ -1515,8 +1519,15 @@ extern "C" nova_status nova_adjoint_grad(nova_ctx *ctx, const nova_adj_desc *ad,
     ekin(mu, ctx->d_row);
     double row[2 * NOVA_HIST_COLS];
     CK(cudaMemcpyAsync(row, ctx->d_row, sizeof(row), cudaMemcpyDeviceToHost, st));
-    launch_scale_copy((long long)V, (window ? -1.0 : 1.0) / (double)ctx->g.N3, mu, lam, st);
-    ctx->launches += 1;
+    if (linear) {  // J = <w, U_N> / N^3, lambda_N = w / N^3
+        launch_dot((long long)V, ad->weight->d64, mu, 1.0 / (double)ctx->g.N3, ctx->d_part, 592, ctx->d_scalar, st);
+        launch_scale_copy((long long)V, 1.0 / (double)ctx->g.N3, ad->weight->d64, lam, st);
+        ctx->launches += 3;
+        CK(cudaMemcpyAsync(row + 2, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, st));
+    } else {
+        launch_scale_copy((long long)V, (window ? -1.0 : 1.0) / (double)ctx->g.N3, mu, lam, st);
+        ctx->launches += 1;
+    }
     CKL("adjoint seed");
 
     // reverse sweep, segment by segment

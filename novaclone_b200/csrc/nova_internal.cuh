@@ -240,6 +240,9 @@ cudaError_t launch_adj_mhd(int kind, int s, const Geo &g, const Coef<double> &co
                            double visc, const AdjArgs &a, double *acc, cudaStream_t st, int *err = nullptr);
 void launch_scale_copy(long long n, double a, const double *x, double *y, cudaStream_t st);  // y = a x
 void launch_axpy(long long n, double a, const double *x, double *y, cudaStream_t st);        // y += a x
+// *out = scale * sum_t x[t] y[t] (nb blocks of partials in part)
+void launch_dot(long long n, const double *x, const double *y, double scale, double *part, int nb, double *out,
+                cudaStream_t st);
 
 // Which kernel runs the Navier-Stokes stage: STAGE_AUTO = the TMA pipeline
 // (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits: periodic y,
@@ -294,6 +297,16 @@ cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef
                                const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
                                cudaStream_t st, const StageDiag *dg = nullptr,
                                bool *dg_done = nullptr);
+// MHD stage kernels on the TMA pipeline (nova_stage_mhd_tma.cu): periodic y,
+// N2 % 32 == 0, N1 a multiple of the tile height 8 (FP64) or 16 (FP32) and at
+// least twice it; a.X is the frozen field
+bool mhd_tma_fits(const Geo &g, bool fp64);
+cudaError_t launch_mhd_tma64(int phys, int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
+                             const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
+                             cudaStream_t st);
+cudaError_t launch_mhd_tma32(int phys, int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
+                             const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
+                             cudaStream_t st);
 cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
                                const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
                                cudaStream_t st);

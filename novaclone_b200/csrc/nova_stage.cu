@@ -131,55 +131,12 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
                 // comps 0-2: U (stage state), 3-5: B (frozen)
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
                 const T b0[3] = {q[H][3], q[H][4], q[H][5]};
-                T advU[3] = {0, 0, 0}, advB[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, gb[3], divU = 0, divB = 0;
-                T duz[3] = {0, 0, 0};
-                auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        advU[c] += adv1<T, H>(v, c, d, u0[d], a);
-                        advB[c] += adv1<T, H>(v, 3 + c, 3 + d, b0[d], a);
-                        lap[c] += lsum<T, H>(v, c, b);
-                        if (STRETCH && zdir) duz[c] = d1<T, H>(v, c, a);
-                    }
-                    divU += d1<T, H>(v, d, a);
-                    divB += d1<T, H>(v, 3 + d, a);
-                    // grad(0.5*(B&B)) along d (src/ex/grad/grad.cpp:43-54 on the product field)
-                    auto e = [&](int, int s) -> T {
-                        return (v(3, s) * v(3, s) + v(4, s) * v(4, s) + v(5, s) * v(5, s)) * T(0.5);
-                    };
-                    gb[d] = d1<T, H>(e, 0, a);
-                };
-                dir(vx, 0, co.a[0], co.b[0], false);
-                dir(vy, 1, co.a[1], co.b[1], false);
-                dir(vz, 2, az, bz, true);
-#pragma unroll
-                for (int c = 0; c < 3; c++)
-                    rhs[c] = T(-0.5) * fma(u0[c], divU, advU[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c])
-                             + T(0.5) * fma(b0[c], divB, advB[c]) - gb[c];
+                mhd_u_rhs<T, H, STRETCH>(vx, vy, vz, u0, b0, co, az, bz, bsum, c2k, visc, rhs);
             } else {
                 // comps 0-2: B (stage state), 3-5: U (frozen)
                 const T b0[3] = {q[H][0], q[H][1], q[H][2]};
                 const T u0[3] = {q[H][3], q[H][4], q[H][5]};
-                T advUB[3] = {0, 0, 0}, advBU[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, divU = 0, divB = 0;
-                T dbz[3] = {0, 0, 0};
-                auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        advUB[c] += adv1<T, H>(v, c, 3 + d, u0[d], a);
-                        advBU[c] += adv1<T, H>(v, 3 + c, d, b0[d], a);
-                        lap[c] += lsum<T, H>(v, c, b);
-                        if (STRETCH && zdir) dbz[c] = d1<T, H>(v, c, a);
-                    }
-                    divU += d1<T, H>(v, 3 + d, a);
-                    divB += d1<T, H>(v, d, a);
-                };
-                dir(vx, 0, co.a[0], co.b[0], false);
-                dir(vy, 1, co.a[1], co.b[1], false);
-                dir(vz, 2, az, bz, true);
-#pragma unroll
-                for (int c = 0; c < 3; c++)
-                    rhs[c] = T(-0.5) * fma(b0[c], divU, advUB[c]) + T(0.5) * fma(u0[c], divB, advBU[c])
-                             + visc * (fma(-bsum, b0[c], lap[c]) - c2k * dbz[c]);
+                mhd_b_rhs<T, H, STRETCH>(vx, vy, vz, b0, u0, co, az, bz, bsum, c2k, visc, rhs);
             }
 
             if constexpr (std::is_same<T, double>::value) {
@@ -260,7 +217,9 @@ cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, cons
 {
     if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage <= 4 && stage_tma_fits(g, true))
         return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st, dg, dg_done);
-    if (phys == PHYS_NS && ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
+    if (phys != PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && ex.err && stage <= 4 && mhd_tma_fits(g, true))
+        return launch_mhd_tma64(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
+    if (ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
     launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;
 }
@@ -271,7 +230,9 @@ cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, cons
 {
     if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage <= 4 && stage_tma_fits(g, false))
         return launch_stage_tma32(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
-    if (phys == PHYS_NS && ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
+    if (phys != PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && ex.err && stage <= 4 && mhd_tma_fits(g, false))
+        return launch_mhd_tma32(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
+    if (ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
     launch_stage_any<float>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;
 }

@@ -85,6 +85,72 @@ __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz,
     }
 }
 
+// The MHD right-hand sides (comps 0-2 of the accessors: the evolved field,
+// 3-5: the frozen one), ex::div(V,F) in the skew form above:
+//   U loop (app/OT_Poisson/UEqn.H:16-23):
+//     -div(U,U) + laplacian(nu,U) + div(B,B) - grad(0.5*(B&B))
+//   B loop (app/OT_Poisson/BEqn.H:72-78):
+//     -div(U,B) + div(B,U) + laplacian(eta,B)
+// az, bz: the z weights with the metric (a_l iak, b_l iak^2); bsum: the
+// Laplacian's centre weight of the three directions; c2k: the stretched-z
+// Laplacian term's coefficient (0 on uniform meshes).
+template <typename T, int H, bool STRETCH, class VX, class VY, class VZ>
+__device__ __forceinline__ void mhd_u_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&u0)[3],
+                                          const T (&b0)[3], const Coef<T> &co, const T *az, const T *bz, T bsum,
+                                          T c2k, T visc, T (&rhs)[3])
+{
+    T advU[3] = {0, 0, 0}, advB[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, gb[3], divU = 0, divB = 0;
+    T duz[3] = {0, 0, 0};
+    auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            advU[c] += adv1<T, H>(v, c, d, u0[d], a);
+            advB[c] += adv1<T, H>(v, 3 + c, 3 + d, b0[d], a);
+            lap[c] += lsum<T, H>(v, c, b);
+            if (STRETCH && zdir) duz[c] = d1<T, H>(v, c, a);
+        }
+        divU += d1<T, H>(v, d, a);
+        divB += d1<T, H>(v, 3 + d, a);
+        // grad(0.5*(B&B)) along d (src/ex/grad/grad.cpp:43-54 on the product field)
+        auto e = [&](int, int s) -> T { return (v(3, s) * v(3, s) + v(4, s) * v(4, s) + v(5, s) * v(5, s)) * T(0.5); };
+        gb[d] = d1<T, H>(e, 0, a);
+    };
+    dir(vx, 0, co.a[0], co.b[0], false);
+    dir(vy, 1, co.a[1], co.b[1], false);
+    dir(vz, 2, az, bz, true);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        rhs[c] = T(-0.5) * fma(u0[c], divU, advU[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c]) +
+                 T(0.5) * fma(b0[c], divB, advB[c]) - gb[c];
+}
+
+template <typename T, int H, bool STRETCH, class VX, class VY, class VZ>
+__device__ __forceinline__ void mhd_b_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&b0)[3],
+                                          const T (&u0)[3], const Coef<T> &co, const T *az, const T *bz, T bsum,
+                                          T c2k, T visc, T (&rhs)[3])
+{
+    T advUB[3] = {0, 0, 0}, advBU[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, divU = 0, divB = 0;
+    T dbz[3] = {0, 0, 0};
+    auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            advUB[c] += adv1<T, H>(v, c, 3 + d, u0[d], a);
+            advBU[c] += adv1<T, H>(v, 3 + c, d, b0[d], a);
+            lap[c] += lsum<T, H>(v, c, b);
+            if (STRETCH && zdir) dbz[c] = d1<T, H>(v, c, a);
+        }
+        divU += d1<T, H>(v, 3 + d, a);
+        divB += d1<T, H>(v, d, a);
+    };
+    dir(vx, 0, co.a[0], co.b[0], false);
+    dir(vy, 1, co.a[1], co.b[1], false);
+    dir(vz, 2, az, bz, true);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        rhs[c] = T(-0.5) * fma(b0[c], divU, advUB[c]) + T(0.5) * fma(u0[c], divB, advBU[c]) +
+                 visc * (fma(-bsum, b0[c], lap[c]) - c2k * dbz[c]);
+}
+
 // Stage update of one component at node o (classical RK4 of
 // src/settings/settings.cpp:44-51 in the association order of
 // app/TG_Piosson/RKLoop.H:24-28; STAGE 4 = the loop as written, one dU):

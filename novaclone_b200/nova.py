@@ -29,7 +29,7 @@ HIST_COLS = 16
 HIST_NAMES = ("step", "t", "Ek", "Em", "max_div_U", "max_div_B", "omega", "Jav", "Jmax", "epsilon", "Umax",
               "cfl_x", "cfl_y", "cfl_z", "enstrophy_U", "enstrophy_B")
 K_STAGE, K_DIV, K_FFT, K_CORRECT, K_DIAG, K_ADJ = range(6)
-OBJ_EKIN_FINAL, OBJ_DISSIPATION_WINDOW, OBJ_ETOT_FINAL = 0, 1, 2
+OBJ_EKIN_FINAL, OBJ_DISSIPATION_WINDOW, OBJ_ETOT_FINAL, OBJ_LINEAR_FINAL = 0, 1, 2, 3
 WC_TG, WC_SHEAR = 0, 1
 STATUS_NAMES = {0: "NOVA_OK", 1: "NOVA_E_INVALID", 2: "NOVA_E_CUDA", 3: "NOVA_E_OOM", 4: "NOVA_E_NONFINITE",
                 5: "NOVA_E_TIMEOUT", 6: "NOVA_E_UNSUPPORTED"}
@@ -69,7 +69,7 @@ class RunDesc(C.Structure):
 
 class AdjDesc(C.Structure):
     _fields_ = [("run", RunDesc), ("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("objective", C.c_int),
-                ("window_start", C.c_int)]
+                ("window_start", C.c_int), ("weight", C.c_void_p)]
 
 
 class State(C.Structure):
@@ -521,10 +521,11 @@ def advance(mesh: Mesh, rd: RunDesc, U: Field, p: Field, B: Field = None, pB: Fi
 
 
 def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_every: int = 20,
-                 window_start: int = None, B0: Field = None, total_energy: bool = False):
+                 window_start: int = None, B0: Field = None, total_energy: bool = False, weight: Field = None):
     """Gradient of J by the discrete adjoint.  J = Ek(nsteps); with total_energy
     (MHD) Ek + Em; with window_start = n0 the dissipation over steps n0+1..nsteps,
-    E(n0) - E(nsteps) (E = Ek, or Ek + Em for MHD).  Returns (J, dJ/dU0) for
+    E(n0) - E(nsteps) (E = Ek, or Ek + Em for MHD); with a weight field w
+    (Navier-Stokes, FP64) J = <w, U(nsteps)> / N^3.  Returns (J, dJ/dU0) for
     Navier-Stokes and (J, dJ/dU0, dJ/dB0) for MHD (rd.model MHD, B0 given).
     With rd.precision F32SPLIT (U0, B0 split fields) the trajectory is the split
     path's and the adjoint stages run in FP32; the gradients are FP64."""
@@ -532,7 +533,10 @@ def adjoint_grad(mesh: Mesh, rd: RunDesc, U0: Field, nsteps: int, checkpoint_eve
     a.run = rd
     a.nsteps = int(nsteps)
     a.checkpoint_every = int(checkpoint_every)
-    if window_start is not None:
+    a.weight = weight.h if weight is not None else None
+    if weight is not None:
+        a.objective = OBJ_LINEAR_FINAL
+    elif window_start is not None:
         a.objective = OBJ_DISSIPATION_WINDOW
     else:
         a.objective = OBJ_ETOT_FINAL if total_energy else OBJ_EKIN_FINAL

@@ -375,3 +375,46 @@ def test_split_mhd_adjoint_checkpoints_and_window(nova, oracle):
     assert J32 == pytest.approx(J64, rel=1e-5)
     assert rel_l2(u32.download_soa(), u64.download_soa()) < SPLIT_TOL
     assert rel_l2(b32.download_soa(), b64.download_soa()) < SPLIT_TOL
+
+
+@pytest.mark.parametrize("N", [(24, 24, 24), (16, 16, 32)])
+def test_dot_product_identity(nova, oracle, N):
+    """<D Phi v, w> = <v, D Phi^T w> for the N-step map Phi of nova_advance
+    (classical RK4 + projection, FP64).  The adjoint side is nova_adjoint_grad
+    with the linear objective J = <w, U(N)>/N^3 (its gradient is D Phi^T w / N^3);
+    the tangent side is the central difference of the forward states,
+    (Phi(U0 + e v) - Phi(U0 - e v)) / (2 e), e = 1e-6.  w and v are seeded white
+    noise (every mode, no symmetry of the base state annihilates them)."""
+    nsteps, nu, eps = 8, 1e-2, 1e-6
+    U0, dt = base_state(oracle, N)
+    rng = np.random.default_rng(77)
+    v = rng.standard_normal((3,) + N)
+    w = rng.standard_normal((3,) + N)
+    n3 = float(np.prod(N))
+    GM = nova.Mesh(N)
+    rd = nova.run_desc(model="ns", rk_mode="classical", dt=dt, nu=nu, diag_every=0)
+
+    def phi(U_init):
+        U = nova.Field(GM, 3).upload_soa(U_init)
+        nova.advance(GM, rd, U, nova.Field(GM, 1), nsteps=nsteps, history=False)
+        return U.download_soa()
+
+    J, g = nova.adjoint_grad(GM, rd, nova.Field(GM, 3).upload_soa(U0), nsteps, checkpoint_every=3,
+                             weight=nova.Field(GM, 3).upload_soa(w))
+    UN = phi(U0)
+    assert J == pytest.approx(float(np.sum(w * UN)) / n3, rel=1e-12)
+    tangent = (phi(U0 + eps * v) - phi(U0 - eps * v)) / (2 * eps)
+    lhs = float(np.sum(tangent * w)) / n3
+    rhs = float(np.sum(v * g.download_soa()))
+    err = abs(lhs - rhs) / abs(rhs)
+    print("dot-product test %s: <J v, w> = %.15e, <v, J^T w> = %.15e, rel. err %.2e" % (N, lhs, rhs, err))
+    assert err < 1e-7
+
+
+def test_linear_objective_is_refused_where_not_built(nova):
+    GM = nova.Mesh((16, 16, 16))
+    U, w = nova.Field(GM, 3, nova.F32SPLIT), nova.Field(GM, 3)
+    rd = nova.run_desc(model="ns", rk_mode="classical", precision=nova.F32SPLIT, dt=1e-3, nu=1e-2)
+    with pytest.raises(nova.NovaError) as e:
+        nova.adjoint_grad(GM, rd, U, 2, checkpoint_every=1, weight=w)
+    assert e.value.status == nova.E_UNSUPPORTED
