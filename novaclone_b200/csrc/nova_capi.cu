@@ -62,6 +62,12 @@ struct nova_ctx {
     // transforms and the i direction runs fused with the scale (k_pois_i)
     bool pois_i = false;
     double *d_twN = nullptr;  // W_N0^m, m = 0..N0-1 (re, im)
+    // N1 = N2 = 256 as well: the (j, k) planes by the one-pass cluster kernels
+    // (nova_fft2d.cu) instead of the cuFFT plans; NOVA_FFT=cufft keeps cuFFT
+    bool fft2 = false;
+    bool fft_cufft_only = false;
+    bool fft_ready = false;
+    double *d_tw256 = nullptr;
     cufftHandle dct_f = 0, dct_b = 0;  // wall Poisson on the even extension in y
     bool dct_plans = false;
     double *d_ext = nullptr, *d_ky2e = nullptr;
@@ -281,24 +287,45 @@ struct ProfScope {
     ~ProfScope() { prof_end(ctx, cls, a); }
 };
 
+// W_N^m = exp(-2 pi i m / N), m = 0..N-1, rounded from extended precision
+std::vector<double> twiddles(int N)
+{
+    std::vector<double> tw(2 * (size_t)N);
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < N; m++) {
+        const long double a = 2.0L * pi_l * (long double)m / (long double)N;
+        tw[2 * m] = (double)cosl(a);
+        tw[2 * m + 1] = (double)-sinl(a);
+    }
+    return tw;
+}
+
 nova_status ensure_fft(nova_ctx *ctx)
 {
-    if (ctx->plans) return NOVA_OK;
+    if (ctx->fft_ready) return NOVA_OK;
     const Geo &g = ctx->g;
     nova_status s;
+    if (pois_i_fits(g) && !ctx->fft_cufft_only && fft2_fits(g)) {
+        // the (j, k) planes by the cluster kernels, the i direction by k_pois_i
+        std::vector<double> tw = twiddles(g.N0), t256 = twiddles(256);
+        if ((s = dalloc(ctx, &ctx->d_twN, tw.size())) != NOVA_OK) return s;
+        CK(cudaMemcpy(ctx->d_twN, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice));
+        if ((s = dalloc(ctx, &ctx->d_tw256, t256.size())) != NOVA_OK) return s;
+        CK(cudaMemcpy(ctx->d_tw256, t256.data(), sizeof(double) * t256.size(), cudaMemcpyHostToDevice));
+        ctx->pois_i = true;
+        ctx->fft2 = true;
+        const size_t nspec = (size_t)g.N0 * g.N1 * (g.N2 / 2 + 1);
+        if ((s = dalloc(ctx, (double **)&ctx->d_spec, 2 * nspec)) != NOVA_OK) return s;
+        if ((s = dalloc(ctx, &ctx->d_rhs, (size_t)g.N3)) != NOVA_OK) return s;
+        ctx->fft_ready = true;
+        return NOVA_OK;
+    }
     // the transform runs over the N[1] unique y nodes of poisson::rhs (poisson.cpp:167-181),
     // which with walls are the first N[1] of the N[1]+1 stored rows
     const int ny = ctx->md.N[1];
     const bool pi = pois_i_fits(g);
     if (pi) {
-        // W_N0^m = exp(-2 pi i m / N0), rounded from extended precision
-        std::vector<double> tw(2 * (size_t)g.N0);
-        const long double pi_l = 3.141592653589793238462643383279502884L;
-        for (int m = 0; m < g.N0; m++) {
-            const long double a = 2.0L * pi_l * (long double)m / (long double)g.N0;
-            tw[2 * m] = (double)cosl(a);
-            tw[2 * m + 1] = (double)-sinl(a);
-        }
+        std::vector<double> tw = twiddles(g.N0);
         if ((s = dalloc(ctx, &ctx->d_twN, tw.size())) != NOVA_OK) return s;
         CK(cudaMemcpy(ctx->d_twN, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice));
     }
@@ -323,6 +350,7 @@ nova_status ensure_fft(nova_ctx *ctx)
     const size_t nspec = (size_t)g.N0 * ny * (g.N2 / 2 + 1);
     if ((s = dalloc(ctx, (double **)&ctx->d_spec, 2 * nspec)) != NOVA_OK) return s;
     if ((s = dalloc(ctx, &ctx->d_rhs, (size_t)g.N3)) != NOVA_OK) return s;
+    ctx->fft_ready = true;
     return NOVA_OK;
 }
 
@@ -351,12 +379,21 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
     nova_status s;
     if ((s = ensure_fft(ctx)) != NOVA_OK) return s;
     ProfScope ps(ctx, NOVA_K_FFT);
+    const long long nuniq = (long long)ctx->g.N0 * ctx->md.N[1] * ctx->g.N2;
+    if (ctx->fft2) {
+        launch_fft2_fwd(ctx->g, rhs, ctx->d_spec, ctx->d_tw256, ctx->stream);
+        launch_pois_i(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_twN, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
+                      1.0 / (double)nuniq, ctx->stream);
+        launch_fft2_inv(ctx->g, ctx->d_spec, p, ctx->d_tw256, ctx->stream);
+        ctx->launches += 3;
+        CKL("cluster FFT / k_pois_i");
+        return NOVA_OK;
+    }
     cufftSetStream(ctx->plan_f, ctx->stream);
     cufftSetStream(ctx->plan_b, ctx->stream);
     if ((s = fft_check(ctx, cufftExecD2Z(ctx->plan_f, (cufftDoubleReal *)rhs, (cufftDoubleComplex *)ctx->d_spec),
                        "cufftExecD2Z")) != NOVA_OK)
         return s;
-    const long long nuniq = (long long)ctx->g.N0 * ctx->md.N[1] * ctx->g.N2;
     if (ctx->pois_i) {
         launch_pois_i(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_twN, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                       1.0 / (double)nuniq, ctx->stream);
@@ -463,6 +500,7 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
         if (!std::strcmp(impl, "march")) ctx->stage_impl = STAGE_MARCH;
         if (!std::strcmp(impl, "tma")) ctx->stage_impl = STAGE_TMA;
     }
+    if (const char *f = std::getenv("NOVA_FFT")) ctx->fft_cufft_only = !std::strcmp(f, "cufft");
     for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
     Geo &g = ctx->g;
     g.wallY = md->walls[1];
@@ -546,7 +584,7 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
     }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->w32x};
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->w32x, ctx->d_tw256};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -934,6 +972,8 @@ nova_status ensure_work(nova_ctx *ctx, int prec)
         else
             s = dalloc(ctx, &ctx->w32[q], n);
     }
+    // the FP32-split path's U* (FP64, the projection's input)
+    if (s == NOVA_OK && prec != NOVA_F64) s = dalloc(ctx, &ctx->w64[0], n);
     if (s == NOVA_OK) s = ensure_fft(ctx);
     if (s == NOVA_OK) s = ensure_red(ctx);
     return s;
@@ -1136,7 +1176,6 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
                         phys_of(dg->fin));
             ctx->launches += 2;
         }
-        const float *Ushi, *Uslo;
         nova_status sst = NOVA_OK;
         auto run32 = [&](int stage, const StageArgs32 &a) {
             ProfScope ps(ctx, NOVA_K_STAGE);
@@ -1147,11 +1186,13 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             ctx->launches += 1;
         };
         const float *Xp = X ? X->hi : nullptr;
+        // U* leaves the last stage in FP64 (as many bytes as the (hi, lo) pair)
+        // for the FP64 projection, which reads it as the FP64 path does
+        double *Us64 = ctx->w64[0];
         if (lit) {
-            run32(4, StageArgs32{Y->hi, Xp, nullptr, Y->lo, nullptr, nullptr, ctx->w32[0], ctx->w32[1]});
-            fixpair(ctx->w32[0], ctx->w32[1]);
-            Ushi = ctx->w32[0];
-            Uslo = ctx->w32[1];
+            StageArgs32 a{Y->hi, Xp, nullptr, Y->lo, nullptr, nullptr, nullptr, nullptr};
+            a.out64 = Us64;
+            run32(4, a);
         } else {
             float *w0 = ctx->w32[0], *w1 = ctx->w32[1], *A = ctx->w32[2];
             run32(0, StageArgs32{Y->hi, Xp, nullptr, nullptr, A, w0, nullptr, nullptr});
@@ -1160,16 +1201,19 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             fix32(w1);
             run32(2, StageArgs32{w1, Xp, Y->hi, nullptr, A, w0, nullptr, nullptr});
             fix32(w0);
-            run32(3, StageArgs32{w0, Xp, Y->hi, Y->lo, A, nullptr, Y->hi, Y->lo});
-            fixpair(Y->hi, Y->lo);
-            Ushi = Y->hi;
-            Uslo = Y->lo;
+            StageArgs32 a{w0, Xp, Y->hi, Y->lo, A, nullptr, nullptr, nullptr};
+            a.out64 = Us64;
+            run32(3, a);
+        }
+        if (walls) {
+            launch_wall_fix64(g, yfix, Us64, st);
+            ctx->launches += 1;
         }
         if (sst != NOVA_OK) return sst;
         CKL("stage kernel");
         {
             ProfScope ps(ctx, NOVA_K_DIV);
-            const cudaError_t e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, nullptr, Ushi, Uslo,
+            const cudaError_t e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, Us64, nullptr, nullptr,
                                                   divisor, ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
             if (e != cudaSuccess) return stage_fail(ctx, e);
             ctx->launches += 1;
@@ -1183,8 +1227,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
         }
         {
             ProfScope ps(ctx, NOVA_K_CORRECT);
-            const cudaError_t e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, nullptr,
-                                                 nullptr, Ushi, Uslo, Y->hi, Y->lo, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
+            const cudaError_t e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, corr_scale, Us64,
+                                                 nullptr, nullptr, nullptr, Y->hi, Y->lo, st,
+                                                 StageExec{ctx->stage_impl, ctx->d_flag + 1});
             if (e != cudaSuccess) return stage_fail(ctx, e);
             ctx->launches += 1;
         }
@@ -1361,18 +1406,23 @@ nova_status rk_loop32(nova_ctx *ctx, const nova_run_desc *rd, int phys, double v
     run(0, StageArgs32{hi, X, nullptr, nullptr, A, S2, nullptr, nullptr});
     run(1, StageArgs32{S2, X, hi, nullptr, A, S3, nullptr, nullptr});
     run(2, StageArgs32{S3, X, hi, nullptr, A, S4, nullptr, nullptr});
-    if (full) run(3, StageArgs32{S4, X, hi, lo, A, nullptr, ohi, olo});
+    double *Us64 = ctx->w64[0];  // U* in FP64, as nova_advance's split path keeps it
+    if (full) {
+        StageArgs32 a{S4, X, hi, lo, A, nullptr, nullptr, nullptr};
+        a.out64 = Us64;
+        run(3, a);
+    }
     if (sst != NOVA_OK) return sst;
     CKL("stage kernel");
     if (!full) return NOVA_OK;
-    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, nullptr, ohi, olo, div,
+    cudaError_t e = launch_div_proj(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, Us64, nullptr, nullptr, div,
                                     ctx->d_rhs, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
     if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;
     CKL("k_div_tiled");
     nova_status s = poisson_device(ctx, ctx->d_rhs, pbuf);
     if (s != NOVA_OK) return s;
-    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, div, nullptr, nullptr, ohi, olo,
+    e = launch_correct(ctx->h, g, Walls<double>{}, ctx->co64, ctx->d_ia64, pbuf, div, Us64, nullptr, nullptr, nullptr,
                        ohi, olo, st, StageExec{ctx->stage_impl, ctx->d_flag + 1});
     if (e != cudaSuccess) return stage_fail(ctx, e);
     ctx->launches += 1;

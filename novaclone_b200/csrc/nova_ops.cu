@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kThreads) k_correct_tiled(Geo g, Walls<double>
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const long long o = c * g.N3 + idx;
-            us[c] = SPLIT ? (double)Ushi[o] + (double)Uslo[o] : Us64[o];
+            us[c] = (SPLIT && !Us64) ? (double)Ushi[o] + (double)Uslo[o] : Us64[o];
         }
         const double gr[3] = {d1<double, H>(vx, 0, co.a[0]), d1<double, H>(vy, 0, co.a[1]), d1<double, H>(vz, 0, az)};
 #pragma unroll
@@ -740,6 +740,7 @@ cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const C
         constexpr size_t sb = tile_smem_bytes<double, HH, 1>();                                           \
         k_correct_tiled<HH, SPL, W><<<grid, block, sb, st>>>(g, pw, co, ia, p, s, Us64, U64, Ushi, Uslo, hi, lo, ch); \
     })
+    // SPLIT: (hi, lo) output, from an FP64 U* (Us64) or a (hi, lo) one
     if (U64) {
         if (pw.on) { NOVA_CORR(false, true); } else { NOVA_CORR(false, false); }
     } else {

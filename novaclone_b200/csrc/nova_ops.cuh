@@ -35,6 +35,13 @@ void launch_scale(const Geo &g, int ny, void *spec, const double *kx2, const dou
 // (nova_pois_i.cu): in place on the half spectrum [i][j][kz] of the 2-D
 // (j, k) transforms; twN = W_N0^m, m = 0..N0-1 (interleaved re, im)
 bool pois_i_fits(const Geo &g);
+// the (j, k) plane transforms in one pass each (nova_fft2d.cu, clusters of
+// eight CTAs): periodic y, N1 = N2 = 256, and the device can hold a cluster;
+// x real [i][j][k] <-> spec [i][j][kz] (kz < 129), unnormalised like cuFFT's
+// batched 2-D D2Z / Z2D; tw256 = W_256^m (interleaved re, im)
+bool fft2_fits(const Geo &g);
+void launch_fft2_fwd(const Geo &g, const double *x, void *spec, const double *tw256, cudaStream_t st);
+void launch_fft2_inv(const Geo &g, const void *spec, double *x, const double *tw256, cudaStream_t st);
 void launch_pois_i(const Geo &g, int ny, void *spec, const double *twN, const double *kx2, const double *ky2,
                    const double *kz2, double invN3, cudaStream_t st);
 cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,

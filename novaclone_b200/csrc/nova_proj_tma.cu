@@ -33,7 +33,8 @@ constexpr int kRowsE = (TJ + 2 * kH) * kTK;  // a component's rows with the j ha
 constexpr int kTileE = TJ * kTK;             // a component's tile rows
 constexpr int kLRE = TJ * 4;                 // one side's k halo of a component
 
-enum ProjMode { PROJ_DIV = 0, PROJ_CORR = 1 };
+// PROJ_CORR_MIX: the correction of an FP32-split state whose U* arrives in FP64
+enum ProjMode { PROJ_DIV = 0, PROJ_CORR = 1, PROJ_CORR_MIX = 2 };
 
 // map indices
 enum {
@@ -54,13 +55,13 @@ struct ProjMaps {
 template <int MODE, bool SPLIT> struct ProjCfg {
     static constexpr bool kDivLoads = MODE == PROJ_DIV;
     using TS = typename std::conditional<kDivLoads && SPLIT, float, double>::type;  // stencil element
-    using TE = typename std::conditional<SPLIT, float, double>::type;              // U* element
+    using TE = typename std::conditional<SPLIT && MODE == PROJ_CORR, float, double>::type;  // U* element
     static constexpr int kSets = (kDivLoads && SPLIT) ? 2 : 1;
     // elements of one set: DIV c0 tile | c1 rows | c2 tile | L | R;  CORR p rows | L | R
     static constexpr int kSetE = kDivLoads ? kTileE + kRowsE + kTileE + 2 * kLRE : kRowsE + 2 * kLRE;
     static constexpr int kSlotE = kSets * kSetE;
     static constexpr uint32_t kSlotBytes = kSlotE * sizeof(TS);
-    static constexpr int kNE = MODE == PROJ_CORR ? (SPLIT ? 2 : 1) : 0;  // epilogue fields
+    static constexpr int kNE = MODE == PROJ_CORR ? (SPLIT ? 2 : 1) : (MODE == PROJ_CORR_MIX ? 1 : 0);  // epilogue fields
     static constexpr int kEpiE = 3 * kTileE;
     static constexpr uint32_t kEpiBytes = kEpiE * sizeof(TE);
     static constexpr size_t kSmem =
@@ -254,7 +255,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             double us[3];
 #pragma unroll
             for (int c = 0; c < 3; c++)
-                us[c] = SPLIT ? (double)se[c * kTK] + (double)se[C::kEpiE + c * kTK] : (double)se[c * kTK];
+                us[c] = (SPLIT && MODE == PROJ_CORR) ? (double)se[c * kTK] + (double)se[C::kEpiE + c * kTK]
+                                                     : (double)se[c * kTK];
             release(eempty(p % kERing));
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -392,6 +394,11 @@ cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const doubl
     a.hi = hi;
     a.lo = lo;
     bool ok = encode_rows(pm, 0, p, g) && encode3(&pm.m[M_LR], p, g, 4, kLRB);
+    if (Us64 && hi) {  // FP64 U*, FP32-split output
+        ok = ok && encode4(&pm.m[M_EPI], Us64, g);
+        if (!ok) return cudaErrorInvalidValue;
+        return launch<PROJ_CORR_MIX, true>(g, co, ia, a, pm, err, st);
+    }
     if (Us64) {
         ok = ok && encode4(&pm.m[M_EPI], Us64, g);
         if (!ok) return cudaErrorInvalidValue;

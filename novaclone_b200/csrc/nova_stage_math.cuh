@@ -183,7 +183,8 @@ __device__ __forceinline__ void rk_store64(const StageArgs64 &a, long long o, do
 }
 
 // FP32-split: A is an FP32 sum of increments; the last stage adds it to the
-// (hi, lo) base in FP64.  e0: U0hi (stages 1-3, 5), e1: A, lo: U0lo (stages 3-5)
+// (hi, lo) base in FP64 and stores U* as a (hi, lo) pair, or in FP64 for the
+// projection (a.out64).  e0: U0hi (stages 1-3, 5), e1: A, lo: U0lo (stages 3-5)
 template <int STAGE>
 __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, float y0, float e0, float e1, float lo,
                                            float du)
@@ -197,6 +198,10 @@ __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, fl
     } else if constexpr (STAGE == 4) {
         const float inc = ((du * w6 + du * w3) + du * w3) + du * w6;
         const double x = ((double)y0 + (double)lo) + (double)inc;
+        if (a.out64) {
+            a.out64[o] = x;
+            return;
+        }
         const float hi = (float)x;
         a.outhi[o] = hi;
         a.outlo[o] = (float)(x - (double)hi);
@@ -212,6 +217,10 @@ __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, fl
     } else {
         const float inc = e1 + du * w6;
         const double x = ((double)e0 + (double)lo) + (double)inc;
+        if (a.out64) {
+            a.out64[o] = x;
+            return;
+        }
         const float hi = (float)x;
         a.outhi[o] = hi;
         a.outlo[o] = (float)(x - (double)hi);

@@ -73,8 +73,10 @@ def test_operators_vs_reference_golden(nova, oracle, name):
 
 
 # N0 = 64 and 256 run the i-direction FFT fused with the scale (k_pois_i);
-# N2 = 10 and 18 leave a ragged last group of kz columns
-@pytest.mark.parametrize("N", [(16, 16, 16), (24, 12, 18), (9, 6, 15), (64, 12, 18), (256, 8, 10), (64, 32, 64)])
+# N2 = 10 and 18 leave a ragged last group of kz columns; (64, 256, 256) runs
+# the (j, k) planes on the cluster kernels (nova_fft2d.cu)
+@pytest.mark.parametrize("N", [(16, 16, 16), (24, 12, 18), (9, 6, 15), (64, 12, 18), (256, 8, 10), (64, 32, 64),
+                               (64, 256, 256)])
 def test_poisson_vs_oracle(nova, oracle, N):
     rng = np.random.default_rng(2)
     OM = oracle.Mesh(N)
@@ -272,3 +274,32 @@ def test_fields_of_another_mesh_are_refused(nova):
     rd = nova.run_desc(dt=1e-3)
     calls["advance"] = L.nova_advance(h, C.byref(rd), C.byref(st), 1, None)
     assert calls == {k: nova.E_INVALID for k in calls}, calls
+
+
+def test_cluster_plane_transforms_match_cufft(nova):
+    """The one-pass (j, k) plane transforms (clusters of eight CTAs sharing
+    their rows through distributed shared memory) against cuFFT's batched 2-D
+    transforms (NOVA_FFT=cufft) in the same spectral solve: a random
+    right-hand side on 64 x 256 x 256, relative max difference <= 1e-13."""
+    import os
+    N = (64, 256, 256)
+    s = np.random.default_rng(12).standard_normal((1,) + N)
+    out = {}
+    for impl in ("cluster", "cufft"):
+        old = os.environ.get("NOVA_FFT")
+        if impl == "cufft":
+            os.environ["NOVA_FFT"] = "cufft"
+        try:
+            GM = nova.Mesh(N)
+        finally:
+            if old is None:
+                os.environ.pop("NOVA_FFT", None)
+            else:
+                os.environ["NOVA_FFT"] = old
+        p = nova.Field(GM, 1)
+        pe = nova.poisson(p)
+        pe.rhs(nova.Field(GM, 1).upload_soa(s))
+        pe.solve()
+        out[impl] = p.download_soa()
+    assert rel_max(out["cluster"], out["cufft"]) < 1e-13
+    assert np.abs(out["cluster"]).max() > 1e-3
