@@ -62,10 +62,10 @@ struct nova_ctx {
     // transforms and the i direction runs fused with the scale (k_pois_i)
     bool pois_i = false;
     double *d_twN = nullptr;  // W_N0^m, m = 0..N0-1 (re, im)
-    // N1 = N2 = 256 as well: the (j, k) planes by the one-pass cluster kernels
-    // (nova_fft2d.cu) instead of the cuFFT plans; NOVA_FFT=cufft keeps cuFFT
+    // N1 = N2 = 256 as well and NOVA_FFT=cluster: the (j, k) planes by the
+    // one-pass cluster kernels (nova_fft2d.cu) instead of the cuFFT plans
     bool fft2 = false;
-    bool fft_cufft_only = false;
+    bool fft_cluster = false;
     bool fft_ready = false;
     double *d_tw256 = nullptr;
     cufftHandle dct_f = 0, dct_b = 0;  // wall Poisson on the even extension in y
@@ -305,7 +305,7 @@ nova_status ensure_fft(nova_ctx *ctx)
     if (ctx->fft_ready) return NOVA_OK;
     const Geo &g = ctx->g;
     nova_status s;
-    if (pois_i_fits(g) && !ctx->fft_cufft_only && fft2_fits(g)) {
+    if (pois_i_fits(g) && ctx->fft_cluster && fft2_fits(g)) {
         // the (j, k) planes by the cluster kernels, the i direction by k_pois_i
         std::vector<double> tw = twiddles(g.N0), t256 = twiddles(256);
         if ((s = dalloc(ctx, &ctx->d_twN, tw.size())) != NOVA_OK) return s;
@@ -500,7 +500,7 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
         if (!std::strcmp(impl, "march")) ctx->stage_impl = STAGE_MARCH;
         if (!std::strcmp(impl, "tma")) ctx->stage_impl = STAGE_TMA;
     }
-    if (const char *f = std::getenv("NOVA_FFT")) ctx->fft_cufft_only = !std::strcmp(f, "cufft");
+    if (const char *f = std::getenv("NOVA_FFT")) ctx->fft_cluster = !std::strcmp(f, "cluster");
     for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
     Geo &g = ctx->g;
     g.wallY = md->walls[1];

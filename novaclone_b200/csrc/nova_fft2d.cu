@@ -24,7 +24,12 @@
 // the column results stored into the row owners' shared memory.
 //
 // HBM traffic is one read and one write of the plane (512 KB real, 528 KB
-// complex), where the batched 2-D cuFFT makes two passes.
+// complex), where the batched 2-D cuFFT makes two passes.  At 256^3 the pair
+// still runs slower than cuFFT's (about 335 and 310 us against about 118 us
+// a direction): with 133 KB of shared memory and 168 registers a CTA, one
+// 8-warp CTA sits on an SM and the distributed-shared-memory reads and the
+// phase barriers are not hidden (8 % of DRAM bandwidth).  So the solver keeps
+// cuFFT and runs these kernels only under NOVA_FFT=cluster.
 #include "nova_fft.cuh"
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"

@@ -75,7 +75,7 @@ __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz,
         ns_dir<T, H>(vy, 1, u0[1], sc.ha[1], co.a[1], vb, s, dv);
     }
     divu = dv;
-    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * (iak * iak);
+    const T bsum = fma(co.b2[2], iak * iak, co.b2[0] + co.b2[1]);
     const T K = fma(T(-0.5), dv, -visc * bsum);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -189,6 +189,8 @@ template <int STAGE>
 __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, float y0, float e0, float e1, float lo,
                                            float du)
 {
+    // every product-sum is an explicit fmaf, so that the paired form
+    // (rk_store32x2) reproduces these bits
     const float w6 = 1.0f / 6.0f, w3 = 1.0f / 3.0f;
     if constexpr (STAGE == 5) {
         const double x = ((double)e0 + (double)lo) + (double)(du * a.w);
@@ -196,7 +198,7 @@ __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, fl
         a.outhi[o] = hi;
         a.outlo[o] = (float)(x - (double)hi);
     } else if constexpr (STAGE == 4) {
-        const float inc = ((du * w6 + du * w3) + du * w3) + du * w6;
+        const float inc = fmaf(du, w6, fmaf(du, w3, fmaf(du, w3, du * w6)));
         const double x = ((double)y0 + (double)lo) + (double)inc;
         if (a.out64) {
             a.out64[o] = x;
@@ -206,16 +208,16 @@ __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, fl
         a.outhi[o] = hi;
         a.outlo[o] = (float)(x - (double)hi);
     } else if constexpr (STAGE == 0) {
-        a.Ynext[o] = y0 + du * 0.5f;
+        a.Ynext[o] = fmaf(du, 0.5f, y0);
         a.A[o] = du * w6;
     } else if constexpr (STAGE == 1) {
-        a.Ynext[o] = e0 + du * 0.5f;
-        a.A[o] = e1 + du * w3;
+        a.Ynext[o] = fmaf(du, 0.5f, e0);
+        a.A[o] = fmaf(du, w3, e1);
     } else if constexpr (STAGE == 2) {
-        a.Ynext[o] = e0 + du;
-        a.A[o] = e1 + du * w3;
+        a.Ynext[o] = __fadd_rn(e0, du);  // not contracted with du = dt * rhs
+        a.A[o] = fmaf(du, w3, e1);
     } else {
-        const float inc = e1 + du * w6;
+        const float inc = fmaf(du, w6, e1);
         const double x = ((double)e0 + (double)lo) + (double)inc;
         if (a.out64) {
             a.out64[o] = x;
@@ -224,6 +226,123 @@ __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, fl
         const float hi = (float)x;
         a.outhi[o] = hi;
         a.outlo[o] = (float)(x - (double)hi);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Paired FP32: two adjacent k nodes per thread in the sm_100 f32x2
+// instructions (one FFMA2 / FADD2 / FMUL2 per pair).  Each function is the
+// scalar one above operation for operation (fma for fma, product for product,
+// p - m as fma(m, -1, p), which rounds identically), so the pair produces the
+// bits of two scalar evaluations.
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+
+template <int H, class V>
+__device__ __forceinline__ void ns_dir2(const V &v, int d, float2 v0, const float *ha, const float *a,
+                                        const float2 (&vb)[H], float2 (&s)[3], float2 &dd)
+{
+    float2 wp[H], wm[H];
+#pragma unroll
+    for (int l = 0; l < H; l++) {
+        const float2 p = v(d, l + 1), m = v(d, -l - 1);
+        wp[l] = fma2(f2(-ha[l]), add2(p, v0), vb[l]);
+        wm[l] = fma2(f2(ha[l]), add2(m, v0), vb[l]);
+        dd = fma2(f2(a[l]), sub2(p, m), dd);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        float2 r = s[c];
+#pragma unroll
+        for (int l = 0; l < H; l++) {
+            r = fma2(v(c, l + 1), wp[l], r);
+            r = fma2(v(c, -l - 1), wm[l], r);
+        }
+        s[c] = r;
+    }
+}
+
+template <int H, class V> __device__ __forceinline__ float2 d1x2(const V &v, int c, const float *a)
+{
+    float2 r = mul2(f2(a[0]), sub2(v(c, 1), v(c, -1)));
+#pragma unroll
+    for (int l = 1; l < H; l++) r = fma2(f2(a[l]), sub2(v(c, l + 1), v(c, -l - 1)), r);
+    return r;
+}
+
+// ns_rhs for a pair: accessors return float2 pairs; iak, c2k the columns' metric terms
+template <int H, bool STRETCH, class VX, class VY, class VZ>
+__device__ __forceinline__ void ns_rhs2(const VX &vx, const VY &vy, const VZ &vz, const float2 (&u0)[3],
+                                        const Coef<float> &co, const StageCoef<float> &sc, float2 iak, float2 c2k,
+                                        float visc, float2 (&rhs)[3])
+{
+    const float2 z = f2(0.0f);
+    float2 s[3] = {z, z, z}, dv = z;
+    {
+        float2 vb[H];
+        const float2 viak = mul2(f2(visc), iak);
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = mul2(viak, f2(co.b[2][l]));
+        ns_dir2<H>(vz, 2, u0[2], sc.ha[2], co.a[2], vb, s, dv);
+#pragma unroll
+        for (int c = 0; c < 3; c++) s[c] = mul2(s[c], iak);
+        dv = mul2(dv, iak);
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = f2(sc.vb[0][l]);
+        ns_dir2<H>(vx, 0, u0[0], sc.ha[0], co.a[0], vb, s, dv);
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = f2(sc.vb[1][l]);
+        ns_dir2<H>(vy, 1, u0[1], sc.ha[1], co.a[1], vb, s, dv);
+    }
+    const float2 bsum = fma2(f2(co.b2[2]), mul2(iak, iak), f2(co.b2[0] + co.b2[1]));
+    const float2 K = fma2(f2(-0.5f), dv, mul2(f2(-visc), bsum));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        float2 r = s[c];
+        if (STRETCH) r = fma2(mul2(f2(-visc), c2k), mul2(iak, d1x2<H>(vz, c, co.a[2])), r);
+        rhs[c] = fma2(u0[c], K, r);
+    }
+}
+
+__device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+
+// U* = (hi, lo) base + FP32 increment, per node in FP64 (rk_store32's last step)
+__device__ __forceinline__ void store_split2(const StageArgs32 &a, long long o, float2 base, float2 lo, float2 inc)
+{
+    const double x0 = ((double)base.x + (double)lo.x) + (double)inc.x;
+    const double x1 = ((double)base.y + (double)lo.y) + (double)inc.y;
+    if (a.out64) {
+        *reinterpret_cast<double2 *>(a.out64 + o) = make_double2(x0, x1);
+        return;
+    }
+    const float h0 = (float)x0, h1 = (float)x1;
+    st2(a.outhi + o, make_float2(h0, h1));
+    st2(a.outlo + o, make_float2((float)(x0 - (double)h0), (float)(x1 - (double)h1)));
+}
+
+// rk_store32 for the pair of nodes o, o + 1 (stages 0-4)
+template <int STAGE>
+__device__ __forceinline__ void rk_store32x2(const StageArgs32 &a, long long o, float2 y0, float2 e0, float2 e1,
+                                             float2 lo, float2 du)
+{
+    static_assert(STAGE >= 0 && STAGE <= 4, "stages 0-4");
+    const float2 w6 = f2(1.0f / 6.0f), w3 = f2(1.0f / 3.0f), h = f2(0.5f);
+    if constexpr (STAGE == 4) {
+        store_split2(a, o, y0, lo, fma2(du, w6, fma2(du, w3, fma2(du, w3, mul2(du, w6)))));
+    } else if constexpr (STAGE == 0) {
+        st2(a.Ynext + o, fma2(du, h, y0));
+        st2(a.A + o, mul2(du, w6));
+    } else if constexpr (STAGE == 1) {
+        st2(a.Ynext + o, fma2(du, h, e0));
+        st2(a.A + o, fma2(du, w3, e1));
+    } else if constexpr (STAGE == 2) {
+        st2(a.Ynext + o, add2(e0, du));
+        st2(a.A + o, fma2(du, w3, e1));
+    } else {
+        store_split2(a, o, e0, lo, fma2(du, w6, e1));
     }
 }
 

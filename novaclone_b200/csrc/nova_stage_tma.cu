@@ -46,14 +46,16 @@ constexpr int kRowE = 3 * kTK;  // one halo'd row, three components
 constexpr int kLRB = 8;         // rows of one k-halo box
 
 // Tile and ring configuration per precision.  FP64: a 32 x 16 tile, one block
-// per SM; FP32: a 32 x 8 tile, three blocks per SM.  Each block has one
-// consumer warp per tile row and one producer warp, whose elected lane issues
-// the loads in the order the consumers need them and blocks on the ring's
-// `empty` barriers alone, so it never delays the arithmetic.
+// per SM, one consumer warp per tile row.  FP32: a 32 x 8 tile, three blocks
+// per SM, one consumer warp per two tile rows (a half-warp per row, each lane
+// two adjacent k nodes in the paired f32x2 arithmetic).  Each block also has
+// one producer warp, whose elected lane issues the loads in the order the
+// consumers need them and blocks on the ring's `empty` barriers alone, so it
+// never delays the arithmetic.
 template <typename T> struct TmaCfg {
     static constexpr int TJ = sizeof(T) == 8 ? 16 : 8;
-    static constexpr int kWarps = TJ;                  // consumer warps (one per tile row)
-    static constexpr int kThreads = kTK * (TJ + 1);    // plus the producer warp
+    static constexpr int kWarps = sizeof(T) == 8 ? TJ : TJ / 2;  // consumer warps
+    static constexpr int kThreads = kTK * (kWarps + 1);          // plus the producer warp
     static constexpr int kBlocksPerSM = sizeof(T) == 8 ? 1 : 3;
     static constexpr int kRing = 7;   // stencil slots: the queue head runs kRing - 2H - 1 planes behind the loads
     static constexpr int kERing = 3;  // epilogue slots
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     const int ib = blockIdx.z * ichunk, ie = min(ib + ichunk, g.N0);
     const int nout = ie - ib, nld = nout + 2 * H;
 
-    if (ty == TJ && lane == 0) {
+    if (ty == C::kWarps && lane == 0) {  // the producer warp's lane initialises the barriers
         for (int r = 0; r < kRing; r++) {
             mbar_init(full(r), 1);
             mbar_init(empty(r), C::kWarps);
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     __syncthreads();
 
     // ---- producer warp: lane 0 issues every load of the block ----
-    if (ty == TJ) {
+    if (ty == C::kWarps) {
         if (lane != 0) return;
         const bool jlo = j0 < H, jhi = j0 + TJ + H > g.N1;
         const int kl = (k0 == 0 ? g.N2 : k0) - 4, kr = (k0 + kTK == g.N2) ? 0 : k0 + kTK;
@@ -216,17 +218,12 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
         __syncwarp();
         if (lane == 0) mbar_arrive(bar);
     };
-    const int kw = k0 + tx;
-    const T iak = ia[kw];
-    const T c2k = STRETCH ? corr2[kw] : T(0);
-
-    // slot offsets: centre, and the k neighbour at s (inside the row box or in
-    // the left/right halo boxes, [box][c][8 rows][4]); component stride kTK in both
-    const int cen = (H + ty) * kRowE + tx;
-    const int lrrow = (ty / kLRB) * 3 * kLRB * 4 + (ty % kLRB) * 4;
-    auto zoff = [&](int s) -> int {
-        const int x = tx + s;
-        return x < 0 ? kTcbE + lrrow + 4 + x : (x >= kTK ? kTcbE + kLRE + lrrow + (x - kTK) : cen + s);
+    // slot offset of the element at tile row r, tile column x (-4 <= x < kTK + 4):
+    // the row box, or the left/right halo boxes ([box][c][8 rows][4]);
+    // component stride kTK in both
+    auto soff = [&](int r, int x) -> int {
+        const int lrrow = (r / kLRB) * 3 * kLRB * 4 + (r % kLRB) * 4;
+        return x < 0 ? kTcbE + lrrow + 4 + x : (x >= kTK ? kTcbE + kLRE + lrrow + (x - kTK) : (H + r) * kRowE + x);
     };
 
     // i-stencil queue of the centre values of planes cur-3 .. cur+3.
@@ -241,6 +238,11 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
     DiagAccSm dacc{dred + kDiagParts * C::kWarps + ty * kTK + tx, C::kWarps * kTK};
     if constexpr (DIAG) dacc.init();
     if constexpr (sizeof(T) == 8) {
+        const int kw = k0 + tx;
+        const T iak = ia[kw];
+        const T c2k = STRETCH ? corr2[kw] : T(0);
+        const int cen = (H + ty) * kRowE + tx;
+        auto zoff = [&](int s) -> int { return soff(ty, tx + s); };
         T q[2 * H + 1][3];
         bool ok = true;
         for (int n = 0; n < 2 * H; n++) {  // queue: planes ib-3 .. ib+2
@@ -311,8 +313,19 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             release(empty(cur % kRing));
         }
     } else {
+        // FP32: warp ty computes tile rows 2 ty and 2 ty + 1 (one per half-warp),
+        // each lane the two adjacent k nodes kk, kk + 1 of its row in the paired
+        // arithmetic (ns_rhs2); pairs load as 8-byte shared-memory words.
         static_assert(kRing == 2 * H + 1, "queue rotation and ring slots share one period");
-        T q[2 * H + 1][3];
+        static_assert(2 * C::kWarps == TJ, "two tile rows per consumer warp");
+        const int r = 2 * ty + (lane >> 4), kk = 2 * (lane & 15);
+        const int cen = (H + r) * kRowE + kk;
+        // the z neighbours' pairs starting at kk - 4, kk - 2, kk + 2, kk + 4
+        const int zm4 = soff(r, kk - 4), zm2 = soff(r, kk - 2), zp2 = soff(r, kk + 2), zp4 = soff(r, kk + 4);
+        const float2 iak = *reinterpret_cast<const float2 *>(ia + k0 + kk);
+        const float2 c2k = STRETCH ? *reinterpret_cast<const float2 *>(corr2 + k0 + kk) : f2(0.0f);
+        auto ld2 = [](const T *b, int o) -> float2 { return *reinterpret_cast<const float2 *>(b + o); };
+        float2 q[2 * H + 1][3];
         bool ok = true;
         for (int n = 0; n < 2 * H; n++) {  // queue: planes ib-3 .. ib+2
             ok = mbar_wait(full(n % kRing), (n / kRing) & 1, err);
@@ -322,7 +335,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             }
             const T *sl = ring + (n % kRing) * kSlotE;
 #pragma unroll
-            for (int c = 0; c < 3; c++) q[n][c] = sl[cen + c * kTK];
+            for (int c = 0; c < 3; c++) q[n][c] = ld2(sl, cen + c * kTK);
             if (n < H || n >= H + nout) release(empty(n % kRing));  // queue-only plane
         }
 
@@ -338,34 +351,55 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                 constexpr int kQ = (R + 2 * H) % (2 * H + 1);
                 const T *sh = ring + sHd * kSlotE;
 #pragma unroll
-                for (int c = 0; c < 3; c++) q[kQ][c] = sh[cen + c * kTK];
+                for (int c = 0; c < 3; c++) q[kQ][c] = ld2(sh, cen + c * kTK);
                 if (hd >= H + nout) release(empty(sHd));
             }
             const T *sl = ring + sCur * kSlotE;
-            auto vx = [&](int c, int s) -> T { return q[(R + H + s + 2 * H + 1) % (2 * H + 1)][c]; };
-            auto vy = [&](int c, int s) -> T { return sl[cen + s * kRowE + c * kTK]; };
-            auto vz = [&](int c, int s) -> T { return sl[zoff(s) + c * kTK]; };
             constexpr int kC = (R + H) % (2 * H + 1);
-            const T u0[3] = {q[kC][0], q[kC][1], q[kC][2]};
-            T rhs[3], divu;
-            ns_rhs<T, H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs, divu);
+            auto vx = [&](int c, int s) -> float2 { return q[(R + H + s + 2 * H + 1) % (2 * H + 1)][c]; };
+            auto vy = [&](int c, int s) -> float2 { return ld2(sl, cen + s * kRowE + c * kTK); };
+            // odd offsets straddle two loaded pairs (the centre pair is the queue's)
+            auto vz = [&](int c, int s) -> float2 {
+                const int o = c * kTK;
+                switch (s) {
+                case -3: return make_float2(ld2(sl, zm4 + o).y, ld2(sl, zm2 + o).x);
+                case -2: return ld2(sl, zm2 + o);
+                case -1: return make_float2(ld2(sl, zm2 + o).y, q[kC][c].x);
+                case 1: return make_float2(q[kC][c].y, ld2(sl, zp2 + o).x);
+                case 2: return ld2(sl, zp2 + o);
+                case 3: return make_float2(ld2(sl, zp2 + o).y, ld2(sl, zp4 + o).x);
+                default: return q[kC][c];
+                }
+            };
+            const float2 u0[3] = {q[kC][0], q[kC][1], q[kC][2]};
+            float2 rhs[3];
+            ns_rhs2<H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
 
-            T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
+            const float2 zz = f2(0.0f);
+            float2 e0[3] = {zz, zz, zz}, e1[3] = {zz, zz, zz}, lo[3] = {zz, zz, zz};
             if constexpr (NE > 0) {
                 if (!__all_sync(0xffffffffu, mbar_wait(efull(es), eph, err))) return false;
-                const T *se = ering + es * NE * kEpiE + ty * kRowE + tx;
+                const T *se = ering + es * NE * kEpiE + r * kRowE + kk;
 #pragma unroll
-                for (int c = 0; c < 3; c++) epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
+                for (int c = 0; c < 3; c++) {
+                    const int o = c * kTK;
+                    if constexpr (STAGE == 1 || STAGE == 2) {
+                        e0[c] = ld2(se, o);
+                        e1[c] = ld2(se, kEpiE + o);
+                    } else if constexpr (STAGE == 3) {
+                        e0[c] = ld2(se, o);
+                        e1[c] = ld2(se, kEpiE + o);
+                        lo[c] = ld2(se, 2 * kEpiE + o);
+                    } else if constexpr (STAGE == 4) {
+                        lo[c] = ld2(se, o);
+                    }
+                }
             }
-            const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
+            const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + r) * g.N2 + k0 + kk;
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const long long o = (long long)c * g.N3 + idx;
-                if constexpr (sizeof(T) == 8)
-                    rk_store64<STAGE>(args, o, u0[c], e0[c], e1[c], dt * rhs[c]);
-                else
-                    rk_store32<STAGE>(args, o, u0[c], e0[c], e1[c], lo[c], dt * rhs[c]);
-            }
+            for (int c = 0; c < 3; c++)
+                rk_store32x2<STAGE>(args, (long long)c * g.N3 + idx, u0[c], e0[c], e1[c], lo[c],
+                                    mul2(f2(dt), rhs[c]));
             if constexpr (NE > 0) {
                 release(eempty(es));
                 if (++es == kERing) {
@@ -489,7 +523,7 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     }
     const int ch = tma_ichunk<T>(g);
     const dim3 grid(g.N2 / kTK, g.N1 / Cf::TJ, (g.N0 + ch - 1) / ch);
-    kern<<<grid, dim3(kTK, Cf::TJ + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err,
+    kern<<<grid, dim3(kTK, Cf::kWarps + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err,
                                                      dpart);
     return cudaSuccess;
 }

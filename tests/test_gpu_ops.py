@@ -279,7 +279,7 @@ def test_fields_of_another_mesh_are_refused(nova):
 def test_cluster_plane_transforms_match_cufft(nova):
     """The one-pass (j, k) plane transforms (clusters of eight CTAs sharing
     their rows through distributed shared memory) against cuFFT's batched 2-D
-    transforms (NOVA_FFT=cufft) in the same spectral solve: a random
+    transforms (the default) in the same spectral solve: a random
     right-hand side on 64 x 256 x 256, relative max difference <= 1e-13."""
     import os
     N = (64, 256, 256)
@@ -287,8 +287,10 @@ def test_cluster_plane_transforms_match_cufft(nova):
     out = {}
     for impl in ("cluster", "cufft"):
         old = os.environ.get("NOVA_FFT")
-        if impl == "cufft":
-            os.environ["NOVA_FFT"] = "cufft"
+        if impl == "cluster":
+            os.environ["NOVA_FFT"] = "cluster"
+        else:
+            os.environ.pop("NOVA_FFT", None)
         try:
             GM = nova.Mesh(N)
         finally:
