@@ -66,6 +66,7 @@ struct nova_ctx {
     // one-pass cluster kernels (nova_fft2d.cu) instead of the cuFFT plans
     bool fft2 = false;
     bool fft_cluster = false;
+    bool pois_direct = false;  // NOVA_POIS_I=direct: k_pois_i also where k_pois_tma fits
     bool fft_ready = false;
     double *d_tw256 = nullptr;
     cufftHandle dct_f = 0, dct_b = 0;  // wall Poisson on the even extension in y
@@ -378,12 +379,13 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
 {
     nova_status s;
     if ((s = ensure_fft(ctx)) != NOVA_OK) return s;
+    if ((s = ensure_red(ctx)) != NOVA_OK) return s;  // the error word of k_pois_tma
     ProfScope ps(ctx, NOVA_K_FFT);
     const long long nuniq = (long long)ctx->g.N0 * ctx->md.N[1] * ctx->g.N2;
     if (ctx->fft2) {
         launch_fft2_fwd(ctx->g, rhs, ctx->d_spec, ctx->d_tw256, ctx->stream);
         launch_pois_i(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_twN, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
-                      1.0 / (double)nuniq, ctx->stream);
+                      1.0 / (double)nuniq, ctx->pois_direct ? nullptr : ctx->d_flag + 1, ctx->stream);
         launch_fft2_inv(ctx->g, ctx->d_spec, p, ctx->d_tw256, ctx->stream);
         ctx->launches += 3;
         CKL("cluster FFT / k_pois_i");
@@ -396,7 +398,7 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
         return s;
     if (ctx->pois_i) {
         launch_pois_i(ctx->g, ctx->md.N[1], ctx->d_spec, ctx->d_twN, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
-                      1.0 / (double)nuniq, ctx->stream);
+                      1.0 / (double)nuniq, ctx->pois_direct ? nullptr : ctx->d_flag + 1, ctx->stream);
         ctx->launches += 1;
         CKL("k_pois_i");
     } else {
@@ -501,6 +503,7 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
         if (!std::strcmp(impl, "tma")) ctx->stage_impl = STAGE_TMA;
     }
     if (const char *f = std::getenv("NOVA_FFT")) ctx->fft_cluster = !std::strcmp(f, "cluster");
+    if (const char *f = std::getenv("NOVA_POIS_I")) ctx->pois_direct = !std::strcmp(f, "direct");
     for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
     Geo &g = ctx->g;
     g.wallY = md->walls[1];
@@ -897,10 +900,15 @@ extern "C" nova_status nova_poisson_solve(nova_ctx *ctx, const nova_field *rhs, 
     if (rhs->nc != 1 || p->nc != 1 || rhs->prec != NOVA_F64 || p->prec != NOVA_F64)
         return fail(ctx, NOVA_E_INVALID, "nova_poisson_solve: needs FP64 scalar fields");
     nova_status s = ensure_fft(ctx);
+    if (s == NOVA_OK) s = ensure_red(ctx);
     if (s != NOVA_OK) return s;
+    CK(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_rhs, rhs->d64, sizeof(double) * ctx->g.N3, cudaMemcpyDeviceToDevice, ctx->stream));
     if ((s = poisson_device(ctx, ctx->d_rhs, p->d64)) != NOVA_OK) return s;
+    int perr = 0;
+    CK(cudaMemcpyAsync(&perr, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (perr) return fail(ctx, NOVA_E_CUDA, "nova_poisson_solve: a k_pois_tma pipeline wait timed out");
     return NOVA_OK;
 }
 

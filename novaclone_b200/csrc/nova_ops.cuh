@@ -42,8 +42,11 @@ bool pois_i_fits(const Geo &g);
 bool fft2_fits(const Geo &g);
 void launch_fft2_fwd(const Geo &g, const double *x, void *spec, const double *tw256, cudaStream_t st);
 void launch_fft2_inv(const Geo &g, const void *spec, double *x, const double *tw256, cudaStream_t st);
+// err: the pipeline's error word (a bounded wait that gives up raises it);
+// null runs the register kernel k_pois_i, else N0 = 256 meshes with
+// N2 % 16 == 0 and N1 % 8 == 0 run the TMA-fed k_pois_tma
 void launch_pois_i(const Geo &g, int ny, void *spec, const double *twN, const double *kx2, const double *ky2,
-                   const double *kz2, double invN3, cudaStream_t st);
+                   const double *kz2, double invN3, int *err, cudaStream_t st);
 cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const Coef<double> &co, const double *ia,
                            const double *p, double s, const double *Us64, double *U64, const float *Ushi,
                            const float *Uslo, float *hi, float *lo, cudaStream_t st,

@@ -160,26 +160,41 @@ __device__ __forceinline__ void mhd_b_rhs(const VX &vx, const VY &vy, const VZ &
 //   s=3: U* = A  + dU*1/6
 //   s=5: U* = U0 + dU*w   (app/shearLayer/UEqn.H:28-29, w = RK4[rk] of the stage)
 // y0: the stage state at the node; e0: U0 (stages 1, 2, 5); e1: A (stages 1-3)
+// (every product-sum an explicit fma and the stage-2 sum unfused, so the
+// result does not depend on the compiler's contraction choices)
+template <int STAGE> struct RK64 {
+    // the (Ynext, A) values of one node
+    __device__ __forceinline__ static void eval(const StageArgs64 &a, double y0, double e0, double e1, double du,
+                                                double &yn, double &an)
+    {
+        const double w6 = 1.0 / 6.0, w3 = 1.0 / 3.0;
+        if constexpr (STAGE == 5) {
+            yn = fma(du, a.w, e0);
+        } else if constexpr (STAGE == 4) {
+            yn = fma(du, w6, fma(du, w3, fma(du, w3, fma(du, w6, y0))));
+        } else if constexpr (STAGE == 0) {
+            yn = fma(du, 0.5, y0);
+            an = fma(du, w6, y0);
+        } else if constexpr (STAGE == 1) {
+            yn = fma(du, 0.5, e0);
+            an = fma(du, w3, e1);
+        } else if constexpr (STAGE == 2) {
+            yn = __dadd_rn(e0, du);  // not contracted with du = dt * rhs
+            an = fma(du, w3, e1);
+        } else {
+            yn = fma(du, w6, e1);
+        }
+    }
+    static constexpr bool kA = STAGE <= 2;  // the stage writes the accumulator
+};
+
 template <int STAGE>
 __device__ __forceinline__ void rk_store64(const StageArgs64 &a, long long o, double y0, double e0, double e1, double du)
 {
-    const double w6 = 1.0 / 6.0, w3 = 1.0 / 3.0;
-    if constexpr (STAGE == 5) {
-        a.Ynext[o] = e0 + du * a.w;
-    } else if constexpr (STAGE == 4) {
-        a.Ynext[o] = (((y0 + du * w6) + du * w3) + du * w3) + du * w6;
-    } else if constexpr (STAGE == 0) {
-        a.Ynext[o] = y0 + du * 0.5;
-        a.A[o] = y0 + du * w6;
-    } else if constexpr (STAGE == 1) {
-        a.Ynext[o] = e0 + du * 0.5;
-        a.A[o] = e1 + du * w3;
-    } else if constexpr (STAGE == 2) {
-        a.Ynext[o] = e0 + du * 1.0;
-        a.A[o] = e1 + du * w3;
-    } else {
-        a.Ynext[o] = e1 + du * w6;
-    }
+    double yn, an;
+    RK64<STAGE>::eval(a, y0, e0, e1, du, yn, an);
+    a.Ynext[o] = yn;
+    if constexpr (RK64<STAGE>::kA) a.A[o] = an;
 }
 
 // FP32-split: A is an FP32 sum of increments; the last stage adds it to the

@@ -73,10 +73,11 @@ def test_operators_vs_reference_golden(nova, oracle, name):
 
 
 # N0 = 64 and 256 run the i-direction FFT fused with the scale (k_pois_i);
-# N2 = 10 and 18 leave a ragged last group of kz columns; (64, 256, 256) runs
-# the (j, k) planes on the cluster kernels (nova_fft2d.cu)
+# N2 = 10 and 18 leave a ragged last group of kz columns; (256, 16, 32) and
+# (256, 24, 16) run the TMA-fed k_pois_tma (8-column tiles, the last kz of 8
+# j per remainder tile: 2 and 3 of them)
 @pytest.mark.parametrize("N", [(16, 16, 16), (24, 12, 18), (9, 6, 15), (64, 12, 18), (256, 8, 10), (64, 32, 64),
-                               (64, 256, 256)])
+                               (64, 256, 256), (256, 16, 32), (256, 24, 16)])
 def test_poisson_vs_oracle(nova, oracle, N):
     rng = np.random.default_rng(2)
     OM = oracle.Mesh(N)
@@ -305,3 +306,33 @@ def test_cluster_plane_transforms_match_cufft(nova):
         out[impl] = p.download_soa()
     assert rel_max(out["cluster"], out["cufft"]) < 1e-13
     assert np.abs(out["cluster"]).max() > 1e-3
+
+
+@pytest.mark.parametrize("N", [(256, 16, 32), (256, 32, 64)])
+def test_pois_tma_equals_register_kernel(nova, N):
+    """k_pois_tma (double-buffered bulk-copy tiles, persistent grid) against
+    k_pois_i (NOVA_POIS_I=direct) in the same spectral solve: the same
+    arithmetic in the same order, so identical bits."""
+    import os
+    s = np.random.default_rng(13).standard_normal((1,) + N)
+    out = {}
+    for impl in ("tma", "direct"):
+        old = os.environ.get("NOVA_POIS_I")
+        if impl == "direct":
+            os.environ["NOVA_POIS_I"] = "direct"
+        else:
+            os.environ.pop("NOVA_POIS_I", None)
+        try:
+            GM = nova.Mesh(N)
+        finally:
+            if old is None:
+                os.environ.pop("NOVA_POIS_I", None)
+            else:
+                os.environ["NOVA_POIS_I"] = old
+        p = nova.Field(GM, 1)
+        pe = nova.poisson(p)
+        pe.rhs(nova.Field(GM, 1).upload_soa(s))
+        pe.solve()
+        out[impl] = p.download_soa()
+    assert np.array_equal(out["tma"], out["direct"])
+    assert np.abs(out["tma"]).max() > 1e-3
