@@ -70,13 +70,6 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
 
     // z metric of this thread's column (src/ex/*: terms divided by dzdxi(k))
     const T iak = ia[kw];
-    T az[H], bz[H];
-#pragma unroll
-    for (int l = 0; l < H; l++) {
-        az[l] = co.a[2][l] * iak;
-        bz[l] = co.b[2][l] * iak * iak;
-    }
-    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
     const T c2k = STRETCH ? corr2[kw] : T(0);
 
     const T *src[NC];
@@ -131,12 +124,12 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
                 // comps 0-2: U (stage state), 3-5: B (frozen)
                 const T u0[3] = {q[H][0], q[H][1], q[H][2]};
                 const T b0[3] = {q[H][3], q[H][4], q[H][5]};
-                mhd_u_rhs<T, H, STRETCH>(vx, vy, vz, u0, b0, co, az, bz, bsum, c2k, visc, rhs);
+                mhd_rhs<T, H, STRETCH, true>(vx, vy, vz, u0, b0, co, sc, iak, c2k, visc, rhs);
             } else {
                 // comps 0-2: B (stage state), 3-5: U (frozen)
                 const T b0[3] = {q[H][0], q[H][1], q[H][2]};
                 const T u0[3] = {q[H][3], q[H][4], q[H][5]};
-                mhd_b_rhs<T, H, STRETCH>(vx, vy, vz, b0, u0, co, az, bz, bsum, c2k, visc, rhs);
+                mhd_rhs<T, H, STRETCH, false>(vx, vy, vz, b0, u0, co, sc, iak, c2k, visc, rhs);
             }
 
             if constexpr (std::is_same<T, double>::value) {

@@ -85,70 +85,103 @@ __device__ __forceinline__ void ns_rhs(const VX &vx, const VY &vy, const VZ &vz,
     }
 }
 
-// The MHD right-hand sides (comps 0-2 of the accessors: the evolved field,
-// 3-5: the frozen one), ex::div(V,F) in the skew form above:
-//   U loop (app/OT_Poisson/UEqn.H:16-23):
+// The MHD right-hand sides (comps 0-2 of the accessors: the evolved field E,
+// 3-5: the frozen one F), ex::div(V,F) in the skew form above:
+//   U loop (app/OT_Poisson/UEqn.H:16-23), E = U, F = B:
 //     -div(U,U) + laplacian(nu,U) + div(B,B) - grad(0.5*(B&B))
-//   B loop (app/OT_Poisson/BEqn.H:72-78):
+//   B loop (app/OT_Poisson/BEqn.H:72-78), E = B, F = U:
 //     -div(U,B) + div(B,U) + laplacian(eta,B)
-// az, bz: the z weights with the metric (a_l iak, b_l iak^2); bsum: the
-// Laplacian's centre weight of the three directions; c2k: the stretched-z
-// Laplacian term's coefficient (0 on uniform meshes).
-template <typename T, int H, bool STRETCH, class VX, class VY, class VZ>
-__device__ __forceinline__ void mhd_u_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&u0)[3],
-                                          const T (&b0)[3], const Coef<T> &co, const T *az, const T *bz, T bsum,
-                                          T c2k, T visc, T (&rhs)[3])
+// Both are, per direction d, shared-weight sums over the neighbours (the
+// ns_dir form): -1/2 A_d(U,E)_c + visc lsum_d(E_c) = sum_l E_c(+-l) W+-_l with
+// W+-_l = -+(a_l/2)(U_d(+-l) + U_d(0)) + visc b_l, and +1/2 A_d(B,F)_c =
+// sum_l F_c(+-l) V+-_l with V+-_l = +-(a_l/2)(B_d(+-l) + B_d(0)); the
+// remaining skew terms are -1/2 E_c div U + 1/2 F_c div B.  So
+//   rhs_c = sum_d [E-sum + F-sum] + E_c(0) K1 + F_c(0) K2 (- d_c 0.5|B|^2, U loop),
+//   K1 = -div U / 2 - visc bsum,  K2 = div B / 2,
+// with the stretched-z term -visc c2k dE_c/dz.  z is evaluated first with the
+// uniform weights (and vb = visc iak b_l) and scaled by iak = 1/dzdxi, as in
+// ns_rhs.  About 310 operations per node for the U loop (the term-by-term
+// form: about 430).
+
+// one direction d: s[c] += the E- and F-sums; du += D_d U_d, db += D_d B_d,
+// gb (GRADB) = D_d 0.5|B|^2.  uo, bo: the component offsets of U and B.
+template <typename T, int H, bool GRADB, class V>
+__device__ __forceinline__ void mhd_dir(const V &v, int d, int uo, int bo, T ud0, T bd0, const T *ha, const T *a,
+                                        const T (&vb)[H], T (&s)[3], T &du, T &db, T &gb)
 {
-    T advU[3] = {0, 0, 0}, advB[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, gb[3], divU = 0, divB = 0;
-    T duz[3] = {0, 0, 0};
-    auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
+    T wp[H], wm[H], xp[H], xm[H];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            advU[c] += adv1<T, H>(v, c, d, u0[d], a);
-            advB[c] += adv1<T, H>(v, 3 + c, 3 + d, b0[d], a);
-            lap[c] += lsum<T, H>(v, c, b);
-            if (STRETCH && zdir) duz[c] = d1<T, H>(v, c, a);
+    for (int l = 0; l < H; l++) {
+        const T up = v(uo + d, l + 1), um = v(uo + d, -l - 1);
+        wp[l] = fma(-ha[l], up + ud0, vb[l]);
+        wm[l] = fma(ha[l], um + ud0, vb[l]);
+        du = fma(a[l], up - um, du);
+        const T bp = v(bo + d, l + 1), bm = v(bo + d, -l - 1);
+        xp[l] = ha[l] * (bp + bd0);
+        xm[l] = -ha[l] * (bm + bd0);
+        db = fma(a[l], bp - bm, db);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        T r = s[c];
+#pragma unroll
+        for (int l = 0; l < H; l++) {
+            r = fma(v(c, l + 1), wp[l], r);
+            r = fma(v(c, -l - 1), wm[l], r);
         }
-        divU += d1<T, H>(v, d, a);
-        divB += d1<T, H>(v, 3 + d, a);
-        // grad(0.5*(B&B)) along d (src/ex/grad/grad.cpp:43-54 on the product field)
-        auto e = [&](int, int s) -> T { return (v(3, s) * v(3, s) + v(4, s) * v(4, s) + v(5, s) * v(5, s)) * T(0.5); };
-        gb[d] = d1<T, H>(e, 0, a);
-    };
-    dir(vx, 0, co.a[0], co.b[0], false);
-    dir(vy, 1, co.a[1], co.b[1], false);
-    dir(vz, 2, az, bz, true);
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-        rhs[c] = T(-0.5) * fma(u0[c], divU, advU[c]) + visc * (fma(-bsum, u0[c], lap[c]) - c2k * duz[c]) +
-                 T(0.5) * fma(b0[c], divB, advB[c]) - gb[c];
+        for (int l = 0; l < H; l++) {
+            r = fma(v(3 + c, l + 1), xp[l], r);
+            r = fma(v(3 + c, -l - 1), xm[l], r);
+        }
+        s[c] = r;
+    }
+    if constexpr (GRADB) {
+        auto e = [&](int, int t) -> T {
+            return (v(bo, t) * v(bo, t) + v(bo + 1, t) * v(bo + 1, t) + v(bo + 2, t) * v(bo + 2, t)) * T(0.5);
+        };
+        gb = d1<T, H>(e, 0, a);
+    }
 }
 
-template <typename T, int H, bool STRETCH, class VX, class VY, class VZ>
-__device__ __forceinline__ void mhd_b_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&b0)[3],
-                                          const T (&u0)[3], const Coef<T> &co, const T *az, const T *bz, T bsum,
-                                          T c2k, T visc, T (&rhs)[3])
+// PHYS_MHD_U (E = U, F = B) or PHYS_MHD_B (E = B, F = U); e0, f0 = E, F at the
+// node; iak, c2k the column's metric terms (as ns_rhs)
+template <typename T, int H, bool STRETCH, bool ULOOP, class VX, class VY, class VZ>
+__device__ __forceinline__ void mhd_rhs(const VX &vx, const VY &vy, const VZ &vz, const T (&e0)[3], const T (&f0)[3],
+                                        const Coef<T> &co, const StageCoef<T> &sc, T iak, T c2k, T visc,
+                                        T (&rhs)[3])
 {
-    T advUB[3] = {0, 0, 0}, advBU[3] = {0, 0, 0}, lap[3] = {0, 0, 0}, divU = 0, divB = 0;
-    T dbz[3] = {0, 0, 0};
-    auto dir = [&](const auto &v, int d, const T *a, const T *b, bool zdir) {
+    constexpr int uo = ULOOP ? 0 : 3, bo = ULOOP ? 3 : 0;
+    const T (&u0)[3] = ULOOP ? e0 : f0;
+    const T (&b0)[3] = ULOOP ? f0 : e0;
+    T s[3] = {0, 0, 0}, du = 0, db = 0, gb[3] = {0, 0, 0};
+    {
+        T vb[H];
+        const T viak = visc * iak;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            advUB[c] += adv1<T, H>(v, c, 3 + d, u0[d], a);
-            advBU[c] += adv1<T, H>(v, 3 + c, d, b0[d], a);
-            lap[c] += lsum<T, H>(v, c, b);
-            if (STRETCH && zdir) dbz[c] = d1<T, H>(v, c, a);
-        }
-        divU += d1<T, H>(v, 3 + d, a);
-        divB += d1<T, H>(v, d, a);
-    };
-    dir(vx, 0, co.a[0], co.b[0], false);
-    dir(vy, 1, co.a[1], co.b[1], false);
-    dir(vz, 2, az, bz, true);
+        for (int l = 0; l < H; l++) vb[l] = viak * co.b[2][l];
+        mhd_dir<T, H, ULOOP>(vz, 2, uo, bo, u0[2], b0[2], sc.ha[2], co.a[2], vb, s, du, db, gb[2]);
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-        rhs[c] = T(-0.5) * fma(b0[c], divU, advUB[c]) + T(0.5) * fma(u0[c], divB, advBU[c]) +
-                 visc * (fma(-bsum, b0[c], lap[c]) - c2k * dbz[c]);
+        for (int c = 0; c < 3; c++) s[c] *= iak;
+        du *= iak;
+        db *= iak;
+        gb[2] *= iak;
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = sc.vb[0][l];
+        mhd_dir<T, H, ULOOP>(vx, 0, uo, bo, u0[0], b0[0], sc.ha[0], co.a[0], vb, s, du, db, gb[0]);
+#pragma unroll
+        for (int l = 0; l < H; l++) vb[l] = sc.vb[1][l];
+        mhd_dir<T, H, ULOOP>(vy, 1, uo, bo, u0[1], b0[1], sc.ha[1], co.a[1], vb, s, du, db, gb[1]);
+    }
+    const T bsum = fma(co.b2[2], iak * iak, co.b2[0] + co.b2[1]);
+    const T K1 = fma(T(-0.5), du, -visc * bsum), K2 = T(0.5) * db;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        T r = fma(f0[c], K2, s[c]);
+        if constexpr (ULOOP) r -= gb[c];
+        if (STRETCH) r = fma(-visc * c2k, iak * d1<T, H>(vz, c, co.a[2]), r);
+        rhs[c] = fma(e0[c], K1, r);
+    }
 }
 
 // Stage update of one component at node o (classical RK4 of

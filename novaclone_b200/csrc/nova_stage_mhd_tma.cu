@@ -93,8 +93,8 @@ __device__ __forceinline__ void mhd_epi_read(const T *se, int c, T &e0, T &e1, T
 
 template <typename T, int PHYS, int STAGE, bool STRETCH, class Args>
 __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
-    k_mhd_tma(Geo g, Coef<T> co, const T *__restrict__ ia, const T *__restrict__ corr2, T dt, T visc, Args args,
-              const __grid_constant__ MhdMaps maps, int ichunk, int *err)
+    k_mhd_tma(Geo g, Coef<T> co, StageCoef<T> sc, const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
+              T visc, Args args, const __grid_constant__ MhdMaps maps, int ichunk, int *err)
 {
     using C = MhdCfg<T>;
     constexpr int H = kH, TJ = C::TJ, kRing = C::kRing, kERing = C::kERing;
@@ -195,13 +195,6 @@ __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
     };
     const int kw = k0 + tx;
     const T iak = ia[kw];
-    T az[H], bz[H];
-#pragma unroll
-    for (int l = 0; l < H; l++) {
-        az[l] = co.a[2][l] * iak;
-        bz[l] = co.b[2][l] * iak * iak;
-    }
-    const T bsum = co.b2[0] + co.b2[1] + co.b2[2] * iak * iak;
     const T c2k = STRETCH ? corr2[kw] : T(0);
 
     // slot offsets within a field: centre, and the k neighbour at s (inside the
@@ -255,10 +248,7 @@ __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
         const T y0[3] = {q[H][0], q[H][1], q[H][2]};
         const T x0[3] = {q[H][3], q[H][4], q[H][5]};
         T rhs[3];
-        if constexpr (PHYS == PHYS_MHD_U)
-            mhd_u_rhs<T, H, STRETCH>(vx, vy, vz, y0, x0, co, az, bz, bsum, c2k, visc, rhs);
-        else
-            mhd_b_rhs<T, H, STRETCH>(vx, vy, vz, y0, x0, co, az, bz, bsum, c2k, visc, rhs);
+        mhd_rhs<T, H, STRETCH, PHYS == PHYS_MHD_U>(vx, vy, vz, y0, x0, co, sc, iak, c2k, visc, rhs);
 
         T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
         if constexpr (NE > 0) {
@@ -361,7 +351,7 @@ cudaError_t launch_mhd(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     }
     const int ch = mhd_ichunk<T>(g);
     const dim3 grid(g.N2 / kTK, g.N1 / Cf::TJ, (g.N0 + ch - 1) / ch);
-    kern<<<grid, dim3(kTK, Cf::TJ + 1), smem, st>>>(g, co, ia, corr2, dt, visc, a, maps, ch, err);
+    kern<<<grid, dim3(kTK, Cf::TJ + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err);
     return cudaSuccess;
 }
 
