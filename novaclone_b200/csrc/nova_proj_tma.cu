@@ -38,7 +38,7 @@ enum ProjMode { PROJ_DIV = 0, PROJ_CORR = 1, PROJ_CORR_MIX = 2 };
 
 // map indices
 enum {
-    M_C0 = 0,   // DIV: component 0 tile (box 32 x TJ)
+    M_C0 = 0,   // DIV: component 0 tile (box 32 x TJ); CORR: p's tile rows (the queue-only planes)
     M_RA = 1,   // rows with j halos: TJ + 6, 3, TJ + 3 rows (DIV: component 1, CORR: p)
     M_R3 = 2,
     M_RB = 3,
@@ -143,8 +143,21 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int r = n % kRing;
             if (n >= kRing && !mbar_wait(empty(r), ((n / kRing) + 1) & 1, err)) return false;
             const uint32_t bar = full(r);
-            mbar_expect_tx(bar, C::kSlotBytes);
             const int plane = wrapi(ib - H + n, g.N0);
+            if (n < H || n >= H + nout) {
+                // a queue-only plane: the consumers read the i-stencil component's
+                // tile rows alone (DIV: component 0 at the set's start; CORR: p's
+                // rows at their place after the H halo rows)
+                mbar_expect_tx(bar, C::kSets * kTileE * sizeof(TS));
+#pragma unroll
+                for (int set = 0; set < C::kSets; set++) {
+                    const uint32_t dst = s0 + r * C::kSlotBytes + set * C::kSetE * sizeof(TS);
+                    tma_load_3d(C::kDivLoads ? dst : dst + H * kRowBytes, &maps.m[set * M_SET + M_C0], bar, k0, j0,
+                                plane);
+                }
+                return true;
+            }
+            mbar_expect_tx(bar, C::kSlotBytes);
 #pragma unroll
             for (int set = 0; set < C::kSets; set++) {
                 const uint32_t dst = s0 + r * C::kSlotBytes + set * C::kSetE * sizeof(TS);
@@ -326,14 +339,17 @@ template <typename T> bool encode_rows(ProjMaps &pm, int ms, const T *f, const G
            encode3(&pm.m[ms + M_RB], f, g, kTK, TJ + kH);
 }
 
-// i-chunk: >= ~2 waves of the 2 resident blocks per SM; longer chunks than the
-// stage kernel's carry fewer warm-up planes (whose whole slot is loaded for
-// the queue's component), measured 7% faster than 4 waves at 256^3
-int proj_ichunk(const Geo &g)
+// i-chunk: at least `waves` waves of the 2 resident blocks per SM.  The 2H
+// warm-up planes of a chunk load the queue's tile rows alone; for DIV that is
+// a third of the slot (component 0's tile is in every slot), so its longer
+// chunks (2 waves at 256^3) win, while the correction's p rows and halos make
+// shorter chunks with a smaller last wave pay (4 waves: 156 -> 146 us at 256^3,
+// DIV 115 -> 120 us)
+int proj_ichunk(const Geo &g, int waves)
 {
     const long long tiles = (long long)(g.N2 / kTK) * (g.N1 / TJ);
     int ch = g.N0;
-    while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * 2 * 2) ch /= 2;
+    while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * 2 * waves) ch /= 2;
     return ch;
 }
 
@@ -349,7 +365,7 @@ cudaError_t launch(const Geo &g, const Coef<double> &co, const double *ia, const
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         attr = true;
     }
-    const int ch = proj_ichunk(g);
+    const int ch = proj_ichunk(g, MODE == PROJ_DIV ? 2 : 4);
     const dim3 grid(g.N2 / kTK, g.N1 / TJ, (g.N0 + ch - 1) / ch);
     kern<<<grid, dim3(kTK, TJ + 1), C::kSmem, st>>>(g, co, ia, a, pm, ch, err);
     return cudaSuccess;
@@ -393,7 +409,7 @@ cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const doubl
     a.U64 = U64;
     a.hi = hi;
     a.lo = lo;
-    bool ok = encode_rows(pm, 0, p, g) && encode3(&pm.m[M_LR], p, g, 4, kLRB);
+    bool ok = encode_rows(pm, 0, p, g) && encode3(&pm.m[M_LR], p, g, 4, kLRB) && encode3(&pm.m[M_C0], p, g, kTK, TJ);
     if (Us64 && hi) {  // FP64 U*, FP32-split output
         ok = ok && encode4(&pm.m[M_EPI], Us64, g);
         if (!ok) return cudaErrorInvalidValue;

@@ -68,6 +68,7 @@ template <typename T, int NE> constexpr size_t mhd_smem_bytes()
 
 struct MhdMaps {
     CUtensorMap tcbA[2], tcb3[2], tcbB[2];  // halo'd rows of each field: TJ+6, 3 or TJ+3 rows
+    CUtensorMap tcbC[2];                    // each field's TJ tile rows alone (the queue-only planes)
     CUtensorMap lr[2];                      // k-halo boxes (4 x 8 x 3) of each field
     CUtensorMap e[3];                       // epilogue operands
 };
@@ -140,8 +141,17 @@ __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
             const int r = n % kRing;
             if (n >= kRing && !mbar_wait(empty(r), ((n / kRing) + 1) & 1, err)) return false;
             const uint32_t bar = full(r);
-            mbar_expect_tx(bar, kSlotBytes);
             const int plane = wrapi(ib - H + n, g.N0);
+            if (n < H || n >= H + nout) {
+                // a queue-only plane: the consumers read the tile rows' centre values alone
+                mbar_expect_tx(bar, 2 * TJ * kRowBytes);
+#pragma unroll
+                for (int f = 0; f < 2; f++)
+                    tma_load_4d(s0 + r * kSlotBytes + f * kFieldBytes + H * kRowBytes, &maps.tcbC[f], bar, k0, 0, j0,
+                                plane);
+                return true;
+            }
+            mbar_expect_tx(bar, kSlotBytes);
 #pragma unroll
             for (int f = 0; f < 2; f++) {
                 const uint32_t dst = s0 + r * kSlotBytes + f * kFieldBytes;
@@ -338,7 +348,8 @@ cudaError_t launch_mhd(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     bool ok = true;
     for (int f = 0; f < 2; f++)
         ok = ok && encode(&maps.tcbA[f], fld[f], g, Cf::TJ + 2 * kH) && encode(&maps.tcb3[f], fld[f], g, kH) &&
-             encode(&maps.tcbB[f], fld[f], g, Cf::TJ + kH) && encode(&maps.lr[f], fld[f], g, 0);
+             encode(&maps.tcbB[f], fld[f], g, Cf::TJ + kH) && encode(&maps.tcbC[f], fld[f], g, Cf::TJ) &&
+             encode(&maps.lr[f], fld[f], g, 0);
     for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, Cf::TJ);
     if (!ok) return cudaErrorInvalidValue;
     constexpr size_t smem = mhd_smem_bytes<T, NE>();

@@ -90,6 +90,7 @@ template <typename T, int NE, bool DIAG = false> constexpr size_t tma_smem_bytes
 
 struct StageMaps {
     CUtensorMap tcbA, tcb3, tcbB;  // halo'd rows of the stencil field: TJ+6, 3 or TJ+3 rows
+    CUtensorMap tcbC;              // its TJ tile rows alone (the queue-only planes)
     CUtensorMap lr;                // k-halo boxes (4 x 8 x 3) of the stencil field
     CUtensorMap e[3];              // epilogue operands
 };
@@ -168,8 +169,14 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             const int r = n % kRing;
             if (n >= kRing && !mbar_wait(empty(r), ((n / kRing) + 1) & 1, err)) return false;
             const uint32_t dst = s0 + r * kSlotBytes, bar = full(r);
-            mbar_expect_tx(bar, kSlotBytes);
             const int plane = wrapi(ib - H + n, g.N0);
+            if (n < H || n >= H + nout) {
+                // a queue-only plane: the consumers read the tile rows' centre values alone
+                mbar_expect_tx(bar, TJ * kRowBytes);
+                tma_load_4d(dst + H * kRowBytes, &maps.tcbC, bar, k0, 0, j0, plane);
+                return true;
+            }
+            mbar_expect_tx(bar, kSlotBytes);
             if (jlo) {
                 tma_load_4d(dst, &maps.tcb3, bar, k0, 0, g.N1 - H, plane);
                 tma_load_4d(dst + H * kRowBytes, &maps.tcbB, bar, k0, 0, 0, plane);
@@ -510,7 +517,7 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     memset(&maps, 0, sizeof maps);
     using Cf = TmaCfg<T>;
     bool ok = encode(&maps.tcbA, Y, g, Cf::TJ + 2 * kH) && encode(&maps.tcb3, Y, g, kH) &&
-              encode(&maps.tcbB, Y, g, Cf::TJ + kH) && encode(&maps.lr, Y, g, 0);
+              encode(&maps.tcbB, Y, g, Cf::TJ + kH) && encode(&maps.tcbC, Y, g, Cf::TJ) && encode(&maps.lr, Y, g, 0);
     for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, Cf::TJ);
     if (!ok) return cudaErrorInvalidValue;
     constexpr size_t smem = tma_smem_bytes<T, NE, DIAG>();
