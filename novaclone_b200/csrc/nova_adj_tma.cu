@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const double g0[3] = {q[kC][3], q[kC][4], q[kC][5]};
         double Sx[3], At[3], divP, divG;
         adj_terms<double, H, KIND == ADJ_UB>(vx, vy, vz, p0, g0, co, az, bz, kRec ? nu : 0.0, Sx, At, divP, divG);
+        release(empty(sCur));  // the slot's values are in registers
         constexpr double gs = S == 4 ? 1.0 / 6.0 : 1.0;  // g4 = mu / 6
         double r[3];
 #pragma unroll
@@ -240,6 +241,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 e0[c] = se[c * kTK];
                 if constexpr (NE > 1) e1[c] = se[kEpiE + c * kTK];
             }
+            release(eempty(es));
+            if (++es == kERing) {
+                es = 0;
+                eph ^= 1;
+            }
         } else {
 #pragma unroll
             for (int c = 0; c < 3; c++) e0[c] = g0[c];  // mu: the g field at s = 4
@@ -253,14 +259,6 @@ __global__ void __launch_bounds__(kThreads, 1)
             else
                 acc[o] = e0[e] + r[e];
         }
-        if constexpr (NE > 0) {
-            release(eempty(es));
-            if (++es == kERing) {
-                es = 0;
-                eph ^= 1;
-            }
-        }
-        release(empty(sCur));
         return true;
     };
     using I0 = std::integral_constant<int, 0>;

@@ -255,10 +255,12 @@ __global__ void __launch_bounds__(kThreads, 2)
         const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
         if constexpr (MODE == PROJ_DIV) {
             const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
+            release(empty(cur % kRing));  // the slot's values are in registers
             a.rhs[idx] = d / a.divisor;
         } else {
             const double gr[3] = {d1<double, H>(vx, 0, co.a[0]), d1<double, H>(vy, 0, co.a[1]),
                                   d1<double, H>(vz, 0, az)};
+            release(empty(cur % kRing));  // the slot's values are in registers
             ok = mbar_wait(efull(p % kERing), (p / kERing) & 1, err);
             if (!__all_sync(0xffffffffu, ok)) {
                 ok = false;
@@ -284,7 +286,6 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
         }
-        release(empty(cur % kRing));
     }
 }
 

@@ -259,6 +259,7 @@ __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
         const T x0[3] = {q[H][3], q[H][4], q[H][5]};
         T rhs[3];
         mhd_rhs<T, H, STRETCH, PHYS == PHYS_MHD_U>(vx, vy, vz, y0, x0, co, sc, iak, c2k, visc, rhs);
+        release(empty(cur % kRing));  // the slot's values are in registers
 
         T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
         if constexpr (NE > 0) {
@@ -270,6 +271,7 @@ __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
             const T *se = ering + (p % kERing) * NE * kEpiE + ty * kRowE + tx;
 #pragma unroll
             for (int c = 0; c < 3; c++) mhd_epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
+            release(eempty(p % kERing));
         }
         const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
 #pragma unroll
@@ -280,8 +282,6 @@ __global__ void __launch_bounds__(MhdCfg<T>::kThreads, 1)
             else
                 rk_store32<STAGE>(args, o, y0[c], e0[c], e1[c], lo[c], dt * rhs[c]);
         }
-        if constexpr (NE > 0) release(eempty(p % kERing));
-        release(empty(cur % kRing));
     }
 }
 

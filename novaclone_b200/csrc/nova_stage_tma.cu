@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                 curl_terms<H>(vx, vy, vz, 0, co.a[0], co.a[1], co.a[2], iak, q1, hs);
                 dacc.add(u0, divu, q1, hs);
             }
+            release(empty(cur % kRing));  // the slot's values are in registers
 
             T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
             if constexpr (NE > 0) {
@@ -306,6 +307,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                 const T *se = ering + (p % kERing) * NE * kEpiE + ty * kRowE + tx;
 #pragma unroll
                 for (int c = 0; c < 3; c++) epi_read<T, STAGE, kEpiE>(se, c, e0[c], e1[c], lo[c]);
+                release(eempty(p % kERing));
             }
             const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
 #pragma unroll
@@ -316,8 +318,6 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                 else
                     rk_store32<STAGE>(args, o, q[H][c], e0[c], e1[c], lo[c], dt * rhs[c]);
             }
-            if constexpr (NE > 0) release(eempty(p % kERing));
-            release(empty(cur % kRing));
         }
     } else {
         // FP32: warp ty computes tile rows 2 ty and 2 ty + 1 (one per half-warp),
@@ -381,6 +381,7 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             const float2 u0[3] = {q[kC][0], q[kC][1], q[kC][2]};
             float2 rhs[3];
             ns_rhs2<H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+            release(empty(sCur));  // the slot's values are in registers
 
             const float2 zz = f2(0.0f);
             float2 e0[3] = {zz, zz, zz}, e1[3] = {zz, zz, zz}, lo[3] = {zz, zz, zz};
@@ -401,20 +402,17 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                         lo[c] = ld2(se, o);
                     }
                 }
-            }
-            const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + r) * g.N2 + k0 + kk;
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-                rk_store32x2<STAGE>(args, (long long)c * g.N3 + idx, u0[c], e0[c], e1[c], lo[c],
-                                    mul2(f2(dt), rhs[c]));
-            if constexpr (NE > 0) {
                 release(eempty(es));
                 if (++es == kERing) {
                     es = 0;
                     eph ^= 1;
                 }
             }
-            release(empty(sCur));
+            const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + r) * g.N2 + k0 + kk;
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                rk_store32x2<STAGE>(args, (long long)c * g.N3 + idx, u0[c], e0[c], e1[c], lo[c],
+                                    mul2(f2(dt), rhs[c]));
             return true;
         };
         using I0 = std::integral_constant<int, 0>;
