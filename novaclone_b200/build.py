@@ -22,7 +22,8 @@ INCLUDE = os.path.join(ROOT, "include")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-SOURCES = ["nova_stage.cu", "nova_stage_tma.cu", "nova_stage_mhd_tma.cu", "nova_proj_tma.cu", "nova_ops.cu", "nova_pois_i.cu", "nova_fft2d.cu", "nova_adjoint.cu", "nova_adj_tma.cu", "nova_wc.cu", "nova_io.cu", "nova_im.cu", "nova_capi.cu"]
+SOURCES = ["nova_stage.cu", "nova_stage_tma.cu", "nova_stage_mhd_tma.cu", "nova_proj_tma.cu", "nova_ops.cu", "nova_pois_i.cu",
+    "nova_pois_dct.cu", "nova_fft2d.cu", "nova_adjoint.cu", "nova_adj_tma.cu", "nova_wc.cu", "nova_io.cu", "nova_im.cu", "nova_capi.cu"]
 HEADERS = ["nova_internal.cuh", "nova_ops.cuh", "nova_tile.cuh", "nova_stage_math.cuh", "nova_tma.cuh", "nova_adj_math.cuh", "nova_wc.cuh", "nova_mesh.cuh", "nova_diag.cuh", "nova_fft.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-diag-suppress", "177", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]

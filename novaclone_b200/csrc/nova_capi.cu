@@ -73,6 +73,13 @@ struct nova_ctx {
     bool dct_plans = false;
     double *d_ext = nullptr, *d_ky2e = nullptr;
     void *d_spec2 = nullptr;
+    // wall Poisson with N[1] = 256: batched 2-D (i, k) transforms of the stored
+    // rows and k_pois_dct (DCT-I along y); NOVA_DCT=extend keeps the even extension
+    cufftHandle dct2_f = 0, dct2_b = 0;
+    bool dct2_plans = false;
+    bool dct_extend = false;
+    void *d_spec3 = nullptr;
+    double *d_t512 = nullptr;
     void *d_spec = nullptr;
     double *d_rhs = nullptr;
     double *w64[3] = {nullptr, nullptr, nullptr};
@@ -413,6 +420,63 @@ nova_status poisson_device(nova_ctx *ctx, const double *rhs, double *p)
     return NOVA_OK;
 }
 
+// the y modified wavenumbers of the wall solve: period 2 L_y on 2 N[1] points
+// (the even extension's), folded
+std::vector<double> ky2_walls(const nova_ctx *ctx)
+{
+    const int ny = ctx->md.N[1];
+    const double *c = kCoef[(ctx->md.m - 2) / 2];
+    return kp2_table(2 * ny, 2.0 * ctx->md.L[1], ctx->md.L[1] / ny, ctx->h, c, true, 2 * ny);
+}
+
+// the wall Poisson with DCT-I along y on the N[1] + 1 stored rows (N[1] = 256):
+// batched 2-D D2Z over (i, k), k_pois_dct (DCT-I, scale, DCT-I), 2-D Z2D
+nova_status poisson_device_dct1(nova_ctx *ctx, const double *rhs, double *p)
+{
+    const Geo &g = ctx->g;
+    const int ny = ctx->md.N[1], nzh = g.N2 / 2 + 1;
+    nova_status s;
+    if (!ctx->dct2_plans) {
+        // element (i, j, k) of a batch-j plane at j N2 + i N1 N2 + k; spectrum at (i N1 + j) nzh + kz
+        int n[2] = {g.N0, g.N2}, rin[2] = {g.N0, (int)g.N12}, cin[2] = {g.N0, g.N1 * nzh};
+        if ((s = fft_check(ctx, cufftPlanMany(&ctx->dct2_f, 2, n, rin, 1, g.N2, cin, 1, nzh, CUFFT_D2Z, g.N1),
+                           "cufftPlanMany D2Z (walls, DCT)")) != NOVA_OK)
+            return s;
+        if ((s = fft_check(ctx, cufftPlanMany(&ctx->dct2_b, 2, n, cin, 1, nzh, rin, 1, g.N2, CUFFT_Z2D, g.N1),
+                           "cufftPlanMany Z2D (walls, DCT)")) != NOVA_OK) {
+            cufftDestroy(ctx->dct2_f);
+            return s;
+        }
+        ctx->dct2_plans = true;
+        if ((s = dalloc(ctx, (double **)&ctx->d_spec3, 2 * (size_t)g.N0 * g.N1 * nzh)) != NOVA_OK) return s;
+        const std::vector<double> t256 = twiddles(256), t512 = twiddles(512), ky2e = ky2_walls(ctx);
+        if (!ctx->d_tw256) {
+            if ((s = dalloc(ctx, &ctx->d_tw256, t256.size())) != NOVA_OK) return s;
+            CK(cudaMemcpy(ctx->d_tw256, t256.data(), sizeof(double) * t256.size(), cudaMemcpyHostToDevice));
+        }
+        if ((s = dalloc(ctx, &ctx->d_t512, 512)) != NOVA_OK) return s;  // W_512^n, n < 256
+        CK(cudaMemcpy(ctx->d_t512, t512.data(), sizeof(double) * 512, cudaMemcpyHostToDevice));
+        if (!ctx->d_ky2e) {
+            if ((s = dalloc(ctx, &ctx->d_ky2e, ky2e.size())) != NOVA_OK) return s;
+            CK(cudaMemcpy(ctx->d_ky2e, ky2e.data(), sizeof(double) * ky2e.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    ProfScope ps(ctx, NOVA_K_FFT);
+    cufftSetStream(ctx->dct2_f, ctx->stream);
+    cufftSetStream(ctx->dct2_b, ctx->stream);
+    if ((s = fft_check(ctx, cufftExecD2Z(ctx->dct2_f, const_cast<double *>(rhs), (cufftDoubleComplex *)ctx->d_spec3),
+                       "cufftExecD2Z")) != NOVA_OK)
+        return s;
+    launch_pois_dct(g, ctx->d_spec3, ctx->d_tw256, ctx->d_t512, ctx->d_kx2, ctx->d_ky2e, ctx->d_kz2,
+                    1.0 / ((double)g.N0 * 2.0 * ny * g.N2), ctx->stream);
+    if ((s = fft_check(ctx, cufftExecZ2D(ctx->dct2_b, (cufftDoubleComplex *)ctx->d_spec3, p), "cufftExecZ2D")) !=
+        NOVA_OK)
+        return s;
+    ctx->launches += 1;
+    CKL("wall poisson (DCT-I)");
+    return NOVA_OK;
+}
+
 // the wall Poisson of NOVA_POISSON_DCT: even extension in y, periodic solve on
 // the doubled domain (modified wavenumbers of period 2 L_y), restriction to
 // the stored rows
@@ -421,6 +485,7 @@ nova_status poisson_device_dct(nova_ctx *ctx, const double *rhs, double *p)
     const Geo &g = ctx->g;
     const int ny = ctx->md.N[1];
     nova_status s;
+    if (!ctx->dct_extend && pois_dct_fits(g, ny)) return poisson_device_dct1(ctx, rhs, p);
     if (!ctx->dct_plans) {
         if ((s = fft_check(ctx, cufftPlan3d(&ctx->dct_f, g.N0, 2 * ny, g.N2, CUFFT_D2Z), "cufftPlan3d D2Z (walls)")) !=
             NOVA_OK)
@@ -434,9 +499,7 @@ nova_status poisson_device_dct(nova_ctx *ctx, const double *rhs, double *p)
         const size_t next = (size_t)g.N0 * 2 * ny * g.N2;
         if ((s = dalloc(ctx, &ctx->d_ext, next)) != NOVA_OK) return s;
         if ((s = dalloc(ctx, (double **)&ctx->d_spec2, 2 * (size_t)g.N0 * 2 * ny * (g.N2 / 2 + 1))) != NOVA_OK) return s;
-        const double *c = kCoef[(ctx->md.m - 2) / 2];
-        const double dy = ctx->md.L[1] / ny;
-        std::vector<double> ky2e = kp2_table(2 * ny, 2.0 * ctx->md.L[1], dy, ctx->h, c, true, 2 * ny);
+        const std::vector<double> ky2e = ky2_walls(ctx);
         if ((s = dalloc(ctx, &ctx->d_ky2e, ky2e.size())) != NOVA_OK) return s;
         CK(cudaMemcpy(ctx->d_ky2e, ky2e.data(), sizeof(double) * ky2e.size(), cudaMemcpyHostToDevice));
     }
@@ -504,6 +567,7 @@ extern "C" nova_status nova_create(const nova_mesh_desc *md, nova_ctx **out)
     }
     if (const char *f = std::getenv("NOVA_FFT")) ctx->fft_cluster = !std::strcmp(f, "cluster");
     if (const char *f = std::getenv("NOVA_POIS_I")) ctx->pois_direct = !std::strcmp(f, "direct");
+    if (const char *f = std::getenv("NOVA_DCT")) ctx->dct_extend = !std::strcmp(f, "extend");
     for (int a = 0; a < 3; a++) ctx->local_n[a] = md->N[a] + 1 + md->m;
     Geo &g = ctx->g;
     g.wallY = md->walls[1];
@@ -585,9 +649,14 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
         cufftDestroy(ctx->dct_f);
         cufftDestroy(ctx->dct_b);
     }
+    if (ctx->dct2_plans) {
+        cufftDestroy(ctx->dct2_f);
+        cufftDestroy(ctx->dct2_b);
+    }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->w32x, ctx->d_tw256};
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->w32x, ctx->d_tw256,
+                    ctx->d_spec3, ctx->d_t512};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -42,6 +42,16 @@ bool pois_i_fits(const Geo &g);
 bool fft2_fits(const Geo &g);
 void launch_fft2_fwd(const Geo &g, const double *x, void *spec, const double *tw256, cudaStream_t st);
 void launch_fft2_inv(const Geo &g, const void *spec, double *x, const double *tw256, cudaStream_t st);
+// the wall Poisson's y direction in DCT mode (nova_pois_dct.cu): in place on
+// the half spectrum [i][j][kz] (j = 0..256) of the batched 2-D (i, k) D2Z of
+// the stored rows, per (i, kz) column DCT-I along j, the scale
+// -invN3 / (kx'^2 + ky'^2 + kz'^2) (ky2e: the even extension's table) and
+// DCT-I back; walls in y with N[1] = 256, N2 % 16 == 0, N0 % 8 == 0.
+// tw256 = W_256^m, t512 = W_512^n (n < 256), interleaved (re, im)
+bool pois_dct_fits(const Geo &g, int ny);
+void launch_pois_dct(const Geo &g, void *spec, const double *tw256, const double *t512, const double *kx2,
+                     const double *ky2e, const double *kz2, double invN3, cudaStream_t st);
+
 // err: the pipeline's error word (a bounded wait that gives up raises it);
 // null runs the register kernel k_pois_i, else N0 = 256 meshes with
 // N2 % 16 == 0 and N1 % 8 == 0 run the TMA-fed k_pois_tma

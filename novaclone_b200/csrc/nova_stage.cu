@@ -77,18 +77,21 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
     for (int c = 0; c < NC; c++) src[c] = ((c < 3) ? args.Y : args.X) + (long long)(c % 3) * g.N3;
 
     // pointwise epilogue operands (base, accumulator): prefetched one plane
-    // ahead in FP64; the FP32 kernels load them at the start of the plane
-    // (measured faster there: fewer live registers)
+    // ahead in FP64 and in the FP32 shear-layer stage (5: base hi and lo, the
+    // latter in the accumulator's place); the other FP32 stages load them at
+    // the start of the plane (measured faster there: fewer live registers)
+    constexpr bool kSplit5 = !std::is_same<T, double>::value && STAGE == 5;
     constexpr bool kE0 = (STAGE == 1 || STAGE == 2 || STAGE == 5) || (!std::is_same<T, double>::value && STAGE == 3);
-    constexpr bool kE1 = (STAGE >= 1 && STAGE <= 3);
-    constexpr bool kAhead = std::is_same<T, double>::value;
+    constexpr bool kE1 = (STAGE >= 1 && STAGE <= 3) || kSplit5;
+    constexpr bool kAhead = std::is_same<T, double>::value || kSplit5;
     const T *e0p = nullptr, *e1p = nullptr;
     if constexpr (std::is_same<T, double>::value) {
         e0p = args.U0;
+        e1p = args.A;
     } else {
         e0p = args.U0hi;
+        e1p = kSplit5 ? args.U0lo : args.A;
     }
-    e1p = args.A;
     T e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0}, e0n[3] = {0, 0, 0}, e1n[3] = {0, 0, 0};
     auto pre = [&](long long nidx, bool load) {
         if constexpr (kAhead) {
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, (stage_minb<T, PHYS>())) k_stage(Geo
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const long long o = (long long)c * g.N3 + idx;
-                    const float lo = (STAGE >= 3) ? args.U0lo[o] : 0.0f;
+                    const float lo = kSplit5 ? e1[c] : ((STAGE >= 3) ? args.U0lo[o] : 0.0f);
                     rk_store32<STAGE>(args, o, q[H][c], e0[c], e1[c], lo, dt * rhs[c]);
                 }
             }
