@@ -376,7 +376,7 @@ nova_status stage_fail(nova_ctx *ctx, cudaError_t e)
 {
     if (e == cudaErrorNotSupported)
         return fail(ctx, NOVA_E_UNSUPPORTED,
-                    "NOVA_STAGE_IMPL=tma: the TMA stage kernel needs periodic y, N2 % 32 == 0 and N1 a multiple of 16 (FP64) or 8 (FP32), at least twice that");
+                    "NOVA_STAGE_IMPL=tma: the TMA stage kernel needs N2 % 32 == 0 and N1 at least twice the tile height (16 rows FP64, 8 FP32), with periodic y a multiple of it; walls in y only in FP32");
     if (e == cudaErrorInvalidValue) return fail(ctx, NOVA_E_CUDA, "stage kernel: cuTensorMapEncodeTiled failed");
     return cuda_check(ctx, e, "stage kernel");
 }

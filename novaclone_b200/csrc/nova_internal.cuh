@@ -246,9 +246,9 @@ void launch_dot(long long n, const double *x, const double *y, double scale, dou
                 cudaStream_t st);
 
 // Which kernel runs the Navier-Stokes stage: STAGE_AUTO = the TMA pipeline
-// (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits: periodic y,
-// N2 % 32 == 0, N1 a multiple of the tile height 16 (FP64) or 8 (FP32) and
-// at least twice it), else the
+// (nova_stage_tma.cu) where the mesh fits it (stage_tma_fits: N2 % 32 == 0,
+// N1 at least twice the tile height 16 (FP64) or 8 (FP32), and with periodic y
+// a multiple of it; FP32 walls in y take ragged last tiles), else the
 // register-queue march (nova_stage.cu); STAGE_MARCH / STAGE_TMA force one
 // (STAGE_TMA on a mesh that does not fit is an error).  err: device word
 // raised by a pipeline wait that timed out.
@@ -294,10 +294,9 @@ struct StageDiag {
     int *flag;
     DiagFinal fin;
 };
-cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
-                               const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
-                               cudaStream_t st, const StageDiag *dg = nullptr,
-                               bool *dg_done = nullptr);
+cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Walls<double> &wl, const Coef<double> &co,
+                               const double *ia, const double *corr2, double dt, double visc, const StageArgs64 &a,
+                               int *err, cudaStream_t st, const StageDiag *dg = nullptr, bool *dg_done = nullptr);
 // MHD stage kernels on the TMA pipeline (nova_stage_mhd_tma.cu): periodic y,
 // N2 % 32 == 0, N1 a multiple of the tile height 8 (FP64) or 16 (FP32) and at
 // least twice it; a.X is the frozen field
@@ -308,13 +307,12 @@ cudaError_t launch_mhd_tma64(int phys, int stage, bool stretch, const Geo &g, co
 cudaError_t launch_mhd_tma32(int phys, int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
                              const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
                              cudaStream_t st);
-cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
-                               const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
-                               cudaStream_t st);
+cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Walls<float> &wl, const Coef<float> &co,
+                               const float *ia, const float *corr2, float dt, float visc, const StageArgs32 &a,
+                               int *err, cudaStream_t st);
 
 // stage: 0..3 classical RK4 stages, 4 = literal reference loop (one RHS, 4-term sum),
-// 5 = the shear-layer loop's stage U* = U0 + w dU (app/shearLayer/UEqn.H:28-29;
-// always the register-queue march)
+// 5 = the shear-layer loop's stage U* = U0 + w dU (app/shearLayer/UEqn.H:28-29)
 // stretch: apply the stretched-z Laplacian term (Mesh "hypz:"); on uniform
 // meshes d2zdxi2 is round-off (|.| < 1e-9) and the term is skipped
 // Returns cudaErrorNotSupported when STAGE_TMA is forced on a mesh it does not

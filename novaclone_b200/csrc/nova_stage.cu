@@ -211,11 +211,11 @@ cudaError_t launch_stage64(int phys, int stage, bool stretch, const Geo &g, cons
                            const StageArgs64 &a, cudaStream_t st, const StageExec &ex, const StageDiag *dg,
                            bool *dg_done)
 {
-    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage <= 4 && stage_tma_fits(g, true))
-        return launch_stage_tma64(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st, dg, dg_done);
+    if (phys == PHYS_NS && ex.impl != STAGE_MARCH && ex.err && stage_tma_fits(g, true))
+        return launch_stage_tma64(stage, stretch, g, wl, co, ia, corr2, dt, visc, a, ex.err, st, dg, dg_done);
     if (phys != PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && ex.err && stage <= 4 && mhd_tma_fits(g, true))
         return launch_mhd_tma64(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
-    if (ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
+    if (ex.impl == STAGE_TMA && (phys == PHYS_NS || stage <= 4)) return cudaErrorNotSupported;
     launch_stage_any<double>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;
 }
@@ -224,11 +224,11 @@ cudaError_t launch_stage32(int phys, int stage, bool stretch, const Geo &g, cons
                            const Coef<float> &co, const float *ia, const float *corr2, float dt, float visc,
                            const StageArgs32 &a, cudaStream_t st, const StageExec &ex)
 {
-    if (phys == PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && stage <= 4 && stage_tma_fits(g, false))
-        return launch_stage_tma32(stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
+    if (phys == PHYS_NS && ex.impl != STAGE_MARCH && ex.err && stage_tma_fits(g, false))
+        return launch_stage_tma32(stage, stretch, g, wl, co, ia, corr2, dt, visc, a, ex.err, st);
     if (phys != PHYS_NS && !wl.on && ex.impl != STAGE_MARCH && ex.err && stage <= 4 && mhd_tma_fits(g, false))
         return launch_mhd_tma32(phys, stage, stretch, g, co, ia, corr2, dt, visc, a, ex.err, st);
-    if (ex.impl == STAGE_TMA && stage <= 4) return cudaErrorNotSupported;
+    if (ex.impl == STAGE_TMA && (phys == PHYS_NS || stage <= 4)) return cudaErrorNotSupported;
     launch_stage_any<float>(phys, stage, stretch, g, wl, co, ia, corr2, dt, visc, a, st);
     return cudaSuccess;
 }

@@ -371,14 +371,16 @@ __device__ __forceinline__ void store_split2(const StageArgs32 &a, long long o, 
     st2(a.outlo + o, make_float2((float)(x0 - (double)h0), (float)(x1 - (double)h1)));
 }
 
-// rk_store32 for the pair of nodes o, o + 1 (stages 0-4)
+// rk_store32 for the pair of nodes o, o + 1
 template <int STAGE>
 __device__ __forceinline__ void rk_store32x2(const StageArgs32 &a, long long o, float2 y0, float2 e0, float2 e1,
                                              float2 lo, float2 du)
 {
-    static_assert(STAGE >= 0 && STAGE <= 4, "stages 0-4");
+    static_assert(STAGE >= 0 && STAGE <= 5, "stages 0-5");
     const float2 w6 = f2(1.0f / 6.0f), w3 = f2(1.0f / 3.0f), h = f2(0.5f);
-    if constexpr (STAGE == 4) {
+    if constexpr (STAGE == 5) {
+        store_split2(a, o, e0, lo, mul2(du, f2(a.w)));
+    } else if constexpr (STAGE == 4) {
         store_split2(a, o, y0, lo, fma2(du, w6, fma2(du, w3, fma2(du, w3, mul2(du, w6)))));
     } else if constexpr (STAGE == 0) {
         st2(a.Ynext + o, fma2(du, h, y0));

@@ -68,14 +68,14 @@ template <typename T> struct TmaCfg {
 };
 
 // epilogue operands per stage, in load order
-//   FP64:  s=1,2: U0, A   s=3: A
-//   split: s=1,2: U0hi, A   s=3: U0hi, A, U0lo   s=4: U0lo
+//   FP64:  s=1,2: U0, A   s=3: A   s=5: U0
+//   split: s=1,2: U0hi, A   s=3: U0hi, A, U0lo   s=4: U0lo   s=5: U0hi, U0lo
 template <typename T, int STAGE> __host__ __device__ constexpr int epi_fields()
 {
     if constexpr (sizeof(T) == 8)
-        return (STAGE == 1 || STAGE == 2) ? 2 : (STAGE == 3 ? 1 : 0);
+        return (STAGE == 1 || STAGE == 2) ? 2 : ((STAGE == 3 || STAGE == 5) ? 1 : 0);
     else
-        return (STAGE == 1 || STAGE == 2) ? 2 : (STAGE == 3 ? 3 : (STAGE == 4 ? 1 : 0));
+        return (STAGE == 1 || STAGE == 2 || STAGE == 5) ? 2 : (STAGE == 3 ? 3 : (STAGE == 4 ? 1 : 0));
 }
 
 // ring data, the ring barriers, then (DIAG launches) kDiagParts doubles per
@@ -111,6 +111,8 @@ __device__ __forceinline__ void epi_read(const T *se, int c, T &e0, T &e1, T &lo
         }
     } else if constexpr (STAGE == 4 && sizeof(T) == 4) {
         lo = se[c * kTK];
+    } else if constexpr (STAGE == 5 && sizeof(T) == 8) {
+        e0 = se[c * kTK];
     }
 }
 
@@ -118,13 +120,22 @@ __device__ __forceinline__ void epi_read(const T *se, int c, T &e0, T &e1, T &lo
 // periodic mesh): the block also reduces the history row's terms of U over its
 // nodes (nova_diag.cuh: energy, |U|, U_x, the divergence the stage arithmetic
 // forms anyway, and the two curls from the stencil values it holds) into
-// dpart[block * kDiagParts] (the B terms zero)
-template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG>
+// dpart[block * kDiagParts] (the B terms zero).
+// WALLS (FP32, walls on the y nodes j = 0 and j = N1 - 1): one row box per
+// plane from j0 - H (the bulk copy fills rows outside 0..N1-1 with zeros, the
+// last tile may be ragged); in a warp with a row within H of a wall, a valid
+// row's j neighbour across the wall is the wall_ghost of its mirror row (the
+// march's formula); rows past N1 - 1 compute but store nothing.  (FP64 wall
+// stages stay on the march: at 96 registers a thread the ghost branch spills.)
+template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG, bool WALLS = false>
 __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
-    k_stage_tma(Geo g, Coef<T> co, StageCoef<T> sc, const T *__restrict__ ia, const T *__restrict__ corr2, T dt,
-                T visc, Args args, const __grid_constant__ StageMaps maps, int ichunk, int *err, double *dpart)
+    k_stage_tma(Geo g, Coef<T> co, StageCoef<T> sc, const Walls<T> wl, const T *__restrict__ ia,
+                const T *__restrict__ corr2, T dt, T visc, Args args, const __grid_constant__ StageMaps maps,
+                int ichunk, int *err, double *dpart)
 {
     static_assert(!DIAG || (sizeof(T) == 8 && (STAGE == 0 || STAGE == 4)), "diagnostics of an FP64 state only");
+    static_assert(!(DIAG && WALLS), "diagnostics on periodic meshes");
+    static_assert(!WALLS || sizeof(T) == 4, "FP64 wall stages run the register-queue march");
     using C = TmaCfg<T>;
     constexpr int H = kH, TJ = C::TJ, kRing = C::kRing, kERing = C::kERing;
     constexpr int kTcbE = C::kTcbE, kLRE = C::kLRE, kSlotE = C::kSlotE, kEpiE = C::kEpiE;
@@ -177,7 +188,9 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                 return true;
             }
             mbar_expect_tx(bar, kSlotBytes);
-            if (jlo) {
+            if (WALLS) {
+                tma_load_4d(dst, &maps.tcbA, bar, k0, 0, j0 - H, plane);
+            } else if (jlo) {
                 tma_load_4d(dst, &maps.tcb3, bar, k0, 0, g.N1 - H, plane);
                 tma_load_4d(dst + H * kRowBytes, &maps.tcbB, bar, k0, 0, 0, plane);
             } else if (jhi) {
@@ -327,6 +340,11 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
         static_assert(2 * C::kWarps == TJ, "two tile rows per consumer warp");
         const int r = 2 * ty + (lane >> 4), kk = 2 * (lane & 15);
         const int cen = (H + r) * kRowE + kk;
+        const int jrow = j0 + r;
+        // the rows next to a wall take the j neighbours across it from ghosts
+        // (the choice is made per warp: its two rows together)
+        const bool nearw =
+            WALLS && __any_sync(0xffffffffu, jrow < g.N1 && (jrow < H || jrow + H > g.N1 - 1));
         // the z neighbours' pairs starting at kk - 4, kk - 2, kk + 2, kk + 4
         const int zm4 = soff(r, kk - 4), zm2 = soff(r, kk - 2), zp2 = soff(r, kk + 2), zp4 = soff(r, kk + 4);
         const float2 iak = *reinterpret_cast<const float2 *>(ia + k0 + kk);
@@ -365,6 +383,16 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             constexpr int kC = (R + H) % (2 * H + 1);
             auto vx = [&](int c, int s) -> float2 { return q[(R + H + s + 2 * H + 1) % (2 * H + 1)][c]; };
             auto vy = [&](int c, int s) -> float2 { return ld2(sl, cen + s * kRowE + c * kTK); };
+            auto vyg = [&](int c, int s) -> float2 {
+                const int jj = jrow + s;
+                if (jrow < g.N1 && (jj < 0 || jj > g.N1 - 1)) {
+                    const int side = jj < 0 ? 0 : 1, l = jj < 0 ? -jj : jj - (g.N1 - 1);
+                    const int jm = jj < 0 ? l : g.N1 - 1 - l;  // the mirror row, inside the slot
+                    const float2 f = ld2(sl, cen + (jm - jrow) * kRowE + c * kTK);
+                    return make_float2(wall_ghost(wl, side, c, l, f.x), wall_ghost(wl, side, c, l, f.y));
+                }
+                return ld2(sl, cen + s * kRowE + c * kTK);
+            };
             // odd offsets straddle two loaded pairs (the centre pair is the queue's)
             auto vz = [&](int c, int s) -> float2 {
                 const int o = c * kTK;
@@ -380,7 +408,10 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
             };
             const float2 u0[3] = {q[kC][0], q[kC][1], q[kC][2]};
             float2 rhs[3];
-            ns_rhs2<H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
+            if (WALLS && nearw)
+                ns_rhs2<H, STRETCH>(vx, vyg, vz, u0, co, sc, iak, c2k, visc, rhs);
+            else
+                ns_rhs2<H, STRETCH>(vx, vy, vz, u0, co, sc, iak, c2k, visc, rhs);
             release(empty(sCur));  // the slot's values are in registers
 
             const float2 zz = f2(0.0f);
@@ -400,6 +431,9 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                         lo[c] = ld2(se, 2 * kEpiE + o);
                     } else if constexpr (STAGE == 4) {
                         lo[c] = ld2(se, o);
+                    } else if constexpr (STAGE == 5) {
+                        e0[c] = ld2(se, o);
+                        lo[c] = ld2(se, kEpiE + o);
                     }
                 }
                 release(eempty(es));
@@ -409,10 +443,12 @@ __global__ void __launch_bounds__(TmaCfg<T>::kThreads, TmaCfg<T>::kBlocksPerSM)
                 }
             }
             const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + r) * g.N2 + k0 + kk;
+            if (!WALLS || jrow < g.N1) {
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-                rk_store32x2<STAGE>(args, (long long)c * g.N3 + idx, u0[c], e0[c], e1[c], lo[c],
-                                    mul2(f2(dt), rhs[c]));
+                for (int c = 0; c < 3; c++)
+                    rk_store32x2<STAGE>(args, (long long)c * g.N3 + idx, u0[c], e0[c], e1[c], lo[c],
+                                        mul2(f2(dt), rhs[c]));
+            }
             return true;
         };
         using I0 = std::integral_constant<int, 0>;
@@ -500,15 +536,16 @@ template <typename T> bool encode(CUtensorMap *m, const T *base, const Geo &g, u
 template <typename T> int tma_ichunk(const Geo &g)
 {
     using C = TmaCfg<T>;
-    const long long tiles = (long long)(g.N2 / kTK) * (g.N1 / C::TJ);
+    const long long tiles = (long long)(g.N2 / kTK) * ((g.N1 + C::TJ - 1) / C::TJ);
     int ch = g.N0;
     while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * C::kBlocksPerSM * 4) ch /= 2;
     return ch;
 }
 
-template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG = false>
+template <typename T, int STAGE, bool STRETCH, class Args, bool DIAG = false, bool WALLS = false>
 cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc, const Args &a,
-                       const T *Y, const T *const *ef, int *err, cudaStream_t st, double *dpart = nullptr)
+                       const T *Y, const T *const *ef, int *err, cudaStream_t st, double *dpart = nullptr,
+                       const Walls<T> &wl = Walls<T>{})
 {
     constexpr int NE = epi_fields<T, STAGE>();
     StageMaps maps;
@@ -519,7 +556,7 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
     for (int f = 0; f < NE; f++) ok = ok && encode(&maps.e[f], ef[f], g, Cf::TJ);
     if (!ok) return cudaErrorInvalidValue;
     constexpr size_t smem = tma_smem_bytes<T, NE, DIAG>();
-    auto kern = k_stage_tma<T, STAGE, STRETCH, Args, DIAG>;
+    auto kern = k_stage_tma<T, STAGE, STRETCH, Args, DIAG, WALLS>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -527,23 +564,41 @@ cudaError_t launch_tma(const Geo &g, const Coef<T> &co, const T *ia, const T *co
         attr = true;
     }
     const int ch = tma_ichunk<T>(g);
-    const dim3 grid(g.N2 / kTK, g.N1 / Cf::TJ, (g.N0 + ch - 1) / ch);
-    kern<<<grid, dim3(kTK, Cf::kWarps + 1), smem, st>>>(g, co, stage_coef(co, visc), ia, corr2, dt, visc, a, maps, ch, err,
-                                                     dpart);
+    const dim3 grid(g.N2 / kTK, (g.N1 + Cf::TJ - 1) / Cf::TJ, (g.N0 + ch - 1) / ch);
+    kern<<<grid, dim3(kTK, Cf::kWarps + 1), smem, st>>>(g, co, stage_coef(co, visc), wl, ia, corr2, dt, visc, a, maps,
+                                                     ch, err, dpart);
     return cudaSuccess;
 }
 
-template <typename T, bool STRETCH, class Args>
-cudaError_t launch_tma_stage(int stage, const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
-                             const Args &a, const T *const *ef, int *err, cudaStream_t st)
+template <typename T, bool STRETCH, class Args, bool WALLS>
+cudaError_t launch_tma_stage_w(int stage, const Geo &g, const Coef<T> &co, const T *ia, const T *corr2, T dt, T visc,
+                               const Args &a, const T *const *ef, int *err, cudaStream_t st, const Walls<T> &wl)
 {
     switch (stage) {
-    case 0: return launch_tma<T, 0, STRETCH>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st);
-    case 1: return launch_tma<T, 1, STRETCH>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st);
-    case 2: return launch_tma<T, 2, STRETCH>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st);
-    case 3: return launch_tma<T, 3, STRETCH>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st);
-    default: return launch_tma<T, 4, STRETCH>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st);
+    case 0: return launch_tma<T, 0, STRETCH, Args, false, WALLS>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st, nullptr, wl);
+    case 1: return launch_tma<T, 1, STRETCH, Args, false, WALLS>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st, nullptr, wl);
+    case 2: return launch_tma<T, 2, STRETCH, Args, false, WALLS>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st, nullptr, wl);
+    case 3: return launch_tma<T, 3, STRETCH, Args, false, WALLS>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st, nullptr, wl);
+    case 5: return launch_tma<T, 5, STRETCH, Args, false, WALLS>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st, nullptr, wl);
+    default: return launch_tma<T, 4, STRETCH, Args, false, WALLS>(g, co, ia, corr2, dt, visc, a, a.Y, ef, err, st, nullptr, wl);
     }
+}
+
+template <typename T, class Args>
+cudaError_t launch_tma_stage(int stage, bool stretch, const Geo &g, const Coef<T> &co, const T *ia, const T *corr2,
+                             T dt, T visc, const Args &a, const T *const *ef, int *err, cudaStream_t st,
+                             const Walls<T> &wl)
+{
+    if constexpr (sizeof(T) == 4) {
+        if (wl.on)
+            return stretch
+                       ? launch_tma_stage_w<T, true, Args, true>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st, wl)
+                       : launch_tma_stage_w<T, false, Args, true>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st, wl);
+    } else {
+        if (wl.on) return cudaErrorNotSupported;
+    }
+    return stretch ? launch_tma_stage_w<T, true, Args, false>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st, wl)
+                   : launch_tma_stage_w<T, false, Args, false>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st, wl);
 }
 
 }  // namespace
@@ -555,16 +610,19 @@ bool tma_encode_field(CUtensorMap *m, const double *base, const Geo &g, unsigned
 
 bool stage_tma_fits(const Geo &g, bool fp64)
 {
-    // tile width divides N2 (k halo boxes start at a wrapped column), tile
-    // height (16 rows for FP64, 8 for FP32) divides N1 with at most one wrap
-    // per tile in j, periodic y
+    // tile width divides N2 (k halo boxes start at a wrapped column); periodic
+    // y: the tile height (16 rows for FP64, 8 for FP32) divides N1 with at
+    // most one wrap per tile in j; walls in y (FP32 only: the FP64 wall
+    // stages run faster on the march): any N1 of at least two tiles (the
+    // last tile may be ragged)
     const int tj = fp64 ? TmaCfg<double>::TJ : TmaCfg<float>::TJ;
-    return !g.wallY && g.N2 % kTK == 0 && g.N1 % tj == 0 && g.N1 >= 2 * tj;
+    if (g.wallY && fp64) return false;
+    return g.N2 % kTK == 0 && g.N1 >= 2 * tj && (g.wallY || g.N1 % tj == 0);
 }
 
-cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef<double> &co, const double *ia,
-                               const double *corr2, double dt, double visc, const StageArgs64 &a, int *err,
-                               cudaStream_t st, const StageDiag *dg, bool *dg_done)
+cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Walls<double> &wl, const Coef<double> &co,
+                               const double *ia, const double *corr2, double dt, double visc, const StageArgs64 &a,
+                               int *err, cudaStream_t st, const StageDiag *dg, bool *dg_done)
 {
     const double *ef[3] = {nullptr, nullptr, nullptr};
     if (stage == 1 || stage == 2) {
@@ -572,8 +630,10 @@ cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef
         ef[1] = a.A;
     } else if (stage == 3) {
         ef[0] = a.A;
+    } else if (stage == 5) {
+        ef[0] = a.U0;
     }
-    if (dg && !stretch && (stage == 0 || stage == 4)) {
+    if (dg && !stretch && !wl.on && (stage == 0 || stage == 4)) {
         using Cf = TmaCfg<double>;
         const int ch = tma_ichunk<double>(g);
         const long long nb = (long long)(g.N2 / kTK) * (g.N1 / Cf::TJ) * ((g.N0 + ch - 1) / ch);
@@ -589,13 +649,12 @@ cudaError_t launch_stage_tma64(int stage, bool stretch, const Geo &g, const Coef
             return cudaSuccess;
         }
     }
-    return stretch ? launch_tma_stage<double, true>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st)
-                   : launch_tma_stage<double, false>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st);
+    return launch_tma_stage<double>(stage, stretch, g, co, ia, corr2, dt, visc, a, ef, err, st, wl);
 }
 
-cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef<float> &co, const float *ia,
-                               const float *corr2, float dt, float visc, const StageArgs32 &a, int *err,
-                               cudaStream_t st)
+cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Walls<float> &wl, const Coef<float> &co,
+                               const float *ia, const float *corr2, float dt, float visc, const StageArgs32 &a,
+                               int *err, cudaStream_t st)
 {
     const float *ef[3] = {nullptr, nullptr, nullptr};
     if (stage == 1 || stage == 2) {
@@ -607,9 +666,11 @@ cudaError_t launch_stage_tma32(int stage, bool stretch, const Geo &g, const Coef
         ef[2] = a.U0lo;
     } else if (stage == 4) {
         ef[0] = a.U0lo;
+    } else if (stage == 5) {
+        ef[0] = a.U0hi;
+        ef[1] = a.U0lo;
     }
-    return stretch ? launch_tma_stage<float, true>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st)
-                   : launch_tma_stage<float, false>(stage, g, co, ia, corr2, dt, visc, a, ef, err, st);
+    return launch_tma_stage<float>(stage, stretch, g, co, ia, corr2, dt, visc, a, ef, err, st, wl);
 }
 
 }  // namespace nova

@@ -2,9 +2,9 @@
 march (NOVA_STAGE_IMPL=tma / march, read when a mesh context is created).
 Both run the same point arithmetic, so whole runs must agree bit for bit; the
 march itself is pinned to the oracle by test_gpu_advance.py, and meshes of
-32^3 and up (periodic y, N2 % 32 == 0, N1 a multiple of the tile height 16
-(FP64) or 8 (FP32) and at least twice it) take the TMA path by default, so
-those oracle tests cover it directly too."""
+32^3 and up (N2 % 32 == 0, N1 at least twice the tile height 16 (FP64) or 8
+(FP32) and, with periodic y, a multiple of it; walls in y for FP32 only) take
+the TMA path by default, so those oracle tests cover it directly too."""
 import os
 
 import numpy as np
@@ -159,3 +159,47 @@ def test_mhd_tma_equals_march(nova, N, prec, rk_mode):
         nova.advance(GM, rd, U, nova.Field(GM, 1), B, nova.Field(GM, 1), nsteps=3)
         out[impl] = np.concatenate([U.download_soa(), B.download_soa()])
     assert rel_l2(out["tma"], out["march"]) < (1e-14 if prec == 0 else 1e-7)
+
+
+# walls in y: N1 = N[1] + 1 stored rows, the last tile ragged.  (12, 40, 32)
+# stores 41 rows: FP32 tiles of 5 x 8 rows and one of 1.  Non-zero wall values
+# exercise both ghost formulas on every component.
+WALL_N, WALL_L = (12, 40, 32), (2 * np.pi, 2 * np.pi, np.pi)
+
+
+def wall_run(nova, impl, prec, rk_mode, poisson, steps=3):
+    GM = mesh_with(nova, impl, WALL_N, L=WALL_L, walls=(0, 1, 0))
+    y = np.arange(WALL_N[1] + 1) * WALL_L[1] / WALL_N[1]
+    U0 = np.zeros((3, WALL_N[0], WALL_N[1] + 1, WALL_N[2]))
+    U0[0] = np.tanh(3.0 * (y - np.pi))[None, :, None]
+    U0 = U0 + 1e-2 * np.random.default_rng(9).standard_normal(U0.shape)
+    types, vals = [0] * 18, [0.0] * 18
+    for c in range(3):  # u, w Neumann, v Dirichlet on both walls, non-zero values
+        types[6 * c] = types[6 * c + 1] = 2 if c == 1 else 1
+        vals[6 * c], vals[6 * c + 1] = 0.1 * (c + 1), -0.05 * (c + 1)
+    U = nova.Field(GM, 3, prec).set_bc(types, vals).upload_soa(U0)
+    p = nova.Field(GM, 1).set_bc([1, 1] + [0] * 16)
+    nova.advance(GM, nova.run_desc(model="ns", rk_mode=rk_mode, precision=prec, dt=2e-3, nu=0.01, poisson=poisson),
+                 U, p, nsteps=steps)
+    return U.download_soa(), p.download_soa()
+
+
+@pytest.mark.parametrize("rk_mode,poisson", [("classical", "fft"), ("literal", "fft"), ("shear", "dct")])
+def test_tma_equals_march_with_walls(nova, rk_mode, poisson):
+    """The FP32-split TMA stage on a wall mesh (one row box per plane from
+    j0 - 3, zero filled outside the stored rows, ghosts of the mirror rows
+    formed by the warps next to a wall, ragged last tiles) gives the march's
+    bits; the shear-layer loop runs its stage 5 on it."""
+    a = wall_run(nova, "tma", nova.F32SPLIT, rk_mode, poisson)
+    b = wall_run(nova, "march", nova.F32SPLIT, rk_mode, poisson)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.abs(a[0]).max() > 0.5
+
+
+def test_fp64_walls_stay_on_the_march(nova):
+    """FP64 wall stages run the march by default; forcing the TMA pipeline on
+    a wall mesh in FP64 is refused."""
+    wall_run(nova, "auto", nova.F64, "shear", "dct", steps=1)
+    with pytest.raises(nova.NovaError) as e:
+        wall_run(nova, "tma", nova.F64, "shear", "dct", steps=1)
+    assert e.value.status == nova.E_UNSUPPORTED
