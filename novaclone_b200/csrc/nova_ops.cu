@@ -698,8 +698,8 @@ cudaError_t launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const 
                             const double *U64, const float *hi, const float *lo, double divisor, double *rhs,
                             cudaStream_t st, const StageExec &ex)
 {
-    if (ex.err && h == 3 && !wl.on && ex.impl != STAGE_MARCH && proj_tma_fits(g))
-        return launch_div_tma(g, co, ia, U64, hi, lo, divisor, rhs, ex.err, st);
+    if (ex.err && h == 3 && ex.impl != STAGE_MARCH && proj_tma_fits(g, wl.on))
+        return launch_div_tma(g, co, wl, ia, U64, hi, lo, divisor, rhs, ex.err, st);
     const int ch = pick_ichunk(g, 3);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
 #define NOVA_DIV(LDT, LDV, W)                                                                             \
@@ -731,8 +731,8 @@ cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const C
                            const double *p, double s, const double *Us64, double *U64, const float *Ushi,
                            const float *Uslo, float *hi, float *lo, cudaStream_t st, const StageExec &ex)
 {
-    if (ex.err && h == 3 && !pw.on && ex.impl != STAGE_MARCH && proj_tma_fits(g))
-        return launch_correct_tma(g, co, ia, p, s, Us64, U64, Ushi, Uslo, hi, lo, ex.err, st);
+    if (ex.err && h == 3 && ex.impl != STAGE_MARCH && proj_tma_fits(g, pw.on))
+        return launch_correct_tma(g, co, pw, ia, p, s, Us64, U64, Ushi, Uslo, hi, lo, ex.err, st);
     const int ch = pick_ichunk(g, 4);
     const dim3 grid = tile_grid(g, ch), block(kTK, kTJ);
 #define NOVA_CORR(SPL, W)                                                                                 \

@@ -21,9 +21,10 @@ struct WallFix {
 };
 
 // ex: with a non-null error word (ex.err) the TMA-pipelined kernels of
-// nova_proj_tma.cu run where the mesh fits them (proj_tma_fits: periodic y,
-// N2 % 32 == 0, N1 % 16 == 0, N1 >= 32) and StageExec::impl is not
-// STAGE_MARCH; otherwise the tiled march kernels.  Returns
+// nova_proj_tma.cu run where the mesh fits them (proj_tma_fits: N2 % 32 == 0,
+// N1 >= 32 and, with periodic y, N1 % 16 == 0; walls in y when the field's
+// ghost BCs are on) and StageExec::impl is not STAGE_MARCH; otherwise the
+// tiled march kernels.  Returns
 // cudaErrorInvalidValue when a tensor map cannot be encoded.
 cudaError_t launch_div_proj(int h, const Geo &g, const Walls<double> &wl, const Coef<double> &co, const double *ia,
                             const double *U64, const float *hi, const float *lo, double divisor, double *rhs,
@@ -61,12 +62,13 @@ cudaError_t launch_correct(int h, const Geo &g, const Walls<double> &pw, const C
                            const double *p, double s, const double *Us64, double *U64, const float *Ushi,
                            const float *Uslo, float *hi, float *lo, cudaStream_t st,
                            const StageExec &ex = StageExec{STAGE_MARCH, nullptr});
-bool proj_tma_fits(const Geo &g);
-cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *hi,
-                           const float *lo, double divisor, double *rhs, int *err, cudaStream_t st);
-cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,
-                               const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi,
-                               float *lo, int *err, cudaStream_t st);
+bool proj_tma_fits(const Geo &g, bool wl_on);
+cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const Walls<double> &wl, const double *ia,
+                           const double *U64, const float *hi, const float *lo, double divisor, double *rhs, int *err,
+                           cudaStream_t st);
+cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const Walls<double> &pw, const double *ia,
+                               const double *p, double s, const double *Us64, double *U64, const float *Ushi,
+                               const float *Uslo, float *hi, float *lo, int *err, cudaStream_t st);
 int diag_blocks(const Geo &g);
 // implicit operators (nova_im.cu): coef = 8 FP64 fields [al0..al5 | ap | b]
 void launch_fdm_laplacian(const Geo &g, const Coef<double> &co, const double *ia, const double *corr2, int h,

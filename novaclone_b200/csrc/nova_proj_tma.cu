@@ -9,6 +9,12 @@
 //         slot = p rows with j halos and k halos; epilogue ring = U* (3 components)
 // FP32-split fields arrive as hi and lo boxes and are joined in FP64 as the
 // march kernels do ((double)hi + (double)lo), so both produce the same bits.
+// WALLS (walls on the y nodes j = 0 and j = N1 - 1): the j-halo rows arrive
+// as one box from j0 - 3 (rows outside 0..N1-1 zero filled, the last tile
+// may be ragged); in the warps of rows within 3 of a wall, a j neighbour
+// across the wall is the wall_ghost of its mirror row (the field's BC: U*'s
+// component 1 for DIV, p for CORR), the formula of the tiled kernels; rows
+// past N1 - 1 store nothing.
 // Every mbarrier wait is bounded (nova_tma.cuh).
 #include "nova_internal.cuh"
 #include "nova_tma.cuh"
@@ -75,9 +81,9 @@ struct ProjArgs {
     float *hi, *lo;             // CORR output (split)
 };
 
-template <int MODE, bool SPLIT>
+template <int MODE, bool SPLIT, bool WALLS>
 __global__ void __launch_bounds__(kThreads, 2)
-    k_proj_tma(Geo g, Coef<double> co, const double *__restrict__ ia, ProjArgs a,
+    k_proj_tma(Geo g, Coef<double> co, const Walls<double> wl, const double *__restrict__ ia, ProjArgs a,
                const __grid_constant__ ProjMaps maps, int ichunk, int *err)
 {
     using C = ProjCfg<MODE, SPLIT>;
@@ -121,7 +127,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int kl = (k0 == 0 ? g.N2 : k0) - 4, kr = (k0 + kTK == g.N2) ? 0 : k0 + kTK;
         // rows with j halos of map set `ms` into dst
         auto rows = [&](int ms, uint32_t dst, uint32_t bar, int plane) {
-            if (jlo) {
+            if (WALLS) {
+                tma_load_3d(dst, &maps.m[ms + M_RA], bar, k0, j0 - H, plane);
+            } else if (jlo) {
                 tma_load_3d(dst, &maps.m[ms + M_R3], bar, k0, g.N1 - H, plane);
                 tma_load_3d(dst + H * kRowBytes, &maps.m[ms + M_RB], bar, k0, 0, plane);
             } else if (jhi) {
@@ -213,6 +221,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     constexpr int oZ = DL ? kTileE + kRowsE : H * kTK;      // k stencil centre row
     constexpr int oL = DL ? 2 * kTileE + kRowsE : kRowsE;   // left k halo
     const int qoff = oQ + ty * kTK + tx, yoff = oY + ty * kTK + tx;
+    // walls: this warp's row, and whether its j stencil reaches across a wall
+    // (the component whose j derivative is taken: U*_1 for DIV, p for CORR)
+    constexpr int CY = MODE == PROJ_DIV ? 1 : 0;
+    const int jrow = j0 + ty;
+    const bool nearw = WALLS && jrow < g.N1 && (jrow < H || jrow + H > g.N1 - 1);
     auto zoff = [&](int s) -> int {
         const int x = tx + s;
         return x < 0 ? oL + ty * 4 + 4 + x : (x >= kTK ? oL + kLRE + ty * 4 + (x - kTK) : oZ + ty * kTK + x);
@@ -251,15 +264,25 @@ __global__ void __launch_bounds__(kThreads, 2)
         const TS *sl = ring + (cur % kRing) * C::kSlotE;
         auto vx = [&](int, int s) -> double { return q[H + s]; };
         auto vy = [&](int, int s) -> double { return val(sl, yoff + s * kTK); };
+        auto vyg = [&](int, int s) -> double {
+            const int jj = jrow + s;
+            if (jj < 0 || jj > g.N1 - 1) {
+                const int side = jj < 0 ? 0 : 1, l = jj < 0 ? -jj : jj - (g.N1 - 1);
+                const int jm = jj < 0 ? l : g.N1 - 1 - l;  // the mirror row, inside the slot
+                return wall_ghost(wl, side, CY, l, val(sl, yoff + (jm - jrow) * kTK));
+            }
+            return val(sl, yoff + s * kTK);
+        };
         auto vz = [&](int, int s) -> double { return val(sl, zoff(s)); };
+        const double dy = (WALLS && nearw) ? d1<double, H>(vyg, CY, co.a[1]) : d1<double, H>(vy, CY, co.a[1]);
+        const bool store = !WALLS || jrow < g.N1;
         const long long idx = (long long)(ib + p) * g.N12 + (long long)(j0 + ty) * g.N2 + kw;
         if constexpr (MODE == PROJ_DIV) {
-            const double d = d1<double, H>(vx, 0, co.a[0]) + d1<double, H>(vy, 1, co.a[1]) + d1<double, H>(vz, 2, az);
+            const double d = d1<double, H>(vx, 0, co.a[0]) + dy + d1<double, H>(vz, 2, az);
             release(empty(cur % kRing));  // the slot's values are in registers
-            a.rhs[idx] = d / a.divisor;
+            if (store) a.rhs[idx] = d / a.divisor;
         } else {
-            const double gr[3] = {d1<double, H>(vx, 0, co.a[0]), d1<double, H>(vy, 0, co.a[1]),
-                                  d1<double, H>(vz, 0, az)};
+            const double gr[3] = {d1<double, H>(vx, 0, co.a[0]), dy, d1<double, H>(vz, 0, az)};
             release(empty(cur % kRing));  // the slot's values are in registers
             ok = mbar_wait(efull(p % kERing), (p / kERing) & 1, err);
             if (!__all_sync(0xffffffffu, ok)) {
@@ -275,6 +298,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             release(eempty(p % kERing));
 #pragma unroll
             for (int c = 0; c < 3; c++) {
+                if (!store) break;
                 const long long o = (long long)c * g.N3 + idx;
                 const double x = us[c] - gr[c] * a.s;
                 if constexpr (SPLIT) {
@@ -348,18 +372,18 @@ template <typename T> bool encode_rows(ProjMaps &pm, int ms, const T *f, const G
 // DIV 115 -> 120 us)
 int proj_ichunk(const Geo &g, int waves)
 {
-    const long long tiles = (long long)(g.N2 / kTK) * (g.N1 / TJ);
+    const long long tiles = (long long)(g.N2 / kTK) * ((g.N1 + TJ - 1) / TJ);
     int ch = g.N0;
     while (ch > 16 && tiles * ((g.N0 + ch - 1) / ch) < 148LL * 2 * waves) ch /= 2;
     return ch;
 }
 
-template <int MODE, bool SPLIT>
-cudaError_t launch(const Geo &g, const Coef<double> &co, const double *ia, const ProjArgs &a, const ProjMaps &pm,
-                   int *err, cudaStream_t st)
+template <int MODE, bool SPLIT, bool WALLS>
+cudaError_t launch_w(const Geo &g, const Coef<double> &co, const Walls<double> &wl, const double *ia,
+                     const ProjArgs &a, const ProjMaps &pm, int *err, cudaStream_t st)
 {
     using C = ProjCfg<MODE, SPLIT>;
-    auto kern = k_proj_tma<MODE, SPLIT>;
+    auto kern = k_proj_tma<MODE, SPLIT, WALLS>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
@@ -367,17 +391,32 @@ cudaError_t launch(const Geo &g, const Coef<double> &co, const double *ia, const
         attr = true;
     }
     const int ch = proj_ichunk(g, MODE == PROJ_DIV ? 2 : 4);
-    const dim3 grid(g.N2 / kTK, g.N1 / TJ, (g.N0 + ch - 1) / ch);
-    kern<<<grid, dim3(kTK, TJ + 1), C::kSmem, st>>>(g, co, ia, a, pm, ch, err);
+    const dim3 grid(g.N2 / kTK, (g.N1 + TJ - 1) / TJ, (g.N0 + ch - 1) / ch);
+    kern<<<grid, dim3(kTK, TJ + 1), C::kSmem, st>>>(g, co, wl, ia, a, pm, ch, err);
     return cudaSuccess;
+}
+
+template <int MODE, bool SPLIT>
+cudaError_t launch(const Geo &g, const Coef<double> &co, const Walls<double> &wl, const double *ia,
+                   const ProjArgs &a, const ProjMaps &pm, int *err, cudaStream_t st)
+{
+    return wl.on ? launch_w<MODE, SPLIT, true>(g, co, wl, ia, a, pm, err, st)
+                 : launch_w<MODE, SPLIT, false>(g, co, wl, ia, a, pm, err, st);
 }
 
 }  // namespace
 
-bool proj_tma_fits(const Geo &g) { return !g.wallY && g.N2 % kTK == 0 && g.N1 % TJ == 0 && g.N1 >= 2 * TJ; }
+// tile width divides N2; periodic y: the tile height divides N1; walls in y
+// (the field's ghost BCs on, wl_on): any N1 of at least two tiles
+bool proj_tma_fits(const Geo &g, bool wl_on)
+{
+    if (wl_on != (g.wallY != 0)) return false;
+    return g.N2 % kTK == 0 && g.N1 >= 2 * TJ && (g.wallY || g.N1 % TJ == 0);
+}
 
-cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *U64, const float *hi,
-                           const float *lo, double divisor, double *rhs, int *err, cudaStream_t st)
+cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const Walls<double> &wl, const double *ia,
+                           const double *U64, const float *hi, const float *lo, double divisor, double *rhs, int *err,
+                           cudaStream_t st)
 {
     ProjMaps pm;
     memset(&pm, 0, sizeof pm);
@@ -392,16 +431,16 @@ cudaError_t launch_div_tma(const Geo &g, const Coef<double> &co, const double *i
     };
     if (U64) {
         if (!set_maps(0, U64)) return cudaErrorInvalidValue;
-        return launch<PROJ_DIV, false>(g, co, ia, a, pm, err, st);
+        return launch<PROJ_DIV, false>(g, co, wl, ia, a, pm, err, st);
     }
     const bool ok = set_maps(0, hi) && set_maps(M_SET, lo);
     if (!ok) return cudaErrorInvalidValue;
-    return launch<PROJ_DIV, true>(g, co, ia, a, pm, err, st);
+    return launch<PROJ_DIV, true>(g, co, wl, ia, a, pm, err, st);
 }
 
-cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const double *ia, const double *p, double s,
-                               const double *Us64, double *U64, const float *Ushi, const float *Uslo, float *hi,
-                               float *lo, int *err, cudaStream_t st)
+cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const Walls<double> &pw, const double *ia,
+                               const double *p, double s, const double *Us64, double *U64, const float *Ushi,
+                               const float *Uslo, float *hi, float *lo, int *err, cudaStream_t st)
 {
     ProjMaps pm;
     memset(&pm, 0, sizeof pm);
@@ -414,16 +453,16 @@ cudaError_t launch_correct_tma(const Geo &g, const Coef<double> &co, const doubl
     if (Us64 && hi) {  // FP64 U*, FP32-split output
         ok = ok && encode4(&pm.m[M_EPI], Us64, g);
         if (!ok) return cudaErrorInvalidValue;
-        return launch<PROJ_CORR_MIX, true>(g, co, ia, a, pm, err, st);
+        return launch<PROJ_CORR_MIX, true>(g, co, pw, ia, a, pm, err, st);
     }
     if (Us64) {
         ok = ok && encode4(&pm.m[M_EPI], Us64, g);
         if (!ok) return cudaErrorInvalidValue;
-        return launch<PROJ_CORR, false>(g, co, ia, a, pm, err, st);
+        return launch<PROJ_CORR, false>(g, co, pw, ia, a, pm, err, st);
     }
     ok = ok && encode4(&pm.m[M_EPI], Ushi, g) && encode4(&pm.m[M_EPI + 1], Uslo, g);
     if (!ok) return cudaErrorInvalidValue;
-    return launch<PROJ_CORR, true>(g, co, ia, a, pm, err, st);
+    return launch<PROJ_CORR, true>(g, co, pw, ia, a, pm, err, st);
 }
 
 }  // namespace nova

@@ -186,20 +186,25 @@ def wall_run(nova, impl, prec, rk_mode, poisson, steps=3):
 
 @pytest.mark.parametrize("rk_mode,poisson", [("classical", "fft"), ("literal", "fft"), ("shear", "dct")])
 def test_tma_equals_march_with_walls(nova, rk_mode, poisson):
-    """The FP32-split TMA stage on a wall mesh (one row box per plane from
-    j0 - 3, zero filled outside the stored rows, ghosts of the mirror rows
-    formed by the warps next to a wall, ragged last tiles) gives the march's
-    bits; the shear-layer loop runs its stage 5 on it."""
+    """The FP32-split TMA stage and projection on a wall mesh (one row box
+    per plane from j0 - 3, zero filled outside the stored rows, ghosts of the
+    mirror rows formed by the warps next to a wall, ragged last tiles) give
+    the march's bits; the shear-layer loop runs its stage 5 on it."""
     a = wall_run(nova, "tma", nova.F32SPLIT, rk_mode, poisson)
     b = wall_run(nova, "march", nova.F32SPLIT, rk_mode, poisson)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     assert np.abs(a[0]).max() > 0.5
 
 
-def test_fp64_walls_stay_on_the_march(nova):
-    """FP64 wall stages run the march by default; forcing the TMA pipeline on
-    a wall mesh in FP64 is refused."""
-    wall_run(nova, "auto", nova.F64, "shear", "dct", steps=1)
+@pytest.mark.parametrize("rk_mode,poisson", [("classical", "fft"), ("shear", "dct")])
+def test_fp64_walls_projection_on_tma(nova, rk_mode, poisson):
+    """FP64 on a wall mesh: the stages run the march by default, the projection
+    (divergence with U*'s wall ghosts, correction with p's) the TMA pipeline;
+    the run gives the all-march bits.  Forcing the TMA stage in FP64 on a
+    wall mesh is refused."""
+    a = wall_run(nova, "auto", nova.F64, rk_mode, poisson)
+    b = wall_run(nova, "march", nova.F64, rk_mode, poisson)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     with pytest.raises(nova.NovaError) as e:
         wall_run(nova, "tma", nova.F64, "shear", "dct", steps=1)
     assert e.value.status == nova.E_UNSUPPORTED
