@@ -15,6 +15,17 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 w)
 
 __device__ __forceinline__ double2 conj2(double2 w) { return make_double2(w.x, -w.y); }
 
+// 1/a for a >= 1e-16 (normal in FP32 for every mesh the Poisson scales meet):
+// the correctly rounded FP32 reciprocal refined by two Newton-Raphson steps
+// y <- y + y (1 - a y) in FP64 (relative error about 2^-23 -> 2^-46 -> below
+// an ulp of FP64, up to the rounding of the last step)
+__device__ __forceinline__ double recip(double a)
+{
+    double y = (double)__frcp_rn((float)a);
+    y = fma(y, fma(-a, y, 1.0), y);
+    return fma(y, fma(-a, y, 1.0), y);
+}
+
 __host__ __device__ constexpr int bitrev(int x, int bits)
 {
     int r = 0;

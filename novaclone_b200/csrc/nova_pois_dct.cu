@@ -126,11 +126,6 @@ __global__ void __launch_bounds__(kDThreads, 3)
     double2 *red = t512 + kN;                         // [16][8]
     double *ky2 = reinterpret_cast<double *>(red + kR * kCol);
     const int tid = threadIdx.x, c = tid % kCol, t = tid / kCol;
-    for (int m = tid; m < kN; m += kDThreads) {
-        tw[m] = twg[m];
-        t512[m] = t512g[m];
-    }
-    for (int m = tid; m < kRows; m += kDThreads) ky2[m] = ky2e[m];
 
     const int task = blockIdx.x;
     int i0, kz0, di, dkz;  // column c: i = i0 + di c, kz = kz0 + dkz c
@@ -142,16 +137,49 @@ __global__ void __launch_bounds__(kDThreads, 3)
     const long long rowst = nzh;                      // j stride
     const long long ist = (long long)kRows * nzh;     // i stride
     auto addr = [&](int col, int j) -> long long { return (i0 + di * col) * ist + j * rowst + kz0 + dkz * col; };
-    for (int e = tid; e < kRows * kCol; e += kDThreads) S[e] = spec[addr(e % kCol, e / kCol)];
+    // every global load of the block in flight at once: the column tile
+    // (element e = j * 8 + col, thread tid takes e = tid + 128 u) and the tables
+    constexpr int kLd = (kRows * kCol + kDThreads - 1) / kDThreads;
+    constexpr int kTb = kN / kDThreads;
+    double2 ld[kLd], ltw[kTb], lt5[kTb];
+    double lky[kTb + 1];
+#pragma unroll
+    for (int u = 0; u < kLd; u++) {
+        const int e = tid + kDThreads * u;
+        if (u < kLd - 1 || e < kRows * kCol) ld[u] = spec[addr(e % kCol, e / kCol)];
+    }
+#pragma unroll
+    for (int u = 0; u < kTb; u++) {
+        ltw[u] = twg[tid + kDThreads * u];
+        lt5[u] = t512g[tid + kDThreads * u];
+    }
+#pragma unroll
+    for (int u = 0; u <= kTb; u++)
+        if (tid + kDThreads * u < kRows) lky[u] = ky2e[tid + kDThreads * u];
     const double kxx = kx2[i0 + di * c], kzz = kz2[kz0 + dkz * c];
+#pragma unroll
+    for (int u = 0; u < kLd; u++) {
+        const int e = tid + kDThreads * u;
+        if (u < kLd - 1 || e < kRows * kCol) S[e] = ld[u];
+    }
+#pragma unroll
+    for (int u = 0; u < kTb; u++) {
+        tw[tid + kDThreads * u] = ltw[u];
+        t512[tid + kDThreads * u] = lt5[u];
+    }
+#pragma unroll
+    for (int u = 0; u <= kTb; u++)
+        if (tid + kDThreads * u < kRows) ky2[tid + kDThreads * u] = lky[u];
     __syncthreads();
 
     double2 x[kR], xN;
     dct1(S, red, c, t, tw, t512, x, xN);
-    // scale -1 / k'^2 / (N0 2N N2), 0 where k'^2 < 1e-16 (k_scale's sum order)
+    // scale -1 / k'^2 / (N0 2N N2), 0 where k'^2 < 1e-16 (k_scale's sum order;
+    // one reciprocal per element instead of two divisions)
     auto scale = [&](double2 v, int m) -> double2 {
         const double k2 = (kxx + ky2[m]) + kzz;
-        return k2 < 1.0e-16 ? make_double2(0.0, 0.0) : make_double2((-v.x / k2) * invN3, (-v.y / k2) * invN3);
+        const double f = k2 < 1.0e-16 ? 0.0 : -invN3 * recip(k2);
+        return make_double2(v.x * f, v.y * f);
     };
     __syncthreads();  // every read of S inside dct1 done
 #pragma unroll
@@ -164,7 +192,11 @@ __global__ void __launch_bounds__(kDThreads, 3)
     for (int q = 0; q < kR; q++) S[(kR * t + q) * kCol + c] = x[q];
     if (t == kR - 1) S[kN * kCol + c] = xN;
     __syncthreads();
-    for (int e = tid; e < kRows * kCol; e += kDThreads) spec[addr(e % kCol, e / kCol)] = S[e];
+#pragma unroll
+    for (int u = 0; u < kLd; u++) {
+        const int e = tid + kDThreads * u;
+        if (u < kLd - 1 || e < kRows * kCol) spec[addr(e % kCol, e / kCol)] = S[e];
+    }
 }
 
 }  // namespace

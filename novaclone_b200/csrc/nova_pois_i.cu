@@ -38,17 +38,6 @@ namespace {
 
 constexpr int kCols = 16;  // kz columns per block: 16 x 16 B = 256 contiguous bytes per i row
 
-// 1/a for a >= 1e-16 (normal in FP32 for every mesh this solver meets):
-// the correctly rounded FP32 reciprocal refined by two Newton-Raphson steps
-// y <- y + y (1 - a y) in FP64 (relative error about 2^-23 -> 2^-46 -> below
-// an ulp of FP64, up to the rounding of the last step)
-__device__ __forceinline__ double recip(double a)
-{
-    double y = (double)__frcp_rn((float)a);
-    y = fma(y, fma(-a, y, 1.0), y);
-    return fma(y, fma(-a, y, 1.0), y);
-}
-
 template <int R>
 __global__ void __launch_bounds__(kCols *R, R == 16 ? 2 : 4)
     k_pois_i(int ny, int nzh, double2 *__restrict__ spec, const double2 *__restrict__ twN,
