@@ -27,6 +27,7 @@
 #include "nova_fft.cuh"
 #include "nova_internal.cuh"
 #include "nova_ops.cuh"
+#include "nova_tma.cuh"
 
 #include <algorithm>
 
@@ -36,13 +37,28 @@ namespace {
 
 constexpr int kN = 256;            // y intervals: N + 1 stored rows
 constexpr int kR = 16;             // 256 = 16 x 16
-constexpr int kCol = 8;            // columns per block
+constexpr int kCol = 8;            // columns per block (4 blocks per SM)
 constexpr int kDThreads = kCol * kR;  // thread (col = tid % 8, t = tid / 8)
 constexpr int kRows = kN + 1;
 // shared memory: the column tile [257][8], W_256, W_512^n (n < 256), ky'^2 (257), scan scratch [16][8]
 constexpr size_t kDSmem = sizeof(double2) * ((size_t)kRows * kCol + kN + kN + (size_t)kR * kCol) + sizeof(double) * kRows;
 
 __device__ __forceinline__ double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// global -> shared copies that hold no registers while in flight
+// (cp.async; 16 bytes through L2 only, or 8 bytes)
+__device__ __forceinline__ void cp16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 __device__ __forceinline__ double2 sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 
 // X = DCT-I(f) of column c: on entry S[n * 8 + c] = f_n (n = 0..N) for every
@@ -114,7 +130,7 @@ __device__ __forceinline__ void dct1(double2 *S, double2 *red, int c, int t, con
 // Task t < nmain: columns (i, kz0 + c), i = t / nch, kz0 = 8 (t % nch); task
 // t >= nmain: columns (8 (t - nmain) + c, nzh - 1), the last kz of 8
 // consecutive i.  spec[(i (N + 1) + j) nzh + kz], j = 0..N.
-__global__ void __launch_bounds__(kDThreads, 3)
+__global__ void __launch_bounds__(kDThreads, 4)
     k_pois_dct(int nzh, int nch, int nmain, double2 *__restrict__ spec, const double2 *__restrict__ twg,
                const double2 *__restrict__ t512g, const double *__restrict__ kx2, const double *__restrict__ ky2e,
                const double *__restrict__ kz2, double invN3)
@@ -137,39 +153,26 @@ __global__ void __launch_bounds__(kDThreads, 3)
     const long long rowst = nzh;                      // j stride
     const long long ist = (long long)kRows * nzh;     // i stride
     auto addr = [&](int col, int j) -> long long { return (i0 + di * col) * ist + j * rowst + kz0 + dkz * col; };
-    // every global load of the block in flight at once: the column tile
-    // (element e = j * 8 + col, thread tid takes e = tid + 128 u) and the tables
+    // every global load of the block in flight at once, straight into shared
+    // memory: the column tile (element e = j * 8 + col, thread tid takes
+    // e = tid + 128 u) and the tables
     constexpr int kLd = (kRows * kCol + kDThreads - 1) / kDThreads;
     constexpr int kTb = kN / kDThreads;
-    double2 ld[kLd], ltw[kTb], lt5[kTb];
-    double lky[kTb + 1];
 #pragma unroll
     for (int u = 0; u < kLd; u++) {
         const int e = tid + kDThreads * u;
-        if (u < kLd - 1 || e < kRows * kCol) ld[u] = spec[addr(e % kCol, e / kCol)];
+        if (u < kLd - 1 || e < kRows * kCol) cp16(S + e, spec + addr(e % kCol, e / kCol));
     }
 #pragma unroll
     for (int u = 0; u < kTb; u++) {
-        ltw[u] = twg[tid + kDThreads * u];
-        lt5[u] = t512g[tid + kDThreads * u];
+        cp16(tw + tid + kDThreads * u, twg + tid + kDThreads * u);
+        cp16(t512 + tid + kDThreads * u, t512g + tid + kDThreads * u);
     }
 #pragma unroll
     for (int u = 0; u <= kTb; u++)
-        if (tid + kDThreads * u < kRows) lky[u] = ky2e[tid + kDThreads * u];
+        if (tid + kDThreads * u < kRows) cp8(ky2 + tid + kDThreads * u, ky2e + tid + kDThreads * u);
     const double kxx = kx2[i0 + di * c], kzz = kz2[kz0 + dkz * c];
-#pragma unroll
-    for (int u = 0; u < kLd; u++) {
-        const int e = tid + kDThreads * u;
-        if (u < kLd - 1 || e < kRows * kCol) S[e] = ld[u];
-    }
-#pragma unroll
-    for (int u = 0; u < kTb; u++) {
-        tw[tid + kDThreads * u] = ltw[u];
-        t512[tid + kDThreads * u] = lt5[u];
-    }
-#pragma unroll
-    for (int u = 0; u <= kTb; u++)
-        if (tid + kDThreads * u < kRows) ky2[tid + kDThreads * u] = lky[u];
+    cp_wait_all();
     __syncthreads();
 
     double2 x[kR], xN;
