@@ -84,7 +84,6 @@ struct nova_ctx {
     double *d_rhs = nullptr;
     double *w64[3] = {nullptr, nullptr, nullptr};
     float *w32[3] = {nullptr, nullptr, nullptr};
-    float *w32x = nullptr;  // the shear-layer loop's FP32-split U* (lo part)
     double *d_part = nullptr;
     double *d_scalar = nullptr;
     int *d_flag = nullptr;
@@ -655,7 +654,7 @@ extern "C" nova_status nova_destroy(nova_ctx *ctx)
     }
     void *ptrs[] = {ctx->d_ia64, ctx->d_corr64, ctx->d_ia32, ctx->d_corr32, ctx->d_kx2, ctx->d_ky2, ctx->d_kz2,
                     ctx->d_spec, ctx->d_rhs, ctx->w64[0], ctx->w64[1], ctx->w64[2], ctx->w32[0], ctx->w32[1],
-                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->w32x, ctx->d_tw256,
+                    ctx->w32[2], ctx->d_part, ctx->d_scalar, ctx->d_flag, ctx->d_hist, ctx->d_stage, ctx->adj_pool, ctx->d_row, ctx->d_ext, ctx->d_ky2e, ctx->d_spec2, ctx->d_twN, ctx->d_tw256,
                     ctx->d_spec3, ctx->d_t512};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -1093,9 +1092,11 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
                         phys_of(dg->fin));
             ctx->launches += 2;
         }
+        // the split U* leaves stage 5 in FP64 (as many bytes as the (hi, lo)
+        // pair) for the FP64 projection, whose correction writes the pair
         const size_t n3 = 3 * (size_t)g.N3;
-        double *Old64 = ctx->w64[2], *Us64 = ctx->w64[1];
-        float *Oh = ctx->w32[0], *Ol = ctx->w32[1], *Sh = ctx->w32[2], *Sl = ctx->w32x;
+        double *Old64 = ctx->w64[2], *Us64 = f64 ? ctx->w64[1] : ctx->w64[0];
+        float *Oh = ctx->w32[0], *Ol = ctx->w32[1];
         const Walls<double> sw64 = walls_of<double>(ctx, Y, X);
         const Walls<float> sw32 = walls_of<float>(ctx, Y, X);
         if (walls) {
@@ -1119,27 +1120,25 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
                     e = launch_stage64(phys, 5, str, g, sw64, ctx->co64, ctx->d_ia64, ctx->d_corr64, rd->dt, visc,
                                        StageArgs64{Y->d64, X ? X->d64 : nullptr, Old64, nullptr, Us64, kShearW[rk]},
                                        st, ex);
-                else
+                else {
+                    StageArgs32 a{Y->hi, X ? X->hi : nullptr, Oh, Ol, nullptr, nullptr, nullptr, nullptr,
+                                  (float)kShearW[rk]};
+                    a.out64 = Us64;
                     e = launch_stage32(phys, 5, str, g, sw32, ctx->co32, ctx->d_ia32, ctx->d_corr32, (float)rd->dt,
-                                       (float)visc,
-                                       StageArgs32{Y->hi, X ? X->hi : nullptr, Oh, Ol, nullptr, nullptr, Sh, Sl,
-                                                   (float)kShearW[rk]},
-                                       st, ex);
+                                       (float)visc, a, st, ex);
+                }
                 ctx->launches += 1;
             }
             if (e != cudaSuccess) return stage_fail(ctx, e);
             if (walls) {
-                if (f64)
-                    launch_wall_fix64(g, yfix, Us64, st);
-                else
-                    launch_wall_fix_split(g, yfix, Sh, Sl, st);
+                launch_wall_fix64(g, yfix, Us64, st);
                 ctx->launches += 1;
             }
             CKL("stage kernel");
             {
                 ProfScope ps(ctx, NOVA_K_DIV);
-                e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, f64 ? Us64 : nullptr, f64 ? nullptr : Sh,
-                                    f64 ? nullptr : Sl, divisor * kRK4c[rk], ctx->d_rhs, st, ex);
+                e = launch_div_proj(ctx->h, g, yw64, ctx->co64, ctx->d_ia64, Us64, nullptr, nullptr,
+                                    divisor * kRK4c[rk], ctx->d_rhs, st, ex);
                 if (e != cudaSuccess) return stage_fail(ctx, e);
                 ctx->launches += 1;
             }
@@ -1153,9 +1152,9 @@ nova_status evolve(nova_ctx *ctx, const nova_run_desc *rd, int phys, nova_field 
             }
             {
                 ProfScope ps(ctx, NOVA_K_CORRECT);
-                e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, kRK4c[rk] * corr_scale,
-                                   f64 ? Us64 : nullptr, f64 ? Y->d64 : nullptr, f64 ? nullptr : Sh,
-                                   f64 ? nullptr : Sl, f64 ? nullptr : Y->hi, f64 ? nullptr : Y->lo, st, ex);
+                e = launch_correct(ctx->h, g, pw64, ctx->co64, ctx->d_ia64, p->d64, kRK4c[rk] * corr_scale, Us64,
+                                   f64 ? Y->d64 : nullptr, nullptr, nullptr, f64 ? nullptr : Y->hi,
+                                   f64 ? nullptr : Y->lo, st, ex);
                 if (e != cudaSuccess) return stage_fail(ctx, e);
                 ctx->launches += 1;
             }
@@ -1342,8 +1341,6 @@ extern "C" nova_status nova_advance(nova_ctx *ctx, const nova_run_desc *rd, nova
     if (!(rd->dt > 0.0)) return fail(ctx, NOVA_E_INVALID, "nova_advance: dt must be positive");
     nova_status s = ensure_work(ctx, rd->precision);
     if (s != NOVA_OK) return s;
-    if (shear && rd->precision == NOVA_F32SPLIT && (s = dalloc(ctx, &ctx->w32x, 3 * (size_t)ctx->g.N3)) != NOVA_OK)
-        return s;
     if (hist && rd->diag_every > 0) {
         if (ctx->hist_cap < (long long)nsteps * NOVA_HIST_COLS) {
             if (ctx->d_hist) cudaFree(ctx->d_hist);

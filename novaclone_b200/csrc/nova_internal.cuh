@@ -162,7 +162,7 @@ struct StageArgs32 {
     float *Ynext;        // next stage state (FP32)
     float *outhi, *outlo;  // U* (last stage / literal / stage 5)
     float w;             // stage 5: the stage's weight
-    double *out64;       // U* in FP64 instead of (outhi, outlo) (stages 3, 4) when non-null
+    double *out64;       // U* in FP64 instead of (outhi, outlo) (stages 3, 4, 5) when non-null
 };
 
 enum Physics { PHYS_NS = 0, PHYS_MHD_U = 1, PHYS_MHD_B = 2 };

@@ -230,9 +230,10 @@ __device__ __forceinline__ void rk_store64(const StageArgs64 &a, long long o, do
     if constexpr (RK64<STAGE>::kA) a.A[o] = an;
 }
 
-// FP32-split: A is an FP32 sum of increments; the last stage adds it to the
-// (hi, lo) base in FP64 and stores U* as a (hi, lo) pair, or in FP64 for the
-// projection (a.out64).  e0: U0hi (stages 1-3, 5), e1: A, lo: U0lo (stages 3-5)
+// FP32-split: A is an FP32 sum of increments; the last stage (3, 4, or the
+// shear-layer stage 5) adds it to the (hi, lo) base in FP64 and stores U* as a
+// (hi, lo) pair, or in FP64 for the projection (a.out64).  e0: U0hi (stages
+// 1-3, 5), e1: A, lo: U0lo (stages 3-5)
 template <int STAGE>
 __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, float y0, float e0, float e1, float lo,
                                            float du)
@@ -242,6 +243,10 @@ __device__ __forceinline__ void rk_store32(const StageArgs32 &a, long long o, fl
     const float w6 = 1.0f / 6.0f, w3 = 1.0f / 3.0f;
     if constexpr (STAGE == 5) {
         const double x = ((double)e0 + (double)lo) + (double)(du * a.w);
+        if (a.out64) {
+            a.out64[o] = x;
+            return;
+        }
         const float hi = (float)x;
         a.outhi[o] = hi;
         a.outlo[o] = (float)(x - (double)hi);
