@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_u(Geo g, Coef<double> co, co
         dir(vy, 1, co.a[1], co.b[1], false);
         dir(vz, 2, zm.az, zm.bz, true);
         const double T0 = BUOY ? a.T[idx] : 0.0;
+        const double ir = 1.0 / r0;  // the divisions by rho below as products (within an ulp)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const long long o = (long long)c * g.N3 + idx;
@@ -97,9 +98,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_u(Geo g, Coef<double> co, co
             const double acc = (STAGE == 0 ? r0 * q0 : a.acc[o]) + rk4w(STAGE) * d;
             if (STAGE < 3) {
                 a.acc[o] = acc;
-                a.Ynext[o] = (r0 * q0) / r0 + stage_c(STAGE) * (d / r0);
+                a.Ynext[o] = (r0 * q0) * ir + stage_c(STAGE) * (d * ir);
             } else {
-                a.Ynext[o] = acc / r0;
+                a.Ynext[o] = acc * ir;
             }
         }
     });
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_u(Geo g, Coef<double> co, co
 // -------------------------------------------------------------- rho loop --
 // halo'd comps: 0 rho (stage state), 1-3 U; 4+d: rho U_d formed per node
 template <int STAGE, bool STRETCH, int EOS>
-__global__ void __launch_bounds__(kThreads, 1) k_wc_rho(Geo g, Coef<double> co, const double *__restrict__ ia,
+__global__ void __launch_bounds__(kThreads, 2) k_wc_rho(Geo g, Coef<double> co, const double *__restrict__ ia,
                                                         const double *__restrict__ corr2, WcArgs a, int ichunk)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_rho(Geo g, Coef<double> co, 
 // ---------------------------------------------------------------- T loop --
 // halo'd comps: 0 T (stage state), 1 rho, 2-4 U; 5+d: rho U_d formed per node
 template <int STAGE, bool STRETCH>
-__global__ void __launch_bounds__(kThreads, 1) k_wc_t(Geo g, Coef<double> co, const double *__restrict__ ia,
+__global__ void __launch_bounds__(kThreads, 2) k_wc_t(Geo g, Coef<double> co, const double *__restrict__ ia,
                                                       const double *__restrict__ corr2, WcArgs a, int ichunk)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -174,11 +175,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_t(Geo g, Coef<double> co, co
         const double d = a.dt * e;
         const double q0 = STAGE == 0 ? t0 : a.Q0[idx];
         const double acc = (STAGE == 0 ? r0 * q0 : a.acc[idx]) + rk4w(STAGE) * d;
+        const double ir = 1.0 / r0;  // the divisions by rho below as products (within an ulp)
         if (STAGE < 3) {
             a.acc[idx] = acc;
-            a.Ynext[idx] = (r0 * q0) / r0 + stage_c(STAGE) * (d / r0);
+            a.Ynext[idx] = (r0 * q0) * ir + stage_c(STAGE) * (d * ir);
         } else {
-            a.Ynext[idx] = acc / r0;
+            a.Ynext[idx] = acc * ir;
         }
     });
 }
@@ -208,13 +210,15 @@ __global__ void k_wc_hydrostatic(Geo g, double dz, double gz, double rho0, doubl
 void launch_wc_stage(int loop, int stage, int wc_case, bool stretch, const Geo &g, const Coef<double> &co,
                      const double *ia, const double *corr2, const WcArgs &a, cudaStream_t st)
 {
+    // the rho and T loops fit 2 blocks per SM (128 registers), the U loop 1
+    const int bps = loop == WC_LOOP_U ? 1 : 2;
     auto go = [&](auto kern, size_t smem) {
         static bool attr = false;  // once per kernel instantiation
         if (!attr) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             attr = true;
         }
-        const int ch = pick_ichunk(g, 1);
+        const int ch = pick_ichunk(g, bps);
         kern<<<tile_grid(g, ch), dim3(kTK, kTJ), smem, st>>>(g, co, ia, corr2, a, ch);
     };
     constexpr size_t s5 = tile_smem_bytes<double, kH, 5>(), s4 = tile_smem_bytes<double, kH, 4>();
