@@ -64,8 +64,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_u(Geo g, Coef<double> co, co
     auto ld = [&](int c, long long o) -> double {
         return c < 3 ? a.Y[(long long)c * g.N3 + o] : (c == 3 ? a.rho[o] : a.p[o]);
     };
-    tile_march<double, kH, 5, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx,
-                                                               const auto &vy, const auto &vz) {
+    // the pointwise operands (base, accumulator, T) of the next plane load
+    // while this plane computes
+    double q0n[3] = {0, 0, 0}, accn[3] = {0, 0, 0}, Tn = 0.0, q0c[3], accc[3], Tc = 0.0;
+    auto pre = [&](long long nidx, bool load) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            q0c[c] = q0n[c];
+            accc[c] = accn[c];
+            if (STAGE > 0 && load) {
+                q0n[c] = a.Q0[(long long)c * g.N3 + nidx];
+                accn[c] = a.acc[(long long)c * g.N3 + nidx];
+            }
+        }
+        Tc = Tn;
+        if (BUOY && load) Tn = a.T[nidx];
+    };
+    tile_march<double, kH, 5, false>(g, wl, sm, ld, ib, ie, pre, [&](long long idx, auto &q, const auto &vx,
+                                                                    const auto &vy, const auto &vz) {
         const double u0[3] = {q[kH][0], q[kH][1], q[kH][2]};
         const double r0 = q[kH][3];
         const double V0[3] = {r0 * u0[0], r0 * u0[1], r0 * u0[2]};
@@ -84,7 +100,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_u(Geo g, Coef<double> co, co
         dir(vx, 0, co.a[0], co.b[0], false);
         dir(vy, 1, co.a[1], co.b[1], false);
         dir(vz, 2, zm.az, zm.bz, true);
-        const double T0 = BUOY ? a.T[idx] : 0.0;
+        const double T0 = BUOY ? Tc : 0.0;
         const double ir = 1.0 / r0;  // the divisions by rho below as products (within an ulp)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -94,8 +110,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_wc_u(Geo g, Coef<double> co, co
             e = e + a.visc * (fma(-zm.bsum, u0[c], lap[c]) - zm.c2k * duz[c]);
             if (BUOY) e = e - (r0 * T0) * a.g[c];
             const double d = a.dt * e;
-            const double q0 = STAGE == 0 ? u0[c] : a.Q0[o];
-            const double acc = (STAGE == 0 ? r0 * q0 : a.acc[o]) + rk4w(STAGE) * d;
+            const double q0 = STAGE == 0 ? u0[c] : q0c[c];
+            const double acc = (STAGE == 0 ? r0 * q0 : accc[c]) + rk4w(STAGE) * d;
             if (STAGE < 3) {
                 a.acc[o] = acc;
                 a.Ynext[o] = (r0 * q0) * ir + stage_c(STAGE) * (d * ir);
@@ -118,8 +134,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_wc_rho(Geo g, Coef<double> co, 
     const ZMetric zm = zmetric<STRETCH>(co, ia, corr2, wrapi(blockIdx.x * kTK + threadIdx.x, g.N2));
     const Walls<double> wl{};
     auto ld = [&](int c, long long o) -> double { return c == 0 ? a.Y[o] : a.U[(long long)(c - 1) * g.N3 + o]; };
-    tile_march<double, kH, 4, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx,
-                                                               const auto &vy, const auto &vz) {
+    double q0n = 0.0, accn = 0.0, q0c = 0.0, accc = 0.0;  // next plane's base and accumulator, loading ahead
+    auto pre = [&](long long nidx, bool load) {
+        q0c = q0n;
+        accc = accn;
+        if (STAGE > 0 && load) {
+            q0n = a.Q0[nidx];
+            accn = a.acc[nidx];
+        }
+    };
+    tile_march<double, kH, 4, false>(g, wl, sm, ld, ib, ie, pre, [&](long long idx, auto &q, const auto &vx,
+                                                                    const auto &vy, const auto &vz) {
         double divV = 0.0;
         auto dir = [&](const auto &v, int d, const double *aa) {
             auto vv = [&](int c, int s) -> double { return v(0, s) * v(1 + c, s); };
@@ -130,8 +155,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_wc_rho(Geo g, Coef<double> co, 
         dir(vz, 2, zm.az);
         const double d = a.dt * (-divV);
         const double r = q[kH][0];
-        const double rold = STAGE == 0 ? r : a.Q0[idx];
-        const double acc = (STAGE == 0 ? r : a.acc[idx]) + rk4w(STAGE) * d;
+        const double rold = STAGE == 0 ? r : q0c;
+        const double acc = (STAGE == 0 ? r : accc) + rk4w(STAGE) * d;
         if (STAGE < 3) {
             a.acc[idx] = acc;
             a.Ynext[idx] = rold + stage_c(STAGE) * d;
@@ -156,8 +181,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_wc_t(Geo g, Coef<double> co, co
     auto ld = [&](int c, long long o) -> double {
         return c == 0 ? a.Y[o] : (c == 1 ? a.rho[o] : a.U[(long long)(c - 2) * g.N3 + o]);
     };
-    tile_march<double, kH, 5, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx,
-                                                               const auto &vy, const auto &vz) {
+    double q0n = 0.0, accn = 0.0, q0c = 0.0, accc = 0.0;  // next plane's base and accumulator, loading ahead
+    auto pre = [&](long long nidx, bool load) {
+        q0c = q0n;
+        accc = accn;
+        if (STAGE > 0 && load) {
+            q0n = a.Q0[nidx];
+            accn = a.acc[nidx];
+        }
+    };
+    tile_march<double, kH, 5, false>(g, wl, sm, ld, ib, ie, pre, [&](long long idx, auto &q, const auto &vx,
+                                                                    const auto &vy, const auto &vz) {
         const double t0 = q[kH][0], r0 = q[kH][1];
         const double V0[3] = {r0 * q[kH][2], r0 * q[kH][3], r0 * q[kH][4]};
         double adv = 0.0, lap = 0.0, duz = 0.0, divV = 0.0;
@@ -173,8 +207,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_wc_t(Geo g, Coef<double> co, co
         dir(vz, 2, zm.az, zm.bz, true);
         const double e = -(0.5 * fma(t0, divV, adv)) + a.visc * (fma(-zm.bsum, t0, lap) - zm.c2k * duz);
         const double d = a.dt * e;
-        const double q0 = STAGE == 0 ? t0 : a.Q0[idx];
-        const double acc = (STAGE == 0 ? r0 * q0 : a.acc[idx]) + rk4w(STAGE) * d;
+        const double q0 = STAGE == 0 ? t0 : q0c;
+        const double acc = (STAGE == 0 ? r0 * q0 : accc) + rk4w(STAGE) * d;
         const double ir = 1.0 / r0;  // the divisions by rho below as products (within an ulp)
         if (STAGE < 3) {
             a.acc[idx] = acc;
