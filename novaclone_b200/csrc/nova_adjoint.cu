@@ -32,15 +32,22 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
         return a.G[(long long)(c - 3) * g.N3 + o];
     };
     const Walls<T> wl{};  // the adjoint is built for periodic meshes
-    tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
-                                                  const auto &vz) {
-        double mu[3];
-        T lam[3] = {0, 0, 0};
+    // the pointwise operands (mu, lambda) of the next plane load while this plane computes
+    double mun[3] = {0, 0, 0}, mu[3];
+    T lamn[3] = {0, 0, 0}, lam[3];
+    auto pre = [&](long long nidx, bool load) {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            mu[c] = a.mu[(long long)c * g.N3 + idx];
-            if (S != 4) lam[c] = a.Lam[(long long)c * g.N3 + idx];
+            mu[c] = mun[c];
+            lam[c] = lamn[c];
+            if (load) {
+                mun[c] = a.mu[(long long)c * g.N3 + nidx];
+                if (S != 4) lamn[c] = a.Lam[(long long)c * g.N3 + nidx];
+            }
         }
+    };
+    tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, pre, [&](long long idx, auto &q, const auto &vx,
+                                                       const auto &vy, const auto &vz) {
         const T y0[3] = {q[H][0], q[H][1], q[H][2]};
         const T g0[3] = {q[H][3], q[H][4], q[H][5]};
         T xi[3];
@@ -105,8 +112,24 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
         return a.G[(long long)(c - 3) * g.N3 + o];
     };
     const Walls<T> wl{};
-    tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, [&](long long idx, auto &q, const auto &vx, const auto &vy,
-                                                  const auto &vz) {
+    // the pointwise operands of the next plane load while this plane computes:
+    // BB mu and lambda, UB and BU the FP64 accumulator they add to
+    double pn[3] = {0, 0, 0}, pc[3];
+    T lamn[3] = {0, 0, 0}, lamc[3];
+    auto pre = [&](long long nidx, bool load) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            pc[c] = pn[c];
+            lamc[c] = lamn[c];
+            if (load) {
+                const long long o = (long long)c * g.N3 + nidx;
+                pn[c] = KIND == ADJ_BB ? a.mu[o] : acc[o];
+                if (KIND == ADJ_BB && S != 4) lamn[c] = a.Lam[o];
+            }
+        }
+    };
+    tile_march<T, H, 6, false>(g, wl, sm, ld, ib, ie, pre, [&](long long idx, auto &q, const auto &vx,
+                                                       const auto &vy, const auto &vz) {
         const T p0[3] = {q[H][0], q[H][1], q[H][2]};
         const T g0[3] = {q[H][3], q[H][4], q[H][5]};
         T Sx[3], At[3], divP, divG;
@@ -117,11 +140,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
             const long long o = (long long)e * g.N3 + idx;
             if constexpr (KIND == ADJ_BB) {
                 const T xi = dt * (Sx[e] + T(0.5) * fma(-g0[e], divP, At[e]) - visc * bsum * g0[e]);
-                adj_store<T, S>(a, o, a.mu[o], S == 4 ? T(0) : a.Lam[o], xi);
+                adj_store<T, S>(a, o, pc[e], S == 4 ? T(0) : lamc[e], xi);
             } else if constexpr (KIND == ADJ_UB) {
-                acc[o] += (double)(dt * (fma(T(0.5) * g0[e], divP, -Sx[e]) + fma(T(0.5), At[e], p0[e] * divG)));
+                acc[o] = pc[e] + (double)(dt * (fma(T(0.5) * g0[e], divP, -Sx[e]) + fma(T(0.5), At[e], p0[e] * divG)));
             } else {
-                acc[o] += (double)(dt * (fma(T(0.5) * g0[e], divP, -Sx[e]) - T(0.5) * At[e]));
+                acc[o] = pc[e] + (double)(dt * (fma(T(0.5) * g0[e], divP, -Sx[e]) - T(0.5) * At[e]));
             }
         }
     });
