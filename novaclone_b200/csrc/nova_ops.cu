@@ -198,7 +198,7 @@ constexpr int kRedThreads = 256;
 // the divergence maxima and U_x cover every stored node (tools::maximum,
 // src/Tools/Tools.h:19-36; tools::CFL, src/Tools/Tools.cpp:15-25).
 template <int H, int NC, class LD, bool WALLS>
-__global__ void __launch_bounds__(kThreads) k_diag_tiled(Geo g, Walls<double> wl, Coef<double> co,
+__global__ void __launch_bounds__(kThreads, NC == 3 ? 2 : 1) k_diag_tiled(Geo g, Walls<double> wl, Coef<double> co,
                                                          const double *__restrict__ ia, LD U, LD B, int ichunk,
                                                          double *__restrict__ part)
 {
