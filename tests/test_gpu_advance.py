@@ -1,6 +1,6 @@
 """GPU parity of the fused time advance (nova_advance) against the oracle and
 the reference's golden vectors: FP64 relative L2 error per field <= 1e-11
-after N steps (the survey's parity bar), the diagnostics history overlaid,
+after N steps (the FP64 parity bar), the diagnostics history overlaid,
 and the FP32-split path's error against FP64 stated and bounded."""
 import os
 import subprocess
