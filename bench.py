@@ -539,11 +539,13 @@ def hbm_roof(alg_bytes, sec, what):
 # of every input stream and one write of every output stream per fused pass;
 # projection = divergence 3s+8, spectral solve 32, correction 8+3s+3s):
 #   shear-layer loop (app/shearLayer/UEqn.H), per stage: the stage kernel
-#   reads the stage state and the base and writes U* (FP64 72, split 60), then
-#   a projection (120 either way; split reads and writes (hi, lo) pairs);
-#   the wall Poisson solve on the even extension moves twice the spectral bytes
+#   reads the stage state and the base and writes U* (FP64 72, split 60: U*
+#   leaves in FP64 either way), then a projection of 136: the divergence 32,
+#   the wall Poisson solve 48 (2-D (i, k) transform of the stored rows, the
+#   DCT-I pass along y, the inverse transform: one read and one write of the
+#   spectrum each) and the correction 56 (the split one writes the (hi, lo) pair)
 SHEAR_STAGE_BYTES = {"f64": 72.0, "f32split": 60.0}
-SHEAR_STEP_BYTES = {k: 4 * (v + 32 + 64 + 56) for k, v in SHEAR_STAGE_BYTES.items()}
+SHEAR_STEP_BYTES = {k: 4 * (v + 32 + 48 + 56) for k, v in SHEAR_STAGE_BYTES.items()}
 #   MHD jet, the app's scheme (literal U loop: one stage reading U, B and
 #   writing U*; projection; classical B loop with U frozen: 96, 144, 144, 96
 #   FP64 / 48, 72, 72, 84 split; cleaning projection)
