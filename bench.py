@@ -592,8 +592,8 @@ def shear_leg(args, nova, torch, dist, world):
                           "roofline": hbm_roof(SHEAR_STEP_BYTES[prec_name] * npts * steps, sec,
                                                "whole step, %g B/point-step" % SHEAR_STEP_BYTES[prec_name]),
                           "stage_kernel": hbm_roof(SHEAR_STAGE_BYTES[prec_name] * npts * st_n, st_ms / 1e3,
-                                                   "shear-loop stage kernel (march, walls), %g B/point"
-                                                   % SHEAR_STAGE_BYTES[prec_name])}
+                                                   "shear-loop stage kernel (walls; FP64 on the march, split on "
+                                                   "the TMA pipeline), %g B/point" % SHEAR_STAGE_BYTES[prec_name])}
         finals[prec_name] = U.download_soa()
         U.close()
         p.close()
